@@ -1,0 +1,1060 @@
+/*
+ * hs_oracle.c -- CPU FP64 restatement of hsolver's SIMPLE conjugate-heat-
+ * transfer outer step (the path SolverSolve -> FluidSolver::solve ->
+ * MobSolver::solve -> interface swap -> setForNext).
+ *
+ * TEST INFRASTRUCTURE ONLY.  This file is the parity oracle: it is imported
+ * by tests/, by __graft_entry__.smoke() as the checker, and by bench.py's
+ * cpu_baseline / --impl reference leg.  The product (hsolver_b200/) never
+ * links or calls it.
+ *
+ * Parity pin: the restatement is checked bit-for-bit against the reference's
+ * own sources compiled by oracle/ref/Makefile (single-rank shims for MPI,
+ * HYPRE IJ/PCG and Scotch), see tests/golden/.  The HYPRE PCG itself is a
+ * restatement of HYPRE 2.27.0's pcg.c algorithm (not vendored in the
+ * reference), so the pressure-correction solve is pinned only through the
+ * reference's own call site (fluid_solver.h:1758-1811, 1871-1875).
+ *
+ * Everything is sequential and in the reference's loop order, so the
+ * arithmetic (operation order, no FMA contraction: build with
+ * -ffp-contract=off) is the reference's.  Index conventions follow the
+ * reference: "padded" arrays carry one ghost layer on each side and are
+ * x-fastest, i + j*nx + k*nx*ny (distributed_mesh.h:332-338).
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+typedef int64_t I64;
+
+/* ------------------------------------------------------------------ */
+/* parameters (reference macros: fluid_solver.h:21-37, mobs_solver.h:15-29) */
+typedef struct {
+  double nu;          /* NU 0.001 */
+  double rho;         /* RHO 1 */
+  double alpha;       /* ALPHA 0.001 (fluid thermal diffusivity) */
+  double u_lid;       /* U0 0.1 */
+  double relax;       /* UNDER_RELAX 0.3 (fluid) */
+  double relax_solid; /* UNDER_RELAX 0.3 (mobs_solver.h:27) */
+  double mom_tol;     /* CONVERGENCE 2e-3 (fluid_solver.h:27) */
+  double energy_tol;  /* CONVERGENCE 2e-3 (fluid_solver.h:27, used by solveTemp) */
+  double solid_tol;   /* CONVERGENCE2 1e-3 (mobs_solver.h:22) */
+  int gs_max;         /* GS_STEP 100 */
+  double t_fluid0;    /* 293: t_temp init (fluid_solver.h:108) */
+  double t_wall;      /* 293: boundary cell output (fluid_solver.h:401) */
+  double t_solid0;    /* T1 333 (mobs_solver.h:18,55) */
+  double pcg_tol;     /* 1e-5 (fluid_solver.h:1874) */
+  int pcg_maxiter;    /* 1000 (fluid_solver.h:1873) */
+  int frozen_matrix;  /* 1: reference behaviour (values1d read from start, fluid_solver.h:2188-2193) */
+} or_params;
+
+void or_params_default(or_params *p) {
+  p->nu = 0.001; p->rho = 1; p->alpha = 0.001; p->u_lid = 0.1;
+  p->relax = 0.3; p->relax_solid = 0.3;
+  p->mom_tol = 2e-3; p->energy_tol = 2e-3; p->solid_tol = 1e-3;
+  p->gs_max = 100; p->t_fluid0 = 293; p->t_wall = 293; p->t_solid0 = 333;
+  p->pcg_tol = 1e-5; p->pcg_maxiter = 1000; p->frozen_matrix = 1;
+}
+
+/* ------------------------------------------------------------------ */
+/* deck (".in") parsing -- StructuredMesh::readMesh, mesh/mesh.cpp:1616-1796 */
+
+typedef struct {
+  int nx_pts, ny_pts, nz_pts;
+  double *xs, *ys, *zs;
+  int nmobs; int (*mobs)[6];
+  int nwalls; int (*walls)[8];
+  int nholes; int (*holes)[13];
+} or_deck;
+
+static char err_buf[512];
+const char *or_last_error(void) { return err_buf; }
+
+/* Parse "value<sep>" pairs from one comment-stripped line the way
+ * `while (lineiss >> value >> spliter)` does (mesh/mesh.cpp:1677): a value
+ * followed by end-of-line (no separator) is dropped. */
+static int parse_line_doubles(const char *s, size_t n, double **out, int *cnt, int *cap) {
+  char buf[4096];
+  size_t m = n < sizeof(buf) - 1 ? n : sizeof(buf) - 1;
+  memcpy(buf, s, m); buf[m] = 0;
+  char *q = strchr(buf, ';');               /* sliceInputString, mesh/mesh.cpp:27-40 */
+  if (q) *q = 0;
+  char *p = buf;
+  for (;;) {
+    while (*p == ' ' || *p == '\t' || *p == '\r' || *p == '\v' || *p == '\f') p++;
+    if (!*p) break;
+    /* only decimal floating forms, like std::num_get */
+    if (!((*p >= '0' && *p <= '9') || *p == '-' || *p == '+' || *p == '.')) break;
+    char *e; double v = strtod(p, &e);
+    if (e == p) break;
+    p = e;
+    while (*p == ' ' || *p == '\t' || *p == '\r' || *p == '\v' || *p == '\f') p++;
+    if (!*p) break;                          /* no separator -> value dropped */
+    p++;                                     /* consume one separator char */
+    if (*cnt == *cap) { *cap = *cap ? 2 * *cap : 64; *out = (double *)realloc(*out, sizeof(double) * (size_t)*cap); }
+    (*out)[(*cnt)++] = v;
+  }
+  return 0;
+}
+
+static int parse_line_ints(const char *s, size_t n, int *vals, int maxv) {
+  char buf[4096];
+  size_t m = n < sizeof(buf) - 1 ? n : sizeof(buf) - 1;
+  memcpy(buf, s, m); buf[m] = 0;
+  char *q = strchr(buf, ';');
+  if (q) *q = 0;
+  char *p = buf; int cnt = 0;
+  for (;;) {
+    while (*p == ' ' || *p == '\t' || *p == '\r' || *p == '\v' || *p == '\f') p++;
+    if (!*p) break;
+    if (!((*p >= '0' && *p <= '9') || *p == '-' || *p == '+')) break;
+    char *e; long v = strtol(p, &e, 10);
+    if (e == p) break;
+    p = e;
+    while (*p == ' ' || *p == '\t' || *p == '\r' || *p == '\v' || *p == '\f') p++;
+    if (!*p) break;
+    p++;
+    if (cnt < maxv) vals[cnt] = (int)v;
+    cnt++;
+  }
+  return cnt;
+}
+
+/* Section [pos, pos+len) of `content` per the reference's substring rules
+ * (mesh/mesh.cpp:1662-1671): starts after the first '=' following the key,
+ * runs `next_key_pos - key_pos` characters (or to the end for the last key). */
+static void section_range(const char *content, size_t clen, long key_pos, const long *sorted, int nsorted,
+                          size_t *beg, size_t *len) {
+  const char *eq = strchr(content + key_pos, '=');
+  size_t xstart = eq ? (size_t)(eq - (content + key_pos)) : 0;
+  long endIndex = -1;
+  for (int i = 0; i < nsorted; ++i)
+    if (sorted[i] == key_pos && i != nsorted - 1) { endIndex = i + 1; break; }
+  size_t length;
+  if (endIndex < 0) length = clen - xstart - 2;
+  else length = (size_t)(sorted[endIndex] - key_pos);
+  size_t b = (size_t)key_pos + xstart + 1;
+  if (b > clen) b = clen;
+  if (b + length > clen) length = clen - b;
+  *beg = b; *len = length;
+}
+
+static void foreach_line(const char *content, size_t beg, size_t len, void (*cb)(const char *, size_t, void *), void *ud) {
+  size_t i = beg, end = beg + len;
+  while (i < end) {
+    size_t j = i;
+    while (j < end && content[j] != '\n') j++;
+    cb(content + i, j - i, ud);
+    i = j + 1;
+  }
+}
+
+typedef struct { double **out; int *cnt; int *cap; } dl_ud;
+static void cb_doubles(const char *s, size_t n, void *ud) {
+  dl_ud *u = (dl_ud *)ud; parse_line_doubles(s, n, u->out, u->cnt, u->cap);
+}
+typedef struct { or_deck *d; int kind; } il_ud;
+static void cb_ints(const char *s, size_t n, void *ud) {
+  il_ud *u = (il_ud *)ud; int v[32]; int c = parse_line_ints(s, n, v, 32);
+  or_deck *d = u->d;
+  if (u->kind == 0) {            /* mobs: any non-empty line (mesh/mesh.cpp:1754) */
+    if (c == 0) return;
+    if (c < 6) { d->nmobs = -1000000; return; }
+    d->mobs = realloc(d->mobs, sizeof(int[6]) * (size_t)(d->nmobs + 1));
+    for (int i = 0; i < 6; ++i) d->mobs[d->nmobs][i] = v[i];
+    d->nmobs++;
+  } else if (u->kind == 1) {     /* walls: exactly 8 values (mesh/mesh.cpp:1774) */
+    if (c != 8) return;
+    d->walls = realloc(d->walls, sizeof(int[8]) * (size_t)(d->nwalls + 1));
+    for (int i = 0; i < 8; ++i) d->walls[d->nwalls][i] = v[i];
+    d->nwalls++;
+  } else {                       /* holes: exactly 13 values (mesh/mesh.cpp:1794) */
+    if (c != 13) return;
+    d->holes = realloc(d->holes, sizeof(int[13]) * (size_t)(d->nholes + 1));
+    for (int i = 0; i < 13; ++i) d->holes[d->nholes][i] = v[i];
+    d->nholes++;
+  }
+}
+
+static int cmp_long(const void *a, const void *b) {
+  long x = *(const long *)a, y = *(const long *)b; return (x > y) - (x < y);
+}
+
+int or_deck_parse(const char *content, or_deck *d) {
+  memset(d, 0, sizeof(*d));
+  size_t clen = strlen(content);
+  const char *keys[6] = {"xgrid", "ygrid", "zgrid", "mobs", "walls", "holes"};
+  long pos[6];
+  for (int i = 0; i < 6; ++i) {
+    const char *f = strstr(content, keys[i]);
+    if (!f) { snprintf(err_buf, sizeof err_buf, "deck: section '%s' missing", keys[i]); return -1; }
+    pos[i] = (long)(f - content);
+  }
+  long sorted[6]; memcpy(sorted, pos, sizeof pos); qsort(sorted, 6, sizeof(long), cmp_long);
+  double **arr[3] = {&d->xs, &d->ys, &d->zs}; int *cnts[3] = {&d->nx_pts, &d->ny_pts, &d->nz_pts};
+  for (int a = 0; a < 3; ++a) {
+    size_t b, l; section_range(content, clen, pos[a], sorted, 6, &b, &l);
+    int cap = 0; dl_ud u = {arr[a], cnts[a], &cap};
+    foreach_line(content, b, l, cb_doubles, &u);
+  }
+  for (int kind = 0; kind < 3; ++kind) {
+    size_t b, l; section_range(content, clen, pos[3 + kind], sorted, 6, &b, &l);
+    il_ud u = {d, kind}; foreach_line(content, b, l, cb_ints, &u);
+  }
+  if (d->nmobs < 0) { snprintf(err_buf, sizeof err_buf, "deck: mobs line with fewer than 6 values"); return -1; }
+  if (d->nx_pts < 2 || d->ny_pts < 2 || d->nz_pts < 2) { snprintf(err_buf, sizeof err_buf, "deck: grid needs >=2 points per axis"); return -1; }
+  return 0;
+}
+
+void or_deck_free(or_deck *d) { free(d->xs); free(d->ys); free(d->zs); free(d->mobs); free(d->walls); free(d->holes); memset(d, 0, sizeof(*d)); }
+
+/* ------------------------------------------------------------------ */
+/* mesh classification: cell type (mesh/mesh.cpp:84-114), wall faces
+ * (mesh/mesh.cpp:116-237), connected regions (mesh/mesh.cpp:298-454, 1583-1604) */
+
+typedef struct {
+  I64 Nx, Ny, Nz, NxP, NyP, NzP;
+  unsigned char *ctype;           /* Nx*Ny*Nz, 0 fluid 1 obstacle */
+  unsigned char *wx, *wy, *wz;    /* wall flags per x/y/z face: NxP*Ny*Nz, Nx*NyP*Nz, Nx*Ny*NzP */
+  int *region;                    /* region id within its type */
+  int nfluid_regions, nsolid_regions;
+} or_mesh;
+
+#define CID(i, j, k) ((i) + (j) * m->Nx + (k) * m->Nx * m->Ny)          /* 0-based cell */
+#define FXID(i, j, k) ((i) + (j) * m->NxP + (k) * m->NxP * m->Ny)      /* 0-based x-face (i in 0..Nx) */
+#define FYID(i, j, k) ((i) + (j) * m->Nx + (k) * m->Nx * m->NyP)
+#define FZID(i, j, k) ((i) + (j) * m->Nx + (k) * m->Nx * m->Ny)
+
+int or_mesh_build(const or_deck *d, or_mesh *m) {
+  memset(m, 0, sizeof(*m));
+  m->NxP = d->nx_pts; m->NyP = d->ny_pts; m->NzP = d->nz_pts;
+  m->Nx = m->NxP - 1; m->Ny = m->NyP - 1; m->Nz = m->NzP - 1;
+  I64 N = m->Nx * m->Ny * m->Nz;
+  m->ctype = calloc((size_t)N, 1);
+  for (I64 k = 1; k <= m->Nz; ++k)
+    for (I64 j = 1; j <= m->Ny; ++j)
+      for (I64 i = 1; i <= m->Nx; ++i)
+        for (int b = 0; b < d->nmobs; ++b) {
+          const int *mb = d->mobs[b];
+          if (i >= mb[0] && i <= mb[1] && j >= mb[2] && j <= mb[3] && k >= mb[4] && k <= mb[5]) {
+            m->ctype[CID(i - 1, j - 1, k - 1)] = 1; break;
+          }
+        }
+  m->wx = calloc((size_t)(m->NxP * m->Ny * m->Nz), 1);
+  m->wy = calloc((size_t)(m->Nx * m->NyP * m->Nz), 1);
+  m->wz = calloc((size_t)(m->Nx * m->Ny * m->NzP), 1);
+  for (I64 k = 0; k < m->Nz; ++k) for (I64 j = 0; j < m->Ny; ++j) { m->wx[FXID(0, j, k)] = 1; m->wx[FXID(m->Nx, j, k)] = 1; }
+  for (I64 k = 0; k < m->Nz; ++k) for (I64 i = 0; i < m->Nx; ++i) { m->wy[FYID(i, 0, k)] = 1; m->wy[FYID(i, m->Ny, k)] = 1; }
+  for (I64 j = 0; j < m->Ny; ++j) for (I64 i = 0; i < m->Nx; ++i) { m->wz[FZID(i, j, 0)] = 1; m->wz[FZID(i, j, m->Nz)] = 1; }
+  for (int w = 0; w < d->nwalls; ++w) {
+    const int *wl = d->walls[w];
+    int i0 = wl[0], i1 = wl[1], j0 = wl[2], j1 = wl[3], k0 = wl[4], k1 = wl[5];
+    if (i0 == i1 && i0 >= 1 && i0 <= m->NxP)
+      for (I64 j = 1; j <= m->Ny; ++j) for (I64 k = 1; k <= m->Nz; ++k)
+        if (j >= j0 && j <= j1 && k >= k0 && k <= k1) m->wx[FXID(i0 - 1, j - 1, k - 1)] = 1;
+    if (j0 == j1 && j0 >= 1 && j0 <= m->NyP)
+      for (I64 i = 1; i <= m->Nx; ++i) for (I64 k = 1; k <= m->Nz; ++k)
+        if (i >= i0 && i <= i1 && k >= k0 && k <= k1) m->wy[FYID(i - 1, j0 - 1, k - 1)] = 1;
+    if (k0 == k1 && k0 >= 1 && k0 <= m->NzP)
+      for (I64 i = 1; i <= m->Nx; ++i) for (I64 j = 1; j <= m->Ny; ++j)
+        if (i >= i0 && i <= i1 && j >= j0 && j <= j1) m->wz[FZID(i - 1, j - 1, k0 - 1)] = 1;
+  }
+  /* connected components of same-type cells through non-wall faces; ids in
+   * order of the lowest cell index (BFS started from increasing indices) */
+  m->region = malloc(sizeof(int) * (size_t)N);
+  for (I64 c = 0; c < N; ++c) m->region[c] = -1;
+  I64 *queue = malloc(sizeof(I64) * (size_t)N);
+  int nreg[2] = {0, 0};
+  for (I64 s = 0; s < N; ++s) {
+    if (m->region[s] >= 0) continue;
+    int t = m->ctype[s]; int id = nreg[t]++;
+    I64 qh = 0, qt = 0; queue[qt++] = s; m->region[s] = id;
+    while (qh < qt) {
+      I64 c = queue[qh++];
+      I64 i = c % m->Nx, j = (c / m->Nx) % m->Ny, k = c / (m->Nx * m->Ny);
+      I64 nb[6]; int ok[6];
+      nb[0] = c - 1; ok[0] = i > 0 && !m->wx[FXID(i, j, k)];
+      nb[1] = c + 1; ok[1] = i < m->Nx - 1 && !m->wx[FXID(i + 1, j, k)];
+      nb[2] = c - m->Nx; ok[2] = j > 0 && !m->wy[FYID(i, j, k)];
+      nb[3] = c + m->Nx; ok[3] = j < m->Ny - 1 && !m->wy[FYID(i, j + 1, k)];
+      nb[4] = c - m->Nx * m->Ny; ok[4] = k > 0 && !m->wz[FZID(i, j, k)];
+      nb[5] = c + m->Nx * m->Ny; ok[5] = k < m->Nz - 1 && !m->wz[FZID(i, j, k + 1)];
+      for (int n = 0; n < 6; ++n)
+        if (ok[n] && m->region[nb[n]] < 0 && m->ctype[nb[n]] == t) { m->region[nb[n]] = id; queue[qt++] = nb[n]; }
+    }
+  }
+  free(queue);
+  m->nfluid_regions = nreg[0]; m->nsolid_regions = nreg[1];
+  return 0;
+}
+
+void or_mesh_free(or_mesh *m) { free(m->ctype); free(m->wx); free(m->wy); free(m->wz); free(m->region); memset(m, 0, sizeof(*m)); }
+
+/* ------------------------------------------------------------------ */
+/* solver state */
+
+typedef struct {
+  I64 cx, cy, cz, fx, fy, fz, ox, oy, oz;  /* metadata (distributed_mesh.h:152-154), 1-based offsets */
+} or_meta;
+
+typedef struct {
+  or_meta md;
+  unsigned char *empty;        /* cx*cy*cz */
+  double *t;                   /* cell output (cx*cy*cz) */
+  double *t_temp;              /* padded (cx+2)(cy+2)(cz+2) */
+  int sweeps;                  /* last solveTemperature sweep count */
+  double residual;
+} or_solid;
+
+typedef struct {
+  or_meta md;
+  unsigned char *empty;                        /* cx*cy*cz */
+  double *p, *t;                               /* LocalCell data (cx*cy*cz) */
+  double *ux, *uy, *uz;                        /* LocalFace u (fx*cy*cz, cx*fy*cz, cx*cy*fz) */
+  int *id;                                     /* HYPRE row id per cell (-1 empty) */
+  double *u_star, *v_star, *w_star, *up, *vp, *wp, *p_temp, *p_prime, *t_temp;
+  /* per padded-index geometry (fluid_solver.h:1248-1261) */
+  double *xp, *xw, *xe, *yp, *ys, *yn, *zp, *zf, *zb;
+  /* frozen pressure-correction coefficients per cell (fluid_solver.h:1990-1995) */
+  int have_matrix;
+  double *acx, *acy, *acz;
+  double *b, *x, *r, *pv, *s;                  /* CG work, padded-cell shaped */
+  /* stats */
+  int sweeps_u, sweeps_v, sweeps_w, sweeps_t;
+  double res_u, res_v, res_w, res_t;
+  int pcg_iters; double pcg_relres;
+  I64 nfluid;
+} or_fluid;
+
+typedef struct { I64 f_send, f_recv, s_send, s_recv; int region; } or_swap;
+
+typedef struct {
+  or_params prm;
+  or_deck deck;
+  or_mesh mesh;
+  or_fluid fl;
+  int nsolid; or_solid *sol;
+  I64 nswap; or_swap *swap;
+  int inited;
+  long steps;
+} or_case;
+
+#define PIDX(md, i, j, k, nx, ny) ((i) + (j) * (nx) + (k) * (nx) * (ny))
+/* fluid padded index helpers (fluid_solver.h:184-207) */
+#define IU(i, j, k) ((i) + (j) * (F->md.fx + 2) + (k) * (F->md.fx + 2) * (F->md.cy + 2))
+#define IV(i, j, k) ((i) + (j) * (F->md.cx + 2) + (k) * (F->md.cx + 2) * (F->md.fy + 2))
+#define IW(i, j, k) ((i) + (j) * (F->md.cx + 2) + (k) * (F->md.cx + 2) * (F->md.cy + 2))
+#define IP(i, j, k) ((i) + (j) * (F->md.cx + 2) + (k) * (F->md.cx + 2) * (F->md.cy + 2))
+#define GC(i, j, k) ((i) + (j) * F->md.cx + (k) * F->md.cx * F->md.cy)
+#define GX(i, j, k) ((i) + (j) * F->md.fx + (k) * F->md.fx * F->md.cy)
+#define GY(i, j, k) ((i) + (j) * F->md.cx + (k) * F->md.cx * F->md.fy)
+#define GZ(i, j, k) ((i) + (j) * F->md.cx + (k) * F->md.cx * F->md.cy)
+
+static double maxd(double a, double b) { return a < b ? b : a; }  /* std::max */
+
+/* ---- boundary conditions: fluid_solver.h:209-405 ------------------------ */
+static void applyX(or_case *C) {
+  or_fluid *F = &C->fl; or_meta *md = &F->md; or_mesh *m = &C->mesh;
+  I64 cx = md->cx, cy = md->cy, cz = md->cz, fx = md->fx;
+  if (md->ox == 1) {
+    for (I64 k = 0; k < cz + 2; ++k) for (I64 j = 0; j < cy + 2; ++j) {
+      F->u_star[IU(0, j, k)] = 0; F->v_star[IV(0, j, k)] = 0; F->w_star[IW(0, j, k)] = 0;
+    }
+  } else if (md->ox - 1 + fx == m->Nx + 1) {
+    for (I64 k = 0; k < cz + 2; ++k) for (I64 j = 0; j < cy + 2; ++j) {
+      F->u_star[IU(fx + 1, j, k)] = 0; F->v_star[IV(cx + 1, j, k)] = 0; F->w_star[IW(cx + 1, j, k)] = 0;
+    }
+  }
+  for (I64 k = 0; k < cz; ++k) for (I64 j = 0; j < cy; ++j)
+    if (md->ox - 1 + fx - 1 == m->Nx) { F->ux[GX(fx - 1, j, k)] = 0; F->u_star[IU(fx, j + 1, k + 1)] = 0; }
+}
+
+static void applyZ(or_case *C) {
+  or_fluid *F = &C->fl; or_meta *md = &F->md; or_mesh *m = &C->mesh;
+  I64 cx = md->cx, cy = md->cy, cz = md->cz, fz = md->fz;
+  if (md->oz == 1) {
+    for (I64 j = 0; j < cy + 2; ++j) for (I64 i = 0; i < cx + 2; ++i) {
+      F->u_star[IU(i, j, 0)] = 0; F->v_star[IV(i, j, 0)] = 0; F->w_star[IW(i, j, 0)] = 0;
+    }
+  } else if (md->oz - 1 + fz == m->Nz + 1) {
+    for (I64 j = 0; j < cy + 2; ++j) for (I64 i = 0; i < cx + 2; ++i) {
+      F->u_star[IU(i, j, cz + 1)] = 0; F->v_star[IV(i, j, cz + 1)] = 0; F->w_star[IW(i, j, fz + 1)] = 0;
+    }
+  }
+  for (I64 j = 0; j < cy; ++j) for (I64 i = 0; i < cx; ++i)
+    if (md->oz - 1 + fz - 1 == m->Nz) { F->uz[GZ(i, j, fz - 1)] = 0; F->w_star[IW(i + 1, j + 1, fz)] = 0; }
+}
+
+static void applyY(or_case *C) {
+  or_fluid *F = &C->fl; or_meta *md = &F->md; or_mesh *m = &C->mesh;
+  I64 cx = md->cx, cy = md->cy, cz = md->cz, fy = md->fy;
+  double U0 = C->prm.u_lid;
+  if (md->oy == 1) {
+    for (I64 k = 0; k < cz + 2; ++k) for (I64 i = 0; i < cx + 2; ++i) {
+      F->u_star[IU(i, 0, k)] = 0; F->v_star[IV(i, 0, k)] = 0; F->w_star[IW(i, 0, k)] = 0;
+    }
+  } else if (md->oy - 1 + fy == m->Ny + 1) {
+    for (I64 k = 0; k < cz + 2; ++k) for (I64 i = 0; i < cx + 2; ++i) {
+      F->u_star[IU(i, cy + 1, k)] = U0; F->v_star[IV(i, fy + 1, k)] = 0; F->w_star[IW(i, cy + 1, k)] = 0;
+    }
+  }
+  for (I64 k = 0; k < cz; ++k) for (I64 i = 0; i < cx; ++i)
+    if (md->oy - 1 + fy - 1 == m->Ny) {
+      F->uy[GY(i, fy - 1, k)] = 0; F->v_star[IV(i + 1, fy, k + 1)] = 0;
+      F->ux[GX(i, cy - 1, k)] = U0; F->u_star[IU(i + 1, cy, k + 1)] = U0;
+    }
+}
+
+static void applyCell(or_case *C) {
+  or_fluid *F = &C->fl; or_meta *md = &F->md; or_mesh *m = &C->mesh;
+  I64 cx = md->cx, cy = md->cy, cz = md->cz;
+  double *p = F->p, *pt = F->p_temp;
+  for (I64 k = 0; k < cz; ++k) for (I64 j = 0; j < cy; ++j) for (I64 i = 0; i < cx; ++i) {
+    I64 gx = i + md->ox - 1, gy = j + md->oy - 1, gz = k + md->oz - 1;
+    if (gx == 0) p[GC(i, j, k)] = p[GC(i + 1, j, k)];
+    else if (gx == m->Nx - 1) p[GC(i, j, k)] = p[GC(i - 1, j, k)];
+    else if (gy == 0) p[GC(i, j, k)] = p[GC(i, j + 1, k)];
+    else if (gy == m->Ny - 1) p[GC(i, j, k)] = p[GC(i, j - 1, k)];
+    else if (gz == 0) p[GC(i, j, k)] = p[GC(i, j, k + 1)];
+    else if (gz == m->Nz - 1) p[GC(i, j, k)] = p[GC(i, j, k - 1)];
+    double v = p[GC(i, j, k)];
+    if (gx == 0) { pt[IP(i + 1, j + 1, k + 1)] = v; pt[IP(i, j + 1, k + 1)] = v; }
+    else if (gx == m->Nx - 1) { pt[IP(i + 1, j + 1, k + 1)] = v; pt[IP(i + 2, j + 1, k + 1)] = v; }
+    else if (gy == 0) { pt[IP(i + 1, j + 1, k + 1)] = v; pt[IP(i + 1, j, k + 1)] = v; }
+    else if (gy == m->Ny - 1) {
+      pt[IP(i + 1, j + 1, k + 1)] = v; pt[IP(i + 1, j + 2, k + 1)] = v;
+      if (i + 1 == cx) pt[IP(i + 2, j + 2, k + 1)] = v;
+      if (k + 1 == cz) pt[IP(i + 1, j + 2, k + 2)] = v;
+      if (i + 1 == 1) pt[IP(i, j + 2, k + 1)] = v;
+      if (k + 1 == 1) pt[IP(i + 1, j + 2, k)] = v;
+      if (i + 1 == cx && k + 1 == cz) pt[IP(i + 2, j + 2, k + 2)] = v;
+      if (i + 1 == 1 && k + 1 == 1) pt[IP(i, j + 2, k)] = v;
+    } else if (gz == 0) { pt[IP(i + 1, j + 1, k + 1)] = v; pt[IP(i + 1, j + 1, k)] = v; }
+    else if (gz == m->Nz - 1) { pt[IP(i + 1, j + 1, k + 1)] = v; pt[IP(i + 1, j + 1, k + 2)] = v; }
+  }
+  p[GC(0, 0, 0)] = 0;
+  for (I64 k = 0; k < cz; ++k) for (I64 j = 0; j < cy; ++j) for (I64 i = 0; i < cx; ++i) {
+    I64 gx = i + md->ox - 1, gy = j + md->oy - 1, gz = k + md->oz - 1;
+    if (gx == 0 || gy == 0 || gz == 0 || gx == m->Nx - 1 || gz == m->Nz - 1 || gy == m->Ny - 1)
+      F->t[GC(i, j, k)] = C->prm.t_wall;
+  }
+}
+
+/* ---- momentum GS: fluid_solver.h:407-659 ------------------------------- */
+static void solveX(or_case *C) {
+  or_fluid *F = &C->fl; or_meta *md = &F->md; const or_params *P = &C->prm;
+  double *u = F->u_star, *v = F->v_star, *w = F->w_star, *pt = F->p_temp;
+  I64 xs = 1, xe_ = md->fx, ys_ = 1, ye = md->cy, zs = 1, ze = md->cz;
+  double residual = 1, gres = residual; int step = 0;
+  while (step < P->gs_max) {
+    if (gres < P->mom_tol) break;
+    for (I64 k = zs; k <= ze; ++k) for (I64 j = ys_; j <= ye; ++j) for (I64 i = xs; i <= xe_ - 1; ++i) {
+      if (F->empty[GC(i - 1, j - 1, k - 1)]) continue;
+      double xp = F->xp[i], xw = F->xw[i], xe = F->xe[i];
+      double yp = F->yp[j], ys = F->ys[j], yn = F->yn[j];
+      double zp = F->zp[k], zf = F->zf[k], zb = F->zb[k];
+      double facexy = xp * yp, facexz = xp * zp, faceyz = yp * zp;
+      double Dw = 2 * P->nu * faceyz / (xp + xw), De = 2 * P->nu * faceyz / (xp + xe);
+      double Ds = 2 * P->nu * facexz / (ys + yp), Dn = 2 * P->nu * facexz / (yn + yp);
+      double Db = 2 * P->nu * facexy / (zb + zp), Df = 2 * P->nu * facexy / (zf + zp);
+      double fw = 0.5 * P->rho * faceyz * (u[IU(i, j, k)] + u[IU(i - 1, j, k)]);
+      double fe = 0.5 * P->rho * faceyz * (u[IU(i, j, k)] + u[IU(i + 1, j, k)]);
+      double fs = 0.5 * P->rho * facexz * (v[IV(i, j, k)] + v[IV(i - 1, j, k)]);
+      double fn = 0.5 * P->rho * facexz * (v[IV(i, j + 1, k)] + v[IV(i - 1, j + 1, k)]);
+      double fb = 0.5 * P->rho * facexy * (w[IW(i, j, k + 1)] + w[IW(i - 1, j, k + 1)]);
+      double ff = 0.5 * P->rho * facexy * (w[IW(i, j, k)] + w[IW(i - 1, j, k)]);
+      double ae = De + maxd(-fe, 0.0), aw = Dw + maxd(fw, 0.0), an = Dn + maxd(-fn, 0.0);
+      double as = Ds + maxd(fs, 0.0), ab = Db + maxd(-fb, 0.0), af = Df + maxd(ff, 0.0);
+      double ap = ae + aw + an + as + ab + af;
+      double b = faceyz * (pt[IP(i - 1, j, k)] - pt[IP(i, j, k)]);
+      double old = u[IU(i, j, k)];
+      double nv = (ae * u[IU(i + 1, j, k)] + aw * u[IU(i - 1, j, k)] + an * u[IU(i, j + 1, k)] + as * u[IU(i, j - 1, k)] +
+                   af * u[IU(i, j, k - 1)] + ab * u[IU(i, j, k + 1)] + b) / ap;
+      nv = P->relax * nv + (1 - P->relax) * old;
+      u[IU(i, j, k)] = nv;
+      F->up[IU(i, j, k)] = ap;
+      residual += (nv - old) * (nv - old);
+    }
+    step++;
+    residual = residual / (double)(ze - zs + 1) / (double)(ye - ys_ + 1) / (double)(xe_ - xs + 1);
+    gres = sqrt(residual);
+    applyX(C);
+  }
+  F->sweeps_u = step; F->res_u = gres;
+}
+
+static void solveY(or_case *C) {
+  or_fluid *F = &C->fl; or_meta *md = &F->md; const or_params *P = &C->prm;
+  double *u = F->u_star, *v = F->v_star, *w = F->w_star, *pt = F->p_temp;
+  I64 xs = 1, xe_ = md->cx, ys_ = 1, ye = md->fy, zs = 1, ze = md->cz;
+  double residual = 1, gres = residual; int step = 0;
+  while (step < P->gs_max) {
+    if (gres < P->mom_tol) break;
+    for (I64 k = zs; k <= ze; ++k) for (I64 j = ys_; j <= ye - 1; ++j) for (I64 i = xs; i <= xe_; ++i) {
+      if (F->empty[GC(i - 1, j - 1, k - 1)]) continue;
+      double xp = F->xp[i], xw = F->xw[i], xe = F->xe[i];
+      double yp = F->yp[j], ys = F->ys[j], yn = F->yn[j];
+      double zp = F->zp[k], zf = F->zf[k], zb = F->zb[k];
+      double facexy = xp * yp, facexz = xp * zp, faceyz = yp * zp;
+      double Dw = 2 * P->nu * faceyz / (xp + xw), De = 2 * P->nu * faceyz / (xp + xe);
+      double Ds = 2 * P->nu * facexz / (ys + yp), Dn = 2 * P->nu * facexz / (yn + yp);
+      double Db = 2 * P->nu * facexy / (zb + zp), Df = 2 * P->nu * facexy / (zf + zp);
+      double fn = 0.5 * P->rho * facexz * (v[IV(i, j, k)] + v[IV(i, j - 1, k)]);
+      double fs = 0.5 * P->rho * facexz * (v[IV(i, j, k)] + v[IV(i, j + 1, k)]);
+      double fe = 0.5 * P->rho * faceyz * (u[IU(i, j, k)] + u[IU(i, j - 1, k)]);
+      double fw = 0.5 * P->rho * faceyz * (u[IU(i + 1, j, k)] + u[IU(i + 1, j - 1, k)]);
+      double fb = 0.5 * P->rho * facexy * (w[IW(i, j, k + 1)] + w[IW(i, j - 1, k + 1)]);
+      double ff = 0.5 * P->rho * facexy * (w[IW(i, j, k)] + w[IW(i, j - 1, k)]);
+      double ae = De + maxd(-fe, 0.0), aw = Dw + maxd(fw, 0.0), an = Dn + maxd(-fn, 0.0);
+      double as = Ds + maxd(fs, 0.0), ab = Db + maxd(-fb, 0.0), af = Df + maxd(ff, 0.0);
+      double ap = ae + aw + an + as + ab + af;
+      double b = facexz * (pt[IP(i, j - 1, k)] - pt[IP(i, j, k)]);
+      double old = v[IV(i, j, k)];
+      double nv = (ae * v[IV(i + 1, j, k)] + aw * v[IV(i - 1, j, k)] + an * v[IV(i, j + 1, k)] + as * v[IV(i, j - 1, k)] +
+                   af * v[IV(i, j, k - 1)] + ab * v[IV(i, j, k + 1)] + b) / ap;
+      nv = P->relax * nv + (1 - P->relax) * old;
+      v[IV(i, j, k)] = nv;
+      F->vp[IV(i, j, k)] = ap;
+      residual += (nv - old) * (nv - old);
+    }
+    step++;
+    residual = residual / (double)(ze - zs + 1) / (double)(ye - ys_ + 1) / (double)(xe_ - xs + 1);
+    gres = sqrt(residual);
+    applyY(C);
+  }
+  F->sweeps_v = step; F->res_v = gres;
+}
+
+static void solveZ(or_case *C) {
+  or_fluid *F = &C->fl; or_meta *md = &F->md; const or_params *P = &C->prm;
+  double *u = F->u_star, *v = F->v_star, *w = F->w_star, *pt = F->p_temp;
+  I64 xs = 1, xe_ = md->cx, ys_ = 1, ye = md->cy, zs = 1, ze = md->fz;
+  double residual = 1, gres = residual; int step = 0;
+  while (step < P->gs_max) {
+    if (gres < P->mom_tol) break;
+    for (I64 k = zs; k <= ze - 1; ++k) for (I64 j = ys_; j <= ye; ++j) for (I64 i = xs; i <= xe_; ++i) {
+      if (F->empty[GC(i - 1, j - 1, k - 1)]) continue;
+      double xp = F->xp[i], xw = F->xw[i], xe = F->xe[i];
+      double yp = F->yp[j], ys = F->ys[j], yn = F->yn[j];
+      double zp = F->zp[k], zf = F->zf[k], zb = F->zb[k];
+      double facexy = xp * yp, facexz = xp * zp, faceyz = yp * zp;
+      double Dw = 2 * P->nu * faceyz / (xp + xw), De = 2 * P->nu * faceyz / (xp + xe);
+      double Ds = 2 * P->nu * facexz / (ys + yp), Dn = 2 * P->nu * facexz / (yn + yp);
+      double Db = 2 * P->nu * facexy / (zb + zp), Df = 2 * P->nu * facexy / (zf + zp);
+      double fb = 0.5 * P->rho * facexy * (w[IW(i, j, k)] + w[IW(i, j, k - 1)]);
+      double ff = 0.5 * P->rho * facexy * (w[IW(i, j, k)] + w[IW(i, j, k + 1)]);
+      double fw = 0.5 * P->rho * faceyz * (u[IU(i, j, k)] + u[IU(i, j, k - 1)]);
+      double fe = 0.5 * P->rho * faceyz * (u[IU(i + 1, j, k)] + u[IU(i + 1, j, k - 1)]);
+      double fs = 0.5 * P->rho * facexz * (v[IV(i, j, k)] + v[IV(i, j, k - 1)]);
+      double fn = 0.5 * P->rho * facexz * (v[IV(i, j + 1, k)] + v[IV(i, j + 1, k - 1)]);
+      double ae = De + maxd(-fe, 0.0), aw = Dw + maxd(fw, 0.0), an = Dn + maxd(-fn, 0.0);
+      double as = Ds + maxd(fs, 0.0), ab = Db + maxd(-fb, 0.0), af = Df + maxd(ff, 0.0);
+      double ap = ae + aw + an + as + ab + af;
+      double b = facexy * (pt[IP(i, j, k - 1)] - pt[IP(i, j, k)]);
+      double old = w[IW(i, j, k)];
+      double nv = (ae * w[IW(i + 1, j, k)] + aw * w[IW(i - 1, j, k)] + an * w[IW(i, j + 1, k)] + as * w[IW(i, j - 1, k)] +
+                   af * w[IW(i, j, k - 1)] + ab * w[IW(i, j, k + 1)] + b) / ap;
+      nv = P->relax * nv + (1 - P->relax) * old;
+      w[IW(i, j, k)] = nv;
+      F->wp[IW(i, j, k)] = ap;
+      residual += (nv - old) * (nv - old);
+    }
+    step++;
+    residual = residual / (double)(ze - zs + 1) / (double)(ye - ys_ + 1) / (double)(xe_ - xs + 1);
+    gres = sqrt(residual);
+    applyZ(C);
+  }
+  F->sweeps_w = step; F->res_w = gres;
+}
+
+/* ---- pressure correction: fluid_solver.h:1713-2194 + HYPRE PCG --------- */
+/* Matrix-free row: diag*x_P - cz*x_B - cy*x_S - cx*x_W - cx*x_E - cy*x_N - cz*x_F
+ * over fluid neighbours (non-fluid x entries are held at 0). */
+static void spmv(or_fluid *F, const double *x, double *y) {
+  I64 cx = F->md.cx, cy = F->md.cy, cz = F->md.cz;
+  for (I64 k = 0; k < cz; ++k) for (I64 j = 0; j < cy; ++j) for (I64 i = 0; i < cx; ++i) {
+    I64 c = GC(i, j, k), q = IP(i + 1, j + 1, k + 1);
+    if (F->empty[c]) { y[q] = 0; continue; }
+    double ax = F->acx[c], ay = F->acy[c], az = F->acz[c];
+    double d = ax + ax + ay + ay + az + az;
+    y[q] = d * x[q] - az * x[IP(i + 1, j + 1, k)] - ay * x[IP(i + 1, j, k + 1)] - ax * x[IP(i, j + 1, k + 1)]
+           - ax * x[IP(i + 2, j + 1, k + 1)] - ay * x[IP(i + 1, j + 2, k + 1)] - az * x[IP(i + 1, j + 1, k + 2)];
+  }
+}
+
+static double dotf(or_fluid *F, const double *a, const double *b) {
+  I64 cx = F->md.cx, cy = F->md.cy, cz = F->md.cz; double s = 0;
+  for (I64 k = 0; k < cz; ++k) for (I64 j = 0; j < cy; ++j) for (I64 i = 0; i < cx; ++i) {
+    I64 c = GC(i, j, k); if (F->empty[c]) continue;
+    I64 q = IP(i + 1, j + 1, k + 1); s += a[q] * b[q];
+  }
+  return s;
+}
+
+/* HYPRE 2.27 hypre_PCGSolve restated: identity preconditioner, two-norm
+ * stopping <r,r>/<b,b> < tol^2, zero initial guess, maxiter. */
+static void pcg(or_case *C) {
+  or_fluid *F = &C->fl; const or_params *P = &C->prm;
+  I64 np = (F->md.cx + 2) * (F->md.cy + 2) * (F->md.cz + 2);
+  double *b = F->b, *x = F->x, *r = F->r, *p = F->pv, *s = F->s;
+  memset(x, 0, sizeof(double) * (size_t)np);
+  double bb = dotf(F, b, b);
+  F->pcg_iters = 0; F->pcg_relres = 0;
+  if (bb == 0.0) return;
+  double eps = P->pcg_tol * P->pcg_tol;
+  memcpy(r, b, sizeof(double) * (size_t)np);
+  memcpy(p, r, sizeof(double) * (size_t)np);
+  double gamma = dotf(F, r, p);
+  int i = 0; double iprod = gamma;
+  while (i + 1 <= P->pcg_maxiter) {
+    i++;
+    spmv(F, p, s);
+    double sdotp = dotf(F, s, p);
+    if (sdotp == 0.0) break;
+    double alpha = gamma / sdotp, gamma_old = gamma;
+    for (I64 q = 0; q < np; ++q) { x[q] = x[q] + alpha * p[q]; r[q] = r[q] - alpha * s[q]; }
+    gamma = dotf(F, r, r);
+    iprod = gamma;
+    if (iprod / bb < eps) break;
+    double beta = gamma / gamma_old;
+    for (I64 q = 0; q < np; ++q) p[q] = r[q] + beta * p[q];
+  }
+  F->pcg_iters = i; F->pcg_relres = sqrt(iprod / bb);
+}
+
+static void pressure_correction(or_case *C) {
+  or_fluid *F = &C->fl; or_meta *md = &F->md;
+  I64 cx = md->cx, cy = md->cy, cz = md->cz;
+  I64 np = (cx + 2) * (cy + 2) * (cz + 2);
+  memset(F->b, 0, sizeof(double) * (size_t)np);
+  int assemble = !F->have_matrix || !C->prm.frozen_matrix;
+  for (I64 k = 0; k < cz; ++k) for (I64 j = 0; j < cy; ++j) for (I64 i = 0; i < cx; ++i) {
+    I64 c = GC(i, j, k); if (F->empty[c]) continue;
+    if (assemble) {
+      double xp = F->xp[i + 1], yp = F->yp[j + 1], zp = F->zp[k + 1];
+      double facexy = xp * yp, facexz = xp * zp, faceyz = yp * zp;
+      F->acx[c] = faceyz / F->up[IU(i + 1, j + 1, k + 1)];
+      F->acy[c] = facexz / F->vp[IV(i + 1, j + 1, k + 1)];
+      F->acz[c] = facexy / F->wp[IW(i + 1, j + 1, k + 1)];
+    }
+    F->b[IP(i + 1, j + 1, k + 1)] =
+        -(F->u_star[IU(i + 2, j + 1, k + 1)] - F->u_star[IU(i + 1, j + 1, k + 1)])
+        - (F->v_star[IV(i + 1, j + 2, k + 1)] - F->v_star[IV(i + 1, j + 1, k + 1)])
+        - (F->w_star[IW(i + 1, j + 1, k + 2)] - F->w_star[IW(i + 1, j + 1, k + 1)]);
+  }
+  F->have_matrix = 1;
+  pcg(C);
+  for (I64 k = 0; k < cz; ++k) for (I64 j = 0; j < cy; ++j) for (I64 i = 0; i < cx; ++i) {
+    I64 c = GC(i, j, k); if (F->empty[c]) continue;
+    I64 q = IP(i + 1, j + 1, k + 1); F->p_prime[q] = F->x[q];
+  }
+}
+
+/* ---- fluid energy GS: fluid_solver.h:794-881 --------------------------- */
+static void solveTemp(or_case *C) {
+  or_fluid *F = &C->fl; or_meta *md = &F->md; const or_params *P = &C->prm;
+  double *u = F->u_star, *v = F->v_star, *w = F->w_star, *T = F->t_temp;
+  I64 cx = md->cx, cy = md->cy, cz = md->cz;
+  double residual = 1, gres = residual; int step = 0;
+  while (step < P->gs_max) {
+    if (gres < P->energy_tol) break;
+    for (I64 k = 1; k <= cz; ++k) for (I64 j = 1; j <= cy; ++j) for (I64 i = 1; i <= cx; ++i) {
+      if (F->empty[GC(i - 1, j - 1, k - 1)]) continue;
+      double xp = F->xp[i], xw = F->xw[i], yp = F->yp[j], ys = F->ys[j], zp = F->zp[k], zf = F->zf[k];
+      double sx = (xp + xw) / 2.0, sy = (yp + ys) / 2.0, sz = (zp + zf) / 2.0;
+      double conv = -u[IU(i, j, k)] * (T[IP(i + 1, j, k)] - T[IP(i - 1, j, k)])
+                    - v[IV(i, j, k)] * (T[IP(i, j + 1, k)] - T[IP(i, j - 1, k)])
+                    - w[IW(i, j, k)] * (T[IP(i, j, k + 1)] - T[IP(i, j, k - 1)]);
+      double diff = P->alpha * (T[IP(i + 1, j, k)] + T[IP(i - 1, j, k)]) / sx / sx
+                    + P->alpha * (T[IP(i, j + 1, k)] + T[IP(i, j - 1, k)]) / sy / sy
+                    + P->alpha * (T[IP(i, j, k + 1)] + T[IP(i, j, k - 1)]) / sz / sz;
+      double denom = 2 * P->alpha * (1 / sx / sx + 1 / sy / sy + 1 / sz / sz);
+      double old = T[IP(i, j, k)];
+      double nv = (conv + diff) / denom * (P->relax) + (1 - P->relax) * old;
+      T[IP(i, j, k)] = nv;
+      residual += (nv - old) * (nv - old);
+    }
+    step++;
+    residual = residual / (double)cz / (double)cy / (double)cx;
+    gres = sqrt(residual);
+  }
+  F->sweeps_t = step; F->res_t = gres;
+}
+
+/* ---- FluidSolver::solve: fluid_solver.h:1401-1633 ---------------------- */
+static void fluid_solve(or_case *C) {
+  or_fluid *F = &C->fl; or_meta *md = &F->md; const or_params *P = &C->prm;
+  I64 cx = md->cx, cy = md->cy, cz = md->cz, fx = md->fx, fy = md->fy, fz = md->fz;
+  solveX(C); solveY(C); solveZ(C);
+  pressure_correction(C);
+  for (I64 k = 1; k <= cz; ++k) for (I64 j = 1; j <= cy; ++j) for (I64 i = 1; i <= fx - 1; ++i) {
+    if (F->empty[GC(i - 1, j - 1, k - 1)]) continue;
+    double faceyz = F->yp[j] * F->zp[k];
+    double ap = F->up[IU(i, j, k)]; if (ap == 0) ap = 1e-10;
+    double corr = (F->p_prime[IP(i - 1, j, k)] - F->p_prime[IP(i, j, k)]) * faceyz / ap;
+    F->ux[GX(i - 1, j - 1, k - 1)] = F->u_star[IU(i, j, k)] + corr;
+    F->u_star[IU(i, j, k)] = F->ux[GX(i - 1, j - 1, k - 1)];
+  }
+  for (I64 k = 1; k <= cz; ++k) for (I64 j = 1; j <= fy - 1; ++j) for (I64 i = 1; i <= cx; ++i) {
+    if (F->empty[GC(i - 1, j - 1, k - 1)]) continue;
+    double facexz = F->xp[i] * F->zp[k];
+    double ap = F->vp[IV(i, j, k)]; if (ap == 0) ap = 1e-10;
+    double corr = (F->p_prime[IP(i, j - 1, k)] - F->p_prime[IP(i, j, k)]) * facexz / ap;
+    F->uy[GY(i - 1, j - 1, k - 1)] = F->v_star[IV(i, j, k)] + corr;
+    F->v_star[IV(i, j, k)] = F->uy[GY(i - 1, j - 1, k - 1)];
+  }
+  for (I64 k = 1; k <= fz - 1; ++k) for (I64 j = 1; j <= cy; ++j) for (I64 i = 1; i <= cx; ++i) {
+    if (F->empty[GC(i - 1, j - 1, k - 1)]) continue;
+    double facexy = F->xp[i] * F->yp[j];
+    double ap = F->wp[IW(i, j, k)]; if (ap == 0) ap = 1e-10;
+    double corr = (F->p_prime[IP(i, j, k - 1)] - F->p_prime[IP(i, j, k)]) * facexy / ap;
+    F->uz[GZ(i - 1, j - 1, k - 1)] = F->w_star[IW(i, j, k)] + corr;
+    F->w_star[IW(i, j, k)] = F->uz[GZ(i - 1, j - 1, k - 1)];
+  }
+  for (I64 k = 0; k < cz; ++k) for (I64 j = 0; j < cy; ++j) for (I64 i = 0; i < cx; ++i) {
+    if (F->empty[GC(i, j, k)]) continue;
+    F->p[GC(i, j, k)] += P->relax * F->p_prime[IP(i + 1, j + 1, k + 1)];
+  }
+  for (I64 k = 0; k < cz; ++k) for (I64 j = 0; j < cy; ++j) for (I64 i = 0; i < cx; ++i) {
+    if (F->empty[GC(i, j, k)]) continue;
+    F->p_temp[IP(i + 1, j + 1, k + 1)] = F->p[GC(i, j, k)];
+  }
+  memset(F->p_prime, 0, sizeof(double) * (size_t)((cx + 2) * (cy + 2) * (cz + 2)));
+  solveTemp(C);
+}
+
+static void fluid_setForNext(or_case *C) {
+  or_fluid *F = &C->fl; or_meta *md = &F->md;
+  I64 cx = md->cx, cy = md->cy, cz = md->cz;
+  for (I64 k = 0; k < cz; ++k) for (I64 j = 0; j < cy; ++j) for (I64 i = 0; i < cx; ++i)
+    F->t[GC(i, j, k)] = F->t_temp[IP(i + 1, j + 1, k + 1)];
+  applyX(C); applyY(C); applyZ(C); applyCell(C);
+  for (I64 k = 0; k < cz; ++k) for (I64 j = 0; j < cy; ++j) for (I64 i = 0; i < cx; ++i)
+    F->p_temp[IP(i + 1, j + 1, k + 1)] = F->p[GC(i, j, k)];
+}
+
+/* ---- solid: mobs_solver.h:105-115, 290-301, 303-408, 467-500 ------------ */
+#define ST(i, j, k) ((i) + (j) * (S->md.cx + 2) + (k) * (S->md.cx + 2) * (S->md.cy + 2))
+#define SC(i, j, k) ((i) + (j) * S->md.cx + (k) * S->md.cx * S->md.cy)
+static void solid_solve(or_case *C, or_solid *S) {
+  const or_params *P = &C->prm;
+  I64 cx = S->md.cx, cy = S->md.cy, cz = S->md.cz;
+  for (I64 c = 0; c < cx * cy * cz; ++c) S->t[c] = P->t_solid0;     /* applyOuterBoundaryCondition */
+  double r2 = 1; int it = 0;
+  for (; it < P->gs_max; ++it) {
+    if (r2 < P->solid_tol) break;
+    for (I64 k = 1; k <= cz; ++k) for (I64 j = 1; j <= cy; ++j) for (I64 i = 1; i <= cx; ++i) {
+      I64 c = SC(i - 1, j - 1, k - 1);
+      if (S->empty[c]) { if (S->t[c] < 1e-5 || S->t[c] > 1000) S->t[c] = 293; continue; }
+      double *T = S->t_temp; double old = T[ST(i, j, k)];
+      double nv = 1.0 / 6.0 * (T[ST(i + 1, j, k)] + T[ST(i - 1, j, k)] + T[ST(i, j - 1, k)] + T[ST(i, j + 1, k)]
+                               + T[ST(i, j, k - 1)] + T[ST(i, j, k + 1)]);
+      nv = nv * P->relax_solid + (1 - P->relax_solid) * old;
+      T[ST(i, j, k)] = nv;
+      r2 += (nv - old) * (nv - old);
+    }
+    r2 = sqrt(r2 / (double)cz / (double)cy / (double)cx);
+  }
+  S->sweeps = it; S->residual = r2;
+}
+
+static void solid_setForNext(or_solid *S) {
+  I64 cx = S->md.cx, cy = S->md.cy, cz = S->md.cz;
+  for (I64 k = 0; k < cz; ++k) for (I64 j = 0; j < cy; ++j) for (I64 i = 0; i < cx; ++i) {
+    if (S->empty[SC(i, j, k)]) continue;
+    S->t[SC(i, j, k)] = S->t_temp[ST(i + 1, j + 1, k + 1)];
+  }
+}
+
+/* ---- interface swap: solver.h:62-148 ----------------------------------- */
+static void interface_swap(or_case *C) {
+  or_fluid *F = &C->fl;
+  /* all sends packed before any receive is written (Isend/Irecv/Waitall) */
+  double *fs = malloc(sizeof(double) * (size_t)(C->nswap ? C->nswap : 1));
+  double *ss = malloc(sizeof(double) * (size_t)(C->nswap ? C->nswap : 1));
+  for (I64 n = 0; n < C->nswap; ++n) {
+    fs[n] = F->t_temp[C->swap[n].f_send];
+    ss[n] = C->sol[C->swap[n].region].t_temp[C->swap[n].s_send];
+  }
+  for (I64 n = 0; n < C->nswap; ++n) {
+    F->t_temp[C->swap[n].f_recv] = ss[n];
+    C->sol[C->swap[n].region].t_temp[C->swap[n].s_recv] = fs[n];
+  }
+  free(fs); free(ss);
+}
+
+/* ------------------------------------------------------------------ */
+/* case construction (DistributedMesh::generateLocalDomain +
+ * FluidSolver::init + MobSolver::init), single rank, nParts = 1 */
+
+static void bbox_of(const or_mesh *m, int type, int reg, or_meta *md) {
+  I64 mn[3] = {1 << 30, 1 << 30, 1 << 30}, mx[3] = {-1, -1, -1};
+  for (I64 k = 0; k < m->Nz; ++k) for (I64 j = 0; j < m->Ny; ++j) for (I64 i = 0; i < m->Nx; ++i) {
+    I64 c = CID(i, j, k);
+    if (m->ctype[c] != type || m->region[c] != reg) continue;
+    I64 g[3] = {i + 1, j + 1, k + 1};
+    for (int a = 0; a < 3; ++a) { if (g[a] < mn[a]) mn[a] = g[a]; if (g[a] > mx[a]) mx[a] = g[a]; }
+  }
+  md->cx = mx[0] - mn[0] + 1; md->cy = mx[1] - mn[1] + 1; md->cz = mx[2] - mn[2] + 1;
+  md->fx = md->cx + 1; md->fy = md->cy + 1; md->fz = md->cz + 1;
+  md->ox = mn[0]; md->oy = mn[1]; md->oz = mn[2];
+}
+
+static void geometry_axis(const double *pts, I64 npts, I64 off, I64 n, double **p, double **m_, double **pl) {
+  /* padded index i in 1..n -> global 0-based g = i + off - 2 (fluid_solver.h:1248-1251) */
+  *p = calloc((size_t)(n + 2), sizeof(double)); *m_ = calloc((size_t)(n + 2), sizeof(double)); *pl = calloc((size_t)(n + 2), sizeof(double));
+  for (I64 i = 1; i <= n; ++i) {
+    I64 g = i + off - 2;
+    double xp = (g + 1) < npts ? (pts[g + 1] - pts[g]) : (pts[g] - pts[g - 1]);
+    double xw = (g - 1) >= 0 ? (pts[g] - pts[g - 1]) : xp;
+    double xe = (g + 2) < npts ? (pts[g + 2] - pts[g + 1]) : xp;
+    (*p)[i] = xp; (*m_)[i] = xw; (*pl)[i] = xe;
+  }
+}
+
+or_case *or_create(const char *deck_text, const or_params *prm) {
+  or_case *C = calloc(1, sizeof(or_case));
+  if (prm) C->prm = *prm; else or_params_default(&C->prm);
+  if (or_deck_parse(deck_text, &C->deck)) { free(C); return NULL; }
+  or_mesh_build(&C->deck, &C->mesh);
+  or_mesh *m = &C->mesh;
+  if (m->nfluid_regions != 1) {
+    snprintf(err_buf, sizeof err_buf, "exactly one connected fluid region is supported (found %d)", m->nfluid_regions);
+    or_mesh_free(m); or_deck_free(&C->deck); free(C); return NULL;
+  }
+  or_fluid *F = &C->fl;
+  bbox_of(m, 0, 0, &F->md);
+  or_meta *md = &F->md;
+  I64 cx = md->cx, cy = md->cy, cz = md->cz, fx = md->fx, fy = md->fy, fz = md->fz;
+  I64 ncell = cx * cy * cz, np = (cx + 2) * (cy + 2) * (cz + 2);
+  F->empty = malloc((size_t)ncell);
+  F->nfluid = 0;
+  for (I64 k = 0; k < cz; ++k) for (I64 j = 0; j < cy; ++j) for (I64 i = 0; i < cx; ++i) {
+    I64 g = CID(i + md->ox - 1, j + md->oy - 1, k + md->oz - 1);
+    int fl = m->ctype[g] == 0 && m->region[g] == 0;
+    F->empty[GC(i, j, k)] = !fl; F->nfluid += fl;
+  }
+  F->p = calloc((size_t)ncell, sizeof(double)); F->t = calloc((size_t)ncell, sizeof(double));
+  F->id = malloc(sizeof(int) * (size_t)ncell);
+  F->ux = calloc((size_t)(fx * cy * cz), sizeof(double));
+  F->uy = calloc((size_t)(cx * fy * cz), sizeof(double));
+  F->uz = calloc((size_t)(cx * cy * fz), sizeof(double));
+  I64 nu_ = (fx + 2) * (cy + 2) * (cz + 2), nv_ = (cx + 2) * (fy + 2) * (cz + 2), nw_ = (cx + 2) * (cy + 2) * (fz + 2);
+  F->u_star = calloc((size_t)nu_, sizeof(double)); F->up = calloc((size_t)nu_, sizeof(double));
+  F->v_star = calloc((size_t)nv_, sizeof(double)); F->vp = calloc((size_t)nv_, sizeof(double));
+  F->w_star = calloc((size_t)nw_, sizeof(double)); F->wp = calloc((size_t)nw_, sizeof(double));
+  F->p_temp = calloc((size_t)np, sizeof(double)); F->p_prime = calloc((size_t)np, sizeof(double));
+  F->t_temp = malloc(sizeof(double) * (size_t)np);
+  for (I64 q = 0; q < np; ++q) F->t_temp[q] = C->prm.t_fluid0;
+  F->acx = calloc((size_t)ncell, sizeof(double)); F->acy = calloc((size_t)ncell, sizeof(double)); F->acz = calloc((size_t)ncell, sizeof(double));
+  F->b = calloc((size_t)np, sizeof(double)); F->x = calloc((size_t)np, sizeof(double)); F->r = calloc((size_t)np, sizeof(double));
+  F->pv = calloc((size_t)np, sizeof(double)); F->s = calloc((size_t)np, sizeof(double));
+  geometry_axis(C->deck.xs, m->NxP, md->ox, cx, &F->xp, &F->xw, &F->xe);
+  geometry_axis(C->deck.ys, m->NyP, md->oy, cy, &F->yp, &F->ys, &F->yn);
+  geometry_axis(C->deck.zs, m->NzP, md->oz, cz, &F->zp, &F->zf, &F->zb);
+  /* HYPRE row ids in k-j-i order over fluid cells (fluid_solver.h:1894-1906) */
+  { int row = 0; for (I64 c = 0; c < ncell; ++c) F->id[c] = F->empty[c] ? -1 : row++; }
+
+  /* solid regions */
+  C->nsolid = m->nsolid_regions;
+  C->sol = calloc((size_t)(C->nsolid ? C->nsolid : 1), sizeof(or_solid));
+  for (int r = 0; r < C->nsolid; ++r) {
+    or_solid *S = &C->sol[r];
+    bbox_of(m, 1, r, &S->md);
+    I64 n = S->md.cx * S->md.cy * S->md.cz, nps = (S->md.cx + 2) * (S->md.cy + 2) * (S->md.cz + 2);
+    S->empty = malloc((size_t)n); S->t = calloc((size_t)n, sizeof(double));
+    S->t_temp = malloc(sizeof(double) * (size_t)nps);
+    for (I64 q = 0; q < nps; ++q) S->t_temp[q] = C->prm.t_solid0;
+    for (I64 k = 0; k < S->md.cz; ++k) for (I64 j = 0; j < S->md.cy; ++j) for (I64 i = 0; i < S->md.cx; ++i) {
+      I64 g = CID(i + S->md.ox - 1, j + S->md.oy - 1, k + S->md.oz - 1);
+      S->empty[SC(i, j, k)] = !(m->ctype[g] == 1 && m->region[g] == r);
+    }
+  }
+  /* interface ("ib_") faces, x then y then z, each in k-j-i order over the
+   * fluid box (fluid_solver.h:900-1229) */
+  I64 cap = 1024; C->swap = malloc(sizeof(or_swap) * (size_t)cap); C->nswap = 0;
+  for (int dir = 0; dir < 3; ++dir) {
+    I64 nfi = dir == 0 ? fx : cx, nfj = dir == 1 ? fy : cy, nfk = dir == 2 ? fz : cz;
+    for (I64 k = 0; k < nfk; ++k) for (I64 j = 0; j < nfj; ++j) for (I64 i = 0; i < nfi; ++i) {
+      /* global 0-based cell coords on the two sides of local face (i,j,k) */
+      I64 ga[3] = {i + md->ox - 1, j + md->oy - 1, k + md->oz - 1};
+      I64 gb[3] = {ga[0], ga[1], ga[2]};
+      ga[dir] -= 1;  /* minus side */
+      I64 Nd = dir == 0 ? m->Nx : dir == 1 ? m->Ny : m->Nz;
+      if (ga[dir] < 0 || gb[dir] >= Nd) continue;                      /* domain boundary: wall */
+      int wall = dir == 0 ? m->wx[FXID(gb[0], gb[1], gb[2])] : dir == 1 ? m->wy[FYID(gb[0], gb[1], gb[2])] : m->wz[FZID(gb[0], gb[1], gb[2])];
+      if (wall) continue;
+      I64 ca = CID(ga[0], ga[1], ga[2]), cb = CID(gb[0], gb[1], gb[2]);
+      int fa = m->ctype[ca] == 0 && m->region[ca] == 0, fb = m->ctype[cb] == 0 && m->region[cb] == 0;
+      int sa = m->ctype[ca] == 1, sb = m->ctype[cb] == 1;
+      I64 *gf, *gs; int reg;
+      if (fa && sb) { gf = ga; gs = gb; reg = m->region[cb]; }
+      else if (fb && sa) { gf = gb; gs = ga; reg = m->region[ca]; }
+      else continue;
+      or_solid *S = &C->sol[reg];
+      if (C->nswap == cap) { cap *= 2; C->swap = realloc(C->swap, sizeof(or_swap) * (size_t)cap); }
+      or_swap *sw = &C->swap[C->nswap++];
+      sw->region = reg;
+      sw->f_send = IP(gf[0] - md->ox + 2, gf[1] - md->oy + 2, gf[2] - md->oz + 2);
+      sw->f_recv = IP(gs[0] - md->ox + 2, gs[1] - md->oy + 2, gs[2] - md->oz + 2);
+      sw->s_send = ST(gs[0] - S->md.ox + 2, gs[1] - S->md.oy + 2, gs[2] - S->md.oz + 2);
+      sw->s_recv = ST(gf[0] - S->md.ox + 2, gf[1] - S->md.oy + 2, gf[2] - S->md.oz + 2);
+    }
+  }
+  return C;
+}
+
+/* FluidSolver::init (fluid_solver.h:882-1237) + MobSolver::init (mobs_solver.h:116-288) */
+int or_init(or_case *C) {
+  applyX(C); applyY(C); applyZ(C); applyCell(C);
+  /* ib faces: ux.u = u_star = 0 (fluid_solver.h:1005,1116,1225) */
+  or_fluid *F = &C->fl; or_meta *md = &F->md; or_mesh *m = &C->mesh;
+  for (int dir = 0; dir < 3; ++dir) {
+    I64 nfi = dir == 0 ? md->fx : md->cx, nfj = dir == 1 ? md->fy : md->cy, nfk = dir == 2 ? md->fz : md->cz;
+    for (I64 k = 0; k < nfk; ++k) for (I64 j = 0; j < nfj; ++j) for (I64 i = 0; i < nfi; ++i) {
+      I64 ga[3] = {i + md->ox - 1, j + md->oy - 1, k + md->oz - 1}, gb[3] = {ga[0], ga[1], ga[2]};
+      ga[dir] -= 1;
+      I64 Nd = dir == 0 ? m->Nx : dir == 1 ? m->Ny : m->Nz;
+      if (ga[dir] < 0 || gb[dir] >= Nd) continue;
+      int wall = dir == 0 ? m->wx[FXID(gb[0], gb[1], gb[2])] : dir == 1 ? m->wy[FYID(gb[0], gb[1], gb[2])] : m->wz[FZID(gb[0], gb[1], gb[2])];
+      if (wall) continue;
+      I64 ca = CID(ga[0], ga[1], ga[2]), cb = CID(gb[0], gb[1], gb[2]);
+      int fa = m->ctype[ca] == 0 && m->region[ca] == 0, fb = m->ctype[cb] == 0 && m->region[cb] == 0;
+      if (!((fa && m->ctype[cb] == 1) || (fb && m->ctype[ca] == 1))) continue;
+      if (dir == 0) { F->ux[GX(i, j, k)] = 0; F->u_star[IU(i + 1, j + 1, k + 1)] = 0; }
+      else if (dir == 1) { F->uy[GY(i, j, k)] = 0; F->v_star[IV(i + 1, j + 1, k + 1)] = 0; }
+      else { F->uz[GZ(i, j, k)] = 0; F->w_star[IW(i + 1, j + 1, k + 1)] = 0; }
+    }
+  }
+  for (int r = 0; r < C->nsolid; ++r) {
+    or_solid *S = &C->sol[r];
+    for (I64 c = 0; c < S->md.cx * S->md.cy * S->md.cz; ++c) S->t[c] = C->prm.t_solid0;
+  }
+  C->inited = 1;
+  return 0;
+}
+
+/* one outer iteration of Solver::solve (solver.h:55-154) */
+int or_step(or_case *C, int n) {
+  if (!C->inited) or_init(C);
+  for (int s = 0; s < n; ++s) {
+    fluid_solve(C);
+    for (int r = 0; r < C->nsolid; ++r) solid_solve(C, &C->sol[r]);
+    interface_swap(C);
+    fluid_setForNext(C);
+    for (int r = 0; r < C->nsolid; ++r) solid_setForNext(&C->sol[r]);
+    C->steps++;
+  }
+  return 0;
+}
+
+void or_destroy(or_case *C) {
+  if (!C) return;
+  or_fluid *F = &C->fl;
+  void *ptrs[] = {F->empty, F->p, F->t, F->id, F->ux, F->uy, F->uz, F->u_star, F->v_star, F->w_star, F->up, F->vp, F->wp,
+                  F->p_temp, F->p_prime, F->t_temp, F->xp, F->xw, F->xe, F->yp, F->ys, F->yn, F->zp, F->zf, F->zb,
+                  F->acx, F->acy, F->acz, F->b, F->x, F->r, F->pv, F->s};
+  for (size_t i = 0; i < sizeof(ptrs) / sizeof(ptrs[0]); ++i) free(ptrs[i]);
+  for (int r = 0; r < C->nsolid; ++r) { free(C->sol[r].empty); free(C->sol[r].t); free(C->sol[r].t_temp); }
+  free(C->sol); free(C->swap);
+  or_mesh_free(&C->mesh); or_deck_free(&C->deck);
+  free(C);
+}
+
+/* ------------------------------------------------------------------ */
+/* accessors for the ctypes harness */
+
+void or_fluid_meta(const or_case *C, I64 *out9) {
+  const or_meta *md = &C->fl.md;
+  I64 v[9] = {md->cx, md->cy, md->cz, md->fx, md->fy, md->fz, md->ox, md->oy, md->oz};
+  memcpy(out9, v, sizeof v);
+}
+int or_num_solids(const or_case *C) { return C->nsolid; }
+void or_solid_meta(const or_case *C, int r, I64 *out9) {
+  const or_meta *md = &C->sol[r].md;
+  I64 v[9] = {md->cx, md->cy, md->cz, md->fx, md->fy, md->fz, md->ox, md->oy, md->oz};
+  memcpy(out9, v, sizeof v);
+}
+void or_grid_dims(const or_case *C, I64 *out3) { out3[0] = C->mesh.Nx; out3[1] = C->mesh.Ny; out3[2] = C->mesh.Nz; }
+
+/* field ids shared with the product's hs_field enum */
+enum { F_U_STAR = 0, F_V_STAR, F_W_STAR, F_P_TEMP, F_T_TEMP, F_UP, F_VP, F_WP, F_UX, F_UY, F_UZ, F_P, F_T, F_P_PRIME };
+
+static const double *field_ptr(const or_case *C, int f, I64 *n) {
+  const or_fluid *F = &C->fl; const or_meta *md = &F->md;
+  I64 nu_ = (md->fx + 2) * (md->cy + 2) * (md->cz + 2), nv_ = (md->cx + 2) * (md->fy + 2) * (md->cz + 2);
+  I64 nw_ = (md->cx + 2) * (md->cy + 2) * (md->fz + 2), np = (md->cx + 2) * (md->cy + 2) * (md->cz + 2);
+  I64 nc = md->cx * md->cy * md->cz;
+  switch (f) {
+    case F_U_STAR: *n = nu_; return F->u_star;
+    case F_V_STAR: *n = nv_; return F->v_star;
+    case F_W_STAR: *n = nw_; return F->w_star;
+    case F_P_TEMP: *n = np; return F->p_temp;
+    case F_T_TEMP: *n = np; return F->t_temp;
+    case F_UP: *n = nu_; return F->up;
+    case F_VP: *n = nv_; return F->vp;
+    case F_WP: *n = nw_; return F->wp;
+    case F_UX: *n = md->fx * md->cy * md->cz; return F->ux;
+    case F_UY: *n = md->cx * md->fy * md->cz; return F->uy;
+    case F_UZ: *n = md->cx * md->cy * md->fz; return F->uz;
+    case F_P: *n = nc; return F->p;
+    case F_T: *n = nc; return F->t;
+    case F_P_PRIME: *n = np; return F->p_prime;
+  }
+  *n = 0; return NULL;
+}
+
+I64 or_field_size(const or_case *C, int f) { I64 n; field_ptr(C, f, &n); return n; }
+int or_get_field(const or_case *C, int f, double *out, I64 n) {
+  I64 m; const double *p = field_ptr(C, f, &m);
+  if (!p || n != m) return -1;
+  memcpy(out, p, sizeof(double) * (size_t)n); return 0;
+}
+I64 or_solid_size(const or_case *C, int r) { const or_meta *md = &C->sol[r].md; return (md->cx + 2) * (md->cy + 2) * (md->cz + 2); }
+int or_get_solid(const or_case *C, int r, int which, double *out, I64 n) {
+  const or_solid *S = &C->sol[r];
+  if (which == 0) { if (n != or_solid_size(C, r)) return -1; memcpy(out, S->t_temp, sizeof(double) * (size_t)n); }
+  else { if (n != S->md.cx * S->md.cy * S->md.cz) return -1; memcpy(out, S->t, sizeof(double) * (size_t)n); }
+  return 0;
+}
+int or_get_fluid_mask(const or_case *C, unsigned char *out, I64 n) {
+  const or_meta *md = &C->fl.md; if (n != md->cx * md->cy * md->cz) return -1;
+  memcpy(out, C->fl.empty, (size_t)n); return 0;
+}
+int or_get_cell_types(const or_case *C, unsigned char *out, int *region, I64 n) {
+  if (n != C->mesh.Nx * C->mesh.Ny * C->mesh.Nz) return -1;
+  memcpy(out, C->mesh.ctype, (size_t)n); memcpy(region, C->mesh.region, sizeof(int) * (size_t)n); return 0;
+}
+int or_get_grid(const or_case *C, int axis, double *out, I64 n) {
+  const or_deck *d = &C->deck; const double *p = axis == 0 ? d->xs : axis == 1 ? d->ys : d->zs;
+  I64 m = axis == 0 ? d->nx_pts : axis == 1 ? d->ny_pts : d->nz_pts;
+  if (n != m) return -1; memcpy(out, p, sizeof(double) * (size_t)n); return 0;
+}
+I64 or_num_swap(const or_case *C) { return C->nswap; }
+int or_get_swap(const or_case *C, I64 *out5, I64 n) {
+  if (n != C->nswap) return -1;
+  for (I64 i = 0; i < n; ++i) {
+    out5[5 * i] = C->swap[i].f_send; out5[5 * i + 1] = C->swap[i].f_recv;
+    out5[5 * i + 2] = C->swap[i].s_send; out5[5 * i + 3] = C->swap[i].s_recv; out5[5 * i + 4] = C->swap[i].region;
+  }
+  return 0;
+}
+/* stats: sweeps u,v,w,t, pcg iters, then residuals u,v,w,t, pcg relres */
+void or_stats(const or_case *C, int *iout5, double *dout5) {
+  const or_fluid *F = &C->fl;
+  iout5[0] = F->sweeps_u; iout5[1] = F->sweeps_v; iout5[2] = F->sweeps_w; iout5[3] = F->sweeps_t; iout5[4] = F->pcg_iters;
+  dout5[0] = F->res_u; dout5[1] = F->res_v; dout5[2] = F->res_w; dout5[3] = F->res_t; dout5[4] = F->pcg_relres;
+}
+int or_solid_sweeps(const or_case *C, int r) { return C->sol[r].sweeps; }
+int or_get_row_ids(const or_case *C, int *out, I64 n) {
+  const or_meta *md = &C->fl.md; if (n != md->cx * md->cy * md->cz) return -1;
+  memcpy(out, C->fl.id, sizeof(int) * (size_t)n); return 0;
+}
+/* state injection for state-perturbation tests */
+int or_set_field(or_case *C, int f, const double *in, I64 n) {
+  I64 m; double *p = (double *)field_ptr(C, f, &m);
+  if (!p || n != m) return -1;
+  memcpy(p, in, sizeof(double) * (size_t)n); return 0;
+}

@@ -1,0 +1,194 @@
+"""ctypes harness over oracle/liboracle.so, the plain-C FP64 restatement of
+hsolver's SIMPLE conjugate-heat-transfer outer step (hs_oracle.c).
+
+Test infrastructure: the parity checker and the CPU baseline, never the product.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = os.path.join(_HERE, "liboracle.so")
+
+FIELDS = {"u_star": 0, "v_star": 1, "w_star": 2, "p_temp": 3, "t_temp": 4, "up": 5, "vp": 6, "wp": 7,
+          "ux": 8, "uy": 9, "uz": 10, "p": 11, "t": 12, "p_prime": 13}
+
+
+class Params(ctypes.Structure):
+    """Mirror of or_params (reference macros, fluid_solver.h:21-37, mobs_solver.h:15-29)."""
+    _fields_ = [("nu", ctypes.c_double), ("rho", ctypes.c_double), ("alpha", ctypes.c_double),
+                ("u_lid", ctypes.c_double), ("relax", ctypes.c_double), ("relax_solid", ctypes.c_double),
+                ("mom_tol", ctypes.c_double), ("energy_tol", ctypes.c_double), ("solid_tol", ctypes.c_double),
+                ("gs_max", ctypes.c_int), ("t_fluid0", ctypes.c_double), ("t_wall", ctypes.c_double),
+                ("t_solid0", ctypes.c_double), ("pcg_tol", ctypes.c_double), ("pcg_maxiter", ctypes.c_int),
+                ("frozen_matrix", ctypes.c_int)]
+
+
+def build():
+    """Compile liboracle.so with the committed Makefile."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB):
+            build()
+        L = ctypes.CDLL(_LIB)
+        vp, i64, i64p = ctypes.c_void_p, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)
+        dp = ctypes.POINTER(ctypes.c_double)
+        L.or_create.restype = vp
+        L.or_create.argtypes = [ctypes.c_char_p, ctypes.POINTER(Params)]
+        L.or_params_default.argtypes = [ctypes.POINTER(Params)]
+        L.or_last_error.restype = ctypes.c_char_p
+        L.or_init.argtypes = [vp]
+        L.or_step.argtypes = [vp, ctypes.c_int]
+        L.or_destroy.argtypes = [vp]
+        L.or_fluid_meta.argtypes = [vp, i64p]
+        L.or_solid_meta.argtypes = [vp, ctypes.c_int, i64p]
+        L.or_num_solids.argtypes = [vp]
+        L.or_grid_dims.argtypes = [vp, i64p]
+        L.or_field_size.restype = i64
+        L.or_field_size.argtypes = [vp, ctypes.c_int]
+        L.or_get_field.argtypes = [vp, ctypes.c_int, dp, i64]
+        L.or_set_field.argtypes = [vp, ctypes.c_int, dp, i64]
+        L.or_solid_size.restype = i64
+        L.or_solid_size.argtypes = [vp, ctypes.c_int]
+        L.or_get_solid.argtypes = [vp, ctypes.c_int, ctypes.c_int, dp, i64]
+        L.or_get_fluid_mask.argtypes = [vp, ctypes.POINTER(ctypes.c_uint8), i64]
+        L.or_get_cell_types.argtypes = [vp, ctypes.POINTER(ctypes.c_uint8), ctypes.POINTER(ctypes.c_int), i64]
+        L.or_get_grid.argtypes = [vp, ctypes.c_int, dp, i64]
+        L.or_num_swap.restype = i64
+        L.or_num_swap.argtypes = [vp]
+        L.or_get_swap.argtypes = [vp, i64p, i64]
+        L.or_stats.argtypes = [vp, ctypes.POINTER(ctypes.c_int), dp]
+        L.or_solid_sweeps.argtypes = [vp, ctypes.c_int]
+        L.or_get_row_ids.argtypes = [vp, ctypes.POINTER(ctypes.c_int), i64]
+        _lib = L
+    return _lib
+
+
+def default_params():
+    p = Params()
+    lib().or_params_default(ctypes.byref(p))
+    return p
+
+
+class OracleCase:
+    """One case: fluid region 0 plus every solid region of a `.in` deck."""
+
+    def __init__(self, deck_text, params=None):
+        L = lib()
+        self._p = params if params is not None else default_params()
+        h = L.or_create(deck_text.encode() if isinstance(deck_text, str) else deck_text, ctypes.byref(self._p))
+        if not h:
+            raise ValueError(L.or_last_error().decode())
+        self.h = h
+        m = (ctypes.c_int64 * 9)()
+        L.or_fluid_meta(h, m)
+        self.meta = tuple(m)
+        d = (ctypes.c_int64 * 3)()
+        L.or_grid_dims(h, d)
+        self.dims = tuple(d)
+        self.nsolid = L.or_num_solids(h)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().or_destroy(self.h)
+            self.h = None
+
+    def init(self):
+        lib().or_init(self.h)
+
+    def step(self, n=1):
+        lib().or_step(self.h, n)
+
+    def field(self, name):
+        L = lib()
+        f = FIELDS[name]
+        n = L.or_field_size(self.h, f)
+        out = np.empty(n, np.float64)
+        assert L.or_get_field(self.h, f, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), n) == 0
+        return out
+
+    def set_field(self, name, arr):
+        L = lib()
+        arr = np.ascontiguousarray(arr, np.float64)
+        assert L.or_set_field(self.h, FIELDS[name], arr.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), arr.size) == 0
+
+    def solid_meta(self, r):
+        m = (ctypes.c_int64 * 9)()
+        lib().or_solid_meta(self.h, r, m)
+        return tuple(m)
+
+    def solid(self, r, which="t_temp"):
+        L = lib()
+        md = self.solid_meta(r)
+        n = L.or_solid_size(self.h, r) if which == "t_temp" else md[0] * md[1] * md[2]
+        out = np.empty(n, np.float64)
+        assert L.or_get_solid(self.h, r, 0 if which == "t_temp" else 1,
+                              out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), n) == 0
+        return out
+
+    def fluid_empty(self):
+        cx, cy, cz = self.meta[:3]
+        out = np.empty(cx * cy * cz, np.uint8)
+        assert lib().or_get_fluid_mask(self.h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)), out.size) == 0
+        return out
+
+    def cell_types(self):
+        n = self.dims[0] * self.dims[1] * self.dims[2]
+        t = np.empty(n, np.uint8)
+        r = np.empty(n, np.int32)
+        assert lib().or_get_cell_types(self.h, t.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)),
+                                       r.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), n) == 0
+        return t, r
+
+    def swap_pairs(self):
+        n = lib().or_num_swap(self.h)
+        out = np.empty(5 * n, np.int64)
+        assert lib().or_get_swap(self.h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), n) == 0
+        return out.reshape(n, 5)
+
+    def row_ids(self):
+        cx, cy, cz = self.meta[:3]
+        out = np.empty(cx * cy * cz, np.int32)
+        assert lib().or_get_row_ids(self.h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), out.size) == 0
+        return out
+
+    def stats(self):
+        i = (ctypes.c_int * 5)()
+        d = (ctypes.c_double * 5)()
+        lib().or_stats(self.h, i, d)
+        return {"sweeps_u": i[0], "sweeps_v": i[1], "sweeps_w": i[2], "sweeps_t": i[3], "pcg_iters": i[4],
+                "res_u": d[0], "res_v": d[1], "res_w": d[2], "res_t": d[3], "pcg_relres": d[4],
+                "sweeps_solid": [lib().or_solid_sweeps(self.h, r) for r in range(self.nsolid)]}
+
+
+def read_dump(path):
+    """Parse a record file written by oracle/ref/ref_driver (or tests/golden)."""
+    out = {}
+    with open(path, "rb") as f:
+        data = f.read()
+    pos = 0
+    while pos < len(data):
+        name = data[pos:pos + 32].split(b"\0", 1)[0].decode()
+        kind = int.from_bytes(data[pos + 32:pos + 36], "little", signed=True)
+        n = int.from_bytes(data[pos + 36:pos + 44], "little", signed=True)
+        pos += 44
+        dt = np.float64 if kind == 0 else np.int32
+        nb = n * (8 if kind == 0 else 4)
+        arr = np.frombuffer(data[pos:pos + nb], dt).copy()
+        pos += nb
+        key = name
+        k = 1
+        while key in out:
+            key = "%s#%d" % (name, k)
+            k += 1
+        out[key] = arr
+    return out
