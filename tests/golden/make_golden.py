@@ -1,0 +1,75 @@
+"""Regenerate the golden fixtures from the reference's own sources.
+
+Runs oracle/_ref/ref_driver (the reference's FluidSolver / MobSolver /
+Solver compiled single-rank against the shims in oracle/ref/shim; build it
+with `make -C oracle/ref`) on every deck in tests/golden/decks and stores:
+
+* golden_<deck>.npz: full state arrays after the listed outer steps (small
+  decks), keys "<step>/<array>";
+* golden_digests.json: per-array SHA-256 of the raw FP64 bytes, the L2 norm
+  and the PCG iteration count for larger decks, where full arrays would not
+  be small fixtures.
+
+Needs the reference tree (default /root/reference); run it in the build
+container, never on the GPU box.  Usage: python tests/golden/make_golden.py
+"""
+import hashlib
+import json
+import os
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, REPO)
+from oracle.oracle import read_dump  # noqa: E402
+
+DRIVER = os.path.join(REPO, "oracle", "_ref", "ref_driver")
+FULL = {"small": [1, 2, 5], "inner": [1, 5, 20], "quirk": [1, 3]}
+DIGEST = {"config1": [1, 2, 5], "config3": [1, 3], "example13": [1, 2, 10]}
+KEEP = ["u_star", "v_star", "w_star", "up", "vp", "wp", "p_temp", "t_temp", "ux", "uy", "uz", "p", "t",
+        "id", "fluid.empty", "fluid.t_boundary", "fluid.t_halo", "solid.t_temp", "solid.t", "solid.empty",
+        "solid.t_boundary", "solid.t_halo", "fluid.meta", "solid.meta", "pcg_iters"]
+
+
+def run(deck, steps, work):
+    prefix = os.path.join(work, "d")
+    subprocess.run([DRIVER, os.path.join(HERE, "decks", deck + ".in"), os.path.join(work, "wd"), prefix,
+                    ",".join(str(s) for s in steps)], check=True, stdout=subprocess.DEVNULL)
+    return {s: read_dump("%s.step%d.bin" % (prefix, s)) for s in steps}
+
+
+def main():
+    if not os.path.exists(DRIVER):
+        subprocess.run(["make", "-C", os.path.join(REPO, "oracle", "ref")], check=True)
+    digests = {}
+    for deck, steps in FULL.items():
+        with tempfile.TemporaryDirectory() as work:
+            res = run(deck, steps, work)
+        arrays = {}
+        for s, d in res.items():
+            for k in KEEP:
+                if k in d:
+                    arrays["%d/%s" % (s, k)] = d[k]
+        np.savez_compressed(os.path.join(HERE, "golden_%s.npz" % deck), **arrays)
+    for deck, steps in DIGEST.items():
+        with tempfile.TemporaryDirectory() as work:
+            res = run(deck, steps, work)
+        digests[deck] = {}
+        for s, d in res.items():
+            ent = {}
+            for k in KEEP:
+                if k in d and d[k].dtype == np.float64:
+                    ent[k] = {"sha256": hashlib.sha256(d[k].tobytes()).hexdigest(),
+                              "l2": float(np.linalg.norm(d[k])), "n": int(d[k].size)}
+            ent["pcg_iters"] = int(d["pcg_iters"][0])
+            digests[deck][str(s)] = ent
+    with open(os.path.join(HERE, "golden_digests.json"), "w") as f:
+        json.dump(digests, f, indent=1, sort_keys=True)
+
+
+if __name__ == "__main__":
+    main()
