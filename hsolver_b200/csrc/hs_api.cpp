@@ -1,0 +1,307 @@
+// extern "C" boundary of hsolver_b200 (declared in include/hsolver_b200.h).
+// Every entry point catches C++ exceptions and maps them to an int status;
+// the message is kept per context (and per thread for context-less errors).
+#include <cstring>
+#include <new>
+#include <stdexcept>
+#include <string>
+
+#include "../../include/hsolver_b200.h"
+#include "hs_case.hpp"
+#include "hs_engine.hpp"
+
+struct hs_ctx {
+  hs::Engine *engine = nullptr;
+  std::string err;
+};
+
+struct hs_case {
+  hs::Case c;
+};
+
+namespace {
+thread_local std::string g_err;
+
+int fail(hs_ctx *ctx, int code, const std::string &msg) {
+  g_err = msg;
+  if (ctx) ctx->err = msg;
+  return code;
+}
+
+int classify(const std::exception &e) {
+  std::string m = e.what();
+  if (m.rfind("CUDA alloc", 0) == 0) return HS_ERR_NOMEM;
+  if (m.rfind("CUDA", 0) == 0) return HS_ERR_CUDA;
+  if (dynamic_cast<const std::invalid_argument *>(&e)) return HS_ERR_ARG;
+  if (dynamic_cast<const std::logic_error *>(&e)) return HS_ERR_STATE;
+  return HS_ERR_INTERNAL;
+}
+
+template <class Fn>
+int guarded(hs_ctx *ctx, Fn fn) {
+  if (!ctx || !ctx->engine) return fail(ctx, HS_ERR_ARG, "null context");
+  try {
+    return fn(*ctx->engine);
+  } catch (const std::bad_alloc &) {
+    return fail(ctx, HS_ERR_NOMEM, "host allocation failed");
+  } catch (const std::exception &e) {
+    return fail(ctx, classify(e), e.what());
+  }
+}
+}  // namespace
+
+extern "C" {
+
+void hs_params_default(hs_params *p) {
+  if (!p) return;
+  std::memset(p, 0, sizeof(*p));
+  p->nu = 0.001; p->rho = 1; p->alpha = 0.001; p->u_lid = 0.1;
+  p->relax = 0.3; p->relax_solid = 0.3;
+  p->mom_tol = 2e-3; p->energy_tol = 2e-3; p->solid_tol = 1e-3;
+  p->gs_max = 100; p->t_fluid0 = 293; p->t_wall = 293; p->t_solid0 = 333;
+  p->pcg_tol = 1e-5; p->pcg_maxiter = 1000; p->frozen_matrix = 1;
+  p->pressure_solver = HS_PSOLVE_CG;
+}
+
+int hs_create(const char *deck, const hs_params *prm, int device, hs_ctx **out) {
+  if (!deck || !out) return fail(nullptr, HS_ERR_ARG, "null deck or output pointer");
+  *out = nullptr;
+  hs_params p;
+  if (prm) p = *prm; else hs_params_default(&p);
+  if (p.gs_max < 0 || p.pcg_maxiter < 0 || !(p.pcg_tol >= 0)) return fail(nullptr, HS_ERR_ARG, "invalid parameters");
+  if (p.pressure_solver != HS_PSOLVE_CG) return fail(nullptr, HS_ERR_UNSUPPORTED, "pressure solver not available in this build");
+  std::string err;
+  hs::Deck d;
+  if (!hs::parse_deck(deck, d, err)) return fail(nullptr, HS_ERR_DECK, err);
+  hs::Case c;
+  if (!hs::build_case(d, c, err)) return fail(nullptr, err.rfind("deck", 0) == 0 ? HS_ERR_DECK : HS_ERR_UNSUPPORTED, err);
+  hs_ctx *ctx = new (std::nothrow) hs_ctx();
+  if (!ctx) return fail(nullptr, HS_ERR_NOMEM, "host allocation failed");
+  try {
+    ctx->engine = new hs::Engine(c, p, device);
+  } catch (const std::exception &e) {
+    int code = classify(e);
+    std::string m = e.what();
+    delete ctx;
+    return fail(nullptr, code, m);
+  }
+  *out = ctx;
+  return HS_OK;
+}
+
+int hs_init(hs_ctx *ctx) {
+  return guarded(ctx, [](hs::Engine &e) { e.init(); return HS_OK; });
+}
+
+int hs_step(hs_ctx *ctx, int n, hs_stats *stats) {
+  if (n < 0) return fail(ctx, HS_ERR_ARG, "negative step count");
+  return guarded(ctx, [&](hs::Engine &e) {
+    if (!e.inited()) throw std::logic_error("hs_step before hs_init");
+    e.step(n);
+    if (stats) {
+      e.stats(stats);
+      double r[5] = {stats->res_u, stats->res_v, stats->res_w, stats->res_t, stats->pcg_relres};
+      for (double v : r)
+        if (!(v == v) || v > 1e300 || v < -1e300) {
+          ctx->err = g_err = "non-finite residual";
+          return HS_ERR_DIVERGED;
+        }
+    }
+    return HS_OK;
+  });
+}
+
+int hs_sync(hs_ctx *ctx) {
+  return guarded(ctx, [](hs::Engine &e) { e.sync(); return HS_OK; });
+}
+
+int hs_field_size(hs_ctx *ctx, int field, long long *n) {
+  return guarded(ctx, [&](hs::Engine &e) {
+    long m = e.field_size(field);
+    if (m < 0 || !n) throw std::invalid_argument("unknown field id");
+    *n = m;
+    return HS_OK;
+  });
+}
+
+int hs_get_field(hs_ctx *ctx, int field, double *host, long long n) {
+  if (!host) return fail(ctx, HS_ERR_ARG, "null buffer");
+  return guarded(ctx, [&](hs::Engine &e) { e.get_field(field, host, (long)n); return HS_OK; });
+}
+
+int hs_set_field(hs_ctx *ctx, int field, const double *host, long long n) {
+  if (!host) return fail(ctx, HS_ERR_ARG, "null buffer");
+  return guarded(ctx, [&](hs::Engine &e) { e.set_field(field, host, (long)n); return HS_OK; });
+}
+
+int hs_field_device_ptr(hs_ctx *ctx, int field, double **dptr, long long *n) {
+  if (!dptr || !n) return fail(ctx, HS_ERR_ARG, "null output pointer");
+  return guarded(ctx, [&](hs::Engine &e) {
+    long m;
+    double *p = e.field_device_ptr(field, &m);
+    if (!p) throw std::invalid_argument("unknown field id");
+    *dptr = p;
+    *n = m;
+    return HS_OK;
+  });
+}
+
+int hs_fluid_meta(hs_ctx *ctx, long long out9[9]) {
+  return guarded(ctx, [&](hs::Engine &e) {
+    const hs::Meta &m = e.kase().fluid;
+    long long v[9] = {m.cx, m.cy, m.cz, m.fx, m.fy, m.fz, m.ox, m.oy, m.oz};
+    std::memcpy(out9, v, sizeof v);
+    return HS_OK;
+  });
+}
+
+int hs_grid_dims(hs_ctx *ctx, long long out3[3]) {
+  return guarded(ctx, [&](hs::Engine &e) {
+    out3[0] = e.kase().Nx; out3[1] = e.kase().Ny; out3[2] = e.kase().Nz;
+    return HS_OK;
+  });
+}
+
+int hs_num_solids(hs_ctx *ctx) {
+  return guarded(ctx, [](hs::Engine &e) { return (int)e.kase().solids.size(); });
+}
+
+int hs_solid_meta(hs_ctx *ctx, int region, long long out9[9]) {
+  return guarded(ctx, [&](hs::Engine &e) {
+    if (region < 0 || region >= (int)e.kase().solids.size()) throw std::invalid_argument("solid region out of range");
+    const hs::Meta &m = e.kase().solids[region];
+    long long v[9] = {m.cx, m.cy, m.cz, m.fx, m.fy, m.fz, m.ox, m.oy, m.oz};
+    std::memcpy(out9, v, sizeof v);
+    return HS_OK;
+  });
+}
+
+int hs_get_solid(hs_ctx *ctx, int region, int which, double *host, long long n) {
+  if (!host) return fail(ctx, HS_ERR_ARG, "null buffer");
+  return guarded(ctx, [&](hs::Engine &e) { e.get_solid(region, which, host, (long)n); return HS_OK; });
+}
+
+int hs_get_fluid_mask(hs_ctx *ctx, unsigned char *host, long long n) {
+  if (!host) return fail(ctx, HS_ERR_ARG, "null buffer");
+  return guarded(ctx, [&](hs::Engine &e) {
+    const auto &m = e.kase().fluid_empty;
+    if ((long long)m.size() != n) throw std::invalid_argument("mask size mismatch");
+    std::memcpy(host, m.data(), m.size());
+    return HS_OK;
+  });
+}
+
+int hs_get_cell_types(hs_ctx *ctx, unsigned char *type, int *region, long long n) {
+  if (!type || !region) return fail(ctx, HS_ERR_ARG, "null buffer");
+  return guarded(ctx, [&](hs::Engine &e) {
+    const auto &c = e.kase();
+    if ((long long)c.ctype.size() != n) throw std::invalid_argument("cell-type size mismatch");
+    std::memcpy(type, c.ctype.data(), c.ctype.size());
+    std::memcpy(region, c.region.data(), c.region.size() * sizeof(int));
+    return HS_OK;
+  });
+}
+
+int hs_get_row_ids(hs_ctx *ctx, int *host, long long n) {
+  if (!host) return fail(ctx, HS_ERR_ARG, "null buffer");
+  return guarded(ctx, [&](hs::Engine &e) {
+    const auto &r = e.kase().row_id;
+    if ((long long)r.size() != n) throw std::invalid_argument("row-id size mismatch");
+    std::memcpy(host, r.data(), r.size() * sizeof(int));
+    return HS_OK;
+  });
+}
+
+int hs_case_create(const char *deck, hs_case **out) {
+  if (!deck || !out) return fail(nullptr, HS_ERR_ARG, "null deck or output pointer");
+  *out = nullptr;
+  try {
+    std::string err;
+    hs::Deck d;
+    if (!hs::parse_deck(deck, d, err)) return fail(nullptr, HS_ERR_DECK, err);
+    hs_case *c = new hs_case();
+    if (!hs::build_case(d, c->c, err)) {
+      delete c;
+      return fail(nullptr, err.rfind("deck", 0) == 0 ? HS_ERR_DECK : HS_ERR_UNSUPPORTED, err);
+    }
+    *out = c;
+    return HS_OK;
+  } catch (const std::exception &e) {
+    return fail(nullptr, HS_ERR_INTERNAL, e.what());
+  }
+}
+
+int hs_case_dims(const hs_case *c, long long out3[3]) {
+  if (!c || !out3) return fail(nullptr, HS_ERR_ARG, "null argument");
+  out3[0] = c->c.Nx; out3[1] = c->c.Ny; out3[2] = c->c.Nz;
+  return HS_OK;
+}
+
+static void meta9(const hs::Meta &m, long long *o) {
+  long long v[9] = {m.cx, m.cy, m.cz, m.fx, m.fy, m.fz, m.ox, m.oy, m.oz};
+  std::memcpy(o, v, sizeof v);
+}
+
+int hs_case_fluid_meta(const hs_case *c, long long out9[9]) {
+  if (!c || !out9) return fail(nullptr, HS_ERR_ARG, "null argument");
+  meta9(c->c.fluid, out9);
+  return HS_OK;
+}
+
+int hs_case_num_solids(const hs_case *c) {
+  if (!c) return fail(nullptr, HS_ERR_ARG, "null argument");
+  return (int)c->c.solids.size();
+}
+
+int hs_case_solid_meta(const hs_case *c, int region, long long out9[9]) {
+  if (!c || !out9 || region < 0 || region >= (int)c->c.solids.size()) return fail(nullptr, HS_ERR_ARG, "bad region");
+  meta9(c->c.solids[region], out9);
+  return HS_OK;
+}
+
+int hs_case_cell_types(const hs_case *c, unsigned char *type, int *region, long long n) {
+  if (!c || !type || !region || n != (long long)c->c.ctype.size()) return fail(nullptr, HS_ERR_ARG, "bad buffer");
+  std::memcpy(type, c->c.ctype.data(), c->c.ctype.size());
+  std::memcpy(region, c->c.region.data(), c->c.region.size() * sizeof(int));
+  return HS_OK;
+}
+
+int hs_case_fluid_mask(const hs_case *c, unsigned char *empty, long long n) {
+  if (!c || !empty || n != (long long)c->c.fluid_empty.size()) return fail(nullptr, HS_ERR_ARG, "bad buffer");
+  std::memcpy(empty, c->c.fluid_empty.data(), c->c.fluid_empty.size());
+  return HS_OK;
+}
+
+long long hs_case_num_interface(const hs_case *c) { return c ? (long long)c->c.swap.size() : -1; }
+
+int hs_case_interface(const hs_case *c, long long *out5, long long n) {
+  if (!c || !out5 || n != (long long)c->c.swap.size()) return fail(nullptr, HS_ERR_ARG, "bad buffer");
+  for (long long i = 0; i < n; ++i) {
+    const hs::SwapPair &s = c->c.swap[i];
+    out5[5 * i] = s.f_send; out5[5 * i + 1] = s.f_recv; out5[5 * i + 2] = s.s_send;
+    out5[5 * i + 3] = s.s_recv; out5[5 * i + 4] = s.region;
+  }
+  return HS_OK;
+}
+
+int hs_case_geometry(const hs_case *c, int axis, double *out, long long n) {
+  if (!c || !out || axis < 0 || axis > 2) return fail(nullptr, HS_ERR_ARG, "bad argument");
+  const hs::Case &k = c->c;
+  const std::vector<double> *a[3][3] = {{&k.xp, &k.xw, &k.xe}, {&k.yp, &k.ys, &k.yn}, {&k.zp, &k.zf, &k.zb}};
+  long long m = (long long)a[axis][0]->size();
+  if (n != 3 * m) return fail(nullptr, HS_ERR_ARG, "geometry size mismatch");
+  for (int q = 0; q < 3; ++q) std::memcpy(out + q * m, a[axis][q]->data(), m * sizeof(double));
+  return HS_OK;
+}
+
+void hs_case_destroy(hs_case *c) { delete c; }
+
+void hs_destroy(hs_ctx *ctx) {
+  if (!ctx) return;
+  delete ctx->engine;
+  delete ctx;
+}
+
+const char *hs_last_error(const hs_ctx *ctx) { return ctx ? ctx->err.c_str() : g_err.c_str(); }
+
+}  // extern "C"

@@ -1,0 +1,48 @@
+// Single-GPU engine for the SIMPLE conjugate-heat-transfer step: owns the
+// case, all device state and the stream; runs FluidSolver::init/solve/
+// setForNext, MobSolver::init/solve/setForNext and the interface swap as
+// sm_100a kernels.
+#pragma once
+#include <cstdint>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/hsolver_b200.h"
+#include "hs_case.hpp"
+
+namespace hs {
+
+struct DeviceState;  // defined in hs_engine.cu
+
+class Engine {
+ public:
+  Engine(const Case &c, const hs_params &p, int device);
+  ~Engine();
+  Engine(const Engine &) = delete;
+  Engine &operator=(const Engine &) = delete;
+
+  void init();
+  void step(int n);
+  void sync();
+  void stats(hs_stats *out);
+
+  long field_size(int f) const;
+  void get_field(int f, double *host, long n);
+  void set_field(int f, const double *host, long n);
+  double *field_device_ptr(int f, long *n);
+  void get_solid(int r, int which, double *host, long n);
+
+  const Case &kase() const { return case_; }
+  bool inited() const { return inited_; }
+
+ private:
+  Case case_;
+  hs_params prm_;
+  int device_;
+  bool inited_ = false;
+  long long steps_ = 0;
+  std::unique_ptr<DeviceState> d_;
+};
+
+}  // namespace hs

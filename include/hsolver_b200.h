@@ -1,0 +1,157 @@
+/*
+ * hsolver_b200.h -- C ABI of the B200-native SIMPLE conjugate-heat-transfer
+ * step (one process, one GPU, the whole mesh resident in HBM).
+ *
+ * The reference (bolyme/hsolver) exposes this path as C++ classes driven by
+ * main.cpp; there is no FFI.  Each entry point below replaces the reference
+ * call named beside it, with plain pointers and sizes and an int status
+ * (0 = HS_OK, negative = error; hs_last_error() gives the text).  No C++
+ * exception crosses this boundary.  Calls on one context are serialised by
+ * the caller; several contexts may share a GPU.
+ */
+#ifndef HSOLVER_B200_H
+#define HSOLVER_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HS_OK 0
+#define HS_ERR_ARG (-1)         /* bad argument or size */
+#define HS_ERR_DECK (-2)        /* deck parse / classification error */
+#define HS_ERR_UNSUPPORTED (-3) /* case outside what the path supports */
+#define HS_ERR_CUDA (-4)        /* CUDA runtime error */
+#define HS_ERR_NOMEM (-5)       /* device allocation failed */
+#define HS_ERR_STATE (-6)       /* call out of order */
+#define HS_ERR_DIVERGED (-7)    /* non-finite residual */
+#define HS_ERR_INTERNAL (-8)    /* a bounded device wait gave up */
+
+/* Pressure-correction solver choice. */
+#define HS_PSOLVE_CG 0   /* HYPRE PCG restated: identity preconditioner (fluid_solver.h:1871-1875) */
+#define HS_PSOLVE_MGCG 1 /* CG preconditioned by the structured-grid multigrid V-cycle */
+
+/* Field ids (the FluidSolver members of fluid_solver.h:60-67, 93-108). */
+enum hs_field {
+  HS_F_U_STAR = 0, /* u*  padded (fx+2)(cy+2)(cz+2) */
+  HS_F_V_STAR = 1, /* v*  padded (cx+2)(fy+2)(cz+2) */
+  HS_F_W_STAR = 2, /* w*  padded (cx+2)(cy+2)(fz+2) */
+  HS_F_P_TEMP = 3, /* p   padded (cx+2)(cy+2)(cz+2) */
+  HS_F_T_TEMP = 4, /* T   padded (cx+2)(cy+2)(cz+2) */
+  HS_F_UP = 5,     /* a_P of the u faces, padded like u* */
+  HS_F_VP = 6,
+  HS_F_WP = 7,
+  HS_F_UX = 8,     /* LocalFace u of x faces, fx*cy*cz */
+  HS_F_UY = 9,     /* cx*fy*cz */
+  HS_F_UZ = 10,    /* cx*cy*fz */
+  HS_F_P = 11,     /* LocalCell p, cx*cy*cz */
+  HS_F_T = 12,     /* LocalCell t, cx*cy*cz */
+  HS_F_P_PRIME = 13 /* p' padded (zero between steps, fluid_solver.h:1598) */
+};
+
+/* Runtime form of the reference's compile-time macros
+ * (fluid_solver.h:21-37, mobs_solver.h:15-29). */
+typedef struct hs_params {
+  double nu;          /* NU 0.001 */
+  double rho;         /* RHO 1 */
+  double alpha;       /* ALPHA 0.001 */
+  double u_lid;       /* U0 0.1 */
+  double relax;       /* UNDER_RELAX 0.3 (fluid) */
+  double relax_solid; /* UNDER_RELAX 0.3 (solid) */
+  double mom_tol;     /* CONVERGENCE 2e-3 */
+  double energy_tol;  /* CONVERGENCE 2e-3 */
+  double solid_tol;   /* CONVERGENCE2 1e-3 (mobs_solver.h) */
+  int gs_max;         /* GS_STEP 100 */
+  double t_fluid0;    /* 293 */
+  double t_wall;      /* 293 */
+  double t_solid0;    /* 333 */
+  double pcg_tol;     /* 1e-5 */
+  int pcg_maxiter;    /* 1000 */
+  int frozen_matrix;  /* 1 = the reference's first-assembly matrix (fluid_solver.h:2188-2193) */
+  int pressure_solver;/* HS_PSOLVE_* */
+  int reserved[7];
+} hs_params;
+
+typedef struct hs_stats {
+  int sweeps_u, sweeps_v, sweeps_w, sweeps_t, sweeps_solid_max, pcg_iters;
+  double res_u, res_v, res_w, res_t, pcg_relres;
+  long long steps;
+} hs_stats;
+
+typedef struct hs_ctx hs_ctx;
+
+/* Defaults equal to the reference's macros. */
+void hs_params_default(hs_params *p);
+
+/* StructuredMesh(deck) + getConnectedRegions + decomposeMesh(nParts=1) +
+ * CYCASMesh/DistributedMesh::generateLocalDomain + FluidSolver/MobSolver
+ * constructors (mesh/mesh.cpp:42-58, 298-454; distributed_mesh.h:97-318;
+ * fluid_solver.h:93-109; mobs_solver.h:50-56).  `deck` is the `.in` text.
+ * Allocates all device state on `device`. */
+int hs_create(const char *deck, const hs_params *prm, int device, hs_ctx **out);
+
+/* FluidSolver::init + MobSolver::init (fluid_solver.h:882-1237,
+ * mobs_solver.h:116-288). */
+int hs_init(hs_ctx *ctx);
+
+/* n passes of the Solver::solve loop body (solver.h:55-154): fluid solve,
+ * solid solves, interface temperature swap, setForNext.  Asynchronous on the
+ * context's stream unless `stats` is non-NULL (then it synchronises and
+ * fills the last step's statistics). */
+int hs_step(hs_ctx *ctx, int n, hs_stats *stats);
+
+/* Wait for the context's stream. */
+int hs_sync(hs_ctx *ctx);
+
+/* Field access (host buffers; blocking). */
+int hs_field_size(hs_ctx *ctx, int field, long long *n);
+int hs_get_field(hs_ctx *ctx, int field, double *host, long long n);
+int hs_set_field(hs_ctx *ctx, int field, const double *host, long long n);
+/* Device address of a field (for callers that keep data in HBM). */
+int hs_field_device_ptr(hs_ctx *ctx, int field, double **dptr, long long *n);
+
+/* Case description: fluid metadata {cx,cy,cz,fx,fy,fz,ox,oy,oz}
+ * (distributed_mesh.h:152-154), grid dims, solid regions. */
+int hs_fluid_meta(hs_ctx *ctx, long long out9[9]);
+int hs_grid_dims(hs_ctx *ctx, long long out3[3]);
+int hs_num_solids(hs_ctx *ctx);
+int hs_solid_meta(hs_ctx *ctx, int region, long long out9[9]);
+/* which = 0: padded t_temp, 1: LocalCell t. */
+int hs_get_solid(hs_ctx *ctx, int region, int which, double *host, long long n);
+/* 1 where the fluid box cell is not fluid (LocalCell::isEmpty). */
+int hs_get_fluid_mask(hs_ctx *ctx, unsigned char *host, long long n);
+/* Global cell type (0 fluid, 1 obstacle) and region id, Nx*Ny*Nz. */
+int hs_get_cell_types(hs_ctx *ctx, unsigned char *type, int *region, long long n);
+/* HYPRE row id per fluid-box cell (-1 for empty), fluid_solver.h:1966. */
+int hs_get_row_ids(hs_ctx *ctx, int *host, long long n);
+
+/* Host-only case model (no GPU needed): the reference's decompose step for
+ * one rank -- deck parse, cell types, connected regions, local boxes and the
+ * fluid<->solid interface pairs (mesh/mesh.cpp:42-58, 84-454, 1124-1581;
+ * distributed_mesh.h:97-318; fluid_solver.h:900-1229). */
+typedef struct hs_case hs_case;
+int hs_case_create(const char *deck, hs_case **out);
+int hs_case_dims(const hs_case *c, long long out3[3]);
+int hs_case_fluid_meta(const hs_case *c, long long out9[9]);
+int hs_case_num_solids(const hs_case *c);
+int hs_case_solid_meta(const hs_case *c, int region, long long out9[9]);
+int hs_case_cell_types(const hs_case *c, unsigned char *type, int *region, long long n);
+int hs_case_fluid_mask(const hs_case *c, unsigned char *empty, long long n);
+/* Interface pairs as rows {fluid send, fluid recv, solid send, solid recv,
+ * solid region}; padded indices into the fluid / solid t_temp arrays. */
+long long hs_case_num_interface(const hs_case *c);
+int hs_case_interface(const hs_case *c, long long *out5, long long n);
+/* Per padded index geometry {xp,xw,xe | yp,ys,yn | zp,zf,zb} of the fluid
+ * box (fluid_solver.h:1248-1261); axis 0..2, out3 = 3 arrays of n+2. */
+int hs_case_geometry(const hs_case *c, int axis, double *out, long long n);
+void hs_case_destroy(hs_case *c);
+
+/* Release all device and host state. */
+void hs_destroy(hs_ctx *ctx);
+
+/* Text of the last error on `ctx` (or of the calling thread when ctx is NULL). */
+const char *hs_last_error(const hs_ctx *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HSOLVER_B200_H */
