@@ -86,6 +86,10 @@ def load(path=LIB_PATH):
     L.hs_destroy.restype = None
     L.hs_last_error.argtypes = [vp]
     L.hs_last_error.restype = ctypes.c_char_p
+    L.hs_stream.argtypes = [vp, ctypes.POINTER(vp)]
+    L.hs_profile.argtypes = [vp, ctypes.c_int]
+    L.hs_profile_read.argtypes = [vp, dp, ctypes.POINTER(ctypes.c_int)]
+    L.hs_counters.argtypes = [vp, llp]
     _lib = L
     return L
 
@@ -203,6 +207,28 @@ class Solver:
         out = np.empty(cx * cy * cz, np.int32)
         self._check(self._L.hs_get_row_ids(self.h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), out.size))
         return out
+
+    PHASES = ["mom_u", "mom_v", "mom_w", "pressure", "correct", "energy", "solid", "swap_setfornext"]
+
+    def profile(self, on=True):
+        self._check(self._L.hs_profile(self.h, 1 if on else 0))
+
+    def profile_read(self):
+        ms = (ctypes.c_double * 8)()
+        n = ctypes.c_int()
+        self._check(self._L.hs_profile_read(self.h, ms, ctypes.byref(n)))
+        return dict(zip(self.PHASES, list(ms))), n.value
+
+    def counters(self):
+        c = (ctypes.c_longlong * 8)()
+        self._check(self._L.hs_counters(self.h, c))
+        keys = ["sweeps_u", "sweeps_v", "sweeps_w", "sweeps_t", "solid_cell_sweeps", "pcg_iters", "pcg_solves", "steps"]
+        return dict(zip(keys, list(c)))
+
+    def stream(self):
+        p = ctypes.c_void_p()
+        self._check(self._L.hs_stream(self.h, ctypes.byref(p)))
+        return p.value
 
     def solve(self, n_outer=100):
         """Solver::solve (solver.h:44-158): init, then n_outer outer steps."""

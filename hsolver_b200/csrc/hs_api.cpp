@@ -115,6 +115,29 @@ int hs_sync(hs_ctx *ctx) {
   return guarded(ctx, [](hs::Engine &e) { e.sync(); return HS_OK; });
 }
 
+int hs_stream(hs_ctx *ctx, void **stream) {
+  if (!stream) return fail(ctx, HS_ERR_ARG, "null output pointer");
+  return guarded(ctx, [&](hs::Engine &e) { *stream = e.stream_handle(); return HS_OK; });
+}
+
+int hs_profile(hs_ctx *ctx, int on) {
+  return guarded(ctx, [&](hs::Engine &e) { e.profile(on != 0); return HS_OK; });
+}
+
+int hs_profile_read(hs_ctx *ctx, double ms[HS_NPHASE], int *steps) {
+  if (!ms) return fail(ctx, HS_ERR_ARG, "null buffer");
+  return guarded(ctx, [&](hs::Engine &e) {
+    int c = e.profile_read(ms, HS_NPHASE);
+    if (steps) *steps = c;
+    return HS_OK;
+  });
+}
+
+int hs_counters(hs_ctx *ctx, long long out8[8]) {
+  if (!out8) return fail(ctx, HS_ERR_ARG, "null buffer");
+  return guarded(ctx, [&](hs::Engine &e) { e.counters(out8); return HS_OK; });
+}
+
 int hs_field_size(hs_ctx *ctx, int field, long long *n) {
   return guarded(ctx, [&](hs::Engine &e) {
     long m = e.field_size(field);

@@ -58,6 +58,9 @@ struct FluidDev {
   double *pc, *tc, *ux, *uy, *uz;              // LocalCell / LocalFace values
   const uint8_t *empty;                        // cx*cy*cz
   const double *xp, *xw, *xe, *yp, *ys, *yn, *zp, *zf, *zb;
+  // 1/s/s per axis index with s = (p + m)/2 (fluid_solver.h:831-842), so the
+  // energy denominator 2*alpha*(1/sx/sx + 1/sy/sy + 1/sz/sz) costs no division
+  const double *ix2, *iy2, *iz2;
   double *acx, *acy, *acz;                     // padded, frozen pressure-correction coefficients
   double *x, *r, *pa, *pb, *s;                 // padded CG vectors; x is p'
   double *pscr;                                // cx*cy*cz scratch for the cell BC
@@ -75,6 +78,11 @@ struct DevStats {
   double pcg_relres;
   int solid_sweeps_max;
   int pad;
+  // running totals since creation (bench byte accounting)
+  long long cum_sweeps[4];
+  long long cum_solid_cell_sweeps;
+  long long cum_pcg_iters;
+  long long cum_pcg_solves;
 };
 
 __device__ __forceinline__ int IU(const FluidDev &F, int i, int j, int k) { return i + (F.fx + 2) * (j + (F.cy + 2) * k); }
@@ -324,34 +332,52 @@ __device__ void slot_totals(double acc, int walloc, int w, double *partials, int
 
 template <int EQ>
 __device__ __forceinline__ void gs_point(const FluidDev &F, const Prm &P, int i, int j, int k, bool lid, double &acc) {
+  // the face is updated only when the cell on its plus side is fluid; the
+  // mask load is issued with the others and only gates the stores
+  const bool fl = !F.empty[GC(F, i - 1, j - 1, k - 1)];
   double ap, old, nv;
   int idx;
-  if (EQ == 0) { nv = upd_u(F, P, i, j, k, ap, old); idx = IU(F, i, j, k); F.u[idx] = nv; F.up[idx] = ap; }
-  else if (EQ == 1) { nv = upd_v(F, P, i, j, k, ap, old, lid); idx = IV(F, i, j, k); F.v[idx] = nv; F.vp[idx] = ap; }
-  else if (EQ == 2) { nv = upd_w(F, P, i, j, k, ap, old); idx = IW(F, i, j, k); F.w[idx] = nv; F.wp[idx] = ap; }
+  if (EQ == 0) { nv = upd_u(F, P, i, j, k, ap, old); idx = IU(F, i, j, k); if (fl) { F.u[idx] = nv; F.up[idx] = ap; } }
+  else if (EQ == 1) { nv = upd_v(F, P, i, j, k, ap, old, lid); idx = IV(F, i, j, k); if (fl) { F.v[idx] = nv; F.vp[idx] = ap; } }
+  else if (EQ == 2) { nv = upd_w(F, P, i, j, k, ap, old); idx = IW(F, i, j, k); if (fl) { F.w[idx] = nv; F.wp[idx] = ap; } }
   else {
-    // solveTemp body (fluid_solver.h:810-846)
-    double *Tt = F.tt;
-    double xp = F.xp[i], xw = F.xw[i], yp = F.yp[j], ys = F.ys[j], zp = F.zp[k], zf = F.zf[k];
-    double sx = (xp + xw) / 2.0, sy = (yp + ys) / 2.0, sz = (zp + zf) / 2.0;
-    double te = ld(Tt + IP(F, i + 1, j, k)), tw = ld(Tt + IP(F, i - 1, j, k));
-    double tn = ld(Tt + IP(F, i, j + 1, k)), ts = ld(Tt + IP(F, i, j - 1, k));
-    double tf = ld(Tt + IP(F, i, j, k + 1)), tb = ld(Tt + IP(F, i, j, k - 1));
-    double conv = -__ldg(F.u + IU(F, i, j, k)) * (te - tw) - __ldg(F.v + IV(F, i, j, k)) * (tn - ts) -
-                  __ldg(F.w + IW(F, i, j, k)) * (tf - tb);
-    double diff = P.alpha * (te + tw) / sx / sx + P.alpha * (tn + ts) / sy / sy + P.alpha * (tf + tb) / sz / sz;
-    double denom = 2 * P.alpha * (1 / sx / sx + 1 / sy / sy + 1 / sz / sz);
-    idx = IP(F, i, j, k);
-    old = ld(Tt + idx);
-    nv = (conv + diff) / denom * (P.relax) + (1 - P.relax) * old;
-    Tt[idx] = nv;
+    nv = 0; old = 0; idx = 0;  // the energy equation runs through energy_apply
   }
-  acc += (nv - old) * (nv - old);
+  (void)idx;
+  if (fl) acc += (nv - old) * (nv - old);
+}
+
+// solveTemp body (fluid_solver.h:810-846) for up to four independent cells of
+// one time step: every load of the four is issued before any arithmetic.
+struct EnergyIn {
+  double te, tw, tn, ts, tf, tb, tc, u, v, w;
+  int q, i, j, k;
+  bool ok;
+};
+__device__ __forceinline__ void energy_gather(const FluidDev &F, int i, int j, int k, EnergyIn &e) {
+  const double *Tt = F.tt;
+  const int q = IP(F, i, j, k);
+  e.q = q; e.i = i; e.j = j; e.k = k;
+  const int PX = F.cx + 2, PXY = (F.cx + 2) * (F.cy + 2);
+  e.te = ld(Tt + q + 1); e.tw = ld(Tt + q - 1); e.tn = ld(Tt + q + PX); e.ts = ld(Tt + q - PX);
+  e.tf = ld(Tt + q + PXY); e.tb = ld(Tt + q - PXY); e.tc = ld(Tt + q);
+  e.u = __ldg(F.u + IU(F, i, j, k)); e.v = __ldg(F.v + IV(F, i, j, k)); e.w = __ldg(F.w + IW(F, i, j, k));
+  e.ok = e.ok && !F.empty[GC(F, i - 1, j - 1, k - 1)];
+}
+__device__ __forceinline__ void energy_apply(const FluidDev &F, const Prm &P, const EnergyIn &e, double &acc) {
+  double xp = F.xp[e.i], xw = F.xw[e.i], yp = F.yp[e.j], ys = F.ys[e.j], zp = F.zp[e.k], zf = F.zf[e.k];
+  double sx = (xp + xw) / 2.0, sy = (yp + ys) / 2.0, sz = (zp + zf) / 2.0;
+  double conv = -e.u * (e.te - e.tw) - e.v * (e.tn - e.ts) - e.w * (e.tf - e.tb);
+  double diff = P.alpha * (e.te + e.tw) / sx / sx + P.alpha * (e.tn + e.ts) / sy / sy + P.alpha * (e.tf + e.tb) / sz / sz;
+  double denom = 2 * P.alpha * (F.ix2[e.i] + F.iy2[e.j] + F.iz2[e.k]);
+  double nv = (conv + diff) / denom * (P.relax) + (1 - P.relax) * e.tc;
+  F.tt[e.q] = nv;
+  acc += (nv - e.tc) * (nv - e.tc);
 }
 
 // One GS solve of equation EQ (0 u, 1 v, 2 w momentum; 3 fluid energy).
 template <int EQ>
-__global__ void __launch_bounds__(kBlock) k_gs(FluidDev F, Prm P, double *partials, DevStats *st, double *snap) {
+__global__ void __launch_bounds__(kBlock, 2) k_gs(FluidDev F, Prm P, double *partials, DevStats *st, double *snap) {
   cg::grid_group grid = cg::this_grid();
   __shared__ double red[kBlock];
   __shared__ double tot[kBlock];
@@ -386,15 +412,39 @@ __global__ void __launch_bounds__(kBlock) k_gs(FluidDev F, Prm P, double *partia
       const int n = tid % walloc;
       double acc = 0.0;
       const int steps = S + 2 * (W - 1);
+      // this thread's rows: row0 + m*R, stepped incrementally in (j, k)
+      const int R = T / walloc, row0 = tid / walloc;
+      const int dj = R % NJ, dk = R / NJ;
+      const int j0 = row0 % NJ + 1, k0 = row0 / NJ + 1;
       for (int t = 0; t < steps; ++t) {
         if (n < W) {
           const bool lid = EQ == 1 && lid_row && (done + n) >= 1;
-          for (int item = tid; item < nrows * walloc; item += T) {
-            const int row = item / walloc;
-            const int j = row % NJ + 1, k = row / NJ + 1, i = t - 2 * n - (j - 1) - (k - 1) + 1;
-            if (i < 1 || i > NI) continue;
-            if (F.empty[GC(F, i - 1, j - 1, k - 1)]) continue;
-            gs_point<EQ>(F, P, i, j, k, lid, acc);
+          const int base = t - 2 * n + 1;  // i = base - (j - 1) - (k - 1)
+          int j = j0, k = k0;
+          if (EQ == 3) {
+            // groups of four of this thread's rows; loads of the active ones
+            // are issued together (static indices keep them in registers)
+            for (int row = row0; row < nrows; row += 4 * R) {
+              EnergyIn e[4];
+#pragma unroll
+              for (int b = 0; b < 4; ++b) {
+                const int i = base - (j - 1) - (k - 1);
+                e[b].ok = row + b * R < nrows && (unsigned)(i - 1) < (unsigned)NI;
+                if (e[b].ok) energy_gather(F, i, j, k, e[b]);
+                j += dj; k += dk;
+                if (j > NJ) { j -= NJ; ++k; }
+              }
+#pragma unroll
+              for (int b = 0; b < 4; ++b)
+                if (e[b].ok) energy_apply(F, P, e[b], acc);
+            }
+          } else {
+            for (int row = row0; row < nrows; row += R) {
+              const int i = base - (j - 1) - (k - 1);
+              if ((unsigned)(i - 1) < (unsigned)NI) gs_point<EQ>(F, P, i, j, k, lid, acc);
+              j += dj; k += dk;
+              if (j > NJ) { j -= NJ; ++k; }
+            }
           }
         }
         grid.sync();
@@ -424,7 +474,7 @@ __global__ void __launch_bounds__(kBlock) k_gs(FluidDev F, Prm P, double *partia
   if (EQ == 0) bc_x(F, tid, T2);
   else if (EQ == 1) bc_y(F, P, tid, T2);
   else if (EQ == 2) bc_z(F, tid, T2);
-  if (tid == 0) { st->sweeps[EQ] = done; st->res[EQ] = gres; }
+  if (tid == 0) { st->sweeps[EQ] = done; st->res[EQ] = gres; st->cum_sweeps[EQ] += done; }
 }
 
 // ---------------------------------------------------------------- solid energy
@@ -433,7 +483,7 @@ __global__ void __launch_bounds__(kBlock) k_gs(FluidDev F, Prm P, double *partia
 // speculated like k_gs; each region keeps its own residual, stop test and
 // sweep count.
 constexpr int kMaxRegions = 256;
-__global__ void __launch_bounds__(kBlock) k_solid(const SolidReg *regs, int nreg, const int *blk_reg, double *tt_all,
+__global__ void __launch_bounds__(kBlock, 2) k_solid(const SolidReg *regs, int nreg, const int *blk_reg, double *tt_all,
                                                   double *tc_all, const uint8_t *em_all, Prm P, double *partials,
                                                   DevStats *st, double *snap, int *pred_all) {
   cg::grid_group grid = cg::this_grid();
@@ -482,21 +532,42 @@ __global__ void __launch_bounds__(kBlock) k_solid(const SolidReg *regs, int nreg
       const int n = ltid % walloc;
       double acc = 0.0;
       const int steps = ctl[1];
+      const int Rr = LT / walloc, row0 = ltid / walloc;
+      const int dj = Rr % R.cy, dk = Rr / R.cy;
+      const int j0 = row0 % R.cy + 1, k0 = row0 / R.cy + 1;
       for (int t = 0; t < steps; ++t) {
-        if (n < w)
-          for (int item = ltid; item < R.rows * walloc; item += LT) {
-            const int row = item / walloc;
-            const int j = row % R.cy + 1, k = row / R.cy + 1, i = t - 2 * n - (j - 1) - (k - 1) + 1;
-            if (i < 1 || i > R.cx) continue;
-            if (em[(i - 1) + R.cx * ((j - 1) + R.cy * (k - 1))]) continue;
-            const int q = i + PX * j + PXY * k;
-            double old = ld(Tr + q);
-            double nv = 1.0 / 6.0 * (ld(Tr + q + 1) + ld(Tr + q - 1) + ld(Tr + q - PX) + ld(Tr + q + PX) +
-                                     ld(Tr + q - PXY) + ld(Tr + q + PXY));
-            nv = nv * P.relax_solid + (1 - P.relax_solid) * old;
-            Tr[q] = nv;
-            acc += (nv - old) * (nv - old);
+        if (n < w) {
+          const int base = t - 2 * n + 1;
+          int j = j0, k = k0;
+          for (int row = row0; row < R.rows; row += 4 * Rr) {
+            double v[4][7];
+            int qq[4];
+            bool ok[4];
+#pragma unroll
+            for (int b = 0; b < 4; ++b) {
+              const int i = base - (j - 1) - (k - 1);
+              ok[b] = row + b * Rr < R.rows && (unsigned)(i - 1) < (unsigned)R.cx;
+              if (ok[b]) {
+                const int q = i + PX * j + PXY * k;
+                qq[b] = q;
+                ok[b] = !em[(i - 1) + R.cx * ((j - 1) + R.cy * (k - 1))];
+                v[b][0] = ld(Tr + q); v[b][1] = ld(Tr + q + 1); v[b][2] = ld(Tr + q - 1); v[b][3] = ld(Tr + q - PX);
+                v[b][4] = ld(Tr + q + PX); v[b][5] = ld(Tr + q - PXY); v[b][6] = ld(Tr + q + PXY);
+              }
+              j += dj; k += dk;
+              if (j > R.cy) { j -= R.cy; ++k; }
+            }
+#pragma unroll
+            for (int b = 0; b < 4; ++b)
+              if (ok[b]) {
+                const double old = v[b][0];
+                double nv = 1.0 / 6.0 * (v[b][1] + v[b][2] + v[b][3] + v[b][4] + v[b][5] + v[b][6]);
+                nv = nv * P.relax_solid + (1 - P.relax_solid) * old;
+                Tr[qq[b]] = nv;
+                acc += (nv - old) * (nv - old);
+              }
           }
+        }
         grid.sync();
       }
       // per-(region, slot) totals: block partial per slot, region sum in block order
@@ -557,8 +628,13 @@ __global__ void __launch_bounds__(kBlock) k_solid(const SolidReg *regs, int nreg
     for (int q = threadIdx.x; q < nreg; q += blockDim.x) pred_all[q] = done[q];
     if (threadIdx.x == 0) {
       int m = 0;
-      for (int q = 0; q < nreg; ++q) m = max(m, done[q]);
+      long long cells = 0;
+      for (int q = 0; q < nreg; ++q) {
+        m = max(m, done[q]);
+        cells += (long long)done[q] * regs[q].cx * regs[q].cy * regs[q].cz;
+      }
       st->solid_sweeps_max = m;
+      st->cum_solid_cell_sweeps += cells;
     }
   }
 }
@@ -593,11 +669,25 @@ __global__ void k_swap_scatter(const long long *f_recv, const long long *s_recv,
 
 // ---------------------------------------------------------------- pressure correction
 // Assembly (fluid_solver.h:1969-2002 / 2123-2162) + HYPRE PCG restated.
-__global__ void __launch_bounds__(kBlock) k_pcorr(FluidDev F, Prm P, double *partials, DevStats *st, int assemble) {
+//
+// Pass A of an iteration (p = r + beta p, s = A p, x += alpha_prev p_old,
+// <s,p>) runs over 32 x 8 x TZ tiles: each block marches a tile column in
+// z, keeping three planes of the new direction (with a one-cell halo) in
+// shared memory, so every neighbour comes from shared memory and each cell's
+// r and p are read once.  Coefficients are zero off the fluid cells, where
+// r, p, x, s stay zero, so no mask test is needed.  Pass B (r -= alpha s,
+// <r,r>) streams the padded arrays as double2.
+constexpr int kTX = 32, kTY = 16;  // tile of 32 x 16 columns; a thread owns rows ty and ty + 8
+
+__global__ void __launch_bounds__(kBlock) k_pcorr(FluidDev F, Prm P, double *partials, DevStats *st, int assemble,
+                                                  int TZ) {
   cg::grid_group grid = cg::this_grid();
   __shared__ double sh[33];
+  // four plane slots: the plane written at kk never aliases the three read at kk - 1
+  __shared__ double pl[4][kTY + 2][kTX + 2];
   const int cx = F.cx, cy = F.cy, cz = F.cz, n = cx * cy * cz;
   const int PX = cx + 2, PXY = (cx + 2) * (cy + 2);
+  const long long npad = (long long)PXY * (cz + 2);
   const int tid = blockIdx.x * blockDim.x + threadIdx.x, T = gridDim.x * blockDim.x;
   int buf = 0;
   double acc = 0.0;
@@ -622,54 +712,112 @@ __global__ void __launch_bounds__(kBlock) k_pcorr(FluidDev F, Prm P, double *par
   }
   const double bb = grid_sum(acc, partials, buf, sh, grid);
   if (bb == 0.0) {
-    if (tid == 0) { st->pcg_iters = 0; st->pcg_relres = 0.0; }
+    if (tid == 0) { st->pcg_iters = 0; st->pcg_relres = 0.0; st->cum_pcg_solves += 1; }
     return;
   }
   const double eps = P.pcg_tol * P.pcg_tol;
   double gamma = bb, iprod = bb, beta = 0.0, alpha_prev = 0.0;
   double *pold = F.pa, *pnew = F.pb;
+  const int ntx = (cx + kTX - 1) / kTX, nty = (cy + kTY - 1) / kTY, ntz = (cz + TZ - 1) / TZ;
+  const int ntiles = ntx * nty * ntz;
+  const int tx = threadIdx.x % kTX, ty = threadIdx.x / kTX;  // ty in [0, 8)
+  // halo role (96 cells: y-1 row, y+16 row, x-1 column, x+32 column)
+  const int h = threadIdx.x;
+  int hx = -1, hy = -1;
+  if (h < kTX) { hx = h + 1; hy = 0; }
+  else if (h < 2 * kTX) { hx = h - kTX + 1; hy = kTY + 1; }
+  else if (h < 2 * kTX + kTY) { hx = 0; hy = h - 2 * kTX + 1; }
+  else if (h < 2 * kTX + 2 * kTY) { hx = kTX + 1; hy = h - 2 * kTX - kTY + 1; }
   int it = 0;
   bool pending = false;
   while (it + 1 <= P.pcg_maxiter) {
     it++;
     acc = 0.0;
-    for (int c = tid; c < n; c += T) {
-      if (F.empty[c]) continue;
-      const int i = c % cx, j = (c / cx) % cy, k = c / (cx * cy);
-      const int q = (i + 1) + PX * (j + 1) + PXY * (k + 1);
-      double pc, pB, pS, pW, pE, pN, pF;
-      if (it == 1) {
-        pc = ld(pold + q); pB = ld(pold + q - PXY); pS = ld(pold + q - PX); pW = ld(pold + q - 1);
-        pE = ld(pold + q + 1); pN = ld(pold + q + PX); pF = ld(pold + q + PXY);
-      } else {
-        const double *r = F.r;
-        pc = ld(r + q) + beta * ld(pold + q);
-        pB = ld(r + q - PXY) + beta * ld(pold + q - PXY);
-        pS = ld(r + q - PX) + beta * ld(pold + q - PX);
-        pW = ld(r + q - 1) + beta * ld(pold + q - 1);
-        pE = ld(r + q + 1) + beta * ld(pold + q + 1);
-        pN = ld(r + q + PX) + beta * ld(pold + q + PX);
-        pF = ld(r + q + PXY) + beta * ld(pold + q + PXY);
-        F.x[q] = ld(F.x + q) + alpha_prev * ld(pold + q);
+    const double *r = F.r;
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+      const int tz = tile / (ntx * nty), rem = tile % (ntx * nty);
+      const int i0 = 1 + (rem % ntx) * kTX, j0 = 1 + (rem / ntx) * kTY, k0 = 1 + tz * TZ;
+      const int kend = min(k0 + TZ - 1, cz);
+      const int i = i0 + tx, ja = j0 + ty, jb = ja + 8;
+      const bool inA = i <= cx && ja <= cy, inB = i <= cx && jb <= cy;
+      const bool padA = i <= cx + 1 && ja <= cy + 1, padB = i <= cx + 1 && jb <= cy + 1;
+      const int hi = i0 - 1 + hx, hj = j0 - 1 + hy;
+      const bool hin = hx >= 0 && hi <= cx + 1 && hj <= cy + 1;
+      double poA = 0.0, poB = 0.0;  // p_old of the plane being computed (kk - 1)
+      double nA = 0.0, nB = 0.0;    // p_old of plane kk
+      for (int kk = k0 - 1; kk <= kend + 1; ++kk) {
+        const int slot = (kk - k0 + 1) & 3;
+        const bool comp = kk >= k0 + 1;
+        // issue every load of this plane step before using any of them
+        const int qA = i + PX * ja + PXY * kk, qB = qA + 8 * PX;
+        double rA = 0.0, rB = 0.0, hr = 0.0, hp = 0.0;
+        poA = nA; poB = nB;
+        nA = 0.0; nB = 0.0;
+        if (padA) { nA = ld(pold + qA); if (it > 1) rA = ld(r + qA); }
+        if (padB) { nB = ld(pold + qB); if (it > 1) rB = ld(r + qB); }
+        if (hin) {
+          const int qh = hi + PX * hj + PXY * kk;
+          hp = ld(pold + qh);
+          if (it > 1) hr = ld(r + qh);
+        }
+        const int cA = qA - PXY, cB = qB - PXY;
+        double axA = 0, ayA = 0, azA = 0, xA = 0, axB = 0, ayB = 0, azB = 0, xB = 0;
+        if (comp && inA) { axA = F.acx[cA]; ayA = F.acy[cA]; azA = F.acz[cA]; if (it > 1) xA = ld(F.x + cA); }
+        if (comp && inB) { axB = F.acx[cB]; ayB = F.acy[cB]; azB = F.acz[cB]; if (it > 1) xB = ld(F.x + cB); }
+        pl[slot][ty + 1][tx + 1] = it == 1 ? nA : rA + beta * nA;
+        pl[slot][ty + 9][tx + 1] = it == 1 ? nB : rB + beta * nB;
+        if (hx >= 0) pl[slot][hy][hx] = it == 1 ? hp : hr + beta * hp;
+        __syncthreads();
+        if (comp) {
+          const int sc = (slot + 3) & 3, sb = (slot + 2) & 3;
+          if (inA) {
+            const int y = ty + 1;
+            const double c0 = pl[sc][y][tx + 1];
+            const double d = axA + axA + ayA + ayA + azA + azA;
+            const double sv = d * c0 - azA * pl[sb][y][tx + 1] - ayA * pl[sc][y - 1][tx + 1] - axA * pl[sc][y][tx] -
+                              axA * pl[sc][y][tx + 2] - ayA * pl[sc][y + 1][tx + 1] - azA * pl[slot][y][tx + 1];
+            if (it > 1) F.x[cA] = xA + alpha_prev * poA;
+            pnew[cA] = c0;
+            F.s[cA] = sv;
+            acc += sv * c0;
+          }
+          if (inB) {
+            const int y = ty + 9;
+            const double c0 = pl[sc][y][tx + 1];
+            const double d = axB + axB + ayB + ayB + azB + azB;
+            const double sv = d * c0 - azB * pl[sb][y][tx + 1] - ayB * pl[sc][y - 1][tx + 1] - axB * pl[sc][y][tx] -
+                              axB * pl[sc][y][tx + 2] - ayB * pl[sc][y + 1][tx + 1] - azB * pl[slot][y][tx + 1];
+            if (it > 1) F.x[cB] = xB + alpha_prev * poB;
+            pnew[cB] = c0;
+            F.s[cB] = sv;
+            acc += sv * c0;
+          }
+        }
       }
-      const double ax = F.acx[q], ay = F.acy[q], az = F.acz[q];
-      const double d = ax + ax + ay + ay + az + az;
-      const double sv = d * pc - az * pB - ay * pS - ax * pW - ax * pE - ay * pN - az * pF;
-      pnew[q] = pc;
-      F.s[q] = sv;
-      acc += sv * pc;
+      __syncthreads();  // the next tile reuses the slots
     }
     const double sdotp = grid_sum(acc, partials, buf, sh, grid);
     if (sdotp == 0.0) { pending = false; break; }
     const double alpha = gamma / sdotp, gamma_old = gamma;
     acc = 0.0;
-    for (int c = tid; c < n; c += T) {
-      if (F.empty[c]) continue;
-      const int i = c % cx, j = (c / cx) % cy, k = c / (cx * cy);
-      const int q = (i + 1) + PX * (j + 1) + PXY * (k + 1);
-      const double rv = ld(F.r + q) - alpha * ld(F.s + q);
-      F.r[q] = rv;
-      acc += rv * rv;
+    {
+      double2 *r2 = reinterpret_cast<double2 *>(F.r);
+      const double2 *s2 = reinterpret_cast<const double2 *>(F.s);
+      const long long nh = npad / 2;
+      for (long long e = tid; e < nh; e += T) {
+        double2 rv = __ldcg(r2 + e), sv = __ldcg(s2 + e);
+        rv.x = rv.x - alpha * sv.x;
+        rv.y = rv.y - alpha * sv.y;
+        r2[e] = rv;
+        acc += rv.x * rv.x;
+        acc += rv.y * rv.y;
+      }
+      if ((npad & 1) && tid == 0) {
+        const long long e = npad - 1;
+        double rv = ld(F.r + e) - alpha * ld(F.s + e);
+        F.r[e] = rv;
+        acc += rv * rv;
+      }
     }
     gamma = grid_sum(acc, partials, buf, sh, grid);
     iprod = gamma;
@@ -686,7 +834,7 @@ __global__ void __launch_bounds__(kBlock) k_pcorr(FluidDev F, Prm P, double *par
       const int q = (i + 1) + PX * (j + 1) + PXY * (k + 1);
       F.x[q] = ld(F.x + q) + alpha_prev * ld(pold + q);
     }
-  if (tid == 0) { st->pcg_iters = it; st->pcg_relres = sqrt(iprod / bb); }
+  if (tid == 0) { st->pcg_iters = it; st->pcg_relres = sqrt(iprod / bb); st->cum_pcg_iters += it; st->cum_pcg_solves += 1; }
 }
 
 // Velocity correction, pressure update and p_temp refresh
@@ -831,7 +979,21 @@ struct DeviceState {
             *ibw_face = nullptr;
   int nibu = 0, nibv = 0, nibw = 0;
   // cooperative grid sizes
-  int g_gs[4] = {0, 0, 0, 0}, g_pcorr = 0;
+  int g_gs[4] = {0, 0, 0, 0}, g_pcorr = 0, tz = 16;
+  // optional per-phase CUDA-event timing on the engine stream
+  bool profiling = false;
+  std::vector<cudaEvent_t> ev_pool;
+  std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> ev_used;
+  cudaEvent_t ev_get() {
+    if (ev_pool.empty()) {
+      cudaEvent_t e;
+      HS_CUDA(cudaEventCreate(&e));
+      return e;
+    }
+    cudaEvent_t e = ev_pool.back();
+    ev_pool.pop_back();
+    return e;
+  }
   double *snap = nullptr, *ssnap = nullptr;
   int *spred = nullptr;
   bool have_matrix = false;
@@ -853,6 +1015,8 @@ struct DeviceState {
     return p;
   }
   ~DeviceState() {
+    for (auto &u : ev_used) { cudaEventDestroy(u.second.first); cudaEventDestroy(u.second.second); }
+    for (auto e : ev_pool) cudaEventDestroy(e);
     for (void *p : allocs) cudaFree(p);
     if (stats_host) cudaFreeHost(stats_host);
     if (stream) cudaStreamDestroy(stream);
@@ -913,6 +1077,17 @@ Engine::Engine(const Case &c, const hs_params &p, int device) : case_(c), prm_(p
   F.xp = D.upload(c.xp); F.xw = D.upload(c.xw); F.xe = D.upload(c.xe);
   F.yp = D.upload(c.yp); F.ys = D.upload(c.ys); F.yn = D.upload(c.yn);
   F.zp = D.upload(c.zp); F.zf = D.upload(c.zf); F.zb = D.upload(c.zb);
+  {
+    auto inv2 = [](const std::vector<double> &p, const std::vector<double> &m) {
+      std::vector<double> o(p.size(), 0.0);
+      for (size_t i = 1; i + 1 < p.size(); ++i) {
+        double sp = (p[i] + m[i]) / 2.0;
+        o[i] = 1 / sp / sp;
+      }
+      return o;
+    };
+    F.ix2 = D.upload(inv2(c.xp, c.xw)); F.iy2 = D.upload(inv2(c.yp, c.ys)); F.iz2 = D.upload(inv2(c.zp, c.zf));
+  }
   F.acx = D.alloc<double>(M.npad()); F.acy = D.alloc<double>(M.npad()); F.acz = D.alloc<double>(M.npad());
   F.x = D.alloc<double>(M.npad()); F.r = D.alloc<double>(M.npad()); F.pa = D.alloc<double>(M.npad());
   F.pb = D.alloc<double>(M.npad()); F.s = D.alloc<double>(M.npad());
@@ -1006,6 +1181,18 @@ Engine::Engine(const Case &c, const hs_params &p, int device) : case_(c), prm_(p
     D.g_gs[3] = coop_blocks(k_gs<3>, D.nsm, (int)std::min<long>((rows[3] + 1) / 2, 1 << 20));
   }
   D.g_pcorr = coop_blocks(k_pcorr, D.nsm, 1 << 30);
+  {
+    // z-depth of the CG tiles: balance tiles over the resident blocks and
+    // keep the two halo planes a small share of each tile
+    long ntxy = ((M.cx + kTX - 1) / kTX) * ((M.cy + kTY - 1) / kTY);
+    double best = -1;
+    for (int tz = 4; tz <= 64; ++tz) {
+      long nt = ntxy * ((M.cz + tz - 1) / tz);
+      long rounds = (nt + D.g_pcorr - 1) / D.g_pcorr;
+      double eff = (double)M.cz / ((double)rounds * D.g_pcorr / ntxy * tz) * (double)tz / (tz + 2);
+      if (eff > best) { best = eff; D.tz = tz; }
+    }
+  }
   D.snap = D.alloc<double>(std::max({M.nu(), M.nv(), M.nw(), M.npad()}));
   D.ssnap = D.alloc<double>(std::max<long long>(D.ntt, 1));
   D.spred = D.alloc<int>(std::max(D.nreg, 1));
@@ -1053,36 +1240,93 @@ void Engine::step(int nsteps) {
   cudaStream_t s = D.stream;
   const long n = (long)D.F.cx * D.F.cy * D.F.cz;
   const long nplane = std::max({(D.F.cz + 2) * (D.F.cy + 2), (D.F.cz + 2) * (D.F.cx + 2), (D.F.cy + 2) * (D.F.cx + 2)});
+  struct Mark {
+    DeviceState &D;
+    int phase;
+    cudaEvent_t a = nullptr;
+    Mark(DeviceState &d, int ph) : D(d), phase(ph) {
+      if (D.profiling) { a = D.ev_get(); HS_CUDA(cudaEventRecord(a, D.stream)); }
+    }
+    ~Mark() {
+      if (a) {
+        cudaEvent_t b = D.ev_get();
+        cudaEventRecord(b, D.stream);
+        D.ev_used.push_back({phase, {a, b}});
+      }
+    }
+  };
   for (int it = 0; it < nsteps; ++it) {
     // FluidSolver::solve (fluid_solver.h:1401-1633)
-    coop_launch(k_gs<0>, D.g_gs[0], s, D.F, D.P, D.partials, D.stats, D.snap);
-    coop_launch(k_gs<1>, D.g_gs[1], s, D.F, D.P, D.partials, D.stats, D.snap);
-    coop_launch(k_gs<2>, D.g_gs[2], s, D.F, D.P, D.partials, D.stats, D.snap);
+    { Mark m(D, 0); coop_launch(k_gs<0>, D.g_gs[0], s, D.F, D.P, D.partials, D.stats, D.snap); }
+    { Mark m(D, 1); coop_launch(k_gs<1>, D.g_gs[1], s, D.F, D.P, D.partials, D.stats, D.snap); }
+    { Mark m(D, 2); coop_launch(k_gs<2>, D.g_gs[2], s, D.F, D.P, D.partials, D.stats, D.snap); }
     int assemble = (!D.have_matrix || !prm_.frozen_matrix) ? 1 : 0;
-    coop_launch(k_pcorr, D.g_pcorr, s, D.F, D.P, D.partials, D.stats, assemble);
+    { Mark m(D, 3); coop_launch(k_pcorr, D.g_pcorr, s, D.F, D.P, D.partials, D.stats, assemble, D.tz); }
     D.have_matrix = true;
-    k_correct<<<grid_for(n), kBlock, 0, s>>>(D.F, D.P);
-    HS_CUDA(cudaMemsetAsync(D.F.x, 0, sizeof(double) * (size_t)case_.fluid.npad(), s));
-    coop_launch(k_gs<3>, D.g_gs[3], s, D.F, D.P, D.partials, D.stats, D.snap);
+    {
+      Mark m(D, 4);
+      k_correct<<<grid_for(n), kBlock, 0, s>>>(D.F, D.P);
+      HS_CUDA(cudaMemsetAsync(D.F.x, 0, sizeof(double) * (size_t)case_.fluid.npad(), s));
+    }
+    { Mark m(D, 5); coop_launch(k_gs<3>, D.g_gs[3], s, D.F, D.P, D.partials, D.stats, D.snap); }
     // MobSolver::solve for every region
-    if (D.nreg)
+    if (D.nreg) {
+      Mark m(D, 6);
       coop_launch(k_solid, D.solid_blocks, s, (const SolidReg *)D.regs, D.nreg, (const int *)D.blk_reg, D.stt, D.stc,
                   (const uint8_t *)D.sem, D.P, D.partials, D.stats, D.ssnap, D.spred);
-    // interface swap (solver.h:83-148)
-    if (D.nswap) {
-      k_swap_gather<<<grid_for(D.nswap), kBlock, 0, s>>>(D.f_send, D.s_send, D.nswap, D.F.tt, D.stt, D.fbuf, D.sbuf);
-      k_swap_scatter<<<grid_for(D.nswap), kBlock, 0, s>>>(D.f_recv, D.s_recv, D.nswap, D.F.tt, D.stt, D.fbuf, D.sbuf);
     }
-    // FluidSolver::setForNext (fluid_solver.h:1634-1682)
-    for (int which = 0; which < 3; ++which) k_bc<<<grid_for(nplane), kBlock, 0, s>>>(D.F, D.P, which);
-    k_cellbc_resolve<<<grid_for(n), kBlock, 0, s>>>(D.F);
-    k_cellbc_commit<<<grid_for(n), kBlock, 0, s>>>(D.F, D.P, 1);
-    // MobSolver::setForNext
-    if (D.nreg) k_solid_setfornext<<<dim3(64, std::min(D.nreg, 64)), kBlock, 0, s>>>(D.regs, D.nreg, D.stt, D.stc, D.sem);
+    {
+      Mark m(D, 7);
+      // interface swap (solver.h:83-148)
+      if (D.nswap) {
+        k_swap_gather<<<grid_for(D.nswap), kBlock, 0, s>>>(D.f_send, D.s_send, D.nswap, D.F.tt, D.stt, D.fbuf, D.sbuf);
+        k_swap_scatter<<<grid_for(D.nswap), kBlock, 0, s>>>(D.f_recv, D.s_recv, D.nswap, D.F.tt, D.stt, D.fbuf, D.sbuf);
+      }
+      // FluidSolver::setForNext (fluid_solver.h:1634-1682)
+      for (int which = 0; which < 3; ++which) k_bc<<<grid_for(nplane), kBlock, 0, s>>>(D.F, D.P, which);
+      k_cellbc_resolve<<<grid_for(n), kBlock, 0, s>>>(D.F);
+      k_cellbc_commit<<<grid_for(n), kBlock, 0, s>>>(D.F, D.P, 1);
+      // MobSolver::setForNext
+      if (D.nreg) k_solid_setfornext<<<dim3(64, std::min(D.nreg, 64)), kBlock, 0, s>>>(D.regs, D.nreg, D.stt, D.stc, D.sem);
+    }
     HS_CUDA(cudaGetLastError());
     steps_++;
   }
 }
+
+void Engine::profile(bool on) {
+  HS_CUDA(cudaSetDevice(device_));
+  d_->profiling = on;
+}
+
+int Engine::profile_read(double *ms, int nphase) {
+  HS_CUDA(cudaSetDevice(device_));
+  DeviceState &D = *d_;
+  HS_CUDA(cudaStreamSynchronize(D.stream));
+  for (int q = 0; q < nphase; ++q) ms[q] = 0.0;
+  int count = 0;
+  for (auto &u : D.ev_used) {
+    float t = 0.f;
+    HS_CUDA(cudaEventElapsedTime(&t, u.second.first, u.second.second));
+    if (u.first < nphase) ms[u.first] += t;
+    if (u.first == 0) ++count;
+    D.ev_pool.push_back(u.second.first);
+    D.ev_pool.push_back(u.second.second);
+  }
+  D.ev_used.clear();
+  return count;
+}
+
+void Engine::counters(long long *out8) {
+  DeviceState &D = *d_;
+  HS_CUDA(cudaMemcpyAsync(D.stats_host, D.stats, sizeof(DevStats), cudaMemcpyDeviceToHost, D.stream));
+  HS_CUDA(cudaStreamSynchronize(D.stream));
+  const DevStats &h = *D.stats_host;
+  out8[0] = h.cum_sweeps[0]; out8[1] = h.cum_sweeps[1]; out8[2] = h.cum_sweeps[2]; out8[3] = h.cum_sweeps[3];
+  out8[4] = h.cum_solid_cell_sweeps; out8[5] = h.cum_pcg_iters; out8[6] = h.cum_pcg_solves; out8[7] = steps_;
+}
+
+void *Engine::stream_handle() { return (void *)d_->stream; }
 
 void Engine::sync() {
   HS_CUDA(cudaSetDevice(device_));

@@ -26,6 +26,10 @@ class Engine {
   void step(int n);
   void sync();
   void stats(hs_stats *out);
+  void profile(bool on);
+  int profile_read(double *ms, int nphase);
+  void counters(long long *out8);
+  void *stream_handle();
 
   long field_size(int f) const;
   void get_field(int f, double *host, long n);

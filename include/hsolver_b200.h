@@ -101,6 +101,21 @@ int hs_step(hs_ctx *ctx, int n, hs_stats *stats);
 
 /* Wait for the context's stream. */
 int hs_sync(hs_ctx *ctx);
+/* The context's cudaStream_t (as void*), for callers that order their own
+ * work after hs_step. */
+int hs_stream(hs_ctx *ctx, void **stream);
+
+/* Per-phase timing with CUDA events on the context's stream.  Phases:
+ * 0-2 u/v/w momentum, 3 pressure-correction solve, 4 velocity/pressure
+ * correction, 5 fluid energy, 6 solid energy, 7 swap + setForNext.
+ * hs_profile_read returns the summed milliseconds per phase since the last
+ * read and the number of steps they cover. */
+#define HS_NPHASE 8
+int hs_profile(hs_ctx *ctx, int on);
+int hs_profile_read(hs_ctx *ctx, double ms[HS_NPHASE], int *steps);
+/* Running counters since creation: sweeps of u, v, w, fluid T; solid
+ * cell-sweeps; CG iterations; CG solves; outer steps. */
+int hs_counters(hs_ctx *ctx, long long out8[8]);
 
 /* Field access (host buffers; blocking). */
 int hs_field_size(hs_ctx *ctx, int field, long long *n);
