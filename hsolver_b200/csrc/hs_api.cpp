@@ -19,6 +19,10 @@ struct hs_case {
   hs::Case c;
 };
 
+struct hs_pcg {
+  hs::PcgWork *w = nullptr;
+};
+
 namespace {
 thread_local std::string g_err;
 
@@ -318,6 +322,43 @@ int hs_case_geometry(const hs_case *c, int axis, double *out, long long n) {
 }
 
 void hs_case_destroy(hs_case *c) { delete c; }
+
+int hs_pcg_create(int nx, int ny, int nz, int device, hs_pcg **out) {
+  if (!out) return fail(nullptr, HS_ERR_ARG, "null output pointer");
+  *out = nullptr;
+  try {
+    hs_pcg *h = new hs_pcg();
+    try {
+      h->w = hs::pcg_create(nx, ny, nz, device);
+    } catch (...) {
+      delete h;
+      throw;
+    }
+    *out = h;
+    return HS_OK;
+  } catch (const std::bad_alloc &) {
+    return fail(nullptr, HS_ERR_NOMEM, "host allocation failed");
+  } catch (const std::exception &e) {
+    return fail(nullptr, classify(e), e.what());
+  }
+}
+
+int hs_pcg_solve(hs_pcg *h, const double *acx, const double *acy, const double *acz, const double *b, double *x,
+                 double tol, int maxiter, void *stream, int *iters, double *relres) {
+  if (!h || !h->w) return fail(nullptr, HS_ERR_ARG, "null solver handle");
+  try {
+    hs::pcg_solve(h->w, acx, acy, acz, b, x, tol, maxiter, stream, iters, relres);
+    return HS_OK;
+  } catch (const std::exception &e) {
+    return fail(nullptr, classify(e), e.what());
+  }
+}
+
+void hs_pcg_destroy(hs_pcg *h) {
+  if (!h) return;
+  hs::pcg_destroy(h->w);
+  delete h;
+}
 
 void hs_destroy(hs_ctx *ctx) {
   if (!ctx) return;

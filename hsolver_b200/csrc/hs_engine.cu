@@ -677,14 +677,145 @@ __global__ void k_swap_scatter(const long long *f_recv, const long long *s_recv,
 // r and p are read once.  Coefficients are zero off the fluid cells, where
 // r, p, x, s stay zero, so no mask test is needed.  Pass B (r -= alpha s,
 // <r,r>) streams the padded arrays as double2.
-constexpr int kTX = 32, kTY = 16;  // tile of 32 x 16 columns; a thread owns rows ty and ty + 8
+constexpr int kTX = 32, kTY = 16;  // CG tiles of 32 x 16 columns; a thread owns rows ty and ty + 8
+
+// The CG iterations of hypre_PCGSolve restated (identity preconditioner,
+// two-norm test <r,r>/<b,b> < tol^2, maxiter): on entry r = p_a = b, x = 0 on
+// the padded grid and bb = <b,b>.  Coefficients are zero off the unknowns.
+struct CgView {
+  int cx, cy, cz;
+  const double *acx, *acy, *acz;
+  double *x, *r, *pa, *pb, *s;
+};
+
+__device__ void cg_core(const CgView &V, double bb, double tol, int maxiter, double *partials, int &buf, double *sh,
+                        cg::grid_group &grid, int TZ, int *out_iters, double *out_relres) {
+  __shared__ double pl[4][kTY + 2][kTX + 2];  // four plane slots: the plane written at kk never aliases those read at kk - 1
+  const int cx = V.cx, cy = V.cy, cz = V.cz;
+  const int PX = cx + 2, PXY = (cx + 2) * (cy + 2);
+  const long long npad = (long long)PXY * (cz + 2);
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x, T = gridDim.x * blockDim.x;
+  const double eps = tol * tol;
+  double gamma = bb, iprod = bb, beta = 0.0, alpha_prev = 0.0, acc;
+  double *pold = V.pa, *pnew = V.pb;
+  const int ntx = (cx + kTX - 1) / kTX, nty = (cy + kTY - 1) / kTY, ntz = (cz + TZ - 1) / TZ;
+  const int ntiles = ntx * nty * ntz;
+  const int tx = threadIdx.x % kTX, ty = threadIdx.x / kTX;  // ty in [0, 8)
+  // halo role (96 cells: y-1 row, y+16 row, x-1 column, x+32 column)
+  const int h = threadIdx.x;
+  int hx = -1, hy = -1;
+  if (h < kTX) { hx = h + 1; hy = 0; }
+  else if (h < 2 * kTX) { hx = h - kTX + 1; hy = kTY + 1; }
+  else if (h < 2 * kTX + kTY) { hx = 0; hy = h - 2 * kTX + 1; }
+  else if (h < 2 * kTX + 2 * kTY) { hx = kTX + 1; hy = h - 2 * kTX - kTY + 1; }
+  int it = 0;
+  bool pending = false;
+  while (it + 1 <= maxiter) {
+    it++;
+    acc = 0.0;
+    const double *r = V.r;
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+      const int tz = tile / (ntx * nty), rem = tile % (ntx * nty);
+      const int i0 = 1 + (rem % ntx) * kTX, j0 = 1 + (rem / ntx) * kTY, k0 = 1 + tz * TZ;
+      const int kend = min(k0 + TZ - 1, cz);
+      const int i = i0 + tx, ja = j0 + ty, jb = ja + 8;
+      const bool inA = i <= cx && ja <= cy, inB = i <= cx && jb <= cy;
+      const bool padA = i <= cx + 1 && ja <= cy + 1, padB = i <= cx + 1 && jb <= cy + 1;
+      const int hi = i0 - 1 + hx, hj = j0 - 1 + hy;
+      const bool hin = hx >= 0 && hi <= cx + 1 && hj <= cy + 1;
+      double poA = 0.0, poB = 0.0;  // p_old of the plane being computed (kk - 1)
+      double nA = 0.0, nB = 0.0;    // p_old of plane kk
+      for (int kk = k0 - 1; kk <= kend + 1; ++kk) {
+        const int slot = (kk - k0 + 1) & 3;
+        const bool comp = kk >= k0 + 1;
+        // issue every load of this plane step before using any of them
+        const int qA = i + PX * ja + PXY * kk, qB = qA + 8 * PX;
+        double rA = 0.0, rB = 0.0, hr = 0.0, hp = 0.0;
+        poA = nA; poB = nB;
+        nA = 0.0; nB = 0.0;
+        if (padA) { nA = ld(pold + qA); if (it > 1) rA = ld(r + qA); }
+        if (padB) { nB = ld(pold + qB); if (it > 1) rB = ld(r + qB); }
+        if (hin) {
+          const int qh = hi + PX * hj + PXY * kk;
+          hp = ld(pold + qh);
+          if (it > 1) hr = ld(r + qh);
+        }
+        const int cA = qA - PXY, cB = qB - PXY;
+        double axA = 0, ayA = 0, azA = 0, xA = 0, axB = 0, ayB = 0, azB = 0, xB = 0;
+        if (comp && inA) { axA = V.acx[cA]; ayA = V.acy[cA]; azA = V.acz[cA]; if (it > 1) xA = ld(V.x + cA); }
+        if (comp && inB) { axB = V.acx[cB]; ayB = V.acy[cB]; azB = V.acz[cB]; if (it > 1) xB = ld(V.x + cB); }
+        pl[slot][ty + 1][tx + 1] = it == 1 ? nA : rA + beta * nA;
+        pl[slot][ty + 9][tx + 1] = it == 1 ? nB : rB + beta * nB;
+        if (hx >= 0) pl[slot][hy][hx] = it == 1 ? hp : hr + beta * hp;
+        __syncthreads();
+        if (comp) {
+          const int sc = (slot + 3) & 3, sb = (slot + 2) & 3;
+          if (inA) {
+            const int y = ty + 1;
+            const double c0 = pl[sc][y][tx + 1];
+            const double d = axA + axA + ayA + ayA + azA + azA;
+            const double sv = d * c0 - azA * pl[sb][y][tx + 1] - ayA * pl[sc][y - 1][tx + 1] - axA * pl[sc][y][tx] -
+                              axA * pl[sc][y][tx + 2] - ayA * pl[sc][y + 1][tx + 1] - azA * pl[slot][y][tx + 1];
+            if (it > 1) V.x[cA] = xA + alpha_prev * poA;
+            pnew[cA] = c0;
+            V.s[cA] = sv;
+            acc += sv * c0;
+          }
+          if (inB) {
+            const int y = ty + 9;
+            const double c0 = pl[sc][y][tx + 1];
+            const double d = axB + axB + ayB + ayB + azB + azB;
+            const double sv = d * c0 - azB * pl[sb][y][tx + 1] - ayB * pl[sc][y - 1][tx + 1] - axB * pl[sc][y][tx] -
+                              axB * pl[sc][y][tx + 2] - ayB * pl[sc][y + 1][tx + 1] - azB * pl[slot][y][tx + 1];
+            if (it > 1) V.x[cB] = xB + alpha_prev * poB;
+            pnew[cB] = c0;
+            V.s[cB] = sv;
+            acc += sv * c0;
+          }
+        }
+      }
+      __syncthreads();  // the next tile reuses the slots
+    }
+    const double sdotp = grid_sum(acc, partials, buf, sh, grid);
+    if (sdotp == 0.0) { pending = false; break; }
+    const double alpha = gamma / sdotp, gamma_old = gamma;
+    acc = 0.0;
+    {
+      double2 *r2 = reinterpret_cast<double2 *>(V.r);
+      const double2 *s2 = reinterpret_cast<const double2 *>(V.s);
+      const long long nh = npad / 2;
+      for (long long e = tid; e < nh; e += T) {
+        double2 rv = __ldcg(r2 + e), sv = __ldcg(s2 + e);
+        rv.x = rv.x - alpha * sv.x;
+        rv.y = rv.y - alpha * sv.y;
+        r2[e] = rv;
+        acc += rv.x * rv.x;
+        acc += rv.y * rv.y;
+      }
+      if ((npad & 1) && tid == 0) {
+        const long long e = npad - 1;
+        double rv = ld(V.r + e) - alpha * ld(V.s + e);
+        V.r[e] = rv;
+        acc += rv * rv;
+      }
+    }
+    gamma = grid_sum(acc, partials, buf, sh, grid);
+    iprod = gamma;
+    alpha_prev = alpha;
+    pending = true;
+    double *t = pold; pold = pnew; pnew = t;
+    if (iprod / bb < eps) break;
+    beta = gamma / gamma_old;
+  }
+  if (pending)
+    for (long long e = tid; e < npad; e += T) V.x[e] = ld(V.x + e) + alpha_prev * ld(pold + e);
+  if (tid == 0) { *out_iters = it; *out_relres = sqrt(iprod / bb); }
+}
 
 __global__ void __launch_bounds__(kBlock) k_pcorr(FluidDev F, Prm P, double *partials, DevStats *st, int assemble,
                                                   int TZ) {
   cg::grid_group grid = cg::this_grid();
   __shared__ double sh[33];
-  // four plane slots: the plane written at kk never aliases the three read at kk - 1
-  __shared__ double pl[4][kTY + 2][kTX + 2];
   const int cx = F.cx, cy = F.cy, cz = F.cz, n = cx * cy * cz;
   const int PX = cx + 2, PXY = (cx + 2) * (cy + 2);
   const long long npad = (long long)PXY * (cz + 2);
@@ -715,126 +846,40 @@ __global__ void __launch_bounds__(kBlock) k_pcorr(FluidDev F, Prm P, double *par
     if (tid == 0) { st->pcg_iters = 0; st->pcg_relres = 0.0; st->cum_pcg_solves += 1; }
     return;
   }
-  const double eps = P.pcg_tol * P.pcg_tol;
-  double gamma = bb, iprod = bb, beta = 0.0, alpha_prev = 0.0;
-  double *pold = F.pa, *pnew = F.pb;
-  const int ntx = (cx + kTX - 1) / kTX, nty = (cy + kTY - 1) / kTY, ntz = (cz + TZ - 1) / TZ;
-  const int ntiles = ntx * nty * ntz;
-  const int tx = threadIdx.x % kTX, ty = threadIdx.x / kTX;  // ty in [0, 8)
-  // halo role (96 cells: y-1 row, y+16 row, x-1 column, x+32 column)
-  const int h = threadIdx.x;
-  int hx = -1, hy = -1;
-  if (h < kTX) { hx = h + 1; hy = 0; }
-  else if (h < 2 * kTX) { hx = h - kTX + 1; hy = kTY + 1; }
-  else if (h < 2 * kTX + kTY) { hx = 0; hy = h - 2 * kTX + 1; }
-  else if (h < 2 * kTX + 2 * kTY) { hx = kTX + 1; hy = h - 2 * kTX - kTY + 1; }
-  int it = 0;
-  bool pending = false;
-  while (it + 1 <= P.pcg_maxiter) {
-    it++;
-    acc = 0.0;
-    const double *r = F.r;
-    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-      const int tz = tile / (ntx * nty), rem = tile % (ntx * nty);
-      const int i0 = 1 + (rem % ntx) * kTX, j0 = 1 + (rem / ntx) * kTY, k0 = 1 + tz * TZ;
-      const int kend = min(k0 + TZ - 1, cz);
-      const int i = i0 + tx, ja = j0 + ty, jb = ja + 8;
-      const bool inA = i <= cx && ja <= cy, inB = i <= cx && jb <= cy;
-      const bool padA = i <= cx + 1 && ja <= cy + 1, padB = i <= cx + 1 && jb <= cy + 1;
-      const int hi = i0 - 1 + hx, hj = j0 - 1 + hy;
-      const bool hin = hx >= 0 && hi <= cx + 1 && hj <= cy + 1;
-      double poA = 0.0, poB = 0.0;  // p_old of the plane being computed (kk - 1)
-      double nA = 0.0, nB = 0.0;    // p_old of plane kk
-      for (int kk = k0 - 1; kk <= kend + 1; ++kk) {
-        const int slot = (kk - k0 + 1) & 3;
-        const bool comp = kk >= k0 + 1;
-        // issue every load of this plane step before using any of them
-        const int qA = i + PX * ja + PXY * kk, qB = qA + 8 * PX;
-        double rA = 0.0, rB = 0.0, hr = 0.0, hp = 0.0;
-        poA = nA; poB = nB;
-        nA = 0.0; nB = 0.0;
-        if (padA) { nA = ld(pold + qA); if (it > 1) rA = ld(r + qA); }
-        if (padB) { nB = ld(pold + qB); if (it > 1) rB = ld(r + qB); }
-        if (hin) {
-          const int qh = hi + PX * hj + PXY * kk;
-          hp = ld(pold + qh);
-          if (it > 1) hr = ld(r + qh);
-        }
-        const int cA = qA - PXY, cB = qB - PXY;
-        double axA = 0, ayA = 0, azA = 0, xA = 0, axB = 0, ayB = 0, azB = 0, xB = 0;
-        if (comp && inA) { axA = F.acx[cA]; ayA = F.acy[cA]; azA = F.acz[cA]; if (it > 1) xA = ld(F.x + cA); }
-        if (comp && inB) { axB = F.acx[cB]; ayB = F.acy[cB]; azB = F.acz[cB]; if (it > 1) xB = ld(F.x + cB); }
-        pl[slot][ty + 1][tx + 1] = it == 1 ? nA : rA + beta * nA;
-        pl[slot][ty + 9][tx + 1] = it == 1 ? nB : rB + beta * nB;
-        if (hx >= 0) pl[slot][hy][hx] = it == 1 ? hp : hr + beta * hp;
-        __syncthreads();
-        if (comp) {
-          const int sc = (slot + 3) & 3, sb = (slot + 2) & 3;
-          if (inA) {
-            const int y = ty + 1;
-            const double c0 = pl[sc][y][tx + 1];
-            const double d = axA + axA + ayA + ayA + azA + azA;
-            const double sv = d * c0 - azA * pl[sb][y][tx + 1] - ayA * pl[sc][y - 1][tx + 1] - axA * pl[sc][y][tx] -
-                              axA * pl[sc][y][tx + 2] - ayA * pl[sc][y + 1][tx + 1] - azA * pl[slot][y][tx + 1];
-            if (it > 1) F.x[cA] = xA + alpha_prev * poA;
-            pnew[cA] = c0;
-            F.s[cA] = sv;
-            acc += sv * c0;
-          }
-          if (inB) {
-            const int y = ty + 9;
-            const double c0 = pl[sc][y][tx + 1];
-            const double d = axB + axB + ayB + ayB + azB + azB;
-            const double sv = d * c0 - azB * pl[sb][y][tx + 1] - ayB * pl[sc][y - 1][tx + 1] - axB * pl[sc][y][tx] -
-                              axB * pl[sc][y][tx + 2] - ayB * pl[sc][y + 1][tx + 1] - azB * pl[slot][y][tx + 1];
-            if (it > 1) F.x[cB] = xB + alpha_prev * poB;
-            pnew[cB] = c0;
-            F.s[cB] = sv;
-            acc += sv * c0;
-          }
-        }
-      }
-      __syncthreads();  // the next tile reuses the slots
-    }
-    const double sdotp = grid_sum(acc, partials, buf, sh, grid);
-    if (sdotp == 0.0) { pending = false; break; }
-    const double alpha = gamma / sdotp, gamma_old = gamma;
-    acc = 0.0;
-    {
-      double2 *r2 = reinterpret_cast<double2 *>(F.r);
-      const double2 *s2 = reinterpret_cast<const double2 *>(F.s);
-      const long long nh = npad / 2;
-      for (long long e = tid; e < nh; e += T) {
-        double2 rv = __ldcg(r2 + e), sv = __ldcg(s2 + e);
-        rv.x = rv.x - alpha * sv.x;
-        rv.y = rv.y - alpha * sv.y;
-        r2[e] = rv;
-        acc += rv.x * rv.x;
-        acc += rv.y * rv.y;
-      }
-      if ((npad & 1) && tid == 0) {
-        const long long e = npad - 1;
-        double rv = ld(F.r + e) - alpha * ld(F.s + e);
-        F.r[e] = rv;
-        acc += rv * rv;
-      }
-    }
-    gamma = grid_sum(acc, partials, buf, sh, grid);
-    iprod = gamma;
-    alpha_prev = alpha;
-    pending = true;
-    double *t = pold; pold = pnew; pnew = t;
-    if (iprod / bb < eps) break;
-    beta = gamma / gamma_old;
+  CgView V{cx, cy, cz, F.acx, F.acy, F.acz, F.x, F.r, F.pa, F.pb, F.s};
+  int iters = 0;
+  double relres = 0.0;
+  cg_core(V, bb, P.pcg_tol, P.pcg_maxiter, partials, buf, sh, grid, TZ, &iters, &relres);
+  if (tid == 0) {
+    st->pcg_iters = iters; st->pcg_relres = relres; st->cum_pcg_iters += iters; st->cum_pcg_solves += 1;
   }
-  if (pending)
-    for (int c = tid; c < n; c += T) {
-      if (F.empty[c]) continue;
-      const int i = c % cx, j = (c / cx) % cy, k = c / (cx * cy);
-      const int q = (i + 1) + PX * (j + 1) + PXY * (k + 1);
-      F.x[q] = ld(F.x + q) + alpha_prev * ld(pold + q);
-    }
-  if (tid == 0) { st->pcg_iters = it; st->pcg_relres = sqrt(iprod / bb); st->cum_pcg_iters += it; st->cum_pcg_solves += 1; }
+}
+
+// Standalone HYPRE-rule CG on caller-provided padded arrays: r = p_a = b,
+// x = 0, then cg_core (hs_pcg_solve).
+__global__ void __launch_bounds__(kBlock) k_pcg(CgView V, const double *b, double tol, int maxiter, double *partials,
+                                                int TZ, int *out_iters, double *out_relres) {
+  cg::grid_group grid = cg::this_grid();
+  __shared__ double sh[33];
+  const long long npad = (long long)(V.cx + 2) * (V.cy + 2) * (V.cz + 2);
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x, T = gridDim.x * blockDim.x;
+  int buf = 0;
+  double acc = 0.0;
+  for (long long e = tid; e < npad; e += T) {
+    const double bv = b[e];
+    V.r[e] = bv;
+    V.pa[e] = bv;
+    V.pb[e] = 0.0;
+    V.s[e] = 0.0;
+    V.x[e] = 0.0;
+    acc += bv * bv;
+  }
+  const double bb = grid_sum(acc, partials, buf, sh, grid);
+  if (bb == 0.0) {
+    if (tid == 0) { *out_iters = 0; *out_relres = 0.0; }
+    return;
+  }
+  cg_core(V, bb, tol, maxiter, partials, buf, sh, grid, TZ, out_iters, out_relres);
 }
 
 // Velocity correction, pressure update and p_temp refresh
@@ -1034,6 +1079,21 @@ int coop_blocks(K kernel, int nsm, int want) {
   return std::max(1, std::min(cap, want));
 }
 
+// z-depth of the CG tiles: balance tiles over the resident blocks and keep
+// the two halo planes a small share of each tile
+int choose_tz(long cx, long cy, long cz, int grid) {
+  long ntxy = ((cx + kTX - 1) / kTX) * ((cy + kTY - 1) / kTY);
+  double best = -1;
+  int tz_best = 16;
+  for (int tz = 4; tz <= 64; ++tz) {
+    long nt = ntxy * ((cz + tz - 1) / tz);
+    long rounds = (nt + grid - 1) / grid;
+    double eff = (double)cz / ((double)rounds * grid / ntxy * tz) * (double)tz / (tz + 2);
+    if (eff > best) { best = eff; tz_best = tz; }
+  }
+  return tz_best;
+}
+
 template <class K, class... A>
 void coop_launch(K kernel, int blocks, cudaStream_t s, A... args) {
   void *argv[] = {(void *)&args...};
@@ -1181,18 +1241,7 @@ Engine::Engine(const Case &c, const hs_params &p, int device) : case_(c), prm_(p
     D.g_gs[3] = coop_blocks(k_gs<3>, D.nsm, (int)std::min<long>((rows[3] + 1) / 2, 1 << 20));
   }
   D.g_pcorr = coop_blocks(k_pcorr, D.nsm, 1 << 30);
-  {
-    // z-depth of the CG tiles: balance tiles over the resident blocks and
-    // keep the two halo planes a small share of each tile
-    long ntxy = ((M.cx + kTX - 1) / kTX) * ((M.cy + kTY - 1) / kTY);
-    double best = -1;
-    for (int tz = 4; tz <= 64; ++tz) {
-      long nt = ntxy * ((M.cz + tz - 1) / tz);
-      long rounds = (nt + D.g_pcorr - 1) / D.g_pcorr;
-      double eff = (double)M.cz / ((double)rounds * D.g_pcorr / ntxy * tz) * (double)tz / (tz + 2);
-      if (eff > best) { best = eff; D.tz = tz; }
-    }
-  }
+  D.tz = choose_tz(M.cx, M.cy, M.cz, D.g_pcorr);
   D.snap = D.alloc<double>(std::max({M.nu(), M.nv(), M.nw(), M.npad()}));
   D.ssnap = D.alloc<double>(std::max<long long>(D.ntt, 1));
   D.spred = D.alloc<int>(std::max(D.nreg, 1));
@@ -1405,6 +1454,65 @@ void Engine::get_solid(int r, int which, double *host, long n) {
   const double *src = which == 0 ? D.stt + R.tt_off : D.stc + R.tc_off;
   HS_CUDA(cudaMemcpyAsync(host, src, sizeof(double) * n, cudaMemcpyDeviceToHost, D.stream));
   HS_CUDA(cudaStreamSynchronize(D.stream));
+}
+
+// ---------------------------------------------------------------- standalone CG
+struct PcgWork {
+  int device = 0, cx = 0, cy = 0, cz = 0, grid = 0, tz = 16;
+  double *r = nullptr, *pa = nullptr, *pb = nullptr, *s = nullptr, *partials = nullptr, *relres = nullptr;
+  int *iters = nullptr;
+};
+
+PcgWork *pcg_create(int nx, int ny, int nz, int device) {
+  if (nx < 1 || ny < 1 || nz < 1) throw std::invalid_argument("grid dimensions must be positive");
+  long long npad = (long long)(nx + 2) * (ny + 2) * (nz + 2);
+  if (npad > (1LL << 31) - 1) throw std::invalid_argument("grid too large for 32-bit indexing");
+  HS_CUDA(cudaSetDevice(device));
+  int nsm = 0;
+  HS_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
+  std::unique_ptr<PcgWork> w(new PcgWork());
+  w->device = device; w->cx = nx; w->cy = ny; w->cz = nz;
+  w->grid = coop_blocks(k_pcg, nsm, 1 << 30);
+  w->tz = choose_tz(nx, ny, nz, w->grid);
+  auto get = [](void **p, size_t bytes) {
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess) throw std::runtime_error(std::string("CUDA alloc: ") + cudaGetErrorString(e));
+  };
+  try {
+    get((void **)&w->r, npad * 8); get((void **)&w->pa, npad * 8); get((void **)&w->pb, npad * 8);
+    get((void **)&w->s, npad * 8); get((void **)&w->partials, 2 * (size_t)w->grid * kBlock * 8);
+    get((void **)&w->relres, 8); get((void **)&w->iters, 4);
+  } catch (...) {
+    pcg_destroy(w.release());
+    throw;
+  }
+  return w.release();
+}
+
+void pcg_destroy(PcgWork *w) {
+  if (!w) return;
+  cudaSetDevice(w->device);
+  for (void *p : {(void *)w->r, (void *)w->pa, (void *)w->pb, (void *)w->s, (void *)w->partials, (void *)w->relres,
+                  (void *)w->iters})
+    if (p) cudaFree(p);
+  delete w;
+}
+
+void pcg_solve(PcgWork *w, const double *acx, const double *acy, const double *acz, const double *b, double *x,
+               double tol, int maxiter, void *stream, int *iters, double *relres) {
+  if (!acx || !acy || !acz || !b || !x) throw std::invalid_argument("null device pointer");
+  if (maxiter < 0 || !(tol >= 0)) throw std::invalid_argument("invalid tolerance or iteration limit");
+  HS_CUDA(cudaSetDevice(w->device));
+  cudaStream_t st = (cudaStream_t)stream;
+  CgView V{w->cx, w->cy, w->cz, acx, acy, acz, x, w->r, w->pa, w->pb, w->s};
+  coop_launch(k_pcg, w->grid, st, V, b, tol, maxiter, w->partials, w->tz, w->iters, w->relres);
+  int it = 0;
+  double rr = 0;
+  HS_CUDA(cudaMemcpyAsync(&it, w->iters, sizeof(int), cudaMemcpyDeviceToHost, st));
+  HS_CUDA(cudaMemcpyAsync(&rr, w->relres, sizeof(double), cudaMemcpyDeviceToHost, st));
+  HS_CUDA(cudaStreamSynchronize(st));
+  if (iters) *iters = it;
+  if (relres) *relres = rr;
 }
 
 }  // namespace hs

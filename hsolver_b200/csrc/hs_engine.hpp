@@ -49,4 +49,11 @@ class Engine {
   std::unique_ptr<DeviceState> d_;
 };
 
+// Standalone pressure-correction CG with its own device workspace.
+struct PcgWork;
+PcgWork *pcg_create(int nx, int ny, int nz, int device);
+void pcg_destroy(PcgWork *w);
+void pcg_solve(PcgWork *w, const double *acx, const double *acy, const double *acz, const double *b, double *x,
+               double tol, int maxiter, void *stream, int *iters, double *relres);
+
 }  // namespace hs

@@ -160,6 +160,23 @@ int hs_case_interface(const hs_case *c, long long *out5, long long n);
 int hs_case_geometry(const hs_case *c, int axis, double *out, long long n);
 void hs_case_destroy(hs_case *c);
 
+/* Standalone pressure-correction solve, the counterpart of the reference's
+ * HYPRE IJ/ParCSR PCG call (fluid_solver.h:1758-1799 with the settings of
+ * fluid_solver.h:1871-1875): CG with the identity preconditioner, stopping
+ * when <r,r>/<b,b> < tol^2 or after maxiter iterations, zero initial guess.
+ * The system lives on a padded (nx+2)(ny+2)(nz+2) x-fastest grid; row P is
+ *   (2cx+2cy+2cz) x_P - cz x_B - cy x_S - cx x_W - cx x_E - cy x_N - cz x_F
+ * with cx, cy, cz = acx[P], acy[P], acz[P] (the coefficient construction of
+ * fluid_solver.h:1990-1996).  Coefficients and b must be zero at every
+ * padded index that is not an unknown; x is written everywhere (zero there).
+ * All arrays are device pointers.  hs_pcg_create allocates the workspace
+ * (four padded vectors and the reduction buffers). */
+typedef struct hs_pcg hs_pcg;
+int hs_pcg_create(int nx, int ny, int nz, int device, hs_pcg **out);
+int hs_pcg_solve(hs_pcg *h, const double *acx, const double *acy, const double *acz, const double *b, double *x,
+                 double tol, int maxiter, void *stream, int *iters, double *relres);
+void hs_pcg_destroy(hs_pcg *h);
+
 /* Release all device and host state. */
 void hs_destroy(hs_ctx *ctx);
 

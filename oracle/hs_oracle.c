@@ -1030,7 +1030,9 @@ int or_get_cell_types(const or_case *C, unsigned char *out, int *region, I64 n) 
 int or_get_grid(const or_case *C, int axis, double *out, I64 n) {
   const or_deck *d = &C->deck; const double *p = axis == 0 ? d->xs : axis == 1 ? d->ys : d->zs;
   I64 m = axis == 0 ? d->nx_pts : axis == 1 ? d->ny_pts : d->nz_pts;
-  if (n != m) return -1; memcpy(out, p, sizeof(double) * (size_t)n); return 0;
+  if (n != m) return -1;
+  memcpy(out, p, sizeof(double) * (size_t)n);
+  return 0;
 }
 I64 or_num_swap(const or_case *C) { return C->nswap; }
 int or_get_swap(const or_case *C, I64 *out5, I64 n) {
@@ -1057,4 +1059,45 @@ int or_set_field(or_case *C, int f, const double *in, I64 n) {
   I64 m; double *p = (double *)field_ptr(C, f, &m);
   if (!p || n != m) return -1;
   memcpy(p, in, sizeof(double) * (size_t)n); return 0;
+}
+
+/* Standalone form of the pressure-correction solve on caller arrays (padded
+ * (nx+2)(ny+2)(nz+2), zero coefficients and rhs off the unknowns): the same
+ * HYPRE PCG recurrences as pcg() above, used to check hs_pcg_solve. */
+int or_pcg_solve(I64 nx, I64 ny, I64 nz, const double *acx, const double *acy, const double *acz, const double *b,
+                 double *x, double tol, int maxiter, double *relres) {
+  I64 PX = nx + 2, PXY = (nx + 2) * (ny + 2), np = PXY * (nz + 2);
+  double *r = malloc(sizeof(double) * (size_t)np), *p = malloc(sizeof(double) * (size_t)np);
+  double *s = calloc((size_t)np, sizeof(double));
+  double bb = 0;
+  for (I64 q = 0; q < np; ++q) { x[q] = 0; r[q] = b[q]; p[q] = b[q]; bb += b[q] * b[q]; }
+  int i = 0;
+  double iprod = bb;
+  if (bb != 0.0) {
+    double gamma = 0;
+    for (I64 q = 0; q < np; ++q) gamma += r[q] * p[q];
+    double eps = tol * tol;
+    while (i + 1 <= maxiter) {
+      i++;
+      double sdotp = 0;
+      for (I64 k = 1; k <= nz; ++k) for (I64 j = 1; j <= ny; ++j) for (I64 ii = 1; ii <= nx; ++ii) {
+        I64 q = ii + j * PX + k * PXY;
+        double ax = acx[q], ay = acy[q], az = acz[q], d = ax + ax + ay + ay + az + az;
+        s[q] = d * p[q] - az * p[q - PXY] - ay * p[q - PX] - ax * p[q - 1] - ax * p[q + 1] - ay * p[q + PX] - az * p[q + PXY];
+      }
+      for (I64 q = 0; q < np; ++q) sdotp += s[q] * p[q];
+      if (sdotp == 0.0) break;
+      double alpha = gamma / sdotp, gamma_old = gamma;
+      for (I64 q = 0; q < np; ++q) { x[q] = x[q] + alpha * p[q]; r[q] = r[q] - alpha * s[q]; }
+      gamma = 0;
+      for (I64 q = 0; q < np; ++q) gamma += r[q] * r[q];
+      iprod = gamma;
+      if (iprod / bb < eps) break;
+      double beta = gamma / gamma_old;
+      for (I64 q = 0; q < np; ++q) p[q] = r[q] + beta * p[q];
+    }
+  }
+  if (relres) *relres = bb != 0.0 ? sqrt(iprod / bb) : 0.0;
+  free(r); free(p); free(s);
+  return i;
 }

@@ -192,3 +192,18 @@ def read_dump(path):
             k += 1
         out[key] = arr
     return out
+
+
+def pcg_solve(nx, ny, nz, acx, acy, acz, b, tol=1e-5, maxiter=1000):
+    """or_pcg_solve: the oracle's HYPRE-rule CG on padded arrays; returns
+    (x, iterations, final relative residual)."""
+    L = lib()
+    dp = ctypes.POINTER(ctypes.c_double)
+    L.or_pcg_solve.restype = ctypes.c_int
+    L.or_pcg_solve.argtypes = [ctypes.c_int64] * 3 + [dp] * 5 + [ctypes.c_double, ctypes.c_int, dp]
+    arrs = [np.ascontiguousarray(a, np.float64) for a in (acx, acy, acz, b)]
+    x = np.zeros_like(arrs[3])
+    rr = ctypes.c_double()
+    it = L.or_pcg_solve(nx, ny, nz, *[a.ctypes.data_as(dp) for a in arrs], x.ctypes.data_as(dp), tol, maxiter,
+                        ctypes.byref(rr))
+    return x, it, rr.value
