@@ -354,6 +354,16 @@ int hs_pcg_solve(hs_pcg *h, const double *acx, const double *acy, const double *
   }
 }
 
+int hs_pcg_solve_noalloc(int nx, int ny, int nz, const double *acx, const double *acy, const double *acz,
+                         const double *b, double *x, double tol, int maxiter, void *stream, int *iters, double *relres) {
+  try {
+    hs::pcg_solve_noalloc(nx, ny, nz, acx, acy, acz, b, x, tol, maxiter, stream, iters, relres);
+    return HS_OK;
+  } catch (const std::exception &e) {
+    return fail(nullptr, classify(e), e.what());
+  }
+}
+
 void hs_pcg_destroy(hs_pcg *h) {
   if (!h) return;
   hs::pcg_destroy(h->w);

@@ -28,7 +28,9 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <stdexcept>
+#include <string>
 
 #include "hs_engine.hpp"
 
@@ -1510,6 +1512,84 @@ void pcg_solve(PcgWork *w, const double *acx, const double *acy, const double *a
   double rr = 0;
   HS_CUDA(cudaMemcpyAsync(&it, w->iters, sizeof(int), cudaMemcpyDeviceToHost, st));
   HS_CUDA(cudaMemcpyAsync(&rr, w->relres, sizeof(double), cudaMemcpyDeviceToHost, st));
+  HS_CUDA(cudaStreamSynchronize(st));
+  if (iters) *iters = it;
+  if (relres) *relres = rr;
+}
+
+// ---------------------------------------------------------------- allocation-free CG
+// Some callers cannot allocate device memory while they run: hosts whose whole
+// GPU memory is owned by their own arena (a coupled multiphysics code that
+// reserves HBM at start-up and hands each component a fixed budget), and
+// loops that must not call cudaMalloc/cudaFree after set-up because those
+// calls may synchronise the device and stall work queued on other streams.
+// pcg_solve_noalloc serves them: the same CG kernel as pcg_solve, with its
+// scratch (four padded vectors, the reduction partials and the two result
+// words) in this file-scope array.  It is loaded with the library and held by
+// every GPU that loads it until the process exits (8.06 MiB per device).
+// Every call shares the array: calls that overlap on the GPU race, so a
+// caller issuing from several streams or threads must serialise them.
+constexpr long long kNoAllocMaxPad = 1LL << 18;  // padded cells (nx+2)(ny+2)(nz+2)
+constexpr int kNoAllocMaxBlocks = 4096;           // cooperative grid limit for the partials
+constexpr long long kNoAllocDoubles = 4 * kNoAllocMaxPad + 2 * kNoAllocMaxBlocks + 2;
+static __device__ __align__(256) double g_noalloc_scratch[kNoAllocDoubles];
+
+namespace {
+// Device address of g_noalloc_scratch and the cooperative grid, resolved once
+// per device with that device current (the host-side name of a __device__
+// array is not a device address).
+struct NoAllocSetup {
+  double *base = nullptr;
+  int grid = 0, nsm = 0;
+};
+std::mutex g_noalloc_mu;
+NoAllocSetup g_noalloc_dev[64];
+
+NoAllocSetup noalloc_setup(int device) {
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (device < 0 || device >= 64) throw std::invalid_argument("device ordinal out of range");
+  NoAllocSetup &S = g_noalloc_dev[device];
+  if (!S.base) {
+    void *ptr = nullptr;
+    HS_CUDA(cudaGetSymbolAddress(&ptr, g_noalloc_scratch));
+    HS_CUDA(cudaDeviceGetAttribute(&S.nsm, cudaDevAttrMultiProcessorCount, device));
+    S.grid = coop_blocks(k_pcg, S.nsm, kNoAllocMaxBlocks);
+    S.base = (double *)ptr;
+  }
+  return S;
+}
+}  // namespace
+
+long long noalloc_max_padded_cells() { return kNoAllocMaxPad; }
+
+void pcg_solve_noalloc(int nx, int ny, int nz, const double *acx, const double *acy, const double *acz, const double *b,
+                       double *x, double tol, int maxiter, void *stream, int *iters, double *relres) {
+  if (nx < 1 || ny < 1 || nz < 1) throw std::invalid_argument("grid dimensions must be positive");
+  const long long npad = (long long)(nx + 2) * (ny + 2) * (nz + 2);
+  if (npad > kNoAllocMaxPad)
+    throw std::invalid_argument("grid too large for the allocation-free solve: (nx+2)(ny+2)(nz+2) = " +
+                                std::to_string(npad) + " padded cells, the static scratch holds " +
+                                std::to_string(kNoAllocMaxPad));
+  if (!acx || !acy || !acz || !b || !x) throw std::invalid_argument("null device pointer");
+  if (maxiter < 0 || !(tol >= 0)) throw std::invalid_argument("invalid tolerance or iteration limit");
+  int device = 0;
+  HS_CUDA(cudaGetDevice(&device));
+  const NoAllocSetup S = noalloc_setup(device);
+  double *base = S.base;
+  double *r = base, *pa = base + kNoAllocMaxPad, *pb = base + 2 * kNoAllocMaxPad, *sv = base + 3 * kNoAllocMaxPad;
+  double *partials = base + 4 * kNoAllocMaxPad;
+  double *out_rel = partials + 2 * kNoAllocMaxBlocks;
+  int *out_it = reinterpret_cast<int *>(out_rel + 1);
+  cudaStream_t st = (cudaStream_t)stream;
+  CgView V{nx, ny, nz, acx, acy, acz, x, r, pa, pb, sv};
+  // k_pcg writes every scratch word it later reads (r, p, s over the padded
+  // grid, each partial before its reduction, both results), so the previous
+  // call's contents never leak into this one
+  coop_launch(k_pcg, S.grid, st, V, b, tol, maxiter, partials, choose_tz(nx, ny, nz, S.grid), out_it, out_rel);
+  int it = 0;
+  double rr = 0;
+  HS_CUDA(cudaMemcpyAsync(&it, out_it, sizeof(int), cudaMemcpyDeviceToHost, st));
+  HS_CUDA(cudaMemcpyAsync(&rr, out_rel, sizeof(double), cudaMemcpyDeviceToHost, st));
   HS_CUDA(cudaStreamSynchronize(st));
   if (iters) *iters = it;
   if (relres) *relres = rr;

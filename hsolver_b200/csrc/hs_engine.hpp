@@ -56,4 +56,9 @@ void pcg_destroy(PcgWork *w);
 void pcg_solve(PcgWork *w, const double *acx, const double *acy, const double *acz, const double *b, double *x,
                double tol, int maxiter, void *stream, int *iters, double *relres);
 
+// Same solve with no allocation: scratch in a static device array.
+long long noalloc_max_padded_cells();
+void pcg_solve_noalloc(int nx, int ny, int nz, const double *acx, const double *acy, const double *acz, const double *b,
+                       double *x, double tol, int maxiter, void *stream, int *iters, double *relres);
+
 }  // namespace hs

@@ -177,6 +177,21 @@ int hs_pcg_solve(hs_pcg *h, const double *acx, const double *acy, const double *
                  double tol, int maxiter, void *stream, int *iters, double *relres);
 void hs_pcg_destroy(hs_pcg *h);
 
+/* Allocation-free form of hs_pcg_solve; no counterpart in the reference.
+ * For callers that cannot allocate device memory while they run -- hosts
+ * whose GPU memory is all owned by their own arena, or loops that must not
+ * call cudaMalloc/cudaFree after set-up because those calls can synchronise
+ * the device -- it solves the same system with the same kernel on the
+ * calling thread's current device, keeping its scratch in a static device
+ * array of 8.06 MiB that every GPU loading the library holds until exit.
+ * Limit: (nx+2)(ny+2)(nz+2) <= 262144 padded cells; larger grids return
+ * HS_ERR_ARG.  The first call on a device looks up the array's device
+ * address; make that first call before any stream capture.  All calls share
+ * the array, so calls that overlap on the GPU race: serialise them.  It
+ * allocates nothing: no cudaMalloc, no cudaFree. */
+int hs_pcg_solve_noalloc(int nx, int ny, int nz, const double *acx, const double *acy, const double *acz,
+                         const double *b, double *x, double tol, int maxiter, void *stream, int *iters, double *relres);
+
 /* Release all device and host state. */
 void hs_destroy(hs_ctx *ctx);
 
