@@ -73,7 +73,8 @@ int hs_create(const char *deck, const hs_params *prm, int device, hs_ctx **out) 
   hs_params p;
   if (prm) p = *prm; else hs_params_default(&p);
   if (p.gs_max < 0 || p.pcg_maxiter < 0 || !(p.pcg_tol >= 0)) return fail(nullptr, HS_ERR_ARG, "invalid parameters");
-  if (p.pressure_solver != HS_PSOLVE_CG) return fail(nullptr, HS_ERR_UNSUPPORTED, "pressure solver not available in this build");
+  if (p.pressure_solver != HS_PSOLVE_CG && p.pressure_solver != HS_PSOLVE_MGCG)
+    return fail(nullptr, HS_ERR_ARG, "unknown pressure solver");
   std::string err;
   hs::Deck d;
   if (!hs::parse_deck(deck, d, err)) return fail(nullptr, HS_ERR_DECK, err);

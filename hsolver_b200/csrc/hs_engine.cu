@@ -884,6 +884,292 @@ __global__ void __launch_bounds__(kBlock) k_pcg(CgView V, const double *b, doubl
   cg_core(V, bb, tol, maxiter, partials, buf, sh, grid, TZ, out_iters, out_relres);
 }
 
+// ---------------------------------------------------------------- multigrid-preconditioned CG
+// HS_PSOLVE_MGCG: the same pressure-correction system, solved by CG with a
+// geometric multigrid V-cycle as preconditioner.  The V-cycle runs in FP32
+// (fields, coefficients, smoother, transfers); the CG recurrences, residual,
+// dot products and the coarsest-grid direct solve are FP64.
+//   coarsening   2x per axis (ceil), masked: a coarse cell is an unknown when
+//                any child is; per-cell coefficients c_C = (sum of children)/4
+//                (a 2x2 face patch summed, halved for the doubled spacing)
+//   smoother     red-black Gauss-Seidel, one pre (red, black) and one post
+//                (black, red) sweep, x = 0 start
+//   transfers    sum restriction of the residual, constant prolongation
+//   coarsest     <= 64 cells, LU with partial pivoting factored on the host
+constexpr int kMaxLevels = 14;
+constexpr int kMaxCoarse = 64;
+
+struct MgLevel {
+  int nx, ny, nz;
+  float *x, *rhs, *ax, *ay, *az;
+  uint8_t *m;  // 1 = unknown
+};
+struct MgView {
+  int L;
+  MgLevel lv[kMaxLevels];
+  int nc;             // unknowns of the coarsest level (all its padded-interior cells)
+  const double *lu;   // nc x nc, row-major, L (unit) and U packed
+  const int *piv;
+  double *yc;         // nc scratch
+};
+
+__device__ __forceinline__ int mgidx(const MgLevel &L, int i, int j, int k) { return i + (L.nx + 2) * (j + (L.ny + 2) * k); }
+
+// level 0 coefficients and mask from the FP64 frozen coefficients
+__global__ void k_mg_fine(FluidDev F, MgLevel L0) {
+  const int cx = F.cx, cy = F.cy, n = cx * cy * F.cz;
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
+    const int i = c % cx, j = (c / cx) % cy, k = c / (cx * cy);
+    const int q = (i + 1) + (cx + 2) * ((j + 1) + (cy + 2) * (k + 1));
+    const bool u = !F.empty[c];
+    L0.m[q] = u;
+    L0.ax[q] = u ? (float)F.acx[q] : 0.f;
+    L0.ay[q] = u ? (float)F.acy[q] : 0.f;
+    L0.az[q] = u ? (float)F.acz[q] : 0.f;
+  }
+}
+
+__global__ void k_mg_coarsen(MgLevel Fl, MgLevel C) {
+  const int n = C.nx * C.ny * C.nz;
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
+    const int I = c % C.nx, J = (c / C.nx) % C.ny, K = c / (C.nx * C.ny);
+    float sx = 0.f, sy = 0.f, sz = 0.f;
+    int any = 0;
+    for (int dk = 0; dk < 2; ++dk)
+      for (int dj = 0; dj < 2; ++dj)
+        for (int di = 0; di < 2; ++di) {
+          const int i = 2 * I + di, j = 2 * J + dj, k = 2 * K + dk;
+          if (i >= Fl.nx || j >= Fl.ny || k >= Fl.nz) continue;
+          const int q = mgidx(Fl, i + 1, j + 1, k + 1);
+          if (!Fl.m[q]) continue;
+          any = 1;
+          sx += Fl.ax[q]; sy += Fl.ay[q]; sz += Fl.az[q];
+        }
+    const int qc = mgidx(C, I + 1, J + 1, K + 1);
+    C.m[qc] = any;
+    C.ax[qc] = 0.25f * sx; C.ay[qc] = 0.25f * sy; C.az[qc] = 0.25f * sz;
+  }
+}
+
+// one red-black half sweep on level L; zero_nb: neighbours read as zero (first pass of a cycle)
+__device__ void mg_smooth(const MgLevel &L, int color, bool zero_nb, int tid, int T) {
+  const int n = L.nx * L.ny * L.nz, PX = L.nx + 2, PXY = (L.nx + 2) * (L.ny + 2);
+  for (int c = tid; c < n; c += T) {
+    const int i = c % L.nx, j = (c / L.nx) % L.ny, k = c / (L.nx * L.ny);
+    if (((i + j + k) & 1) != color) continue;
+    const int q = (i + 1) + PX * (j + 1) + PXY * (k + 1);
+    if (!L.m[q]) continue;
+    const float ax = L.ax[q], ay = L.ay[q], az = L.az[q];
+    const float d = 2.f * (ax + ay + az);
+    float sum = L.rhs[q];
+    if (!zero_nb) {
+      const float *x = L.x;
+      sum += ax * (__ldcg(x + q - 1) + __ldcg(x + q + 1)) + ay * (__ldcg(x + q - PX) + __ldcg(x + q + PX)) +
+             az * (__ldcg(x + q - PXY) + __ldcg(x + q + PXY));
+    }
+    L.x[q] = sum / d;
+  }
+}
+
+// coarse rhs = sum over the children of (rhs - A x)
+__device__ void mg_restrict(const MgLevel &Fl, const MgLevel &C, int tid, int T) {
+  const int n = C.nx * C.ny * C.nz, PX = Fl.nx + 2, PXY = (Fl.nx + 2) * (Fl.ny + 2);
+  for (int c = tid; c < n; c += T) {
+    const int I = c % C.nx, J = (c / C.nx) % C.ny, K = c / (C.nx * C.ny);
+    float acc = 0.f;
+    for (int dk = 0; dk < 2; ++dk)
+      for (int dj = 0; dj < 2; ++dj)
+        for (int di = 0; di < 2; ++di) {
+          const int i = 2 * I + di, j = 2 * J + dj, k = 2 * K + dk;
+          if (i >= Fl.nx || j >= Fl.ny || k >= Fl.nz) continue;
+          const int q = (i + 1) + PX * (j + 1) + PXY * (k + 1);
+          if (!Fl.m[q]) continue;
+          const float *x = Fl.x;
+          const float ax = Fl.ax[q], ay = Fl.ay[q], az = Fl.az[q];
+          const float r = Fl.rhs[q] - (2.f * (ax + ay + az) * __ldcg(x + q) -
+                                       ax * (__ldcg(x + q - 1) + __ldcg(x + q + 1)) -
+                                       ay * (__ldcg(x + q - PX) + __ldcg(x + q + PX)) -
+                                       az * (__ldcg(x + q - PXY) + __ldcg(x + q + PXY)));
+          acc += r;
+        }
+    const int qc = mgidx(C, I + 1, J + 1, K + 1);
+    C.rhs[qc] = C.m[qc] ? acc : 0.f;
+  }
+}
+
+__device__ void mg_prolong(const MgLevel &Fl, const MgLevel &C, int tid, int T) {
+  const int n = Fl.nx * Fl.ny * Fl.nz;
+  for (int c = tid; c < n; c += T) {
+    const int i = c % Fl.nx, j = (c / Fl.nx) % Fl.ny, k = c / (Fl.nx * Fl.ny);
+    const int q = mgidx(Fl, i + 1, j + 1, k + 1);
+    if (!Fl.m[q]) continue;
+    Fl.x[q] = __ldcg(Fl.x + q) + __ldcg(C.x + mgidx(C, i / 2 + 1, j / 2 + 1, k / 2 + 1));
+  }
+}
+
+// z = V-cycle(rhs of level 0), result in lv[0].x
+__device__ void mg_vcycle(const MgView &M, cg::grid_group &grid, int tid, int T) {
+  for (int l = 0; l < M.L - 1; ++l) {
+    mg_smooth(M.lv[l], 0, true, tid, T);
+    grid.sync();
+    mg_smooth(M.lv[l], 1, false, tid, T);
+    grid.sync();
+    mg_restrict(M.lv[l], M.lv[l + 1], tid, T);
+    grid.sync();
+  }
+  {
+    // coarsest: FP64 LU solve by one warp of block 0
+    const MgLevel &C = M.lv[M.L - 1];
+    if (blockIdx.x == 0 && threadIdx.x < 32) {
+      const int nc = M.nc, lane = threadIdx.x;
+      double *y = M.yc;
+      // permuted rhs
+      if (lane == 0)
+        for (int r = 0; r < nc; ++r) {
+          const int s = M.piv[r];
+          y[r] = (double)C.rhs[mgidx(C, s % C.nx + 1, (s / C.nx) % C.ny + 1, s / (C.nx * C.ny) + 1)];
+        }
+      __syncwarp();
+      for (int r = 0; r < nc; ++r) {  // forward (unit lower)
+        double a = 0.0;
+        for (int c2 = lane; c2 < r; c2 += 32) a += M.lu[r * nc + c2] * y[c2];
+        for (int o = 16; o; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+        if (lane == 0) y[r] -= a;
+        __syncwarp();
+      }
+      for (int r = nc - 1; r >= 0; --r) {  // backward
+        double a = 0.0;
+        for (int c2 = r + 1 + lane; c2 < nc; c2 += 32) a += M.lu[r * nc + c2] * y[c2];
+        for (int o = 16; o; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+        if (lane == 0) y[r] = (y[r] - a) / M.lu[r * nc + r];
+        __syncwarp();
+      }
+      for (int r = lane; r < nc; r += 32) {
+        const int q = mgidx(C, r % C.nx + 1, (r / C.nx) % C.ny + 1, r / (C.nx * C.ny) + 1);
+        C.x[q] = C.m[q] ? (float)y[r] : 0.f;
+      }
+    }
+    grid.sync();
+  }
+  for (int l = M.L - 2; l >= 0; --l) {
+    mg_prolong(M.lv[l], M.lv[l + 1], tid, T);
+    grid.sync();
+    mg_smooth(M.lv[l], 1, false, tid, T);
+    grid.sync();
+    mg_smooth(M.lv[l], 0, false, tid, T);
+    grid.sync();
+  }
+}
+
+// Pressure correction by MG-preconditioned CG (HYPRE PCG with a
+// preconditioner: r = b, z = M r, p = z, gamma = <r,z>; s = A p,
+// alpha = gamma/<s,p>, x += alpha p, r -= alpha s, z = M r, gamma' = <r,z>,
+// stop on <r,r>/<b,b> < tol^2, p = z + beta p).  Assembly (coefficients, b)
+// has been done by k_pcorr_setup.
+__global__ void __launch_bounds__(kBlock) k_mgcg(FluidDev F, Prm P, MgView M, double *partials, DevStats *st) {
+  cg::grid_group grid = cg::this_grid();
+  __shared__ double sh[33];
+  const int cx = F.cx, cy = F.cy, n = cx * cy * F.cz;
+  const int PX = cx + 2, PXY = (cx + 2) * (cy + 2);
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x, T = gridDim.x * blockDim.x;
+  int buf = 0;
+  const MgLevel &L0 = M.lv[0];
+  // r = b is in F.r, x = 0; bb
+  double acc = 0.0;
+  for (int c = tid; c < n; c += T) {
+    if (F.empty[c]) continue;
+    const int q = (c % cx + 1) + PX * ((c / cx) % cy + 1) + PXY * (c / (cx * cy) + 1);
+    const double rv = F.r[q];
+    acc += rv * rv;
+    L0.rhs[q] = (float)rv;
+  }
+  const double bb = grid_sum(acc, partials, buf, sh, grid);
+  if (bb == 0.0) {
+    if (tid == 0) { st->pcg_iters = 0; st->pcg_relres = 0.0; st->cum_pcg_solves += 1; }
+    return;
+  }
+  const double eps = P.pcg_tol * P.pcg_tol;
+  mg_vcycle(M, grid, tid, T);
+  acc = 0.0;
+  for (int c = tid; c < n; c += T) {
+    if (F.empty[c]) continue;
+    const int q = (c % cx + 1) + PX * ((c / cx) % cy + 1) + PXY * (c / (cx * cy) + 1);
+    const double z = (double)__ldcg(L0.x + q);
+    F.pa[q] = z;
+    acc += F.r[q] * z;
+  }
+  double gamma = grid_sum(acc, partials, buf, sh, grid), iprod = bb;
+  int it = 0;
+  while (it + 1 <= P.pcg_maxiter) {
+    it++;
+    acc = 0.0;
+    for (int c = tid; c < n; c += T) {
+      if (F.empty[c]) continue;
+      const int q = (c % cx + 1) + PX * ((c / cx) % cy + 1) + PXY * (c / (cx * cy) + 1);
+      const double *p = F.pa;
+      const double ax = F.acx[q], ay = F.acy[q], az = F.acz[q], d = ax + ax + ay + ay + az + az;
+      const double sv = d * ld(p + q) - az * ld(p + q - PXY) - ay * ld(p + q - PX) - ax * ld(p + q - 1) -
+                        ax * ld(p + q + 1) - ay * ld(p + q + PX) - az * ld(p + q + PXY);
+      F.s[q] = sv;
+      acc += sv * ld(p + q);
+    }
+    const double sdotp = grid_sum(acc, partials, buf, sh, grid);
+    if (sdotp == 0.0) break;
+    const double alpha = gamma / sdotp, gamma_old = gamma;
+    acc = 0.0;
+    for (int c = tid; c < n; c += T) {
+      if (F.empty[c]) continue;
+      const int q = (c % cx + 1) + PX * ((c / cx) % cy + 1) + PXY * (c / (cx * cy) + 1);
+      F.x[q] = F.x[q] + alpha * F.pa[q];
+      const double rv = F.r[q] - alpha * F.s[q];
+      F.r[q] = rv;
+      acc += rv * rv;
+      L0.rhs[q] = (float)rv;
+    }
+    iprod = grid_sum(acc, partials, buf, sh, grid);
+    if (iprod / bb < eps) break;
+    mg_vcycle(M, grid, tid, T);
+    acc = 0.0;
+    for (int c = tid; c < n; c += T) {
+      if (F.empty[c]) continue;
+      const int q = (c % cx + 1) + PX * ((c / cx) % cy + 1) + PXY * (c / (cx * cy) + 1);
+      acc += F.r[q] * (double)__ldcg(L0.x + q);
+    }
+    gamma = grid_sum(acc, partials, buf, sh, grid);
+    const double beta = gamma / gamma_old;
+    for (int c = tid; c < n; c += T) {
+      if (F.empty[c]) continue;
+      const int q = (c % cx + 1) + PX * ((c / cx) % cy + 1) + PXY * (c / (cx * cy) + 1);
+      F.pa[q] = (double)__ldcg(L0.x + q) + beta * F.pa[q];
+    }
+    grid.sync();
+  }
+  if (tid == 0) { st->pcg_iters = it; st->pcg_relres = sqrt(iprod / bb); st->cum_pcg_iters += it; st->cum_pcg_solves += 1; }
+}
+
+// Assembly of the pressure-correction system for the MG path: coefficients
+// (when `assemble`), r = b, x = 0 (fluid_solver.h:1969-2002 / 2123-2162).
+__global__ void k_pcorr_setup(FluidDev F, int assemble) {
+  const int cx = F.cx, cy = F.cy, n = cx * cy * F.cz;
+  const int PX = cx + 2, PXY = (cx + 2) * (cy + 2);
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
+    if (F.empty[c]) continue;
+    const int i = c % cx, j = (c / cx) % cy, k = c / (cx * cy);
+    const int q = (i + 1) + PX * (j + 1) + PXY * (k + 1);
+    if (assemble) {
+      double xp = F.xp[i + 1], yp = F.yp[j + 1], zp = F.zp[k + 1];
+      double facexy = xp * yp, facexz = xp * zp, faceyz = yp * zp;
+      F.acx[q] = faceyz / F.up[IU(F, i + 1, j + 1, k + 1)];
+      F.acy[q] = facexz / F.vp[IV(F, i + 1, j + 1, k + 1)];
+      F.acz[q] = facexy / F.wp[IW(F, i + 1, j + 1, k + 1)];
+    }
+    F.r[q] = -(F.u[IU(F, i + 2, j + 1, k + 1)] - F.u[IU(F, i + 1, j + 1, k + 1)]) -
+             (F.v[IV(F, i + 1, j + 2, k + 1)] - F.v[IV(F, i + 1, j + 1, k + 1)]) -
+             (F.w[IW(F, i + 1, j + 1, k + 2)] - F.w[IW(F, i + 1, j + 1, k + 1)]);
+    F.x[q] = 0.0;
+  }
+}
+
 // Velocity correction, pressure update and p_temp refresh
 // (fluid_solver.h:1460-1597); p' is the CG solution x.
 __global__ void k_correct(FluidDev F, Prm P) {
@@ -1044,6 +1330,10 @@ struct DeviceState {
   double *snap = nullptr, *ssnap = nullptr;
   int *spred = nullptr;
   bool have_matrix = false;
+  // multigrid hierarchy (HS_PSOLVE_MGCG)
+  MgView mg{};
+  int g_mgcg = 0;
+  bool mg_ready = false;
 
   template <class T>
   T *alloc(size_t n) {
@@ -1248,6 +1538,31 @@ Engine::Engine(const Case &c, const hs_params &p, int device) : case_(c), prm_(p
   D.ssnap = D.alloc<double>(std::max<long long>(D.ntt, 1));
   D.spred = D.alloc<int>(std::max(D.nreg, 1));
   int gmax = std::max({D.g_gs[0], D.g_gs[1], D.g_gs[2], D.g_gs[3], D.g_pcorr, D.solid_blocks, 1});
+  if (p.pressure_solver == HS_PSOLVE_MGCG) {
+    MgView &G = D.mg;
+    int nx = (int)M.cx, ny = (int)M.cy, nz = (int)M.cz;
+    int L = 0;
+    for (;;) {
+      MgLevel &lv = G.lv[L];
+      lv.nx = nx; lv.ny = ny; lv.nz = nz;
+      size_t np = (size_t)(nx + 2) * (ny + 2) * (nz + 2);
+      lv.x = D.alloc<float>(np); lv.rhs = D.alloc<float>(np);
+      lv.ax = D.alloc<float>(np); lv.ay = D.alloc<float>(np); lv.az = D.alloc<float>(np);
+      lv.m = D.alloc<uint8_t>(np);
+      ++L;
+      if ((long)nx * ny * nz <= kMaxCoarse || L == kMaxLevels) break;
+      nx = (nx + 1) / 2; ny = (ny + 1) / 2; nz = (nz + 1) / 2;
+    }
+    if ((long)G.lv[L - 1].nx * G.lv[L - 1].ny * G.lv[L - 1].nz > kMaxCoarse)
+      throw std::runtime_error("multigrid hierarchy too deep for this grid");
+    G.L = L;
+    G.nc = G.lv[L - 1].nx * G.lv[L - 1].ny * G.lv[L - 1].nz;
+    G.lu = D.alloc<double>((size_t)G.nc * G.nc);
+    G.piv = D.alloc<int>(G.nc);
+    G.yc = D.alloc<double>(G.nc);
+    D.g_mgcg = coop_blocks(k_mgcg, D.nsm, 1 << 30);
+    gmax = std::max(gmax, D.g_mgcg);
+  }
   D.partials = D.alloc<double>(2 * (size_t)gmax * kBlock);
   D.stats = D.alloc<DevStats>(1);
   HS_CUDA(cudaMallocHost(&D.stats_host, sizeof(DevStats)));
@@ -1312,7 +1627,15 @@ void Engine::step(int nsteps) {
     { Mark m(D, 1); coop_launch(k_gs<1>, D.g_gs[1], s, D.F, D.P, D.partials, D.stats, D.snap); }
     { Mark m(D, 2); coop_launch(k_gs<2>, D.g_gs[2], s, D.F, D.P, D.partials, D.stats, D.snap); }
     int assemble = (!D.have_matrix || !prm_.frozen_matrix) ? 1 : 0;
-    { Mark m(D, 3); coop_launch(k_pcorr, D.g_pcorr, s, D.F, D.P, D.partials, D.stats, assemble, D.tz); }
+    if (prm_.pressure_solver == HS_PSOLVE_MGCG) {
+      Mark m(D, 3);
+      k_pcorr_setup<<<grid_for(n), kBlock, 0, s>>>(D.F, assemble);
+      if (assemble) build_multigrid();
+      coop_launch(k_mgcg, D.g_mgcg, s, D.F, D.P, D.mg, D.partials, D.stats);
+    } else {
+      Mark m(D, 3);
+      coop_launch(k_pcorr, D.g_pcorr, s, D.F, D.P, D.partials, D.stats, assemble, D.tz);
+    }
     D.have_matrix = true;
     {
       Mark m(D, 4);
@@ -1378,6 +1701,67 @@ void Engine::counters(long long *out8) {
 }
 
 void *Engine::stream_handle() { return (void *)d_->stream; }
+
+// Coefficients of every level from the frozen FP64 matrix, then the dense
+// FP64 LU (partial pivoting) of the coarsest level on the host.
+void Engine::build_multigrid() {
+  DeviceState &D = *d_;
+  MgView &G = D.mg;
+  cudaStream_t s = D.stream;
+  const long n = (long)D.F.cx * D.F.cy * D.F.cz;
+  k_mg_fine<<<grid_for(n), kBlock, 0, s>>>(D.F, G.lv[0]);
+  for (int l = 0; l + 1 < G.L; ++l) {
+    long nc = (long)G.lv[l + 1].nx * G.lv[l + 1].ny * G.lv[l + 1].nz;
+    k_mg_coarsen<<<grid_for(nc), kBlock, 0, s>>>(G.lv[l], G.lv[l + 1]);
+  }
+  const MgLevel &C = G.lv[G.L - 1];
+  const size_t np = (size_t)(C.nx + 2) * (C.ny + 2) * (C.nz + 2);
+  std::vector<float> ax(np), ay(np), az(np);
+  std::vector<uint8_t> m(np);
+  HS_CUDA(cudaMemcpyAsync(ax.data(), C.ax, np * 4, cudaMemcpyDeviceToHost, s));
+  HS_CUDA(cudaMemcpyAsync(ay.data(), C.ay, np * 4, cudaMemcpyDeviceToHost, s));
+  HS_CUDA(cudaMemcpyAsync(az.data(), C.az, np * 4, cudaMemcpyDeviceToHost, s));
+  HS_CUDA(cudaMemcpyAsync(m.data(), C.m, np, cudaMemcpyDeviceToHost, s));
+  HS_CUDA(cudaStreamSynchronize(s));
+  const int nc = G.nc;
+  std::vector<double> A((size_t)nc * nc, 0.0);
+  auto pid = [&](int i, int j, int k) { return (size_t)(i + 1) + (C.nx + 2) * ((j + 1) + (size_t)(C.ny + 2) * (k + 1)); };
+  for (int r = 0; r < nc; ++r) {
+    const int i = r % C.nx, j = (r / C.nx) % C.ny, k = r / (C.nx * C.ny);
+    const size_t q = pid(i, j, k);
+    if (!m[q]) { A[(size_t)r * nc + r] = 1.0; continue; }
+    const double cxv = ax[q], cyv = ay[q], czv = az[q];
+    A[(size_t)r * nc + r] = 2.0 * (cxv + cyv + czv);
+    auto nb = [&](int ii, int jj, int kk, double cval) {
+      if (ii < 0 || jj < 0 || kk < 0 || ii >= C.nx || jj >= C.ny || kk >= C.nz) return;
+      if (!m[pid(ii, jj, kk)]) return;
+      A[(size_t)r * nc + (ii + C.nx * (jj + C.ny * kk))] -= cval;
+    };
+    nb(i - 1, j, k, cxv); nb(i + 1, j, k, cxv); nb(i, j - 1, k, cyv); nb(i, j + 1, k, cyv);
+    nb(i, j, k - 1, czv); nb(i, j, k + 1, czv);
+  }
+  std::vector<int> piv(nc);
+  for (int r = 0; r < nc; ++r) piv[r] = r;
+  for (int c = 0; c < nc; ++c) {  // Doolittle LU with row pivoting; piv maps row -> original row
+    int best = c;
+    for (int r = c + 1; r < nc; ++r)
+      if (std::fabs(A[(size_t)r * nc + c]) > std::fabs(A[(size_t)best * nc + c])) best = r;
+    if (A[(size_t)best * nc + c] == 0.0) throw std::runtime_error("singular coarsest multigrid matrix");
+    if (best != c) {
+      for (int k2 = 0; k2 < nc; ++k2) std::swap(A[(size_t)c * nc + k2], A[(size_t)best * nc + k2]);
+      std::swap(piv[c], piv[best]);
+    }
+    for (int r = c + 1; r < nc; ++r) {
+      const double f = A[(size_t)r * nc + c] / A[(size_t)c * nc + c];
+      A[(size_t)r * nc + c] = f;
+      for (int k2 = c + 1; k2 < nc; ++k2) A[(size_t)r * nc + k2] -= f * A[(size_t)c * nc + k2];
+    }
+  }
+  HS_CUDA(cudaMemcpyAsync((void *)G.lu, A.data(), A.size() * 8, cudaMemcpyHostToDevice, s));
+  HS_CUDA(cudaMemcpyAsync((void *)G.piv, piv.data(), piv.size() * 4, cudaMemcpyHostToDevice, s));
+  HS_CUDA(cudaStreamSynchronize(s));
+  D.mg_ready = true;
+}
 
 void Engine::sync() {
   HS_CUDA(cudaSetDevice(device_));

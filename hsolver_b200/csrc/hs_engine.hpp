@@ -41,6 +41,7 @@ class Engine {
   bool inited() const { return inited_; }
 
  private:
+  void build_multigrid();
   Case case_;
   hs_params prm_;
   int device_;
