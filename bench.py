@@ -151,29 +151,33 @@ def run_gpu(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
 
-    # end to end through the C ABI with pinned host buffers: every step uploads
-    # the solver state, runs one outer step and reads the state back
+    # end to end through the C ABI with pinned host buffers: a fresh solver
+    # replays the same outer steps; every step uploads the solver state from
+    # pinned memory, runs one outer step and reads the state back
     state = ["u_star", "v_star", "w_star", "p_temp", "t_temp", "p"]
-    host = {f: torch.empty(g.field_size(f), dtype=torch.float64, pin_memory=True) for f in state}
+    ge = hsolver_b200.Solver(deck, device=local)
+    ge.init()
+    for _ in range(args.warmup):
+        ge.step(1)
+    host = {f: torch.empty(ge.field_size(f), dtype=torch.float64, pin_memory=True) for f in state}
     for f in state:
-        g.field(f, out=host[f].numpy())
+        ge.field(f, out=host[f].numpy())
     L = hsolver_b200.load()
     ids = hsolver_b200.FIELDS
     h2d = sum(host[f].numel() * 8 for f in state)
-    e2e_steps = max(1, min(args.steps, 5))
+    e2e_steps = args.steps
 
     def e2e_step():
         for f in state:
             p = ctypes.cast(host[f].data_ptr(), ctypes.POINTER(ctypes.c_double))
-            if L.hs_set_field(g.h, ids[f], p, host[f].numel()) != 0:
-                raise RuntimeError(L.hs_last_error(g.h).decode())
-        g.step(1)
+            if L.hs_set_field(ge.h, ids[f], p, host[f].numel()) != 0:
+                raise RuntimeError(L.hs_last_error(ge.h).decode())
+        ge.step(1)
         for f in state:
             p = ctypes.cast(host[f].data_ptr(), ctypes.POINTER(ctypes.c_double))
-            if L.hs_get_field(g.h, ids[f], p, host[f].numel()) != 0:
-                raise RuntimeError(L.hs_last_error(g.h).decode())
+            if L.hs_get_field(ge.h, ids[f], p, host[f].numel()) != 0:
+                raise RuntimeError(L.hs_last_error(ge.h).decode())
 
-    e2e_step()
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
@@ -182,10 +186,44 @@ def run_gpu(args):
         e2e_step()
     torch.cuda.synchronize()
     e2e_s = time.perf_counter() - t0
+    ge.close()
     if dist:
         t = torch.tensor([e2e_s], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_s = float(t.item())
+
+    # the mixed-precision pressure solve (FP32 multigrid V-cycle inside FP64
+    # CG) on the same case and steps, device-timed the same way
+    mixed = None
+    if not args.no_variants:
+        gm = hsolver_b200.Solver(deck, hsolver_b200.default_params(pressure_solver=hsolver_b200.PSOLVE_MGCG),
+                                 device=local)
+        gm.init()
+        for _ in range(args.warmup):
+            gm.step(1)
+        gm.sync()
+        sm = torch.cuda.ExternalStream(gm.stream(), device=local)
+        gm.profile(True)
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        m0 = torch.cuda.Event(enable_timing=True)
+        m1 = torch.cuda.Event(enable_timing=True)
+        m0.record(sm)
+        gm.step(args.steps)
+        m1.record(sm)
+        m1.synchronize()
+        mms = m0.elapsed_time(m1)
+        mph, mn = gm.profile_read()
+        mst = gm.step(0, stats=True)
+        if dist:
+            t = torch.tensor([mms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            mms = float(t.item())
+        mixed = {"pressure_solver": "CG + FP32 multigrid V-cycle, FP64 recurrences", "value": world * args.steps / (mms * 1e-3),
+                 "unit": UNIT, "ms_per_step": mms / args.steps,
+                 "phase_ms_per_step": {k: v / max(1, mn) for k, v in mph.items()}, "pcg_iters_last": mst["pcg_iters"]}
+        gm.close()
 
     if rank == 0:
         peak, peak_kind = hbm_peak()
@@ -209,6 +247,7 @@ def run_gpu(args):
             "sweeps_per_step": {k: (c1[k] - c0[k]) / max(1, args.steps) for k in ["sweeps_u", "sweeps_v", "sweeps_w", "sweeps_t"]},
             "last_step": {k: st[k] for k in ["pcg_iters", "pcg_relres", "sweeps_t", "sweeps_solid_max"]},
             "gpu_launches": 17 * args.steps,
+            "variants": {"mixed_mgcg": mixed},
             "clocks": clk,
         }
         if not args.no_cpu_baseline:
@@ -268,6 +307,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="native", choices=["native", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-variants", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

@@ -371,6 +371,14 @@ void hs_pcg_destroy(hs_pcg *h) {
   delete h;
 }
 
+long long hs_check_division(const double *a, const double *b, long long n) {
+  try {
+    return hs::div_check(a, b, n);
+  } catch (const std::exception &e) {
+    return fail(nullptr, classify(e), e.what());
+  }
+}
+
 void hs_destroy(hs_ctx *ctx) {
   if (!ctx) return;
   delete ctx->engine;

@@ -63,6 +63,17 @@ struct FluidDev {
   // 1/s/s per axis index with s = (p + m)/2 (fluid_solver.h:831-842), so the
   // energy denominator 2*alpha*(1/sx/sx + 1/sy/sy + 1/sz/sz) costs no division
   const double *ix2, *iy2, *iz2;
+  // RN(1/s) of the energy spacings s = (p + m)/2 per axis index
+  const double *rsx, *rsy, *rsz;
+  // RN(1/(p+m)) and RN(1/(p+q)) of the momentum diffusion distances per axis
+  // index: xp+xw, xp+xe | ys+yp, yn+yp | zb+zp, zf+zp (fluid_solver.h:1266-1268)
+  const double *rxw, *rxe, *rys, *ryn, *rzb, *rzf;
+  // parity-split copies used inside the energy solve: cell (i,j,k) of the
+  // padded grid at (i&1)*hs + (i>>1) + hx*(j + (cy+2)*k), so the cells of one
+  // parity that a time step updates are contiguous
+  double *ts, *us, *vs, *ws;
+  int hx;
+  long long hs;
   double *acx, *acy, *acz;                     // padded, frozen pressure-correction coefficients
   double *x, *r, *pa, *pb, *s;                 // padded CG vectors; x is p'
   double *pscr;                                // cx*cy*cz scratch for the cell BC
@@ -97,6 +108,17 @@ __device__ __forceinline__ int GY(const FluidDev &F, int i, int j, int k) { retu
 __device__ __forceinline__ int GZ(const FluidDev &F, int i, int j, int k) { return i + F.cx * (j + F.cy * k); }
 
 __device__ __forceinline__ double dmax0(double a) { return a < 0.0 ? 0.0 : a; }  // std::max(a, 0.0)
+
+// a / b for a divisor known ahead of time, from its correctly rounded
+// reciprocal y = RN(1/b) (Markstein, IBM J. Res. Dev. 34(1), 1990): q = RN(a*y)
+// is within one ulp of a/b, the remainder a - q*b is exact in one FMA, and
+// RN(q + r*y) is the correctly rounded quotient RN(a/b) -- the same value the
+// IEEE division gives, for finite, normal operands and a nonzero a.
+__device__ __forceinline__ double div_pre(double a, double b, double y) {
+  const double q = a * y;
+  const double r = __fma_rn(-q, b, a);
+  return __fma_rn(r, y, q);
+}
 __device__ __forceinline__ double ld(const double *p) { return __ldcg(p); }   // L2-coherent load
 
 // ---------------------------------------------------------------- reductions
@@ -212,9 +234,9 @@ __device__ __forceinline__ double upd_u(const FluidDev &F, const Prm &P, int i, 
   double xp = F.xp[i], xw = F.xw[i], xe = F.xe[i], yp = F.yp[j], ys = F.ys[j], yn = F.yn[j];
   double zp = F.zp[k], zf = F.zf[k], zb = F.zb[k];
   double facexy = xp * yp, facexz = xp * zp, faceyz = yp * zp;
-  double Dw = 2 * P.nu * faceyz / (xp + xw), De = 2 * P.nu * faceyz / (xp + xe);
-  double Ds = 2 * P.nu * facexz / (ys + yp), Dn = 2 * P.nu * facexz / (yn + yp);
-  double Db = 2 * P.nu * facexy / (zb + zp), Df = 2 * P.nu * facexy / (zf + zp);
+  double Dw = div_pre(2 * P.nu * faceyz, xp + xw, F.rxw[i]), De = div_pre(2 * P.nu * faceyz, xp + xe, F.rxe[i]);
+  double Ds = div_pre(2 * P.nu * facexz, ys + yp, F.rys[j]), Dn = div_pre(2 * P.nu * facexz, yn + yp, F.ryn[j]);
+  double Db = div_pre(2 * P.nu * facexy, zb + zp, F.rzb[k]), Df = div_pre(2 * P.nu * facexy, zf + zp, F.rzf[k]);
   double uc = ld(u + IU(F, i, j, k));
   double fw = 0.5 * P.rho * faceyz * (uc + ld(u + IU(F, i - 1, j, k)));
   double fe = 0.5 * P.rho * faceyz * (uc + ld(u + IU(F, i + 1, j, k)));
@@ -238,9 +260,9 @@ __device__ __forceinline__ double upd_v(const FluidDev &F, const Prm &P, int i, 
   double xp = F.xp[i], xw = F.xw[i], xe = F.xe[i], yp = F.yp[j], ys = F.ys[j], yn = F.yn[j];
   double zp = F.zp[k], zf = F.zf[k], zb = F.zb[k];
   double facexy = xp * yp, facexz = xp * zp, faceyz = yp * zp;
-  double Dw = 2 * P.nu * faceyz / (xp + xw), De = 2 * P.nu * faceyz / (xp + xe);
-  double Ds = 2 * P.nu * facexz / (ys + yp), Dn = 2 * P.nu * facexz / (yn + yp);
-  double Db = 2 * P.nu * facexy / (zb + zp), Df = 2 * P.nu * facexy / (zf + zp);
+  double Dw = div_pre(2 * P.nu * faceyz, xp + xw, F.rxw[i]), De = div_pre(2 * P.nu * faceyz, xp + xe, F.rxe[i]);
+  double Ds = div_pre(2 * P.nu * facexz, ys + yp, F.rys[j]), Dn = div_pre(2 * P.nu * facexz, yn + yp, F.ryn[j]);
+  double Db = div_pre(2 * P.nu * facexy, zb + zp, F.rzb[k]), Df = div_pre(2 * P.nu * facexy, zf + zp, F.rzf[k]);
   double vc = ld(v + IV(F, i, j, k));
   double fn = 0.5 * P.rho * facexz * (vc + ld(v + IV(F, i, j - 1, k)));
   double fs = 0.5 * P.rho * facexz * (vc + ld(v + IV(F, i, j + 1, k)));
@@ -267,9 +289,9 @@ __device__ __forceinline__ double upd_w(const FluidDev &F, const Prm &P, int i, 
   double xp = F.xp[i], xw = F.xw[i], xe = F.xe[i], yp = F.yp[j], ys = F.ys[j], yn = F.yn[j];
   double zp = F.zp[k], zf = F.zf[k], zb = F.zb[k];
   double facexy = xp * yp, facexz = xp * zp, faceyz = yp * zp;
-  double Dw = 2 * P.nu * faceyz / (xp + xw), De = 2 * P.nu * faceyz / (xp + xe);
-  double Ds = 2 * P.nu * facexz / (ys + yp), Dn = 2 * P.nu * facexz / (yn + yp);
-  double Db = 2 * P.nu * facexy / (zb + zp), Df = 2 * P.nu * facexy / (zf + zp);
+  double Dw = div_pre(2 * P.nu * faceyz, xp + xw, F.rxw[i]), De = div_pre(2 * P.nu * faceyz, xp + xe, F.rxe[i]);
+  double Ds = div_pre(2 * P.nu * facexz, ys + yp, F.rys[j]), Dn = div_pre(2 * P.nu * facexz, yn + yp, F.ryn[j]);
+  double Db = div_pre(2 * P.nu * facexy, zb + zp, F.rzb[k]), Df = div_pre(2 * P.nu * facexy, zf + zp, F.rzf[k]);
   double wc = ld(w + IW(F, i, j, k));
   double fb = 0.5 * P.rho * facexy * (wc + ld(w + IW(F, i, j, k - 1)));
   double ff = 0.5 * P.rho * facexy * (wc + ld(w + IW(F, i, j, k + 1)));
@@ -357,23 +379,29 @@ struct EnergyIn {
   bool ok;
 };
 __device__ __forceinline__ void energy_gather(const FluidDev &F, int i, int j, int k, EnergyIn &e) {
-  const double *Tt = F.tt;
-  const int q = IP(F, i, j, k);
-  e.q = q; e.i = i; e.j = j; e.k = k;
-  const int PX = F.cx + 2, PXY = (F.cx + 2) * (F.cy + 2);
-  e.te = ld(Tt + q + 1); e.tw = ld(Tt + q - 1); e.tn = ld(Tt + q + PX); e.ts = ld(Tt + q - PX);
-  e.tf = ld(Tt + q + PXY); e.tb = ld(Tt + q - PXY); e.tc = ld(Tt + q);
-  e.u = __ldg(F.u + IU(F, i, j, k)); e.v = __ldg(F.v + IV(F, i, j, k)); e.w = __ldg(F.w + IW(F, i, j, k));
+  const double *Ts = F.ts;
+  const long long row = (long long)F.hx * (j + (long long)(F.cy + 2) * k);
+  const long long q = (i & 1) * F.hs + (i >> 1) + row, qo = ((i & 1) ^ 1) * F.hs + row;
+  e.q = (int)q; e.i = i; e.j = j; e.k = k;
+  const int PY = F.hx, PZ = F.hx * (F.cy + 2);
+  e.te = ld(Ts + qo + ((i + 1) >> 1)); e.tw = ld(Ts + qo + ((i - 1) >> 1));
+  e.tn = ld(Ts + q + PY); e.ts = ld(Ts + q - PY); e.tf = ld(Ts + q + PZ); e.tb = ld(Ts + q - PZ);
+  e.tc = ld(Ts + q);
+  e.u = __ldg(F.us + q); e.v = __ldg(F.vs + q); e.w = __ldg(F.ws + q);
   e.ok = e.ok && !F.empty[GC(F, i - 1, j - 1, k - 1)];
 }
 __device__ __forceinline__ void energy_apply(const FluidDev &F, const Prm &P, const EnergyIn &e, double &acc) {
   double xp = F.xp[e.i], xw = F.xw[e.i], yp = F.yp[e.j], ys = F.ys[e.j], zp = F.zp[e.k], zf = F.zf[e.k];
   double sx = (xp + xw) / 2.0, sy = (yp + ys) / 2.0, sz = (zp + zf) / 2.0;
   double conv = -e.u * (e.te - e.tw) - e.v * (e.tn - e.ts) - e.w * (e.tf - e.tb);
-  double diff = P.alpha * (e.te + e.tw) / sx / sx + P.alpha * (e.tn + e.ts) / sy / sy + P.alpha * (e.tf + e.tb) / sz / sz;
+  const double rx = F.rsx[e.i], ry = F.rsy[e.j], rz = F.rsz[e.k];
+  // alpha*(te+tw)/sx/sx etc. (fluid_solver.h:838-840) with exact divisions
+  double diff = div_pre(div_pre(P.alpha * (e.te + e.tw), sx, rx), sx, rx) +
+                div_pre(div_pre(P.alpha * (e.tn + e.ts), sy, ry), sy, ry) +
+                div_pre(div_pre(P.alpha * (e.tf + e.tb), sz, rz), sz, rz);
   double denom = 2 * P.alpha * (F.ix2[e.i] + F.iy2[e.j] + F.iz2[e.k]);
   double nv = (conv + diff) / denom * (P.relax) + (1 - P.relax) * e.tc;
-  F.tt[e.q] = nv;
+  F.ts[e.q] = nv;
   acc += (nv - e.tc) * (nv - e.tc);
 }
 
@@ -388,11 +416,23 @@ __global__ void __launch_bounds__(kBlock, 2) k_gs(FluidDev F, Prm P, double *par
   const double tol = EQ == 3 ? P.energy_tol : P.mom_tol;
   const int nrows = NJ * NK, S = NI + NJ + NK - 2;
   const int tid = blockIdx.x * blockDim.x + threadIdx.x, T = gridDim.x * blockDim.x;
-  double *own = EQ == 0 ? F.u : EQ == 1 ? F.v : EQ == 2 ? F.w : F.tt;
+  double *own = EQ == 0 ? F.u : EQ == 1 ? F.v : EQ == 2 ? F.w : F.ts;
   const long long nown = EQ == 0 ? (long long)(F.fx + 2) * (F.cy + 2) * (F.cz + 2)
                        : EQ == 1 ? (long long)(F.cx + 2) * (F.fy + 2) * (F.cz + 2)
                        : EQ == 2 ? (long long)(F.cx + 2) * (F.cy + 2) * (F.fz + 2)
-                                 : (long long)(F.cx + 2) * (F.cy + 2) * (F.cz + 2);
+                                 : 2 * F.hs;
+  const long long npadT = (long long)(F.cx + 2) * (F.cy + 2) * (F.cz + 2);
+  if (EQ == 3) {
+    // parity-split copies of T, u, v, w for this solve
+    for (long long q = tid; q < npadT; q += T) {
+      const int i = (int)(q % (F.cx + 2)), j = (int)((q / (F.cx + 2)) % (F.cy + 2)), k = (int)(q / ((long long)(F.cx + 2) * (F.cy + 2)));
+      const long long sq = (i & 1) * F.hs + (i >> 1) + (long long)F.hx * (j + (long long)(F.cy + 2) * k);
+      F.ts[sq] = F.tt[q];
+      F.us[sq] = F.u[IU(F, i, j, k)];
+      F.vs[sq] = F.v[IV(F, i, j, k)];
+      F.ws[sq] = F.w[IW(F, i, j, k)];
+    }
+  }
   const bool lid_row = (F.oy - 1 + F.fy - 1 == F.Ny);
   int buf = 0;
   const int pred = st->sweeps[EQ] > 0 ? st->sweeps[EQ] : 2;
@@ -473,6 +513,11 @@ __global__ void __launch_bounds__(kBlock, 2) k_gs(FluidDev F, Prm P, double *par
     gres = g_new;
   }
   const int T2 = T;
+  if (EQ == 3)
+    for (long long q = tid; q < npadT; q += T) {
+      const int i = (int)(q % (F.cx + 2)), j = (int)((q / (F.cx + 2)) % (F.cy + 2)), k = (int)(q / ((long long)(F.cx + 2) * (F.cy + 2)));
+      F.tt[q] = ld(F.ts + (i & 1) * F.hs + (i >> 1) + (long long)F.hx * (j + (long long)(F.cy + 2) * k));
+    }
   if (EQ == 0) bc_x(F, tid, T2);
   else if (EQ == 1) bc_y(F, P, tid, T2);
   else if (EQ == 2) bc_z(F, tid, T2);
@@ -1439,11 +1484,29 @@ Engine::Engine(const Case &c, const hs_params &p, int device) : case_(c), prm_(p
       return o;
     };
     F.ix2 = D.upload(inv2(c.xp, c.xw)); F.iy2 = D.upload(inv2(c.yp, c.ys)); F.iz2 = D.upload(inv2(c.zp, c.zf));
+    auto rcp = [](const std::vector<double> &p, const std::vector<double> &m) {
+      std::vector<double> o(p.size(), 0.0);
+      for (size_t i = 1; i + 1 < p.size(); ++i) o[i] = 1.0 / ((p[i] + m[i]) / 2.0);
+      return o;
+    };
+    F.rsx = D.upload(rcp(c.xp, c.xw)); F.rsy = D.upload(rcp(c.yp, c.ys)); F.rsz = D.upload(rcp(c.zp, c.zf));
+    auto rsum = [](const std::vector<double> &p, const std::vector<double> &m) {
+      std::vector<double> o(p.size(), 0.0);
+      for (size_t i = 1; i + 1 < p.size(); ++i) o[i] = 1.0 / (p[i] + m[i]);
+      return o;
+    };
+    F.rxw = D.upload(rsum(c.xp, c.xw)); F.rxe = D.upload(rsum(c.xp, c.xe));
+    F.rys = D.upload(rsum(c.ys, c.yp)); F.ryn = D.upload(rsum(c.yn, c.yp));
+    F.rzb = D.upload(rsum(c.zb, c.zp)); F.rzf = D.upload(rsum(c.zf, c.zp));
   }
   F.acx = D.alloc<double>(M.npad()); F.acy = D.alloc<double>(M.npad()); F.acz = D.alloc<double>(M.npad());
   F.x = D.alloc<double>(M.npad()); F.r = D.alloc<double>(M.npad()); F.pa = D.alloc<double>(M.npad());
   F.pb = D.alloc<double>(M.npad()); F.s = D.alloc<double>(M.npad());
   F.pscr = D.alloc<double>(M.ncell());
+  F.hx = (int)((M.cx + 3) / 2);
+  F.hs = (long long)F.hx * (M.cy + 2) * (M.cz + 2);
+  F.ts = D.alloc<double>(2 * F.hs); F.us = D.alloc<double>(2 * F.hs);
+  F.vs = D.alloc<double>(2 * F.hs); F.ws = D.alloc<double>(2 * F.hs);
 
   // solids: one contiguous buffer per quantity, per-region offsets
   D.nreg = (int)c.solids.size();
@@ -1534,7 +1597,7 @@ Engine::Engine(const Case &c, const hs_params &p, int device) : case_(c), prm_(p
   }
   D.g_pcorr = coop_blocks(k_pcorr, D.nsm, 1 << 30);
   D.tz = choose_tz(M.cx, M.cy, M.cz, D.g_pcorr);
-  D.snap = D.alloc<double>(std::max({M.nu(), M.nv(), M.nw(), M.npad()}));
+  D.snap = D.alloc<double>(std::max({M.nu(), M.nv(), M.nw(), M.npad(), 2 * (long)F.hs}));
   D.ssnap = D.alloc<double>(std::max<long long>(D.ntt, 1));
   D.spred = D.alloc<int>(std::max(D.nreg, 1));
   int gmax = std::max({D.g_gs[0], D.g_gs[1], D.g_gs[2], D.g_gs[3], D.g_pcorr, D.solid_blocks, 1});
@@ -1977,6 +2040,33 @@ void pcg_solve_noalloc(int nx, int ny, int nz, const double *acx, const double *
   HS_CUDA(cudaStreamSynchronize(st));
   if (iters) *iters = it;
   if (relres) *relres = rr;
+}
+
+// Check of div_pre against the IEEE quotient over caller arrays: out[i] = 1
+// where div_pre(a[i], b[i], RN(1/b[i])) differs from a[i]/b[i] in any bit.
+__global__ void k_div_check(const double *a, const double *b, long long n, unsigned char *out) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const double y = 1.0 / b[i];
+    const double q1 = div_pre(a[i], b[i], y), q2 = a[i] / b[i];
+    out[i] = __double_as_longlong(q1) != __double_as_longlong(q2);
+  }
+}
+
+long long div_check(const double *a, const double *b, long long n) {
+  unsigned char *out = nullptr;
+  double *da = nullptr, *db = nullptr;
+  HS_CUDA(cudaMalloc(&da, n * 8));
+  HS_CUDA(cudaMalloc(&db, n * 8));
+  HS_CUDA(cudaMalloc(&out, n));
+  HS_CUDA(cudaMemcpy(da, a, n * 8, cudaMemcpyHostToDevice));
+  HS_CUDA(cudaMemcpy(db, b, n * 8, cudaMemcpyHostToDevice));
+  k_div_check<<<1024, 256>>>(da, db, n, out);
+  std::vector<unsigned char> h(n);
+  HS_CUDA(cudaMemcpy(h.data(), out, n, cudaMemcpyDeviceToHost));
+  cudaFree(da); cudaFree(db); cudaFree(out);
+  long long bad = 0;
+  for (auto v : h) bad += v;
+  return bad;
 }
 
 }  // namespace hs

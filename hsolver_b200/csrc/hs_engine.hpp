@@ -62,4 +62,8 @@ long long noalloc_max_padded_cells();
 void pcg_solve_noalloc(int nx, int ny, int nz, const double *acx, const double *acy, const double *acz, const double *b,
                        double *x, double tol, int maxiter, void *stream, int *iters, double *relres);
 
+// Number of (a, b) pairs where the precomputed-reciprocal division used by the
+// sweeps differs from IEEE a/b (validation helper).
+long long div_check(const double *a, const double *b, long long n);
+
 }  // namespace hs

@@ -192,6 +192,12 @@ void hs_pcg_destroy(hs_pcg *h);
 int hs_pcg_solve_noalloc(int nx, int ny, int nz, const double *acx, const double *acy, const double *acz,
                          const double *b, double *x, double tol, int maxiter, void *stream, int *iters, double *relres);
 
+/* Validation of the divisions the sweeps perform with precomputed
+ * reciprocals: returns how many of the n host pairs (a[i], b[i]) give a
+ * quotient that differs in any bit from IEEE a/b on the current device
+ * (negative HS_ERR_* on failure). */
+long long hs_check_division(const double *a, const double *b, long long n);
+
 /* Release all device and host state. */
 void hs_destroy(hs_ctx *ctx);
 
