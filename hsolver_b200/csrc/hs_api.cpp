@@ -8,6 +8,7 @@
 
 #include "../../include/hsolver_b200.h"
 #include "hs_case.hpp"
+#include "hs_cht.hpp"
 #include "hs_engine.hpp"
 
 struct hs_ctx {
@@ -21,6 +22,13 @@ struct hs_case {
 
 struct hs_pcg {
   hs::PcgWork *w = nullptr;
+};
+
+struct hs_cht {
+  hs_ctx *ctx = nullptr;
+  hs::ChtState *st = nullptr;
+  double k_fluid = 1.0;
+  std::string err;
 };
 
 namespace {
@@ -368,6 +376,98 @@ int hs_pcg_solve_noalloc(int nx, int ny, int nz, const double *acx, const double
 void hs_pcg_destroy(hs_pcg *h) {
   if (!h) return;
   hs::pcg_destroy(h->w);
+  delete h;
+}
+
+void hs_cht_params_default(hs_cht_params *p) {
+  if (!p) return;
+  std::memset(p, 0, sizeof(*p));
+  p->k_fluid = 1.0;
+  p->t_boundary = 293.0;
+  p->tol = 1e-10;
+  p->maxiter = 5000;
+}
+
+int hs_cht_create(hs_ctx *ctx, const hs_cht_params *prm, hs_cht **out) {
+  if (!out) return fail(ctx, HS_ERR_ARG, "null output pointer");
+  *out = nullptr;
+  return guarded(ctx, [&](hs::Engine &e) {
+    hs_cht_params p;
+    if (prm) p = *prm; else hs_cht_params_default(&p);
+    if (!(p.k_fluid > 0) || !(p.tol > 0) || p.maxiter < 1) throw std::invalid_argument("invalid CHT parameters");
+    const hs::Case &c = e.kase();
+    hs::ChtSetup S;
+    S.device = e.device(); S.stream = e.stream_handle();
+    S.Nx = (int)c.Nx; S.Ny = (int)c.Ny; S.Nz = (int)c.Nz; S.nreg = (int)c.solids.size();
+    S.xs = c.deck.xs.data(); S.ys = c.deck.ys.data(); S.zs = c.deck.zs.data();
+    S.ctype = c.ctype.data();
+    std::vector<int> reg(c.region.size());
+    for (size_t i = 0; i < reg.size(); ++i) reg[i] = c.ctype[i] ? c.region[i] : -1;
+    S.region = reg.data();
+    S.t_boundary = p.t_boundary; S.tol = p.tol; S.maxiter = p.maxiter;
+    hs_cht *h = new hs_cht();
+    h->ctx = ctx;
+    h->k_fluid = p.k_fluid;
+    try {
+      h->st = hs::cht_create(S);
+      std::vector<double> kr(S.nreg, p.k_fluid);
+      hs::cht_set_solid(h->st, p.k_fluid, kr.data(), nullptr);
+    } catch (...) {
+      if (h->st) hs::cht_destroy(h->st);
+      delete h;
+      throw;
+    }
+    *out = h;
+    return HS_OK;
+  });
+}
+
+int hs_cht_set_solid(hs_cht *h, const double *k_region, const double *q_cell) {
+  if (!h || !k_region) return fail(nullptr, HS_ERR_ARG, "null argument");
+  return guarded(h->ctx, [&](hs::Engine &) {
+    hs::cht_set_solid(h->st, h->k_fluid, k_region, q_cell);
+    return HS_OK;
+  });
+}
+
+int hs_cht_forward(hs_cht *h, double *T, double *J, int *iters, double *relres) {
+  if (!h) return fail(nullptr, HS_ERR_ARG, "null handle");
+  return guarded(h->ctx, [&](hs::Engine &e) {
+    const hs::Case &c = e.kase();
+    hs::ChtVelSrc V;
+    V.Nx = (int)c.Nx; V.Ny = (int)c.Ny; V.Nz = (int)c.Nz;
+    V.cx = (int)c.fluid.cx; V.cy = (int)c.fluid.cy; V.cz = (int)c.fluid.cz;
+    V.fx = (int)c.fluid.fx; V.fy = (int)c.fluid.fy; V.fz = (int)c.fluid.fz;
+    V.ox = (int)c.fluid.ox; V.oy = (int)c.fluid.oy; V.oz = (int)c.fluid.oz;
+    long n;
+    V.u = e.field_device_ptr(HS_F_U_STAR, &n); V.v = e.field_device_ptr(HS_F_V_STAR, &n);
+    V.w = e.field_device_ptr(HS_F_W_STAR, &n);
+    V.ctype = nullptr;
+    hs::cht_set_velocities(h->st, V);
+    hs::cht_forward(h->st, T, J, iters, relres);
+    return HS_OK;
+  });
+}
+
+int hs_cht_adjoint(hs_cht *h, double *dJdq, double *dJdk, int *iters, double *relres) {
+  if (!h) return fail(nullptr, HS_ERR_ARG, "null handle");
+  return guarded(h->ctx, [&](hs::Engine &) {
+    hs::cht_adjoint(h->st, dJdq, dJdk, iters, relres);
+    return HS_OK;
+  });
+}
+
+int hs_cht_velocities(hs_cht *h, double *ug, double *vg, double *wg) {
+  if (!h || !ug || !vg || !wg) return fail(nullptr, HS_ERR_ARG, "null argument");
+  return guarded(h->ctx, [&](hs::Engine &) {
+    hs::cht_get_velocities(h->st, ug, vg, wg);
+    return HS_OK;
+  });
+}
+
+void hs_cht_destroy(hs_cht *h) {
+  if (!h) return;
+  hs::cht_destroy(h->st);
   delete h;
 }
 

@@ -1,0 +1,565 @@
+// Conjugate-heat-transfer energy equation on the whole grid (fluid and solid
+// cells as one operator) with the flow frozen at the solver's current face
+// velocities, and its adjoint for J = (sum_solid T^8 dV)^(1/8).
+//
+// The reference couples fluid and solid temperatures only through a ghost
+// value swap (solver.h:62-148) and has no heat source, conductivity ratio or
+// adjoint; this module is the monolithic form: per face between cells P, N
+//   G = A / (dP/(2 kP) + dN/(2 kN))     (harmonic-mean interface conductance)
+//   F = u A (outward from P)            (first-order upwind convection)
+// boundary faces carry Dirichlet Tb through G_b = 2 kP A / dP; row P is
+//   (sum G + max(F,0)) T_P - sum (G + max(-F,0)) T_N = q_P V_P + boundary terms.
+// The transposed operator has the same stencil with the upwind side swapped:
+// A^T_{P,N} = A_{N,P}, read from the neighbour's stored coefficient.
+// Both solves use the same cooperative Jacobi-preconditioned BiCGStab.
+#include <cooperative_groups.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "hs_cht.hpp"
+
+namespace cg = cooperative_groups;
+
+namespace hs {
+
+#define HC_CUDA(call)                                                                              \
+  do {                                                                                             \
+    cudaError_t e_ = (call);                                                                       \
+    if (e_ != cudaSuccess) throw std::runtime_error(std::string("CUDA: ") + cudaGetErrorString(e_) + \
+                                                    " at " #call);                                 \
+  } while (0)
+
+namespace {
+
+constexpr int kB = 256;
+
+struct ChtDev {
+  int Nx, Ny, Nz;
+  const double *dx, *dy, *dz;      // cell widths
+  const uint8_t *solid;            // padded
+  const double *k;                 // padded conductivity
+  const double *q;                 // padded source
+  const double *ug, *vg, *wg;      // global face velocities
+  double *d, *aw, *ae, *as, *an, *ab, *af, *b, *dinv;  // padded coefficients
+};
+
+__device__ __forceinline__ int pidx(const ChtDev &H, int i, int j, int k) {  // 0-based cell -> padded
+  return (i + 1) + (H.Nx + 2) * ((j + 1) + (H.Ny + 2) * (k + 1));
+}
+
+__device__ double blk_sum(double v, double *sh) {
+  for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) sh[wid] = v;
+  __syncthreads();
+  double t = 0.0;
+  if (wid == 0) {
+    t = lane < (int)(blockDim.x >> 5) ? sh[lane] : 0.0;
+    for (int o = 16; o; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+  }
+  __syncthreads();
+  return t;
+}
+
+// several sums at once over the grid, identical in every thread
+template <int M>
+__device__ void grid_sums(double (&v)[M], double *partials, int &buf, double *sh, cg::grid_group &grid) {
+  double *pp = partials + (size_t)buf * gridDim.x * M;
+  buf ^= 1;
+#pragma unroll
+  for (int m = 0; m < M; ++m) {
+    double b = blk_sum(v[m], sh);
+    if (threadIdx.x == 0) pp[(size_t)blockIdx.x * M + m] = b;
+  }
+  grid.sync();
+  if (threadIdx.x < 32) {
+#pragma unroll
+    for (int m = 0; m < M; ++m) {
+      double a = 0.0;
+      for (int q = threadIdx.x; q < (int)gridDim.x; q += 32) a += __ldcg(pp + (size_t)q * M + m);
+      for (int o = 16; o; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+      if (threadIdx.x == 0) sh[40 + m] = a;
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int m = 0; m < M; ++m) v[m] = sh[40 + m];
+  __syncthreads();
+}
+
+// face (direction d: W E S N B F) of cell (i,j,k): conductance, outward flux, neighbour exists
+__device__ __forceinline__ void face(const ChtDev &H, int i, int j, int k, int d, double &G, double &F, bool &has) {
+  const double dxi = H.dx[i], dyj = H.dy[j], dzk = H.dz[k];
+  const double kp = H.k[pidx(H, i, j, k)];
+  const int ax = d >> 1, hi = d & 1;
+  double A, dP, dN = 0, u;
+  int ii = i, jj = j, kk = k;
+  if (ax == 0) {
+    A = dyj * dzk; dP = dxi; ii = hi ? i + 1 : i - 1;
+    u = H.ug[(hi ? i + 1 : i) + (H.Nx + 1) * (j + H.Ny * k)];
+    has = ii >= 0 && ii < H.Nx; if (has) dN = H.dx[ii];
+  } else if (ax == 1) {
+    A = dxi * dzk; dP = dyj; jj = hi ? j + 1 : j - 1;
+    u = H.vg[i + H.Nx * ((hi ? j + 1 : j) + (H.Ny + 1) * k)];
+    has = jj >= 0 && jj < H.Ny; if (has) dN = H.dy[jj];
+  } else {
+    A = dxi * dyj; dP = dzk; kk = hi ? k + 1 : k - 1;
+    u = H.wg[i + H.Nx * (j + H.Ny * (hi ? k + 1 : k))];
+    has = kk >= 0 && kk < H.Nz; if (has) dN = H.dz[kk];
+  }
+  if (has) G = A / (dP / (2 * kp) + dN / (2 * H.k[pidx(H, ii, jj, kk)]));
+  else G = 2 * kp * A / dP;
+  F = (hi ? u : -u) * A;
+}
+
+__global__ void k_cht_assemble(ChtDev H, double Tb) {
+  const int n = H.Nx * H.Ny * H.Nz;
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
+    const int i = c % H.Nx, j = (c / H.Nx) % H.Ny, k = c / (H.Nx * H.Ny);
+    const int q = pidx(H, i, j, k);
+    double diag = 0.0, a[6], rhs = H.q[q] * H.dx[i] * H.dy[j] * H.dz[k];
+    for (int d = 0; d < 6; ++d) {
+      double G, F;
+      bool has;
+      face(H, i, j, k, d, G, F, has);
+      diag += G + fmax(F, 0.0);
+      a[d] = has ? G + fmax(-F, 0.0) : 0.0;
+      if (!has) rhs += (G + fmax(-F, 0.0)) * Tb;
+    }
+    H.d[q] = diag; H.dinv[q] = 1.0 / diag;
+    H.aw[q] = a[0]; H.ae[q] = a[1]; H.as[q] = a[2]; H.an[q] = a[3]; H.ab[q] = a[4]; H.af[q] = a[5];
+    H.b[q] = rhs;
+  }
+}
+
+// y = A x (transpose = 0) or A^T x at padded q
+__device__ __forceinline__ double apply_at(const ChtDev &H, const double *x, int q, int PX, int PXY, bool tr) {
+  const double off = tr ? H.ae[q - 1] * __ldcg(x + q - 1) + H.aw[q + 1] * __ldcg(x + q + 1) +
+                              H.an[q - PX] * __ldcg(x + q - PX) + H.as[q + PX] * __ldcg(x + q + PX) +
+                              H.af[q - PXY] * __ldcg(x + q - PXY) + H.ab[q + PXY] * __ldcg(x + q + PXY)
+                        : H.aw[q] * __ldcg(x + q - 1) + H.ae[q] * __ldcg(x + q + 1) + H.as[q] * __ldcg(x + q - PX) +
+                              H.an[q] * __ldcg(x + q + PX) + H.ab[q] * __ldcg(x + q - PXY) + H.af[q] * __ldcg(x + q + PXY);
+  return H.d[q] * __ldcg(x + q) - off;
+}
+
+struct Vec {
+  double *x, *r, *rh, *p, *v, *ph, *s, *sh, *t;
+};
+
+// Jacobi-preconditioned BiCGStab (van der Vorst, SIAM J. Sci. Stat. Comput.
+// 13(2), 1992) for A x = rhs or A^T x = rhs; x holds the start.
+__global__ void __launch_bounds__(kB) k_cht_bicgstab(ChtDev H, Vec V, const double *rhs, int transpose, double tol,
+                                                     int maxiter, double *partials, int *out_it, double *out_rel) {
+  cg::grid_group grid = cg::this_grid();
+  __shared__ double sh[48];
+  const int Nx = H.Nx, Ny = H.Ny, n = Nx * H.Ny * H.Nz;
+  const int PX = Nx + 2, PXY = (Nx + 2) * (Ny + 2);
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x, T = gridDim.x * blockDim.x;
+  const bool tr = transpose != 0;
+  int buf = 0;
+  double red[2] = {0.0, 0.0};
+  for (int c = tid; c < n; c += T) {
+    const int q = pidx(H, c % Nx, (c / Nx) % Ny, c / (Nx * Ny));
+    const double rv = rhs[q] - apply_at(H, V.x, q, PX, PXY, tr);
+    V.r[q] = rv; V.rh[q] = rv; V.p[q] = 0.0; V.v[q] = 0.0;
+    red[0] += rhs[q] * rhs[q];
+    red[1] += rv * rv;
+  }
+  grid_sums<2>(red, partials, buf, sh, grid);
+  double bb = red[0] > 0 ? red[0] : 1.0, rr = red[1];
+  const double eps = tol * tol;
+  double rho = 1.0, alpha = 1.0, omega = 1.0;
+  int it = 0;
+  while (it < maxiter && !(rr / bb < eps)) {
+    it++;
+    double s1[1] = {0.0};
+    for (int c = tid; c < n; c += T) {
+      const int q = pidx(H, c % Nx, (c / Nx) % Ny, c / (Nx * Ny));
+      s1[0] += V.rh[q] * V.r[q];
+    }
+    grid_sums<1>(s1, partials, buf, sh, grid);
+    const double rho1 = s1[0];
+    const double beta = (rho1 / rho) * (alpha / omega);
+    for (int c = tid; c < n; c += T) {
+      const int q = pidx(H, c % Nx, (c / Nx) % Ny, c / (Nx * Ny));
+      const double pv = V.r[q] + beta * (V.p[q] - omega * V.v[q]);
+      V.p[q] = pv;
+      V.ph[q] = pv * H.dinv[q];
+    }
+    grid.sync();
+    double s2[1] = {0.0};
+    for (int c = tid; c < n; c += T) {
+      const int q = pidx(H, c % Nx, (c / Nx) % Ny, c / (Nx * Ny));
+      const double vv = apply_at(H, V.ph, q, PX, PXY, tr);
+      V.v[q] = vv;
+      s2[0] += V.rh[q] * vv;
+    }
+    grid_sums<1>(s2, partials, buf, sh, grid);
+    alpha = rho1 / s2[0];
+    double s3[1] = {0.0};
+    for (int c = tid; c < n; c += T) {
+      const int q = pidx(H, c % Nx, (c / Nx) % Ny, c / (Nx * Ny));
+      const double sv = V.r[q] - alpha * V.v[q];
+      V.s[q] = sv;
+      V.sh[q] = sv * H.dinv[q];
+      s3[0] += sv * sv;
+    }
+    grid_sums<1>(s3, partials, buf, sh, grid);
+    if (s3[0] / bb < eps) {
+      for (int c = tid; c < n; c += T) {
+        const int q = pidx(H, c % Nx, (c / Nx) % Ny, c / (Nx * Ny));
+        V.x[q] += alpha * V.ph[q];
+      }
+      rr = s3[0];
+      break;
+    }
+    double s4[2] = {0.0, 0.0};
+    for (int c = tid; c < n; c += T) {
+      const int q = pidx(H, c % Nx, (c / Nx) % Ny, c / (Nx * Ny));
+      const double tv = apply_at(H, V.sh, q, PX, PXY, tr);
+      V.t[q] = tv;
+      s4[0] += tv * V.s[q];
+      s4[1] += tv * tv;
+    }
+    grid_sums<2>(s4, partials, buf, sh, grid);
+    omega = s4[0] / s4[1];
+    double s5[1] = {0.0};
+    for (int c = tid; c < n; c += T) {
+      const int q = pidx(H, c % Nx, (c / Nx) % Ny, c / (Nx * Ny));
+      V.x[q] += alpha * V.ph[q] + omega * V.sh[q];
+      const double rv = V.s[q] - omega * V.t[q];
+      V.r[q] = rv;
+      s5[0] += rv * rv;
+    }
+    grid_sums<1>(s5, partials, buf, sh, grid);
+    rr = s5[0];
+    rho = rho1;
+  }
+  if (tid == 0) { *out_it = it; *out_rel = sqrt(rr / bb); }
+}
+
+// dJ/dT (into g) and the per-block sum of T^8 dV for J
+__global__ void k_cht_objective(ChtDev H, const double *T, double *g, double *partial_sum8) {
+  __shared__ double sh[48];
+  const int n = H.Nx * H.Ny * H.Nz;
+  double acc = 0.0;
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
+    const int i = c % H.Nx, j = (c / H.Nx) % H.Ny, k = c / (H.Nx * H.Ny);
+    const int q = pidx(H, i, j, k);
+    if (!H.solid[q]) continue;
+    const double t = T[q], t2 = t * t, t4 = t2 * t2;
+    acc += t4 * t4 * H.dx[i] * H.dy[j] * H.dz[k];
+  }
+  double b = blk_sum(acc, sh);
+  if (threadIdx.x == 0) partial_sum8[blockIdx.x] = b;
+  (void)g;
+}
+
+__global__ void k_cht_djdt(ChtDev H, const double *T, double f, double *g) {
+  const int n = H.Nx * H.Ny * H.Nz;
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
+    const int i = c % H.Nx, j = (c / H.Nx) % H.Ny, k = c / (H.Nx * H.Ny);
+    const int q = pidx(H, i, j, k);
+    if (!H.solid[q]) { g[q] = 0.0; continue; }
+    const double t = T[q], t2 = t * t, t3 = t2 * t, t7 = t3 * t3 * t;
+    g[q] = f * t7 * H.dx[i] * H.dy[j] * H.dz[k];
+  }
+}
+
+// per-cell pieces of the gradients: dJ/dq_P = lam_P V_P and the cell's share
+// of dJ/dk (sum over its faces of -dG/dk_P (lam_P - lam_N)(T_P - T_N))
+__global__ void k_cht_grad(ChtDev H, const double *T, const double *lam, double Tb, double *dJdq, double *dk_cell) {
+  const int n = H.Nx * H.Ny * H.Nz;
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
+    const int i = c % H.Nx, j = (c / H.Nx) % H.Ny, k = c / (H.Nx * H.Ny);
+    const int q = pidx(H, i, j, k);
+    if (!H.solid[q]) { dJdq[c] = 0.0; dk_cell[c] = 0.0; continue; }
+    const double dx = H.dx[i], dy = H.dy[j], dz = H.dz[k], kp = H.k[q];
+    dJdq[c] = lam[q] * dx * dy * dz;
+    double acc = 0.0;
+    for (int d = 0; d < 6; ++d) {
+      double G, F;
+      bool has;
+      face(H, i, j, k, d, G, F, has);
+      const int ax = d >> 1;
+      const double A = ax == 0 ? dy * dz : ax == 1 ? dx * dz : dx * dy, dP = ax == 0 ? dx : ax == 1 ? dy : dz;
+      const double dG = has ? G * G * dP / (2 * A * kp * kp) : G / kp;
+      int qn = q;
+      if (d == 0) qn = q - 1; else if (d == 1) qn = q + 1;
+      else if (d == 2) qn = q - (H.Nx + 2); else if (d == 3) qn = q + (H.Nx + 2);
+      else if (d == 4) qn = q - (H.Nx + 2) * (H.Ny + 2); else qn = q + (H.Nx + 2) * (H.Ny + 2);
+      const double tn = has ? T[qn] : Tb, ln = has ? lam[qn] : 0.0;
+      acc -= dG * (lam[q] - ln) * (T[q] - tn);
+    }
+    dk_cell[c] = acc;
+  }
+}
+
+// face velocities of the global grid from the fluid box's u*, v*, w*; faces
+// outside the fluid box or touching a solid cell carry no flow
+__global__ void k_cht_velocities(ChtVelSrc S, double *ug, double *vg, double *wg) {
+  const int Nx = S.Nx, Ny = S.Ny, Nz = S.Nz;
+  const long long nu = (long long)(Nx + 1) * Ny * Nz, nv = (long long)Nx * (Ny + 1) * Nz, nw = (long long)Nx * Ny * (Nz + 1);
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < nu + nv + nw; e += (long long)gridDim.x * blockDim.x) {
+    int dir, i, j, k;
+    if (e < nu) { dir = 0; i = e % (Nx + 1); j = (e / (Nx + 1)) % Ny; k = e / ((long long)(Nx + 1) * Ny); }
+    else if (e < nu + nv) { long long f = e - nu; dir = 1; i = f % Nx; j = (f / Nx) % (Ny + 1); k = f / ((long long)Nx * (Ny + 1)); }
+    else { long long f = e - nu - nv; dir = 2; i = f % Nx; j = (f / Nx) % Ny; k = f / ((long long)Nx * Ny); }
+    // the two cells the face separates (0-based global); -1 outside
+    int ia = i, ja = j, ka = k;
+    if (dir == 0) ia = i - 1; else if (dir == 1) ja = j - 1; else ka = k - 1;
+    auto is_solid = [&](int a, int b, int c) {
+      if (a < 0 || b < 0 || c < 0 || a >= Nx || b >= Ny || c >= Nz) return false;
+      return S.ctype[a + Nx * (b + Ny * c)] != 0;
+    };
+    double val = 0.0;
+    if (!is_solid(ia, ja, ka) && !is_solid(i, j, k)) {
+      // local face index in the fluid box (1-based offsets)
+      const int li = i - (S.ox - 1), lj = j - (S.oy - 1), lk = k - (S.oz - 1);
+      if (dir == 0 && li >= 0 && li < S.fx && lj >= 0 && lj < S.cy && lk >= 0 && lk < S.cz)
+        val = S.u[(li + 1) + (S.fx + 2) * ((lj + 1) + (S.cy + 2) * (lk + 1))];
+      else if (dir == 1 && li >= 0 && li < S.cx && lj >= 0 && lj < S.fy && lk >= 0 && lk < S.cz)
+        val = S.v[(li + 1) + (S.cx + 2) * ((lj + 1) + (S.fy + 2) * (lk + 1))];
+      else if (dir == 2 && li >= 0 && li < S.cx && lj >= 0 && lj < S.cy && lk >= 0 && lk < S.fz)
+        val = S.w[(li + 1) + (S.cx + 2) * ((lj + 1) + (S.cy + 2) * (lk + 1))];
+    }
+    if (dir == 0) ug[e] = val; else if (dir == 1) vg[e - nu] = val; else wg[e - nu - nv] = val;
+  }
+}
+
+int coop_grid(const void *kernel, int device) {
+  int nsm = 0, per = 0;
+  HC_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
+  HC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, kB, 0));
+  if (per < 1) throw std::runtime_error("cooperative kernel cannot be resident");
+  return per * nsm;
+}
+
+int gfor(long long n) { return (int)std::max<long long>(1, std::min<long long>((n + kB - 1) / kB, 148LL * 16)); }
+
+}  // namespace
+
+struct ChtState {
+  int device;
+  cudaStream_t stream;
+  ChtDev H{};
+  Vec V{};
+  double Tb, tol;
+  int maxiter, grid, nreg;
+  std::vector<void *> allocs;
+  double *T = nullptr, *lam = nullptr, *g = nullptr, *partials = nullptr, *res = nullptr;
+  double *ug = nullptr, *vg = nullptr, *wg = nullptr, *dJdq = nullptr, *dkc = nullptr;
+  double *kp = nullptr, *qp = nullptr;
+  uint8_t *solid = nullptr, *ctype_dev = nullptr;
+  int *it = nullptr;
+  std::vector<int> region;      // per global cell (-1 fluid)
+  std::vector<uint8_t> ctype;
+  double J = 0;
+  bool have_T = false;
+  template <class T_>
+  T_ *alloc(size_t n) {
+    void *p = nullptr;
+    cudaError_t e = cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(T_));
+    if (e != cudaSuccess) throw std::runtime_error(std::string("CUDA alloc: ") + cudaGetErrorString(e));
+    allocs.push_back(p);
+    HC_CUDA(cudaMemsetAsync(p, 0, std::max<size_t>(n, 1) * sizeof(T_), stream));
+    return (T_ *)p;
+  }
+  ~ChtState() {
+    for (void *p : allocs) cudaFree(p);
+  }
+};
+
+ChtState *cht_create(const ChtSetup &S) {
+  HC_CUDA(cudaSetDevice(S.device));
+  std::unique_ptr<ChtState> C(new ChtState());
+  C->device = S.device;
+  C->stream = (cudaStream_t)S.stream;
+  C->Tb = S.t_boundary; C->tol = S.tol; C->maxiter = S.maxiter; C->nreg = S.nreg;
+  ChtDev &H = C->H;
+  H.Nx = S.Nx; H.Ny = S.Ny; H.Nz = S.Nz;
+  const size_t np = (size_t)(S.Nx + 2) * (S.Ny + 2) * (S.Nz + 2), n = (size_t)S.Nx * S.Ny * S.Nz;
+  auto up = [&](const std::vector<double> &v) {
+    double *p = C->alloc<double>(v.size());
+    HC_CUDA(cudaMemcpyAsync(p, v.data(), v.size() * 8, cudaMemcpyHostToDevice, C->stream));
+    return p;
+  };
+  std::vector<double> dx(S.Nx), dy(S.Ny), dz(S.Nz);
+  for (int i = 0; i < S.Nx; ++i) dx[i] = S.xs[i + 1] - S.xs[i];
+  for (int j = 0; j < S.Ny; ++j) dy[j] = S.ys[j + 1] - S.ys[j];
+  for (int k = 0; k < S.Nz; ++k) dz[k] = S.zs[k + 1] - S.zs[k];
+  H.dx = up(dx); H.dy = up(dy); H.dz = up(dz);
+  C->ctype.assign(S.ctype, S.ctype + n);
+  C->region.assign(S.region, S.region + n);
+  std::vector<uint8_t> solid(np, 0);
+  for (int k = 0; k < S.Nz; ++k)
+    for (int j = 0; j < S.Ny; ++j)
+      for (int i = 0; i < S.Nx; ++i)
+        solid[(i + 1) + (S.Nx + 2) * ((j + 1) + (S.Ny + 2) * (k + 1))] = S.ctype[i + S.Nx * (j + S.Ny * k)];
+  C->ctype_dev = C->alloc<uint8_t>(n);
+  HC_CUDA(cudaMemcpyAsync(C->ctype_dev, S.ctype, n, cudaMemcpyHostToDevice, C->stream));
+  C->solid = C->alloc<uint8_t>(np);
+  HC_CUDA(cudaMemcpyAsync(C->solid, solid.data(), np, cudaMemcpyHostToDevice, C->stream));
+  H.solid = C->solid;
+  C->kp = C->alloc<double>(np); C->qp = C->alloc<double>(np);
+  H.k = C->kp; H.q = C->qp;
+  C->ug = C->alloc<double>((size_t)(S.Nx + 1) * S.Ny * S.Nz);
+  C->vg = C->alloc<double>((size_t)S.Nx * (S.Ny + 1) * S.Nz);
+  C->wg = C->alloc<double>((size_t)S.Nx * S.Ny * (S.Nz + 1));
+  H.ug = C->ug; H.vg = C->vg; H.wg = C->wg;
+  double **coef[] = {&H.d, &H.aw, &H.ae, &H.as, &H.an, &H.ab, &H.af, &H.b, &H.dinv};
+  for (double **c : coef) *c = C->alloc<double>(np);
+  double **vec[] = {&C->V.x, &C->V.r, &C->V.rh, &C->V.p, &C->V.v, &C->V.ph, &C->V.s, &C->V.sh, &C->V.t};
+  for (double **v : vec) *v = C->alloc<double>(np);
+  C->T = C->alloc<double>(np); C->lam = C->alloc<double>(np); C->g = C->alloc<double>(np);
+  C->dJdq = C->alloc<double>(n); C->dkc = C->alloc<double>(n);
+  C->grid = coop_grid((const void *)k_cht_bicgstab, S.device);
+  C->partials = C->alloc<double>((size_t)2 * C->grid * 2 + 4096);
+  C->res = C->alloc<double>(1); C->it = C->alloc<int>(1);
+  HC_CUDA(cudaStreamSynchronize(C->stream));
+  return C.release();
+}
+
+void cht_destroy(ChtState *C) {
+  if (!C) return;
+  cudaSetDevice(C->device);
+  cudaStreamSynchronize(C->stream);
+  delete C;
+}
+
+void cht_set_solid(ChtState *C, double k_fluid, const double *k_region, const double *q_cell) {
+  HC_CUDA(cudaSetDevice(C->device));
+  const ChtDev &H = C->H;
+  const size_t np = (size_t)(H.Nx + 2) * (H.Ny + 2) * (H.Nz + 2);
+  std::vector<double> k(np, 0.0), q(np, 0.0);
+  for (int kk = 0; kk < H.Nz; ++kk)
+    for (int j = 0; j < H.Ny; ++j)
+      for (int i = 0; i < H.Nx; ++i) {
+        const size_t c = i + (size_t)H.Nx * (j + (size_t)H.Ny * kk);
+        const size_t p = (i + 1) + (H.Nx + 2) * ((j + 1) + (size_t)(H.Ny + 2) * (kk + 1));
+        if (C->ctype[c]) {
+          const int r = C->region[c];
+          if (r < 0 || r >= C->nreg) throw std::invalid_argument("solid cell without a region");
+          if (!(k_region[r] > 0)) throw std::invalid_argument("solid conductivity must be positive");
+          k[p] = k_region[r];
+          q[p] = q_cell ? q_cell[c] : 0.0;
+        } else {
+          k[p] = k_fluid;
+        }
+      }
+  HC_CUDA(cudaMemcpyAsync(C->kp, k.data(), np * 8, cudaMemcpyHostToDevice, C->stream));
+  HC_CUDA(cudaMemcpyAsync(C->qp, q.data(), np * 8, cudaMemcpyHostToDevice, C->stream));
+  HC_CUDA(cudaStreamSynchronize(C->stream));
+}
+
+void cht_set_velocities(ChtState *C, const ChtVelSrc &src) {
+  HC_CUDA(cudaSetDevice(C->device));
+  const ChtDev &H = C->H;
+  long long nf = (long long)(H.Nx + 1) * H.Ny * H.Nz + (long long)H.Nx * (H.Ny + 1) * H.Nz + (long long)H.Nx * H.Ny * (H.Nz + 1);
+  ChtVelSrc S = src;
+  S.ctype = C->ctype_dev;
+  k_cht_velocities<<<gfor(nf), kB, 0, C->stream>>>(S, C->ug, C->vg, C->wg);
+  HC_CUDA(cudaGetLastError());
+}
+
+void cht_get_velocities(ChtState *C, double *ug, double *vg, double *wg) {
+  const ChtDev &H = C->H;
+  HC_CUDA(cudaMemcpyAsync(ug, C->ug, (size_t)(H.Nx + 1) * H.Ny * H.Nz * 8, cudaMemcpyDeviceToHost, C->stream));
+  HC_CUDA(cudaMemcpyAsync(vg, C->vg, (size_t)H.Nx * (H.Ny + 1) * H.Nz * 8, cudaMemcpyDeviceToHost, C->stream));
+  HC_CUDA(cudaMemcpyAsync(wg, C->wg, (size_t)H.Nx * H.Ny * (H.Nz + 1) * 8, cudaMemcpyDeviceToHost, C->stream));
+  HC_CUDA(cudaStreamSynchronize(C->stream));
+}
+
+namespace {
+template <class K, class... A>
+void launch_coop(K kernel, int blocks, cudaStream_t s, A... args) {
+  void *argv[] = {(void *)&args...};
+  HC_CUDA(cudaLaunchCooperativeKernel((void *)kernel, dim3(blocks), dim3(kB), argv, 0, s));
+}
+
+void unpad(const ChtDev &H, const double *dev, double *host, cudaStream_t s) {
+  const size_t np = (size_t)(H.Nx + 2) * (H.Ny + 2) * (H.Nz + 2);
+  std::vector<double> tmp(np);
+  HC_CUDA(cudaMemcpyAsync(tmp.data(), dev, np * 8, cudaMemcpyDeviceToHost, s));
+  HC_CUDA(cudaStreamSynchronize(s));
+  for (int k = 0; k < H.Nz; ++k)
+    for (int j = 0; j < H.Ny; ++j)
+      for (int i = 0; i < H.Nx; ++i)
+        host[i + (size_t)H.Nx * (j + (size_t)H.Ny * k)] = tmp[(i + 1) + (H.Nx + 2) * ((j + 1) + (size_t)(H.Ny + 2) * (k + 1))];
+}
+
+double objective(ChtState *C, bool grad) {
+  const ChtDev &H = C->H;
+  const int nb = gfor((long long)H.Nx * H.Ny * H.Nz);
+  k_cht_objective<<<nb, kB, 0, C->stream>>>(H, C->T, C->g, C->partials);
+  std::vector<double> part(nb);
+  HC_CUDA(cudaMemcpyAsync(part.data(), C->partials, nb * 8, cudaMemcpyDeviceToHost, C->stream));
+  HC_CUDA(cudaStreamSynchronize(C->stream));
+  double s = 0;
+  for (double v : part) s += v;
+  const double J = std::pow(s, 1.0 / 8.0);
+  if (grad) k_cht_djdt<<<nb, kB, 0, C->stream>>>(H, C->T, std::pow(J, -7.0), C->g);
+  return J;
+}
+}  // namespace
+
+void cht_forward(ChtState *C, double *T_host, double *J, int *iters, double *relres) {
+  HC_CUDA(cudaSetDevice(C->device));
+  const ChtDev &H = C->H;
+  const size_t np = (size_t)(H.Nx + 2) * (H.Ny + 2) * (H.Nz + 2);
+  k_cht_assemble<<<gfor((long long)H.Nx * H.Ny * H.Nz), kB, 0, C->stream>>>(H, C->Tb);
+  std::vector<double> x0(np, C->Tb);
+  HC_CUDA(cudaMemcpyAsync(C->V.x, x0.data(), np * 8, cudaMemcpyHostToDevice, C->stream));
+  launch_coop(k_cht_bicgstab, C->grid, C->stream, H, C->V, (const double *)H.b, 0, C->tol, C->maxiter, C->partials, C->it,
+              C->res);
+  HC_CUDA(cudaMemcpyAsync(C->T, C->V.x, np * 8, cudaMemcpyDeviceToDevice, C->stream));
+  int it = 0;
+  double rr = 0;
+  HC_CUDA(cudaMemcpyAsync(&it, C->it, 4, cudaMemcpyDeviceToHost, C->stream));
+  HC_CUDA(cudaMemcpyAsync(&rr, C->res, 8, cudaMemcpyDeviceToHost, C->stream));
+  HC_CUDA(cudaStreamSynchronize(C->stream));
+  C->J = objective(C, false);
+  C->have_T = true;
+  if (T_host) unpad(H, C->T, T_host, C->stream);
+  if (J) *J = C->J;
+  if (iters) *iters = it;
+  if (relres) *relres = rr;
+}
+
+void cht_adjoint(ChtState *C, double *dJdq_host, double *dJdk_host, int *iters, double *relres) {
+  HC_CUDA(cudaSetDevice(C->device));
+  if (!C->have_T) throw std::logic_error("adjoint before forward solve");
+  const ChtDev &H = C->H;
+  const size_t np = (size_t)(H.Nx + 2) * (H.Ny + 2) * (H.Nz + 2);
+  const long long n = (long long)H.Nx * H.Ny * H.Nz;
+  objective(C, true);
+  HC_CUDA(cudaMemsetAsync(C->V.x, 0, np * 8, C->stream));
+  launch_coop(k_cht_bicgstab, C->grid, C->stream, H, C->V, (const double *)C->g, 1, C->tol, C->maxiter, C->partials, C->it,
+              C->res);
+  HC_CUDA(cudaMemcpyAsync(C->lam, C->V.x, np * 8, cudaMemcpyDeviceToDevice, C->stream));
+  k_cht_grad<<<gfor(n), kB, 0, C->stream>>>(H, C->T, C->lam, C->Tb, C->dJdq, C->dkc);
+  std::vector<double> dq(n), dk(n);
+  int it = 0;
+  double rr = 0;
+  HC_CUDA(cudaMemcpyAsync(dq.data(), C->dJdq, n * 8, cudaMemcpyDeviceToHost, C->stream));
+  HC_CUDA(cudaMemcpyAsync(dk.data(), C->dkc, n * 8, cudaMemcpyDeviceToHost, C->stream));
+  HC_CUDA(cudaMemcpyAsync(&it, C->it, 4, cudaMemcpyDeviceToHost, C->stream));
+  HC_CUDA(cudaMemcpyAsync(&rr, C->res, 8, cudaMemcpyDeviceToHost, C->stream));
+  HC_CUDA(cudaStreamSynchronize(C->stream));
+  if (dJdq_host) std::copy(dq.begin(), dq.end(), dJdq_host);
+  if (dJdk_host) {
+    for (int r = 0; r < C->nreg; ++r) dJdk_host[r] = 0.0;
+    for (long long c = 0; c < n; ++c)
+      if (C->ctype[c]) dJdk_host[C->region[c]] += dk[c];
+  }
+  if (iters) *iters = it;
+  if (relres) *relres = rr;
+}
+
+}  // namespace hs

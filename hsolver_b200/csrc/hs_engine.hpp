@@ -38,6 +38,7 @@ class Engine {
   void get_solid(int r, int which, double *host, long n);
 
   const Case &kase() const { return case_; }
+  int device() const { return device_; }
   bool inited() const { return inited_; }
 
  private:

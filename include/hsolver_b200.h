@@ -192,6 +192,38 @@ void hs_pcg_destroy(hs_pcg *h);
 int hs_pcg_solve_noalloc(int nx, int ny, int nz, const double *acx, const double *acy, const double *acz,
                          const double *b, double *x, double tol, int maxiter, void *stream, int *iters, double *relres);
 
+/* Conjugate-heat-transfer energy equation and its adjoint (no counterpart in
+ * the reference, whose fluid and solid temperatures meet only through a
+ * ghost-value swap, solver.h:62-148).  One operator over all cells of the
+ * grid: harmonic-mean face conductance G = A/(dP/(2kP) + dN/(2kN)) (so a
+ * fluid-solid face gets the series conductance of its two halves), upwind
+ * convection with the face velocities of the owning solver at the time of
+ * hs_cht_forward (faces touching a solid carry none), volumetric sources q in
+ * solid cells, Dirichlet t_boundary on the domain boundary.  The objective is
+ * J = (sum over solid cells of T^8 dV)^(1/8); hs_cht_adjoint solves the
+ * transposed operator with the same BiCGStab and returns dJ/dq per cell
+ * (zero in fluid) and dJ/dk per solid region. */
+typedef struct hs_cht hs_cht;
+typedef struct hs_cht_params {
+  double k_fluid;     /* fluid conductivity (rho c = 1) */
+  double t_boundary;  /* Dirichlet temperature on the domain boundary */
+  double tol;         /* BiCGStab relative residual */
+  int maxiter;
+  int reserved[5];
+} hs_cht_params;
+void hs_cht_params_default(hs_cht_params *p);
+int hs_cht_create(hs_ctx *ctx, const hs_cht_params *prm, hs_cht **out);
+/* k per solid region (hs_num_solids values) and q per cell (Nx*Ny*Nz, host;
+ * read in solid cells only, NULL = no source). */
+int hs_cht_set_solid(hs_cht *h, const double *k_region, const double *q_cell);
+/* Freeze the solver's current face velocities, solve; T (Nx*Ny*Nz host) and
+ * J optional. */
+int hs_cht_forward(hs_cht *h, double *T, double *J, int *iters, double *relres);
+int hs_cht_adjoint(hs_cht *h, double *dJdq, double *dJdk, int *iters, double *relres);
+/* The frozen face velocities ((Nx+1)NyNz, Nx(Ny+1)Nz, NxNy(Nz+1), host). */
+int hs_cht_velocities(hs_cht *h, double *ug, double *vg, double *wg);
+void hs_cht_destroy(hs_cht *h);
+
 /* Validation of the divisions the sweeps perform with precomputed
  * reciprocals: returns how many of the n host pairs (a[i], b[i]) give a
  * quotient that differs in any bit from IEEE a/b on the current device

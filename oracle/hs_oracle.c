@@ -1101,3 +1101,202 @@ int or_pcg_solve(I64 nx, I64 ny, I64 nz, const double *acx, const double *acy, c
   free(r); free(p); free(s);
   return i;
 }
+
+/* ------------------------------------------------------------------ */
+/* Conjugate-heat-transfer energy equation on the whole grid (fluid and
+ * solid cells) with a frozen flow field, and its adjoint.  This physics has
+ * no counterpart in the reference (its fluid and solid temperatures are
+ * coupled only by a ghost-value swap, solver.h:62-148); the oracle restates
+ * the in-repo discretisation used by the GPU path:
+ *   per face f between cells P, N (areas A, widths dP, dN, conductivities kP, kN)
+ *     G_f = A / (dP/(2 kP) + dN/(2 kN))            harmonic-mean conductance
+ *     F_f = u_f A (outward from P), first-order upwind convection
+ *   boundary faces: Dirichlet Tb through G_b = 2 kP A / dP, upwind inflow of Tb
+ *   row P: (sum_f G_f + max(F_f, 0)) T_P - sum_f (G_f + max(-F_f, 0)) T_N = q_P V_P + boundary terms
+ * Objective J = (sum_solid T^8 V)^(1/8); adjoint A^T lam = dJ/dT;
+ * dJ/dq_P = lam_P V_P; dJ/dk_b = -lam^T (dA/dk_b) T. */
+
+typedef struct {
+  I64 Nx, Ny, Nz;
+  const double *xs, *ys, *zs;      /* grid points */
+  const unsigned char *solid;      /* Nx*Ny*Nz, 1 = solid cell */
+  const int *region;               /* solid region per cell */
+  const double *kcell;             /* conductivity per cell */
+  const double *qcell;             /* volumetric source per cell */
+  const double *ug, *vg, *wg;      /* face velocities (Nx+1)NyNz, Nx(Ny+1)Nz, NxNy(Nz+1) */
+  double Tb;
+} or_cht;
+
+#define CC(i, j, k) ((i) + (j) * H->Nx + (k) * H->Nx * H->Ny)
+
+/* face data of cell c=(i,j,k) toward direction d in 0..5 (W,E,S,N,B,F): G, F (outward), neighbour (-1 = boundary) */
+static void cht_face(const or_cht *H, I64 i, I64 j, I64 k, int d, double *G, double *F, I64 *nb) {
+  double dx = H->xs[i + 1] - H->xs[i], dy = H->ys[j + 1] - H->ys[j], dz = H->zs[k + 1] - H->zs[k];
+  I64 c = CC(i, j, k);
+  double kp = H->kcell[c];
+  double A, dP, dN = 0, kn = 0, u;
+  I64 n = -1;
+  int ax = d / 2, hi = d % 2;
+  if (ax == 0) {
+    A = dy * dz; dP = dx;
+    I64 ii = hi ? i + 1 : i - 1;
+    u = H->ug[(hi ? i + 1 : i) + (H->Nx + 1) * (j + H->Ny * k)];
+    if (ii >= 0 && ii < H->Nx) { n = CC(ii, j, k); dN = H->xs[ii + 1] - H->xs[ii]; }
+  } else if (ax == 1) {
+    A = dx * dz; dP = dy;
+    I64 jj = hi ? j + 1 : j - 1;
+    u = H->vg[i + H->Nx * ((hi ? j + 1 : j) + (H->Ny + 1) * k)];
+    if (jj >= 0 && jj < H->Ny) { n = CC(i, jj, k); dN = H->ys[jj + 1] - H->ys[jj]; }
+  } else {
+    A = dx * dy; dP = dz;
+    I64 kk = hi ? k + 1 : k - 1;
+    u = H->wg[i + H->Nx * (j + H->Ny * (hi ? k + 1 : k))];
+    if (kk >= 0 && kk < H->Nz) { n = CC(i, j, kk); dN = H->zs[kk + 1] - H->zs[kk]; }
+  }
+  if (n >= 0) { kn = H->kcell[n]; *G = A / (dP / (2 * kp) + dN / (2 * kn)); }
+  else *G = 2 * kp * A / dP;
+  *F = (hi ? u : -u) * A;
+  *nb = n;
+}
+
+static void cht_apply(const or_cht *H, const double *x, double *y, int transpose) {
+  for (I64 k = 0; k < H->Nz; ++k) for (I64 j = 0; j < H->Ny; ++j) for (I64 i = 0; i < H->Nx; ++i) {
+    I64 c = CC(i, j, k);
+    double diag = 0, off = 0;
+    for (int d = 0; d < 6; ++d) {
+      double G, F; I64 n;
+      cht_face(H, i, j, k, d, &G, &F, &n);
+      diag += G + maxd(F, 0.0);
+      if (n < 0) continue;
+      /* A_{P,N} = -(G + max(-F,0)); A^T_{P,N} = A_{N,P} = -(G + max(F,0)) */
+      off += (G + (transpose ? maxd(F, 0.0) : maxd(-F, 0.0))) * x[n];
+    }
+    y[c] = diag * x[c] - off;
+  }
+}
+
+static void cht_rhs(const or_cht *H, double *b) {
+  for (I64 k = 0; k < H->Nz; ++k) for (I64 j = 0; j < H->Ny; ++j) for (I64 i = 0; i < H->Nx; ++i) {
+    I64 c = CC(i, j, k);
+    double V = (H->xs[i + 1] - H->xs[i]) * (H->ys[j + 1] - H->ys[j]) * (H->zs[k + 1] - H->zs[k]);
+    double s = H->qcell[c] * V;
+    for (int d = 0; d < 6; ++d) {
+      double G, F; I64 n;
+      cht_face(H, i, j, k, d, &G, &F, &n);
+      if (n >= 0) continue;
+      s += (G + maxd(-F, 0.0)) * H->Tb;
+    }
+    b[c] = s;
+  }
+}
+
+static double cht_diag(const or_cht *H, I64 i, I64 j, I64 k) {
+  double diag = 0;
+  for (int d = 0; d < 6; ++d) { double G, F; I64 n; cht_face(H, i, j, k, d, &G, &F, &n); diag += G + maxd(F, 0.0); }
+  return diag;
+}
+
+/* Jacobi-preconditioned BiCGStab (van der Vorst 1992) on A or A^T. */
+static int cht_bicgstab(const or_cht *H, int transpose, const double *b, double *x, double tol, int maxiter, double *relres) {
+  I64 N = H->Nx * H->Ny * H->Nz;
+  double *r = malloc(8 * N), *rh = malloc(8 * N), *p = calloc(N, 8), *v = calloc(N, 8), *ph = malloc(8 * N);
+  double *s = malloc(8 * N), *sh = malloc(8 * N), *t = malloc(8 * N), *dinv = malloc(8 * N);
+  for (I64 k = 0; k < H->Nz; ++k) for (I64 j = 0; j < H->Ny; ++j) for (I64 i = 0; i < H->Nx; ++i) dinv[CC(i, j, k)] = 1.0 / cht_diag(H, i, j, k);
+  cht_apply(H, x, r, transpose);
+  double bb = 0;
+  for (I64 c = 0; c < N; ++c) { r[c] = b[c] - r[c]; rh[c] = r[c]; bb += b[c] * b[c]; }
+  double rho = 1, alpha = 1, omega = 1, rr = 0;
+  int it = 0;
+  for (I64 c = 0; c < N; ++c) rr += r[c] * r[c];
+  if (bb == 0) bb = 1;
+  while (it < maxiter && rr / bb >= tol * tol) {
+    it++;
+    double rho1 = 0;
+    for (I64 c = 0; c < N; ++c) rho1 += rh[c] * r[c];
+    double beta = (rho1 / rho) * (alpha / omega);
+    for (I64 c = 0; c < N; ++c) { p[c] = r[c] + beta * (p[c] - omega * v[c]); ph[c] = p[c] * dinv[c]; }
+    cht_apply(H, ph, v, transpose);
+    double rv = 0;
+    for (I64 c = 0; c < N; ++c) rv += rh[c] * v[c];
+    alpha = rho1 / rv;
+    double ss = 0;
+    for (I64 c = 0; c < N; ++c) { s[c] = r[c] - alpha * v[c]; sh[c] = s[c] * dinv[c]; ss += s[c] * s[c]; }
+    if (ss / bb < tol * tol) { for (I64 c = 0; c < N; ++c) x[c] += alpha * ph[c]; rr = ss; break; }
+    cht_apply(H, sh, t, transpose);
+    double ts = 0, tt = 0;
+    for (I64 c = 0; c < N; ++c) { ts += t[c] * s[c]; tt += t[c] * t[c]; }
+    omega = ts / tt;
+    rr = 0;
+    for (I64 c = 0; c < N; ++c) { x[c] += alpha * ph[c] + omega * sh[c]; r[c] = s[c] - omega * t[c]; rr += r[c] * r[c]; }
+    rho = rho1;
+  }
+  if (relres) *relres = sqrt(rr / bb);
+  free(r); free(rh); free(p); free(v); free(ph); free(s); free(sh); free(t); free(dinv);
+  return it;
+}
+
+static double cht_objective(const or_cht *H, const double *T, double *dJdT) {
+  double sum = 0;
+  I64 N = H->Nx * H->Ny * H->Nz;
+  for (I64 k = 0; k < H->Nz; ++k) for (I64 j = 0; j < H->Ny; ++j) for (I64 i = 0; i < H->Nx; ++i) {
+    I64 c = CC(i, j, k);
+    if (!H->solid[c]) continue;
+    double V = (H->xs[i + 1] - H->xs[i]) * (H->ys[j + 1] - H->ys[j]) * (H->zs[k + 1] - H->zs[k]);
+    double t2 = T[c] * T[c], t4 = t2 * t2;
+    sum += t4 * t4 * V;
+  }
+  double J = pow(sum, 1.0 / 8.0);
+  if (dJdT) {
+    for (I64 c = 0; c < N; ++c) dJdT[c] = 0;
+    double f = pow(J, -7.0);
+    for (I64 k = 0; k < H->Nz; ++k) for (I64 j = 0; j < H->Ny; ++j) for (I64 i = 0; i < H->Nx; ++i) {
+      I64 c = CC(i, j, k);
+      if (!H->solid[c]) continue;
+      double V = (H->xs[i + 1] - H->xs[i]) * (H->ys[j + 1] - H->ys[j]) * (H->zs[k + 1] - H->zs[k]);
+      double t = T[c], t2 = t * t, t3 = t2 * t, t7 = t3 * t3 * t;
+      dJdT[c] = f * t7 * V;
+    }
+  }
+  return J;
+}
+
+int or_cht_forward(const or_cht *H, double *T, double tol, int maxiter, double *J, double *relres) {
+  I64 N = H->Nx * H->Ny * H->Nz;
+  double *b = malloc(8 * N);
+  cht_rhs(H, b);
+  for (I64 c = 0; c < N; ++c) T[c] = H->Tb;
+  int it = cht_bicgstab(H, 0, b, T, tol, maxiter, relres);
+  if (J) *J = cht_objective(H, T, NULL);
+  free(b);
+  return it;
+}
+
+/* lam solves A^T lam = dJ/dT; dJdq per cell (zero off solid); dJdk per solid region */
+int or_cht_adjoint(const or_cht *H, const double *T, double *lam, double *dJdq, double *dJdk, int nreg, double tol, int maxiter,
+                   double *relres) {
+  I64 N = H->Nx * H->Ny * H->Nz;
+  double *g = malloc(8 * N);
+  cht_objective(H, T, g);
+  for (I64 c = 0; c < N; ++c) lam[c] = 0;
+  int it = cht_bicgstab(H, 1, g, lam, tol, maxiter, relres);
+  for (int r = 0; r < nreg; ++r) dJdk[r] = 0;
+  for (I64 k = 0; k < H->Nz; ++k) for (I64 j = 0; j < H->Ny; ++j) for (I64 i = 0; i < H->Nx; ++i) {
+    I64 c = CC(i, j, k);
+    double dx = H->xs[i + 1] - H->xs[i], dy = H->ys[j + 1] - H->ys[j], dz = H->zs[k + 1] - H->zs[k];
+    dJdq[c] = H->solid[c] ? lam[c] * dx * dy * dz : 0.0;
+    if (!H->solid[c]) continue;
+    double kp = H->kcell[c];
+    /* dR/dk_P over the faces of P: face residual G (T_P - T_N) on row P and G (T_N - T_P) on row N */
+    for (int d = 0; d < 6; ++d) {
+      double G, F; I64 n;
+      cht_face(H, i, j, k, d, &G, &F, &n);
+      int ax = d / 2;
+      double A = ax == 0 ? dy * dz : ax == 1 ? dx * dz : dx * dy, dP = ax == 0 ? dx : ax == 1 ? dy : dz;
+      double dG = (n >= 0) ? G * G * dP / (2 * A * kp * kp) : G / kp;
+      double tn = n >= 0 ? T[n] : H->Tb, ln = n >= 0 ? lam[n] : 0.0;
+      dJdk[H->region[c]] -= dG * (lam[c] - ln) * (T[c] - tn);
+    }
+  }
+  free(g);
+  return it;
+}

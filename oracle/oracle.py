@@ -207,3 +207,40 @@ def pcg_solve(nx, ny, nz, acx, acy, acz, b, tol=1e-5, maxiter=1000):
     it = L.or_pcg_solve(nx, ny, nz, *[a.ctypes.data_as(dp) for a in arrs], x.ctypes.data_as(dp), tol, maxiter,
                         ctypes.byref(rr))
     return x, it, rr.value
+
+
+class _Cht(ctypes.Structure):
+    _fields_ = [("Nx", ctypes.c_int64), ("Ny", ctypes.c_int64), ("Nz", ctypes.c_int64),
+                ("xs", ctypes.c_void_p), ("ys", ctypes.c_void_p), ("zs", ctypes.c_void_p),
+                ("solid", ctypes.c_void_p), ("region", ctypes.c_void_p), ("kcell", ctypes.c_void_p),
+                ("qcell", ctypes.c_void_p), ("ug", ctypes.c_void_p), ("vg", ctypes.c_void_p), ("wg", ctypes.c_void_p),
+                ("Tb", ctypes.c_double)]
+
+
+def cht_solve(xs, ys, zs, ctype, region, kcell, qcell, ug, vg, wg, Tb=293.0, tol=1e-13, maxiter=20000, nreg=0):
+    """Oracle forward + adjoint of the monolithic conjugate-heat-transfer
+    energy equation (hs_oracle.c: or_cht_forward / or_cht_adjoint).
+    Returns dict(T, J, dJdq, dJdk, iters)."""
+    L = lib()
+    keep = [np.ascontiguousarray(a, dt) for a, dt in [(xs, np.float64), (ys, np.float64), (zs, np.float64),
+                                                      (ctype, np.uint8), (region, np.int32), (kcell, np.float64),
+                                                      (qcell, np.float64), (ug, np.float64), (vg, np.float64),
+                                                      (wg, np.float64)]]
+    Nx, Ny, Nz = len(xs) - 1, len(ys) - 1, len(zs) - 1
+    H = _Cht(Nx, Ny, Nz, *[a.ctypes.data for a in keep], Tb)
+    dp = ctypes.POINTER(ctypes.c_double)
+    L.or_cht_forward.restype = ctypes.c_int
+    L.or_cht_forward.argtypes = [ctypes.POINTER(_Cht), dp, ctypes.c_double, ctypes.c_int, dp, dp]
+    L.or_cht_adjoint.restype = ctypes.c_int
+    L.or_cht_adjoint.argtypes = [ctypes.POINTER(_Cht), dp, dp, dp, dp, ctypes.c_int, ctypes.c_double, ctypes.c_int, dp]
+    N = Nx * Ny * Nz
+    T = np.empty(N)
+    J = ctypes.c_double()
+    rr = ctypes.c_double()
+    it1 = L.or_cht_forward(ctypes.byref(H), T.ctypes.data_as(dp), tol, maxiter, ctypes.byref(J), ctypes.byref(rr))
+    lam = np.empty(N)
+    dJdq = np.empty(N)
+    dJdk = np.zeros(max(nreg, 1))
+    it2 = L.or_cht_adjoint(ctypes.byref(H), T.ctypes.data_as(dp), lam.ctypes.data_as(dp), dJdq.ctypes.data_as(dp),
+                           dJdk.ctypes.data_as(dp), nreg, tol, maxiter, ctypes.byref(rr))
+    return {"T": T, "J": J.value, "dJdq": dJdq, "dJdk": dJdk[:nreg], "iters": (it1, it2)}
