@@ -18,10 +18,14 @@ LIB_PATH = os.path.join(_HERE, "libhsolver_b200.so")
 
 HS_OK = 0
 ERRORS = {-1: "HS_ERR_ARG", -2: "HS_ERR_DECK", -3: "HS_ERR_UNSUPPORTED", -4: "HS_ERR_CUDA", -5: "HS_ERR_NOMEM",
-          -6: "HS_ERR_STATE", -7: "HS_ERR_DIVERGED", -8: "HS_ERR_INTERNAL"}
+          -6: "HS_ERR_STATE", -7: "HS_ERR_DIVERGED", -8: "HS_ERR_INTERNAL", -9: "HS_ERR_MAXITER"}
 FIELDS = {"u_star": 0, "v_star": 1, "w_star": 2, "p_temp": 3, "t_temp": 4, "up": 5, "vp": 6, "wp": 7,
           "ux": 8, "uy": 9, "uz": 10, "p": 11, "t": 12, "p_prime": 13}
 PSOLVE_CG, PSOLVE_MGCG = 0, 1
+PREC_FP64, PREC_MIXED = 0, 1
+CH_SKIP_PRESSURE, CH_SKIP_ENERGY = 1, 2
+CH_FIELDS = {"u": 0, "v": 1, "w": 2, "p": 3, "T": 4, "u_star": 5, "v_star": 6, "w_star": 7, "d_u": 8, "d_v": 9,
+             "d_w": 10, "p_prime": 11}
 
 
 class HsError(RuntimeError):
@@ -307,3 +311,169 @@ class Case:
         out = np.empty(3 * n, np.float64)
         assert self._L.hs_case_geometry(self.h, axis, _dptr(out), 3 * n) == HS_OK
         return out.reshape(3, n)
+
+
+class ChannelParams(ctypes.Structure):
+    """hs_channel_params (include/hsolver_b200.h)."""
+    _fields_ = [("re", ctypes.c_double), ("pr", ctypes.c_double), ("u_in", ctypes.c_double), ("t_in", ctypes.c_double),
+                ("alpha_u", ctypes.c_double), ("alpha_p", ctypes.c_double), ("alpha_t", ctypes.c_double),
+                ("mom_sweeps", ctypes.c_int), ("p_tol", ctypes.c_double), ("p_maxiter", ctypes.c_int),
+                ("t_tol", ctypes.c_double), ("t_maxiter", ctypes.c_int), ("precision", ctypes.c_int),
+                ("p_precond", ctypes.c_int), ("reserved", ctypes.c_double * 6)]
+
+
+class ChannelStats(ctypes.Structure):
+    _fields_ = [("res", ctypes.c_double * 5), ("norm", ctypes.c_double * 5), ("global_", ctypes.c_double),
+                ("iter", ctypes.c_int), ("pcg_iters", ctypes.c_int), ("t_iters", ctypes.c_int),
+                ("pcg_relres", ctypes.c_double), ("t_relres", ctypes.c_double)]
+
+    def as_dict(self):
+        return {"res": list(self.res), "norm": list(self.norm), "global": self.global_, "iter": self.iter,
+                "pcg_iters": self.pcg_iters, "t_iters": self.t_iters, "pcg_relres": self.pcg_relres,
+                "t_relres": self.t_relres}
+
+
+class AdjointInfo(ctypes.Structure):
+    _fields_ = [("fwd_iters", ctypes.c_int), ("adj_iters", ctypes.c_int), ("fwd_ms", ctypes.c_double),
+                ("adj_ms", ctypes.c_double)]
+
+
+def _channel_api(L):
+    if getattr(L, "_channel_ready", False):
+        return
+    vp, ll = ctypes.c_void_p, ctypes.c_longlong
+    dp = ctypes.POINTER(ctypes.c_double)
+    sig = {
+        "hs_channel_params_default": ([ctypes.POINTER(ChannelParams)], None),
+        "hs_channel_create": ([ctypes.c_char_p, ctypes.POINTER(ChannelParams), ctypes.c_int, ctypes.POINTER(vp)], ctypes.c_int),
+        "hs_channel_num_blocks": ([vp, ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
+        "hs_channel_set_solid": ([vp, dp, ctypes.c_int, dp, ll], ctypes.c_int),
+        "hs_channel_init": ([vp], ctypes.c_int),
+        "hs_channel_step": ([vp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ChannelStats)], ctypes.c_int),
+        "hs_channel_solve_to": ([vp, ctypes.c_double, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                 ctypes.POINTER(ChannelStats)], ctypes.c_int),
+        "hs_channel_field_size": ([vp, ctypes.c_int, ctypes.POINTER(ll)], ctypes.c_int),
+        "hs_channel_get_field": ([vp, ctypes.c_int, dp, ll], ctypes.c_int),
+        "hs_channel_set_field": ([vp, ctypes.c_int, dp, ll], ctypes.c_int),
+        "hs_channel_stream": ([vp, ctypes.POINTER(vp)], ctypes.c_int),
+        "hs_channel_sync": ([vp], ctypes.c_int),
+        "hs_channel_device_bytes": ([vp, ctypes.POINTER(ll)], ctypes.c_int),
+        "hs_channel_adjoint": ([vp, ctypes.c_double, ctypes.c_int, dp, dp, ll, dp, ctypes.c_int,
+                                ctypes.POINTER(AdjointInfo)], ctypes.c_int),
+        "hs_channel_destroy": ([vp], None),
+    }
+    for name, (args, res) in sig.items():
+        fn = getattr(L, name)
+        fn.argtypes = args
+        fn.restype = res
+    L._channel_ready = True
+
+
+def channel_params(**over):
+    L = load()
+    _channel_api(L)
+    p = ChannelParams()
+    L.hs_channel_params_default(ctypes.byref(p))
+    for k, v in over.items():
+        setattr(p, k, v)
+    return p
+
+
+class Channel:
+    """Channel conjugate-heat-transfer case on one GPU (hs_channel_*): inlet
+    plug flow, zero-gradient outlet, the deck's mobs boxes as heated solid
+    blocks; SIMPLE outer steps until a global residual tolerance."""
+
+    def __init__(self, deck_text, params=None, device=0, **over):
+        L = load()
+        _channel_api(L)
+        self._L = L
+        self.h = None
+        p = params if params is not None else channel_params(**over)
+        h = ctypes.c_void_p()
+        rc = L.hs_channel_create(deck_text.encode() if isinstance(deck_text, str) else deck_text, ctypes.byref(p), device,
+                                 ctypes.byref(h))
+        if rc != HS_OK:
+            raise HsError(rc, L.hs_last_error(None).decode())
+        self.h = h
+        self.params = p
+        n = ctypes.c_int()
+        self._check(L.hs_channel_num_blocks(h, ctypes.byref(n)))
+        self.nblocks = n.value
+        self.ncell = self.field_size("p")
+
+    def _check(self, rc):
+        if rc < 0:
+            raise HsError(rc, self._L.hs_last_error(None).decode())
+        return rc
+
+    def close(self):
+        if self.h:
+            self._L.hs_channel_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_solid(self, k_ratio, q_cell):
+        k = np.ascontiguousarray(k_ratio, np.float64)
+        q = np.ascontiguousarray(q_cell, np.float64)
+        self._check(self._L.hs_channel_set_solid(self.h, _dptr(k), k.size, _dptr(q), q.size))
+
+    def init(self):
+        self._check(self._L.hs_channel_init(self.h))
+
+    def step(self, n=1, flags=0):
+        st = ChannelStats()
+        self._check(self._L.hs_channel_step(self.h, n, flags, ctypes.byref(st)))
+        return st.as_dict()
+
+    def solve_to(self, tol=1e-6, max_outer=500):
+        """Outer steps until the global residual <= tol; returns (converged, steps, stats)."""
+        st = ChannelStats()
+        steps = ctypes.c_int()
+        rc = self._L.hs_channel_solve_to(self.h, tol, max_outer, ctypes.byref(steps), ctypes.byref(st))
+        if rc < 0 and rc != -9:
+            self._check(rc)
+        return rc == HS_OK, steps.value, st.as_dict()
+
+    def field_size(self, name):
+        n = ctypes.c_longlong()
+        self._check(self._L.hs_channel_field_size(self.h, CH_FIELDS[name], ctypes.byref(n)))
+        return n.value
+
+    def field(self, name, out=None):
+        n = self.field_size(name)
+        out = np.empty(n, np.float64) if out is None else out
+        self._check(self._L.hs_channel_get_field(self.h, CH_FIELDS[name], _dptr(out), n))
+        return out
+
+    def set_field(self, name, arr):
+        arr = np.ascontiguousarray(arr, np.float64)
+        self._check(self._L.hs_channel_set_field(self.h, CH_FIELDS[name], _dptr(arr), arr.size))
+
+    def stream(self):
+        p = ctypes.c_void_p()
+        self._check(self._L.hs_channel_stream(self.h, ctypes.byref(p)))
+        return p.value
+
+    def sync(self):
+        self._check(self._L.hs_channel_sync(self.h))
+
+    def device_bytes(self):
+        b = ctypes.c_longlong()
+        self._check(self._L.hs_channel_device_bytes(self.h, ctypes.byref(b)))
+        return b.value
+
+    def adjoint(self, tol=1e-10, maxiter=20000):
+        """Energy forward + adjoint on the current flow: (J, dJdq per cell, dJdk per block, info dict)."""
+        J = ctypes.c_double()
+        dq = np.empty(self.ncell)
+        dk = np.empty(max(self.nblocks, 1))
+        info = AdjointInfo()
+        self._check(self._L.hs_channel_adjoint(self.h, tol, maxiter, ctypes.byref(J), _dptr(dq), dq.size, _dptr(dk),
+                                               self.nblocks, ctypes.byref(info)))
+        return J.value, dq, dk[:self.nblocks], {k: getattr(info, k) for k, _ in AdjointInfo._fields_}

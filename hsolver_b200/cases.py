@@ -114,3 +114,29 @@ def config5(seed=0):
 
 
 CONFIGS = {"config1": config1, "config2": config2, "config3": config3, "config4": config4, "config5": config5}
+
+
+# Physics of the seeded configurations: Reynolds number and per-block
+# conductivity ratio / heat-source ranges.
+PHYSICS = {
+    "config1": {"re": 100.0, "k": (100.0, 100.0), "q": (1.0, 1.0)},
+    "config2": {"re": 400.0, "k": (10.0, 1000.0), "q": (0.5, 2.0)},
+    "config3": {"re": 100.0, "k": (100.0, 100.0), "q": (1.0, 1.0)},
+    "config4": {"re": 400.0, "k": (10.0, 1000.0), "q": (0.5, 2.0)},
+    "config5": {"re": 1000.0, "k": (10.0, 1000.0), "q": (0.1, 5.0)},
+}
+
+
+def block_physics(name, ctype, region, seed=0):
+    """(re, k_ratio per solid region, q per cell) for a configuration: one
+    uniform draw per block (regions in the order of their lowest cell index),
+    q constant inside each block and zero in the fluid."""
+    ph = PHYSICS[name]
+    ctype = np.asarray(ctype)
+    region = np.asarray(region)
+    nreg = int(region[ctype == 1].max()) + 1 if np.any(ctype == 1) else 0
+    rng = np.random.default_rng(1000 + seed)
+    k = rng.uniform(ph["k"][0], ph["k"][1], nreg)
+    qb = rng.uniform(ph["q"][0], ph["q"][1], nreg)
+    q = np.where(ctype == 1, qb[np.maximum(region, 0)], 0.0)
+    return ph["re"], k, q

@@ -8,6 +8,7 @@
 
 #include "../../include/hsolver_b200.h"
 #include "hs_case.hpp"
+#include "hs_channel.hpp"
 #include "hs_cht.hpp"
 #include "hs_engine.hpp"
 
@@ -22,6 +23,12 @@ struct hs_case {
 
 struct hs_pcg {
   hs::PcgWork *w = nullptr;
+};
+
+struct hs_channel {
+  hs::ChannelState *st = nullptr;
+  int nreg = 0;
+  long long ncell = 0;
 };
 
 struct hs_cht {
@@ -59,6 +66,33 @@ int guarded(hs_ctx *ctx, Fn fn) {
   } catch (const std::exception &e) {
     return fail(ctx, classify(e), e.what());
   }
+}
+}  // namespace
+
+namespace {
+template <class Fn>
+int ch_guarded(hs_channel *h, Fn fn) {
+  if (!h || !h->st) return fail(nullptr, HS_ERR_ARG, "null channel handle");
+  try {
+    return fn(*h);
+  } catch (const std::bad_alloc &) {
+    return fail(nullptr, HS_ERR_NOMEM, "host allocation failed");
+  } catch (const std::exception &e) {
+    return fail(nullptr, classify(e), e.what());
+  }
+}
+
+void ch_copy_stats(const hs::ChStats &a, hs_channel_stats *b) {
+  if (!b) return;
+  for (int x = 0; x < 5; ++x) { b->res[x] = a.res[x]; b->norm[x] = a.norm[x]; }
+  b->global = a.global; b->iter = a.iter; b->pcg_iters = a.pcg_iters; b->t_iters = a.t_iters;
+  b->pcg_relres = a.pcg_relres; b->t_relres = a.t_relres;
+}
+
+bool ch_finite(const hs::ChStats &a) {
+  for (int x = 0; x < 5; ++x)
+    if (!(a.res[x] == a.res[x]) || a.res[x] > 1e300) return false;
+  return true;
 }
 }  // namespace
 
@@ -404,7 +438,7 @@ int hs_cht_create(hs_ctx *ctx, const hs_cht_params *prm, hs_cht **out) {
     std::vector<int> reg(c.region.size());
     for (size_t i = 0; i < reg.size(); ++i) reg[i] = c.ctype[i] ? c.region[i] : -1;
     S.region = reg.data();
-    S.t_boundary = p.t_boundary; S.tol = p.tol; S.maxiter = p.maxiter;
+    S.t_boundary = p.t_boundary; S.tol = p.tol; S.maxiter = p.maxiter; S.bc = 0;
     hs_cht *h = new hs_cht();
     h->ctx = ctx;
     h->k_fluid = p.k_fluid;
@@ -468,6 +502,144 @@ int hs_cht_velocities(hs_cht *h, double *ug, double *vg, double *wg) {
 void hs_cht_destroy(hs_cht *h) {
   if (!h) return;
   hs::cht_destroy(h->st);
+  delete h;
+}
+
+void hs_channel_params_default(hs_channel_params *p) {
+  if (!p) return;
+  std::memset(p, 0, sizeof(*p));
+  p->re = 100; p->pr = 0.71; p->u_in = 1.0; p->t_in = 0.0;
+  p->alpha_u = 0.7; p->alpha_p = 0.3; p->alpha_t = 0.9;
+  p->mom_sweeps = 2; p->p_tol = 1e-8; p->p_maxiter = 1000; p->t_tol = 1e-2; p->t_maxiter = 200;
+  p->precision = HS_PREC_FP64; p->p_precond = 1;
+}
+
+
+int hs_channel_create(const char *deck, const hs_channel_params *prm, int device, hs_channel **out) {
+  if (!deck || !out) return fail(nullptr, HS_ERR_ARG, "null deck or output pointer");
+  *out = nullptr;
+  hs_channel_params p;
+  if (prm) p = *prm; else hs_channel_params_default(&p);
+  std::string err;
+  hs::Deck d;
+  if (!hs::parse_deck(deck, d, err)) return fail(nullptr, HS_ERR_DECK, err);
+  hs::Case c;
+  if (!hs::build_case(d, c, err)) return fail(nullptr, err.rfind("deck", 0) == 0 ? HS_ERR_DECK : HS_ERR_UNSUPPORTED, err);
+  hs::ChParams q;
+  q.re = p.re; q.pr = p.pr; q.u_in = p.u_in; q.t_in = p.t_in;
+  q.alpha_u = p.alpha_u; q.alpha_p = p.alpha_p; q.alpha_t = p.alpha_t;
+  q.mom_sweeps = p.mom_sweeps; q.p_tol = p.p_tol; q.p_maxiter = p.p_maxiter; q.t_tol = p.t_tol; q.t_maxiter = p.t_maxiter;
+  q.precision = p.precision; q.p_precond = p.p_precond;
+  hs_channel *h = new (std::nothrow) hs_channel();
+  if (!h) return fail(nullptr, HS_ERR_NOMEM, "host allocation failed");
+  try {
+    h->st = hs::ch_create(c, q, device);
+  } catch (const std::exception &e) {
+    int code = classify(e);
+    std::string m = e.what();
+    delete h;
+    return fail(nullptr, code, m);
+  }
+  h->nreg = hs::ch_nreg(h->st);
+  h->ncell = (long long)c.Nx * c.Ny * c.Nz;
+  *out = h;
+  return HS_OK;
+}
+
+int hs_channel_num_blocks(hs_channel *h, int *n) {
+  if (!n) return fail(nullptr, HS_ERR_ARG, "null output pointer");
+  return ch_guarded(h, [&](hs_channel &c) { *n = c.nreg; return HS_OK; });
+}
+
+int hs_channel_set_solid(hs_channel *h, const double *k_ratio, int n_blocks, const double *q_cell, long long n) {
+  return ch_guarded(h, [&](hs_channel &c) {
+    if (!k_ratio || !q_cell || n_blocks != c.nreg || n != c.ncell) throw std::invalid_argument("set_solid: sizes");
+    hs::ch_set_solid(c.st, k_ratio, q_cell);
+    return HS_OK;
+  });
+}
+
+int hs_channel_init(hs_channel *h) {
+  return ch_guarded(h, [&](hs_channel &c) { hs::ch_init(c.st); return HS_OK; });
+}
+
+int hs_channel_step(hs_channel *h, int n, int flags, hs_channel_stats *stats) {
+  if (n < 0 || (flags & ~3)) return fail(nullptr, HS_ERR_ARG, "bad step count or flags");
+  return ch_guarded(h, [&](hs_channel &c) {
+    hs::ChStats st{};
+    hs::ch_step(c.st, n, flags, &st);
+    ch_copy_stats(st, stats);
+    if (n > 0 && !ch_finite(st)) return fail(nullptr, HS_ERR_DIVERGED, "non-finite residual");
+    return HS_OK;
+  });
+}
+
+int hs_channel_solve_to(hs_channel *h, double tol, int max_outer, int *steps, hs_channel_stats *stats) {
+  if (!(tol > 0) || max_outer < 0) return fail(nullptr, HS_ERR_ARG, "bad tolerance or step limit");
+  return ch_guarded(h, [&](hs_channel &c) {
+    hs::ChStats st{};
+    const int s = hs::ch_solve_to(c.st, tol, max_outer, &st);
+    if (steps) *steps = s;
+    ch_copy_stats(st, stats);
+    if (s > 0 && !ch_finite(st)) return fail(nullptr, HS_ERR_DIVERGED, "non-finite residual");
+    if (!(st.iter > 5 && st.global <= tol)) return fail(nullptr, HS_ERR_MAXITER, "global residual above tolerance");
+    return HS_OK;
+  });
+}
+
+int hs_channel_field_size(hs_channel *h, int field, long long *n) {
+  if (!n) return fail(nullptr, HS_ERR_ARG, "null output pointer");
+  return ch_guarded(h, [&](hs_channel &c) {
+    const long v = hs::ch_field_size(c.st, field);
+    if (v < 0) throw std::invalid_argument("unknown field");
+    *n = v;
+    return HS_OK;
+  });
+}
+
+int hs_channel_get_field(hs_channel *h, int field, double *host, long long n) {
+  if (!host) return fail(nullptr, HS_ERR_ARG, "null buffer");
+  return ch_guarded(h, [&](hs_channel &c) { hs::ch_get_field(c.st, field, host, (long)n); return HS_OK; });
+}
+
+int hs_channel_set_field(hs_channel *h, int field, const double *host, long long n) {
+  if (!host) return fail(nullptr, HS_ERR_ARG, "null buffer");
+  return ch_guarded(h, [&](hs_channel &c) { hs::ch_set_field(c.st, field, host, (long)n); return HS_OK; });
+}
+
+int hs_channel_stream(hs_channel *h, void **stream) {
+  if (!stream) return fail(nullptr, HS_ERR_ARG, "null output pointer");
+  return ch_guarded(h, [&](hs_channel &c) { *stream = hs::ch_stream(c.st); return HS_OK; });
+}
+
+int hs_channel_sync(hs_channel *h) {
+  return ch_guarded(h, [&](hs_channel &c) { hs::ch_sync(c.st); return HS_OK; });
+}
+
+int hs_channel_device_bytes(hs_channel *h, long long *bytes) {
+  if (!bytes) return fail(nullptr, HS_ERR_ARG, "null output pointer");
+  return ch_guarded(h, [&](hs_channel &c) { *bytes = hs::ch_device_bytes(c.st); return HS_OK; });
+}
+
+int hs_channel_adjoint(hs_channel *h, double tol, int maxiter, double *J, double *dJdq, long long n, double *dJdk,
+                       int n_blocks, hs_adjoint_info *info) {
+  if (!(tol > 0) || maxiter < 1) return fail(nullptr, HS_ERR_ARG, "bad tolerance or iteration limit");
+  return ch_guarded(h, [&](hs_channel &c) {
+    if ((dJdq && n != c.ncell) || (dJdk && n_blocks != c.nreg)) throw std::invalid_argument("adjoint: sizes");
+    int fi = 0, ai = 0;
+    double fm = 0, am = 0;
+    hs::ch_adjoint(c.st, tol, maxiter, J, dJdq, dJdk, &fi, &ai, &fm, &am);
+    if (info) { info->fwd_iters = fi; info->adj_iters = ai; info->fwd_ms = fm; info->adj_ms = am; }
+    return HS_OK;
+  });
+}
+
+void hs_channel_destroy(hs_channel *h) {
+  if (!h) return;
+  try {
+    hs::ch_destroy(h->st);
+  } catch (...) {
+  }
   delete h;
 }
 

@@ -1,0 +1,1215 @@
+// Channel conjugate-heat-transfer SIMPLE solver on the GPU.
+//
+// The reference solves a lid-driven cavity only; this is the extended
+// physics of the build (inlet, outlet, heat source, conductivity ratio,
+// global residual), with the reference's differencing scheme (first-order
+// upwind a_nb = D + max(-+F, 0), a_P = sum a_nb, fluid_solver.h:577-659) kept.
+//
+//   faces of axis a, index c = (i,j,k), c_a in [0, N_a] (x-fastest, unpadded):
+//     c_a = 0      x: inlet (u = u_in over fluid cells); y, z: wall (0)
+//     c_a = N_a    x: outlet, u = u*(N_x - 1) + d p'(N_x - 1); y, z: wall (0)
+//     otherwise    unknown when both cells are fluid, else 0
+//   momentum at an unknown face, coefficients frozen at u^n, Patankar relaxation:
+//     (a_P/alpha_u) u_P = sum a_nb u_nb + (p_lo - p_hi) A + (1 - alpha_u)(a_P/alpha_u) u^n_P
+//     stencil order E W N S T B; the outlet neighbour is zero-gradient (dropped),
+//     a wall or inlet neighbour is 0 at half a cell; d = A / (a_P/alpha_u)
+//   red-black Gauss-Seidel on the face colour (i+j+k)&1: one pass per colour,
+//   all three components in one launch (they only read each other's u^n)
+//   p': couplings A d per face (A d(N_x - 1) at the outlet, p' = 0 outside),
+//     b = mass imbalance of u* (u*(N_x) := u*(N_x - 1)); SPD, CG preconditioned
+//     by a geometric multigrid V-cycle
+//   correction u = u* + d (p'_lo - p'_hi), p += alpha_p p'
+//   energy: the conjugate-heat-transfer operator of hs_cht.cu (bc = 1) with a
+//     warm-started BiCGStab and relaxation alpha_t
+// Every point update is written in the operation order of the CPU oracle, with
+// FMA contraction off, so the FP64 form reproduces it bit for bit; sums of
+// residuals and dot products are per-block partials reduced in a fixed order.
+//
+// Precision: R = double (plain form) or float (mixed form: fields, sweeps and
+// the V-cycle in FP32; residuals, the CG recurrences, dot products, mass
+// imbalance and the coarsest-grid solve in FP64).
+#include <cooperative_groups.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "hs_channel.hpp"
+#include "hs_cht.hpp"
+
+namespace cg = cooperative_groups;
+
+namespace hs {
+
+#define CH_CUDA(call)                                                                              \
+  do {                                                                                             \
+    cudaError_t e_ = (call);                                                                       \
+    if (e_ != cudaSuccess) throw std::runtime_error(std::string("CUDA: ") + cudaGetErrorString(e_) + \
+                                                    " at " #call);                                 \
+  } while (0)
+
+namespace {
+
+constexpr int kT = 256;
+constexpr int kMaxLv = 16;
+constexpr int kMaxCoarse = 64;
+
+template <class R>
+struct ChDev {
+  int N0, N1, N2;
+  const R *d0, *d1, *d2;      // cell widths
+  const R *h0, *h1, *h2;      // centre distances, [0] and [N] half widths
+  const uint8_t *solid;       // N0 N1 N2
+  R *U0, *U1, *U2;            // u^n (after correction: the new iterate)
+  R *S0, *S1, *S2;            // u*
+  R *D0, *D1, *D2;            // d = A / (a_P / alpha_u)
+  R *p;                       // pressure, cells
+  double *Ud0, *Ud1, *Ud2;    // FP64 copy of the corrected velocities (mixed form), energy input
+  R nu, au, u_in;
+  double ap;                  // alpha_p
+};
+
+template <int A, class R> __device__ __forceinline__ R *Uarr(const ChDev<R> &H) { return A == 0 ? H.U0 : A == 1 ? H.U1 : H.U2; }
+template <int A, class R> __device__ __forceinline__ R *Sarr(const ChDev<R> &H) { return A == 0 ? H.S0 : A == 1 ? H.S1 : H.S2; }
+template <int A, class R> __device__ __forceinline__ R *Darr(const ChDev<R> &H) { return A == 0 ? H.D0 : A == 1 ? H.D1 : H.D2; }
+template <int A, class R> __device__ __forceinline__ R wid(const ChDev<R> &H, int i) { return A == 0 ? H.d0[i] : A == 1 ? H.d1[i] : H.d2[i]; }
+template <int A, class R> __device__ __forceinline__ R ctr(const ChDev<R> &H, int i) { return A == 0 ? H.h0[i] : A == 1 ? H.h1[i] : H.h2[i]; }
+template <int A, class R> __device__ __forceinline__ int ncell(const ChDev<R> &H) { return A == 0 ? H.N0 : A == 1 ? H.N1 : H.N2; }
+
+template <int A, class R>
+__device__ __forceinline__ int fidx(const ChDev<R> &H, int i, int j, int k) {
+  return i + (H.N0 + (A == 0)) * (j + (H.N1 + (A == 1)) * k);
+}
+template <class R>
+__device__ __forceinline__ int cidx(const ChDev<R> &H, int i, int j, int k) { return i + H.N0 * (j + H.N1 * k); }
+
+template <class R> __device__ __forceinline__ R rmax0(R a) { return a < R(0) ? R(0) : a; }  // maxd(a, 0)
+
+// 0 unknown, 1 fixed, 2 outlet
+template <int A, class R>
+__device__ __forceinline__ int face_kind(const ChDev<R> &H, const int (&c)[3]) {
+  const int f = c[A];
+  if (f == 0 || f == ncell<A>(H)) return (A == 0 && f == H.N0) ? 2 : 1;
+  int lo[3] = {c[0], c[1], c[2]};
+  lo[A] -= 1;
+  return (!H.solid[cidx(H, lo[0], lo[1], lo[2])] && !H.solid[cidx(H, c[0], c[1], c[2])]) ? 0 : 1;
+}
+
+template <int A, class R>
+__device__ __forceinline__ R face_fixed(const ChDev<R> &H, const int (&c)[3]) {
+  if (A == 0 && c[0] == 0 && !H.solid[cidx(H, 0, c[1], c[2])]) return H.u_in;
+  return R(0);
+}
+
+template <int A, class R>
+__device__ __forceinline__ R face_area(const ChDev<R> &H, const int (&c)[3]) {
+  if (A == 0) return H.d1[c[1]] * H.d2[c[2]];
+  if (A == 1) return H.d0[c[0]] * H.d2[c[2]];
+  return H.d0[c[0]] * H.d1[c[1]];
+}
+
+template <int A, class R>
+__device__ __forceinline__ int fidx3(const ChDev<R> &H, const int (&c)[3]) { return fidx<A>(H, c[0], c[1], c[2]); }
+
+// one stencil term (neighbour across axis B, high side when HI) of the unknown
+// face (A, c): coefficient, neighbour value from src and (resid) from u^n
+template <int A, int B, int HI, class R>
+__device__ __forceinline__ void term(const ChDev<R> &H, const int (&c)[3], R Ar, R da, const R *src, bool resid, R &coef,
+                                     R &val, R &valn) {
+  coef = R(0); val = R(0); valn = R(0);
+  const R *UA = Uarr<A>(H);
+  if constexpr (B == A) {
+    int q[3] = {c[0], c[1], c[2]};
+    if (HI) {
+      q[A] += 1;
+      if (!(A == 0 && q[0] == H.N0)) {
+        const R F = R(0.5) * (UA[fidx3<A>(H, c)] + UA[fidx3<A>(H, q)]) * Ar;
+        const R Dd = H.nu * Ar / wid<A>(H, c[A]);
+        coef = Dd + rmax0(-F);
+        val = src[fidx3<A>(H, q)];
+        if (resid) valn = UA[fidx3<A>(H, q)];
+      }
+    } else {
+      q[A] -= 1;
+      const R F = R(0.5) * (UA[fidx3<A>(H, q)] + UA[fidx3<A>(H, c)]) * Ar;
+      const R Dd = H.nu * Ar / wid<A>(H, c[A] - 1);
+      coef = Dd + rmax0(F);
+      val = src[fidx3<A>(H, q)];
+      if (resid) valn = UA[fidx3<A>(H, q)];
+    }
+  } else {
+    constexpr int O = 3 - A - B;
+    const R *UB = Uarr<B>(H);
+    const R wo = wid<O>(H, c[O]);
+    const R ar = da * wo;
+    int flo[3] = {c[0], c[1], c[2]}, fhi[3] = {c[0], c[1], c[2]};
+    flo[A] -= 1;
+    if (HI) { flo[B] += 1; fhi[B] += 1; }
+    const R F = R(0.5) * (UB[fidx3<B>(H, flo)] * wid<A>(H, c[A] - 1) + UB[fidx3<B>(H, fhi)] * wid<A>(H, c[A])) * wo;
+    int q[3] = {c[0], c[1], c[2]};
+    if (HI) {
+      if (c[B] + 1 == ncell<B>(H)) {
+        if (B != 0) coef = H.nu * ar / ctr<B>(H, ncell<B>(H)) + rmax0(-F);
+      } else {
+        coef = H.nu * ar / ctr<B>(H, c[B] + 1) + rmax0(-F);
+        q[B] += 1;
+        val = src[fidx3<A>(H, q)];
+        if (resid) valn = UA[fidx3<A>(H, q)];
+      }
+    } else {
+      if (c[B] == 0) {
+        coef = H.nu * ar / ctr<B>(H, 0) + rmax0(F);
+      } else {
+        coef = H.nu * ar / ctr<B>(H, c[B]) + rmax0(F);
+        q[B] -= 1;
+        val = src[fidx3<A>(H, q)];
+        if (resid) valn = UA[fidx3<A>(H, q)];
+      }
+    }
+  }
+}
+
+// momentum work on face (A, c): residual at u^n (resid), relaxed GS update (upd), d (last)
+template <int A, class R>
+__device__ __forceinline__ void mom_face(const ChDev<R> &H, const int (&c)[3], bool first, bool upd, bool resid,
+                                         bool last, double &racc) {
+  const int f = fidx3<A>(H, c);
+  const R Ar = face_area<A>(H, c);
+  const R da = ctr<A>(H, c[A]);
+  const R *src = first ? Uarr<A>(H) : Sarr<A>(H);
+  R an[6], v[6], vn[6];
+  term<A, 0, 1>(H, c, Ar, da, src, resid, an[0], v[0], vn[0]);
+  term<A, 0, 0>(H, c, Ar, da, src, resid, an[1], v[1], vn[1]);
+  term<A, 1, 1>(H, c, Ar, da, src, resid, an[2], v[2], vn[2]);
+  term<A, 1, 0>(H, c, Ar, da, src, resid, an[3], v[3], vn[3]);
+  term<A, 2, 1>(H, c, Ar, da, src, resid, an[4], v[4], vn[4]);
+  term<A, 2, 0>(H, c, Ar, da, src, resid, an[5], v[5], vn[5]);
+  const R aP = an[0] + an[1] + an[2] + an[3] + an[4] + an[5];
+  int lo[3] = {c[0], c[1], c[2]};
+  lo[A] -= 1;
+  const R bs = (H.p[cidx(H, lo[0], lo[1], lo[2])] - H.p[cidx(H, c[0], c[1], c[2])]) * Ar;
+  const R un = Uarr<A>(H)[f];
+  if (resid) {
+    double s = 0.0;
+#pragma unroll
+    for (int n = 0; n < 6; ++n) s += (double)an[n] * (double)vn[n];
+    const double r = (double)aP * (double)un - (s + (double)bs);
+    racc += r * r;
+  }
+  if (upd) {
+    const R apr = aP / H.au;
+    R s = R(0);
+#pragma unroll
+    for (int n = 0; n < 6; ++n) s += an[n] * v[n];
+    const R rhs = s + bs + (R(1) - H.au) * apr * un;
+    Sarr<A>(H)[f] = rhs / apr;
+    if (last) Darr<A>(H)[f] = Ar / apr;
+  }
+}
+
+__device__ double block_sum(double v, double *sh) {
+  for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  const int lane = threadIdx.x & 31, wid_ = threadIdx.x >> 5;
+  if (lane == 0) sh[wid_] = v;
+  __syncthreads();
+  double t = 0.0;
+  if (wid_ == 0) {
+    t = lane < (int)(blockDim.x >> 5) ? sh[lane] : 0.0;
+    for (int o = 16; o; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+  }
+  __syncthreads();
+  return t;
+}
+
+// One red-black pass of all three momentum components (blockIdx.y = axis).
+// first: the pass of colour 0 in sweep 0, which also evaluates the residual of
+// every unknown face at u^n and writes the fixed faces of u*.
+template <int A, class R>
+__device__ void mom_pass_axis(const ChDev<R> &H, int color, bool first, bool last, double &racc) {
+  const int nf0 = H.N0 + (A == 0), nf1 = H.N1 + (A == 1), nf2 = H.N2 + (A == 2);
+  const int T = gridDim.x * blockDim.x;
+  if (first) {
+    const long long n = (long long)nf0 * nf1 * nf2;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += T) {
+      const int c[3] = {(int)(e % nf0), (int)((e / nf0) % nf1), (int)(e / ((long long)nf0 * nf1))};
+      const int kind = face_kind<A>(H, c);
+      if (kind != 0) {
+        const int f = fidx3<A>(H, c);
+        Sarr<A>(H)[f] = face_fixed<A>(H, c);
+        Darr<A>(H)[f] = R(0);
+        continue;
+      }
+      const bool mine = ((c[0] + c[1] + c[2]) & 1) == color;
+      mom_face<A>(H, c, true, mine, true, last && mine, racc);
+    }
+  } else {
+    const int half = (nf0 + 1) / 2;
+    const long long n = (long long)half * nf1 * nf2;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += T) {
+      const int m = (int)(e % half), j = (int)((e / half) % nf1), k = (int)(e / ((long long)half * nf1));
+      const int i = 2 * m + ((j + k + color) & 1);
+      if (i >= nf0) continue;
+      const int c[3] = {i, j, k};
+      if (face_kind<A>(H, c) != 0) continue;
+      mom_face<A>(H, c, false, true, false, last, racc);
+    }
+  }
+}
+
+template <class R>
+__global__ void __launch_bounds__(kT) k_ch_mom(ChDev<R> H, int color, int first, int last, double *partials) {
+  __shared__ double sh[32];
+  double racc = 0.0;
+  if (blockIdx.y == 0) mom_pass_axis<0>(H, color, first, last, racc);
+  else if (blockIdx.y == 1) mom_pass_axis<1>(H, color, first, last, racc);
+  else mom_pass_axis<2>(H, color, first, last, racc);
+  if (first) {
+    const double b = block_sum(racc, sh);
+    if (threadIdx.x == 0) partials[blockIdx.y * gridDim.x + blockIdx.x] = b;
+  }
+}
+
+// padded cell index of the CG arrays
+__device__ __forceinline__ int pq(int N0, int N1, int i, int j, int k) { return (i + 1) + (N0 + 2) * ((j + 1) + (N1 + 2) * (k + 1)); }
+
+// p' couplings per face into padded cell arrays (the coupling of the face on a
+// cell's low side; the outlet face sits in the ghost cell i = N0) and the mass
+// imbalance b per cell (r = b, x = 0)
+template <class R>
+__global__ void k_ch_passemble(ChDev<R> H, double *acx, double *acy, double *acz, double *r, double *x, double *partials) {
+  __shared__ double sh[32];
+  const int T = gridDim.x * blockDim.x;
+  const int N0 = H.N0, N1 = H.N1, N2 = H.N2;
+  double acc = 0.0;
+  if (blockIdx.y == 0) {
+    const long long n = (long long)(N0 + 1) * N1 * N2;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += T) {
+      const int c[3] = {(int)(e % (N0 + 1)), (int)((e / (N0 + 1)) % N1), (int)(e / ((long long)(N0 + 1) * N1))};
+      const int kind = face_kind<0>(H, c);
+      double v = 0.0;
+      if (kind == 0) v = (double)face_area<0>(H, c) * (double)H.D0[fidx3<0>(H, c)];
+      else if (kind == 2 && !H.solid[cidx(H, c[0] - 1, c[1], c[2])])
+        v = (double)face_area<0>(H, c) * (double)H.D0[fidx<0>(H, c[0] - 1, c[1], c[2])];
+      acx[pq(N0, N1, c[0], c[1], c[2])] = v;
+    }
+  } else if (blockIdx.y == 1) {
+    const long long n = (long long)N0 * (N1 + 1) * N2;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += T) {
+      const int c[3] = {(int)(e % N0), (int)((e / N0) % (N1 + 1)), (int)(e / ((long long)N0 * (N1 + 1)))};
+      acy[pq(N0, N1, c[0], c[1], c[2])] = face_kind<1>(H, c) == 0 ? (double)face_area<1>(H, c) * (double)H.D1[fidx3<1>(H, c)] : 0.0;
+    }
+  } else if (blockIdx.y == 2) {
+    const long long n = (long long)N0 * N1 * (N2 + 1);
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += T) {
+      const int c[3] = {(int)(e % N0), (int)((e / N0) % N1), (int)(e / ((long long)N0 * N1))};
+      acz[pq(N0, N1, c[0], c[1], c[2])] = face_kind<2>(H, c) == 0 ? (double)face_area<2>(H, c) * (double)H.D2[fidx3<2>(H, c)] : 0.0;
+    }
+  } else {
+    const long long n = (long long)N0 * N1 * N2;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += T) {
+      const int i = (int)(e % N0), j = (int)((e / N0) % N1), k = (int)(e / ((long long)N0 * N1));
+      const int q = pq(N0, N1, i, j, k);
+      x[q] = 0.0;
+      if (H.solid[e]) { r[q] = 0.0; continue; }
+      const double uw = (double)H.S0[fidx<0>(H, i, j, k)];
+      const double ue = (i + 1 == N0) ? uw : (double)H.S0[fidx<0>(H, i + 1, j, k)];
+      const double b = (uw - ue) * ((double)H.d1[j] * (double)H.d2[k]) +
+                       ((double)H.S1[fidx<1>(H, i, j, k)] - (double)H.S1[fidx<1>(H, i, j + 1, k)]) * ((double)H.d0[i] * (double)H.d2[k]) +
+                       ((double)H.S2[fidx<2>(H, i, j, k)] - (double)H.S2[fidx<2>(H, i, j, k + 1)]) * ((double)H.d0[i] * (double)H.d1[j]);
+      r[q] = b;
+      acc += b * b;
+    }
+  }
+  const double bsum = block_sum(acc, sh);
+  if (threadIdx.x == 0 && blockIdx.y == 3) partials[blockIdx.x] = bsum;
+}
+
+template <int A, class R>
+__device__ void correct_axis(const ChDev<R> &H, const double *pp, double *Ud) {
+  const int nf0 = H.N0 + (A == 0), nf1 = H.N1 + (A == 1), nf2 = H.N2 + (A == 2);
+  const long long n = (long long)nf0 * nf1 * nf2;
+  const int T = gridDim.x * blockDim.x;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += T) {
+    const int c[3] = {(int)(e % nf0), (int)((e / nf0) % nf1), (int)(e / ((long long)nf0 * nf1))};
+    const int kind = face_kind<A>(H, c);
+    R val;
+    if (kind == 1) {
+      val = face_fixed<A>(H, c);
+    } else if (kind == 2) {
+      const int fl = fidx<0>(H, c[0] - 1, c[1], c[2]);
+      if (H.solid[cidx(H, c[0] - 1, c[1], c[2])]) val = R(0);
+      else if constexpr (sizeof(R) == 8) val = H.S0[fl] + H.D0[fl] * pp[pq(H.N0, H.N1, c[0] - 1, c[1], c[2])];
+      else val = (R)((double)H.S0[fl] + (double)H.D0[fl] * pp[pq(H.N0, H.N1, c[0] - 1, c[1], c[2])]);
+    } else {
+      int lo[3] = {c[0], c[1], c[2]};
+      lo[A] -= 1;
+      const int f = fidx3<A>(H, c);
+      const double dp = pp[pq(H.N0, H.N1, lo[0], lo[1], lo[2])] - pp[pq(H.N0, H.N1, c[0], c[1], c[2])];
+      if constexpr (sizeof(R) == 8) val = Sarr<A>(H)[f] + Darr<A>(H)[f] * dp;
+      else val = (R)((double)Sarr<A>(H)[f] + (double)Darr<A>(H)[f] * dp);
+    }
+    Uarr<A>(H)[e] = val;
+    if (Ud) Ud[e] = (double)val;
+  }
+}
+
+template <class R>
+__global__ void k_ch_correct(ChDev<R> H, const double *pp) {
+  if (blockIdx.y == 0) correct_axis<0>(H, pp, H.Ud0);
+  else if (blockIdx.y == 1) correct_axis<1>(H, pp, H.Ud1);
+  else if (blockIdx.y == 2) correct_axis<2>(H, pp, H.Ud2);
+  else {
+    const long long n = (long long)H.N0 * H.N1 * H.N2;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+      if (H.solid[e]) continue;
+      const int i = (int)(e % H.N0), j = (int)((e / H.N0) % H.N1), k = (int)(e / ((long long)H.N0 * H.N1));
+      const double v = pp[pq(H.N0, H.N1, i, j, k)];
+      if constexpr (sizeof(R) == 8) H.p[e] = H.p[e] + H.ap * v;
+      else H.p[e] = (R)((double)H.p[e] + H.ap * v);
+    }
+  }
+}
+
+// initial state: u = u_in on the inlet, unknown and outlet faces over fluid, 0 elsewhere; v = w = 0; p = 0
+template <class R>
+__global__ void k_ch_init(ChDev<R> H) {
+  const long long n0 = (long long)(H.N0 + 1) * H.N1 * H.N2;
+  const long long n1 = (long long)H.N0 * (H.N1 + 1) * H.N2, n2 = (long long)H.N0 * H.N1 * (H.N2 + 1);
+  const long long nc = (long long)H.N0 * H.N1 * H.N2;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n0 + n1 + n2 + nc; e += gridDim.x * blockDim.x) {
+    if (e < n0) {
+      const int c[3] = {(int)(e % (H.N0 + 1)), (int)((e / (H.N0 + 1)) % H.N1), (int)(e / ((long long)(H.N0 + 1) * H.N1))};
+      const int kind = face_kind<0>(H, c);
+      R v = R(0);
+      if (kind == 0) v = H.u_in;
+      else if (kind == 1) v = face_fixed<0>(H, c);
+      else v = H.solid[cidx(H, c[0] - 1, c[1], c[2])] ? R(0) : H.u_in;
+      H.U0[e] = v; H.S0[e] = v; H.D0[e] = R(0);
+      if (H.Ud0) H.Ud0[e] = (double)v;
+    } else if (e < n0 + n1) {
+      const long long f = e - n0;
+      H.U1[f] = R(0); H.S1[f] = R(0); H.D1[f] = R(0);
+      if (H.Ud1) H.Ud1[f] = 0.0;
+    } else if (e < n0 + n1 + n2) {
+      const long long f = e - n0 - n1;
+      H.U2[f] = R(0); H.S2[f] = R(0); H.D2[f] = R(0);
+      if (H.Ud2) H.Ud2[f] = 0.0;
+    } else {
+      H.p[e - n0 - n1 - n2] = R(0);
+    }
+  }
+}
+
+// ---------------------------------------------------------------- multigrid-preconditioned CG
+// Symmetric operator on padded cells: (A x)_q = sum_f c_f (x_q - x_nb), with
+// c stored on each cell's low face (acx[q] couples q-1 and q; acx of the
+// ghost cell N0 + 1 is the outlet face, neighbour value 0).
+// V-cycle in precision M: 2x coarsening per axis (ceil); a coarse cell is an
+// unknown when any child is; a coarse face coupling is half the sum of the
+// fine couplings on it (the 2x2 patch of a face, halved for the doubled
+// spacing); red-black Gauss-Seidel 1 pre (red, black) + 1 post (black, red);
+// sum restriction, constant prolongation; FP64 LU on the coarsest (<= 64 cells)
+// factored on the GPU every solve, since the couplings change every step.
+template <class M>
+struct Lv {
+  int nx, ny, nz;
+  M *x, *rhs, *ax, *ay, *az;
+  uint8_t *m;
+};
+template <class M>
+struct Mg {
+  int L;
+  Lv<M> lv[kMaxLv];
+  double *lu;   // kMaxCoarse^2
+  int *piv;     // kMaxCoarse
+  double *y;    // kMaxCoarse
+};
+struct CgVec {
+  int N0, N1, N2;
+  const double *acx, *acy, *acz;
+  const uint8_t *solid;
+  double *x, *r, *p, *s;
+};
+
+template <class M>
+__device__ __forceinline__ int li(const Lv<M> &L, int i, int j, int k) { return i + (L.nx + 2) * (j + (L.ny + 2) * k); }
+
+__device__ double grid_sum(double v, double *partials, int &buf, double *sh, cg::grid_group &grid) {
+  double *pp = partials + (size_t)buf * gridDim.x;
+  buf ^= 1;
+  const double b = block_sum(v, sh);
+  if (threadIdx.x == 0) pp[blockIdx.x] = b;
+  grid.sync();
+  double a = 0.0;
+  if (threadIdx.x < 32) {
+    for (int q = threadIdx.x; q < (int)gridDim.x; q += 32) a += __ldcg(pp + q);
+    for (int o = 16; o; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+    if (threadIdx.x == 0) sh[32] = a;
+  }
+  __syncthreads();
+  a = sh[32];
+  __syncthreads();
+  return a;
+}
+
+template <class M>
+__device__ void mg_build_fine(const CgVec &V, const Lv<M> &L0, int tid, int T) {
+  const int PX = V.N0 + 2, PY = V.N1 + 2;
+  const long long np = (long long)PX * PY * (V.N2 + 2);
+  for (long long q = tid; q < np; q += T) {
+    L0.ax[q] = (M)V.acx[q]; L0.ay[q] = (M)V.acy[q]; L0.az[q] = (M)V.acz[q];
+    const int i = (int)(q % PX) - 1, j = (int)((q / PX) % PY) - 1, k = (int)(q / ((long long)PX * PY)) - 1;
+    const bool in = i >= 0 && j >= 0 && k >= 0 && i < V.N0 && j < V.N1 && k < V.N2;
+    L0.m[q] = in && !V.solid[i + V.N0 * (j + V.N1 * k)];
+  }
+}
+
+template <class M>
+__device__ void mg_coarsen(const Lv<M> &F, const Lv<M> &C, int tid, int T) {
+  const long long n = (long long)(C.nx + 1) * (C.ny + 1) * (C.nz + 1);
+  for (long long e = tid; e < n; e += T) {
+    const int I = (int)(e % (C.nx + 1)), J = (int)((e / (C.nx + 1)) % (C.ny + 1)), K = (int)(e / ((long long)(C.nx + 1) * (C.ny + 1)));
+    const int qc = li(C, I + 1, J + 1, K + 1);
+    if (J < C.ny && K < C.nz) {  // x face I of coarse row (J, K)
+      const int fi = min(2 * I, F.nx);
+      M s = M(0);
+      for (int dk = 0; dk < 2; ++dk)
+        for (int dj = 0; dj < 2; ++dj) {
+          const int j = 2 * J + dj, k = 2 * K + dk;
+          if (j < F.ny && k < F.nz) s += F.ax[li(F, fi + 1, j + 1, k + 1)];
+        }
+      C.ax[qc] = M(0.5) * s;
+    }
+    if (I < C.nx && K < C.nz) {
+      const int fj = min(2 * J, F.ny);
+      M s = M(0);
+      for (int dk = 0; dk < 2; ++dk)
+        for (int di = 0; di < 2; ++di) {
+          const int i = 2 * I + di, k = 2 * K + dk;
+          if (i < F.nx && k < F.nz) s += F.ay[li(F, i + 1, fj + 1, k + 1)];
+        }
+      C.ay[qc] = M(0.5) * s;
+    }
+    if (I < C.nx && J < C.ny) {
+      const int fk = min(2 * K, F.nz);
+      M s = M(0);
+      for (int dj = 0; dj < 2; ++dj)
+        for (int di = 0; di < 2; ++di) {
+          const int i = 2 * I + di, j = 2 * J + dj;
+          if (i < F.nx && j < F.ny) s += F.az[li(F, i + 1, j + 1, fk + 1)];
+        }
+      C.az[qc] = M(0.5) * s;
+    }
+    if (I < C.nx && J < C.ny && K < C.nz) {
+      uint8_t any = 0;
+      for (int dk = 0; dk < 2; ++dk)
+        for (int dj = 0; dj < 2; ++dj)
+          for (int di = 0; di < 2; ++di) {
+            const int i = 2 * I + di, j = 2 * J + dj, k = 2 * K + dk;
+            if (i < F.nx && j < F.ny && k < F.nz && F.m[li(F, i + 1, j + 1, k + 1)]) any = 1;
+          }
+      C.m[qc] = any;
+    }
+  }
+}
+
+template <class M>
+__device__ __forceinline__ M lv_diag(const Lv<M> &L, int q, int PX, int PXY) {
+  return L.ax[q] + L.ax[q + 1] + L.ay[q] + L.ay[q + PX] + L.az[q] + L.az[q + PXY];
+}
+template <class M>
+__device__ __forceinline__ M lv_off(const Lv<M> &L, const M *x, int q, int PX, int PXY) {
+  return L.ax[q] * __ldcg(x + q - 1) + L.ax[q + 1] * __ldcg(x + q + 1) + L.ay[q] * __ldcg(x + q - PX) +
+         L.ay[q + PX] * __ldcg(x + q + PX) + L.az[q] * __ldcg(x + q - PXY) + L.az[q + PXY] * __ldcg(x + q + PXY);
+}
+
+template <class M>
+__device__ void mg_smooth(const Lv<M> &L, int color, bool zero_nb, int tid, int T) {
+  const int PX = L.nx + 2, PXY = (L.nx + 2) * (L.ny + 2);
+  const int half = (L.nx + 1) / 2;
+  const long long n = (long long)half * L.ny * L.nz;
+  for (long long e = tid; e < n; e += T) {
+    const int m = (int)(e % half), j = (int)((e / half) % L.ny), k = (int)(e / ((long long)half * L.ny));
+    const int i = 2 * m + ((j + k + color) & 1);
+    if (i >= L.nx) continue;
+    const int q = li(L, i + 1, j + 1, k + 1);
+    if (!L.m[q]) continue;
+    const M d = lv_diag(L, q, PX, PXY);
+    if (d == M(0)) { L.x[q] = M(0); continue; }
+    M s = L.rhs[q];
+    if (!zero_nb) s += lv_off(L, L.x, q, PX, PXY);
+    L.x[q] = s / d;
+  }
+}
+
+template <class M>
+__device__ void mg_restrict(const Lv<M> &F, const Lv<M> &C, int tid, int T) {
+  const int PX = F.nx + 2, PXY = (F.nx + 2) * (F.ny + 2);
+  const long long n = (long long)C.nx * C.ny * C.nz;
+  for (long long e = tid; e < n; e += T) {
+    const int I = (int)(e % C.nx), J = (int)((e / C.nx) % C.ny), K = (int)(e / ((long long)C.nx * C.ny));
+    M acc = M(0);
+    for (int dk = 0; dk < 2; ++dk)
+      for (int dj = 0; dj < 2; ++dj)
+        for (int di = 0; di < 2; ++di) {
+          const int i = 2 * I + di, j = 2 * J + dj, k = 2 * K + dk;
+          if (i >= F.nx || j >= F.ny || k >= F.nz) continue;
+          const int q = li(F, i + 1, j + 1, k + 1);
+          if (!F.m[q]) continue;
+          acc += F.rhs[q] - (lv_diag(F, q, PX, PXY) * __ldcg(F.x + q) - lv_off(F, F.x, q, PX, PXY));
+        }
+    const int qc = li(C, I + 1, J + 1, K + 1);
+    C.rhs[qc] = C.m[qc] ? acc : M(0);
+  }
+}
+
+template <class M>
+__device__ void mg_prolong(const Lv<M> &F, const Lv<M> &C, int tid, int T) {
+  const long long n = (long long)F.nx * F.ny * F.nz;
+  for (long long e = tid; e < n; e += T) {
+    const int i = (int)(e % F.nx), j = (int)((e / F.nx) % F.ny), k = (int)(e / ((long long)F.nx * F.ny));
+    const int q = li(F, i + 1, j + 1, k + 1);
+    if (!F.m[q]) continue;
+    F.x[q] = __ldcg(F.x + q) + __ldcg(C.x + li(C, i / 2 + 1, j / 2 + 1, k / 2 + 1));
+  }
+}
+
+// dense LU with partial pivoting of the coarsest operator, by block 0
+template <class M>
+__device__ void mg_factor(const Mg<M> &G) {
+  if (blockIdx.x != 0) return;
+  const Lv<M> &C = G.lv[G.L - 1];
+  const int nc = C.nx * C.ny * C.nz, PX = C.nx + 2, PXY = (C.nx + 2) * (C.ny + 2);
+  double *a = G.lu;
+  for (int e = threadIdx.x; e < nc * nc; e += blockDim.x) {
+    const int r = e / nc, c2 = e % nc;
+    const int ri = r % C.nx, rj = (r / C.nx) % C.ny, rk = r / (C.nx * C.ny);
+    const int q = li(C, ri + 1, rj + 1, rk + 1);
+    double v = 0.0;
+    if (!C.m[q]) {
+      v = (r == c2) ? 1.0 : 0.0;
+    } else if (r == c2) {
+      v = (double)lv_diag(C, q, PX, PXY);
+      if (v == 0.0) v = 1.0;
+    } else {
+      const int ci = c2 % C.nx, cj = (c2 / C.nx) % C.ny, ck = c2 / (C.nx * C.ny);
+      const int qc = li(C, ci + 1, cj + 1, ck + 1);
+      if (C.m[qc]) {
+        if (qc == q - 1) v = -(double)C.ax[q];
+        else if (qc == q + 1) v = -(double)C.ax[q + 1];
+        else if (qc == q - PX) v = -(double)C.ay[q];
+        else if (qc == q + PX) v = -(double)C.ay[q + PX];
+        else if (qc == q - PXY) v = -(double)C.az[q];
+        else if (qc == q + PXY) v = -(double)C.az[q + PXY];
+      }
+    }
+    a[e] = v;
+  }
+  __syncthreads();
+  __shared__ int spiv;
+  for (int col = 0; col < nc; ++col) {
+    if (threadIdx.x == 0) {
+      int best = col;
+      double bv = fabs(a[col * nc + col]);
+      for (int r = col + 1; r < nc; ++r)
+        if (fabs(a[r * nc + col]) > bv) { bv = fabs(a[r * nc + col]); best = r; }
+      spiv = best;
+      G.piv[col] = best;
+    }
+    __syncthreads();
+    const int pr = spiv;
+    if (pr != col)
+      for (int c2 = threadIdx.x; c2 < nc; c2 += blockDim.x) {
+        const double t = a[col * nc + c2];
+        a[col * nc + c2] = a[pr * nc + c2];
+        a[pr * nc + c2] = t;
+      }
+    __syncthreads();
+    const double piv = a[col * nc + col];
+    for (int r = col + 1 + threadIdx.x; r < nc; r += blockDim.x) a[r * nc + col] /= piv;
+    __syncthreads();
+    const int rem = nc - col - 1;
+    for (int e = threadIdx.x; e < rem * rem; e += blockDim.x) {
+      const int r = col + 1 + e / rem, c2 = col + 1 + e % rem;
+      a[r * nc + c2] -= a[r * nc + col] * a[col * nc + c2];
+    }
+    __syncthreads();
+  }
+}
+
+template <class M>
+__device__ void mg_coarse_solve(const Mg<M> &G) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  const Lv<M> &C = G.lv[G.L - 1];
+  const int nc = C.nx * C.ny * C.nz;
+  double *y = G.y;
+  for (int r = 0; r < nc; ++r) {
+    const int ri = r % C.nx, rj = (r / C.nx) % C.ny, rk = r / (C.nx * C.ny);
+    y[r] = (double)C.rhs[li(C, ri + 1, rj + 1, rk + 1)];
+  }
+  for (int c2 = 0; c2 < nc; ++c2) {  // apply the row swaps in order
+    const int pr = G.piv[c2];
+    if (pr != c2) { const double t = y[c2]; y[c2] = y[pr]; y[pr] = t; }
+  }
+  for (int r = 0; r < nc; ++r) {
+    double s = y[r];
+    for (int c2 = 0; c2 < r; ++c2) s -= G.lu[r * nc + c2] * y[c2];
+    y[r] = s;
+  }
+  for (int r = nc - 1; r >= 0; --r) {
+    double s = y[r];
+    for (int c2 = r + 1; c2 < nc; ++c2) s -= G.lu[r * nc + c2] * y[c2];
+    y[r] = s / G.lu[r * nc + r];
+  }
+  for (int r = 0; r < nc; ++r) {
+    const int ri = r % C.nx, rj = (r / C.nx) % C.ny, rk = r / (C.nx * C.ny);
+    const int q = li(C, ri + 1, rj + 1, rk + 1);
+    C.x[q] = C.m[q] ? (M)y[r] : M(0);
+  }
+}
+
+template <class M>
+__device__ void mg_vcycle(const Mg<M> &G, cg::grid_group &grid, int tid, int T) {
+  for (int l = 0; l < G.L - 1; ++l) {
+    mg_smooth(G.lv[l], 0, true, tid, T);
+    grid.sync();
+    mg_smooth(G.lv[l], 1, false, tid, T);
+    grid.sync();
+    mg_restrict(G.lv[l], G.lv[l + 1], tid, T);
+    grid.sync();
+  }
+  mg_coarse_solve(G);
+  grid.sync();
+  for (int l = G.L - 2; l >= 0; --l) {
+    mg_prolong(G.lv[l], G.lv[l + 1], tid, T);
+    grid.sync();
+    mg_smooth(G.lv[l], 1, false, tid, T);
+    grid.sync();
+    mg_smooth(G.lv[l], 0, false, tid, T);
+    grid.sync();
+  }
+}
+
+__device__ __forceinline__ double cg_apply(const CgVec &V, const double *x, int q, int PX, int PXY) {
+  const double cw = V.acx[q], ce = V.acx[q + 1], cs = V.acy[q], cn = V.acy[q + PX], cb = V.acz[q], cf = V.acz[q + PXY];
+  const double d = cw + ce + cs + cn + cb + cf;
+  return d * __ldcg(x + q) - (cw * __ldcg(x + q - 1) + ce * __ldcg(x + q + 1) + cs * __ldcg(x + q - PX) +
+                              cn * __ldcg(x + q + PX) + cb * __ldcg(x + q - PXY) + cf * __ldcg(x + q + PXY));
+}
+
+// PCG: r = b (assembled), x = 0; z = M r (V-cycle, or z = r when precond = 0);
+// s = A p, alpha = <r,z>/<s,p>, x += alpha p, r -= alpha s, stop on ||r||/||b|| < tol
+template <class M>
+__global__ void __launch_bounds__(kT) k_ch_pcg(CgVec V, Mg<M> G, int precond, double tol, int maxiter, double *partials,
+                                               int *out_it, double *out_rel) {
+  cg::grid_group grid = cg::this_grid();
+  __shared__ double sh[40];
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x, T = gridDim.x * blockDim.x;
+  const int N0 = V.N0, N1 = V.N1, PX = N0 + 2, PXY = (N0 + 2) * (N1 + 2);
+  const long long n = (long long)N0 * N1 * V.N2;
+  int buf = 0;
+  const Lv<M> &L0 = G.lv[0];
+  if (precond) {
+    mg_build_fine(V, L0, tid, T);
+    grid.sync();
+    for (int l = 0; l + 1 < G.L; ++l) {
+      mg_coarsen(G.lv[l], G.lv[l + 1], tid, T);
+      grid.sync();
+    }
+    mg_factor(G);
+    grid.sync();
+  }
+  double acc = 0.0;
+  for (long long e = tid; e < n; e += T) {
+    const int q = pq(N0, N1, (int)(e % N0), (int)((e / N0) % N1), (int)(e / ((long long)N0 * N1)));
+    const double rv = V.r[q];
+    acc += rv * rv;
+    if (precond) L0.rhs[q] = (M)rv;
+  }
+  const double bb = grid_sum(acc, partials, buf, sh, grid);
+  if (bb == 0.0) {
+    if (tid == 0) { *out_it = 0; *out_rel = 0.0; }
+    return;
+  }
+  const double eps = tol * tol;
+  if (precond) mg_vcycle(G, grid, tid, T);
+  acc = 0.0;
+  for (long long e = tid; e < n; e += T) {
+    const int q = pq(N0, N1, (int)(e % N0), (int)((e / N0) % N1), (int)(e / ((long long)N0 * N1)));
+    const double z = precond ? (double)__ldcg(L0.x + q) : V.r[q];
+    V.p[q] = z;
+    acc += V.r[q] * z;
+  }
+  double gamma = grid_sum(acc, partials, buf, sh, grid), rr = bb;
+  int it = 0;
+  while (it < maxiter && !(rr / bb < eps)) {
+    it++;
+    acc = 0.0;
+    for (long long e = tid; e < n; e += T) {
+      const int q = pq(N0, N1, (int)(e % N0), (int)((e / N0) % N1), (int)(e / ((long long)N0 * N1)));
+      const double sv = cg_apply(V, V.p, q, PX, PXY);
+      V.s[q] = sv;
+      acc += sv * __ldcg(V.p + q);
+    }
+    const double sp = grid_sum(acc, partials, buf, sh, grid);
+    if (sp == 0.0) break;
+    const double alpha = gamma / sp;
+    acc = 0.0;
+    for (long long e = tid; e < n; e += T) {
+      const int q = pq(N0, N1, (int)(e % N0), (int)((e / N0) % N1), (int)(e / ((long long)N0 * N1)));
+      V.x[q] = V.x[q] + alpha * V.p[q];
+      const double rv = V.r[q] - alpha * V.s[q];
+      V.r[q] = rv;
+      acc += rv * rv;
+      if (precond) L0.rhs[q] = (M)rv;
+    }
+    rr = grid_sum(acc, partials, buf, sh, grid);
+    if (rr / bb < eps) break;
+    if (precond) mg_vcycle(G, grid, tid, T);
+    acc = 0.0;
+    for (long long e = tid; e < n; e += T) {
+      const int q = pq(N0, N1, (int)(e % N0), (int)((e / N0) % N1), (int)(e / ((long long)N0 * N1)));
+      acc += V.r[q] * (precond ? (double)__ldcg(L0.x + q) : V.r[q]);
+    }
+    const double gnew = grid_sum(acc, partials, buf, sh, grid);
+    const double beta = gnew / gamma;
+    gamma = gnew;
+    for (long long e = tid; e < n; e += T) {
+      const int q = pq(N0, N1, (int)(e % N0), (int)((e / N0) % N1), (int)(e / ((long long)N0 * N1)));
+      V.p[q] = (precond ? (double)__ldcg(L0.x + q) : V.r[q]) + beta * V.p[q];
+    }
+    grid.sync();
+  }
+  if (tid == 0) { *out_it = it; *out_rel = sqrt(rr / bb); }
+}
+
+// residual sums of the momentum pass (3 x nb partials) and continuity (nb) -> res[0..3]
+__global__ void k_ch_finalize(const double *mom, const double *cont, int nb, double *res) {
+  if (threadIdx.x >= 32) return;
+  for (int a = 0; a < 4; ++a) {
+    const double *src = a < 3 ? mom + a * nb : cont;
+    double s = 0.0;
+    for (int q = threadIdx.x; q < nb; q += 32) s += src[q];
+    for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (threadIdx.x == 0) res[a] = sqrt(s);
+  }
+}
+
+__global__ void k_zero(double *a, long long n) {
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) a[e] = 0.0;
+}
+
+int blocks_for(long long n) { return (int)std::max<long long>(1, std::min<long long>((n + kT - 1) / kT, 148LL * 8)); }
+
+template <class K, class... A>
+void launch_coop(K kernel, int blocks, cudaStream_t s, A... args) {
+  void *argv[] = {(void *)&args...};
+  CH_CUDA(cudaLaunchCooperativeKernel((void *)kernel, dim3(blocks), dim3(kT), argv, 0, s));
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------- host state
+struct ChannelState {
+  Case kase;
+  ChParams prm;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool mixed = false;
+  int N0 = 0, N1 = 0, N2 = 0, nreg = 0;
+  double nu = 0, kf = 0;
+  std::vector<int> region;
+  std::vector<void *> allocs;
+  long long bytes = 0;
+  ChDev<double> Hd{};
+  ChDev<float> Hf{};
+  CgVec V{};
+  Mg<double> Gd{};
+  Mg<float> Gf{};
+  int mom_blocks = 0, pcg_grid = 0;
+  double *mom_part = nullptr, *cont_part = nullptr, *pcg_part = nullptr, *res = nullptr, *pcg_rel = nullptr;
+  int *pcg_it = nullptr;
+  ChtState *cht = nullptr;
+  std::vector<double> kratio, qcell;
+  ChStats st{};
+  int iter = 0;
+
+  template <class T_>
+  T_ *alloc(size_t n) {
+    void *p = nullptr;
+    const size_t b = std::max<size_t>(n, 1) * sizeof(T_);
+    cudaError_t e = cudaMalloc(&p, b);
+    if (e != cudaSuccess) throw std::runtime_error(std::string("CUDA alloc: ") + cudaGetErrorString(e));
+    allocs.push_back(p);
+    bytes += (long long)b;
+    CH_CUDA(cudaMemsetAsync(p, 0, b, stream));
+    return (T_ *)p;
+  }
+  ~ChannelState() {
+    if (cht) cht_destroy(cht);
+    for (void *p : allocs) cudaFree(p);
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
+namespace {
+
+template <class R>
+void setup_fields(ChannelState &S, ChDev<R> &H, const std::vector<double> (&d)[3], const std::vector<double> (&h)[3],
+                  const uint8_t *solid) {
+  H.N0 = S.N0; H.N1 = S.N1; H.N2 = S.N2;
+  const R **dd[3] = {&H.d0, &H.d1, &H.d2}, **hh[3] = {&H.h0, &H.h1, &H.h2};
+  for (int a = 0; a < 3; ++a) {
+    std::vector<R> dv(d[a].begin(), d[a].end()), hv(h[a].begin(), h[a].end());
+    R *pd = S.alloc<R>(dv.size()), *ph = S.alloc<R>(hv.size());
+    CH_CUDA(cudaMemcpyAsync(pd, dv.data(), dv.size() * sizeof(R), cudaMemcpyHostToDevice, S.stream));
+    CH_CUDA(cudaMemcpyAsync(ph, hv.data(), hv.size() * sizeof(R), cudaMemcpyHostToDevice, S.stream));
+    *dd[a] = pd; *hh[a] = ph;
+  }
+  H.solid = solid;
+  const size_t nf[3] = {(size_t)(S.N0 + 1) * S.N1 * S.N2, (size_t)S.N0 * (S.N1 + 1) * S.N2, (size_t)S.N0 * S.N1 * (S.N2 + 1)};
+  R **U[3] = {&H.U0, &H.U1, &H.U2}, **Sx[3] = {&H.S0, &H.S1, &H.S2}, **D[3] = {&H.D0, &H.D1, &H.D2};
+  for (int a = 0; a < 3; ++a) { *U[a] = S.alloc<R>(nf[a]); *Sx[a] = S.alloc<R>(nf[a]); *D[a] = S.alloc<R>(nf[a]); }
+  H.p = S.alloc<R>((size_t)S.N0 * S.N1 * S.N2);
+  if (sizeof(R) == 4) {
+    H.Ud0 = S.alloc<double>(nf[0]); H.Ud1 = S.alloc<double>(nf[1]); H.Ud2 = S.alloc<double>(nf[2]);
+  } else {
+    H.Ud0 = H.Ud1 = H.Ud2 = nullptr;
+  }
+  H.nu = (R)S.nu; H.au = (R)S.prm.alpha_u; H.u_in = (R)S.prm.u_in; H.ap = S.prm.alpha_p;
+}
+
+template <class M>
+void setup_mg(ChannelState &S, Mg<M> &G) {
+  int nx = S.N0, ny = S.N1, nz = S.N2, L = 0;
+  while (true) {
+    if (L >= kMaxLv) throw std::runtime_error("multigrid: too many levels");
+    Lv<M> &l = G.lv[L];
+    l.nx = nx; l.ny = ny; l.nz = nz;
+    const size_t np = (size_t)(nx + 2) * (ny + 2) * (nz + 2);
+    l.x = S.alloc<M>(np); l.rhs = S.alloc<M>(np);
+    l.ax = S.alloc<M>(np); l.ay = S.alloc<M>(np); l.az = S.alloc<M>(np);
+    l.m = S.alloc<uint8_t>(np);
+    ++L;
+    if ((long long)nx * ny * nz <= kMaxCoarse) break;
+    nx = (nx + 1) / 2; ny = (ny + 1) / 2; nz = (nz + 1) / 2;
+  }
+  G.L = L;
+  G.lu = S.alloc<double>((size_t)kMaxCoarse * kMaxCoarse);
+  G.piv = S.alloc<int>(kMaxCoarse);
+  G.y = S.alloc<double>(kMaxCoarse);
+}
+
+template <class R>
+void mom_solve(ChannelState &S, ChDev<R> &H) {
+  const int sw = std::max(1, S.prm.mom_sweeps);
+  for (int s = 0; s < sw; ++s)
+    for (int color = 0; color < 2; ++color)
+      k_ch_mom<R><<<dim3(S.mom_blocks, 3), kT, 0, S.stream>>>(H, color, s == 0 && color == 0, s == sw - 1, S.mom_part);
+  CH_CUDA(cudaGetLastError());
+}
+
+template <class R>
+void step_once(ChannelState &S, ChDev<R> &H, int flags) {
+  mom_solve(S, H);
+  k_ch_passemble<R><<<dim3(S.mom_blocks, 4), kT, 0, S.stream>>>(H, (double *)S.V.acx, (double *)S.V.acy, (double *)S.V.acz,
+                                                                S.V.r, S.V.x, S.cont_part);
+  k_ch_finalize<<<1, 32, 0, S.stream>>>(S.mom_part, S.cont_part, S.mom_blocks, S.res);
+  CH_CUDA(cudaGetLastError());
+  if (!(flags & 1)) {
+    const int pre = S.prm.p_precond ? 1 : 0;
+    if (S.mixed)
+      launch_coop(k_ch_pcg<float>, S.pcg_grid, S.stream, S.V, S.Gf, pre, S.prm.p_tol, S.prm.p_maxiter, S.pcg_part, S.pcg_it,
+                  S.pcg_rel);
+    else
+      launch_coop(k_ch_pcg<double>, S.pcg_grid, S.stream, S.V, S.Gd, pre, S.prm.p_tol, S.prm.p_maxiter, S.pcg_part, S.pcg_it,
+                  S.pcg_rel);
+  } else {
+    const long long np = (long long)(S.N0 + 2) * (S.N1 + 2) * (S.N2 + 2);
+    k_zero<<<blocks_for(np), kT, 0, S.stream>>>(S.V.x, np);
+    CH_CUDA(cudaMemsetAsync(S.pcg_it, 0, sizeof(int), S.stream));
+  }
+  k_ch_correct<R><<<dim3(S.mom_blocks, 4), kT, 0, S.stream>>>(H, (const double *)S.V.x);
+  CH_CUDA(cudaGetLastError());
+  if (!(flags & 2)) cht_energy_step(S.cht, S.prm.alpha_t, S.prm.t_tol, S.prm.t_maxiter);
+}
+
+void read_stats(ChannelState &S, int flags) {
+  double r[4];
+  int pit = 0;
+  double prel = 0;
+  CH_CUDA(cudaMemcpyAsync(r, S.res, 32, cudaMemcpyDeviceToHost, S.stream));
+  CH_CUDA(cudaMemcpyAsync(&pit, S.pcg_it, 4, cudaMemcpyDeviceToHost, S.stream));
+  CH_CUDA(cudaMemcpyAsync(&prel, S.pcg_rel, 8, cudaMemcpyDeviceToHost, S.stream));
+  CH_CUDA(cudaStreamSynchronize(S.stream));
+  for (int a = 0; a < 4; ++a) S.st.res[a] = r[a];
+  S.st.pcg_iters = (flags & 1) ? 0 : pit;
+  S.st.pcg_relres = (flags & 1) ? 0.0 : prel;
+  if (!(flags & 2)) {
+    double rel, r0;
+    int it;
+    cht_step_results(S.cht, &it, &rel, &r0);
+    S.st.res[4] = r0; S.st.t_iters = it; S.st.t_relres = rel;
+  } else {
+    S.st.res[4] = 0.0; S.st.t_iters = 0; S.st.t_relres = 0.0;
+  }
+  S.iter++;
+  S.st.iter = S.iter;
+  double g = 0.0;
+  for (int x = 0; x < 5; ++x) {
+    if (S.iter <= 5 && S.st.res[x] > S.st.norm[x]) S.st.norm[x] = S.st.res[x];
+    const double q = S.st.res[x] / (S.st.norm[x] > 1e-300 ? S.st.norm[x] : 1e-300);
+    if (q > g) g = q;
+  }
+  S.st.global = g;
+}
+
+}  // namespace
+
+ChannelState *ch_create(const Case &c, const ChParams &p, int device) {
+  if (!(p.re > 0) || !(p.pr > 0) || !(p.alpha_u > 0 && p.alpha_u <= 1) || !(p.alpha_p > 0 && p.alpha_p <= 1) ||
+      !(p.alpha_t > 0 && p.alpha_t <= 1) || p.mom_sweeps < 1 || !(p.p_tol > 0) || p.p_maxiter < 0 || !(p.t_tol > 0) ||
+      p.t_maxiter < 0 || (p.precision != 0 && p.precision != 1))
+    throw std::invalid_argument("invalid channel parameters");
+  if ((long long)(c.Nx + 2) * (c.Ny + 2) * (c.Nz + 2) >= (1LL << 31))
+    throw std::invalid_argument("grid too large for 32-bit indices");
+  CH_CUDA(cudaSetDevice(device));
+  std::unique_ptr<ChannelState> S(new ChannelState());
+  S->kase = c;
+  S->prm = p;
+  S->device = device;
+  S->mixed = p.precision == 1;
+  CH_CUDA(cudaStreamCreateWithFlags(&S->stream, cudaStreamNonBlocking));
+  S->N0 = (int)c.Nx; S->N1 = (int)c.Ny; S->N2 = (int)c.Nz;
+  S->nreg = c.nsolid_regions;
+  const std::vector<double> *pts[3] = {&c.deck.xs, &c.deck.ys, &c.deck.zs};
+  std::vector<double> d[3], h[3];
+  const int N[3] = {S->N0, S->N1, S->N2};
+  for (int a = 0; a < 3; ++a) {
+    const std::vector<double> &x = *pts[a];
+    d[a].resize(N[a]); h[a].resize(N[a] + 1);
+    for (int i = 0; i < N[a]; ++i) d[a][i] = x[i + 1] - x[i];
+    h[a][0] = 0.5 * d[a][0];
+    h[a][N[a]] = 0.5 * d[a][N[a] - 1];
+    for (int i = 1; i < N[a]; ++i) h[a][i] = 0.5 * (x[i] + x[i + 1]) - 0.5 * (x[i - 1] + x[i]);
+  }
+  const double ly = c.deck.ys[S->N1] - c.deck.ys[0];
+  S->nu = p.u_in * ly / p.re;
+  S->kf = S->nu / p.pr;
+  const size_t n = (size_t)S->N0 * S->N1 * S->N2;
+  uint8_t *solid = S->alloc<uint8_t>(n);
+  CH_CUDA(cudaMemcpyAsync(solid, c.ctype.data(), n, cudaMemcpyHostToDevice, S->stream));
+  if (S->mixed) setup_fields(*S, S->Hf, d, h, solid);
+  else setup_fields(*S, S->Hd, d, h, solid);
+  // CG vectors and couplings (FP64, padded)
+  const size_t np = (size_t)(S->N0 + 2) * (S->N1 + 2) * (S->N2 + 2);
+  S->V.N0 = S->N0; S->V.N1 = S->N1; S->V.N2 = S->N2; S->V.solid = solid;
+  S->V.acx = S->alloc<double>(np); S->V.acy = S->alloc<double>(np); S->V.acz = S->alloc<double>(np);
+  S->V.x = S->alloc<double>(np); S->V.r = S->alloc<double>(np); S->V.p = S->alloc<double>(np); S->V.s = S->alloc<double>(np);
+  if (S->mixed) setup_mg(*S, S->Gf);
+  else setup_mg(*S, S->Gd);
+  S->mom_blocks = blocks_for((long long)(S->N0 + 1) * (S->N1 + 1) * (S->N2 + 1));
+  S->mom_part = S->alloc<double>((size_t)3 * S->mom_blocks);
+  S->cont_part = S->alloc<double>((size_t)S->mom_blocks);
+  S->res = S->alloc<double>(4);
+  int per = 0, nsm = 0;
+  CH_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
+  if (S->mixed) CH_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_ch_pcg<float>, kT, 0));
+  else CH_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_ch_pcg<double>, kT, 0));
+  if (per < 1) throw std::runtime_error("pressure-correction kernel cannot be resident");
+  S->pcg_grid = per * nsm;
+  S->pcg_part = S->alloc<double>((size_t)2 * S->pcg_grid + 64);
+  S->pcg_it = S->alloc<int>(1);
+  S->pcg_rel = S->alloc<double>(1);
+  // energy: the conjugate-heat-transfer operator in channel mode, on this stream
+  S->region.resize(n);
+  for (size_t i = 0; i < n; ++i) S->region[i] = c.ctype[i] ? c.region[i] : -1;
+  ChtSetup cs;
+  cs.device = device; cs.stream = S->stream;
+  cs.Nx = S->N0; cs.Ny = S->N1; cs.Nz = S->N2; cs.nreg = S->nreg;
+  cs.xs = c.deck.xs.data(); cs.ys = c.deck.ys.data(); cs.zs = c.deck.zs.data();
+  cs.ctype = c.ctype.data(); cs.region = S->region.data();
+  cs.t_boundary = p.t_in; cs.tol = 1e-10; cs.maxiter = 5000; cs.bc = 1;
+  S->cht = cht_create(cs);
+  if (S->mixed) cht_bind_velocities(S->cht, S->Hf.Ud0, S->Hf.Ud1, S->Hf.Ud2);
+  else cht_bind_velocities(S->cht, S->Hd.U0, S->Hd.U1, S->Hd.U2);
+  S->kratio.assign(S->nreg, 100.0);
+  S->qcell.assign(n, 0.0);
+  std::vector<double> kabs(S->nreg);
+  for (int r = 0; r < S->nreg; ++r) kabs[r] = S->kratio[r] * S->kf;
+  cht_set_solid(S->cht, S->kf, kabs.data(), S->qcell.data());
+  CH_CUDA(cudaStreamSynchronize(S->stream));
+  return S.release();
+}
+
+void ch_destroy(ChannelState *S) {
+  if (!S) return;
+  cudaSetDevice(S->device);
+  if (S->stream) cudaStreamSynchronize(S->stream);
+  delete S;
+}
+
+int ch_nreg(const ChannelState *S) { return S->nreg; }
+
+void ch_set_solid(ChannelState *S, const double *k_ratio, const double *q_cell) {
+  CH_CUDA(cudaSetDevice(S->device));
+  const size_t n = (size_t)S->N0 * S->N1 * S->N2;
+  for (int r = 0; r < S->nreg; ++r)
+    if (!(k_ratio[r] > 0)) throw std::invalid_argument("conductivity ratio must be positive");
+  S->kratio.assign(k_ratio, k_ratio + S->nreg);
+  for (size_t c = 0; c < n; ++c) S->qcell[c] = S->kase.ctype[c] ? q_cell[c] : 0.0;
+  std::vector<double> kabs(S->nreg);
+  for (int r = 0; r < S->nreg; ++r) kabs[r] = S->kratio[r] * S->kf;
+  cht_set_solid(S->cht, S->kf, kabs.data(), S->qcell.data());
+}
+
+void ch_init(ChannelState *S) {
+  CH_CUDA(cudaSetDevice(S->device));
+  const long long tot = (long long)(S->N0 + 1) * (S->N1 + 1) * (S->N2 + 1) * 4;
+  if (S->mixed) k_ch_init<float><<<blocks_for(tot), kT, 0, S->stream>>>(S->Hf);
+  else k_ch_init<double><<<blocks_for(tot), kT, 0, S->stream>>>(S->Hd);
+  CH_CUDA(cudaGetLastError());
+  cht_fill_T(S->cht, S->prm.t_in);
+  S->iter = 0;
+  S->st = ChStats{};
+  S->st.global = 1.0;
+  CH_CUDA(cudaStreamSynchronize(S->stream));
+}
+
+void ch_step(ChannelState *S, int n, int flags, ChStats *out) {
+  CH_CUDA(cudaSetDevice(S->device));
+  for (int s = 0; s < n; ++s) {
+    if (S->mixed) step_once(*S, S->Hf, flags);
+    else step_once(*S, S->Hd, flags);
+    read_stats(*S, flags);
+  }
+  if (out) *out = S->st;
+}
+
+int ch_solve_to(ChannelState *S, double tol, int max_outer, ChStats *out) {
+  CH_CUDA(cudaSetDevice(S->device));
+  int s = 0;
+  while (s < max_outer) {
+    if (S->mixed) step_once(*S, S->Hf, 0);
+    else step_once(*S, S->Hd, 0);
+    read_stats(*S, 0);
+    ++s;
+    if (S->iter > 5 && S->st.global <= tol) break;
+  }
+  if (out) *out = S->st;
+  return s;
+}
+
+// fields: 0..2 u v w, 3 p, 4 T, 5..7 u* v* w*, 8..10 d, 11 p'
+long ch_field_size(const ChannelState *S, int f) {
+  const long n = (long)S->N0 * S->N1 * S->N2;
+  if (f == 3 || f == 4 || f == 11) return n;
+  if (f < 0 || f > 11) return -1;
+  const int a = f < 3 ? f : (f - 5) % 3;
+  return (long)(S->N0 + (a == 0)) * (S->N1 + (a == 1)) * (S->N2 + (a == 2));
+}
+
+namespace {
+template <class R>
+void get_dev(ChannelState *S, const R *src, double *host, long n) {
+  std::vector<R> tmp(n);
+  CH_CUDA(cudaMemcpyAsync(tmp.data(), src, n * sizeof(R), cudaMemcpyDeviceToHost, S->stream));
+  CH_CUDA(cudaStreamSynchronize(S->stream));
+  for (long i = 0; i < n; ++i) host[i] = (double)tmp[i];
+}
+template <class R>
+void put_dev(ChannelState *S, R *dst, const double *host, long n) {
+  std::vector<R> tmp(host, host + n);
+  CH_CUDA(cudaMemcpyAsync(dst, tmp.data(), n * sizeof(R), cudaMemcpyHostToDevice, S->stream));
+  CH_CUDA(cudaStreamSynchronize(S->stream));
+}
+template <class R>
+R *field_ptr(ChDev<R> &H, int f) {
+  R *t[11] = {H.U0, H.U1, H.U2, H.p, nullptr, H.S0, H.S1, H.S2, H.D0, H.D1, H.D2};
+  return f < 11 ? t[f] : nullptr;
+}
+void unpad_cells(ChannelState *S, const double *dev, double *host) {
+  const size_t np = (size_t)(S->N0 + 2) * (S->N1 + 2) * (S->N2 + 2);
+  std::vector<double> tmp(np);
+  CH_CUDA(cudaMemcpyAsync(tmp.data(), dev, np * 8, cudaMemcpyDeviceToHost, S->stream));
+  CH_CUDA(cudaStreamSynchronize(S->stream));
+  for (int k = 0; k < S->N2; ++k)
+    for (int j = 0; j < S->N1; ++j)
+      for (int i = 0; i < S->N0; ++i)
+        host[i + (size_t)S->N0 * (j + (size_t)S->N1 * k)] = tmp[(i + 1) + (S->N0 + 2) * ((j + 1) + (size_t)(S->N1 + 2) * (k + 1))];
+}
+}  // namespace
+
+void ch_get_field(ChannelState *S, int f, double *host, long n) {
+  CH_CUDA(cudaSetDevice(S->device));
+  if (ch_field_size(S, f) != n) throw std::invalid_argument("field size mismatch");
+  if (f == 4) { unpad_cells(S, cht_T_device(S->cht), host); return; }
+  if (f == 11) { unpad_cells(S, S->V.x, host); return; }
+  if (S->mixed) get_dev(S, (const float *)field_ptr(S->Hf, f), host, n);
+  else get_dev(S, (const double *)field_ptr(S->Hd, f), host, n);
+}
+
+void ch_set_field(ChannelState *S, int f, const double *host, long n) {
+  CH_CUDA(cudaSetDevice(S->device));
+  if (ch_field_size(S, f) != n || f > 4) throw std::invalid_argument("field size mismatch or read-only field");
+  if (f == 4) {
+    const size_t np = (size_t)(S->N0 + 2) * (S->N1 + 2) * (S->N2 + 2);
+    std::vector<double> tmp(np, 0.0);
+    for (int k = 0; k < S->N2; ++k)
+      for (int j = 0; j < S->N1; ++j)
+        for (int i = 0; i < S->N0; ++i)
+          tmp[(i + 1) + (S->N0 + 2) * ((j + 1) + (size_t)(S->N1 + 2) * (k + 1))] = host[i + (size_t)S->N0 * (j + (size_t)S->N1 * k)];
+    CH_CUDA(cudaMemcpyAsync(cht_T_device(S->cht), tmp.data(), np * 8, cudaMemcpyHostToDevice, S->stream));
+    CH_CUDA(cudaStreamSynchronize(S->stream));
+    return;
+  }
+  if (S->mixed) {
+    put_dev(S, field_ptr(S->Hf, f), host, n);
+    double *Ud[3] = {S->Hf.Ud0, S->Hf.Ud1, S->Hf.Ud2};
+    if (f < 3) {
+      CH_CUDA(cudaMemcpyAsync(Ud[f], host, n * 8, cudaMemcpyHostToDevice, S->stream));
+      CH_CUDA(cudaStreamSynchronize(S->stream));
+    }
+  } else {
+    put_dev(S, field_ptr(S->Hd, f), host, n);
+  }
+}
+
+void *ch_stream(ChannelState *S) { return S->stream; }
+void ch_sync(ChannelState *S) { CH_CUDA(cudaSetDevice(S->device)); CH_CUDA(cudaStreamSynchronize(S->stream)); }
+long long ch_device_bytes(const ChannelState *S) { return S->bytes; }
+
+void ch_adjoint(ChannelState *S, double tol, int maxiter, double *J, double *dJdq, double *dJdk, int *fwd_iters,
+                int *adj_iters, double *fwd_ms, double *adj_ms) {
+  CH_CUDA(cudaSetDevice(S->device));
+  // the relaxed outer-loop temperature is kept; the adjoint works on a full solve
+  const size_t np = (size_t)(S->N0 + 2) * (S->N1 + 2) * (S->N2 + 2);
+  double *keep = nullptr;
+  CH_CUDA(cudaMalloc(&keep, np * 8));
+  CH_CUDA(cudaMemcpyAsync(keep, cht_T_device(S->cht), np * 8, cudaMemcpyDeviceToDevice, S->stream));
+  cudaEvent_t e0, e1, e2;
+  CH_CUDA(cudaEventCreate(&e0)); CH_CUDA(cudaEventCreate(&e1)); CH_CUDA(cudaEventCreate(&e2));
+  cht_set_tolerance(S->cht, tol, maxiter);
+  double rel = 0;
+  CH_CUDA(cudaEventRecord(e0, S->stream));
+  cht_forward(S->cht, nullptr, J, fwd_iters, &rel);
+  CH_CUDA(cudaEventRecord(e1, S->stream));
+  cht_adjoint(S->cht, dJdq, dJdk, adj_iters, &rel);
+  CH_CUDA(cudaEventRecord(e2, S->stream));
+  CH_CUDA(cudaEventSynchronize(e2));
+  float a = 0, b = 0;
+  CH_CUDA(cudaEventElapsedTime(&a, e0, e1));
+  CH_CUDA(cudaEventElapsedTime(&b, e1, e2));
+  if (fwd_ms) *fwd_ms = a;
+  if (adj_ms) *adj_ms = b;
+  cudaEventDestroy(e0); cudaEventDestroy(e1); cudaEventDestroy(e2);
+  CH_CUDA(cudaMemcpyAsync(cht_T_device(S->cht), keep, np * 8, cudaMemcpyDeviceToDevice, S->stream));
+  CH_CUDA(cudaStreamSynchronize(S->stream));
+  cudaFree(keep);
+}
+
+}  // namespace hs

@@ -7,7 +7,9 @@
 // adjoint; this module is the monolithic form: per face between cells P, N
 //   G = A / (dP/(2 kP) + dN/(2 kN))     (harmonic-mean interface conductance)
 //   F = u A (outward from P)            (first-order upwind convection)
-// boundary faces carry Dirichlet Tb through G_b = 2 kP A / dP; row P is
+// boundary faces carry Dirichlet Tb through G_b = 2 kP A / dP (bc = 0), or,
+// for the channel (bc = 1), only the inlet face x = 0 does and the others are
+// adiabatic, with upwind outflow at x = Nx; row P is
 //   (sum G + max(F,0)) T_P - sum (G + max(-F,0)) T_N = q_P V_P + boundary terms.
 // The transposed operator has the same stencil with the upwind side swapped:
 // A^T_{P,N} = A_{N,P}, read from the neighbour's stored coefficient.
@@ -47,6 +49,7 @@ struct ChtDev {
   const double *q;                 // padded source
   const double *ug, *vg, *wg;      // global face velocities
   double *d, *aw, *ae, *as, *an, *ab, *af, *b, *dinv;  // padded coefficients
+  int bc;                          // 0 Dirichlet everywhere, 1 channel
 };
 
 __device__ __forceinline__ int pidx(const ChtDev &H, int i, int j, int k) {  // 0-based cell -> padded
@@ -114,7 +117,8 @@ __device__ __forceinline__ void face(const ChtDev &H, int i, int j, int k, int d
     has = kk >= 0 && kk < H.Nz; if (has) dN = H.dz[kk];
   }
   if (has) G = A / (dP / (2 * kp) + dN / (2 * H.k[pidx(H, ii, jj, kk)]));
-  else G = 2 * kp * A / dP;
+  else if (H.bc == 0 || (ax == 0 && !hi)) G = 2 * kp * A / dP;
+  else G = 0.0;
   F = (hi ? u : -u) * A;
 }
 
@@ -154,8 +158,10 @@ struct Vec {
 
 // Jacobi-preconditioned BiCGStab (van der Vorst, SIAM J. Sci. Stat. Comput.
 // 13(2), 1992) for A x = rhs or A^T x = rhs; x holds the start.
+// rel0: stop on ||r|| / ||r0|| instead of ||r|| / ||rhs||; out_r0 = ||r0||.
 __global__ void __launch_bounds__(kB) k_cht_bicgstab(ChtDev H, Vec V, const double *rhs, int transpose, double tol,
-                                                     int maxiter, double *partials, int *out_it, double *out_rel) {
+                                                     int maxiter, double *partials, int *out_it, double *out_rel,
+                                                     int rel0, double *out_r0) {
   cg::grid_group grid = cg::this_grid();
   __shared__ double sh[48];
   const int Nx = H.Nx, Ny = H.Ny, n = Nx * H.Ny * H.Nz;
@@ -172,7 +178,9 @@ __global__ void __launch_bounds__(kB) k_cht_bicgstab(ChtDev H, Vec V, const doub
     red[1] += rv * rv;
   }
   grid_sums<2>(red, partials, buf, sh, grid);
-  double bb = red[0] > 0 ? red[0] : 1.0, rr = red[1];
+  double bb = rel0 ? red[1] : red[0], rr = red[1];
+  if (bb == 0) bb = 1.0;
+  if (tid == 0 && out_r0) *out_r0 = sqrt(rr);
   const double eps = tol * tol;
   double rho = 1.0, alpha = 1.0, omega = 1.0;
   int it = 0;
@@ -333,6 +341,21 @@ __global__ void k_cht_velocities(ChtVelSrc S, double *ug, double *vg, double *wg
   }
 }
 
+// T = T + a (x - T) on the interior of padded arrays
+__global__ void k_cht_relax(int n, int Nx, int Ny, double a, const double *x, double *T) {
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
+    const int q = (c % Nx + 1) + (Nx + 2) * ((c / Nx) % Ny + 1 + (Ny + 2) * (c / (Nx * Ny) + 1));
+    T[q] = T[q] + a * (x[q] - T[q]);
+  }
+}
+
+// T = v on the interior
+__global__ void k_cht_fill(int n, int Nx, int Ny, double v, double *T) {
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
+    const int q = (c % Nx + 1) + (Nx + 2) * ((c / Nx) % Ny + 1 + (Ny + 2) * (c / (Nx * Ny) + 1));
+    T[q] = v;
+  }
+}
 int coop_grid(const void *kernel, int device) {
   int nsm = 0, per = 0;
   HC_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
@@ -383,6 +406,7 @@ ChtState *cht_create(const ChtSetup &S) {
   C->stream = (cudaStream_t)S.stream;
   C->Tb = S.t_boundary; C->tol = S.tol; C->maxiter = S.maxiter; C->nreg = S.nreg;
   ChtDev &H = C->H;
+  H.bc = S.bc;
   H.Nx = S.Nx; H.Ny = S.Ny; H.Nz = S.Nz;
   const size_t np = (size_t)(S.Nx + 2) * (S.Ny + 2) * (S.Nz + 2), n = (size_t)S.Nx * S.Ny * S.Nz;
   auto up = [&](const std::vector<double> &v) {
@@ -421,7 +445,7 @@ ChtState *cht_create(const ChtSetup &S) {
   C->dJdq = C->alloc<double>(n); C->dkc = C->alloc<double>(n);
   C->grid = coop_grid((const void *)k_cht_bicgstab, S.device);
   C->partials = C->alloc<double>((size_t)2 * C->grid * 2 + 4096);
-  C->res = C->alloc<double>(1); C->it = C->alloc<int>(1);
+  C->res = C->alloc<double>(2); C->it = C->alloc<int>(1);
   HC_CUDA(cudaStreamSynchronize(C->stream));
   return C.release();
 }
@@ -514,10 +538,9 @@ void cht_forward(ChtState *C, double *T_host, double *J, int *iters, double *rel
   const ChtDev &H = C->H;
   const size_t np = (size_t)(H.Nx + 2) * (H.Ny + 2) * (H.Nz + 2);
   k_cht_assemble<<<gfor((long long)H.Nx * H.Ny * H.Nz), kB, 0, C->stream>>>(H, C->Tb);
-  std::vector<double> x0(np, C->Tb);
-  HC_CUDA(cudaMemcpyAsync(C->V.x, x0.data(), np * 8, cudaMemcpyHostToDevice, C->stream));
+  k_cht_fill<<<gfor((long long)H.Nx * H.Ny * H.Nz), kB, 0, C->stream>>>(H.Nx * H.Ny * H.Nz, H.Nx, H.Ny, C->Tb, C->V.x);
   launch_coop(k_cht_bicgstab, C->grid, C->stream, H, C->V, (const double *)H.b, 0, C->tol, C->maxiter, C->partials, C->it,
-              C->res);
+              C->res, 0, (double *)nullptr);
   HC_CUDA(cudaMemcpyAsync(C->T, C->V.x, np * 8, cudaMemcpyDeviceToDevice, C->stream));
   int it = 0;
   double rr = 0;
@@ -541,7 +564,7 @@ void cht_adjoint(ChtState *C, double *dJdq_host, double *dJdk_host, int *iters, 
   objective(C, true);
   HC_CUDA(cudaMemsetAsync(C->V.x, 0, np * 8, C->stream));
   launch_coop(k_cht_bicgstab, C->grid, C->stream, H, C->V, (const double *)C->g, 1, C->tol, C->maxiter, C->partials, C->it,
-              C->res);
+              C->res, 0, (double *)nullptr);
   HC_CUDA(cudaMemcpyAsync(C->lam, C->V.x, np * 8, cudaMemcpyDeviceToDevice, C->stream));
   k_cht_grad<<<gfor(n), kB, 0, C->stream>>>(H, C->T, C->lam, C->Tb, C->dJdq, C->dkc);
   std::vector<double> dq(n), dk(n);
@@ -561,5 +584,46 @@ void cht_adjoint(ChtState *C, double *dJdq_host, double *dJdk_host, int *iters, 
   if (iters) *iters = it;
   if (relres) *relres = rr;
 }
+
+void cht_bind_velocities(ChtState *C, const double *ug, const double *vg, const double *wg) {
+  C->H.ug = ug; C->H.vg = vg; C->H.wg = wg;
+}
+
+void cht_fill_T(ChtState *C, double v) {
+  HC_CUDA(cudaSetDevice(C->device));
+  const ChtDev &H = C->H;
+  const int n = H.Nx * H.Ny * H.Nz;
+  k_cht_fill<<<gfor(n), kB, 0, C->stream>>>(n, H.Nx, H.Ny, v, C->T);
+  HC_CUDA(cudaGetLastError());
+  C->have_T = false;
+}
+
+double *cht_T_device(ChtState *C) { return C->T; }
+
+void cht_energy_step(ChtState *C, double alpha_t, double tol, int maxiter) {
+  const ChtDev &H = C->H;
+  const int n = H.Nx * H.Ny * H.Nz;
+  const size_t np = (size_t)(H.Nx + 2) * (H.Ny + 2) * (H.Nz + 2);
+  k_cht_assemble<<<gfor(n), kB, 0, C->stream>>>(H, C->Tb);
+  HC_CUDA(cudaMemcpyAsync(C->V.x, C->T, np * 8, cudaMemcpyDeviceToDevice, C->stream));
+  launch_coop(k_cht_bicgstab, C->grid, C->stream, H, C->V, (const double *)H.b, 0, tol, maxiter, C->partials, C->it,
+              C->res, 1, C->res + 1);
+  k_cht_relax<<<gfor(n), kB, 0, C->stream>>>(n, H.Nx, H.Ny, alpha_t, (const double *)C->V.x, C->T);
+  HC_CUDA(cudaGetLastError());
+  C->have_T = false;
+}
+
+void cht_step_results(ChtState *C, int *iters, double *relres, double *r0) {
+  double rr[2];
+  int it = 0;
+  HC_CUDA(cudaMemcpyAsync(&it, C->it, 4, cudaMemcpyDeviceToHost, C->stream));
+  HC_CUDA(cudaMemcpyAsync(rr, C->res, 16, cudaMemcpyDeviceToHost, C->stream));
+  HC_CUDA(cudaStreamSynchronize(C->stream));
+  if (iters) *iters = it;
+  if (relres) *relres = rr[0];
+  if (r0) *r0 = rr[1];
+}
+
+void cht_set_tolerance(ChtState *C, double tol, int maxiter) { C->tol = tol; C->maxiter = maxiter; }
 
 }  // namespace hs

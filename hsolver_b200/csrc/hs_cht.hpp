@@ -14,6 +14,8 @@ struct ChtSetup {
   const int *region;              // host, solid region per cell
   double t_boundary, tol;
   int maxiter;
+  int bc;                         // 0 Dirichlet t_boundary on every boundary face; 1 channel (Dirichlet at
+                                  // x = 0, upwind outflow at x = Nx, adiabatic y / z walls)
 };
 
 // where the face velocities come from: the fluid box's padded u*, v*, w*
@@ -31,5 +33,14 @@ void cht_set_velocities(ChtState *c, const ChtVelSrc &src);
 void cht_get_velocities(ChtState *c, double *ug, double *vg, double *wg);
 void cht_forward(ChtState *c, double *T_host, double *J, int *iters, double *relres);
 void cht_adjoint(ChtState *c, double *dJdq_host, double *dJdk_host, int *iters, double *relres);
+// channel use: the owner's device face velocities, T = v everywhere, one relaxed
+// energy step (BiCGStab from the current T to tol * ||r0||, T += alpha (T~ - T)),
+// its results (iterations, ||r|| / ||r0||, ||r0||) after a stream sync
+void cht_bind_velocities(ChtState *c, const double *ug, const double *vg, const double *wg);
+void cht_fill_T(ChtState *c, double v);
+double *cht_T_device(ChtState *c);
+void cht_energy_step(ChtState *c, double alpha_t, double tol, int maxiter);
+void cht_step_results(ChtState *c, int *iters, double *relres, double *r0);
+void cht_set_tolerance(ChtState *c, double tol, int maxiter);
 
 }  // namespace hs

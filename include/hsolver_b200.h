@@ -25,6 +25,7 @@ extern "C" {
 #define HS_ERR_STATE (-6)       /* call out of order */
 #define HS_ERR_DIVERGED (-7)    /* non-finite residual */
 #define HS_ERR_INTERNAL (-8)    /* a bounded device wait gave up */
+#define HS_ERR_MAXITER (-9)     /* iteration limit reached before the tolerance */
 
 /* Pressure-correction solver choice. */
 #define HS_PSOLVE_CG 0   /* HYPRE PCG restated: identity preconditioner (fluid_solver.h:1871-1875) */
@@ -223,6 +224,83 @@ int hs_cht_adjoint(hs_cht *h, double *dJdq, double *dJdk, int *iters, double *re
 /* The frozen face velocities ((Nx+1)NyNz, Nx(Ny+1)Nz, NxNy(Nz+1), host). */
 int hs_cht_velocities(hs_cht *h, double *ug, double *vg, double *wg);
 void hs_cht_destroy(hs_cht *h);
+
+/* Channel conjugate heat transfer: the SIMPLE outer step with the physics the
+ * reference lacks (its FluidSolver::solve, fluid_solver.h:1401-1633, drives a
+ * lid cavity with no inlet, heat source or conductivity ratio).  Inlet plug
+ * flow u_in at x = 0, zero-gradient outlet at x = Nx (p' = 0 there), no-slip
+ * walls, the deck's mobs boxes as solid blocks with a conductivity ratio per
+ * block and a volumetric source per cell, nu = u_in H / Re on the channel
+ * height H, fluid conductivity nu / Pr.  Momentum keeps the reference's
+ * first-order upwind coefficients (fluid_solver.h:577-659) with Patankar
+ * relaxation alpha_u, solved by red-black Gauss-Seidel; the pressure
+ * correction is SIMPLE's symmetric p' system, solved by CG preconditioned by
+ * a geometric multigrid V-cycle; the energy equation is the conjugate-heat-
+ * transfer operator of hs_cht_* over fluid and solid (inlet Dirichlet t_in,
+ * adiabatic walls, upwind outflow), warm-started BiCGStab, relaxation alpha_t.
+ * Global residual: the largest of the momentum (u, v, w), continuity and
+ * energy residuals, each the L2 norm of its unrelaxed equation residual
+ * divided by its largest value over the first five outer steps. */
+#define HS_PREC_FP64 0
+#define HS_PREC_MIXED 1   /* FP32 fields, sweeps and V-cycle; FP64 residuals, CG recurrences, dots, coarsest solve */
+#define HS_CH_SKIP_PRESSURE 1
+#define HS_CH_SKIP_ENERGY 2
+typedef struct hs_channel hs_channel;
+typedef struct hs_channel_params {
+  double re, pr, u_in, t_in;
+  double alpha_u, alpha_p, alpha_t;
+  int mom_sweeps;      /* red-black sweeps per momentum solve */
+  double p_tol;        /* pressure-correction CG: ||r|| / ||b|| */
+  int p_maxiter;
+  double t_tol;        /* energy BiCGStab per outer step: ||r|| / ||r0|| */
+  int t_maxiter;
+  int precision;       /* HS_PREC_* */
+  int p_precond;       /* 0 plain CG, 1 multigrid V-cycle */
+  double reserved[6];
+} hs_channel_params;
+typedef struct hs_channel_stats {
+  double res[5];       /* u, v, w momentum, continuity, energy (absolute L2) */
+  double norm[5];      /* normalisers: maximum over the first five outer steps */
+  double global;       /* max_x res[x] / norm[x] */
+  int iter;            /* outer steps since hs_channel_init */
+  int pcg_iters, t_iters;
+  double pcg_relres, t_relres;
+} hs_channel_stats;
+/* Channel fields for hs_channel_get_field / set_field (set: 0..4 only):
+ * 0..2 u, v, w on faces ((Nx+1)NyNz, Nx(Ny+1)Nz, NxNy(Nz+1), x fastest),
+ * 3 p, 4 T (Nx*Ny*Nz), 5..7 u*, v*, w*, 8..10 d = A alpha_u / a_P, 11 p'. */
+void hs_channel_params_default(hs_channel_params *p);
+int hs_channel_create(const char *deck, const hs_channel_params *prm, int device, hs_channel **out);
+int hs_channel_num_blocks(hs_channel *h, int *n);
+/* k_solid / k_fluid per block (n_blocks values, blocks numbered as the solid
+ * regions of hs_get_cell_types), q per cell (Nx*Ny*Nz, read in solid cells). */
+int hs_channel_set_solid(hs_channel *h, const double *k_ratio, int n_blocks, const double *q_cell, long long n);
+int hs_channel_init(hs_channel *h);
+/* n outer steps; flags HS_CH_SKIP_* leave out the pressure or energy solve. */
+int hs_channel_step(hs_channel *h, int n, int flags, hs_channel_stats *stats);
+/* Outer steps until the global residual <= tol (HS_OK) or max_outer steps
+ * (HS_ERR_MAXITER); *steps = steps taken. */
+int hs_channel_solve_to(hs_channel *h, double tol, int max_outer, int *steps, hs_channel_stats *stats);
+int hs_channel_field_size(hs_channel *h, int field, long long *n);
+int hs_channel_get_field(hs_channel *h, int field, double *host, long long n);
+int hs_channel_set_field(hs_channel *h, int field, const double *host, long long n);
+int hs_channel_stream(hs_channel *h, void **stream);
+int hs_channel_sync(hs_channel *h);
+/* Device memory the solver holds (bytes). */
+int hs_channel_device_bytes(hs_channel *h, long long *bytes);
+/* Energy adjoint on the current flow, frozen: a forward energy solve from
+ * T = t_in to ||r|| / ||b|| < tol, then the adjoint.  J = (sum over solid
+ * cells of T^8 dV)^(1/8); dJdq per cell (n = Nx*Ny*Nz), dJdk per block
+ * (derivative with respect to the block's conductivity k_solid).  Both
+ * timings are CUDA-event times on the solver's stream.  The outer loop's
+ * temperature is left as it was. */
+typedef struct hs_adjoint_info {
+  int fwd_iters, adj_iters;
+  double fwd_ms, adj_ms;
+} hs_adjoint_info;
+int hs_channel_adjoint(hs_channel *h, double tol, int maxiter, double *J, double *dJdq, long long n, double *dJdk,
+                       int n_blocks, hs_adjoint_info *info);
+void hs_channel_destroy(hs_channel *h);
 
 /* Validation of the divisions the sweeps perform with precomputed
  * reciprocals: returns how many of the n host pairs (a[i], b[i]) give a

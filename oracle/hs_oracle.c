@@ -1125,6 +1125,8 @@ typedef struct {
   const double *qcell;             /* volumetric source per cell */
   const double *ug, *vg, *wg;      /* face velocities (Nx+1)NyNz, Nx(Ny+1)Nz, NxNy(Nz+1) */
   double Tb;
+  int bc;                          /* 0: Dirichlet Tb on every boundary face; 1: channel (Dirichlet Tb
+                                      at x = 0, zero-gradient outflow at x = Nx, adiabatic y/z walls) */
 } or_cht;
 
 #define CC(i, j, k) ((i) + (j) * H->Nx + (k) * H->Nx * H->Ny)
@@ -1154,7 +1156,8 @@ static void cht_face(const or_cht *H, I64 i, I64 j, I64 k, int d, double *G, dou
     if (kk >= 0 && kk < H->Nz) { n = CC(i, j, kk); dN = H->zs[kk + 1] - H->zs[kk]; }
   }
   if (n >= 0) { kn = H->kcell[n]; *G = A / (dP / (2 * kp) + dN / (2 * kn)); }
-  else *G = 2 * kp * A / dP;
+  else if (H->bc == 0 || (ax == 0 && !hi)) *G = 2 * kp * A / dP;
+  else *G = 0.0;
   *F = (hi ? u : -u) * A;
   *nb = n;
 }
@@ -1197,7 +1200,8 @@ static double cht_diag(const or_cht *H, I64 i, I64 j, I64 k) {
 }
 
 /* Jacobi-preconditioned BiCGStab (van der Vorst 1992) on A or A^T. */
-static int cht_bicgstab(const or_cht *H, int transpose, const double *b, double *x, double tol, int maxiter, double *relres) {
+static int cht_bicgstab(const or_cht *H, int transpose, const double *b, double *x, double tol, int maxiter, double *relres,
+                        int rel0, double *r0norm) {
   I64 N = H->Nx * H->Ny * H->Nz;
   double *r = malloc(8 * N), *rh = malloc(8 * N), *p = calloc(N, 8), *v = calloc(N, 8), *ph = malloc(8 * N);
   double *s = malloc(8 * N), *sh = malloc(8 * N), *t = malloc(8 * N), *dinv = malloc(8 * N);
@@ -1208,6 +1212,8 @@ static int cht_bicgstab(const or_cht *H, int transpose, const double *b, double 
   double rho = 1, alpha = 1, omega = 1, rr = 0;
   int it = 0;
   for (I64 c = 0; c < N; ++c) rr += r[c] * r[c];
+  if (r0norm) *r0norm = sqrt(rr);
+  if (rel0) bb = rr;
   if (bb == 0) bb = 1;
   while (it < maxiter && rr / bb >= tol * tol) {
     it++;
@@ -1265,7 +1271,7 @@ int or_cht_forward(const or_cht *H, double *T, double tol, int maxiter, double *
   double *b = malloc(8 * N);
   cht_rhs(H, b);
   for (I64 c = 0; c < N; ++c) T[c] = H->Tb;
-  int it = cht_bicgstab(H, 0, b, T, tol, maxiter, relres);
+  int it = cht_bicgstab(H, 0, b, T, tol, maxiter, relres, 0, NULL);
   if (J) *J = cht_objective(H, T, NULL);
   free(b);
   return it;
@@ -1278,7 +1284,7 @@ int or_cht_adjoint(const or_cht *H, const double *T, double *lam, double *dJdq, 
   double *g = malloc(8 * N);
   cht_objective(H, T, g);
   for (I64 c = 0; c < N; ++c) lam[c] = 0;
-  int it = cht_bicgstab(H, 1, g, lam, tol, maxiter, relres);
+  int it = cht_bicgstab(H, 1, g, lam, tol, maxiter, relres, 0, NULL);
   for (int r = 0; r < nreg; ++r) dJdk[r] = 0;
   for (I64 k = 0; k < H->Nz; ++k) for (I64 j = 0; j < H->Ny; ++j) for (I64 i = 0; i < H->Nx; ++i) {
     I64 c = CC(i, j, k);
@@ -1300,3 +1306,436 @@ int or_cht_adjoint(const or_cht *H, const double *T, double *lam, double *dJdq, 
   free(g);
   return it;
 }
+
+/* ------------------------------------------------------------------ */
+/* Channel conjugate heat transfer: the extended physics the GPU path adds
+ * beside the reference's lid cavity (the reference has no inlet, outlet,
+ * heat source, conductivity ratio or global residual).  The oracle restates
+ * the in-repo discretisation of hsolver_b200/csrc/hs_channel.cu, in the same
+ * operation order, so the momentum sweeps agree bit for bit:
+ *
+ *   staggered faces of axis a, index c = (i,j,k) with c_a in [0, N_a]:
+ *     c_a = 0       x: inlet, u = u_in (fluid cell) / y,z: wall, 0
+ *     c_a = N_a     x: outlet, u = u*(N_x - 1) + d p'(N_x - 1) / y,z: wall, 0
+ *     otherwise     unknown when both cells are fluid, else 0
+ *   momentum (FOU, reference differencing a_nb = D + max(-+F, 0), a_P = sum a_nb,
+ *   fluid_solver.h:577-659), Patankar relaxation
+ *     (a_P/alpha_u) u_P = sum a_nb u_nb + (p_lo - p_hi) A + (1 - alpha_u)(a_P/alpha_u) u_P^n
+ *   with coefficients frozen at u^n, solved by red-black Gauss-Seidel sweeps
+ *   (colour (i+j+k)&1 of the face index); d = A alpha_u / a_P.
+ *   Stencil order E W N S T B (axis 0..2, high side first); a neighbour across
+ *   the outlet is zero-gradient (coefficient dropped), across a wall or the
+ *   inlet it is 0 at half a cell.
+ *   p': couplings A d per unknown face, A d(N_x - 1) at the outlet face
+ *   (p' = 0 outside), b = mass imbalance of u* with u*(N_x) := u*(N_x - 1);
+ *   symmetric positive definite, solved by CG to p_tol.
+ *   correction u = u* + d (p'_lo - p'_hi), p += alpha_p p'.
+ *   energy: the conjugate-heat-transfer operator above with bc = 1, fluid
+ *   conductivity 1/(Re Pr), solid k_ratio/(Re Pr), warm-started BiCGStab to
+ *   t_tol of its initial residual, T += alpha_t (T~ - T).
+ *   residuals: momentum ||a_P u^n - sum a_nb u^n_nb - b|| over unknown faces,
+ *   continuity ||b(u*)||, energy ||b - A T^n||; the global residual is the
+ *   largest of them divided by its maximum over the first five outer steps. */
+
+typedef struct {
+  double re, pr, u_in, t_in, alpha_u, alpha_p, alpha_t;
+  int mom_sweeps;
+  double p_tol;
+  int p_maxiter;
+  double t_tol;
+  int t_maxiter;
+} or_ch_params;
+
+typedef struct {
+  I64 N[3];
+  double *pts[3], *d[3], *h[3];   /* points, widths, centre distances (h[a][0], h[a][N] = half widths) */
+  unsigned char *solid;
+  int *region, nreg;
+  double *kreg, *qcell;
+  or_ch_params P;
+  double nu, kf;
+  double *U[3], *US[3], *D[3];    /* face arrays */
+  double *p, *pp, *T, *kcell, *bc;
+  double *ac[3];                  /* p' couplings per face */
+  double res[5], norm[5], glob;   /* u v w continuity energy */
+  int iter, pcg_iters, t_iters;
+  double pcg_relres;
+} or_ch;
+
+static I64 ch_nf(const or_ch *C, int a, int b) { return C->N[b] + (a == b); }
+static I64 ch_f(const or_ch *C, int a, I64 i, I64 j, I64 k) { return i + ch_nf(C, a, 0) * (j + ch_nf(C, a, 1) * k); }
+static I64 ch_c(const or_ch *C, I64 i, I64 j, I64 k) { return i + C->N[0] * (j + C->N[1] * k); }
+
+/* 0 unknown, 1 fixed, 2 outlet */
+static int ch_kind(const or_ch *C, int a, const I64 *c) {
+  I64 f = c[a];
+  if (f == 0 || f == C->N[a]) return (a == 0 && f == C->N[a]) ? 2 : 1;
+  I64 lo[3] = {c[0], c[1], c[2]};
+  lo[a] -= 1;
+  return (!C->solid[ch_c(C, lo[0], lo[1], lo[2])] && !C->solid[ch_c(C, c[0], c[1], c[2])]) ? 0 : 1;
+}
+
+static double ch_fixed(const or_ch *C, int a, const I64 *c) {
+  if (a == 0 && c[0] == 0 && !C->solid[ch_c(C, 0, c[1], c[2])]) return C->P.u_in;
+  return 0.0;
+}
+
+static double ch_area(const or_ch *C, int a, const I64 *c) {
+  if (a == 0) return C->d[1][c[1]] * C->d[2][c[2]];
+  if (a == 1) return C->d[0][c[0]] * C->d[2][c[2]];
+  return C->d[0][c[0]] * C->d[1][c[1]];
+}
+
+static double ch_get(const or_ch *C, const double *arr, int a, const I64 *c) { return arr[ch_f(C, a, c[0], c[1], c[2])]; }
+
+/* coefficients of the unknown face (a, c) at the frozen u^n: a[6] in order E W N S T B, a_P, the
+ * pressure source, and the six neighbour face positions (valid[n] = 0: value 0) */
+static void ch_coef(const or_ch *C, int a, const I64 *c, double *an, double *aP, double *bsrc, I64 (*nb)[3], int *valid) {
+  const double A = ch_area(C, a, c), da = C->h[a][c[a]], nu = C->nu;
+  for (int b = 0; b < 3; ++b) {
+    for (int hi = 1; hi >= 0; --hi) {
+      int n = 2 * b + (1 - hi);
+      double coef = 0.0;
+      I64 q[3] = {c[0], c[1], c[2]};
+      valid[n] = 0;
+      if (b == a) {
+        if (hi) {
+          q[a] += 1;
+          if (!(a == 0 && q[0] == C->N[0])) {
+            double F = 0.5 * (ch_get(C, C->U[a], a, c) + ch_get(C, C->U[a], a, q)) * A;
+            double Dd = nu * A / C->d[a][c[a]];
+            coef = Dd + maxd(-F, 0.0);
+            valid[n] = 1;
+          }
+        } else {
+          q[a] -= 1;
+          double F = 0.5 * (ch_get(C, C->U[a], a, q) + ch_get(C, C->U[a], a, c)) * A;
+          double Dd = nu * A / C->d[a][c[a] - 1];
+          coef = Dd + maxd(F, 0.0);
+          valid[n] = 1;
+        }
+      } else {
+        int o = 3 - a - b;
+        double ar = da * C->d[o][c[o]];
+        I64 flo[3] = {c[0], c[1], c[2]}, fhi[3] = {c[0], c[1], c[2]};  /* b-faces of the two cells */
+        flo[a] -= 1;
+        if (hi) { flo[b] += 1; fhi[b] += 1; }
+        double F = 0.5 * (ch_get(C, C->U[b], b, flo) * C->d[a][c[a] - 1] + ch_get(C, C->U[b], b, fhi) * C->d[a][c[a]]) *
+                   C->d[o][c[o]];
+        if (hi) {
+          if (c[b] + 1 == C->N[b]) {
+            if (b != 0) coef = nu * ar / C->h[b][C->N[b]] + maxd(-F, 0.0);
+          } else {
+            coef = nu * ar / C->h[b][c[b] + 1] + maxd(-F, 0.0);
+            q[b] += 1; valid[n] = 1;
+          }
+        } else {
+          if (c[b] == 0) coef = nu * ar / C->h[b][0] + maxd(F, 0.0);
+          else { coef = nu * ar / C->h[b][c[b]] + maxd(F, 0.0); q[b] -= 1; valid[n] = 1; }
+        }
+      }
+      an[n] = coef;
+      nb[n][0] = q[0]; nb[n][1] = q[1]; nb[n][2] = q[2];
+    }
+  }
+  *aP = an[0] + an[1] + an[2] + an[3] + an[4] + an[5];
+  I64 lo[3] = {c[0], c[1], c[2]};
+  lo[a] -= 1;
+  *bsrc = (C->p[ch_c(C, lo[0], lo[1], lo[2])] - C->p[ch_c(C, c[0], c[1], c[2])]) * A;
+}
+
+static double ch_nbsum(const or_ch *C, const double *arr, int a, const double *an, I64 (*nb)[3], const int *valid) {
+  double s = 0.0;
+  for (int n = 0; n < 6; ++n) s += an[n] * (valid[n] ? ch_get(C, arr, a, nb[n]) : 0.0);
+  return s;
+}
+
+static void ch_momentum(or_ch *C) {
+  double rs[3] = {0, 0, 0};
+  for (int sw = 0; sw < C->P.mom_sweeps; ++sw)
+    for (int color = 0; color < 2; ++color)
+      for (int a = 0; a < 3; ++a) {
+        const double *src = (sw == 0 && color == 0) ? C->U[a] : C->US[a];
+        for (I64 k = 0; k < ch_nf(C, a, 2); ++k) for (I64 j = 0; j < ch_nf(C, a, 1); ++j) for (I64 i = 0; i < ch_nf(C, a, 0); ++i) {
+          I64 c[3] = {i, j, k};
+          I64 f = ch_f(C, a, i, j, k);
+          int kind = ch_kind(C, a, c);
+          int mine = (int)((i + j + k) & 1) == color;
+          if (kind != 0) {
+            if (sw == 0 && color == 0) { C->US[a][f] = ch_fixed(C, a, c); C->D[a][f] = 0.0; }
+            continue;
+          }
+          double an[6], aP, bs;
+          I64 nb[6][3];
+          int valid[6];
+          if (!(mine || (sw == 0 && color == 0))) continue;
+          ch_coef(C, a, c, an, &aP, &bs, nb, valid);
+          double un = C->U[a][f];
+          if (sw == 0 && color == 0) {
+            double r = aP * un - (ch_nbsum(C, C->U[a], a, an, nb, valid) + bs);
+            rs[a] += r * r;
+          }
+          if (!mine) continue;
+          double apr = aP / C->P.alpha_u;
+          double rhs = ch_nbsum(C, src, a, an, nb, valid) + bs + (1.0 - C->P.alpha_u) * apr * un;
+          C->US[a][f] = rhs / apr;
+          if (sw == C->P.mom_sweeps - 1) C->D[a][f] = ch_area(C, a, c) / apr;
+        }
+      }
+  for (int a = 0; a < 3; ++a) C->res[a] = sqrt(rs[a]);
+}
+
+/* p' couplings per face and the mass imbalance b per cell; returns ||b|| */
+static double ch_passemble(or_ch *C) {
+  for (int a = 0; a < 3; ++a)
+    for (I64 k = 0; k < ch_nf(C, a, 2); ++k) for (I64 j = 0; j < ch_nf(C, a, 1); ++j) for (I64 i = 0; i < ch_nf(C, a, 0); ++i) {
+      I64 c[3] = {i, j, k}, f = ch_f(C, a, i, j, k);
+      int kind = ch_kind(C, a, c);
+      double v = 0.0;
+      if (kind == 0) v = ch_area(C, a, c) * C->D[a][f];
+      else if (kind == 2 && !C->solid[ch_c(C, i - 1, j, k)]) v = ch_area(C, a, c) * C->D[a][ch_f(C, a, i - 1, j, k)];
+      C->ac[a][f] = v;
+    }
+  double bb = 0.0;
+  for (I64 k = 0; k < C->N[2]; ++k) for (I64 j = 0; j < C->N[1]; ++j) for (I64 i = 0; i < C->N[0]; ++i) {
+    I64 c = ch_c(C, i, j, k);
+    if (C->solid[c]) { C->bc[c] = 0.0; continue; }
+    double ue = (i + 1 == C->N[0]) ? C->US[0][ch_f(C, 0, i, j, k)] : C->US[0][ch_f(C, 0, i + 1, j, k)];
+    double b = (C->US[0][ch_f(C, 0, i, j, k)] - ue) * (C->d[1][j] * C->d[2][k]) +
+               (C->US[1][ch_f(C, 1, i, j, k)] - C->US[1][ch_f(C, 1, i, j + 1, k)]) * (C->d[0][i] * C->d[2][k]) +
+               (C->US[2][ch_f(C, 2, i, j, k)] - C->US[2][ch_f(C, 2, i, j, k + 1)]) * (C->d[0][i] * C->d[1][j]);
+    C->bc[c] = b;
+    bb += b * b;
+  }
+  return sqrt(bb);
+}
+
+static void ch_apply(const or_ch *C, const double *x, double *y) {
+  for (I64 k = 0; k < C->N[2]; ++k) for (I64 j = 0; j < C->N[1]; ++j) for (I64 i = 0; i < C->N[0]; ++i) {
+    I64 c = ch_c(C, i, j, k);
+    if (C->solid[c]) { y[c] = 0.0; continue; }
+    double cw = C->ac[0][ch_f(C, 0, i, j, k)], ce = C->ac[0][ch_f(C, 0, i + 1, j, k)];
+    double cs = C->ac[1][ch_f(C, 1, i, j, k)], cn = C->ac[1][ch_f(C, 1, i, j + 1, k)];
+    double cb = C->ac[2][ch_f(C, 2, i, j, k)], cf = C->ac[2][ch_f(C, 2, i, j, k + 1)];
+    double diag = cw + ce + cs + cn + cb + cf;
+    double s = diag * x[c];
+    if (i > 0) s -= cw * x[c - 1];
+    if (i + 1 < C->N[0]) s -= ce * x[c + 1];
+    if (j > 0) s -= cs * x[c - C->N[0]];
+    if (j + 1 < C->N[1]) s -= cn * x[c + C->N[0]];
+    if (k > 0) s -= cb * x[c - C->N[0] * C->N[1]];
+    if (k + 1 < C->N[2]) s -= cf * x[c + C->N[0] * C->N[1]];
+    y[c] = s;
+  }
+}
+
+/* CG on the p' system from x = 0, stop when ||r|| / ||b|| < tol */
+static void ch_pcg(or_ch *C) {
+  I64 N = C->N[0] * C->N[1] * C->N[2];
+  double *r = malloc(8 * N), *p = malloc(8 * N), *s = malloc(8 * N);
+  double bb = 0.0;
+  for (I64 c = 0; c < N; ++c) { C->pp[c] = 0.0; r[c] = C->bc[c]; p[c] = r[c]; bb += r[c] * r[c]; }
+  double rr = bb;
+  int it = 0;
+  while (bb > 0 && it < C->P.p_maxiter && rr / bb >= C->P.p_tol * C->P.p_tol) {
+    it++;
+    ch_apply(C, p, s);
+    double sp = 0.0;
+    for (I64 c = 0; c < N; ++c) sp += s[c] * p[c];
+    double alpha = rr / sp, rr1 = 0.0;
+    for (I64 c = 0; c < N; ++c) { C->pp[c] += alpha * p[c]; r[c] -= alpha * s[c]; rr1 += r[c] * r[c]; }
+    double beta = rr1 / rr;
+    rr = rr1;
+    for (I64 c = 0; c < N; ++c) p[c] = r[c] + beta * p[c];
+  }
+  C->pcg_iters = it;
+  C->pcg_relres = bb > 0 ? sqrt(rr / bb) : 0.0;
+  free(r); free(p); free(s);
+}
+
+static void ch_correct(or_ch *C) {
+  for (int a = 0; a < 3; ++a)
+    for (I64 k = 0; k < ch_nf(C, a, 2); ++k) for (I64 j = 0; j < ch_nf(C, a, 1); ++j) for (I64 i = 0; i < ch_nf(C, a, 0); ++i) {
+      I64 c[3] = {i, j, k}, f = ch_f(C, a, i, j, k);
+      int kind = ch_kind(C, a, c);
+      if (kind == 1) { C->U[a][f] = ch_fixed(C, a, c); continue; }
+      if (kind == 2) {
+        I64 cl = ch_c(C, i - 1, j, k), fl = ch_f(C, 0, i - 1, j, k);
+        C->U[a][f] = C->solid[cl] ? 0.0 : C->US[0][fl] + C->D[0][fl] * C->pp[cl];
+        continue;
+      }
+      I64 lo[3] = {i, j, k};
+      lo[a] -= 1;
+      C->U[a][f] = C->US[a][f] + C->D[a][f] * (C->pp[ch_c(C, lo[0], lo[1], lo[2])] - C->pp[ch_c(C, i, j, k)]);
+    }
+  I64 N = C->N[0] * C->N[1] * C->N[2];
+  for (I64 c = 0; c < N; ++c)
+    if (!C->solid[c]) C->p[c] = C->p[c] + C->P.alpha_p * C->pp[c];
+}
+
+static or_cht ch_cht(const or_ch *C) {
+  or_cht H;
+  H.Nx = C->N[0]; H.Ny = C->N[1]; H.Nz = C->N[2];
+  H.xs = C->pts[0]; H.ys = C->pts[1]; H.zs = C->pts[2];
+  H.solid = C->solid; H.region = C->region; H.kcell = C->kcell; H.qcell = C->qcell;
+  H.ug = C->U[0]; H.vg = C->U[1]; H.wg = C->U[2];
+  H.Tb = C->P.t_in; H.bc = 1;
+  return H;
+}
+
+static void ch_energy(or_ch *C) {
+  I64 N = C->N[0] * C->N[1] * C->N[2];
+  or_cht H = ch_cht(C);
+  double *b = malloc(8 * N), *Tt = malloc(8 * N);
+  cht_rhs(&H, b);
+  memcpy(Tt, C->T, 8 * N);
+  double rel, r0;
+  C->t_iters = cht_bicgstab(&H, 0, b, Tt, C->P.t_tol, C->P.t_maxiter, &rel, 1, &r0);
+  C->res[4] = r0;
+  for (I64 c = 0; c < N; ++c) C->T[c] = C->T[c] + C->P.alpha_t * (Tt[c] - C->T[c]);
+  free(b); free(Tt);
+}
+
+void or_ch_params_default(or_ch_params *P) {
+  P->re = 100; P->pr = 0.71; P->u_in = 1.0; P->t_in = 0.0;
+  P->alpha_u = 0.7; P->alpha_p = 0.3; P->alpha_t = 0.9;
+  P->mom_sweeps = 2; P->p_tol = 1e-8; P->p_maxiter = 1000; P->t_tol = 1e-2; P->t_maxiter = 200;
+}
+
+or_ch *or_ch_create(const char *deck, const or_ch_params *P) {
+  or_deck dk;
+  if (or_deck_parse(deck, &dk) != 0) return NULL;
+  or_mesh m;
+  or_mesh_build(&dk, &m);
+  or_ch *C = calloc(1, sizeof(or_ch));
+  C->P = *P;
+  C->N[0] = m.Nx; C->N[1] = m.Ny; C->N[2] = m.Nz;
+  const double *src[3] = {dk.xs, dk.ys, dk.zs};
+  for (int a = 0; a < 3; ++a) {
+    I64 n = C->N[a];
+    C->pts[a] = malloc(8 * (n + 1)); memcpy(C->pts[a], src[a], 8 * (n + 1));
+    C->d[a] = malloc(8 * n); C->h[a] = malloc(8 * (n + 1));
+    for (I64 i = 0; i < n; ++i) C->d[a][i] = C->pts[a][i + 1] - C->pts[a][i];
+    C->h[a][0] = 0.5 * C->d[a][0];
+    C->h[a][n] = 0.5 * C->d[a][n - 1];
+    for (I64 i = 1; i < n; ++i) C->h[a][i] = 0.5 * (C->pts[a][i] + C->pts[a][i + 1]) - 0.5 * (C->pts[a][i - 1] + C->pts[a][i]);
+  }
+  I64 N = C->N[0] * C->N[1] * C->N[2];
+  C->solid = malloc(N); memcpy(C->solid, m.ctype, N);
+  C->region = malloc(4 * N);
+  for (I64 c = 0; c < N; ++c) C->region[c] = m.ctype[c] ? m.region[c] : -1;
+  C->nreg = m.nsolid_regions;
+  C->kreg = malloc(8 * (C->nreg + 1));
+  for (int r = 0; r < C->nreg; ++r) C->kreg[r] = 100.0;
+  C->qcell = calloc(N, 8);
+  for (int a = 0; a < 3; ++a) {
+    I64 nf = ch_nf(C, a, 0) * ch_nf(C, a, 1) * ch_nf(C, a, 2);
+    C->U[a] = calloc(nf, 8); C->US[a] = calloc(nf, 8); C->D[a] = calloc(nf, 8); C->ac[a] = calloc(nf, 8);
+  }
+  C->p = calloc(N, 8); C->pp = calloc(N, 8); C->T = calloc(N, 8); C->kcell = calloc(N, 8); C->bc = calloc(N, 8);
+  double ly = C->pts[1][C->N[1]] - C->pts[1][0];
+  C->nu = P->u_in * ly / P->re;
+  C->kf = C->nu / P->pr;
+  or_mesh_free(&m);
+  or_deck_free(&dk);
+  return C;
+}
+
+int or_ch_nreg(const or_ch *C) { return C->nreg; }
+
+/* k_ratio per solid region, q per cell (solid cells only) */
+void or_ch_set_solid(or_ch *C, const double *kreg, const double *qcell) {
+  I64 N = C->N[0] * C->N[1] * C->N[2];
+  for (int r = 0; r < C->nreg; ++r) C->kreg[r] = kreg[r];
+  for (I64 c = 0; c < N; ++c) C->qcell[c] = C->solid[c] ? qcell[c] : 0.0;
+}
+
+void or_ch_init(or_ch *C) {
+  for (int a = 0; a < 3; ++a)
+    for (I64 k = 0; k < ch_nf(C, a, 2); ++k) for (I64 j = 0; j < ch_nf(C, a, 1); ++j) for (I64 i = 0; i < ch_nf(C, a, 0); ++i) {
+      I64 c[3] = {i, j, k}, f = ch_f(C, a, i, j, k);
+      int kind = ch_kind(C, a, c);
+      double v = 0.0;
+      if (a == 0) {
+        if (kind == 0) v = C->P.u_in;
+        else if (kind == 1) v = ch_fixed(C, a, c);
+        else v = C->solid[ch_c(C, i - 1, j, k)] ? 0.0 : C->P.u_in;
+      }
+      C->U[a][f] = v; C->US[a][f] = v; C->D[a][f] = 0.0;
+    }
+  I64 N = C->N[0] * C->N[1] * C->N[2];
+  for (I64 c = 0; c < N; ++c) {
+    C->p[c] = 0.0; C->pp[c] = 0.0; C->T[c] = C->P.t_in;
+    C->kcell[c] = C->solid[c] ? C->kreg[C->region[c]] * C->kf : C->kf;
+  }
+  C->iter = 0;
+  for (int x = 0; x < 5; ++x) { C->res[x] = 0; C->norm[x] = 0; }
+  C->glob = 1.0;
+}
+
+void or_ch_step(or_ch *C, int n, int do_pressure, int do_energy) {
+  for (int s = 0; s < n; ++s) {
+    ch_momentum(C);
+    C->res[3] = ch_passemble(C);
+    if (do_pressure) ch_pcg(C);
+    else { I64 N = C->N[0] * C->N[1] * C->N[2]; for (I64 c = 0; c < N; ++c) C->pp[c] = 0.0; C->pcg_iters = 0; }
+    ch_correct(C);
+    if (do_energy) ch_energy(C);
+    else { C->res[4] = 0.0; C->t_iters = 0; }
+    C->iter++;
+    double g = 0.0;
+    for (int x = 0; x < 5; ++x) {
+      if (C->iter <= 5 && C->res[x] > C->norm[x]) C->norm[x] = C->res[x];
+      double r = C->res[x] / (C->norm[x] > 1e-300 ? C->norm[x] : 1e-300);
+      if (r > g) g = r;
+    }
+    C->glob = g;
+  }
+}
+
+/* field ids: 0..2 u v w (faces), 3 p, 4 T, 5..7 u* v* w*, 8..10 d_u d_v d_w, 11 p' */
+int or_ch_get(const or_ch *C, int fid, double *out, I64 n) {
+  const double *src;
+  I64 cnt;
+  I64 N = C->N[0] * C->N[1] * C->N[2];
+  if (fid >= 0 && fid < 3) { src = C->U[fid]; cnt = ch_nf(C, fid, 0) * ch_nf(C, fid, 1) * ch_nf(C, fid, 2); }
+  else if (fid == 3) { src = C->p; cnt = N; }
+  else if (fid == 4) { src = C->T; cnt = N; }
+  else if (fid >= 5 && fid < 8) { int a = fid - 5; src = C->US[a]; cnt = ch_nf(C, a, 0) * ch_nf(C, a, 1) * ch_nf(C, a, 2); }
+  else if (fid >= 8 && fid < 11) { int a = fid - 8; src = C->D[a]; cnt = ch_nf(C, a, 0) * ch_nf(C, a, 1) * ch_nf(C, a, 2); }
+  else if (fid == 11) { src = C->pp; cnt = N; }
+  else return -1;
+  if (n != cnt) return -2;
+  memcpy(out, src, 8 * cnt);
+  return 0;
+}
+
+int or_ch_set(or_ch *C, int fid, const double *in, I64 n) {
+  double *dst;
+  I64 cnt;
+  I64 N = C->N[0] * C->N[1] * C->N[2];
+  if (fid >= 0 && fid < 3) { dst = C->U[fid]; cnt = ch_nf(C, fid, 0) * ch_nf(C, fid, 1) * ch_nf(C, fid, 2); }
+  else if (fid == 3) { dst = C->p; cnt = N; }
+  else if (fid == 4) { dst = C->T; cnt = N; }
+  else return -1;
+  if (n != cnt) return -2;
+  memcpy(dst, in, 8 * cnt);
+  return 0;
+}
+
+/* res[0..4] (u v w continuity energy), norm[0..4], global, iter, pcg iters, energy iters */
+void or_ch_stats(const or_ch *C, double *res5, double *norm5, double *glob, int *iout3) {
+  for (int x = 0; x < 5; ++x) { res5[x] = C->res[x]; norm5[x] = C->norm[x]; }
+  *glob = C->glob;
+  iout3[0] = C->iter; iout3[1] = C->pcg_iters; iout3[2] = C->t_iters;
+}
+
+void or_ch_destroy(or_ch *C) {
+  if (!C) return;
+  for (int a = 0; a < 3; ++a) { free(C->pts[a]); free(C->d[a]); free(C->h[a]); free(C->U[a]); free(C->US[a]); free(C->D[a]); free(C->ac[a]); }
+  free(C->solid); free(C->region); free(C->kreg); free(C->qcell);
+  free(C->p); free(C->pp); free(C->T); free(C->kcell); free(C->bc);
+  free(C);
+}
+
+void or_ch_dims(const or_ch *C, I64 *out3) { out3[0] = C->N[0]; out3[1] = C->N[1]; out3[2] = C->N[2]; }

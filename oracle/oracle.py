@@ -214,10 +214,10 @@ class _Cht(ctypes.Structure):
                 ("xs", ctypes.c_void_p), ("ys", ctypes.c_void_p), ("zs", ctypes.c_void_p),
                 ("solid", ctypes.c_void_p), ("region", ctypes.c_void_p), ("kcell", ctypes.c_void_p),
                 ("qcell", ctypes.c_void_p), ("ug", ctypes.c_void_p), ("vg", ctypes.c_void_p), ("wg", ctypes.c_void_p),
-                ("Tb", ctypes.c_double)]
+                ("Tb", ctypes.c_double), ("bc", ctypes.c_int)]
 
 
-def cht_solve(xs, ys, zs, ctype, region, kcell, qcell, ug, vg, wg, Tb=293.0, tol=1e-13, maxiter=20000, nreg=0):
+def cht_solve(xs, ys, zs, ctype, region, kcell, qcell, ug, vg, wg, Tb=293.0, tol=1e-13, maxiter=20000, nreg=0, bc=0):
     """Oracle forward + adjoint of the monolithic conjugate-heat-transfer
     energy equation (hs_oracle.c: or_cht_forward / or_cht_adjoint).
     Returns dict(T, J, dJdq, dJdk, iters)."""
@@ -227,7 +227,7 @@ def cht_solve(xs, ys, zs, ctype, region, kcell, qcell, ug, vg, wg, Tb=293.0, tol
                                                       (qcell, np.float64), (ug, np.float64), (vg, np.float64),
                                                       (wg, np.float64)]]
     Nx, Ny, Nz = len(xs) - 1, len(ys) - 1, len(zs) - 1
-    H = _Cht(Nx, Ny, Nz, *[a.ctypes.data for a in keep], Tb)
+    H = _Cht(Nx, Ny, Nz, *[a.ctypes.data for a in keep], Tb, bc)
     dp = ctypes.POINTER(ctypes.c_double)
     L.or_cht_forward.restype = ctypes.c_int
     L.or_cht_forward.argtypes = [ctypes.POINTER(_Cht), dp, ctypes.c_double, ctypes.c_int, dp, dp]
@@ -244,3 +244,92 @@ def cht_solve(xs, ys, zs, ctype, region, kcell, qcell, ug, vg, wg, Tb=293.0, tol
     it2 = L.or_cht_adjoint(ctypes.byref(H), T.ctypes.data_as(dp), lam.ctypes.data_as(dp), dJdq.ctypes.data_as(dp),
                            dJdk.ctypes.data_as(dp), nreg, tol, maxiter, ctypes.byref(rr))
     return {"T": T, "J": J.value, "dJdq": dJdq, "dJdk": dJdk[:nreg], "iters": (it1, it2)}
+
+
+class ChParams(ctypes.Structure):
+    """or_ch_params (hs_oracle.c): the channel conjugate-heat-transfer case."""
+    _fields_ = [("re", ctypes.c_double), ("pr", ctypes.c_double), ("u_in", ctypes.c_double), ("t_in", ctypes.c_double),
+                ("alpha_u", ctypes.c_double), ("alpha_p", ctypes.c_double), ("alpha_t", ctypes.c_double),
+                ("mom_sweeps", ctypes.c_int), ("p_tol", ctypes.c_double), ("p_maxiter", ctypes.c_int),
+                ("t_tol", ctypes.c_double), ("t_maxiter", ctypes.c_int)]
+
+    @classmethod
+    def default(cls, **kw):
+        P = cls()
+        lib().or_ch_params_default(ctypes.byref(P))
+        for k, v in kw.items():
+            setattr(P, k, v)
+        return P
+
+
+CH_FIELDS = {"u": 0, "v": 1, "w": 2, "p": 3, "T": 4, "u_star": 5, "v_star": 6, "w_star": 7, "d_u": 8, "d_v": 9,
+             "d_w": 10, "p_prime": 11}
+
+
+class ChannelCase:
+    """Oracle of the channel conjugate-heat-transfer SIMPLE iteration
+    (hs_oracle.c: or_ch_*): inlet plug flow, zero-gradient outlet, solid
+    blocks with a heat source and a conductivity ratio."""
+
+    def __init__(self, deck, **params):
+        L = lib()
+        L.or_ch_create.restype = ctypes.c_void_p
+        L.or_ch_create.argtypes = [ctypes.c_char_p, ctypes.POINTER(ChParams)]
+        L.or_ch_nreg.argtypes = [ctypes.c_void_p]
+        L.or_ch_set_solid.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+        L.or_ch_init.argtypes = [ctypes.c_void_p]
+        L.or_ch_step.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        L.or_ch_get.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int64]
+        L.or_ch_set.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int64]
+        L.or_ch_stats.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+        L.or_ch_destroy.argtypes = [ctypes.c_void_p]
+        self.L = L
+        self.params = ChParams.default(**params)
+        self.h = L.or_ch_create(deck.encode(), ctypes.byref(self.params))
+        if not self.h:
+            raise ValueError("deck rejected")
+        d = np.zeros(3, np.int64)
+        L.or_ch_dims.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        L.or_ch_dims(self.h, d.ctypes.data)
+        self.dims = tuple(int(v) for v in d)
+        self.nreg = L.or_ch_nreg(self.h)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.L.or_ch_destroy(self.h)
+            self.h = None
+
+    def size(self, name):
+        Nx, Ny, Nz = self.dims
+        f = CH_FIELDS[name]
+        if f in (3, 4, 11):
+            return Nx * Ny * Nz
+        a = f % 3 if f < 3 else (f - 5) % 3
+        return (Nx + (a == 0)) * (Ny + (a == 1)) * (Nz + (a == 2))
+
+    def set_solid(self, k_region, q_cell):
+        k = np.ascontiguousarray(k_region, np.float64)
+        q = np.ascontiguousarray(q_cell, np.float64)
+        assert k.size == self.nreg and q.size == self.dims[0] * self.dims[1] * self.dims[2]
+        self.L.or_ch_set_solid(self.h, k.ctypes.data, q.ctypes.data)
+
+    def init(self):
+        self.L.or_ch_init(self.h)
+
+    def step(self, n=1, pressure=True, energy=True):
+        self.L.or_ch_step(self.h, n, int(pressure), int(energy))
+
+    def field(self, name):
+        out = np.empty(self.size(name))
+        assert self.L.or_ch_get(self.h, CH_FIELDS[name], out.ctypes.data, out.size) == 0
+        return out
+
+    def set_field(self, name, arr):
+        a = np.ascontiguousarray(arr, np.float64)
+        assert self.L.or_ch_set(self.h, CH_FIELDS[name], a.ctypes.data, a.size) == 0
+
+    def stats(self):
+        res, norm, glob, it = np.zeros(5), np.zeros(5), ctypes.c_double(), np.zeros(3, np.int32)
+        self.L.or_ch_stats(self.h, res.ctypes.data, norm.ctypes.data, ctypes.byref(glob), it.ctypes.data)
+        return {"res": res, "norm": norm, "global": glob.value, "iter": int(it[0]), "pcg_iters": int(it[1]),
+                "t_iters": int(it[2])}

@@ -1,0 +1,122 @@
+"""Channel conjugate heat transfer (hs_channel_*) on the GPU against the CPU
+oracle (oracle/hs_oracle.c, or_ch_*): the momentum sweeps bit for bit, full
+outer steps with tight inner tolerances, the converged state at a global
+residual of 1e-6, the mixed-precision form against FP64, mass conservation,
+and the energy adjoint on the converged flow."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+FACE = ["u", "v", "w"]
+
+
+def _deck(nx=24, ny=12, nz=12, blocks=((9, 12, 1, 4, 5, 8),)):
+    from hsolver_b200 import cases
+    return cases.channel(nx, ny, nz, list(blocks))
+
+
+def _pair(deck, **kw):
+    import hsolver_b200
+    from oracle import oracle
+    g = hsolver_b200.Channel(deck, **kw)
+    okw = {k: v for k, v in kw.items() if k in ("re", "pr", "u_in", "t_in", "alpha_u", "alpha_p", "alpha_t",
+                                                 "mom_sweeps", "p_tol", "p_maxiter", "t_tol", "t_maxiter")}
+    o = oracle.ChannelCase(deck, **okw)
+    n = o.dims[0] * o.dims[1] * o.dims[2]
+    ctype, region = oracle.OracleCase(deck).cell_types()
+    rng = np.random.default_rng(5)
+    k = rng.uniform(10.0, 1000.0, o.nreg)
+    q = np.where(ctype == 1, rng.uniform(0.5, 2.0, n), 0.0)
+    g.set_solid(k, q)
+    o.set_solid(k, q)
+    g.init()
+    o.init()
+    return g, o, ctype
+
+
+def _rel(a, b):
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
+
+
+def test_momentum_sweeps_bit_exact():
+    g, o, _ = _pair(_deck(), re=100.0)
+    for step in range(4):
+        gs = g.step(1, flags=3)
+        o.step(1, pressure=False, energy=False)
+        for name in FACE + ["u_star", "v_star", "w_star", "d_u", "d_v", "d_w", "p"]:
+            a, b = g.field(name), o.field(name)
+            assert np.array_equal(a, b), (step, name, np.abs(a - b).max())
+        ores = o.stats()["res"]
+        for x in range(3):
+            assert abs(gs["res"][x] - ores[x]) <= 1e-12 * max(ores[x], 1e-300)
+
+
+@pytest.mark.parametrize("precond", [0, 1])
+def test_outer_steps_match_oracle(precond):
+    g, o, _ = _pair(_deck(), re=100.0, p_tol=1e-13, p_maxiter=5000, t_tol=1e-13, t_maxiter=5000, p_precond=precond)
+    for step in range(5):
+        gs = g.step(1)
+        o.step(1)
+        os_ = o.stats()
+        for name in FACE + ["p", "T", "p_prime"]:
+            assert _rel(g.field(name), o.field(name)) < 1e-9, (step, name)
+        for x in range(5):
+            assert abs(gs["res"][x] - os_["res"][x]) <= 1e-8 * max(os_["res"][x], 1e-300), (step, x)
+    if precond:
+        assert gs["pcg_iters"] * 4 < os_["pcg_iters"]  # the V-cycle preconditioner pays
+
+
+def test_converged_state_matches_oracle_and_conserves_mass():
+    deck = _deck()
+    g, o, ctype = _pair(deck, re=100.0)
+    ok, steps, st = g.solve_to(1e-6, 2000)
+    assert ok, st
+    for _ in range(steps):
+        o.step(1)
+    assert o.stats()["global"] <= 1e-6 * 1.5
+    for name in FACE + ["p", "T"]:
+        assert _rel(g.field(name), o.field(name)) < 1e-6, name
+    # inflow = outflow (per unit area the faces are uniform here)
+    Nx, Ny, Nz = o.dims
+    u = g.field("u").reshape(Nz, Ny, Nx + 1)
+    assert abs(u[:, :, 0].sum() - u[:, :, -1].sum()) <= 1e-6 * u[:, :, 0].sum()
+
+
+def test_mixed_precision_against_fp64():
+    deck = _deck()
+    g64, _, _ = _pair(deck, re=100.0)
+    g32, _, _ = _pair(deck, re=100.0, precision=1)
+    ok64, s64, _ = g64.solve_to(1e-6, 2000)
+    ok32, s32, st = g32.solve_to(1e-6, 2000)
+    assert ok64 and ok32, st
+    for name in FACE + ["p", "T"]:
+        assert _rel(g32.field(name), g64.field(name)) < 2e-5, name
+
+
+def test_adjoint_on_converged_flow_matches_oracle():
+    import ctypes
+    from oracle import oracle
+    deck = _deck()
+    g, o, ctype = _pair(deck, re=100.0)
+    g.solve_to(1e-6, 2000)
+    J, dq, dk, info = g.adjoint(tol=1e-12)
+    oc = oracle.OracleCase(deck)
+    _, region = oc.cell_types()
+    grids = []
+    for axis in range(3):
+        a = np.empty(oc.dims[axis] + 1)
+        oracle.lib().or_get_grid(oc.h, axis, a.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), a.size)
+        grids.append(a)
+    rng = np.random.default_rng(5)
+    n = ctype.size
+    k = rng.uniform(10.0, 1000.0, g.nblocks)
+    q = np.where(ctype == 1, rng.uniform(0.5, 2.0, n), 0.0)
+    kf = (1.0 * 1.0 / 100.0) / 0.71
+    kcell = np.where(ctype == 1, k[np.maximum(region, 0)] * kf, kf)
+    ref = oracle.cht_solve(*grids, ctype, region, kcell, q, g.field("u"), g.field("v"), g.field("w"), Tb=0.0, tol=1e-12,
+                           nreg=g.nblocks, bc=1)
+    assert abs(J - ref["J"]) <= 1e-10 * ref["J"]
+    assert _rel(dq, ref["dJdq"]) < 1e-8
+    assert _rel(dk, ref["dJdk"]) < 1e-8
+    assert info["adj_iters"] <= 1.5 * info["fwd_iters"] + 5
