@@ -58,23 +58,36 @@ constexpr int kT = 256;
 constexpr int kMaxLv = 16;
 constexpr int kMaxCoarse = 64;
 
+// Device view.  U and p are the FP64 iterate in both forms.  In the FP64 form
+// C aliases U and S holds u*; in the mixed form C is an FP32 copy of U (the
+// coefficient arithmetic reads it), S holds the correction delta = u* - u^n
+// swept in FP32, and Q the FP64 residual of the relaxed equation at u^n
+// rounded to FP32 (the right-hand side of the delta equation): iterative
+// refinement, so the FP32 rounding scales with delta, which vanishes at the
+// fixed point.
 template <class R>
 struct ChDev {
   int N0, N1, N2;
   const R *d0, *d1, *d2;      // cell widths
   const R *h0, *h1, *h2;      // centre distances, [0] and [N] half widths
   const uint8_t *solid;       // N0 N1 N2
-  R *U0, *U1, *U2;            // u^n (after correction: the new iterate)
-  R *S0, *S1, *S2;            // u*
+  double *U0, *U1, *U2;       // u^n (after correction: the new iterate)
+  R *C0, *C1, *C2;            // coefficient copy of U
+  R *S0, *S1, *S2;            // u* (FP64) or delta (mixed)
+  R *Q0, *Q1, *Q2;            // mixed: right-hand side of the delta sweeps
   R *D0, *D1, *D2;            // d = A / (a_P / alpha_u)
-  R *p;                       // pressure, cells
-  double *Ud0, *Ud1, *Ud2;    // FP64 copy of the corrected velocities (mixed form), energy input
+  double *p;                  // pressure, cells
   R nu, au, u_in;
   double ap;                  // alpha_p
 };
 
-template <int A, class R> __device__ __forceinline__ R *Uarr(const ChDev<R> &H) { return A == 0 ? H.U0 : A == 1 ? H.U1 : H.U2; }
+__host__ __device__ constexpr bool is_mixed(float) { return true; }
+__host__ __device__ constexpr bool is_mixed(double) { return false; }
+
+template <int A, class R> __device__ __forceinline__ double *Uarr(const ChDev<R> &H) { return A == 0 ? H.U0 : A == 1 ? H.U1 : H.U2; }
+template <int A, class R> __device__ __forceinline__ R *Carr(const ChDev<R> &H) { return A == 0 ? H.C0 : A == 1 ? H.C1 : H.C2; }
 template <int A, class R> __device__ __forceinline__ R *Sarr(const ChDev<R> &H) { return A == 0 ? H.S0 : A == 1 ? H.S1 : H.S2; }
+template <int A, class R> __device__ __forceinline__ R *Qarr(const ChDev<R> &H) { return A == 0 ? H.Q0 : A == 1 ? H.Q1 : H.Q2; }
 template <int A, class R> __device__ __forceinline__ R *Darr(const ChDev<R> &H) { return A == 0 ? H.D0 : A == 1 ? H.D1 : H.D2; }
 template <int A, class R> __device__ __forceinline__ R wid(const ChDev<R> &H, int i) { return A == 0 ? H.d0[i] : A == 1 ? H.d1[i] : H.d2[i]; }
 template <int A, class R> __device__ __forceinline__ R ctr(const ChDev<R> &H, int i) { return A == 0 ? H.h0[i] : A == 1 ? H.h1[i] : H.h2[i]; }
@@ -116,40 +129,39 @@ template <int A, class R>
 __device__ __forceinline__ int fidx3(const ChDev<R> &H, const int (&c)[3]) { return fidx<A>(H, c[0], c[1], c[2]); }
 
 // one stencil term (neighbour across axis B, high side when HI) of the unknown
-// face (A, c): coefficient, neighbour value from src and (resid) from u^n
+// face (A, c): coefficient at the frozen iterate and the neighbour's face
+// index (-1: the neighbour value is 0 or the term is dropped)
 template <int A, int B, int HI, class R>
-__device__ __forceinline__ void term(const ChDev<R> &H, const int (&c)[3], R Ar, R da, const R *src, bool resid, R &coef,
-                                     R &val, R &valn) {
-  coef = R(0); val = R(0); valn = R(0);
-  const R *UA = Uarr<A>(H);
+__device__ __forceinline__ void term(const ChDev<R> &H, const int (&c)[3], R Ar, R da, R &coef, int &nb) {
+  coef = R(0);
+  nb = -1;
+  const R *CA = Carr<A>(H);
   if constexpr (B == A) {
     int q[3] = {c[0], c[1], c[2]};
     if (HI) {
       q[A] += 1;
       if (!(A == 0 && q[0] == H.N0)) {
-        const R F = R(0.5) * (UA[fidx3<A>(H, c)] + UA[fidx3<A>(H, q)]) * Ar;
+        const R F = R(0.5) * (CA[fidx3<A>(H, c)] + CA[fidx3<A>(H, q)]) * Ar;
         const R Dd = H.nu * Ar / wid<A>(H, c[A]);
         coef = Dd + rmax0(-F);
-        val = src[fidx3<A>(H, q)];
-        if (resid) valn = UA[fidx3<A>(H, q)];
+        nb = fidx3<A>(H, q);
       }
     } else {
       q[A] -= 1;
-      const R F = R(0.5) * (UA[fidx3<A>(H, q)] + UA[fidx3<A>(H, c)]) * Ar;
+      const R F = R(0.5) * (CA[fidx3<A>(H, q)] + CA[fidx3<A>(H, c)]) * Ar;
       const R Dd = H.nu * Ar / wid<A>(H, c[A] - 1);
       coef = Dd + rmax0(F);
-      val = src[fidx3<A>(H, q)];
-      if (resid) valn = UA[fidx3<A>(H, q)];
+      nb = fidx3<A>(H, q);
     }
   } else {
     constexpr int O = 3 - A - B;
-    const R *UB = Uarr<B>(H);
+    const R *CB = Carr<B>(H);
     const R wo = wid<O>(H, c[O]);
     const R ar = da * wo;
     int flo[3] = {c[0], c[1], c[2]}, fhi[3] = {c[0], c[1], c[2]};
     flo[A] -= 1;
     if (HI) { flo[B] += 1; fhi[B] += 1; }
-    const R F = R(0.5) * (UB[fidx3<B>(H, flo)] * wid<A>(H, c[A] - 1) + UB[fidx3<B>(H, fhi)] * wid<A>(H, c[A])) * wo;
+    const R F = R(0.5) * (CB[fidx3<B>(H, flo)] * wid<A>(H, c[A] - 1) + CB[fidx3<B>(H, fhi)] * wid<A>(H, c[A])) * wo;
     int q[3] = {c[0], c[1], c[2]};
     if (HI) {
       if (c[B] + 1 == ncell<B>(H)) {
@@ -157,8 +169,7 @@ __device__ __forceinline__ void term(const ChDev<R> &H, const int (&c)[3], R Ar,
       } else {
         coef = H.nu * ar / ctr<B>(H, c[B] + 1) + rmax0(-F);
         q[B] += 1;
-        val = src[fidx3<A>(H, q)];
-        if (resid) valn = UA[fidx3<A>(H, q)];
+        nb = fidx3<A>(H, q);
       }
     } else {
       if (c[B] == 0) {
@@ -166,48 +177,80 @@ __device__ __forceinline__ void term(const ChDev<R> &H, const int (&c)[3], R Ar,
       } else {
         coef = H.nu * ar / ctr<B>(H, c[B]) + rmax0(F);
         q[B] -= 1;
-        val = src[fidx3<A>(H, q)];
-        if (resid) valn = UA[fidx3<A>(H, q)];
+        nb = fidx3<A>(H, q);
       }
     }
   }
 }
 
-// momentum work on face (A, c): residual at u^n (resid), relaxed GS update (upd), d (last)
+// momentum work on the unknown face (A, c): residual at u^n (first pass),
+// relaxed Gauss-Seidel update (upd), d (last sweep)
 template <int A, class R>
-__device__ __forceinline__ void mom_face(const ChDev<R> &H, const int (&c)[3], bool first, bool upd, bool resid,
-                                         bool last, double &racc) {
+__device__ __forceinline__ void mom_face(const ChDev<R> &H, const int (&c)[3], bool first, bool upd, bool last,
+                                         double &racc) {
   const int f = fidx3<A>(H, c);
   const R Ar = face_area<A>(H, c);
   const R da = ctr<A>(H, c[A]);
-  const R *src = first ? Uarr<A>(H) : Sarr<A>(H);
-  R an[6], v[6], vn[6];
-  term<A, 0, 1>(H, c, Ar, da, src, resid, an[0], v[0], vn[0]);
-  term<A, 0, 0>(H, c, Ar, da, src, resid, an[1], v[1], vn[1]);
-  term<A, 1, 1>(H, c, Ar, da, src, resid, an[2], v[2], vn[2]);
-  term<A, 1, 0>(H, c, Ar, da, src, resid, an[3], v[3], vn[3]);
-  term<A, 2, 1>(H, c, Ar, da, src, resid, an[4], v[4], vn[4]);
-  term<A, 2, 0>(H, c, Ar, da, src, resid, an[5], v[5], vn[5]);
+  R an[6];
+  int nb[6];
+  term<A, 0, 1>(H, c, Ar, da, an[0], nb[0]);
+  term<A, 0, 0>(H, c, Ar, da, an[1], nb[1]);
+  term<A, 1, 1>(H, c, Ar, da, an[2], nb[2]);
+  term<A, 1, 0>(H, c, Ar, da, an[3], nb[3]);
+  term<A, 2, 1>(H, c, Ar, da, an[4], nb[4]);
+  term<A, 2, 0>(H, c, Ar, da, an[5], nb[5]);
   const R aP = an[0] + an[1] + an[2] + an[3] + an[4] + an[5];
-  int lo[3] = {c[0], c[1], c[2]};
-  lo[A] -= 1;
-  const R bs = (H.p[cidx(H, lo[0], lo[1], lo[2])] - H.p[cidx(H, c[0], c[1], c[2])]) * Ar;
-  const R un = Uarr<A>(H)[f];
-  if (resid) {
-    double s = 0.0;
+  const R apr = aP / H.au;
+  const double *UA = Uarr<A>(H);
+  R *SA = Sarr<A>(H);
+  if constexpr (!is_mixed(R())) {
+    // u* in place: a_P/alpha u_P = sum a_nb u_nb + b + (1 - alpha) a_P/alpha u^n_P
+    int lo[3] = {c[0], c[1], c[2]};
+    lo[A] -= 1;
+    const R bs = (H.p[cidx(H, lo[0], lo[1], lo[2])] - H.p[cidx(H, c[0], c[1], c[2])]) * Ar;
+    const R un = UA[f];
+    const R *src = first ? (const R *)UA : (const R *)SA;
+    if (first) {
+      double s = 0.0;
 #pragma unroll
-    for (int n = 0; n < 6; ++n) s += (double)an[n] * (double)vn[n];
-    const double r = (double)aP * (double)un - (s + (double)bs);
-    racc += r * r;
-  }
-  if (upd) {
-    const R apr = aP / H.au;
-    R s = R(0);
+      for (int n = 0; n < 6; ++n) s += (double)an[n] * (nb[n] >= 0 ? UA[nb[n]] : 0.0);
+      const double r = (double)aP * (double)un - (s + (double)bs);
+      racc += r * r;
+    }
+    if (upd) {
+      R s = R(0);
 #pragma unroll
-    for (int n = 0; n < 6; ++n) s += an[n] * v[n];
-    const R rhs = s + bs + (R(1) - H.au) * apr * un;
-    Sarr<A>(H)[f] = rhs / apr;
-    if (last) Darr<A>(H)[f] = Ar / apr;
+      for (int n = 0; n < 6; ++n) s += an[n] * (nb[n] >= 0 ? src[nb[n]] : R(0));
+      const R rhs = s + bs + (R(1) - H.au) * apr * un;
+      SA[f] = rhs / apr;
+      if (last) Darr<A>(H)[f] = Ar / apr;
+    }
+  } else {
+    // delta: a_P/alpha delta_P - sum a_nb delta_nb = sum a_nb u^n_nb + b - a_P u^n_P (FP64, then FP32)
+    R rhs;
+    if (first) {
+      int lo[3] = {c[0], c[1], c[2]};
+      lo[A] -= 1;
+      const double bs = (H.p[cidx(H, lo[0], lo[1], lo[2])] - H.p[cidx(H, c[0], c[1], c[2])]) * (double)Ar;
+      double s = 0.0;
+#pragma unroll
+      for (int n = 0; n < 6; ++n) s += (double)an[n] * (nb[n] >= 0 ? UA[nb[n]] : 0.0);
+      const double r = (s + bs) - (double)aP * UA[f];
+      racc += r * r;
+      rhs = (R)r;
+      Qarr<A>(H)[f] = rhs;
+    } else {
+      rhs = Qarr<A>(H)[f];
+    }
+    if (upd) {
+      R s = R(0);
+      if (!first) {
+#pragma unroll
+        for (int n = 0; n < 6; ++n) s += an[n] * (nb[n] >= 0 ? SA[nb[n]] : R(0));
+      }
+      SA[f] = (rhs + s) / apr;
+      if (last) Darr<A>(H)[f] = Ar / apr;
+    }
   }
 }
 
@@ -227,7 +270,7 @@ __device__ double block_sum(double v, double *sh) {
 
 // One red-black pass of all three momentum components (blockIdx.y = axis).
 // first: the pass of colour 0 in sweep 0, which also evaluates the residual of
-// every unknown face at u^n and writes the fixed faces of u*.
+// every unknown face at u^n and writes the fixed faces of u* (delta = 0).
 template <int A, class R>
 __device__ void mom_pass_axis(const ChDev<R> &H, int color, bool first, bool last, double &racc) {
   const int nf0 = H.N0 + (A == 0), nf1 = H.N1 + (A == 1), nf2 = H.N2 + (A == 2);
@@ -239,12 +282,12 @@ __device__ void mom_pass_axis(const ChDev<R> &H, int color, bool first, bool las
       const int kind = face_kind<A>(H, c);
       if (kind != 0) {
         const int f = fidx3<A>(H, c);
-        Sarr<A>(H)[f] = face_fixed<A>(H, c);
+        Sarr<A>(H)[f] = is_mixed(R()) ? R(0) : face_fixed<A>(H, c);
         Darr<A>(H)[f] = R(0);
         continue;
       }
       const bool mine = ((c[0] + c[1] + c[2]) & 1) == color;
-      mom_face<A>(H, c, true, mine, true, last && mine, racc);
+      mom_face<A>(H, c, true, mine, last && mine, racc);
     }
   } else {
     const int half = (nf0 + 1) / 2;
@@ -255,7 +298,7 @@ __device__ void mom_pass_axis(const ChDev<R> &H, int color, bool first, bool las
       if (i >= nf0) continue;
       const int c[3] = {i, j, k};
       if (face_kind<A>(H, c) != 0) continue;
-      mom_face<A>(H, c, false, true, false, last, racc);
+      mom_face<A>(H, c, false, true, last, racc);
     }
   }
 }
@@ -275,6 +318,13 @@ __global__ void __launch_bounds__(kT) k_ch_mom(ChDev<R> H, int color, int first,
 
 // padded cell index of the CG arrays
 __device__ __forceinline__ int pq(int N0, int N1, int i, int j, int k) { return (i + 1) + (N0 + 2) * ((j + 1) + (N1 + 2) * (k + 1)); }
+
+// u* of a face in FP64
+template <int A, class R>
+__device__ __forceinline__ double ustar(const ChDev<R> &H, int f) {
+  if constexpr (is_mixed(R())) return Uarr<A>(H)[f] + (double)Sarr<A>(H)[f];
+  else return Sarr<A>(H)[f];
+}
 
 // p' couplings per face into padded cell arrays (the coupling of the face on a
 // cell's low side; the outlet face sits in the ghost cell i = N0) and the mass
@@ -315,11 +365,11 @@ __global__ void k_ch_passemble(ChDev<R> H, double *acx, double *acy, double *acz
       const int q = pq(N0, N1, i, j, k);
       x[q] = 0.0;
       if (H.solid[e]) { r[q] = 0.0; continue; }
-      const double uw = (double)H.S0[fidx<0>(H, i, j, k)];
-      const double ue = (i + 1 == N0) ? uw : (double)H.S0[fidx<0>(H, i + 1, j, k)];
+      const double uw = ustar<0>(H, fidx<0>(H, i, j, k));
+      const double ue = (i + 1 == N0) ? uw : ustar<0>(H, fidx<0>(H, i + 1, j, k));
       const double b = (uw - ue) * ((double)H.d1[j] * (double)H.d2[k]) +
-                       ((double)H.S1[fidx<1>(H, i, j, k)] - (double)H.S1[fidx<1>(H, i, j + 1, k)]) * ((double)H.d0[i] * (double)H.d2[k]) +
-                       ((double)H.S2[fidx<2>(H, i, j, k)] - (double)H.S2[fidx<2>(H, i, j, k + 1)]) * ((double)H.d0[i] * (double)H.d1[j]);
+                       (ustar<1>(H, fidx<1>(H, i, j, k)) - ustar<1>(H, fidx<1>(H, i, j + 1, k))) * ((double)H.d0[i] * (double)H.d2[k]) +
+                       (ustar<2>(H, fidx<2>(H, i, j, k)) - ustar<2>(H, fidx<2>(H, i, j, k + 1))) * ((double)H.d0[i] * (double)H.d1[j]);
       r[q] = b;
       acc += b * b;
     }
@@ -329,47 +379,45 @@ __global__ void k_ch_passemble(ChDev<R> H, double *acx, double *acy, double *acz
 }
 
 template <int A, class R>
-__device__ void correct_axis(const ChDev<R> &H, const double *pp, double *Ud) {
+__device__ void correct_axis(const ChDev<R> &H, const double *pp) {
   const int nf0 = H.N0 + (A == 0), nf1 = H.N1 + (A == 1), nf2 = H.N2 + (A == 2);
   const long long n = (long long)nf0 * nf1 * nf2;
   const int T = gridDim.x * blockDim.x;
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += T) {
     const int c[3] = {(int)(e % nf0), (int)((e / nf0) % nf1), (int)(e / ((long long)nf0 * nf1))};
     const int kind = face_kind<A>(H, c);
-    R val;
+    double val;
     if (kind == 1) {
-      val = face_fixed<A>(H, c);
+      val = (double)face_fixed<A>(H, c);
     } else if (kind == 2) {
       const int fl = fidx<0>(H, c[0] - 1, c[1], c[2]);
-      if (H.solid[cidx(H, c[0] - 1, c[1], c[2])]) val = R(0);
-      else if constexpr (sizeof(R) == 8) val = H.S0[fl] + H.D0[fl] * pp[pq(H.N0, H.N1, c[0] - 1, c[1], c[2])];
-      else val = (R)((double)H.S0[fl] + (double)H.D0[fl] * pp[pq(H.N0, H.N1, c[0] - 1, c[1], c[2])]);
+      if (H.solid[cidx(H, c[0] - 1, c[1], c[2])]) val = 0.0;
+      else if constexpr (!is_mixed(R())) val = H.S0[fl] + H.D0[fl] * pp[pq(H.N0, H.N1, c[0] - 1, c[1], c[2])];
+      else val = ustar<0>(H, fl) + (double)H.D0[fl] * pp[pq(H.N0, H.N1, c[0] - 1, c[1], c[2])];
     } else {
       int lo[3] = {c[0], c[1], c[2]};
       lo[A] -= 1;
       const int f = fidx3<A>(H, c);
       const double dp = pp[pq(H.N0, H.N1, lo[0], lo[1], lo[2])] - pp[pq(H.N0, H.N1, c[0], c[1], c[2])];
-      if constexpr (sizeof(R) == 8) val = Sarr<A>(H)[f] + Darr<A>(H)[f] * dp;
-      else val = (R)((double)Sarr<A>(H)[f] + (double)Darr<A>(H)[f] * dp);
+      if constexpr (!is_mixed(R())) val = Sarr<A>(H)[f] + Darr<A>(H)[f] * dp;
+      else val = ustar<A>(H, f) + (double)Darr<A>(H)[f] * dp;
     }
     Uarr<A>(H)[e] = val;
-    if (Ud) Ud[e] = (double)val;
+    if constexpr (is_mixed(R())) Carr<A>(H)[e] = (R)val;
   }
 }
 
 template <class R>
 __global__ void k_ch_correct(ChDev<R> H, const double *pp) {
-  if (blockIdx.y == 0) correct_axis<0>(H, pp, H.Ud0);
-  else if (blockIdx.y == 1) correct_axis<1>(H, pp, H.Ud1);
-  else if (blockIdx.y == 2) correct_axis<2>(H, pp, H.Ud2);
+  if (blockIdx.y == 0) correct_axis<0>(H, pp);
+  else if (blockIdx.y == 1) correct_axis<1>(H, pp);
+  else if (blockIdx.y == 2) correct_axis<2>(H, pp);
   else {
     const long long n = (long long)H.N0 * H.N1 * H.N2;
     for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
       if (H.solid[e]) continue;
       const int i = (int)(e % H.N0), j = (int)((e / H.N0) % H.N1), k = (int)(e / ((long long)H.N0 * H.N1));
-      const double v = pp[pq(H.N0, H.N1, i, j, k)];
-      if constexpr (sizeof(R) == 8) H.p[e] = H.p[e] + H.ap * v;
-      else H.p[e] = (R)((double)H.p[e] + H.ap * v);
+      H.p[e] = H.p[e] + H.ap * pp[pq(H.N0, H.N1, i, j, k)];
     }
   }
 }
@@ -380,6 +428,7 @@ __global__ void k_ch_init(ChDev<R> H) {
   const long long n0 = (long long)(H.N0 + 1) * H.N1 * H.N2;
   const long long n1 = (long long)H.N0 * (H.N1 + 1) * H.N2, n2 = (long long)H.N0 * H.N1 * (H.N2 + 1);
   const long long nc = (long long)H.N0 * H.N1 * H.N2;
+  const R s0 = is_mixed(R()) ? R(0) : R(1);  // u* starts at u (FP64 form), delta at 0 (mixed)
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n0 + n1 + n2 + nc; e += gridDim.x * blockDim.x) {
     if (e < n0) {
       const int c[3] = {(int)(e % (H.N0 + 1)), (int)((e / (H.N0 + 1)) % H.N1), (int)(e / ((long long)(H.N0 + 1) * H.N1))};
@@ -388,18 +437,18 @@ __global__ void k_ch_init(ChDev<R> H) {
       if (kind == 0) v = H.u_in;
       else if (kind == 1) v = face_fixed<0>(H, c);
       else v = H.solid[cidx(H, c[0] - 1, c[1], c[2])] ? R(0) : H.u_in;
-      H.U0[e] = v; H.S0[e] = v; H.D0[e] = R(0);
-      if (H.Ud0) H.Ud0[e] = (double)v;
+      H.U0[e] = (double)v; H.S0[e] = s0 * v; H.D0[e] = R(0);
+      if constexpr (is_mixed(R())) { H.C0[e] = v; H.Q0[e] = R(0); }
     } else if (e < n0 + n1) {
       const long long f = e - n0;
-      H.U1[f] = R(0); H.S1[f] = R(0); H.D1[f] = R(0);
-      if (H.Ud1) H.Ud1[f] = 0.0;
+      H.U1[f] = 0.0; H.S1[f] = R(0); H.D1[f] = R(0);
+      if constexpr (is_mixed(R())) { H.C1[f] = R(0); H.Q1[f] = R(0); }
     } else if (e < n0 + n1 + n2) {
       const long long f = e - n0 - n1;
-      H.U2[f] = R(0); H.S2[f] = R(0); H.D2[f] = R(0);
-      if (H.Ud2) H.Ud2[f] = 0.0;
+      H.U2[f] = 0.0; H.S2[f] = R(0); H.D2[f] = R(0);
+      if constexpr (is_mixed(R())) { H.C2[f] = R(0); H.Q2[f] = R(0); }
     } else {
-      H.p[e - n0 - n1 - n2] = R(0);
+      H.p[e - n0 - n1 - n2] = 0.0;
     }
   }
 }
@@ -872,14 +921,22 @@ void setup_fields(ChannelState &S, ChDev<R> &H, const std::vector<double> (&d)[3
   }
   H.solid = solid;
   const size_t nf[3] = {(size_t)(S.N0 + 1) * S.N1 * S.N2, (size_t)S.N0 * (S.N1 + 1) * S.N2, (size_t)S.N0 * S.N1 * (S.N2 + 1)};
-  R **U[3] = {&H.U0, &H.U1, &H.U2}, **Sx[3] = {&H.S0, &H.S1, &H.S2}, **D[3] = {&H.D0, &H.D1, &H.D2};
-  for (int a = 0; a < 3; ++a) { *U[a] = S.alloc<R>(nf[a]); *Sx[a] = S.alloc<R>(nf[a]); *D[a] = S.alloc<R>(nf[a]); }
-  H.p = S.alloc<R>((size_t)S.N0 * S.N1 * S.N2);
-  if (sizeof(R) == 4) {
-    H.Ud0 = S.alloc<double>(nf[0]); H.Ud1 = S.alloc<double>(nf[1]); H.Ud2 = S.alloc<double>(nf[2]);
-  } else {
-    H.Ud0 = H.Ud1 = H.Ud2 = nullptr;
+  double **U[3] = {&H.U0, &H.U1, &H.U2};
+  R **C[3] = {&H.C0, &H.C1, &H.C2}, **Sx[3] = {&H.S0, &H.S1, &H.S2}, **Q[3] = {&H.Q0, &H.Q1, &H.Q2};
+  R **D[3] = {&H.D0, &H.D1, &H.D2};
+  for (int a = 0; a < 3; ++a) {
+    *U[a] = S.alloc<double>(nf[a]);
+    *Sx[a] = S.alloc<R>(nf[a]);
+    *D[a] = S.alloc<R>(nf[a]);
+    if (is_mixed(R())) {
+      *C[a] = S.alloc<R>(nf[a]);
+      *Q[a] = S.alloc<R>(nf[a]);
+    } else {
+      *C[a] = (R *)*U[a];  // the FP64 form reads its coefficients from U itself
+      *Q[a] = nullptr;
+    }
   }
+  H.p = S.alloc<double>((size_t)S.N0 * S.N1 * S.N2);
   H.nu = (R)S.nu; H.au = (R)S.prm.alpha_u; H.u_in = (R)S.prm.u_in; H.ap = S.prm.alpha_p;
 }
 
@@ -970,6 +1027,13 @@ void read_stats(ChannelState &S, int flags) {
 
 }  // namespace
 
+namespace {
+double *uarr(ChannelState *S, int a) {
+  double *u[3] = {S->Hd.U0, S->Hd.U1, S->Hd.U2}, *m[3] = {S->Hf.U0, S->Hf.U1, S->Hf.U2};
+  return S->mixed ? m[a] : u[a];
+}
+}  // namespace
+
 ChannelState *ch_create(const Case &c, const ChParams &p, int device) {
   if (!(p.re > 0) || !(p.pr > 0) || !(p.alpha_u > 0 && p.alpha_u <= 1) || !(p.alpha_p > 0 && p.alpha_p <= 1) ||
       !(p.alpha_t > 0 && p.alpha_t <= 1) || p.mom_sweeps < 1 || !(p.p_tol > 0) || p.p_maxiter < 0 || !(p.t_tol > 0) ||
@@ -1035,8 +1099,7 @@ ChannelState *ch_create(const Case &c, const ChParams &p, int device) {
   cs.ctype = c.ctype.data(); cs.region = S->region.data();
   cs.t_boundary = p.t_in; cs.tol = 1e-10; cs.maxiter = 5000; cs.bc = 1;
   S->cht = cht_create(cs);
-  if (S->mixed) cht_bind_velocities(S->cht, S->Hf.Ud0, S->Hf.Ud1, S->Hf.Ud2);
-  else cht_bind_velocities(S->cht, S->Hd.U0, S->Hd.U1, S->Hd.U2);
+  cht_bind_velocities(S->cht, uarr(S.get(), 0), uarr(S.get(), 1), uarr(S.get(), 2));
   S->kratio.assign(S->nreg, 100.0);
   S->qcell.assign(n, 0.0);
   std::vector<double> kabs(S->nreg);
@@ -1127,11 +1190,6 @@ void put_dev(ChannelState *S, R *dst, const double *host, long n) {
   CH_CUDA(cudaMemcpyAsync(dst, tmp.data(), n * sizeof(R), cudaMemcpyHostToDevice, S->stream));
   CH_CUDA(cudaStreamSynchronize(S->stream));
 }
-template <class R>
-R *field_ptr(ChDev<R> &H, int f) {
-  R *t[11] = {H.U0, H.U1, H.U2, H.p, nullptr, H.S0, H.S1, H.S2, H.D0, H.D1, H.D2};
-  return f < 11 ? t[f] : nullptr;
-}
 void unpad_cells(ChannelState *S, const double *dev, double *host) {
   const size_t np = (size_t)(S->N0 + 2) * (S->N1 + 2) * (S->N2 + 2);
   std::vector<double> tmp(np);
@@ -1149,8 +1207,20 @@ void ch_get_field(ChannelState *S, int f, double *host, long n) {
   if (ch_field_size(S, f) != n) throw std::invalid_argument("field size mismatch");
   if (f == 4) { unpad_cells(S, cht_T_device(S->cht), host); return; }
   if (f == 11) { unpad_cells(S, S->V.x, host); return; }
-  if (S->mixed) get_dev(S, (const float *)field_ptr(S->Hf, f), host, n);
-  else get_dev(S, (const double *)field_ptr(S->Hd, f), host, n);
+  if (f < 3) { get_dev(S, (const double *)uarr(S, f), host, n); return; }
+  if (f == 3) { get_dev(S, (const double *)(S->mixed ? S->Hf.p : S->Hd.p), host, n); return; }
+  const int a = (f - 5) % 3;
+  if (f >= 8) {
+    if (S->mixed) get_dev(S, (const float *)(a == 0 ? S->Hf.D0 : a == 1 ? S->Hf.D1 : S->Hf.D2), host, n);
+    else get_dev(S, (const double *)(a == 0 ? S->Hd.D0 : a == 1 ? S->Hd.D1 : S->Hd.D2), host, n);
+    return;
+  }
+  if (!S->mixed) { get_dev(S, (const double *)(a == 0 ? S->Hd.S0 : a == 1 ? S->Hd.S1 : S->Hd.S2), host, n); return; }
+  // mixed: u* = u^n + delta
+  std::vector<double> d(n);
+  get_dev(S, (const float *)(a == 0 ? S->Hf.S0 : a == 1 ? S->Hf.S1 : S->Hf.S2), d.data(), n);
+  get_dev(S, (const double *)uarr(S, a), host, n);
+  for (long i = 0; i < n; ++i) host[i] += d[i];
 }
 
 void ch_set_field(ChannelState *S, int f, const double *host, long n) {
@@ -1167,16 +1237,9 @@ void ch_set_field(ChannelState *S, int f, const double *host, long n) {
     CH_CUDA(cudaStreamSynchronize(S->stream));
     return;
   }
-  if (S->mixed) {
-    put_dev(S, field_ptr(S->Hf, f), host, n);
-    double *Ud[3] = {S->Hf.Ud0, S->Hf.Ud1, S->Hf.Ud2};
-    if (f < 3) {
-      CH_CUDA(cudaMemcpyAsync(Ud[f], host, n * 8, cudaMemcpyHostToDevice, S->stream));
-      CH_CUDA(cudaStreamSynchronize(S->stream));
-    }
-  } else {
-    put_dev(S, field_ptr(S->Hd, f), host, n);
-  }
+  if (f == 3) { put_dev(S, S->mixed ? S->Hf.p : S->Hd.p, host, n); return; }
+  put_dev(S, uarr(S, f), host, n);
+  if (S->mixed) put_dev(S, f == 0 ? S->Hf.C0 : f == 1 ? S->Hf.C1 : S->Hf.C2, host, n);
 }
 
 void *ch_stream(ChannelState *S) { return S->stream; }
