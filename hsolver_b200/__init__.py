@@ -360,6 +360,8 @@ def _channel_api(L):
         "hs_channel_device_bytes": ([vp, ctypes.POINTER(ll)], ctypes.c_int),
         "hs_channel_adjoint": ([vp, ctypes.c_double, ctypes.c_int, dp, dp, ll, dp, ctypes.c_int,
                                 ctypes.POINTER(AdjointInfo)], ctypes.c_int),
+        "hs_channel_profile": ([vp, ctypes.c_int], ctypes.c_int),
+        "hs_channel_profile_read": ([vp, dp, ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
         "hs_channel_destroy": ([vp], None),
     }
     for name, (args, res) in sig.items():
@@ -462,6 +464,17 @@ class Channel:
 
     def sync(self):
         self._check(self._L.hs_channel_sync(self.h))
+
+    PHASES = ["momentum", "p_assembly", "p_solve", "correction", "energy"]
+
+    def profile(self, on=True):
+        self._check(self._L.hs_channel_profile(self.h, 1 if on else 0))
+
+    def profile_read(self):
+        ms = (ctypes.c_double * 5)()
+        n = ctypes.c_int()
+        self._check(self._L.hs_channel_profile_read(self.h, ms, ctypes.byref(n)))
+        return dict(zip(self.PHASES, list(ms))), n.value
 
     def device_bytes(self):
         b = ctypes.c_longlong()

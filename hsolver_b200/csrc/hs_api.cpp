@@ -438,7 +438,7 @@ int hs_cht_create(hs_ctx *ctx, const hs_cht_params *prm, hs_cht **out) {
     std::vector<int> reg(c.region.size());
     for (size_t i = 0; i < reg.size(); ++i) reg[i] = c.ctype[i] ? c.region[i] : -1;
     S.region = reg.data();
-    S.t_boundary = p.t_boundary; S.tol = p.tol; S.maxiter = p.maxiter; S.bc = 0;
+    S.t_boundary = p.t_boundary; S.tol = p.tol; S.maxiter = p.maxiter; S.bc = 0; S.precond = 1;
     hs_cht *h = new hs_cht();
     h->ctx = ctx;
     h->k_fluid = p.k_fluid;
@@ -610,6 +610,19 @@ int hs_channel_set_field(hs_channel *h, int field, const double *host, long long
 int hs_channel_stream(hs_channel *h, void **stream) {
   if (!stream) return fail(nullptr, HS_ERR_ARG, "null output pointer");
   return ch_guarded(h, [&](hs_channel &c) { *stream = hs::ch_stream(c.st); return HS_OK; });
+}
+
+int hs_channel_profile(hs_channel *h, int on) {
+  return ch_guarded(h, [&](hs_channel &c) { hs::ch_profile(c.st, on != 0); return HS_OK; });
+}
+
+int hs_channel_profile_read(hs_channel *h, double ms[HS_CH_NPHASE], int *steps) {
+  if (!ms) return fail(nullptr, HS_ERR_ARG, "null output pointer");
+  return ch_guarded(h, [&](hs_channel &c) {
+    const int n = hs::ch_profile_read(c.st, ms);
+    if (steps) *steps = n;
+    return HS_OK;
+  });
 }
 
 int hs_channel_sync(hs_channel *h) {

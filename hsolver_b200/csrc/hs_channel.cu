@@ -40,6 +40,7 @@
 
 #include "hs_channel.hpp"
 #include "hs_cht.hpp"
+#include "hs_mg.cuh"
 
 namespace cg = cooperative_groups;
 
@@ -55,8 +56,6 @@ namespace hs {
 namespace {
 
 constexpr int kT = 256;
-constexpr int kMaxLv = 16;
-constexpr int kMaxCoarse = 64;
 
 // Device view.  U and p are the FP64 iterate in both forms.  In the FP64 form
 // C aliases U and S holds u*; in the mixed form C is an FP32 copy of U (the
@@ -456,36 +455,15 @@ __global__ void k_ch_init(ChDev<R> H) {
 // ---------------------------------------------------------------- multigrid-preconditioned CG
 // Symmetric operator on padded cells: (A x)_q = sum_f c_f (x_q - x_nb), with
 // c stored on each cell's low face (acx[q] couples q-1 and q; acx of the
-// ghost cell N0 + 1 is the outlet face, neighbour value 0).
-// V-cycle in precision M: 2x coarsening per axis (ceil); a coarse cell is an
-// unknown when any child is; a coarse face coupling is half the sum of the
-// fine couplings on it (the 2x2 patch of a face, halved for the doubled
-// spacing); red-black Gauss-Seidel 1 pre (red, black) + 1 post (black, red);
-// sum restriction, constant prolongation; FP64 LU on the coarsest (<= 64 cells)
-// factored on the GPU every solve, since the couplings change every step.
-template <class M>
-struct Lv {
-  int nx, ny, nz;
-  M *x, *rhs, *ax, *ay, *az;
-  uint8_t *m;
-};
-template <class M>
-struct Mg {
-  int L;
-  Lv<M> lv[kMaxLv];
-  double *lu;   // kMaxCoarse^2
-  int *piv;     // kMaxCoarse
-  double *y;    // kMaxCoarse
-};
+// ghost cell N0 + 1 is the outlet face, neighbour value 0).  Preconditioner:
+// the V-cycle of hs_mg.cuh in precision M on the same couplings (no
+// convection), solid cells masked.
 struct CgVec {
   int N0, N1, N2;
   const double *acx, *acy, *acz;
   const uint8_t *solid;
   double *x, *r, *p, *s;
 };
-
-template <class M>
-__device__ __forceinline__ int li(const Lv<M> &L, int i, int j, int k) { return i + (L.nx + 2) * (j + (L.ny + 2) * k); }
 
 __device__ double grid_sum(double v, double *partials, int &buf, double *sh, cg::grid_group &grid) {
   double *pp = partials + (size_t)buf * gridDim.x;
@@ -506,240 +484,14 @@ __device__ double grid_sum(double v, double *partials, int &buf, double *sh, cg:
 }
 
 template <class M>
-__device__ void mg_build_fine(const CgVec &V, const Lv<M> &L0, int tid, int T) {
+__device__ void mg_fine_from_couplings(const CgVec &V, const mg::Level<M> &L0, int tid, int T) {
   const int PX = V.N0 + 2, PY = V.N1 + 2;
   const long long np = (long long)PX * PY * (V.N2 + 2);
   for (long long q = tid; q < np; q += T) {
-    L0.ax[q] = (M)V.acx[q]; L0.ay[q] = (M)V.acy[q]; L0.az[q] = (M)V.acz[q];
+    L0.gx[q] = (M)V.acx[q]; L0.gy[q] = (M)V.acy[q]; L0.gz[q] = (M)V.acz[q];
     const int i = (int)(q % PX) - 1, j = (int)((q / PX) % PY) - 1, k = (int)(q / ((long long)PX * PY)) - 1;
     const bool in = i >= 0 && j >= 0 && k >= 0 && i < V.N0 && j < V.N1 && k < V.N2;
     L0.m[q] = in && !V.solid[i + V.N0 * (j + V.N1 * k)];
-  }
-}
-
-template <class M>
-__device__ void mg_coarsen(const Lv<M> &F, const Lv<M> &C, int tid, int T) {
-  const long long n = (long long)(C.nx + 1) * (C.ny + 1) * (C.nz + 1);
-  for (long long e = tid; e < n; e += T) {
-    const int I = (int)(e % (C.nx + 1)), J = (int)((e / (C.nx + 1)) % (C.ny + 1)), K = (int)(e / ((long long)(C.nx + 1) * (C.ny + 1)));
-    const int qc = li(C, I + 1, J + 1, K + 1);
-    if (J < C.ny && K < C.nz) {  // x face I of coarse row (J, K)
-      const int fi = min(2 * I, F.nx);
-      M s = M(0);
-      for (int dk = 0; dk < 2; ++dk)
-        for (int dj = 0; dj < 2; ++dj) {
-          const int j = 2 * J + dj, k = 2 * K + dk;
-          if (j < F.ny && k < F.nz) s += F.ax[li(F, fi + 1, j + 1, k + 1)];
-        }
-      C.ax[qc] = M(0.5) * s;
-    }
-    if (I < C.nx && K < C.nz) {
-      const int fj = min(2 * J, F.ny);
-      M s = M(0);
-      for (int dk = 0; dk < 2; ++dk)
-        for (int di = 0; di < 2; ++di) {
-          const int i = 2 * I + di, k = 2 * K + dk;
-          if (i < F.nx && k < F.nz) s += F.ay[li(F, i + 1, fj + 1, k + 1)];
-        }
-      C.ay[qc] = M(0.5) * s;
-    }
-    if (I < C.nx && J < C.ny) {
-      const int fk = min(2 * K, F.nz);
-      M s = M(0);
-      for (int dj = 0; dj < 2; ++dj)
-        for (int di = 0; di < 2; ++di) {
-          const int i = 2 * I + di, j = 2 * J + dj;
-          if (i < F.nx && j < F.ny) s += F.az[li(F, i + 1, j + 1, fk + 1)];
-        }
-      C.az[qc] = M(0.5) * s;
-    }
-    if (I < C.nx && J < C.ny && K < C.nz) {
-      uint8_t any = 0;
-      for (int dk = 0; dk < 2; ++dk)
-        for (int dj = 0; dj < 2; ++dj)
-          for (int di = 0; di < 2; ++di) {
-            const int i = 2 * I + di, j = 2 * J + dj, k = 2 * K + dk;
-            if (i < F.nx && j < F.ny && k < F.nz && F.m[li(F, i + 1, j + 1, k + 1)]) any = 1;
-          }
-      C.m[qc] = any;
-    }
-  }
-}
-
-template <class M>
-__device__ __forceinline__ M lv_diag(const Lv<M> &L, int q, int PX, int PXY) {
-  return L.ax[q] + L.ax[q + 1] + L.ay[q] + L.ay[q + PX] + L.az[q] + L.az[q + PXY];
-}
-template <class M>
-__device__ __forceinline__ M lv_off(const Lv<M> &L, const M *x, int q, int PX, int PXY) {
-  return L.ax[q] * __ldcg(x + q - 1) + L.ax[q + 1] * __ldcg(x + q + 1) + L.ay[q] * __ldcg(x + q - PX) +
-         L.ay[q + PX] * __ldcg(x + q + PX) + L.az[q] * __ldcg(x + q - PXY) + L.az[q + PXY] * __ldcg(x + q + PXY);
-}
-
-template <class M>
-__device__ void mg_smooth(const Lv<M> &L, int color, bool zero_nb, int tid, int T) {
-  const int PX = L.nx + 2, PXY = (L.nx + 2) * (L.ny + 2);
-  const int half = (L.nx + 1) / 2;
-  const long long n = (long long)half * L.ny * L.nz;
-  for (long long e = tid; e < n; e += T) {
-    const int m = (int)(e % half), j = (int)((e / half) % L.ny), k = (int)(e / ((long long)half * L.ny));
-    const int i = 2 * m + ((j + k + color) & 1);
-    if (i >= L.nx) continue;
-    const int q = li(L, i + 1, j + 1, k + 1);
-    if (!L.m[q]) continue;
-    const M d = lv_diag(L, q, PX, PXY);
-    if (d == M(0)) { L.x[q] = M(0); continue; }
-    M s = L.rhs[q];
-    if (!zero_nb) s += lv_off(L, L.x, q, PX, PXY);
-    L.x[q] = s / d;
-  }
-}
-
-template <class M>
-__device__ void mg_restrict(const Lv<M> &F, const Lv<M> &C, int tid, int T) {
-  const int PX = F.nx + 2, PXY = (F.nx + 2) * (F.ny + 2);
-  const long long n = (long long)C.nx * C.ny * C.nz;
-  for (long long e = tid; e < n; e += T) {
-    const int I = (int)(e % C.nx), J = (int)((e / C.nx) % C.ny), K = (int)(e / ((long long)C.nx * C.ny));
-    M acc = M(0);
-    for (int dk = 0; dk < 2; ++dk)
-      for (int dj = 0; dj < 2; ++dj)
-        for (int di = 0; di < 2; ++di) {
-          const int i = 2 * I + di, j = 2 * J + dj, k = 2 * K + dk;
-          if (i >= F.nx || j >= F.ny || k >= F.nz) continue;
-          const int q = li(F, i + 1, j + 1, k + 1);
-          if (!F.m[q]) continue;
-          acc += F.rhs[q] - (lv_diag(F, q, PX, PXY) * __ldcg(F.x + q) - lv_off(F, F.x, q, PX, PXY));
-        }
-    const int qc = li(C, I + 1, J + 1, K + 1);
-    C.rhs[qc] = C.m[qc] ? acc : M(0);
-  }
-}
-
-template <class M>
-__device__ void mg_prolong(const Lv<M> &F, const Lv<M> &C, int tid, int T) {
-  const long long n = (long long)F.nx * F.ny * F.nz;
-  for (long long e = tid; e < n; e += T) {
-    const int i = (int)(e % F.nx), j = (int)((e / F.nx) % F.ny), k = (int)(e / ((long long)F.nx * F.ny));
-    const int q = li(F, i + 1, j + 1, k + 1);
-    if (!F.m[q]) continue;
-    F.x[q] = __ldcg(F.x + q) + __ldcg(C.x + li(C, i / 2 + 1, j / 2 + 1, k / 2 + 1));
-  }
-}
-
-// dense LU with partial pivoting of the coarsest operator, by block 0
-template <class M>
-__device__ void mg_factor(const Mg<M> &G) {
-  if (blockIdx.x != 0) return;
-  const Lv<M> &C = G.lv[G.L - 1];
-  const int nc = C.nx * C.ny * C.nz, PX = C.nx + 2, PXY = (C.nx + 2) * (C.ny + 2);
-  double *a = G.lu;
-  for (int e = threadIdx.x; e < nc * nc; e += blockDim.x) {
-    const int r = e / nc, c2 = e % nc;
-    const int ri = r % C.nx, rj = (r / C.nx) % C.ny, rk = r / (C.nx * C.ny);
-    const int q = li(C, ri + 1, rj + 1, rk + 1);
-    double v = 0.0;
-    if (!C.m[q]) {
-      v = (r == c2) ? 1.0 : 0.0;
-    } else if (r == c2) {
-      v = (double)lv_diag(C, q, PX, PXY);
-      if (v == 0.0) v = 1.0;
-    } else {
-      const int ci = c2 % C.nx, cj = (c2 / C.nx) % C.ny, ck = c2 / (C.nx * C.ny);
-      const int qc = li(C, ci + 1, cj + 1, ck + 1);
-      if (C.m[qc]) {
-        if (qc == q - 1) v = -(double)C.ax[q];
-        else if (qc == q + 1) v = -(double)C.ax[q + 1];
-        else if (qc == q - PX) v = -(double)C.ay[q];
-        else if (qc == q + PX) v = -(double)C.ay[q + PX];
-        else if (qc == q - PXY) v = -(double)C.az[q];
-        else if (qc == q + PXY) v = -(double)C.az[q + PXY];
-      }
-    }
-    a[e] = v;
-  }
-  __syncthreads();
-  __shared__ int spiv;
-  for (int col = 0; col < nc; ++col) {
-    if (threadIdx.x == 0) {
-      int best = col;
-      double bv = fabs(a[col * nc + col]);
-      for (int r = col + 1; r < nc; ++r)
-        if (fabs(a[r * nc + col]) > bv) { bv = fabs(a[r * nc + col]); best = r; }
-      spiv = best;
-      G.piv[col] = best;
-    }
-    __syncthreads();
-    const int pr = spiv;
-    if (pr != col)
-      for (int c2 = threadIdx.x; c2 < nc; c2 += blockDim.x) {
-        const double t = a[col * nc + c2];
-        a[col * nc + c2] = a[pr * nc + c2];
-        a[pr * nc + c2] = t;
-      }
-    __syncthreads();
-    const double piv = a[col * nc + col];
-    for (int r = col + 1 + threadIdx.x; r < nc; r += blockDim.x) a[r * nc + col] /= piv;
-    __syncthreads();
-    const int rem = nc - col - 1;
-    for (int e = threadIdx.x; e < rem * rem; e += blockDim.x) {
-      const int r = col + 1 + e / rem, c2 = col + 1 + e % rem;
-      a[r * nc + c2] -= a[r * nc + col] * a[col * nc + c2];
-    }
-    __syncthreads();
-  }
-}
-
-template <class M>
-__device__ void mg_coarse_solve(const Mg<M> &G) {
-  if (blockIdx.x != 0 || threadIdx.x != 0) return;
-  const Lv<M> &C = G.lv[G.L - 1];
-  const int nc = C.nx * C.ny * C.nz;
-  double *y = G.y;
-  for (int r = 0; r < nc; ++r) {
-    const int ri = r % C.nx, rj = (r / C.nx) % C.ny, rk = r / (C.nx * C.ny);
-    y[r] = (double)C.rhs[li(C, ri + 1, rj + 1, rk + 1)];
-  }
-  for (int c2 = 0; c2 < nc; ++c2) {  // apply the row swaps in order
-    const int pr = G.piv[c2];
-    if (pr != c2) { const double t = y[c2]; y[c2] = y[pr]; y[pr] = t; }
-  }
-  for (int r = 0; r < nc; ++r) {
-    double s = y[r];
-    for (int c2 = 0; c2 < r; ++c2) s -= G.lu[r * nc + c2] * y[c2];
-    y[r] = s;
-  }
-  for (int r = nc - 1; r >= 0; --r) {
-    double s = y[r];
-    for (int c2 = r + 1; c2 < nc; ++c2) s -= G.lu[r * nc + c2] * y[c2];
-    y[r] = s / G.lu[r * nc + r];
-  }
-  for (int r = 0; r < nc; ++r) {
-    const int ri = r % C.nx, rj = (r / C.nx) % C.ny, rk = r / (C.nx * C.ny);
-    const int q = li(C, ri + 1, rj + 1, rk + 1);
-    C.x[q] = C.m[q] ? (M)y[r] : M(0);
-  }
-}
-
-template <class M>
-__device__ void mg_vcycle(const Mg<M> &G, cg::grid_group &grid, int tid, int T) {
-  for (int l = 0; l < G.L - 1; ++l) {
-    mg_smooth(G.lv[l], 0, true, tid, T);
-    grid.sync();
-    mg_smooth(G.lv[l], 1, false, tid, T);
-    grid.sync();
-    mg_restrict(G.lv[l], G.lv[l + 1], tid, T);
-    grid.sync();
-  }
-  mg_coarse_solve(G);
-  grid.sync();
-  for (int l = G.L - 2; l >= 0; --l) {
-    mg_prolong(G.lv[l], G.lv[l + 1], tid, T);
-    grid.sync();
-    mg_smooth(G.lv[l], 1, false, tid, T);
-    grid.sync();
-    mg_smooth(G.lv[l], 0, false, tid, T);
-    grid.sync();
   }
 }
 
@@ -753,7 +505,7 @@ __device__ __forceinline__ double cg_apply(const CgVec &V, const double *x, int 
 // PCG: r = b (assembled), x = 0; z = M r (V-cycle, or z = r when precond = 0);
 // s = A p, alpha = <r,z>/<s,p>, x += alpha p, r -= alpha s, stop on ||r||/||b|| < tol
 template <class M>
-__global__ void __launch_bounds__(kT) k_ch_pcg(CgVec V, Mg<M> G, int precond, double tol, int maxiter, double *partials,
+__global__ void __launch_bounds__(kT) k_ch_pcg(CgVec V, mg::Hier<M> G, int precond, double tol, int maxiter, double *partials,
                                                int *out_it, double *out_rel) {
   cg::grid_group grid = cg::this_grid();
   __shared__ double sh[40];
@@ -761,16 +513,11 @@ __global__ void __launch_bounds__(kT) k_ch_pcg(CgVec V, Mg<M> G, int precond, do
   const int N0 = V.N0, N1 = V.N1, PX = N0 + 2, PXY = (N0 + 2) * (N1 + 2);
   const long long n = (long long)N0 * N1 * V.N2;
   int buf = 0;
-  const Lv<M> &L0 = G.lv[0];
+  const mg::Level<M> &L0 = G.lv[0];
   if (precond) {
-    mg_build_fine(V, L0, tid, T);
+    mg_fine_from_couplings(V, L0, tid, T);
     grid.sync();
-    for (int l = 0; l + 1 < G.L; ++l) {
-      mg_coarsen(G.lv[l], G.lv[l + 1], tid, T);
-      grid.sync();
-    }
-    mg_factor(G);
-    grid.sync();
+    mg::build(G, false, grid, tid, T);
   }
   double acc = 0.0;
   for (long long e = tid; e < n; e += T) {
@@ -785,7 +532,7 @@ __global__ void __launch_bounds__(kT) k_ch_pcg(CgVec V, Mg<M> G, int precond, do
     return;
   }
   const double eps = tol * tol;
-  if (precond) mg_vcycle(G, grid, tid, T);
+  if (precond) mg::vcycle(G, false, grid, tid, T);
   acc = 0.0;
   for (long long e = tid; e < n; e += T) {
     const int q = pq(N0, N1, (int)(e % N0), (int)((e / N0) % N1), (int)(e / ((long long)N0 * N1)));
@@ -818,7 +565,7 @@ __global__ void __launch_bounds__(kT) k_ch_pcg(CgVec V, Mg<M> G, int precond, do
     }
     rr = grid_sum(acc, partials, buf, sh, grid);
     if (rr / bb < eps) break;
-    if (precond) mg_vcycle(G, grid, tid, T);
+    if (precond) mg::vcycle(G, false, grid, tid, T);
     acc = 0.0;
     for (long long e = tid; e < n; e += T) {
       const int q = pq(N0, N1, (int)(e % N0), (int)((e / N0) % N1), (int)(e / ((long long)N0 * N1)));
@@ -877,8 +624,8 @@ struct ChannelState {
   ChDev<double> Hd{};
   ChDev<float> Hf{};
   CgVec V{};
-  Mg<double> Gd{};
-  Mg<float> Gf{};
+  mg::Hier<double> Gd{};
+  mg::Hier<float> Gf{};
   int mom_blocks = 0, pcg_grid = 0;
   double *mom_part = nullptr, *cont_part = nullptr, *pcg_part = nullptr, *res = nullptr, *pcg_rel = nullptr;
   int *pcg_it = nullptr;
@@ -886,6 +633,10 @@ struct ChannelState {
   std::vector<double> kratio, qcell;
   ChStats st{};
   int iter = 0;
+  bool prof = false;
+  cudaEvent_t ev[6] = {};
+  double prof_ms[5] = {0, 0, 0, 0, 0};
+  int prof_steps = 0;
 
   template <class T_>
   T_ *alloc(size_t n) {
@@ -899,6 +650,8 @@ struct ChannelState {
     return (T_ *)p;
   }
   ~ChannelState() {
+    for (cudaEvent_t e : ev)
+      if (e) cudaEventDestroy(e);
     if (cht) cht_destroy(cht);
     for (void *p : allocs) cudaFree(p);
     if (stream) cudaStreamDestroy(stream);
@@ -941,24 +694,25 @@ void setup_fields(ChannelState &S, ChDev<R> &H, const std::vector<double> (&d)[3
 }
 
 template <class M>
-void setup_mg(ChannelState &S, Mg<M> &G) {
+void setup_mg(ChannelState &S, mg::Hier<M> &G) {
   int nx = S.N0, ny = S.N1, nz = S.N2, L = 0;
   while (true) {
-    if (L >= kMaxLv) throw std::runtime_error("multigrid: too many levels");
-    Lv<M> &l = G.lv[L];
+    if (L >= mg::kMgMaxLv) throw std::runtime_error("multigrid: too many levels");
+    mg::Level<M> &l = G.lv[L];
     l.nx = nx; l.ny = ny; l.nz = nz;
     const size_t np = (size_t)(nx + 2) * (ny + 2) * (nz + 2);
     l.x = S.alloc<M>(np); l.rhs = S.alloc<M>(np);
-    l.ax = S.alloc<M>(np); l.ay = S.alloc<M>(np); l.az = S.alloc<M>(np);
+    l.gx = S.alloc<M>(np); l.gy = S.alloc<M>(np); l.gz = S.alloc<M>(np);
+    l.fx = l.fy = l.fz = nullptr;
     l.m = S.alloc<uint8_t>(np);
     ++L;
-    if ((long long)nx * ny * nz <= kMaxCoarse) break;
+    if ((long long)nx * ny * nz <= mg::kMgCoarse) break;
     nx = (nx + 1) / 2; ny = (ny + 1) / 2; nz = (nz + 1) / 2;
   }
   G.L = L;
-  G.lu = S.alloc<double>((size_t)kMaxCoarse * kMaxCoarse);
-  G.piv = S.alloc<int>(kMaxCoarse);
-  G.y = S.alloc<double>(kMaxCoarse);
+  G.lu = S.alloc<double>((size_t)mg::kMgCoarse * mg::kMgCoarse);
+  G.piv = S.alloc<int>(mg::kMgCoarse);
+  G.y = S.alloc<double>(mg::kMgCoarse);
 }
 
 template <class R>
@@ -972,11 +726,14 @@ void mom_solve(ChannelState &S, ChDev<R> &H) {
 
 template <class R>
 void step_once(ChannelState &S, ChDev<R> &H, int flags) {
+  if (S.prof) CH_CUDA(cudaEventRecord(S.ev[0], S.stream));
   mom_solve(S, H);
+  if (S.prof) CH_CUDA(cudaEventRecord(S.ev[1], S.stream));
   k_ch_passemble<R><<<dim3(S.mom_blocks, 4), kT, 0, S.stream>>>(H, (double *)S.V.acx, (double *)S.V.acy, (double *)S.V.acz,
                                                                 S.V.r, S.V.x, S.cont_part);
   k_ch_finalize<<<1, 32, 0, S.stream>>>(S.mom_part, S.cont_part, S.mom_blocks, S.res);
   CH_CUDA(cudaGetLastError());
+  if (S.prof) CH_CUDA(cudaEventRecord(S.ev[2], S.stream));
   if (!(flags & 1)) {
     const int pre = S.prm.p_precond ? 1 : 0;
     if (S.mixed)
@@ -990,9 +747,12 @@ void step_once(ChannelState &S, ChDev<R> &H, int flags) {
     k_zero<<<blocks_for(np), kT, 0, S.stream>>>(S.V.x, np);
     CH_CUDA(cudaMemsetAsync(S.pcg_it, 0, sizeof(int), S.stream));
   }
+  if (S.prof) CH_CUDA(cudaEventRecord(S.ev[3], S.stream));
   k_ch_correct<R><<<dim3(S.mom_blocks, 4), kT, 0, S.stream>>>(H, (const double *)S.V.x);
   CH_CUDA(cudaGetLastError());
+  if (S.prof) CH_CUDA(cudaEventRecord(S.ev[4], S.stream));
   if (!(flags & 2)) cht_energy_step(S.cht, S.prm.alpha_t, S.prm.t_tol, S.prm.t_maxiter);
+  if (S.prof) CH_CUDA(cudaEventRecord(S.ev[5], S.stream));
 }
 
 void read_stats(ChannelState &S, int flags) {
@@ -1004,6 +764,14 @@ void read_stats(ChannelState &S, int flags) {
   CH_CUDA(cudaMemcpyAsync(&prel, S.pcg_rel, 8, cudaMemcpyDeviceToHost, S.stream));
   CH_CUDA(cudaStreamSynchronize(S.stream));
   for (int a = 0; a < 4; ++a) S.st.res[a] = r[a];
+  if (S.prof) {
+    for (int ph = 0; ph < 5; ++ph) {
+      float ms = 0;
+      CH_CUDA(cudaEventElapsedTime(&ms, S.ev[ph], S.ev[ph + 1]));
+      S.prof_ms[ph] += ms;
+    }
+    S.prof_steps++;
+  }
   S.st.pcg_iters = (flags & 1) ? 0 : pit;
   S.st.pcg_relres = (flags & 1) ? 0.0 : prel;
   if (!(flags & 2)) {
@@ -1098,6 +866,7 @@ ChannelState *ch_create(const Case &c, const ChParams &p, int device) {
   cs.xs = c.deck.xs.data(); cs.ys = c.deck.ys.data(); cs.zs = c.deck.zs.data();
   cs.ctype = c.ctype.data(); cs.region = S->region.data();
   cs.t_boundary = p.t_in; cs.tol = 1e-10; cs.maxiter = 5000; cs.bc = 1;
+  cs.precond = p.precision == 1 ? 1 : 2;
   S->cht = cht_create(cs);
   cht_bind_velocities(S->cht, uarr(S.get(), 0), uarr(S.get(), 1), uarr(S.get(), 2));
   S->kratio.assign(S->nreg, 100.0);
@@ -1240,6 +1009,20 @@ void ch_set_field(ChannelState *S, int f, const double *host, long n) {
   if (f == 3) { put_dev(S, S->mixed ? S->Hf.p : S->Hd.p, host, n); return; }
   put_dev(S, uarr(S, f), host, n);
   if (S->mixed) put_dev(S, f == 0 ? S->Hf.C0 : f == 1 ? S->Hf.C1 : S->Hf.C2, host, n);
+}
+
+void ch_profile(ChannelState *S, bool on) {
+  CH_CUDA(cudaSetDevice(S->device));
+  if (on && !S->ev[0])
+    for (cudaEvent_t &e : S->ev) CH_CUDA(cudaEventCreate(&e));
+  S->prof = on;
+  for (double &m : S->prof_ms) m = 0.0;
+  S->prof_steps = 0;
+}
+
+int ch_profile_read(const ChannelState *S, double *ms5) {
+  for (int ph = 0; ph < 5; ++ph) ms5[ph] = S->prof_ms[ph];
+  return S->prof_steps;
 }
 
 void *ch_stream(ChannelState *S) { return S->stream; }

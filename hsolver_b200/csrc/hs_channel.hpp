@@ -43,6 +43,10 @@ long ch_field_size(const ChannelState *s, int f);
 void ch_get_field(ChannelState *s, int f, double *host, long n);
 void ch_set_field(ChannelState *s, int f, const double *host, long n);
 void *ch_stream(ChannelState *s);
+// per-phase CUDA-event times (momentum, p' assembly, p' solve, correction,
+// energy), summed over the steps since profiling was switched on
+void ch_profile(ChannelState *s, bool on);
+int ch_profile_read(const ChannelState *s, double *ms5);
 void ch_sync(ChannelState *s);
 long long ch_device_bytes(const ChannelState *s);
 // energy adjoint on the current (frozen) flow: forward solve of the energy

@@ -13,7 +13,9 @@
 //   (sum G + max(F,0)) T_P - sum (G + max(-F,0)) T_N = q_P V_P + boundary terms.
 // The transposed operator has the same stencil with the upwind side swapped:
 // A^T_{P,N} = A_{N,P}, read from the neighbour's stored coefficient.
-// Both solves use the same cooperative Jacobi-preconditioned BiCGStab.
+// Both solves use the same cooperative BiCGStab, preconditioned by the
+// geometric multigrid V-cycle of hs_mg.cuh on the same operator (or by
+// Jacobi).
 #include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
@@ -25,6 +27,7 @@
 #include <vector>
 
 #include "hs_cht.hpp"
+#include "hs_mg.cuh"
 
 namespace cg = cooperative_groups;
 
@@ -158,10 +161,71 @@ struct Vec {
 
 // Jacobi-preconditioned BiCGStab (van der Vorst, SIAM J. Sci. Stat. Comput.
 // 13(2), 1992) for A x = rhs or A^T x = rhs; x holds the start.
+// level 0 of the multigrid hierarchy: each cell's low-face conductance and +
+// direction flux; the ghost past each high end carries that boundary face
+template <class MT>
+__device__ void cht_mg_fine(const ChtDev &H, const mg::Level<MT> &L0, int tid, int T) {
+  const int PX = H.Nx + 2, PY = H.Ny + 2;
+  const long long np = (long long)PX * PY * (H.Nz + 2);
+  for (long long q = tid; q < np; q += T) {
+    const int i = (int)(q % PX) - 1, j = (int)((q / PX) % PY) - 1, k = (int)(q / ((long long)PX * PY)) - 1;
+    const bool iin = i >= 0 && i < H.Nx, jin = j >= 0 && j < H.Ny, kin = k >= 0 && k < H.Nz;
+    double G, F;
+    bool has;
+    MT g = MT(0), f = MT(0);
+    if (jin && kin && i >= 0 && i <= H.Nx) {
+      if (i < H.Nx) { face(H, i, j, k, 0, G, F, has); g = (MT)G; f = (MT)(-F); }
+      else { face(H, H.Nx - 1, j, k, 1, G, F, has); g = (MT)G; f = (MT)F; }
+    }
+    L0.gx[q] = g; L0.fx[q] = f;
+    g = MT(0); f = MT(0);
+    if (iin && kin && j >= 0 && j <= H.Ny) {
+      if (j < H.Ny) { face(H, i, j, k, 2, G, F, has); g = (MT)G; f = (MT)(-F); }
+      else { face(H, i, H.Ny - 1, k, 3, G, F, has); g = (MT)G; f = (MT)F; }
+    }
+    L0.gy[q] = g; L0.fy[q] = f;
+    g = MT(0); f = MT(0);
+    if (iin && jin && k >= 0 && k <= H.Nz) {
+      if (k < H.Nz) { face(H, i, j, k, 4, G, F, has); g = (MT)G; f = (MT)(-F); }
+      else { face(H, i, j, H.Nz - 1, 5, G, F, has); g = (MT)G; f = (MT)F; }
+    }
+    L0.gz[q] = g; L0.fz[q] = f;
+  }
+}
+
+// z = M^-1 v at the interior cells: a V-cycle, or Jacobi when G.L == 0
+template <class MT>
+__device__ void cht_precond(const ChtDev &H, const mg::Hier<MT> &G, const double *v, double *z, bool tr,
+                            cg::grid_group &grid, int tid, int T) {
+  const int Nx = H.Nx, Ny = H.Ny, n = Nx * H.Ny * H.Nz;
+  if (G.L == 0) {
+    for (int c = tid; c < n; c += T) {
+      const int q = pidx(H, c % Nx, (c / Nx) % Ny, c / (Nx * Ny));
+      z[q] = v[q] * H.dinv[q];
+    }
+    grid.sync();
+    return;
+  }
+  const mg::Level<MT> &L0 = G.lv[0];
+  for (int c = tid; c < n; c += T) {
+    const int q = pidx(H, c % Nx, (c / Nx) % Ny, c / (Nx * Ny));
+    L0.rhs[q] = (MT)v[q];
+  }
+  grid.sync();
+  mg::vcycle(G, tr, grid, tid, T);
+  for (int c = tid; c < n; c += T) {
+    const int q = pidx(H, c % Nx, (c / Nx) % Ny, c / (Nx * Ny));
+    z[q] = (double)__ldcg(L0.x + q);
+  }
+  grid.sync();
+}
+
+// Right-preconditioned BiCGStab; x holds the start.
 // rel0: stop on ||r|| / ||r0|| instead of ||r|| / ||rhs||; out_r0 = ||r0||.
-__global__ void __launch_bounds__(kB) k_cht_bicgstab(ChtDev H, Vec V, const double *rhs, int transpose, double tol,
-                                                     int maxiter, double *partials, int *out_it, double *out_rel,
-                                                     int rel0, double *out_r0) {
+template <class MT>
+__global__ void __launch_bounds__(kB) k_cht_bicgstab(ChtDev H, Vec V, mg::Hier<MT> Gm, const double *rhs, int transpose,
+                                                     double tol, int maxiter, double *partials, int *out_it,
+                                                     double *out_rel, int rel0, double *out_r0) {
   cg::grid_group grid = cg::this_grid();
   __shared__ double sh[48];
   const int Nx = H.Nx, Ny = H.Ny, n = Nx * H.Ny * H.Nz;
@@ -169,6 +233,11 @@ __global__ void __launch_bounds__(kB) k_cht_bicgstab(ChtDev H, Vec V, const doub
   const int tid = blockIdx.x * blockDim.x + threadIdx.x, T = gridDim.x * blockDim.x;
   const bool tr = transpose != 0;
   int buf = 0;
+  if (Gm.L > 0) {
+    cht_mg_fine(H, Gm.lv[0], tid, T);
+    grid.sync();
+    mg::build(Gm, tr, grid, tid, T);
+  }
   double red[2] = {0.0, 0.0};
   for (int c = tid; c < n; c += T) {
     const int q = pidx(H, c % Nx, (c / Nx) % Ny, c / (Nx * Ny));
@@ -198,9 +267,9 @@ __global__ void __launch_bounds__(kB) k_cht_bicgstab(ChtDev H, Vec V, const doub
       const int q = pidx(H, c % Nx, (c / Nx) % Ny, c / (Nx * Ny));
       const double pv = V.r[q] + beta * (V.p[q] - omega * V.v[q]);
       V.p[q] = pv;
-      V.ph[q] = pv * H.dinv[q];
     }
     grid.sync();
+    cht_precond(H, Gm, V.p, V.ph, tr, grid, tid, T);
     double s2[1] = {0.0};
     for (int c = tid; c < n; c += T) {
       const int q = pidx(H, c % Nx, (c / Nx) % Ny, c / (Nx * Ny));
@@ -215,7 +284,6 @@ __global__ void __launch_bounds__(kB) k_cht_bicgstab(ChtDev H, Vec V, const doub
       const int q = pidx(H, c % Nx, (c / Nx) % Ny, c / (Nx * Ny));
       const double sv = V.r[q] - alpha * V.v[q];
       V.s[q] = sv;
-      V.sh[q] = sv * H.dinv[q];
       s3[0] += sv * sv;
     }
     grid_sums<1>(s3, partials, buf, sh, grid);
@@ -227,6 +295,7 @@ __global__ void __launch_bounds__(kB) k_cht_bicgstab(ChtDev H, Vec V, const doub
       rr = s3[0];
       break;
     }
+    cht_precond(H, Gm, V.s, V.sh, tr, grid, tid, T);
     double s4[2] = {0.0, 0.0};
     for (int c = tid; c < n; c += T) {
       const int q = pidx(H, c % Nx, (c / Nx) % Ny, c / (Nx * Ny));
@@ -385,6 +454,9 @@ struct ChtState {
   std::vector<uint8_t> ctype;
   double J = 0;
   bool have_T = false;
+  int precond = 0;              // 0 Jacobi, 1 V-cycle FP32, 2 V-cycle FP64
+  mg::Hier<float> Gf{};
+  mg::Hier<double> Gd{};
   template <class T_>
   T_ *alloc(size_t n) {
     void *p = nullptr;
@@ -398,6 +470,30 @@ struct ChtState {
     for (void *p : allocs) cudaFree(p);
   }
 };
+
+namespace {
+template <class MT>
+void setup_levels(ChtState &C, mg::Hier<MT> &G) {
+  int nx = C.H.Nx, ny = C.H.Ny, nz = C.H.Nz, L = 0;
+  while (true) {
+    if (L >= mg::kMgMaxLv) throw std::runtime_error("multigrid: too many levels");
+    mg::Level<MT> &l = G.lv[L];
+    l.nx = nx; l.ny = ny; l.nz = nz;
+    const size_t np = (size_t)(nx + 2) * (ny + 2) * (nz + 2);
+    l.x = C.alloc<MT>(np); l.rhs = C.alloc<MT>(np);
+    l.gx = C.alloc<MT>(np); l.gy = C.alloc<MT>(np); l.gz = C.alloc<MT>(np);
+    l.fx = C.alloc<MT>(np); l.fy = C.alloc<MT>(np); l.fz = C.alloc<MT>(np);
+    l.m = nullptr;
+    ++L;
+    if ((long long)nx * ny * nz <= mg::kMgCoarse) break;
+    nx = (nx + 1) / 2; ny = (ny + 1) / 2; nz = (nz + 1) / 2;
+  }
+  G.L = L;
+  G.lu = C.alloc<double>((size_t)mg::kMgCoarse * mg::kMgCoarse);
+  G.piv = C.alloc<int>(mg::kMgCoarse);
+  G.y = C.alloc<double>(mg::kMgCoarse);
+}
+}  // namespace
 
 ChtState *cht_create(const ChtSetup &S) {
   HC_CUDA(cudaSetDevice(S.device));
@@ -443,7 +539,11 @@ ChtState *cht_create(const ChtSetup &S) {
   for (double **v : vec) *v = C->alloc<double>(np);
   C->T = C->alloc<double>(np); C->lam = C->alloc<double>(np); C->g = C->alloc<double>(np);
   C->dJdq = C->alloc<double>(n); C->dkc = C->alloc<double>(n);
-  C->grid = coop_grid((const void *)k_cht_bicgstab, S.device);
+  C->precond = S.precond;
+  if (S.precond == 1) setup_levels(*C, C->Gf);
+  if (S.precond == 2) setup_levels(*C, C->Gd);
+  C->grid = std::min(coop_grid((const void *)k_cht_bicgstab<float>, S.device),
+                     coop_grid((const void *)k_cht_bicgstab<double>, S.device));
   C->partials = C->alloc<double>((size_t)2 * C->grid * 2 + 4096);
   C->res = C->alloc<double>(2); C->it = C->alloc<int>(1);
   HC_CUDA(cudaStreamSynchronize(C->stream));
@@ -507,6 +607,18 @@ void launch_coop(K kernel, int blocks, cudaStream_t s, A... args) {
   HC_CUDA(cudaLaunchCooperativeKernel((void *)kernel, dim3(blocks), dim3(kB), argv, 0, s));
 }
 
+void solve(ChtState *C, const double *rhs, int transpose, double tol, int maxiter, int rel0, double *out_r0) {
+  if (C->precond == 2)
+    launch_coop(k_cht_bicgstab<double>, C->grid, C->stream, C->H, C->V, C->Gd, rhs, transpose, tol, maxiter, C->partials,
+                C->it, C->res, rel0, out_r0);
+  else {
+    mg::Hier<float> G = C->Gf;
+    if (C->precond == 0) G.L = 0;
+    launch_coop(k_cht_bicgstab<float>, C->grid, C->stream, C->H, C->V, G, rhs, transpose, tol, maxiter, C->partials,
+                C->it, C->res, rel0, out_r0);
+  }
+}
+
 void unpad(const ChtDev &H, const double *dev, double *host, cudaStream_t s) {
   const size_t np = (size_t)(H.Nx + 2) * (H.Ny + 2) * (H.Nz + 2);
   std::vector<double> tmp(np);
@@ -539,8 +651,7 @@ void cht_forward(ChtState *C, double *T_host, double *J, int *iters, double *rel
   const size_t np = (size_t)(H.Nx + 2) * (H.Ny + 2) * (H.Nz + 2);
   k_cht_assemble<<<gfor((long long)H.Nx * H.Ny * H.Nz), kB, 0, C->stream>>>(H, C->Tb);
   k_cht_fill<<<gfor((long long)H.Nx * H.Ny * H.Nz), kB, 0, C->stream>>>(H.Nx * H.Ny * H.Nz, H.Nx, H.Ny, C->Tb, C->V.x);
-  launch_coop(k_cht_bicgstab, C->grid, C->stream, H, C->V, (const double *)H.b, 0, C->tol, C->maxiter, C->partials, C->it,
-              C->res, 0, (double *)nullptr);
+  solve(C, H.b, 0, C->tol, C->maxiter, 0, nullptr);
   HC_CUDA(cudaMemcpyAsync(C->T, C->V.x, np * 8, cudaMemcpyDeviceToDevice, C->stream));
   int it = 0;
   double rr = 0;
@@ -563,8 +674,7 @@ void cht_adjoint(ChtState *C, double *dJdq_host, double *dJdk_host, int *iters, 
   const long long n = (long long)H.Nx * H.Ny * H.Nz;
   objective(C, true);
   HC_CUDA(cudaMemsetAsync(C->V.x, 0, np * 8, C->stream));
-  launch_coop(k_cht_bicgstab, C->grid, C->stream, H, C->V, (const double *)C->g, 1, C->tol, C->maxiter, C->partials, C->it,
-              C->res, 0, (double *)nullptr);
+  solve(C, C->g, 1, C->tol, C->maxiter, 0, nullptr);
   HC_CUDA(cudaMemcpyAsync(C->lam, C->V.x, np * 8, cudaMemcpyDeviceToDevice, C->stream));
   k_cht_grad<<<gfor(n), kB, 0, C->stream>>>(H, C->T, C->lam, C->Tb, C->dJdq, C->dkc);
   std::vector<double> dq(n), dk(n);
@@ -606,8 +716,7 @@ void cht_energy_step(ChtState *C, double alpha_t, double tol, int maxiter) {
   const size_t np = (size_t)(H.Nx + 2) * (H.Ny + 2) * (H.Nz + 2);
   k_cht_assemble<<<gfor(n), kB, 0, C->stream>>>(H, C->Tb);
   HC_CUDA(cudaMemcpyAsync(C->V.x, C->T, np * 8, cudaMemcpyDeviceToDevice, C->stream));
-  launch_coop(k_cht_bicgstab, C->grid, C->stream, H, C->V, (const double *)H.b, 0, tol, maxiter, C->partials, C->it,
-              C->res, 1, C->res + 1);
+  solve(C, H.b, 0, tol, maxiter, 1, C->res + 1);
   k_cht_relax<<<gfor(n), kB, 0, C->stream>>>(n, H.Nx, H.Ny, alpha_t, (const double *)C->V.x, C->T);
   HC_CUDA(cudaGetLastError());
   C->have_T = false;

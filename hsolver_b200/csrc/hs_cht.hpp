@@ -16,6 +16,7 @@ struct ChtSetup {
   int maxiter;
   int bc;                         // 0 Dirichlet t_boundary on every boundary face; 1 channel (Dirichlet at
                                   // x = 0, upwind outflow at x = Nx, adiabatic y / z walls)
+  int precond;                    // BiCGStab preconditioner: 0 Jacobi, 1 multigrid V-cycle in FP32, 2 in FP64
 };
 
 // where the face velocities come from: the fluid box's padded u*, v*, w*

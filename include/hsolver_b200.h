@@ -285,6 +285,12 @@ int hs_channel_field_size(hs_channel *h, int field, long long *n);
 int hs_channel_get_field(hs_channel *h, int field, double *host, long long n);
 int hs_channel_set_field(hs_channel *h, int field, const double *host, long long n);
 int hs_channel_stream(hs_channel *h, void **stream);
+/* Per-phase CUDA-event times of the outer step (HS_CH_NPHASE: momentum, p'
+ * assembly, p' solve, velocity/pressure correction, energy), summed over the
+ * steps since profiling was switched on (which resets them). */
+#define HS_CH_NPHASE 5
+int hs_channel_profile(hs_channel *h, int on);
+int hs_channel_profile_read(hs_channel *h, double ms[HS_CH_NPHASE], int *steps);
 int hs_channel_sync(hs_channel *h);
 /* Device memory the solver holds (bytes). */
 int hs_channel_device_bytes(hs_channel *h, long long *bytes);
