@@ -483,6 +483,15 @@ __device__ double grid_sum(double v, double *partials, int &buf, double *sh, cg:
   return a;
 }
 
+// padded index of the cell with flat index e (x fastest)
+__device__ __forceinline__ int cell_q(int e, int N0, int N1) {
+  const int row_ = e / N0, i = e - row_ * N0;
+  const int k = row_ / N1, j = row_ - k * N1;
+  return (i + 1) + (N0 + 2) * ((j + 1) + (N1 + 2) * (k + 1));
+}
+
+constexpr int kPcgBlocksPerSm = 3;
+
 template <class M>
 __device__ void mg_fine_from_couplings(const CgVec &V, const mg::Level<M> &L0, int tid, int T) {
   const int PX = V.N0 + 2, PY = V.N1 + 2;
@@ -505,13 +514,13 @@ __device__ __forceinline__ double cg_apply(const CgVec &V, const double *x, int 
 // PCG: r = b (assembled), x = 0; z = M r (V-cycle, or z = r when precond = 0);
 // s = A p, alpha = <r,z>/<s,p>, x += alpha p, r -= alpha s, stop on ||r||/||b|| < tol
 template <class M>
-__global__ void __launch_bounds__(kT) k_ch_pcg(CgVec V, mg::Hier<M> G, int precond, double tol, int maxiter, double *partials,
+__global__ void __launch_bounds__(kT, kPcgBlocksPerSm) k_ch_pcg(CgVec V, mg::Hier<M> G, int precond, double tol, int maxiter, double *partials,
                                                int *out_it, double *out_rel) {
   cg::grid_group grid = cg::this_grid();
   __shared__ double sh[40];
   const int tid = blockIdx.x * blockDim.x + threadIdx.x, T = gridDim.x * blockDim.x;
   const int N0 = V.N0, N1 = V.N1, PX = N0 + 2, PXY = (N0 + 2) * (N1 + 2);
-  const long long n = (long long)N0 * N1 * V.N2;
+  const int n = N0 * N1 * V.N2;
   int buf = 0;
   const mg::Level<M> &L0 = G.lv[0];
   if (precond) {
@@ -520,8 +529,8 @@ __global__ void __launch_bounds__(kT) k_ch_pcg(CgVec V, mg::Hier<M> G, int preco
     mg::build(G, false, grid, tid, T);
   }
   double acc = 0.0;
-  for (long long e = tid; e < n; e += T) {
-    const int q = pq(N0, N1, (int)(e % N0), (int)((e / N0) % N1), (int)(e / ((long long)N0 * N1)));
+  for (int e = tid; e < n; e += T) {
+    const int q = cell_q(e, N0, N1);
     const double rv = V.r[q];
     acc += rv * rv;
     if (precond) L0.rhs[q] = (M)rv;
@@ -534,8 +543,8 @@ __global__ void __launch_bounds__(kT) k_ch_pcg(CgVec V, mg::Hier<M> G, int preco
   const double eps = tol * tol;
   if (precond) mg::vcycle(G, false, grid, tid, T);
   acc = 0.0;
-  for (long long e = tid; e < n; e += T) {
-    const int q = pq(N0, N1, (int)(e % N0), (int)((e / N0) % N1), (int)(e / ((long long)N0 * N1)));
+  for (int e = tid; e < n; e += T) {
+    const int q = cell_q(e, N0, N1);
     const double z = precond ? (double)__ldcg(L0.x + q) : V.r[q];
     V.p[q] = z;
     acc += V.r[q] * z;
@@ -545,8 +554,8 @@ __global__ void __launch_bounds__(kT) k_ch_pcg(CgVec V, mg::Hier<M> G, int preco
   while (it < maxiter && !(rr / bb < eps)) {
     it++;
     acc = 0.0;
-    for (long long e = tid; e < n; e += T) {
-      const int q = pq(N0, N1, (int)(e % N0), (int)((e / N0) % N1), (int)(e / ((long long)N0 * N1)));
+    for (int e = tid; e < n; e += T) {
+      const int q = cell_q(e, N0, N1);
       const double sv = cg_apply(V, V.p, q, PX, PXY);
       V.s[q] = sv;
       acc += sv * __ldcg(V.p + q);
@@ -555,8 +564,8 @@ __global__ void __launch_bounds__(kT) k_ch_pcg(CgVec V, mg::Hier<M> G, int preco
     if (sp == 0.0) break;
     const double alpha = gamma / sp;
     acc = 0.0;
-    for (long long e = tid; e < n; e += T) {
-      const int q = pq(N0, N1, (int)(e % N0), (int)((e / N0) % N1), (int)(e / ((long long)N0 * N1)));
+    for (int e = tid; e < n; e += T) {
+      const int q = cell_q(e, N0, N1);
       V.x[q] = V.x[q] + alpha * V.p[q];
       const double rv = V.r[q] - alpha * V.s[q];
       V.r[q] = rv;
@@ -567,15 +576,15 @@ __global__ void __launch_bounds__(kT) k_ch_pcg(CgVec V, mg::Hier<M> G, int preco
     if (rr / bb < eps) break;
     if (precond) mg::vcycle(G, false, grid, tid, T);
     acc = 0.0;
-    for (long long e = tid; e < n; e += T) {
-      const int q = pq(N0, N1, (int)(e % N0), (int)((e / N0) % N1), (int)(e / ((long long)N0 * N1)));
+    for (int e = tid; e < n; e += T) {
+      const int q = cell_q(e, N0, N1);
       acc += V.r[q] * (precond ? (double)__ldcg(L0.x + q) : V.r[q]);
     }
     const double gnew = grid_sum(acc, partials, buf, sh, grid);
     const double beta = gnew / gamma;
     gamma = gnew;
-    for (long long e = tid; e < n; e += T) {
-      const int q = pq(N0, N1, (int)(e % N0), (int)((e / N0) % N1), (int)(e / ((long long)N0 * N1)));
+    for (int e = tid; e < n; e += T) {
+      const int q = cell_q(e, N0, N1);
       V.p[q] = (precond ? (double)__ldcg(L0.x + q) : V.r[q]) + beta * V.p[q];
     }
     grid.sync();

@@ -145,16 +145,6 @@ __global__ void k_cht_assemble(ChtDev H, double Tb) {
   }
 }
 
-// y = A x (transpose = 0) or A^T x at padded q
-__device__ __forceinline__ double apply_at(const ChtDev &H, const double *x, int q, int PX, int PXY, bool tr) {
-  const double off = tr ? H.ae[q - 1] * __ldcg(x + q - 1) + H.aw[q + 1] * __ldcg(x + q + 1) +
-                              H.an[q - PX] * __ldcg(x + q - PX) + H.as[q + PX] * __ldcg(x + q + PX) +
-                              H.af[q - PXY] * __ldcg(x + q - PXY) + H.ab[q + PXY] * __ldcg(x + q + PXY)
-                        : H.aw[q] * __ldcg(x + q - 1) + H.ae[q] * __ldcg(x + q + 1) + H.as[q] * __ldcg(x + q - PX) +
-                              H.an[q] * __ldcg(x + q + PX) + H.ab[q] * __ldcg(x + q - PXY) + H.af[q] * __ldcg(x + q + PXY);
-  return H.d[q] * __ldcg(x + q) - off;
-}
-
 struct Vec {
   double *x, *r, *rh, *p, *v, *ph, *s, *sh, *t;
 };
@@ -193,55 +183,53 @@ __device__ void cht_mg_fine(const ChtDev &H, const mg::Level<MT> &L0, int tid, i
   }
 }
 
-// z = M^-1 v at the interior cells: a V-cycle, or Jacobi when G.L == 0
-template <class MT>
-__device__ void cht_precond(const ChtDev &H, const mg::Hier<MT> &G, const double *v, double *z, bool tr,
-                            cg::grid_group &grid, int tid, int T) {
-  const int Nx = H.Nx, Ny = H.Ny, n = Nx * H.Ny * H.Nz;
-  if (G.L == 0) {
-    for (int c = tid; c < n; c += T) {
-      const int q = pidx(H, c % Nx, (c / Nx) % Ny, c / (Nx * Ny));
-      z[q] = v[q] * H.dinv[q];
-    }
-    grid.sync();
-    return;
-  }
-  const mg::Level<MT> &L0 = G.lv[0];
-  for (int c = tid; c < n; c += T) {
-    const int q = pidx(H, c % Nx, (c / Nx) % Ny, c / (Nx * Ny));
-    L0.rhs[q] = (MT)v[q];
-  }
-  grid.sync();
-  mg::vcycle(G, tr, grid, tid, T);
-  for (int c = tid; c < n; c += T) {
-    const int q = pidx(H, c % Nx, (c / Nx) % Ny, c / (Nx * Ny));
-    z[q] = (double)__ldcg(L0.x + q);
-  }
-  grid.sync();
+// y = A x (transpose = 0) or A^T x at padded q, x in any precision
+template <class XT>
+__device__ __forceinline__ double apply_any(const ChtDev &H, const XT *x, int q, int PX, int PXY, bool tr) {
+  const double off = tr ? H.ae[q - 1] * (double)__ldcg(x + q - 1) + H.aw[q + 1] * (double)__ldcg(x + q + 1) +
+                              H.an[q - PX] * (double)__ldcg(x + q - PX) + H.as[q + PX] * (double)__ldcg(x + q + PX) +
+                              H.af[q - PXY] * (double)__ldcg(x + q - PXY) + H.ab[q + PXY] * (double)__ldcg(x + q + PXY)
+                        : H.aw[q] * (double)__ldcg(x + q - 1) + H.ae[q] * (double)__ldcg(x + q + 1) +
+                              H.as[q] * (double)__ldcg(x + q - PX) + H.an[q] * (double)__ldcg(x + q + PX) +
+                              H.ab[q] * (double)__ldcg(x + q - PXY) + H.af[q] * (double)__ldcg(x + q + PXY);
+  return H.d[q] * (double)__ldcg(x + q) - off;
 }
 
-// Right-preconditioned BiCGStab; x holds the start.
+__device__ __forceinline__ int cell_pidx(const ChtDev &H, int c) {
+  const int row_ = c / H.Nx, i = c - row_ * H.Nx;
+  const int k = row_ / H.Ny, j = row_ - k * H.Ny;
+  return (i + 1) + (H.Nx + 2) * ((j + 1) + (H.Ny + 2) * (k + 1));
+}
+
+// Right-preconditioned BiCGStab (van der Vorst, SIAM J. Sci. Stat. Comput.
+// 13(2), 1992) for A x = rhs or A^T x = rhs; x holds the start.  The
+// preconditioner is the V-cycle of hs_mg.cuh on the same operator (Gm.L > 0)
+// or Jacobi.  With the V-cycle, the products A p^ and A s^ read the cycle's
+// output directly and store p^, s^ on the way; <r^, r> of the next iteration
+// is summed with <r, r>.
 // rel0: stop on ||r|| / ||r0|| instead of ||r|| / ||rhs||; out_r0 = ||r0||.
 template <class MT>
-__global__ void __launch_bounds__(kB) k_cht_bicgstab(ChtDev H, Vec V, mg::Hier<MT> Gm, const double *rhs, int transpose,
-                                                     double tol, int maxiter, double *partials, int *out_it,
-                                                     double *out_rel, int rel0, double *out_r0) {
+__global__ void __launch_bounds__(kB, 3) k_cht_bicgstab(ChtDev H, Vec V, mg::Hier<MT> Gm, const double *rhs,
+                                                        int transpose, double tol, int maxiter, double *partials,
+                                                        int *out_it, double *out_rel, int rel0, double *out_r0) {
   cg::grid_group grid = cg::this_grid();
   __shared__ double sh[48];
   const int Nx = H.Nx, Ny = H.Ny, n = Nx * H.Ny * H.Nz;
   const int PX = Nx + 2, PXY = (Nx + 2) * (Ny + 2);
   const int tid = blockIdx.x * blockDim.x + threadIdx.x, T = gridDim.x * blockDim.x;
-  const bool tr = transpose != 0;
+  const bool tr = transpose != 0, mgp = Gm.L > 0;
+  const MT *z = mgp ? Gm.lv[0].x : nullptr;
+  MT *zr = mgp ? Gm.lv[0].rhs : nullptr;
   int buf = 0;
-  if (Gm.L > 0) {
+  if (mgp) {
     cht_mg_fine(H, Gm.lv[0], tid, T);
     grid.sync();
     mg::build(Gm, tr, grid, tid, T);
   }
   double red[2] = {0.0, 0.0};
   for (int c = tid; c < n; c += T) {
-    const int q = pidx(H, c % Nx, (c / Nx) % Ny, c / (Nx * Ny));
-    const double rv = rhs[q] - apply_at(H, V.x, q, PX, PXY, tr);
+    const int q = cell_pidx(H, c);
+    const double rv = rhs[q] - apply_any(H, V.x, q, PX, PXY, tr);
     V.r[q] = rv; V.rh[q] = rv; V.p[q] = 0.0; V.v[q] = 0.0;
     red[0] += rhs[q] * rhs[q];
     red[1] += rv * rv;
@@ -251,29 +239,26 @@ __global__ void __launch_bounds__(kB) k_cht_bicgstab(ChtDev H, Vec V, mg::Hier<M
   if (bb == 0) bb = 1.0;
   if (tid == 0 && out_r0) *out_r0 = sqrt(rr);
   const double eps = tol * tol;
-  double rho = 1.0, alpha = 1.0, omega = 1.0;
+  double rho = 1.0, alpha = 1.0, omega = 1.0, rho1 = red[1];
   int it = 0;
   while (it < maxiter && !(rr / bb < eps)) {
     it++;
-    double s1[1] = {0.0};
-    for (int c = tid; c < n; c += T) {
-      const int q = pidx(H, c % Nx, (c / Nx) % Ny, c / (Nx * Ny));
-      s1[0] += V.rh[q] * V.r[q];
-    }
-    grid_sums<1>(s1, partials, buf, sh, grid);
-    const double rho1 = s1[0];
     const double beta = (rho1 / rho) * (alpha / omega);
     for (int c = tid; c < n; c += T) {
-      const int q = pidx(H, c % Nx, (c / Nx) % Ny, c / (Nx * Ny));
+      const int q = cell_pidx(H, c);
       const double pv = V.r[q] + beta * (V.p[q] - omega * V.v[q]);
       V.p[q] = pv;
+      if (mgp) zr[q] = (MT)pv;
+      else V.ph[q] = pv * H.dinv[q];
     }
     grid.sync();
-    cht_precond(H, Gm, V.p, V.ph, tr, grid, tid, T);
+    if (mgp) mg::vcycle(Gm, tr, grid, tid, T);
     double s2[1] = {0.0};
     for (int c = tid; c < n; c += T) {
-      const int q = pidx(H, c % Nx, (c / Nx) % Ny, c / (Nx * Ny));
-      const double vv = apply_at(H, V.ph, q, PX, PXY, tr);
+      const int q = cell_pidx(H, c);
+      double vv;
+      if (mgp) { V.ph[q] = (double)__ldcg(z + q); vv = apply_any(H, z, q, PX, PXY, tr); }
+      else vv = apply_any(H, V.ph, q, PX, PXY, tr);
       V.v[q] = vv;
       s2[0] += V.rh[q] * vv;
     }
@@ -281,42 +266,48 @@ __global__ void __launch_bounds__(kB) k_cht_bicgstab(ChtDev H, Vec V, mg::Hier<M
     alpha = rho1 / s2[0];
     double s3[1] = {0.0};
     for (int c = tid; c < n; c += T) {
-      const int q = pidx(H, c % Nx, (c / Nx) % Ny, c / (Nx * Ny));
+      const int q = cell_pidx(H, c);
       const double sv = V.r[q] - alpha * V.v[q];
       V.s[q] = sv;
+      if (mgp) zr[q] = (MT)sv;
+      else V.sh[q] = sv * H.dinv[q];
       s3[0] += sv * sv;
     }
     grid_sums<1>(s3, partials, buf, sh, grid);
     if (s3[0] / bb < eps) {
       for (int c = tid; c < n; c += T) {
-        const int q = pidx(H, c % Nx, (c / Nx) % Ny, c / (Nx * Ny));
+        const int q = cell_pidx(H, c);
         V.x[q] += alpha * V.ph[q];
       }
       rr = s3[0];
       break;
     }
-    cht_precond(H, Gm, V.s, V.sh, tr, grid, tid, T);
+    if (mgp) mg::vcycle(Gm, tr, grid, tid, T);
     double s4[2] = {0.0, 0.0};
     for (int c = tid; c < n; c += T) {
-      const int q = pidx(H, c % Nx, (c / Nx) % Ny, c / (Nx * Ny));
-      const double tv = apply_at(H, V.sh, q, PX, PXY, tr);
+      const int q = cell_pidx(H, c);
+      double tv;
+      if (mgp) { V.sh[q] = (double)__ldcg(z + q); tv = apply_any(H, z, q, PX, PXY, tr); }
+      else tv = apply_any(H, V.sh, q, PX, PXY, tr);
       V.t[q] = tv;
       s4[0] += tv * V.s[q];
       s4[1] += tv * tv;
     }
     grid_sums<2>(s4, partials, buf, sh, grid);
     omega = s4[0] / s4[1];
-    double s5[1] = {0.0};
+    double s5[2] = {0.0, 0.0};
     for (int c = tid; c < n; c += T) {
-      const int q = pidx(H, c % Nx, (c / Nx) % Ny, c / (Nx * Ny));
+      const int q = cell_pidx(H, c);
       V.x[q] += alpha * V.ph[q] + omega * V.sh[q];
       const double rv = V.s[q] - omega * V.t[q];
       V.r[q] = rv;
       s5[0] += rv * rv;
+      s5[1] += V.rh[q] * rv;
     }
-    grid_sums<1>(s5, partials, buf, sh, grid);
+    grid_sums<2>(s5, partials, buf, sh, grid);
     rr = s5[0];
     rho = rho1;
+    rho1 = s5[1];
   }
   if (tid == 0) { *out_it = it; *out_rel = sqrt(rr / bb); }
 }

@@ -95,10 +95,11 @@ __device__ __forceinline__ bool unknown(const Level<M> &L, int q) { return L.m ?
 // coarse level C from fine level F (every padded cell of C that holds a face)
 template <class M>
 __device__ void coarsen(const Level<M> &F, const Level<M> &C, int tid, int T) {
-  const long long n = (long long)(C.nx + 1) * (C.ny + 1) * (C.nz + 1);
+  const int n = (C.nx + 1) * (C.ny + 1) * (C.nz + 1);
   const bool conv = F.fx != nullptr;
-  for (long long e = tid; e < n; e += T) {
-    const int I = (int)(e % (C.nx + 1)), J = (int)((e / (C.nx + 1)) % (C.ny + 1)), K = (int)(e / ((long long)(C.nx + 1) * (C.ny + 1)));
+  for (int e = tid; e < n; e += T) {
+    const int row_ = e / (C.nx + 1), I = e - row_ * (C.nx + 1);
+    const int K = row_ / (C.ny + 1), J = row_ - K * (C.ny + 1);
     const int qc = idx(C, I + 1, J + 1, K + 1);
     if (J < C.ny && K < C.nz) {
       const int fi = min(2 * I, F.nx);
@@ -158,16 +159,18 @@ __device__ void coarsen(const Level<M> &F, const Level<M> &C, int tid, int T) {
   }
 }
 
+// a masked cell has zero couplings on every face (its faces touch a
+// non-unknown), so d == 0 identifies it without reading the mask
 template <class M>
 __device__ void smooth(const Level<M> &L, int color, bool zero_nb, bool tr, int tid, int T) {
   const int half = (L.nx + 1) / 2;
-  const long long n = (long long)half * L.ny * L.nz;
-  for (long long e = tid; e < n; e += T) {
-    const int m = (int)(e % half), j = (int)((e / half) % L.ny), k = (int)(e / ((long long)half * L.ny));
+  const int n = half * L.ny * L.nz;
+  for (int e = tid; e < n; e += T) {
+    const int row_ = e / half, m = e - row_ * half;
+    const int k = row_ / L.ny, j = row_ - k * L.ny;
     const int i = 2 * m + ((j + k + color) & 1);
     if (i >= L.nx) continue;
     const int q = idx(L, i + 1, j + 1, k + 1);
-    if (!unknown(L, q)) continue;
     M d, o[6];
     row(L, q, tr, d, o);
     if (d == M(0)) { L.x[q] = M(0); continue; }
@@ -180,9 +183,10 @@ __device__ void smooth(const Level<M> &L, int color, bool zero_nb, bool tr, int 
 // coarse rhs = sum over the children of (rhs - A x)
 template <class M>
 __device__ void restrict_res(const Level<M> &F, const Level<M> &C, bool tr, int tid, int T) {
-  const long long n = (long long)C.nx * C.ny * C.nz;
-  for (long long e = tid; e < n; e += T) {
-    const int I = (int)(e % C.nx), J = (int)((e / C.nx) % C.ny), K = (int)(e / ((long long)C.nx * C.ny));
+  const int n = C.nx * C.ny * C.nz;
+  for (int e = tid; e < n; e += T) {
+    const int row_ = e / C.nx, I = e - row_ * C.nx;
+    const int K = row_ / C.ny, J = row_ - K * C.ny;
     M acc = M(0);
     for (int dk = 0; dk < 2; ++dk)
       for (int dj = 0; dj < 2; ++dj)
@@ -190,7 +194,6 @@ __device__ void restrict_res(const Level<M> &F, const Level<M> &C, bool tr, int 
           const int i = 2 * I + di, j = 2 * J + dj, k = 2 * K + dk;
           if (i >= F.nx || j >= F.ny || k >= F.nz) continue;
           const int q = idx(F, i + 1, j + 1, k + 1);
-          if (!unknown(F, q)) continue;
           M d, o[6];
           row(F, q, tr, d, o);
           acc += F.rhs[q] - (d * __ldcg(F.x + q) - offsum(F, o, F.x, q));
@@ -202,9 +205,10 @@ __device__ void restrict_res(const Level<M> &F, const Level<M> &C, bool tr, int 
 
 template <class M>
 __device__ void prolong(const Level<M> &F, const Level<M> &C, int tid, int T) {
-  const long long n = (long long)F.nx * F.ny * F.nz;
-  for (long long e = tid; e < n; e += T) {
-    const int i = (int)(e % F.nx), j = (int)((e / F.nx) % F.ny), k = (int)(e / ((long long)F.nx * F.ny));
+  const int n = F.nx * F.ny * F.nz;
+  for (int e = tid; e < n; e += T) {
+    const int row_ = e / F.nx, i = e - row_ * F.nx;
+    const int k = row_ / F.ny, j = row_ - k * F.ny;
     const int q = idx(F, i + 1, j + 1, k + 1);
     if (!unknown(F, q)) continue;
     F.x[q] = __ldcg(F.x + q) + __ldcg(C.x + idx(C, i / 2 + 1, j / 2 + 1, k / 2 + 1));
@@ -273,29 +277,37 @@ __device__ void factor(const Hier<M> &G, bool tr) {
   }
 }
 
-// exact solve on the coarsest level, by thread 0 of block 0
+// exact solve on the coarsest level, by warp 0 of block 0 (the permuted
+// right-hand side in shared memory, triangular solves with warp dot products)
 template <class M>
 __device__ void coarse_solve(const Hier<M> &G) {
-  if (threadIdx.x != 0) return;
+  if (threadIdx.x >= 32) return;
+  __shared__ double y[kMgCoarse];
   const Level<M> &C = G.lv[G.L - 1];
-  const int nc = C.nx * C.ny * C.nz;
-  double *y = G.y;
-  for (int r = 0; r < nc; ++r) y[r] = (double)C.rhs[idx(C, r % C.nx + 1, (r / C.nx) % C.ny + 1, r / (C.nx * C.ny) + 1)];
-  for (int c2 = 0; c2 < nc; ++c2) {
-    const int pr = G.piv[c2];
-    if (pr != c2) { const double t = y[c2]; y[c2] = y[pr]; y[pr] = t; }
+  const int nc = C.nx * C.ny * C.nz, lane = threadIdx.x;
+  if (lane == 0) {
+    for (int r = 0; r < nc; ++r) y[r] = (double)C.rhs[idx(C, r % C.nx + 1, (r / C.nx) % C.ny + 1, r / (C.nx * C.ny) + 1)];
+    for (int c2 = 0; c2 < nc; ++c2) {
+      const int pr = G.piv[c2];
+      if (pr != c2) { const double t = y[c2]; y[c2] = y[pr]; y[pr] = t; }
+    }
   }
+  __syncwarp();
   for (int r = 0; r < nc; ++r) {
-    double s = y[r];
-    for (int c2 = 0; c2 < r; ++c2) s -= G.lu[r * nc + c2] * y[c2];
-    y[r] = s;
+    double a = 0.0;
+    for (int c2 = lane; c2 < r; c2 += 32) a += G.lu[r * nc + c2] * y[c2];
+    for (int o = 16; o; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+    if (lane == 0) y[r] -= a;
+    __syncwarp();
   }
   for (int r = nc - 1; r >= 0; --r) {
-    double s = y[r];
-    for (int c2 = r + 1; c2 < nc; ++c2) s -= G.lu[r * nc + c2] * y[c2];
-    y[r] = s / G.lu[r * nc + r];
+    double a = 0.0;
+    for (int c2 = r + 1 + lane; c2 < nc; c2 += 32) a += G.lu[r * nc + c2] * y[c2];
+    for (int o = 16; o; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+    if (lane == 0) y[r] = (y[r] - a) / G.lu[r * nc + r];
+    __syncwarp();
   }
-  for (int r = 0; r < nc; ++r) {
+  for (int r = lane; r < nc; r += 32) {
     const int q = idx(C, r % C.nx + 1, (r / C.nx) % C.ny + 1, r / (C.nx * C.ny) + 1);
     C.x[q] = unknown(C, q) ? (M)y[r] : M(0);
   }
