@@ -364,6 +364,14 @@ int hs_case_geometry(const hs_case *c, int axis, double *out, long long n) {
   return HS_OK;
 }
 
+int hs_case_points(const hs_case *c, int axis, double *out, long long n) {
+  if (!c || !out || axis < 0 || axis > 2) return fail(nullptr, HS_ERR_ARG, "bad argument");
+  const std::vector<double> &v = axis == 0 ? c->c.deck.xs : axis == 1 ? c->c.deck.ys : c->c.deck.zs;
+  if (n != (long long)v.size()) return fail(nullptr, HS_ERR_ARG, "points size mismatch");
+  std::memcpy(out, v.data(), v.size() * sizeof(double));
+  return HS_OK;
+}
+
 void hs_case_destroy(hs_case *c) { delete c; }
 
 int hs_pcg_create(int nx, int ny, int nz, int device, hs_pcg **out) {

@@ -159,6 +159,8 @@ int hs_case_interface(const hs_case *c, long long *out5, long long n);
 /* Per padded index geometry {xp,xw,xe | yp,ys,yn | zp,zf,zb} of the fluid
  * box (fluid_solver.h:1248-1261); axis 0..2, out3 = 3 arrays of n+2. */
 int hs_case_geometry(const hs_case *c, int axis, double *out, long long n);
+/* The deck's grid points of one axis (N+1 values; CYCASMesh::xPoints etc.). */
+int hs_case_points(const hs_case *c, int axis, double *out, long long n);
 void hs_case_destroy(hs_case *c);
 
 /* Standalone pressure-correction solve, the counterpart of the reference's
