@@ -6,8 +6,11 @@ channel 2x1x1, inlet plug flow u = 1, zero-gradient outlet, no-slip walls,
 Re = 400, Pr = 0.71, 8 seeded solid blocks (edges 8-24 cells, seed 0) with a
 heat source q ~ U[0.5, 2] and k_solid/k_fluid ~ U[10, 1000] per block;
 relaxation 0.7 / 0.3 / 0.9; FP64 throughout (the plain form); pressure
-correction by multigrid-preconditioned CG to rtol 1e-8; energy over fluid and
-solid by multigrid-preconditioned BiCGStab.  Synthetic input generated
+correction by multigrid-preconditioned CG to the reference's rtol 1e-5
+(fluid_solver.h:1874); energy over fluid and solid by multigrid-preconditioned
+BiCGStab to 1e-1 of its initial residual per outer step.  (The number of outer
+steps to a 1e-6 global residual is the same, 1393, for p' rtol 1e-8 .. 1e-3
+and energy 1e-2 .. 1e-1: SIMPLE's rate is set by the relaxation.)  Synthetic input generated
 in-repo; the state (~790 MB on the device) is larger than L2.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
@@ -37,12 +40,15 @@ UNIT = "iter/s"
 PEAKS_FILE = os.path.join(HERE, "MEASURED_PEAKS.json")
 FALLBACK_HBM_GBS = 6650.0
 NAME = "config2"
+# inner tolerances of the at-scale case (config 1 keeps the library defaults,
+# p' rtol 1e-8 as its specification states)
+SOLVER = {"p_tol": 1e-5, "t_tol": 1e-1}
 CONFIG = {"workload": "channel 256x128x128 (4.19M cells), 8 seeded heated blocks (edges 8-24, q U[0.5,2], "
                       "k_s/k_f U[10,1000]), Re 400, SIMPLE-CHT outer step",
           "grid": [256, 128, 128], "blocks": 8, "seed": 0, "precision": "fp64", "re": 400, "pr": 0.71,
           "relaxation": {"u": 0.7, "p": 0.3, "T": 0.9}, "momentum": "FOU, 2 red-black GS sweeps",
-          "pressure_solver": "CG + multigrid V-cycle (FP64), rtol 1e-8",
-          "energy_solver": "BiCGStab + multigrid V-cycle (FP64), 1e-2 of the initial residual per step",
+          "pressure_solver": "CG + multigrid V-cycle (FP64), rtol 1e-5 (the reference's HYPRE setting)",
+          "energy_solver": "BiCGStab + multigrid V-cycle (FP64), 1e-1 of the initial residual per step",
           "l2_policy": "state ~790 MB on the device, larger than L2 (126 MB)", "parallelism": "replicas"}
 # launches per outer step: 4 momentum passes, p' assembly, residual finalize,
 # p' solve, correction, energy assembly, energy BiCGStab, energy relaxation
@@ -176,7 +182,7 @@ def run_gpu(args):
     ncell = int(ctype.size)
 
     def make(precision=0, **kw):
-        g = hsolver_b200.Channel(deck, device=local, re=re_, precision=precision, **kw)
+        g = hsolver_b200.Channel(deck, device=local, re=re_, precision=precision, **SOLVER, **kw)
         g.set_solid(k, q)
         g.init()
         return g
@@ -301,7 +307,7 @@ def time_to_residual(args, hsolver_b200, local):
         deck, re_, k, q, _ = workload(name)
         res, fields = {}, {}
         for prec, key in ((0, "fp64"), (1, "mixed")):
-            g = hsolver_b200.Channel(deck, device=local, re=re_, precision=prec)
+            g = hsolver_b200.Channel(deck, device=local, re=re_, precision=prec, **(SOLVER if name == NAME else {}))
             g.set_solid(k, q)
             g.init()
             g.sync()
@@ -344,7 +350,7 @@ def cpu_sample():
     after init, with the inner solves capped (CG 20, BiCGStab 2 iterations)."""
     from oracle import oracle
     deck, re_, k, q, _ = workload()
-    o = oracle.ChannelCase(deck, re=re_, p_maxiter=CPU_SAMPLE_P, t_maxiter=CPU_SAMPLE_T)
+    o = oracle.ChannelCase(deck, re=re_, p_maxiter=CPU_SAMPLE_P, t_maxiter=CPU_SAMPLE_T, **SOLVER)
     o.set_solid(k, q)
     o.init()
     t0 = time.perf_counter()

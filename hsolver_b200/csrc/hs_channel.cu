@@ -490,7 +490,9 @@ __device__ __forceinline__ int cell_q(int e, int N0, int N1) {
   return (i + 1) + (N0 + 2) * ((j + 1) + (N1 + 2) * (k + 1));
 }
 
-constexpr int kPcgBlocksPerSm = 3;
+// one 768-thread block per SM: the same warps per SM as three 256-thread
+// blocks, a third of the arrivals at every grid barrier
+constexpr int kPcgT = 768;
 
 template <class M>
 __device__ void mg_fine_from_couplings(const CgVec &V, const mg::Level<M> &L0, int tid, int T) {
@@ -514,7 +516,7 @@ __device__ __forceinline__ double cg_apply(const CgVec &V, const double *x, int 
 // PCG: r = b (assembled), x = 0; z = M r (V-cycle, or z = r when precond = 0);
 // s = A p, alpha = <r,z>/<s,p>, x += alpha p, r -= alpha s, stop on ||r||/||b|| < tol
 template <class M>
-__global__ void __launch_bounds__(kT, kPcgBlocksPerSm) k_ch_pcg(CgVec V, mg::Hier<M> G, int precond, double tol, int maxiter, double *partials,
+__global__ void __launch_bounds__(kPcgT, 1) k_ch_pcg(CgVec V, mg::Hier<M> G, int precond, double tol, int maxiter, double *partials,
                                                int *out_it, double *out_rel) {
   cg::grid_group grid = cg::this_grid();
   __shared__ double sh[40];
@@ -613,7 +615,7 @@ int blocks_for(long long n) { return (int)std::max<long long>(1, std::min<long l
 template <class K, class... A>
 void launch_coop(K kernel, int blocks, cudaStream_t s, A... args) {
   void *argv[] = {(void *)&args...};
-  CH_CUDA(cudaLaunchCooperativeKernel((void *)kernel, dim3(blocks), dim3(kT), argv, 0, s));
+  CH_CUDA(cudaLaunchCooperativeKernel((void *)kernel, dim3(blocks), dim3(kPcgT), argv, 0, s));
 }
 
 }  // namespace
@@ -859,8 +861,8 @@ ChannelState *ch_create(const Case &c, const ChParams &p, int device) {
   S->res = S->alloc<double>(4);
   int per = 0, nsm = 0;
   CH_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
-  if (S->mixed) CH_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_ch_pcg<float>, kT, 0));
-  else CH_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_ch_pcg<double>, kT, 0));
+  if (S->mixed) CH_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_ch_pcg<float>, kPcgT, 0));
+  else CH_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_ch_pcg<double>, kPcgT, 0));
   if (per < 1) throw std::runtime_error("pressure-correction kernel cannot be resident");
   S->pcg_grid = per * nsm;
   S->pcg_part = S->alloc<double>((size_t)2 * S->pcg_grid + 64);
@@ -955,69 +957,83 @@ long ch_field_size(const ChannelState *S, int f) {
 }
 
 namespace {
-template <class R>
-void get_dev(ChannelState *S, const R *src, double *host, long n) {
-  std::vector<R> tmp(n);
-  CH_CUDA(cudaMemcpyAsync(tmp.data(), src, n * sizeof(R), cudaMemcpyDeviceToHost, S->stream));
-  CH_CUDA(cudaStreamSynchronize(S->stream));
-  for (long i = 0; i < n; ++i) host[i] = (double)tmp[i];
+// device-side conversions for the field copies (the caller's host buffer is
+// copied to or from directly; pinned buffers go by DMA)
+__global__ void k_unpad(const double *src, double *dst, int N0, int N1, int N2) {
+  const int n = N0 * N1 * N2;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x)
+    dst[e] = src[cell_q(e, N0, N1)];
+}
+__global__ void k_pad(const double *src, double *dst, int N0, int N1, int N2) {
+  const int n = N0 * N1 * N2;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x)
+    dst[cell_q(e, N0, N1)] = src[e];
 }
 template <class R>
-void put_dev(ChannelState *S, R *dst, const double *host, long n) {
-  std::vector<R> tmp(host, host + n);
-  CH_CUDA(cudaMemcpyAsync(dst, tmp.data(), n * sizeof(R), cudaMemcpyHostToDevice, S->stream));
+__global__ void k_widen(const R *src, const double *add, double *dst, long long n) {
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x)
+    dst[e] = (double)src[e] + (add ? add[e] : 0.0);
+}
+__global__ void k_narrow(const double *src, float *dst, long long n) {
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x)
+    dst[e] = (float)src[e];
+}
+
+void d2h(ChannelState *S, const double *dev, double *host, long n) {
+  CH_CUDA(cudaMemcpyAsync(host, dev, n * sizeof(double), cudaMemcpyDeviceToHost, S->stream));
   CH_CUDA(cudaStreamSynchronize(S->stream));
 }
-void unpad_cells(ChannelState *S, const double *dev, double *host) {
-  const size_t np = (size_t)(S->N0 + 2) * (S->N1 + 2) * (S->N2 + 2);
-  std::vector<double> tmp(np);
-  CH_CUDA(cudaMemcpyAsync(tmp.data(), dev, np * 8, cudaMemcpyDeviceToHost, S->stream));
+void h2d(ChannelState *S, double *dev, const double *host, long n) {
+  CH_CUDA(cudaMemcpyAsync(dev, host, n * sizeof(double), cudaMemcpyHostToDevice, S->stream));
   CH_CUDA(cudaStreamSynchronize(S->stream));
-  for (int k = 0; k < S->N2; ++k)
-    for (int j = 0; j < S->N1; ++j)
-      for (int i = 0; i < S->N0; ++i)
-        host[i + (size_t)S->N0 * (j + (size_t)S->N1 * k)] = tmp[(i + 1) + (S->N0 + 2) * ((j + 1) + (size_t)(S->N1 + 2) * (k + 1))];
 }
 }  // namespace
 
+// Field copies between steps: V.s (a padded FP64 vector that only the
+// pressure solve uses) serves as device scratch.
 void ch_get_field(ChannelState *S, int f, double *host, long n) {
   CH_CUDA(cudaSetDevice(S->device));
   if (ch_field_size(S, f) != n) throw std::invalid_argument("field size mismatch");
-  if (f == 4) { unpad_cells(S, cht_T_device(S->cht), host); return; }
-  if (f == 11) { unpad_cells(S, S->V.x, host); return; }
-  if (f < 3) { get_dev(S, (const double *)uarr(S, f), host, n); return; }
-  if (f == 3) { get_dev(S, (const double *)(S->mixed ? S->Hf.p : S->Hd.p), host, n); return; }
-  const int a = (f - 5) % 3;
-  if (f >= 8) {
-    if (S->mixed) get_dev(S, (const float *)(a == 0 ? S->Hf.D0 : a == 1 ? S->Hf.D1 : S->Hf.D2), host, n);
-    else get_dev(S, (const double *)(a == 0 ? S->Hd.D0 : a == 1 ? S->Hd.D1 : S->Hd.D2), host, n);
+  double *scr = S->V.s;
+  const int g = blocks_for(n);
+  if (f == 4 || f == 11) {
+    k_unpad<<<g, kT, 0, S->stream>>>(f == 4 ? cht_T_device(S->cht) : S->V.x, scr, S->N0, S->N1, S->N2);
+    CH_CUDA(cudaGetLastError());
+    d2h(S, scr, host, n);
     return;
   }
-  if (!S->mixed) { get_dev(S, (const double *)(a == 0 ? S->Hd.S0 : a == 1 ? S->Hd.S1 : S->Hd.S2), host, n); return; }
-  // mixed: u* = u^n + delta
-  std::vector<double> d(n);
-  get_dev(S, (const float *)(a == 0 ? S->Hf.S0 : a == 1 ? S->Hf.S1 : S->Hf.S2), d.data(), n);
-  get_dev(S, (const double *)uarr(S, a), host, n);
-  for (long i = 0; i < n; ++i) host[i] += d[i];
+  if (f < 3) { d2h(S, uarr(S, f), host, n); return; }
+  if (f == 3) { d2h(S, S->mixed ? S->Hf.p : S->Hd.p, host, n); return; }
+  const int a = (f - 5) % 3;
+  if (!S->mixed) {
+    const double *src = f >= 8 ? (a == 0 ? S->Hd.D0 : a == 1 ? S->Hd.D1 : S->Hd.D2)
+                               : (a == 0 ? S->Hd.S0 : a == 1 ? S->Hd.S1 : S->Hd.S2);
+    d2h(S, src, host, n);
+    return;
+  }
+  const float *src = f >= 8 ? (a == 0 ? S->Hf.D0 : a == 1 ? S->Hf.D1 : S->Hf.D2)
+                            : (a == 0 ? S->Hf.S0 : a == 1 ? S->Hf.S1 : S->Hf.S2);
+  k_widen<float><<<g, kT, 0, S->stream>>>(src, f >= 8 ? nullptr : uarr(S, a), scr, n);  // u* = u^n + delta
+  CH_CUDA(cudaGetLastError());
+  d2h(S, scr, host, n);
 }
 
 void ch_set_field(ChannelState *S, int f, const double *host, long n) {
   CH_CUDA(cudaSetDevice(S->device));
   if (ch_field_size(S, f) != n || f > 4) throw std::invalid_argument("field size mismatch or read-only field");
+  const int g = blocks_for(n);
   if (f == 4) {
-    const size_t np = (size_t)(S->N0 + 2) * (S->N1 + 2) * (S->N2 + 2);
-    std::vector<double> tmp(np, 0.0);
-    for (int k = 0; k < S->N2; ++k)
-      for (int j = 0; j < S->N1; ++j)
-        for (int i = 0; i < S->N0; ++i)
-          tmp[(i + 1) + (S->N0 + 2) * ((j + 1) + (size_t)(S->N1 + 2) * (k + 1))] = host[i + (size_t)S->N0 * (j + (size_t)S->N1 * k)];
-    CH_CUDA(cudaMemcpyAsync(cht_T_device(S->cht), tmp.data(), np * 8, cudaMemcpyHostToDevice, S->stream));
-    CH_CUDA(cudaStreamSynchronize(S->stream));
+    h2d(S, S->V.s, host, n);
+    k_pad<<<g, kT, 0, S->stream>>>(S->V.s, cht_T_device(S->cht), S->N0, S->N1, S->N2);
+    CH_CUDA(cudaGetLastError());
     return;
   }
-  if (f == 3) { put_dev(S, S->mixed ? S->Hf.p : S->Hd.p, host, n); return; }
-  put_dev(S, uarr(S, f), host, n);
-  if (S->mixed) put_dev(S, f == 0 ? S->Hf.C0 : f == 1 ? S->Hf.C1 : S->Hf.C2, host, n);
+  if (f == 3) { h2d(S, S->mixed ? S->Hf.p : S->Hd.p, host, n); return; }
+  h2d(S, uarr(S, f), host, n);
+  if (S->mixed) {
+    k_narrow<<<g, kT, 0, S->stream>>>(uarr(S, f), f == 0 ? S->Hf.C0 : f == 1 ? S->Hf.C1 : S->Hf.C2, n);
+    CH_CUDA(cudaGetLastError());
+  }
 }
 
 void ch_profile(ChannelState *S, bool on) {

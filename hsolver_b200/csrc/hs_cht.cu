@@ -43,6 +43,8 @@ namespace hs {
 namespace {
 
 constexpr int kB = 256;
+// the cooperative BiCGStab: one 768-thread block per SM (fewer arrivals at each grid barrier)
+constexpr int kBiT = 768;
 
 struct ChtDev {
   int Nx, Ny, Nz;
@@ -209,7 +211,7 @@ __device__ __forceinline__ int cell_pidx(const ChtDev &H, int c) {
 // is summed with <r, r>.
 // rel0: stop on ||r|| / ||r0|| instead of ||r|| / ||rhs||; out_r0 = ||r0||.
 template <class MT>
-__global__ void __launch_bounds__(kB, 3) k_cht_bicgstab(ChtDev H, Vec V, mg::Hier<MT> Gm, const double *rhs,
+__global__ void __launch_bounds__(kBiT, 1) k_cht_bicgstab(ChtDev H, Vec V, mg::Hier<MT> Gm, const double *rhs,
                                                         int transpose, double tol, int maxiter, double *partials,
                                                         int *out_it, double *out_rel, int rel0, double *out_r0) {
   cg::grid_group grid = cg::this_grid();
@@ -419,7 +421,7 @@ __global__ void k_cht_fill(int n, int Nx, int Ny, double v, double *T) {
 int coop_grid(const void *kernel, int device) {
   int nsm = 0, per = 0;
   HC_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
-  HC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, kB, 0));
+  HC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, kBiT, 0));
   if (per < 1) throw std::runtime_error("cooperative kernel cannot be resident");
   return per * nsm;
 }
@@ -595,7 +597,7 @@ namespace {
 template <class K, class... A>
 void launch_coop(K kernel, int blocks, cudaStream_t s, A... args) {
   void *argv[] = {(void *)&args...};
-  HC_CUDA(cudaLaunchCooperativeKernel((void *)kernel, dim3(blocks), dim3(kB), argv, 0, s));
+  HC_CUDA(cudaLaunchCooperativeKernel((void *)kernel, dim3(blocks), dim3(kBiT), argv, 0, s));
 }
 
 void solve(ChtState *C, const double *rhs, int transpose, double tol, int maxiter, int rel0, double *out_r0) {

@@ -30,7 +30,7 @@ namespace cg = cooperative_groups;
 
 constexpr int kMgMaxLv = 16;
 constexpr int kMgCoarse = 64;
-constexpr long long kMgSmall = 512;
+constexpr long long kMgSmall = 2048;
 
 template <class M>
 struct Level {
