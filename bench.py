@@ -156,9 +156,11 @@ def profiled_steps(g, steps):
 
 
 def max_over_ranks(torch, dist, v):
+    """The largest value over the ranks (NCCL on the GPU, gloo on the host)."""
     if not dist:
         return v
-    t = torch.tensor([v], device="cuda", dtype=torch.float64)
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([v], device=dev, dtype=torch.float64)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
@@ -264,6 +266,7 @@ def run_gpu(args):
         variants["adjoint"] = adj
         variants["time_to_residual"] = time_to_residual(args, hsolver_b200, local)
         variants["reference_physics"] = reference_physics(args, torch, hsolver_b200, local, dist)
+        variants["config5"] = config5(torch, hsolver_b200, local)
 
     if rank == 0:
         peak, peak_kind = hbm_peak()
@@ -323,6 +326,24 @@ def time_to_residual(args, hsolver_b200, local):
             f: float(np.linalg.norm(fields["mixed"][f] - fields["fp64"][f]) / max(np.linalg.norm(fields["fp64"][f]), 1e-300))
             for f in ("u", "v", "w", "p", "T")}
         out[name] = res
+    return out
+
+
+def config5(torch, hsolver_b200, local):
+    """The large single-GPU case: 512x256x256 (33.5M cells), 32 seeded blocks
+    (edges 8-48, q U[0.1,5], k_s/k_f U[10,1000]), Re 1000; device footprint
+    and step time of both forms (3 timed steps after 2 warm-up steps)."""
+    deck, re_, k, q, _ = workload("config5")
+    out = {"workload": "channel 512x256x256 (33.5M cells), 32 seeded blocks, Re 1000"}
+    for prec, key in ((0, "fp64"), (1, "mixed")):
+        g = hsolver_b200.Channel(deck, device=local, re=re_, precision=prec, **SOLVER)
+        g.set_solid(k, q)
+        g.init()
+        g.step(2)
+        ms, st = time_steps(torch, g, 3, local)
+        out[key] = {"device_bytes": g.device_bytes(), "ms_per_step": ms / 3, "pcg_iters": st["pcg_iters"],
+                    "t_iters": st["t_iters"]}
+        g.close()
     return out
 
 

@@ -215,13 +215,16 @@ __device__ void prolong(const Level<M> &F, const Level<M> &C, int tid, int T) {
   }
 }
 
-// LU with partial pivoting of the coarsest operator (A or A^T), by block 0
+// LU with partial pivoting of the coarsest operator (A or A^T), by block 0,
+// in shared memory; the pivot is the largest |a| in the column, the lowest
+// row among equals; the factors are copied to G.lu for coarse_solve
 template <class M>
 __device__ void factor(const Hier<M> &G, bool tr) {
   if (blockIdx.x != 0) return;
+  __shared__ double a[kMgCoarse * kMgCoarse];
+  __shared__ int spiv;
   const Level<M> &C = G.lv[G.L - 1];
   const int nc = C.nx * C.ny * C.nz, PX = C.nx + 2, PXY = (C.nx + 2) * (C.ny + 2);
-  double *a = G.lu;
   for (int e = threadIdx.x; e < nc * nc; e += blockDim.x) {
     const int r = e / nc, c2 = e % nc;
     const int q = idx(C, r % C.nx + 1, (r / C.nx) % C.ny + 1, r / (C.nx * C.ny) + 1);
@@ -246,15 +249,20 @@ __device__ void factor(const Hier<M> &G, bool tr) {
     a[e] = v;
   }
   __syncthreads();
-  __shared__ int spiv;
   for (int col = 0; col < nc; ++col) {
-    if (threadIdx.x == 0) {
-      int best = col;
-      double bv = fabs(a[col * nc + col]);
-      for (int r = col + 1; r < nc; ++r)
-        if (fabs(a[r * nc + col]) > bv) { bv = fabs(a[r * nc + col]); best = r; }
-      spiv = best;
-      G.piv[col] = best;
+    if (threadIdx.x < 32) {
+      double bv = -1.0;
+      int br = nc;
+      for (int r = col + threadIdx.x; r < nc; r += 32) {
+        const double v = fabs(a[r * nc + col]);
+        if (v > bv || (v == bv && r < br)) { bv = v; br = r; }
+      }
+      for (int o = 16; o; o >>= 1) {
+        const double ov = __shfl_xor_sync(0xffffffffu, bv, o);
+        const int orow = __shfl_xor_sync(0xffffffffu, br, o);
+        if (ov > bv || (ov == bv && orow < br)) { bv = ov; br = orow; }
+      }
+      if (threadIdx.x == 0) { spiv = br; G.piv[col] = br; }
     }
     __syncthreads();
     const int pr = spiv;
@@ -275,6 +283,7 @@ __device__ void factor(const Hier<M> &G, bool tr) {
     }
     __syncthreads();
   }
+  for (int e = threadIdx.x; e < nc * nc; e += blockDim.x) G.lu[e] = a[e];
 }
 
 // exact solve on the coarsest level, by warp 0 of block 0 (the permuted
