@@ -53,6 +53,9 @@ CONFIG = {"workload": "channel 256x128x128 (4.19M cells), 8 seeded heated blocks
 # launches per outer step: 4 momentum passes, p' assembly, residual finalize,
 # p' solve, correction, energy assembly, energy BiCGStab, energy relaxation
 LAUNCHES_PER_STEP = 11
+# DRAM bytes per CG iteration of k_ch_pcg on this case, from one ncu capture
+# (profiles/k_ch_pcg_config2_dram.md: 26.67 GB per 17-iteration launch)
+PCG_TRAFFIC_PER_ITER = 26.67e9 / 17
 
 
 def workload(name=NAME, seed=0):
@@ -283,7 +286,10 @@ def run_gpu(args):
             "roofline": {"bound": "hbm", "kernel": "k_ch_pcg (pressure correction, multigrid-preconditioned CG, "
                                                  "one cooperative launch per outer step)",
                          "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
-                         "traffic": None, "peak_source": peak_kind, "algorithmic_bytes_per_launch": b,
+                         "traffic": PCG_TRAFFIC_PER_ITER * it_mean,
+                         "traffic_source": "ncu dram bytes of 3 launches (17 iterations each), per iteration x "
+                                           "this launch's iterations", "peak_source": peak_kind,
+                         "algorithmic_bytes_per_launch": b,
                          "pcg_iters_per_launch": it_mean, "launch_ms": pms},
             "phase_ms_per_step": phases,
             "last_step": {"pcg_iters": st["pcg_iters"], "t_iters": st["t_iters"], "global_residual": st["global"]},
