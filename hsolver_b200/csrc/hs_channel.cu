@@ -462,7 +462,7 @@ struct CgVec {
   int N0, N1, N2;
   const double *acx, *acy, *acz;
   const uint8_t *solid;
-  double *x, *r, *p, *s;
+  double *x, *r, *p, *p2, *s;  // p, p2: search direction, double-buffered
 };
 
 __device__ double grid_sum(double v, double *partials, int &buf, double *sh, cg::grid_group &grid) {
@@ -490,6 +490,16 @@ __device__ __forceinline__ int cell_q(int e, int N0, int N1) {
   return (i + 1) + (N0 + 2) * ((j + 1) + (N1 + 2) * (k + 1));
 }
 
+// V-cycle right-hand side of cell e and its seed (the first red half-sweep)
+template <class M>
+__device__ __forceinline__ void mg_rhs(const mg::Level<M> &L0, int e, int q, int N0, int N1, double v) {
+  const int row_ = e / N0, i = e - row_ * N0;
+  const int k = row_ / N1, j = row_ - k * N1;
+  const M m = (M)v;
+  L0.rhs[q] = m;
+  mg::seed(L0, q, i, j, k, m, false);
+}
+
 // one 768-thread block per SM: the same warps per SM as three 256-thread
 // blocks, a third of the arrivals at every grid barrier
 constexpr int kPcgT = 768;
@@ -506,15 +516,11 @@ __device__ void mg_fine_from_couplings(const CgVec &V, const mg::Level<M> &L0, i
   }
 }
 
-__device__ __forceinline__ double cg_apply(const CgVec &V, const double *x, int q, int PX, int PXY) {
-  const double cw = V.acx[q], ce = V.acx[q + 1], cs = V.acy[q], cn = V.acy[q + PX], cb = V.acz[q], cf = V.acz[q + PXY];
-  const double d = cw + ce + cs + cn + cb + cf;
-  return d * __ldcg(x + q) - (cw * __ldcg(x + q - 1) + ce * __ldcg(x + q + 1) + cs * __ldcg(x + q - PX) +
-                              cn * __ldcg(x + q + PX) + cb * __ldcg(x + q - PXY) + cf * __ldcg(x + q + PXY));
-}
-
 // PCG: r = b (assembled), x = 0; z = M r (V-cycle, or z = r when precond = 0);
-// s = A p, alpha = <r,z>/<s,p>, x += alpha p, r -= alpha s, stop on ||r||/||b|| < tol
+// s = A p, alpha = <r,z>/<s,p>, x += alpha p, r -= alpha s, stop on ||r||/||b|| < tol.
+// The update p = z + beta p is done inside the product A p (each thread
+// forms the new p of its cell and of the six neighbours from z and the old
+// p; p is double-buffered), and <r, z> inside the V-cycle's last pass.
 template <class M>
 __global__ void __launch_bounds__(kPcgT, 1) k_ch_pcg(CgVec V, mg::Hier<M> G, int precond, double tol, int maxiter, double *partials,
                                                int *out_it, double *out_rel) {
@@ -535,7 +541,7 @@ __global__ void __launch_bounds__(kPcgT, 1) k_ch_pcg(CgVec V, mg::Hier<M> G, int
     const int q = cell_q(e, N0, N1);
     const double rv = V.r[q];
     acc += rv * rv;
-    if (precond) L0.rhs[q] = (M)rv;
+    if (precond) mg_rhs(L0, e, q, N0, N1, rv);
   }
   const double bb = grid_sum(acc, partials, buf, sh, grid);
   if (bb == 0.0) {
@@ -543,24 +549,38 @@ __global__ void __launch_bounds__(kPcgT, 1) k_ch_pcg(CgVec V, mg::Hier<M> G, int
     return;
   }
   const double eps = tol * tol;
-  if (precond) mg::vcycle(G, false, grid, tid, T);
-  acc = 0.0;
-  for (int e = tid; e < n; e += T) {
-    const int q = cell_q(e, N0, N1);
-    const double z = precond ? (double)__ldcg(L0.x + q) : V.r[q];
-    V.p[q] = z;
-    acc += V.r[q] * z;
-  }
-  double gamma = grid_sum(acc, partials, buf, sh, grid), rr = bb;
+  // gamma = <r, z>
+  auto rz = [&]() {
+    double a = 0.0;
+    if (!precond) return bb;
+    if (!mg::vcycle(G, false, grid, tid, T, V.r, &a))
+      for (int e = tid; e < n; e += T) {
+        const int q = cell_q(e, N0, N1);
+        a += V.r[q] * (double)__ldcg(L0.x + q);
+      }
+    return grid_sum(a, partials, buf, sh, grid);
+  };
+  double gamma = rz(), rr = bb, beta = 0.0;
+  double *po = V.p, *pn = V.p2;
   int it = 0;
   while (it < maxiter && !(rr / bb < eps)) {
+    const bool first = it == 0;
     it++;
     acc = 0.0;
+    auto pval = [&](int qq) {
+      const double z = precond ? (double)__ldcg(L0.x + qq) : __ldcg(V.r + qq);
+      return first ? z : z + beta * __ldcg(po + qq);
+    };
     for (int e = tid; e < n; e += T) {
       const int q = cell_q(e, N0, N1);
-      const double sv = cg_apply(V, V.p, q, PX, PXY);
+      const double p0 = pval(q);
+      const double cw = V.acx[q], ce = V.acx[q + 1], cs = V.acy[q], cn = V.acy[q + PX], cb = V.acz[q], cf = V.acz[q + PXY];
+      const double d = cw + ce + cs + cn + cb + cf;
+      const double sv = d * p0 - (cw * pval(q - 1) + ce * pval(q + 1) + cs * pval(q - PX) + cn * pval(q + PX) +
+                                  cb * pval(q - PXY) + cf * pval(q + PXY));
+      pn[q] = p0;
       V.s[q] = sv;
-      acc += sv * __ldcg(V.p + q);
+      acc += sv * p0;
     }
     const double sp = grid_sum(acc, partials, buf, sh, grid);
     if (sp == 0.0) break;
@@ -568,28 +588,18 @@ __global__ void __launch_bounds__(kPcgT, 1) k_ch_pcg(CgVec V, mg::Hier<M> G, int
     acc = 0.0;
     for (int e = tid; e < n; e += T) {
       const int q = cell_q(e, N0, N1);
-      V.x[q] = V.x[q] + alpha * V.p[q];
+      V.x[q] = V.x[q] + alpha * pn[q];
       const double rv = V.r[q] - alpha * V.s[q];
       V.r[q] = rv;
       acc += rv * rv;
-      if (precond) L0.rhs[q] = (M)rv;
+      if (precond) mg_rhs(L0, e, q, N0, N1, rv);
     }
     rr = grid_sum(acc, partials, buf, sh, grid);
     if (rr / bb < eps) break;
-    if (precond) mg::vcycle(G, false, grid, tid, T);
-    acc = 0.0;
-    for (int e = tid; e < n; e += T) {
-      const int q = cell_q(e, N0, N1);
-      acc += V.r[q] * (precond ? (double)__ldcg(L0.x + q) : V.r[q]);
-    }
-    const double gnew = grid_sum(acc, partials, buf, sh, grid);
-    const double beta = gnew / gamma;
+    const double gnew = precond ? rz() : rr;
+    beta = gnew / gamma;
     gamma = gnew;
-    for (int e = tid; e < n; e += T) {
-      const int q = cell_q(e, N0, N1);
-      V.p[q] = (precond ? (double)__ldcg(L0.x + q) : V.r[q]) + beta * V.p[q];
-    }
-    grid.sync();
+    double *t = po; po = pn; pn = t;
   }
   if (tid == 0) { *out_it = it; *out_rel = sqrt(rr / bb); }
 }
@@ -853,6 +863,7 @@ ChannelState *ch_create(const Case &c, const ChParams &p, int device) {
   S->V.N0 = S->N0; S->V.N1 = S->N1; S->V.N2 = S->N2; S->V.solid = solid;
   S->V.acx = S->alloc<double>(np); S->V.acy = S->alloc<double>(np); S->V.acz = S->alloc<double>(np);
   S->V.x = S->alloc<double>(np); S->V.r = S->alloc<double>(np); S->V.p = S->alloc<double>(np); S->V.s = S->alloc<double>(np);
+  S->V.p2 = S->alloc<double>(np);
   if (S->mixed) setup_mg(*S, S->Gf);
   else setup_mg(*S, S->Gd);
   S->mom_blocks = blocks_for((long long)(S->N0 + 1) * (S->N1 + 1) * (S->N2 + 1));

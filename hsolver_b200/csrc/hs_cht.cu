@@ -203,6 +203,16 @@ __device__ __forceinline__ int cell_pidx(const ChtDev &H, int c) {
   return (i + 1) + (H.Nx + 2) * ((j + 1) + (H.Ny + 2) * (k + 1));
 }
 
+// V-cycle right-hand side of cell c and its seed (the first red half-sweep)
+template <class MT>
+__device__ __forceinline__ void mg_rhs(const ChtDev &H, const mg::Level<MT> &L0, int c, int q, double v, bool tr) {
+  const int row_ = c / H.Nx, i = c - row_ * H.Nx;
+  const int k = row_ / H.Ny, j = row_ - k * H.Ny;
+  const MT m = (MT)v;
+  L0.rhs[q] = m;
+  mg::seed(L0, q, i, j, k, m, tr);
+}
+
 // Right-preconditioned BiCGStab (van der Vorst, SIAM J. Sci. Stat. Comput.
 // 13(2), 1992) for A x = rhs or A^T x = rhs; x holds the start.  The
 // preconditioner is the V-cycle of hs_mg.cuh on the same operator (Gm.L > 0)
@@ -221,7 +231,6 @@ __global__ void __launch_bounds__(kBiT, 1) k_cht_bicgstab(ChtDev H, Vec V, mg::H
   const int tid = blockIdx.x * blockDim.x + threadIdx.x, T = gridDim.x * blockDim.x;
   const bool tr = transpose != 0, mgp = Gm.L > 0;
   const MT *z = mgp ? Gm.lv[0].x : nullptr;
-  MT *zr = mgp ? Gm.lv[0].rhs : nullptr;
   int buf = 0;
   if (mgp) {
     cht_mg_fine(H, Gm.lv[0], tid, T);
@@ -250,7 +259,7 @@ __global__ void __launch_bounds__(kBiT, 1) k_cht_bicgstab(ChtDev H, Vec V, mg::H
       const int q = cell_pidx(H, c);
       const double pv = V.r[q] + beta * (V.p[q] - omega * V.v[q]);
       V.p[q] = pv;
-      if (mgp) zr[q] = (MT)pv;
+      if (mgp) mg_rhs(H, Gm.lv[0], c, q, pv, tr);
       else V.ph[q] = pv * H.dinv[q];
     }
     grid.sync();
@@ -271,7 +280,7 @@ __global__ void __launch_bounds__(kBiT, 1) k_cht_bicgstab(ChtDev H, Vec V, mg::H
       const int q = cell_pidx(H, c);
       const double sv = V.r[q] - alpha * V.v[q];
       V.s[q] = sv;
-      if (mgp) zr[q] = (MT)sv;
+      if (mgp) mg_rhs(H, Gm.lv[0], c, q, sv, tr);
       else V.sh[q] = sv * H.dinv[q];
       s3[0] += sv * sv;
     }

@@ -17,8 +17,10 @@
 // 4x, the spacing 2x), coarse flux = sum of the fine fluxes (conservative);
 // down to <= kMgCoarse cells, where an LU with partial pivoting (FP64, on the
 // GPU) solves exactly.  Smoother: red-black Gauss-Seidel, one sweep before
-// (red, black) and one after (black, red).  Levels below kMgSmall cells run
-// inside block 0 alone, separated by __syncthreads instead of grid barriers.
+// (red, black) and one after (black, red); the first red half-sweep (from
+// x = 0) is applied by whoever writes the level's rhs, the prolongation is
+// fused into the first post-smoothing half-sweep.  Levels below kMgSmall cells run inside
+// block 0 alone, separated by __syncthreads instead of grid barriers.
 #pragma once
 #include <cooperative_groups.h>
 #include <cstdint>
@@ -162,7 +164,7 @@ __device__ void coarsen(const Level<M> &F, const Level<M> &C, int tid, int T) {
 // a masked cell has zero couplings on every face (its faces touch a
 // non-unknown), so d == 0 identifies it without reading the mask
 template <class M>
-__device__ void smooth(const Level<M> &L, int color, bool zero_nb, bool tr, int tid, int T) {
+__device__ void smooth(const Level<M> &L, int color, bool tr, int tid, int T) {
   const int half = (L.nx + 1) / 2;
   const int n = half * L.ny * L.nz;
   for (int e = tid; e < n; e += T) {
@@ -175,12 +177,59 @@ __device__ void smooth(const Level<M> &L, int color, bool zero_nb, bool tr, int 
     row(L, q, tr, d, o);
     if (d == M(0)) { L.x[q] = M(0); continue; }
     M s = L.rhs[q];
-    if (!zero_nb) s += offsum(L, o, L.x, q);
+    s += offsum(L, o, L.x, q);
     L.x[q] = s / d;
   }
 }
 
-// coarse rhs = sum over the children of (rhs - A x)
+// The last colour-0 half-sweep of level 0, also accumulating sum r x over
+// every cell (colour 0 as it is computed, colour 1 as left by the previous
+// half-sweep): the V-cycle's output dotted with the caller's residual r
+// (padded FP64) without a pass of its own.
+template <class M>
+__device__ void smooth_dot(const Level<M> &L, bool tr, const double *r, double &acc, int tid, int T) {
+  const int half = (L.nx + 1) / 2;
+  const int n = half * L.ny * L.nz;
+  for (int e = tid; e < n; e += T) {
+    const int row_ = e / half, m = e - row_ * half;
+    const int k = row_ / L.ny, j = row_ - k * L.ny;
+    const int i = 2 * m + ((j + k) & 1), ib = 2 * m + ((j + k + 1) & 1);
+    if (i < L.nx) {
+      const int q = idx(L, i + 1, j + 1, k + 1);
+      M d, o[6];
+      row(L, q, tr, d, o);
+      M xv = M(0);
+      if (d != M(0)) {
+        M s = L.rhs[q];
+        s += offsum(L, o, L.x, q);
+        xv = s / d;
+      }
+      L.x[q] = xv;
+      acc += r[q] * (double)xv;
+    }
+    if (ib < L.nx) {
+      const int q = idx(L, ib + 1, j + 1, k + 1);
+      acc += r[q] * (double)__ldcg(L.x + q);
+    }
+  }
+}
+
+// The first pre-smoothing half-sweep starts from x = 0, so on the colour-0
+// cells it is local, x = rhs / d: whoever writes a level's rhs applies it to
+// the cell in the same pass (the restriction for the coarse levels, the
+// Krylov solver for level 0), which saves that half-sweep and its barrier.
+template <class M>
+__device__ __forceinline__ void seed(const Level<M> &L, int q, int i, int j, int k, M rhs, bool tr) {
+  if ((i + j + k) & 1) return;
+  M d, o[6];
+  row(L, q, tr, d, o);
+  L.x[q] = d == M(0) ? M(0) : rhs / d;
+}
+
+// coarse rhs = sum over the children of (rhs - A x), and the coarse seed.  It follows the
+// colour-1 half-sweep, after which a colour-1 cell's residual is zero up to
+// rounding (its update solved its own row), so only the colour-0 children
+// are evaluated.
 template <class M>
 __device__ void restrict_res(const Level<M> &F, const Level<M> &C, bool tr, int tid, int T) {
   const int n = C.nx * C.ny * C.nz;
@@ -192,26 +241,49 @@ __device__ void restrict_res(const Level<M> &F, const Level<M> &C, bool tr, int 
       for (int dj = 0; dj < 2; ++dj)
         for (int di = 0; di < 2; ++di) {
           const int i = 2 * I + di, j = 2 * J + dj, k = 2 * K + dk;
-          if (i >= F.nx || j >= F.ny || k >= F.nz) continue;
+          if (i >= F.nx || j >= F.ny || k >= F.nz || ((i + j + k) & 1)) continue;
           const int q = idx(F, i + 1, j + 1, k + 1);
           M d, o[6];
           row(F, q, tr, d, o);
           acc += F.rhs[q] - (d * __ldcg(F.x + q) - offsum(F, o, F.x, q));
         }
     const int qc = idx(C, I + 1, J + 1, K + 1);
-    C.rhs[qc] = unknown(C, qc) ? acc : M(0);
+    const M v = unknown(C, qc) ? acc : M(0);
+    C.rhs[qc] = v;
+    seed(C, qc, I, J, K, v, tr);
   }
 }
 
+// Prolongation fused into the first post-smoothing half-sweep (colour 1):
+// every neighbour (colour 0) is read as x + x_coarse(parent).  A Gauss-Seidel
+// update never reads its own cell, so the colour-0 cells' prolonged values
+// are needed only as these neighbour values (the colour-0 half-sweep that
+// follows recomputes them) and the colour-1 cells' not at all.  Ghost
+// neighbours are 0, as they are never prolonged; a masked neighbour has a
+// zero coupling.  The arithmetic is that of prolongation followed by smooth().
 template <class M>
-__device__ void prolong(const Level<M> &F, const Level<M> &C, int tid, int T) {
-  const int n = F.nx * F.ny * F.nz;
+__device__ void prolong_smooth(const Level<M> &F, const Level<M> &C, bool tr, int tid, int T) {
+  const int half = (F.nx + 1) / 2;
+  const int n = half * F.ny * F.nz;
+  const int PX = F.nx + 2, PXY = (F.nx + 2) * (F.ny + 2);
   for (int e = tid; e < n; e += T) {
-    const int row_ = e / F.nx, i = e - row_ * F.nx;
+    const int row_ = e / half, m = e - row_ * half;
     const int k = row_ / F.ny, j = row_ - k * F.ny;
+    const int i = 2 * m + ((j + k + 1) & 1);
+    if (i >= F.nx) continue;
     const int q = idx(F, i + 1, j + 1, k + 1);
-    if (!unknown(F, q)) continue;
-    F.x[q] = __ldcg(F.x + q) + __ldcg(C.x + idx(C, i / 2 + 1, j / 2 + 1, k / 2 + 1));
+    M d, o[6];
+    row(F, q, tr, d, o);
+    if (d == M(0)) { F.x[q] = M(0); continue; }
+    auto xp = [&](int ii, int jj, int kk, int qq) -> M {
+      if (ii < 0 || jj < 0 || kk < 0 || ii >= F.nx || jj >= F.ny || kk >= F.nz) return M(0);
+      return __ldcg(F.x + qq) + __ldcg(C.x + idx(C, ii / 2 + 1, jj / 2 + 1, kk / 2 + 1));
+    };
+    const M off = o[0] * xp(i - 1, j, k, q - 1) + o[1] * xp(i + 1, j, k, q + 1) + o[2] * xp(i, j - 1, k, q - PX) +
+                  o[3] * xp(i, j + 1, k, q + PX) + o[4] * xp(i, j, k - 1, q - PXY) + o[5] * xp(i, j, k + 1, q + PXY);
+    M s = F.rhs[q];
+    s += off;
+    F.x[q] = s / d;
   }
 }
 
@@ -342,15 +414,19 @@ __device__ void build(const Hier<M> &G, bool tr, cg::grid_group &grid, int tid, 
   grid.sync();
 }
 
-// lv[0].x = V-cycle applied to lv[0].rhs
+// lv[0].x = V-cycle applied to lv[0].rhs; the caller has written lv[0].rhs
+// and seeded lv[0] (seed() on every interior cell) before the barrier that
+// precedes this call.  With dot_r, the last level-0 pass also adds this
+// thread's share of sum dot_r x to *dot_acc and the final barrier is left to
+// the caller's reduction (returns true); it returns false, with the barrier
+// done and nothing added, when level 0 is handled by block 0 alone.
 template <class M>
-__device__ void vcycle(const Hier<M> &G, bool tr, cg::grid_group &grid, int tid, int T) {
+__device__ bool vcycle(const Hier<M> &G, bool tr, cg::grid_group &grid, int tid, int T,
+                       const double *dot_r = nullptr, double *dot_acc = nullptr) {
   int ls = 0;  // first level handled by block 0 alone
   while (ls < G.L - 1 && !small(G.lv[ls])) ++ls;
   for (int l = 0; l < ls; ++l) {
-    smooth(G.lv[l], 0, true, tr, tid, T);
-    grid.sync();
-    smooth(G.lv[l], 1, false, tr, tid, T);
+    smooth(G.lv[l], 1, tr, tid, T);
     grid.sync();
     restrict_res(G.lv[l], G.lv[l + 1], tr, tid, T);
     grid.sync();
@@ -358,9 +434,7 @@ __device__ void vcycle(const Hier<M> &G, bool tr, cg::grid_group &grid, int tid,
   if (blockIdx.x == 0) {
     const int t = threadIdx.x, B = blockDim.x;
     for (int l = ls; l < G.L - 1; ++l) {
-      smooth(G.lv[l], 0, true, tr, t, B);
-      __syncthreads();
-      smooth(G.lv[l], 1, false, tr, t, B);
+      smooth(G.lv[l], 1, tr, t, B);
       __syncthreads();
       restrict_res(G.lv[l], G.lv[l + 1], tr, t, B);
       __syncthreads();
@@ -368,23 +442,24 @@ __device__ void vcycle(const Hier<M> &G, bool tr, cg::grid_group &grid, int tid,
     coarse_solve(G);
     __syncthreads();
     for (int l = G.L - 2; l >= ls; --l) {
-      prolong(G.lv[l], G.lv[l + 1], t, B);
+      prolong_smooth(G.lv[l], G.lv[l + 1], tr, t, B);
       __syncthreads();
-      smooth(G.lv[l], 1, false, tr, t, B);
-      __syncthreads();
-      smooth(G.lv[l], 0, false, tr, t, B);
+      smooth(G.lv[l], 0, tr, t, B);
       __syncthreads();
     }
   }
   grid.sync();
   for (int l = ls - 1; l >= 0; --l) {
-    prolong(G.lv[l], G.lv[l + 1], tid, T);
+    prolong_smooth(G.lv[l], G.lv[l + 1], tr, tid, T);
     grid.sync();
-    smooth(G.lv[l], 1, false, tr, tid, T);
-    grid.sync();
-    smooth(G.lv[l], 0, false, tr, tid, T);
+    if (l == 0 && dot_r) {
+      smooth_dot(G.lv[0], tr, dot_r, *dot_acc, tid, T);
+      return true;
+    }
+    smooth(G.lv[l], 0, tr, tid, T);
     grid.sync();
   }
+  return false;
 }
 
 }  // namespace mg
