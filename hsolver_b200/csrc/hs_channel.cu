@@ -78,6 +78,8 @@ struct ChDev {
   double *p;                  // pressure, cells
   R nu, au, u_in;
   double ap;                  // alpha_p
+  const double *xd0, *xd1, *xd2, *xh0, *xh1, *xh2;  // FP64 geometry (the residual of the mixed form)
+  double nu_d, au_d, u_in_d;
 };
 
 __host__ __device__ constexpr bool is_mixed(float) { return true; }
@@ -225,16 +227,37 @@ __device__ __forceinline__ void mom_face(const ChDev<R> &H, const int (&c)[3], b
       if (last) Darr<A>(H)[f] = Ar / apr;
     }
   } else {
-    // delta: a_P/alpha delta_P - sum a_nb delta_nb = sum a_nb u^n_nb + b - a_P u^n_P (FP64, then FP32)
+    // delta: a_P/alpha delta_P - sum a_nb delta_nb = sum a_nb u^n_nb + b - a_P u^n_P.  The right-hand
+    // side is the FP64 form's residual (FP64 coefficients from the FP64 iterate), rounded once to FP32;
+    // the sweeps use FP32 coefficients from the FP32 copy, which only approximates the correction
+    // operator: the fixed point solves the FP64 equations (defect correction).
     R rhs;
     if (first) {
+      ChDev<double> H64;
+      H64.N0 = H.N0; H64.N1 = H.N1; H64.N2 = H.N2;
+      H64.d0 = H.xd0; H64.d1 = H.xd1; H64.d2 = H.xd2; H64.h0 = H.xh0; H64.h1 = H.xh1; H64.h2 = H.xh2;
+      H64.solid = H.solid;
+      H64.U0 = H.U0; H64.U1 = H.U1; H64.U2 = H.U2;
+      H64.C0 = H.U0; H64.C1 = H.U1; H64.C2 = H.U2;
+      H64.p = H.p; H64.nu = H.nu_d; H64.au = H.au_d; H64.u_in = H.u_in_d;
+      const double Ad = face_area<A>(H64, c);
+      const double dad = ctr<A>(H64, c[A]);
+      double ad[6];
+      int nd[6];
+      term<A, 0, 1>(H64, c, Ad, dad, ad[0], nd[0]);
+      term<A, 0, 0>(H64, c, Ad, dad, ad[1], nd[1]);
+      term<A, 1, 1>(H64, c, Ad, dad, ad[2], nd[2]);
+      term<A, 1, 0>(H64, c, Ad, dad, ad[3], nd[3]);
+      term<A, 2, 1>(H64, c, Ad, dad, ad[4], nd[4]);
+      term<A, 2, 0>(H64, c, Ad, dad, ad[5], nd[5]);
+      const double aPd = ad[0] + ad[1] + ad[2] + ad[3] + ad[4] + ad[5];
       int lo[3] = {c[0], c[1], c[2]};
       lo[A] -= 1;
-      const double bs = (H.p[cidx(H, lo[0], lo[1], lo[2])] - H.p[cidx(H, c[0], c[1], c[2])]) * (double)Ar;
+      const double bs = (H.p[cidx(H, lo[0], lo[1], lo[2])] - H.p[cidx(H, c[0], c[1], c[2])]) * Ad;
       double s = 0.0;
 #pragma unroll
-      for (int n = 0; n < 6; ++n) s += (double)an[n] * (nb[n] >= 0 ? UA[nb[n]] : 0.0);
-      const double r = (s + bs) - (double)aP * UA[f];
+      for (int n = 0; n < 6; ++n) s += ad[n] * (nd[n] >= 0 ? UA[nd[n]] : 0.0);
+      const double r = (s + bs) - aPd * UA[f];
       racc += r * r;
       rhs = (R)r;
       Qarr<A>(H)[f] = rhs;
@@ -712,6 +735,15 @@ void setup_fields(ChannelState &S, ChDev<R> &H, const std::vector<double> (&d)[3
   }
   H.p = S.alloc<double>((size_t)S.N0 * S.N1 * S.N2);
   H.nu = (R)S.nu; H.au = (R)S.prm.alpha_u; H.u_in = (R)S.prm.u_in; H.ap = S.prm.alpha_p;
+  H.nu_d = S.nu; H.au_d = S.prm.alpha_u; H.u_in_d = S.prm.u_in;
+  const double **xd[3] = {&H.xd0, &H.xd1, &H.xd2}, **xh[3] = {&H.xh0, &H.xh1, &H.xh2};
+  for (int a = 0; a < 3; ++a) {
+    if (!is_mixed(R())) { *xd[a] = (const double *)*dd[a]; *xh[a] = (const double *)*hh[a]; continue; }
+    double *pd = S.alloc<double>(d[a].size()), *ph = S.alloc<double>(h[a].size());
+    CH_CUDA(cudaMemcpyAsync(pd, d[a].data(), d[a].size() * sizeof(double), cudaMemcpyHostToDevice, S.stream));
+    CH_CUDA(cudaMemcpyAsync(ph, h[a].data(), h[a].size() * sizeof(double), cudaMemcpyHostToDevice, S.stream));
+    *xd[a] = pd; *xh[a] = ph;
+  }
 }
 
 template <class M>
