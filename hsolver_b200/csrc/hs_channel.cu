@@ -184,12 +184,64 @@ __device__ __forceinline__ void term(const ChDev<R> &H, const int (&c)[3], R Ar,
   }
 }
 
+// Mixed form, first pass: the FP64 form's residual of the relaxed equation
+// at u^n (FP64 coefficients from the FP64 iterate), stored rounded to FP32
+// as the right-hand side of the correction sweeps, and the first half-sweep
+// of the correction (neighbour corrections are still 0).  The sweeps that
+// follow use FP32 coefficients from the FP32 copy, which only approximates
+// the correction operator: the fixed point solves the FP64 equations (defect
+// correction).
+template <int A>
+__device__ __forceinline__ void mom_face_mixed_first(const ChDev<float> &H, const int (&c)[3], int f, bool upd,
+                                                     bool last, double &racc) {
+  ChDev<double> H64;
+  H64.N0 = H.N0; H64.N1 = H.N1; H64.N2 = H.N2;
+  H64.d0 = H.xd0; H64.d1 = H.xd1; H64.d2 = H.xd2; H64.h0 = H.xh0; H64.h1 = H.xh1; H64.h2 = H.xh2;
+  H64.solid = H.solid;
+  H64.U0 = H.U0; H64.U1 = H.U1; H64.U2 = H.U2;
+  H64.C0 = H.U0; H64.C1 = H.U1; H64.C2 = H.U2;
+  H64.p = H.p; H64.nu = H.nu_d; H64.au = H.au_d; H64.u_in = H.u_in_d;
+  const double Ad = face_area<A>(H64, c);
+  const double dad = ctr<A>(H64, c[A]);
+  double ad[6];
+  int nd[6];
+  term<A, 0, 1>(H64, c, Ad, dad, ad[0], nd[0]);
+  term<A, 0, 0>(H64, c, Ad, dad, ad[1], nd[1]);
+  term<A, 1, 1>(H64, c, Ad, dad, ad[2], nd[2]);
+  term<A, 1, 0>(H64, c, Ad, dad, ad[3], nd[3]);
+  term<A, 2, 1>(H64, c, Ad, dad, ad[4], nd[4]);
+  term<A, 2, 0>(H64, c, Ad, dad, ad[5], nd[5]);
+  const double aPd = ad[0] + ad[1] + ad[2] + ad[3] + ad[4] + ad[5];
+  const double *UA = Uarr<A>(H);
+  int lo[3] = {c[0], c[1], c[2]};
+  lo[A] -= 1;
+  const double bs = (H.p[cidx(H, lo[0], lo[1], lo[2])] - H.p[cidx(H, c[0], c[1], c[2])]) * Ad;
+  double s = 0.0;
+#pragma unroll
+  for (int n = 0; n < 6; ++n) s += ad[n] * (nd[n] >= 0 ? UA[nd[n]] : 0.0);
+  const double r = (s + bs) - aPd * UA[f];
+  racc += r * r;
+  const float rhs = (float)r;
+  Qarr<A>(H)[f] = rhs;
+  if (upd) {
+    const float apr = (float)(aPd / H.au_d);
+    Sarr<A>(H)[f] = rhs / apr;
+    if (last) Darr<A>(H)[f] = face_area<A>(H, c) / apr;
+  }
+}
+
 // momentum work on the unknown face (A, c): residual at u^n (first pass),
 // relaxed Gauss-Seidel update (upd), d (last sweep)
 template <int A, class R>
 __device__ __forceinline__ void mom_face(const ChDev<R> &H, const int (&c)[3], bool first, bool upd, bool last,
                                          double &racc) {
   const int f = fidx3<A>(H, c);
+  if constexpr (is_mixed(R())) {
+    if (first) {
+      mom_face_mixed_first<A>(H, c, f, upd, last, racc);
+      return;
+    }
+  }
   const R Ar = face_area<A>(H, c);
   const R da = ctr<A>(H, c[A]);
   R an[6];
@@ -227,49 +279,12 @@ __device__ __forceinline__ void mom_face(const ChDev<R> &H, const int (&c)[3], b
       if (last) Darr<A>(H)[f] = Ar / apr;
     }
   } else {
-    // delta: a_P/alpha delta_P - sum a_nb delta_nb = sum a_nb u^n_nb + b - a_P u^n_P.  The right-hand
-    // side is the FP64 form's residual (FP64 coefficients from the FP64 iterate), rounded once to FP32;
-    // the sweeps use FP32 coefficients from the FP32 copy, which only approximates the correction
-    // operator: the fixed point solves the FP64 equations (defect correction).
-    R rhs;
-    if (first) {
-      ChDev<double> H64;
-      H64.N0 = H.N0; H64.N1 = H.N1; H64.N2 = H.N2;
-      H64.d0 = H.xd0; H64.d1 = H.xd1; H64.d2 = H.xd2; H64.h0 = H.xh0; H64.h1 = H.xh1; H64.h2 = H.xh2;
-      H64.solid = H.solid;
-      H64.U0 = H.U0; H64.U1 = H.U1; H64.U2 = H.U2;
-      H64.C0 = H.U0; H64.C1 = H.U1; H64.C2 = H.U2;
-      H64.p = H.p; H64.nu = H.nu_d; H64.au = H.au_d; H64.u_in = H.u_in_d;
-      const double Ad = face_area<A>(H64, c);
-      const double dad = ctr<A>(H64, c[A]);
-      double ad[6];
-      int nd[6];
-      term<A, 0, 1>(H64, c, Ad, dad, ad[0], nd[0]);
-      term<A, 0, 0>(H64, c, Ad, dad, ad[1], nd[1]);
-      term<A, 1, 1>(H64, c, Ad, dad, ad[2], nd[2]);
-      term<A, 1, 0>(H64, c, Ad, dad, ad[3], nd[3]);
-      term<A, 2, 1>(H64, c, Ad, dad, ad[4], nd[4]);
-      term<A, 2, 0>(H64, c, Ad, dad, ad[5], nd[5]);
-      const double aPd = ad[0] + ad[1] + ad[2] + ad[3] + ad[4] + ad[5];
-      int lo[3] = {c[0], c[1], c[2]};
-      lo[A] -= 1;
-      const double bs = (H.p[cidx(H, lo[0], lo[1], lo[2])] - H.p[cidx(H, c[0], c[1], c[2])]) * Ad;
-      double s = 0.0;
-#pragma unroll
-      for (int n = 0; n < 6; ++n) s += ad[n] * (nd[n] >= 0 ? UA[nd[n]] : 0.0);
-      const double r = (s + bs) - aPd * UA[f];
-      racc += r * r;
-      rhs = (R)r;
-      Qarr<A>(H)[f] = rhs;
-    } else {
-      rhs = Qarr<A>(H)[f];
-    }
+    // correction sweeps after the first pass (FP32 operator, FP32 right-hand side from the first pass)
+    const R rhs = Qarr<A>(H)[f];
     if (upd) {
       R s = R(0);
-      if (!first) {
 #pragma unroll
-        for (int n = 0; n < 6; ++n) s += an[n] * (nb[n] >= 0 ? SA[nb[n]] : R(0));
-      }
+      for (int n = 0; n < 6; ++n) s += an[n] * (nb[n] >= 0 ? SA[nb[n]] : R(0));
       SA[f] = (rhs + s) / apr;
       if (last) Darr<A>(H)[f] = Ar / apr;
     }
