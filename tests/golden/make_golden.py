@@ -12,6 +12,7 @@ with `make -C oracle/ref`) on every deck in tests/golden/decks and stores:
 
 Needs the reference tree (default /root/reference); run it in the build
 container, never on the GPU box.  Usage: python tests/golden/make_golden.py
+[--only DECK] (one deck's digests, merged into the existing file).
 """
 import hashlib
 import json
@@ -29,7 +30,7 @@ from oracle.oracle import read_dump  # noqa: E402
 
 DRIVER = os.path.join(REPO, "oracle", "_ref", "ref_driver")
 FULL = {"small": [1, 2, 5], "inner": [1, 5, 20], "quirk": [1, 3]}
-DIGEST = {"config1": [1, 2, 5], "config3": [1, 3], "example13": [1, 2, 10]}
+DIGEST = {"config1": [1, 2, 5], "config3": [1, 3], "example13": [1, 2, 10], "example21": [1]}
 KEEP = ["u_star", "v_star", "w_star", "up", "vp", "wp", "p_temp", "t_temp", "ux", "uy", "uz", "p", "t",
         "id", "fluid.empty", "fluid.t_boundary", "fluid.t_halo", "solid.t_temp", "solid.t", "solid.empty",
         "solid.t_boundary", "solid.t_halo", "fluid.meta", "solid.meta", "pcg_iters"]
@@ -42,9 +43,33 @@ def run(deck, steps, work):
     return {s: read_dump("%s.step%d.bin" % (prefix, s)) for s in steps}
 
 
+def digest_entries(res):
+    out = {}
+    for s, d in res.items():
+        ent = {}
+        for k in KEEP:
+            if k in d and d[k].dtype == np.float64:
+                ent[k] = {"sha256": hashlib.sha256(d[k].tobytes()).hexdigest(),
+                          "l2": float(np.linalg.norm(d[k])), "n": int(d[k].size)}
+        ent["pcg_iters"] = int(d["pcg_iters"][0])
+        out[str(s)] = ent
+    return out
+
+
 def main():
     if not os.path.exists(DRIVER):
         subprocess.run(["make", "-C", os.path.join(REPO, "oracle", "ref")], check=True)
+    if len(sys.argv) > 2 and sys.argv[1] == "--only":
+        # regenerate one deck's digests and merge them into the existing file
+        deck = sys.argv[2]
+        path = os.path.join(HERE, "golden_digests.json")
+        with open(path) as f:
+            digests = json.load(f)
+        with tempfile.TemporaryDirectory() as work:
+            digests[deck] = digest_entries(run(deck, DIGEST[deck], work))
+        with open(path, "w") as f:
+            json.dump(digests, f, indent=1, sort_keys=True)
+        return
     digests = {}
     for deck, steps in FULL.items():
         with tempfile.TemporaryDirectory() as work:
@@ -57,16 +82,7 @@ def main():
         np.savez_compressed(os.path.join(HERE, "golden_%s.npz" % deck), **arrays)
     for deck, steps in DIGEST.items():
         with tempfile.TemporaryDirectory() as work:
-            res = run(deck, steps, work)
-        digests[deck] = {}
-        for s, d in res.items():
-            ent = {}
-            for k in KEEP:
-                if k in d and d[k].dtype == np.float64:
-                    ent[k] = {"sha256": hashlib.sha256(d[k].tobytes()).hexdigest(),
-                              "l2": float(np.linalg.norm(d[k])), "n": int(d[k].size)}
-            ent["pcg_iters"] = int(d["pcg_iters"][0])
-            digests[deck][str(s)] = ent
+            digests[deck] = digest_entries(run(deck, steps, work))
     with open(os.path.join(HERE, "golden_digests.json"), "w") as f:
         json.dump(digests, f, indent=1, sort_keys=True)
 

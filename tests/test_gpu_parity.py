@@ -8,6 +8,8 @@ bit-exact with the reference's sources (tests/test_oracle_golden.py).
 * With the reference's CG on, the only difference is the summation order of
   the CG dot products; fields must agree to relative L2 <= 1e-9 per outer
   step (far inside the 1e-6 of the parity target).
+* example21.in (the reference's 120^3 deck with internal walls and holes;
+  oracle bit-exact with the reference on it, golden digests) is in both.
 """
 import numpy as np
 import pytest
@@ -48,7 +50,8 @@ def test_init_state_bit_exact(deck):
         assert np.array_equal(g.solid(r, "t"), o.solid(r, "t"))
 
 
-@pytest.mark.parametrize("deck,steps", [("small", 6), ("inner", 4), ("config1", 3), ("example13", 2)])
+@pytest.mark.parametrize("deck,steps", [("small", 6), ("inner", 4), ("config1", 3), ("example13", 2),
+                                        ("example21", 1)])
 def test_sweeps_bit_exact_without_pressure_solve(deck, steps):
     g, o = _pair(read_deck(deck), pcg_maxiter=0)
     for s in range(steps):
@@ -64,7 +67,8 @@ def test_sweeps_bit_exact_without_pressure_solve(deck, steps):
             assert np.array_equal(g.solid(r), o.solid(r)), "solid %d step %d" % (r, s + 1)
 
 
-@pytest.mark.parametrize("deck,steps", [("small", 10), ("inner", 10), ("config1", 5), ("example13", 3)])
+@pytest.mark.parametrize("deck,steps", [("small", 10), ("inner", 10), ("config1", 5), ("example13", 3),
+                                        ("example21", 2)])
 def test_full_step_matches_oracle(deck, steps):
     g, o = _pair(read_deck(deck))
     for s in range(steps):
