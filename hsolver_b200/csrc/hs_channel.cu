@@ -367,7 +367,7 @@ __device__ __forceinline__ double ustar(const ChDev<R> &H, int f) {
 // cell's low side; the outlet face sits in the ghost cell i = N0) and the mass
 // imbalance b per cell (r = b, x = 0)
 template <class R>
-__global__ void k_ch_passemble(ChDev<R> H, double *acx, double *acy, double *acz, double *r, double *x, double *partials) {
+__global__ void k_ch_passemble(ChDev<R> H, R *acx, R *acy, R *acz, R *r, R *x, double *partials) {
   __shared__ double sh[32];
   const int T = gridDim.x * blockDim.x;
   const int N0 = H.N0, N1 = H.N1, N2 = H.N2;
@@ -381,33 +381,33 @@ __global__ void k_ch_passemble(ChDev<R> H, double *acx, double *acy, double *acz
       if (kind == 0) v = (double)face_area<0>(H, c) * (double)H.D0[fidx3<0>(H, c)];
       else if (kind == 2 && !H.solid[cidx(H, c[0] - 1, c[1], c[2])])
         v = (double)face_area<0>(H, c) * (double)H.D0[fidx<0>(H, c[0] - 1, c[1], c[2])];
-      acx[pq(N0, N1, c[0], c[1], c[2])] = v;
+      acx[pq(N0, N1, c[0], c[1], c[2])] = (R)v;
     }
   } else if (blockIdx.y == 1) {
     const long long n = (long long)N0 * (N1 + 1) * N2;
     for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += T) {
       const int c[3] = {(int)(e % N0), (int)((e / N0) % (N1 + 1)), (int)(e / ((long long)N0 * (N1 + 1)))};
-      acy[pq(N0, N1, c[0], c[1], c[2])] = face_kind<1>(H, c) == 0 ? (double)face_area<1>(H, c) * (double)H.D1[fidx3<1>(H, c)] : 0.0;
+      acy[pq(N0, N1, c[0], c[1], c[2])] = (R)(face_kind<1>(H, c) == 0 ? (double)face_area<1>(H, c) * (double)H.D1[fidx3<1>(H, c)] : 0.0);
     }
   } else if (blockIdx.y == 2) {
     const long long n = (long long)N0 * N1 * (N2 + 1);
     for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += T) {
       const int c[3] = {(int)(e % N0), (int)((e / N0) % N1), (int)(e / ((long long)N0 * N1))};
-      acz[pq(N0, N1, c[0], c[1], c[2])] = face_kind<2>(H, c) == 0 ? (double)face_area<2>(H, c) * (double)H.D2[fidx3<2>(H, c)] : 0.0;
+      acz[pq(N0, N1, c[0], c[1], c[2])] = (R)(face_kind<2>(H, c) == 0 ? (double)face_area<2>(H, c) * (double)H.D2[fidx3<2>(H, c)] : 0.0);
     }
   } else {
     const long long n = (long long)N0 * N1 * N2;
     for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += T) {
       const int i = (int)(e % N0), j = (int)((e / N0) % N1), k = (int)(e / ((long long)N0 * N1));
       const int q = pq(N0, N1, i, j, k);
-      x[q] = 0.0;
-      if (H.solid[e]) { r[q] = 0.0; continue; }
+      x[q] = R(0);
+      if (H.solid[e]) { r[q] = R(0); continue; }
       const double uw = ustar<0>(H, fidx<0>(H, i, j, k));
       const double ue = (i + 1 == N0) ? uw : ustar<0>(H, fidx<0>(H, i + 1, j, k));
       const double b = (uw - ue) * ((double)H.d1[j] * (double)H.d2[k]) +
                        (ustar<1>(H, fidx<1>(H, i, j, k)) - ustar<1>(H, fidx<1>(H, i, j + 1, k))) * ((double)H.d0[i] * (double)H.d2[k]) +
                        (ustar<2>(H, fidx<2>(H, i, j, k)) - ustar<2>(H, fidx<2>(H, i, j, k + 1))) * ((double)H.d0[i] * (double)H.d1[j]);
-      r[q] = b;
+      r[q] = (R)b;
       acc += b * b;
     }
   }
@@ -416,7 +416,7 @@ __global__ void k_ch_passemble(ChDev<R> H, double *acx, double *acy, double *acz
 }
 
 template <int A, class R>
-__device__ void correct_axis(const ChDev<R> &H, const double *pp) {
+__device__ void correct_axis(const ChDev<R> &H, const R *pp) {
   const int nf0 = H.N0 + (A == 0), nf1 = H.N1 + (A == 1), nf2 = H.N2 + (A == 2);
   const long long n = (long long)nf0 * nf1 * nf2;
   const int T = gridDim.x * blockDim.x;
@@ -435,7 +435,7 @@ __device__ void correct_axis(const ChDev<R> &H, const double *pp) {
       int lo[3] = {c[0], c[1], c[2]};
       lo[A] -= 1;
       const int f = fidx3<A>(H, c);
-      const double dp = pp[pq(H.N0, H.N1, lo[0], lo[1], lo[2])] - pp[pq(H.N0, H.N1, c[0], c[1], c[2])];
+      const double dp = (double)pp[pq(H.N0, H.N1, lo[0], lo[1], lo[2])] - (double)pp[pq(H.N0, H.N1, c[0], c[1], c[2])];
       if constexpr (!is_mixed(R())) val = Sarr<A>(H)[f] + Darr<A>(H)[f] * dp;
       else val = ustar<A>(H, f) + (double)Darr<A>(H)[f] * dp;
     }
@@ -445,7 +445,7 @@ __device__ void correct_axis(const ChDev<R> &H, const double *pp) {
 }
 
 template <class R>
-__global__ void k_ch_correct(ChDev<R> H, const double *pp) {
+__global__ void k_ch_correct(ChDev<R> H, const R *pp) {
   if (blockIdx.y == 0) correct_axis<0>(H, pp);
   else if (blockIdx.y == 1) correct_axis<1>(H, pp);
   else if (blockIdx.y == 2) correct_axis<2>(H, pp);
@@ -496,11 +496,15 @@ __global__ void k_ch_init(ChDev<R> H) {
 // ghost cell N0 + 1 is the outlet face, neighbour value 0).  Preconditioner:
 // the V-cycle of hs_mg.cuh in precision M on the same couplings (no
 // convection), solid cells masked.
+// p' system and CG vectors, stored in V (FP64 form: double; mixed form: float,
+// with FP64 arithmetic per element and FP64 dot products: p' is a correction
+// that vanishes at the fixed point, whose residuals are all FP64)
+template <class V>
 struct CgVec {
   int N0, N1, N2;
-  const double *acx, *acy, *acz;
+  const V *acx, *acy, *acz;
   const uint8_t *solid;
-  double *x, *r, *p, *p2, *s;  // p, p2: search direction, double-buffered
+  V *x, *r, *p, *p2, *s;  // p, p2: search direction, double-buffered
 };
 
 __device__ double grid_sum(double v, double *partials, int &buf, double *sh, cg::grid_group &grid) {
@@ -543,7 +547,7 @@ __device__ __forceinline__ void mg_rhs(const mg::Level<M> &L0, int e, int q, int
 constexpr int kPcgT = 768;
 
 template <class M>
-__device__ void mg_fine_from_couplings(const CgVec &V, const mg::Level<M> &L0, int tid, int T) {
+__device__ void mg_fine_from_couplings(const CgVec<M> &V, const mg::Level<M> &L0, int tid, int T) {
   const int PX = V.N0 + 2, PY = V.N1 + 2;
   const long long np = (long long)PX * PY * (V.N2 + 2);
   for (long long q = tid; q < np; q += T) {
@@ -560,7 +564,7 @@ __device__ void mg_fine_from_couplings(const CgVec &V, const mg::Level<M> &L0, i
 // forms the new p of its cell and of the six neighbours from z and the old
 // p; p is double-buffered), and <r, z> inside the V-cycle's last pass.
 template <class M>
-__global__ void __launch_bounds__(kPcgT, 1) k_ch_pcg(CgVec V, mg::Hier<M> G, int precond, double tol, int maxiter, double *partials,
+__global__ void __launch_bounds__(kPcgT, 1) k_ch_pcg(CgVec<M> V, mg::Hier<M> G, int precond, double tol, int maxiter, double *partials,
                                                int *out_it, double *out_rel) {
   cg::grid_group grid = cg::this_grid();
   __shared__ double sh[40];
@@ -577,7 +581,7 @@ __global__ void __launch_bounds__(kPcgT, 1) k_ch_pcg(CgVec V, mg::Hier<M> G, int
   double acc = 0.0;
   for (int e = tid; e < n; e += T) {
     const int q = cell_q(e, N0, N1);
-    const double rv = V.r[q];
+    const double rv = (double)V.r[q];
     acc += rv * rv;
     if (precond) mg_rhs(L0, e, q, N0, N1, rv);
   }
@@ -594,20 +598,20 @@ __global__ void __launch_bounds__(kPcgT, 1) k_ch_pcg(CgVec V, mg::Hier<M> G, int
     if (!mg::vcycle(G, false, grid, tid, T, V.r, &a))
       for (int e = tid; e < n; e += T) {
         const int q = cell_q(e, N0, N1);
-        a += V.r[q] * (double)__ldcg(L0.x + q);
+        a += (double)V.r[q] * (double)__ldcg(L0.x + q);
       }
     return grid_sum(a, partials, buf, sh, grid);
   };
   double gamma = rz(), rr = bb, beta = 0.0;
-  double *po = V.p, *pn = V.p2;
+  M *po = V.p, *pn = V.p2;
   int it = 0;
   while (it < maxiter && !(rr / bb < eps)) {
     const bool first = it == 0;
     it++;
     acc = 0.0;
     auto pval = [&](int qq) {
-      const double z = precond ? (double)__ldcg(L0.x + qq) : __ldcg(V.r + qq);
-      return first ? z : z + beta * __ldcg(po + qq);
+      const double z = precond ? (double)__ldcg(L0.x + qq) : (double)__ldcg(V.r + qq);
+      return (double)(M)(first ? z : z + beta * (double)__ldcg(po + qq));  // as stored
     };
     for (int e = tid; e < n; e += T) {
       const int q = cell_q(e, N0, N1);
@@ -616,9 +620,9 @@ __global__ void __launch_bounds__(kPcgT, 1) k_ch_pcg(CgVec V, mg::Hier<M> G, int
       const double d = cw + ce + cs + cn + cb + cf;
       const double sv = d * p0 - (cw * pval(q - 1) + ce * pval(q + 1) + cs * pval(q - PX) + cn * pval(q + PX) +
                                   cb * pval(q - PXY) + cf * pval(q + PXY));
-      pn[q] = p0;
-      V.s[q] = sv;
-      acc += sv * p0;
+      pn[q] = (M)p0;
+      V.s[q] = (M)sv;
+      acc += (double)(M)sv * p0;
     }
     const double sp = grid_sum(acc, partials, buf, sh, grid);
     if (sp == 0.0) break;
@@ -626,9 +630,9 @@ __global__ void __launch_bounds__(kPcgT, 1) k_ch_pcg(CgVec V, mg::Hier<M> G, int
     acc = 0.0;
     for (int e = tid; e < n; e += T) {
       const int q = cell_q(e, N0, N1);
-      V.x[q] = V.x[q] + alpha * pn[q];
-      const double rv = V.r[q] - alpha * V.s[q];
-      V.r[q] = rv;
+      V.x[q] = (M)((double)V.x[q] + alpha * (double)pn[q]);
+      const double rv = (double)(M)((double)V.r[q] - alpha * (double)V.s[q]);
+      V.r[q] = (M)rv;
       acc += rv * rv;
       if (precond) mg_rhs(L0, e, q, N0, N1, rv);
     }
@@ -637,7 +641,7 @@ __global__ void __launch_bounds__(kPcgT, 1) k_ch_pcg(CgVec V, mg::Hier<M> G, int
     const double gnew = precond ? rz() : rr;
     beta = gnew / gamma;
     gamma = gnew;
-    double *t = po; po = pn; pn = t;
+    M *t = po; po = pn; pn = t;
   }
   if (tid == 0) { *out_it = it; *out_rel = sqrt(rr / bb); }
 }
@@ -652,10 +656,6 @@ __global__ void k_ch_finalize(const double *mom, const double *cont, int nb, dou
     for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
     if (threadIdx.x == 0) res[a] = sqrt(s);
   }
-}
-
-__global__ void k_zero(double *a, long long n) {
-  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) a[e] = 0.0;
 }
 
 int blocks_for(long long n) { return (int)std::max<long long>(1, std::min<long long>((n + kT - 1) / kT, 148LL * 8)); }
@@ -682,7 +682,9 @@ struct ChannelState {
   long long bytes = 0;
   ChDev<double> Hd{};
   ChDev<float> Hf{};
-  CgVec V{};
+  CgVec<double> Vd{};
+  CgVec<float> Vf{};
+  double *scratch = nullptr;  // FP64 staging of field copies (padded cells)
   mg::Hier<double> Gd{};
   mg::Hier<float> Gf{};
   int mom_blocks = 0, pcg_grid = 0;
@@ -761,6 +763,18 @@ void setup_fields(ChannelState &S, ChDev<R> &H, const std::vector<double> (&d)[3
   }
 }
 
+template <class R> CgVec<R> &cg_vec(ChannelState &S);
+template <> CgVec<double> &cg_vec<double>(ChannelState &S) { return S.Vd; }
+template <> CgVec<float> &cg_vec<float>(ChannelState &S) { return S.Vf; }
+
+template <class R>
+void setup_cg(ChannelState &S, CgVec<R> &V, const uint8_t *solid, size_t np) {
+  V.N0 = S.N0; V.N1 = S.N1; V.N2 = S.N2; V.solid = solid;
+  V.acx = S.alloc<R>(np); V.acy = S.alloc<R>(np); V.acz = S.alloc<R>(np);
+  V.x = S.alloc<R>(np); V.r = S.alloc<R>(np); V.p = S.alloc<R>(np); V.s = S.alloc<R>(np);
+  V.p2 = S.alloc<R>(np);
+}
+
 template <class M>
 void setup_mg(ChannelState &S, mg::Hier<M> &G) {
   int nx = S.N0, ny = S.N1, nz = S.N2, L = 0;
@@ -797,26 +811,27 @@ void step_once(ChannelState &S, ChDev<R> &H, int flags) {
   if (S.prof) CH_CUDA(cudaEventRecord(S.ev[0], S.stream));
   mom_solve(S, H);
   if (S.prof) CH_CUDA(cudaEventRecord(S.ev[1], S.stream));
-  k_ch_passemble<R><<<dim3(S.mom_blocks, 4), kT, 0, S.stream>>>(H, (double *)S.V.acx, (double *)S.V.acy, (double *)S.V.acz,
-                                                                S.V.r, S.V.x, S.cont_part);
+  CgVec<R> &V = cg_vec<R>(S);
+  k_ch_passemble<R><<<dim3(S.mom_blocks, 4), kT, 0, S.stream>>>(H, (R *)V.acx, (R *)V.acy, (R *)V.acz, V.r, V.x,
+                                                                S.cont_part);
   k_ch_finalize<<<1, 32, 0, S.stream>>>(S.mom_part, S.cont_part, S.mom_blocks, S.res);
   CH_CUDA(cudaGetLastError());
   if (S.prof) CH_CUDA(cudaEventRecord(S.ev[2], S.stream));
   if (!(flags & 1)) {
     const int pre = S.prm.p_precond ? 1 : 0;
     if (S.mixed)
-      launch_coop(k_ch_pcg<float>, S.pcg_grid, S.stream, S.V, S.Gf, pre, S.prm.p_tol, S.prm.p_maxiter, S.pcg_part, S.pcg_it,
+      launch_coop(k_ch_pcg<float>, S.pcg_grid, S.stream, S.Vf, S.Gf, pre, S.prm.p_tol, S.prm.p_maxiter, S.pcg_part, S.pcg_it,
                   S.pcg_rel);
     else
-      launch_coop(k_ch_pcg<double>, S.pcg_grid, S.stream, S.V, S.Gd, pre, S.prm.p_tol, S.prm.p_maxiter, S.pcg_part, S.pcg_it,
+      launch_coop(k_ch_pcg<double>, S.pcg_grid, S.stream, S.Vd, S.Gd, pre, S.prm.p_tol, S.prm.p_maxiter, S.pcg_part, S.pcg_it,
                   S.pcg_rel);
   } else {
     const long long np = (long long)(S.N0 + 2) * (S.N1 + 2) * (S.N2 + 2);
-    k_zero<<<blocks_for(np), kT, 0, S.stream>>>(S.V.x, np);
+    CH_CUDA(cudaMemsetAsync(V.x, 0, np * sizeof(R), S.stream));
     CH_CUDA(cudaMemsetAsync(S.pcg_it, 0, sizeof(int), S.stream));
   }
   if (S.prof) CH_CUDA(cudaEventRecord(S.ev[3], S.stream));
-  k_ch_correct<R><<<dim3(S.mom_blocks, 4), kT, 0, S.stream>>>(H, (const double *)S.V.x);
+  k_ch_correct<R><<<dim3(S.mom_blocks, 4), kT, 0, S.stream>>>(H, (const R *)V.x);
   CH_CUDA(cudaGetLastError());
   if (S.prof) CH_CUDA(cudaEventRecord(S.ev[4], S.stream));
   if (!(flags & 2)) cht_energy_step(S.cht, S.prm.alpha_t, S.prm.t_tol, S.prm.t_maxiter);
@@ -907,10 +922,9 @@ ChannelState *ch_create(const Case &c, const ChParams &p, int device) {
   else setup_fields(*S, S->Hd, d, h, solid);
   // CG vectors and couplings (FP64, padded)
   const size_t np = (size_t)(S->N0 + 2) * (S->N1 + 2) * (S->N2 + 2);
-  S->V.N0 = S->N0; S->V.N1 = S->N1; S->V.N2 = S->N2; S->V.solid = solid;
-  S->V.acx = S->alloc<double>(np); S->V.acy = S->alloc<double>(np); S->V.acz = S->alloc<double>(np);
-  S->V.x = S->alloc<double>(np); S->V.r = S->alloc<double>(np); S->V.p = S->alloc<double>(np); S->V.s = S->alloc<double>(np);
-  S->V.p2 = S->alloc<double>(np);
+  if (S->mixed) setup_cg(*S, S->Vf, solid, np);
+  else setup_cg(*S, S->Vd, solid, np);
+  S->scratch = S->alloc<double>(np);
   if (S->mixed) setup_mg(*S, S->Gf);
   else setup_mg(*S, S->Gd);
   S->mom_blocks = blocks_for((long long)(S->N0 + 1) * (S->N1 + 1) * (S->N2 + 1));
@@ -1017,7 +1031,8 @@ long ch_field_size(const ChannelState *S, int f) {
 namespace {
 // device-side conversions for the field copies (the caller's host buffer is
 // copied to or from directly; pinned buffers go by DMA)
-__global__ void k_unpad(const double *src, double *dst, int N0, int N1, int N2) {
+template <class T>
+__global__ void k_unpad(const T *src, double *dst, int N0, int N1, int N2) {
   const int n = N0 * N1 * N2;
   for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x)
     dst[e] = src[cell_q(e, N0, N1)];
@@ -1047,15 +1062,16 @@ void h2d(ChannelState *S, double *dev, const double *host, long n) {
 }
 }  // namespace
 
-// Field copies between steps: V.s (a padded FP64 vector that only the
-// pressure solve uses) serves as device scratch.
+// Field copies between steps stage through `scratch` (padded FP64).
 void ch_get_field(ChannelState *S, int f, double *host, long n) {
   CH_CUDA(cudaSetDevice(S->device));
   if (ch_field_size(S, f) != n) throw std::invalid_argument("field size mismatch");
-  double *scr = S->V.s;
+  double *scr = S->scratch;
   const int g = blocks_for(n);
   if (f == 4 || f == 11) {
-    k_unpad<<<g, kT, 0, S->stream>>>(f == 4 ? cht_T_device(S->cht) : S->V.x, scr, S->N0, S->N1, S->N2);
+    if (f == 4) k_unpad<double><<<g, kT, 0, S->stream>>>(cht_T_device(S->cht), scr, S->N0, S->N1, S->N2);
+    else if (S->mixed) k_unpad<float><<<g, kT, 0, S->stream>>>(S->Vf.x, scr, S->N0, S->N1, S->N2);
+    else k_unpad<double><<<g, kT, 0, S->stream>>>(S->Vd.x, scr, S->N0, S->N1, S->N2);
     CH_CUDA(cudaGetLastError());
     d2h(S, scr, host, n);
     return;
@@ -1081,8 +1097,8 @@ void ch_set_field(ChannelState *S, int f, const double *host, long n) {
   if (ch_field_size(S, f) != n || f > 4) throw std::invalid_argument("field size mismatch or read-only field");
   const int g = blocks_for(n);
   if (f == 4) {
-    h2d(S, S->V.s, host, n);
-    k_pad<<<g, kT, 0, S->stream>>>(S->V.s, cht_T_device(S->cht), S->N0, S->N1, S->N2);
+    h2d(S, S->scratch, host, n);
+    k_pad<<<g, kT, 0, S->stream>>>(S->scratch, cht_T_device(S->cht), S->N0, S->N1, S->N2);
     CH_CUDA(cudaGetLastError());
     return;
   }

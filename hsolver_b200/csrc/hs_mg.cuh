@@ -185,9 +185,9 @@ __device__ void smooth(const Level<M> &L, int color, bool tr, int tid, int T) {
 // The last colour-0 half-sweep of level 0, also accumulating sum r x over
 // every cell (colour 0 as it is computed, colour 1 as left by the previous
 // half-sweep): the V-cycle's output dotted with the caller's residual r
-// (padded FP64) without a pass of its own.
-template <class M>
-__device__ void smooth_dot(const Level<M> &L, bool tr, const double *r, double &acc, int tid, int T) {
+// (padded, any precision; FP64 sums) without a pass of its own.
+template <class M, class RT>
+__device__ void smooth_dot(const Level<M> &L, bool tr, const RT *r, double &acc, int tid, int T) {
   const int half = (L.nx + 1) / 2;
   const int n = half * L.ny * L.nz;
   for (int e = tid; e < n; e += T) {
@@ -205,11 +205,11 @@ __device__ void smooth_dot(const Level<M> &L, bool tr, const double *r, double &
         xv = s / d;
       }
       L.x[q] = xv;
-      acc += r[q] * (double)xv;
+      acc += (double)r[q] * (double)xv;
     }
     if (ib < L.nx) {
       const int q = idx(L, ib + 1, j + 1, k + 1);
-      acc += r[q] * (double)__ldcg(L.x + q);
+      acc += (double)r[q] * (double)__ldcg(L.x + q);
     }
   }
 }
@@ -420,9 +420,9 @@ __device__ void build(const Hier<M> &G, bool tr, cg::grid_group &grid, int tid, 
 // thread's share of sum dot_r x to *dot_acc and the final barrier is left to
 // the caller's reduction (returns true); it returns false, with the barrier
 // done and nothing added, when level 0 is handled by block 0 alone.
-template <class M>
+template <class M, class RT = double>
 __device__ bool vcycle(const Hier<M> &G, bool tr, cg::grid_group &grid, int tid, int T,
-                       const double *dot_r = nullptr, double *dot_acc = nullptr) {
+                       const RT *dot_r = nullptr, double *dot_acc = nullptr) {
   int ls = 0;  // first level handled by block 0 alone
   while (ls < G.L - 1 && !small(G.lv[ls])) ++ls;
   for (int l = 0; l < ls; ++l) {
