@@ -135,6 +135,32 @@ def pcg_bytes(ncell, iters, wbytes=8):
     return ncell * (setup + iters * (cg + vc))
 
 
+def kernel_classes(phases, iters_mean, dims, mom_sweeps, peak):
+    """Achieved HBM bandwidth of each phase of the outer step on its
+    algorithmic bytes (FP64 form; each array counted once per pass):
+      momentum: 49 B per face per red-black pass (u^n of the three
+        components, p, u*, mask; u* written), 2 passes per sweep;
+      p' assembly: 89 B per cell (u*, v*, w*, d of the three components,
+        mask; three couplings and b written);
+      p' solve: pcg_bytes();
+      correction: 96 B per cell (u*, d, u per face of the three components;
+        p', p read, p written).
+    The energy solve (BiCGStab with two V-cycles per iteration on six
+    coefficient arrays per level) is not modelled here."""
+    nx, ny, nz = dims
+    ncell = nx * ny * nz
+    nface = (nx + 1) * ny * nz + nx * (ny + 1) * nz + nx * ny * (nz + 1)
+    model = {"momentum": 49.0 * nface * 2 * mom_sweeps, "p_assembly": 89.0 * ncell,
+             "p_solve": pcg_bytes(ncell, iters_mean), "correction": 96.0 * ncell}
+    out = {}
+    for k, b in model.items():
+        ms = phases.get(k, 0.0)
+        gbs = b / (ms * 1e-3) / 1e9 if ms > 0 else None
+        out[k] = {"algorithmic_bytes": b, "ms": ms, "achieved_gbs": gbs, "frac": (gbs / peak) if gbs else None}
+    out["energy"] = {"ms": phases.get("energy"), "achieved_gbs": None, "frac": None, "note": "not modelled"}
+    return out
+
+
 def time_steps(torch, g, steps, local):
     stream = torch.cuda.ExternalStream(g.stream(), device=local)
     torch.cuda.synchronize()
@@ -292,6 +318,7 @@ def run_gpu(args):
                          "algorithmic_bytes_per_launch": b,
                          "pcg_iters_per_launch": it_mean, "launch_ms": pms},
             "phase_ms_per_step": phases,
+            "kernel_classes": kernel_classes(phases, it_mean, CONFIG["grid"], 2, peak),
             "last_step": {"pcg_iters": st["pcg_iters"], "t_iters": st["t_iters"], "global_residual": st["global"]},
             "device_bytes": dev_bytes,
             "gpu_launches": LAUNCHES_PER_STEP * args.steps,

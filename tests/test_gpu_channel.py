@@ -173,3 +173,32 @@ def test_adjoint_at_config4_vs_central_differences():
         km[b] *= 1 - h
         fd = (J(kp, q) - J(km, q)) / (2 * h)          # dJ / d(log k_b)
         assert abs(fd - dk_ratio[b] * k[b]) <= 1e-5 * scale, (b, fd, dk_ratio[b] * k[b])
+
+
+@pytest.mark.parametrize("name", ["config1", "config3"])
+def test_configs_match_oracle(name):
+    """The configuration-1 channel and its wall-stretched variant (tanh
+    clustering in y and z, cell aspect ratio up to 20): five outer steps of
+    the GPU against the oracle with tight inner tolerances, and the momentum
+    sweeps bit for bit with the pressure and energy solves off."""
+    import bench
+    import hsolver_b200
+    from oracle import oracle
+    deck, re_, k, q, ctype = bench.workload(name)
+    kw = dict(re=re_, p_tol=1e-13, p_maxiter=5000, t_tol=1e-13, t_maxiter=5000)
+    g = hsolver_b200.Channel(deck, **kw)
+    o = oracle.ChannelCase(deck, **kw)
+    for s_ in (g, o):
+        s_.set_solid(k, q)
+        s_.init()
+    g.step(3, flags=3)
+    o.step(3, pressure=False, energy=False)
+    for f in FACE + ["u_star", "v_star", "w_star"]:
+        assert np.array_equal(g.field(f), o.field(f)), f
+    g.init()
+    o.init()
+    for _ in range(5):
+        g.step(1)
+        o.step(1)
+    for f in FACE + ["p", "T"]:
+        assert _rel(g.field(f), o.field(f)) < 1e-9, f
