@@ -8,9 +8,11 @@ heat source q ~ U[0.5, 2] and k_solid/k_fluid ~ U[10, 1000] per block;
 relaxation 0.7 / 0.3 / 0.9; FP64 throughout (the plain form); pressure
 correction by multigrid-preconditioned CG to the reference's rtol 1e-5
 (fluid_solver.h:1874); energy over fluid and solid by multigrid-preconditioned
-BiCGStab to 1e-1 of its initial residual per outer step.  (The number of outer
-steps to a 1e-6 global residual is the same, 1393, for p' rtol 1e-8 .. 1e-3
-and energy 1e-2 .. 1e-1: SIMPLE's rate is set by the relaxation.)  Synthetic input generated
+BiCGStab to 0.5 of its initial residual per outer step (the temperature is
+one-way coupled; its residual stays an order below the momentum residuals).
+(The number of outer steps to a 1e-6 global residual is the same, 1393, for
+p' rtol 1e-8 .. 1e-3 and energy 1e-2 .. 0.5: SIMPLE's rate is set by the
+relaxation; the stop test includes the FP64 energy residual.)  Synthetic input generated
 in-repo; the state (~790 MB on the device) is larger than L2.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
@@ -42,13 +44,13 @@ FALLBACK_HBM_GBS = 6650.0
 NAME = "config2"
 # inner tolerances of the at-scale case (config 1 keeps the library defaults,
 # p' rtol 1e-8 as its specification states)
-SOLVER = {"p_tol": 1e-5, "t_tol": 1e-1}
+SOLVER = {"p_tol": 1e-5, "t_tol": 0.5}
 CONFIG = {"workload": "channel 256x128x128 (4.19M cells), 8 seeded heated blocks (edges 8-24, q U[0.5,2], "
                       "k_s/k_f U[10,1000]), Re 400, SIMPLE-CHT outer step",
           "grid": [256, 128, 128], "blocks": 8, "seed": 0, "precision": "fp64", "re": 400, "pr": 0.71,
           "relaxation": {"u": 0.7, "p": 0.3, "T": 0.9}, "momentum": "FOU, 2 red-black GS sweeps",
           "pressure_solver": "CG + multigrid V-cycle (FP64), rtol 1e-5 (the reference's HYPRE setting)",
-          "energy_solver": "BiCGStab + multigrid V-cycle (FP64), 1e-1 of the initial residual per step",
+          "energy_solver": "BiCGStab + multigrid V-cycle (FP64), 0.5 of the initial residual per step",
           "l2_policy": "state ~790 MB on the device, larger than L2 (126 MB)", "parallelism": "replicas"}
 # launches per outer step: 4 momentum passes, p' assembly, residual finalize,
 # p' solve, correction, energy assembly, energy BiCGStab, energy relaxation
