@@ -26,6 +26,9 @@
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
 
 typedef int64_t I64;
 
@@ -1163,6 +1166,7 @@ static void cht_face(const or_cht *H, I64 i, I64 j, I64 k, int d, double *G, dou
 }
 
 static void cht_apply(const or_cht *H, const double *x, double *y, int transpose) {
+#pragma omp parallel for schedule(static)
   for (I64 k = 0; k < H->Nz; ++k) for (I64 j = 0; j < H->Ny; ++j) for (I64 i = 0; i < H->Nx; ++i) {
     I64 c = CC(i, j, k);
     double diag = 0, off = 0;
@@ -1179,6 +1183,7 @@ static void cht_apply(const or_cht *H, const double *x, double *y, int transpose
 }
 
 static void cht_rhs(const or_cht *H, double *b) {
+#pragma omp parallel for schedule(static)
   for (I64 k = 0; k < H->Nz; ++k) for (I64 j = 0; j < H->Ny; ++j) for (I64 i = 0; i < H->Nx; ++i) {
     I64 c = CC(i, j, k);
     double V = (H->xs[i + 1] - H->xs[i]) * (H->ys[j + 1] - H->ys[j]) * (H->zs[k + 1] - H->zs[k]);
@@ -1205,12 +1210,15 @@ static int cht_bicgstab(const or_cht *H, int transpose, const double *b, double 
   I64 N = H->Nx * H->Ny * H->Nz;
   double *r = malloc(8 * N), *rh = malloc(8 * N), *p = calloc(N, 8), *v = calloc(N, 8), *ph = malloc(8 * N);
   double *s = malloc(8 * N), *sh = malloc(8 * N), *t = malloc(8 * N), *dinv = malloc(8 * N);
+#pragma omp parallel for schedule(static)
   for (I64 k = 0; k < H->Nz; ++k) for (I64 j = 0; j < H->Ny; ++j) for (I64 i = 0; i < H->Nx; ++i) dinv[CC(i, j, k)] = 1.0 / cht_diag(H, i, j, k);
   cht_apply(H, x, r, transpose);
   double bb = 0;
+#pragma omp parallel for schedule(static) reduction(+:bb)
   for (I64 c = 0; c < N; ++c) { r[c] = b[c] - r[c]; rh[c] = r[c]; bb += b[c] * b[c]; }
   double rho = 1, alpha = 1, omega = 1, rr = 0;
   int it = 0;
+#pragma omp parallel for schedule(static) reduction(+:rr)
   for (I64 c = 0; c < N; ++c) rr += r[c] * r[c];
   if (r0norm) *r0norm = sqrt(rr);
   if (rel0) bb = rr;
@@ -1218,21 +1226,27 @@ static int cht_bicgstab(const or_cht *H, int transpose, const double *b, double 
   while (it < maxiter && rr / bb >= tol * tol) {
     it++;
     double rho1 = 0;
+#pragma omp parallel for schedule(static) reduction(+:rho1)
     for (I64 c = 0; c < N; ++c) rho1 += rh[c] * r[c];
     double beta = (rho1 / rho) * (alpha / omega);
+#pragma omp parallel for schedule(static)
     for (I64 c = 0; c < N; ++c) { p[c] = r[c] + beta * (p[c] - omega * v[c]); ph[c] = p[c] * dinv[c]; }
     cht_apply(H, ph, v, transpose);
     double rv = 0;
+#pragma omp parallel for schedule(static) reduction(+:rv)
     for (I64 c = 0; c < N; ++c) rv += rh[c] * v[c];
     alpha = rho1 / rv;
     double ss = 0;
+#pragma omp parallel for schedule(static) reduction(+:ss)
     for (I64 c = 0; c < N; ++c) { s[c] = r[c] - alpha * v[c]; sh[c] = s[c] * dinv[c]; ss += s[c] * s[c]; }
     if (ss / bb < tol * tol) { for (I64 c = 0; c < N; ++c) x[c] += alpha * ph[c]; rr = ss; break; }
     cht_apply(H, sh, t, transpose);
     double ts = 0, tt = 0;
+#pragma omp parallel for schedule(static) reduction(+:ts, tt)
     for (I64 c = 0; c < N; ++c) { ts += t[c] * s[c]; tt += t[c] * t[c]; }
     omega = ts / tt;
     rr = 0;
+#pragma omp parallel for schedule(static) reduction(+:rr)
     for (I64 c = 0; c < N; ++c) { x[c] += alpha * ph[c] + omega * sh[c]; r[c] = s[c] - omega * t[c]; rr += r[c] * r[c]; }
     rho = rho1;
   }
@@ -1456,6 +1470,8 @@ static void ch_momentum(or_ch *C) {
     for (int color = 0; color < 2; ++color)
       for (int a = 0; a < 3; ++a) {
         const double *src = (sw == 0 && color == 0) ? C->U[a] : C->US[a];
+        double ra = 0.0;
+#pragma omp parallel for schedule(static) reduction(+:ra)
         for (I64 k = 0; k < ch_nf(C, a, 2); ++k) for (I64 j = 0; j < ch_nf(C, a, 1); ++j) for (I64 i = 0; i < ch_nf(C, a, 0); ++i) {
           I64 c[3] = {i, j, k};
           I64 f = ch_f(C, a, i, j, k);
@@ -1473,7 +1489,7 @@ static void ch_momentum(or_ch *C) {
           double un = C->U[a][f];
           if (sw == 0 && color == 0) {
             double r = aP * un - (ch_nbsum(C, C->U[a], a, an, nb, valid) + bs);
-            rs[a] += r * r;
+            ra += r * r;
           }
           if (!mine) continue;
           double apr = aP / C->P.alpha_u;
@@ -1481,6 +1497,7 @@ static void ch_momentum(or_ch *C) {
           C->US[a][f] = rhs / apr;
           if (sw == C->P.mom_sweeps - 1) C->D[a][f] = ch_area(C, a, c) / apr;
         }
+        rs[a] += ra;
       }
   for (int a = 0; a < 3; ++a) C->res[a] = sqrt(rs[a]);
 }
@@ -1488,6 +1505,7 @@ static void ch_momentum(or_ch *C) {
 /* p' couplings per face and the mass imbalance b per cell; returns ||b|| */
 static double ch_passemble(or_ch *C) {
   for (int a = 0; a < 3; ++a)
+#pragma omp parallel for schedule(static)
     for (I64 k = 0; k < ch_nf(C, a, 2); ++k) for (I64 j = 0; j < ch_nf(C, a, 1); ++j) for (I64 i = 0; i < ch_nf(C, a, 0); ++i) {
       I64 c[3] = {i, j, k}, f = ch_f(C, a, i, j, k);
       int kind = ch_kind(C, a, c);
@@ -1497,6 +1515,7 @@ static double ch_passemble(or_ch *C) {
       C->ac[a][f] = v;
     }
   double bb = 0.0;
+#pragma omp parallel for schedule(static) reduction(+:bb)
   for (I64 k = 0; k < C->N[2]; ++k) for (I64 j = 0; j < C->N[1]; ++j) for (I64 i = 0; i < C->N[0]; ++i) {
     I64 c = ch_c(C, i, j, k);
     if (C->solid[c]) { C->bc[c] = 0.0; continue; }
@@ -1511,6 +1530,7 @@ static double ch_passemble(or_ch *C) {
 }
 
 static void ch_apply(const or_ch *C, const double *x, double *y) {
+#pragma omp parallel for schedule(static)
   for (I64 k = 0; k < C->N[2]; ++k) for (I64 j = 0; j < C->N[1]; ++j) for (I64 i = 0; i < C->N[0]; ++i) {
     I64 c = ch_c(C, i, j, k);
     if (C->solid[c]) { y[c] = 0.0; continue; }
@@ -1534,6 +1554,7 @@ static void ch_pcg(or_ch *C) {
   I64 N = C->N[0] * C->N[1] * C->N[2];
   double *r = malloc(8 * N), *p = malloc(8 * N), *s = malloc(8 * N);
   double bb = 0.0;
+#pragma omp parallel for schedule(static) reduction(+:bb)
   for (I64 c = 0; c < N; ++c) { C->pp[c] = 0.0; r[c] = C->bc[c]; p[c] = r[c]; bb += r[c] * r[c]; }
   double rr = bb;
   int it = 0;
@@ -1541,11 +1562,14 @@ static void ch_pcg(or_ch *C) {
     it++;
     ch_apply(C, p, s);
     double sp = 0.0;
+#pragma omp parallel for schedule(static) reduction(+:sp)
     for (I64 c = 0; c < N; ++c) sp += s[c] * p[c];
     double alpha = rr / sp, rr1 = 0.0;
+#pragma omp parallel for schedule(static) reduction(+:rr1)
     for (I64 c = 0; c < N; ++c) { C->pp[c] += alpha * p[c]; r[c] -= alpha * s[c]; rr1 += r[c] * r[c]; }
     double beta = rr1 / rr;
     rr = rr1;
+#pragma omp parallel for schedule(static)
     for (I64 c = 0; c < N; ++c) p[c] = r[c] + beta * p[c];
   }
   C->pcg_iters = it;
@@ -1555,6 +1579,7 @@ static void ch_pcg(or_ch *C) {
 
 static void ch_correct(or_ch *C) {
   for (int a = 0; a < 3; ++a)
+#pragma omp parallel for schedule(static)
     for (I64 k = 0; k < ch_nf(C, a, 2); ++k) for (I64 j = 0; j < ch_nf(C, a, 1); ++j) for (I64 i = 0; i < ch_nf(C, a, 0); ++i) {
       I64 c[3] = {i, j, k}, f = ch_f(C, a, i, j, k);
       int kind = ch_kind(C, a, c);
@@ -1739,3 +1764,12 @@ void or_ch_destroy(or_ch *C) {
 }
 
 void or_ch_dims(const or_ch *C, I64 *out3) { out3[0] = C->N[0]; out3[1] = C->N[1]; out3[2] = C->N[2]; }
+
+/* threads the OpenMP loops of the channel / CHT paths use (1 without OpenMP) */
+int or_threads(void) {
+#ifdef _OPENMP
+  return omp_get_max_threads();
+#else
+  return 1;
+#endif
+}

@@ -3,6 +3,10 @@ import sys
 
 import pytest
 
+# the oracle's OpenMP loops on one thread: every sum in loop order, so its
+# results are reproducible bit for bit (set before the library loads)
+os.environ["OMP_NUM_THREADS"] = "1"
+
 REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 if REPO not in sys.path:
     sys.path.insert(0, REPO)
