@@ -311,11 +311,10 @@ __device__ double block_sum(double v, double *sh) {
 template <int A, class R>
 __device__ void mom_pass_axis(const ChDev<R> &H, int color, bool first, bool last, double &racc) {
   const int nf0 = H.N0 + (A == 0), nf1 = H.N1 + (A == 1), nf2 = H.N2 + (A == 2);
-  const int T = gridDim.x * blockDim.x;
+  const int T = gridDim.x * blockDim.x, tid = blockIdx.x * blockDim.x + threadIdx.x;
   if (first) {
-    const long long n = (long long)nf0 * nf1 * nf2;
-    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += T) {
-      const int c[3] = {(int)(e % nf0), (int)((e / nf0) % nf1), (int)(e / ((long long)nf0 * nf1))};
+    for (mg::Walk w(nf0, nf1, nf2, tid, T); w.ok(); w.next()) {
+      const int c[3] = {w.m, w.j, w.k};
       const int kind = face_kind<A>(H, c);
       if (kind != 0) {
         const int f = fidx3<A>(H, c);
@@ -327,11 +326,8 @@ __device__ void mom_pass_axis(const ChDev<R> &H, int color, bool first, bool las
       mom_face<A>(H, c, true, mine, last && mine, racc);
     }
   } else {
-    const int half = (nf0 + 1) / 2;
-    const long long n = (long long)half * nf1 * nf2;
-    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += T) {
-      const int m = (int)(e % half), j = (int)((e / half) % nf1), k = (int)(e / ((long long)half * nf1));
-      const int i = 2 * m + ((j + k + color) & 1);
+    for (mg::Walk w((nf0 + 1) / 2, nf1, nf2, tid, T); w.ok(); w.next()) {
+      const int j = w.j, k = w.k, i = 2 * w.m + ((j + k + color) & 1);
       if (i >= nf0) continue;
       const int c[3] = {i, j, k};
       if (face_kind<A>(H, c) != 0) continue;
@@ -369,13 +365,12 @@ __device__ __forceinline__ double ustar(const ChDev<R> &H, int f) {
 template <class R>
 __global__ void k_ch_passemble(ChDev<R> H, R *acx, R *acy, R *acz, R *r, R *x, double *partials) {
   __shared__ double sh[32];
-  const int T = gridDim.x * blockDim.x;
+  const int T = gridDim.x * blockDim.x, tid = blockIdx.x * blockDim.x + threadIdx.x;
   const int N0 = H.N0, N1 = H.N1, N2 = H.N2;
   double acc = 0.0;
   if (blockIdx.y == 0) {
-    const long long n = (long long)(N0 + 1) * N1 * N2;
-    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += T) {
-      const int c[3] = {(int)(e % (N0 + 1)), (int)((e / (N0 + 1)) % N1), (int)(e / ((long long)(N0 + 1) * N1))};
+    for (mg::Walk w(N0 + 1, N1, N2, tid, T); w.ok(); w.next()) {
+      const int c[3] = {w.m, w.j, w.k};
       const int kind = face_kind<0>(H, c);
       double v = 0.0;
       if (kind == 0) v = (double)face_area<0>(H, c) * (double)H.D0[fidx3<0>(H, c)];
@@ -384,21 +379,18 @@ __global__ void k_ch_passemble(ChDev<R> H, R *acx, R *acy, R *acz, R *r, R *x, d
       acx[pq(N0, N1, c[0], c[1], c[2])] = (R)v;
     }
   } else if (blockIdx.y == 1) {
-    const long long n = (long long)N0 * (N1 + 1) * N2;
-    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += T) {
-      const int c[3] = {(int)(e % N0), (int)((e / N0) % (N1 + 1)), (int)(e / ((long long)N0 * (N1 + 1)))};
+    for (mg::Walk w(N0, N1 + 1, N2, tid, T); w.ok(); w.next()) {
+      const int c[3] = {w.m, w.j, w.k};
       acy[pq(N0, N1, c[0], c[1], c[2])] = (R)(face_kind<1>(H, c) == 0 ? (double)face_area<1>(H, c) * (double)H.D1[fidx3<1>(H, c)] : 0.0);
     }
   } else if (blockIdx.y == 2) {
-    const long long n = (long long)N0 * N1 * (N2 + 1);
-    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += T) {
-      const int c[3] = {(int)(e % N0), (int)((e / N0) % N1), (int)(e / ((long long)N0 * N1))};
+    for (mg::Walk w(N0, N1, N2 + 1, tid, T); w.ok(); w.next()) {
+      const int c[3] = {w.m, w.j, w.k};
       acz[pq(N0, N1, c[0], c[1], c[2])] = (R)(face_kind<2>(H, c) == 0 ? (double)face_area<2>(H, c) * (double)H.D2[fidx3<2>(H, c)] : 0.0);
     }
   } else {
-    const long long n = (long long)N0 * N1 * N2;
-    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += T) {
-      const int i = (int)(e % N0), j = (int)((e / N0) % N1), k = (int)(e / ((long long)N0 * N1));
+    for (mg::Walk w(N0, N1, N2, tid, T); w.ok(); w.next()) {
+      const int i = w.m, j = w.j, k = w.k, e = w.flat();
       const int q = pq(N0, N1, i, j, k);
       x[q] = R(0);
       if (H.solid[e]) { r[q] = R(0); continue; }
@@ -418,10 +410,10 @@ __global__ void k_ch_passemble(ChDev<R> H, R *acx, R *acy, R *acz, R *r, R *x, d
 template <int A, class R>
 __device__ void correct_axis(const ChDev<R> &H, const R *pp) {
   const int nf0 = H.N0 + (A == 0), nf1 = H.N1 + (A == 1), nf2 = H.N2 + (A == 2);
-  const long long n = (long long)nf0 * nf1 * nf2;
-  const int T = gridDim.x * blockDim.x;
-  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += T) {
-    const int c[3] = {(int)(e % nf0), (int)((e / nf0) % nf1), (int)(e / ((long long)nf0 * nf1))};
+  const int T = gridDim.x * blockDim.x, tid = blockIdx.x * blockDim.x + threadIdx.x;
+  for (mg::Walk w(nf0, nf1, nf2, tid, T); w.ok(); w.next()) {
+    const int c[3] = {w.m, w.j, w.k};
+    const int e = w.flat();
     const int kind = face_kind<A>(H, c);
     double val;
     if (kind == 1) {
@@ -450,11 +442,10 @@ __global__ void k_ch_correct(ChDev<R> H, const R *pp) {
   else if (blockIdx.y == 1) correct_axis<1>(H, pp);
   else if (blockIdx.y == 2) correct_axis<2>(H, pp);
   else {
-    const long long n = (long long)H.N0 * H.N1 * H.N2;
-    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+    for (mg::Walk w(H.N0, H.N1, H.N2, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x); w.ok(); w.next()) {
+      const int e = w.flat();
       if (H.solid[e]) continue;
-      const int i = (int)(e % H.N0), j = (int)((e / H.N0) % H.N1), k = (int)(e / ((long long)H.N0 * H.N1));
-      H.p[e] = H.p[e] + H.ap * pp[pq(H.N0, H.N1, i, j, k)];
+      H.p[e] = H.p[e] + H.ap * pp[pq(H.N0, H.N1, w.m, w.j, w.k)];
     }
   }
 }
@@ -532,16 +523,6 @@ __device__ __forceinline__ int cell_q(int e, int N0, int N1) {
   return (i + 1) + (N0 + 2) * ((j + 1) + (N1 + 2) * (k + 1));
 }
 
-// V-cycle right-hand side of cell e and its seed (the first red half-sweep)
-template <class M>
-__device__ __forceinline__ void mg_rhs(const mg::Level<M> &L0, int e, int q, int N0, int N1, double v) {
-  const int row_ = e / N0, i = e - row_ * N0;
-  const int k = row_ / N1, j = row_ - k * N1;
-  const M m = (M)v;
-  L0.rhs[q] = m;
-  mg::seed(L0, q, i, j, k, m, false);
-}
-
 // one 768-thread block per SM: the same warps per SM as three 256-thread
 // blocks, a third of the arrivals at every grid barrier
 constexpr int kPcgT = 768;
@@ -569,8 +550,7 @@ __global__ void __launch_bounds__(kPcgT, 1) k_ch_pcg(CgVec<M> V, mg::Hier<M> G, 
   cg::grid_group grid = cg::this_grid();
   __shared__ double sh[40];
   const int tid = blockIdx.x * blockDim.x + threadIdx.x, T = gridDim.x * blockDim.x;
-  const int N0 = V.N0, N1 = V.N1, PX = N0 + 2, PXY = (N0 + 2) * (N1 + 2);
-  const int n = N0 * N1 * V.N2;
+  const int N0 = V.N0, N1 = V.N1, PX = N0 + 2, PY = N1 + 2, PXY = (N0 + 2) * (N1 + 2);
   int buf = 0;
   const mg::Level<M> &L0 = G.lv[0];
   if (precond) {
@@ -579,11 +559,11 @@ __global__ void __launch_bounds__(kPcgT, 1) k_ch_pcg(CgVec<M> V, mg::Hier<M> G, 
     mg::build(G, false, grid, tid, T);
   }
   double acc = 0.0;
-  for (int e = tid; e < n; e += T) {
-    const int q = cell_q(e, N0, N1);
+  for (mg::Walk w(N0, N1, V.N2, tid, T); w.ok(); w.next()) {
+    const int q = (w.m + 1) + PX * ((w.j + 1) + PY * (w.k + 1));
     const double rv = (double)V.r[q];
     acc += rv * rv;
-    if (precond) mg_rhs(L0, e, q, N0, N1, rv);
+    if (precond) mg::seed_at(L0, w.m, w.j, w.k, q, false).store(L0, q, rv);
   }
   const double bb = grid_sum(acc, partials, buf, sh, grid);
   if (bb == 0.0) {
@@ -596,8 +576,8 @@ __global__ void __launch_bounds__(kPcgT, 1) k_ch_pcg(CgVec<M> V, mg::Hier<M> G, 
     double a = 0.0;
     if (!precond) return bb;
     if (!mg::vcycle(G, false, grid, tid, T, V.r, &a))
-      for (int e = tid; e < n; e += T) {
-        const int q = cell_q(e, N0, N1);
+      for (mg::Walk w(N0, N1, V.N2, tid, T); w.ok(); w.next()) {
+        const int q = (w.m + 1) + PX * ((w.j + 1) + PY * (w.k + 1));
         a += (double)V.r[q] * (double)__ldcg(L0.x + q);
       }
     return grid_sum(a, partials, buf, sh, grid);
@@ -613,8 +593,8 @@ __global__ void __launch_bounds__(kPcgT, 1) k_ch_pcg(CgVec<M> V, mg::Hier<M> G, 
       const double z = precond ? (double)__ldcg(L0.x + qq) : (double)__ldcg(V.r + qq);
       return (double)(M)(first ? z : z + beta * (double)__ldcg(po + qq));  // as stored
     };
-    for (int e = tid; e < n; e += T) {
-      const int q = cell_q(e, N0, N1);
+    for (mg::Walk w(N0, N1, V.N2, tid, T); w.ok(); w.next()) {
+      const int q = (w.m + 1) + PX * ((w.j + 1) + PY * (w.k + 1));
       const double p0 = pval(q);
       const double cw = V.acx[q], ce = V.acx[q + 1], cs = V.acy[q], cn = V.acy[q + PX], cb = V.acz[q], cf = V.acz[q + PXY];
       const double d = cw + ce + cs + cn + cb + cf;
@@ -628,13 +608,15 @@ __global__ void __launch_bounds__(kPcgT, 1) k_ch_pcg(CgVec<M> V, mg::Hier<M> G, 
     if (sp == 0.0) break;
     const double alpha = gamma / sp;
     acc = 0.0;
-    for (int e = tid; e < n; e += T) {
-      const int q = cell_q(e, N0, N1);
-      V.x[q] = (M)((double)V.x[q] + alpha * (double)pn[q]);
-      const double rv = (double)(M)((double)V.r[q] - alpha * (double)V.s[q]);
+    for (mg::Walk w(N0, N1, V.N2, tid, T); w.ok(); w.next()) {
+      const int q = (w.m + 1) + PX * ((w.j + 1) + PY * (w.k + 1));
+      const double xv = (double)V.x[q], pv = (double)pn[q], r0 = (double)V.r[q], sv = (double)V.s[q];
+      const mg::Seed<M> sd = precond ? mg::seed_at(L0, w.m, w.j, w.k, q, false) : mg::Seed<M>{};
+      V.x[q] = (M)(xv + alpha * pv);
+      const double rv = (double)(M)(r0 - alpha * sv);
       V.r[q] = (M)rv;
       acc += rv * rv;
-      if (precond) mg_rhs(L0, e, q, N0, N1, rv);
+      if (precond) sd.store(L0, q, rv);
     }
     rr = grid_sum(acc, partials, buf, sh, grid);
     if (rr / bb < eps) break;

@@ -128,9 +128,8 @@ __device__ __forceinline__ void face(const ChtDev &H, int i, int j, int k, int d
 }
 
 __global__ void k_cht_assemble(ChtDev H, double Tb) {
-  const int n = H.Nx * H.Ny * H.Nz;
-  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
-    const int i = c % H.Nx, j = (c / H.Nx) % H.Ny, k = c / (H.Nx * H.Ny);
+  for (mg::Walk w(H.Nx, H.Ny, H.Nz, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x); w.ok(); w.next()) {
+    const int i = w.m, j = w.j, k = w.k;
     const int q = pidx(H, i, j, k);
     double diag = 0.0, a[6], rhs = H.q[q] * H.dx[i] * H.dy[j] * H.dz[k];
     for (int d = 0; d < 6; ++d) {
@@ -197,22 +196,6 @@ __device__ __forceinline__ double apply_any(const ChtDev &H, const XT *x, int q,
   return H.d[q] * (double)__ldcg(x + q) - off;
 }
 
-__device__ __forceinline__ int cell_pidx(const ChtDev &H, int c) {
-  const int row_ = c / H.Nx, i = c - row_ * H.Nx;
-  const int k = row_ / H.Ny, j = row_ - k * H.Ny;
-  return (i + 1) + (H.Nx + 2) * ((j + 1) + (H.Ny + 2) * (k + 1));
-}
-
-// V-cycle right-hand side of cell c and its seed (the first red half-sweep)
-template <class MT>
-__device__ __forceinline__ void mg_rhs(const ChtDev &H, const mg::Level<MT> &L0, int c, int q, double v, bool tr) {
-  const int row_ = c / H.Nx, i = c - row_ * H.Nx;
-  const int k = row_ / H.Ny, j = row_ - k * H.Ny;
-  const MT m = (MT)v;
-  L0.rhs[q] = m;
-  mg::seed(L0, q, i, j, k, m, tr);
-}
-
 // Right-preconditioned BiCGStab (van der Vorst, SIAM J. Sci. Stat. Comput.
 // 13(2), 1992) for A x = rhs or A^T x = rhs; x holds the start.  The
 // preconditioner is the V-cycle of hs_mg.cuh on the same operator (Gm.L > 0)
@@ -226,7 +209,7 @@ __global__ void __launch_bounds__(kBiT, 1) k_cht_bicgstab(ChtDev H, Vec V, mg::H
                                                         int *out_it, double *out_rel, int rel0, double *out_r0) {
   cg::grid_group grid = cg::this_grid();
   __shared__ double sh[48];
-  const int Nx = H.Nx, Ny = H.Ny, n = Nx * H.Ny * H.Nz;
+  const int Nx = H.Nx, Ny = H.Ny;
   const int PX = Nx + 2, PXY = (Nx + 2) * (Ny + 2);
   const int tid = blockIdx.x * blockDim.x + threadIdx.x, T = gridDim.x * blockDim.x;
   const bool tr = transpose != 0, mgp = Gm.L > 0;
@@ -238,11 +221,12 @@ __global__ void __launch_bounds__(kBiT, 1) k_cht_bicgstab(ChtDev H, Vec V, mg::H
     mg::build(Gm, tr, grid, tid, T);
   }
   double red[2] = {0.0, 0.0};
-  for (int c = tid; c < n; c += T) {
-    const int q = cell_pidx(H, c);
-    const double rv = rhs[q] - apply_any(H, V.x, q, PX, PXY, tr);
+  for (mg::Walk w(Nx, Ny, H.Nz, tid, T); w.ok(); w.next()) {
+    const int q = (w.m + 1) + PX * ((w.j + 1) + (Ny + 2) * (w.k + 1));
+    const double bq = rhs[q];
+    const double rv = bq - apply_any(H, V.x, q, PX, PXY, tr);
     V.r[q] = rv; V.rh[q] = rv; V.p[q] = 0.0; V.v[q] = 0.0;
-    red[0] += rhs[q] * rhs[q];
+    red[0] += bq * bq;
     red[1] += rv * rv;
   }
   grid_sums<2>(red, partials, buf, sh, grid);
@@ -255,39 +239,46 @@ __global__ void __launch_bounds__(kBiT, 1) k_cht_bicgstab(ChtDev H, Vec V, mg::H
   while (it < maxiter && !(rr / bb < eps)) {
     it++;
     const double beta = (rho1 / rho) * (alpha / omega);
-    for (int c = tid; c < n; c += T) {
-      const int q = cell_pidx(H, c);
-      const double pv = V.r[q] + beta * (V.p[q] - omega * V.v[q]);
+    // each pass issues every load of a cell before its first store
+    for (mg::Walk w(Nx, Ny, H.Nz, tid, T); w.ok(); w.next()) {
+      const int q = (w.m + 1) + PX * ((w.j + 1) + (Ny + 2) * (w.k + 1));
+      const double r_ = V.r[q], p_ = V.p[q], v_ = V.v[q];
+      const mg::Seed<MT> sd = mgp ? mg::seed_at(Gm.lv[0], w.m, w.j, w.k, q, tr) : mg::Seed<MT>{};
+      const double di = mgp ? 0.0 : H.dinv[q];
+      const double pv = r_ + beta * (p_ - omega * v_);
       V.p[q] = pv;
-      if (mgp) mg_rhs(H, Gm.lv[0], c, q, pv, tr);
-      else V.ph[q] = pv * H.dinv[q];
+      if (mgp) sd.store(Gm.lv[0], q, pv);
+      else V.ph[q] = pv * di;
     }
     grid.sync();
     if (mgp) mg::vcycle(Gm, tr, grid, tid, T);
     double s2[1] = {0.0};
-    for (int c = tid; c < n; c += T) {
-      const int q = cell_pidx(H, c);
-      double vv;
-      if (mgp) { V.ph[q] = (double)__ldcg(z + q); vv = apply_any(H, z, q, PX, PXY, tr); }
-      else vv = apply_any(H, V.ph, q, PX, PXY, tr);
+    for (mg::Walk w(Nx, Ny, H.Nz, tid, T); w.ok(); w.next()) {
+      const int q = (w.m + 1) + PX * ((w.j + 1) + (Ny + 2) * (w.k + 1));
+      const double rh = V.rh[q];
+      const double vv = mgp ? apply_any(H, z, q, PX, PXY, tr) : apply_any(H, V.ph, q, PX, PXY, tr);
+      if (mgp) V.ph[q] = (double)__ldcg(z + q);
       V.v[q] = vv;
-      s2[0] += V.rh[q] * vv;
+      s2[0] += rh * vv;
     }
     grid_sums<1>(s2, partials, buf, sh, grid);
     alpha = rho1 / s2[0];
     double s3[1] = {0.0};
-    for (int c = tid; c < n; c += T) {
-      const int q = cell_pidx(H, c);
-      const double sv = V.r[q] - alpha * V.v[q];
+    for (mg::Walk w(Nx, Ny, H.Nz, tid, T); w.ok(); w.next()) {
+      const int q = (w.m + 1) + PX * ((w.j + 1) + (Ny + 2) * (w.k + 1));
+      const double r_ = V.r[q], v_ = V.v[q];
+      const mg::Seed<MT> sd = mgp ? mg::seed_at(Gm.lv[0], w.m, w.j, w.k, q, tr) : mg::Seed<MT>{};
+      const double di = mgp ? 0.0 : H.dinv[q];
+      const double sv = r_ - alpha * v_;
       V.s[q] = sv;
-      if (mgp) mg_rhs(H, Gm.lv[0], c, q, sv, tr);
-      else V.sh[q] = sv * H.dinv[q];
+      if (mgp) sd.store(Gm.lv[0], q, sv);
+      else V.sh[q] = sv * di;
       s3[0] += sv * sv;
     }
     grid_sums<1>(s3, partials, buf, sh, grid);
     if (s3[0] / bb < eps) {
-      for (int c = tid; c < n; c += T) {
-        const int q = cell_pidx(H, c);
+      for (mg::Walk w(Nx, Ny, H.Nz, tid, T); w.ok(); w.next()) {
+        const int q = (w.m + 1) + PX * ((w.j + 1) + (Ny + 2) * (w.k + 1));
         V.x[q] += alpha * V.ph[q];
       }
       rr = s3[0];
@@ -295,25 +286,26 @@ __global__ void __launch_bounds__(kBiT, 1) k_cht_bicgstab(ChtDev H, Vec V, mg::H
     }
     if (mgp) mg::vcycle(Gm, tr, grid, tid, T);
     double s4[2] = {0.0, 0.0};
-    for (int c = tid; c < n; c += T) {
-      const int q = cell_pidx(H, c);
-      double tv;
-      if (mgp) { V.sh[q] = (double)__ldcg(z + q); tv = apply_any(H, z, q, PX, PXY, tr); }
-      else tv = apply_any(H, V.sh, q, PX, PXY, tr);
+    for (mg::Walk w(Nx, Ny, H.Nz, tid, T); w.ok(); w.next()) {
+      const int q = (w.m + 1) + PX * ((w.j + 1) + (Ny + 2) * (w.k + 1));
+      const double sq = V.s[q];
+      const double tv = mgp ? apply_any(H, z, q, PX, PXY, tr) : apply_any(H, V.sh, q, PX, PXY, tr);
+      if (mgp) V.sh[q] = (double)__ldcg(z + q);
       V.t[q] = tv;
-      s4[0] += tv * V.s[q];
+      s4[0] += tv * sq;
       s4[1] += tv * tv;
     }
     grid_sums<2>(s4, partials, buf, sh, grid);
     omega = s4[0] / s4[1];
     double s5[2] = {0.0, 0.0};
-    for (int c = tid; c < n; c += T) {
-      const int q = cell_pidx(H, c);
-      V.x[q] += alpha * V.ph[q] + omega * V.sh[q];
-      const double rv = V.s[q] - omega * V.t[q];
+    for (mg::Walk w(Nx, Ny, H.Nz, tid, T); w.ok(); w.next()) {
+      const int q = (w.m + 1) + PX * ((w.j + 1) + (Ny + 2) * (w.k + 1));
+      const double x_ = V.x[q], ph = V.ph[q], sh_ = V.sh[q], s_ = V.s[q], t_ = V.t[q], rh = V.rh[q];
+      V.x[q] = x_ + (alpha * ph + omega * sh_);
+      const double rv = s_ - omega * t_;
       V.r[q] = rv;
       s5[0] += rv * rv;
-      s5[1] += V.rh[q] * rv;
+      s5[1] += rh * rv;
     }
     grid_sums<2>(s5, partials, buf, sh, grid);
     rr = s5[0];
@@ -414,8 +406,8 @@ __global__ void k_cht_velocities(ChtVelSrc S, double *ug, double *vg, double *wg
 
 // T = T + a (x - T) on the interior of padded arrays
 __global__ void k_cht_relax(int n, int Nx, int Ny, double a, const double *x, double *T) {
-  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
-    const int q = (c % Nx + 1) + (Nx + 2) * ((c / Nx) % Ny + 1 + (Ny + 2) * (c / (Nx * Ny) + 1));
+  for (mg::Walk w(Nx, Ny, n / (Nx * Ny), blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x); w.ok(); w.next()) {
+    const int q = (w.m + 1) + (Nx + 2) * ((w.j + 1) + (Ny + 2) * (w.k + 1));
     T[q] = T[q] + a * (x[q] - T[q]);
   }
 }

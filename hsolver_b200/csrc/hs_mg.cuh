@@ -52,6 +52,35 @@ struct Hier {
   double *y;   // kMgCoarse
 };
 
+// Grid-stride walk over an mx x ny x nz box in flat order (m fastest): the
+// cell sequence of `for (e = tid; e < mx*ny*nz; e += T)` without a division
+// per cell.  The start and the stride T are split into (m, j, k) once; each
+// step adds the stride and carries (dm < mx and dj < ny, so one carry per
+// axis suffices).  Needs mx, ny >= 1 and mx*ny*nz + T < 2^31.
+struct Walk {
+  int m, j, k, dm, dj, dk, mx, ny, nz;
+  __host__ __device__ __forceinline__ Walk(int mx_, int ny_, int nz_, int tid, int T) : mx(mx_), ny(ny_), nz(nz_) {
+    const int row = tid / mx, srow = T / mx;
+    m = tid - row * mx;
+    j = row % ny;
+    k = row / ny;
+    dm = T - srow * mx;
+    dj = srow % ny;
+    dk = srow / ny;
+  }
+  __host__ __device__ __forceinline__ bool ok() const { return k < nz; }
+  __host__ __device__ __forceinline__ void next() {
+    m += dm;
+    int c = 0;
+    if (m >= mx) { m -= mx; c = 1; }
+    j += dj + c;
+    c = 0;
+    if (j >= ny) { j -= ny; c = 1; }
+    k += dk + c;
+  }
+  __host__ __device__ __forceinline__ int flat() const { return m + mx * (j + ny * k); }
+};
+
 template <class M>
 __device__ __forceinline__ int idx(const Level<M> &L, int i, int j, int k) {
   return i + (L.nx + 2) * (j + (L.ny + 2) * k);
@@ -165,20 +194,14 @@ __device__ void coarsen(const Level<M> &F, const Level<M> &C, int tid, int T) {
 // non-unknown), so d == 0 identifies it without reading the mask
 template <class M>
 __device__ void smooth(const Level<M> &L, int color, bool tr, int tid, int T) {
-  const int half = (L.nx + 1) / 2;
-  const int n = half * L.ny * L.nz;
-  for (int e = tid; e < n; e += T) {
-    const int row_ = e / half, m = e - row_ * half;
-    const int k = row_ / L.ny, j = row_ - k * L.ny;
-    const int i = 2 * m + ((j + k + color) & 1);
+  for (Walk w((L.nx + 1) / 2, L.ny, L.nz, tid, T); w.ok(); w.next()) {
+    const int j = w.j, k = w.k, i = 2 * w.m + ((j + k + color) & 1);
     if (i >= L.nx) continue;
     const int q = idx(L, i + 1, j + 1, k + 1);
     M d, o[6];
     row(L, q, tr, d, o);
-    if (d == M(0)) { L.x[q] = M(0); continue; }
-    M s = L.rhs[q];
-    s += offsum(L, o, L.x, q);
-    L.x[q] = s / d;
+    const M s = L.rhs[q] + offsum(L, o, L.x, q);
+    L.x[q] = d == M(0) ? M(0) : s / d;
   }
 }
 
@@ -188,29 +211,22 @@ __device__ void smooth(const Level<M> &L, int color, bool tr, int tid, int T) {
 // (padded, any precision; FP64 sums) without a pass of its own.
 template <class M, class RT>
 __device__ void smooth_dot(const Level<M> &L, bool tr, const RT *r, double &acc, int tid, int T) {
-  const int half = (L.nx + 1) / 2;
-  const int n = half * L.ny * L.nz;
-  for (int e = tid; e < n; e += T) {
-    const int row_ = e / half, m = e - row_ * half;
-    const int k = row_ / L.ny, j = row_ - k * L.ny;
-    const int i = 2 * m + ((j + k) & 1), ib = 2 * m + ((j + k + 1) & 1);
-    if (i < L.nx) {
-      const int q = idx(L, i + 1, j + 1, k + 1);
+  for (Walk w((L.nx + 1) / 2, L.ny, L.nz, tid, T); w.ok(); w.next()) {
+    const int j = w.j, k = w.k;
+    const int i = 2 * w.m + ((j + k) & 1), ib = 2 * w.m + ((j + k + 1) & 1);
+    const int q = idx(L, i + 1, j + 1, k + 1), qb = idx(L, ib + 1, j + 1, k + 1);
+    const bool ha = i < L.nx, hb = ib < L.nx;
+    const double rb = hb ? (double)r[qb] : 0.0, xb = hb ? (double)__ldcg(L.x + qb) : 0.0;
+    if (ha) {
+      const double ra = (double)r[q];
       M d, o[6];
       row(L, q, tr, d, o);
-      M xv = M(0);
-      if (d != M(0)) {
-        M s = L.rhs[q];
-        s += offsum(L, o, L.x, q);
-        xv = s / d;
-      }
+      const M s = L.rhs[q] + offsum(L, o, L.x, q);
+      const M xv = d == M(0) ? M(0) : s / d;
       L.x[q] = xv;
-      acc += (double)r[q] * (double)xv;
+      acc += ra * (double)xv;
     }
-    if (ib < L.nx) {
-      const int q = idx(L, ib + 1, j + 1, k + 1);
-      acc += (double)r[q] * (double)__ldcg(L.x + q);
-    }
+    if (hb) acc += rb * xb;
   }
 }
 
@@ -218,12 +234,42 @@ __device__ void smooth_dot(const Level<M> &L, bool tr, const RT *r, double &acc,
 // cells it is local, x = rhs / d: whoever writes a level's rhs applies it to
 // the cell in the same pass (the restriction for the coarse levels, the
 // Krylov solver for level 0), which saves that half-sweep and its barrier.
+// In two halves, so that a pass can issue every load before its first store
+// (a load after a store to another array waits for it: the compiler cannot
+// prove that they do not alias): seed_diag() loads the diagonal of a colour-0
+// cell (0 for colour 1, which is not seeded), seed_store() writes rhs and the
+// seed.
 template <class M>
-__device__ __forceinline__ void seed(const Level<M> &L, int q, int i, int j, int k, M rhs, bool tr) {
-  if ((i + j + k) & 1) return;
+__device__ __forceinline__ M seed_diag(const Level<M> &L, int q, int i, int j, int k, bool tr) {
+  if ((i + j + k) & 1) return M(0);
   M d, o[6];
   row(L, q, tr, d, o);
-  L.x[q] = d == M(0) ? M(0) : rhs / d;
+  return d;
+}
+
+template <class M>
+__device__ __forceinline__ void seed_store(const Level<M> &L, int q, int i, int j, int k, M rhs, M d) {
+  L.rhs[q] = rhs;
+  if (!((i + j + k) & 1)) L.x[q] = d == M(0) ? M(0) : rhs / d;
+}
+
+// both halves for cell (i, j, k) of level L (padded index q):
+// Seed s = seed_at(L, i, j, k, q, tr) with the pass's loads, s.store(L, q, v) last
+template <class M>
+struct Seed {
+  int i, j, k;
+  M d;
+  __device__ __forceinline__ void store(const Level<M> &L, int q, double v) const { seed_store(L, q, i, j, k, (M)v, d); }
+};
+
+template <class M>
+__device__ __forceinline__ Seed<M> seed_at(const Level<M> &L, int i, int j, int k, int q, bool tr) {
+  Seed<M> s;
+  s.i = i;
+  s.j = j;
+  s.k = k;
+  s.d = seed_diag(L, q, i, j, k, tr);
+  return s;
 }
 
 // coarse rhs = sum over the children of (rhs - A x), and the coarse seed.  It follows the
@@ -232,10 +278,8 @@ __device__ __forceinline__ void seed(const Level<M> &L, int q, int i, int j, int
 // are evaluated.
 template <class M>
 __device__ void restrict_res(const Level<M> &F, const Level<M> &C, bool tr, int tid, int T) {
-  const int n = C.nx * C.ny * C.nz;
-  for (int e = tid; e < n; e += T) {
-    const int row_ = e / C.nx, I = e - row_ * C.nx;
-    const int K = row_ / C.ny, J = row_ - K * C.ny;
+  for (Walk w(C.nx, C.ny, C.nz, tid, T); w.ok(); w.next()) {
+    const int I = w.m, J = w.j, K = w.k;
     M acc = M(0);
     for (int dk = 0; dk < 2; ++dk)
       for (int dj = 0; dj < 2; ++dj)
@@ -249,8 +293,7 @@ __device__ void restrict_res(const Level<M> &F, const Level<M> &C, bool tr, int 
         }
     const int qc = idx(C, I + 1, J + 1, K + 1);
     const M v = unknown(C, qc) ? acc : M(0);
-    C.rhs[qc] = v;
-    seed(C, qc, I, J, K, v, tr);
+    seed_store(C, qc, I, J, K, v, seed_diag(C, qc, I, J, K, tr));
   }
 }
 
@@ -263,37 +306,56 @@ __device__ void restrict_res(const Level<M> &F, const Level<M> &C, bool tr, int 
 // zero coupling.  The arithmetic is that of prolongation followed by smooth().
 template <class M>
 __device__ void prolong_smooth(const Level<M> &F, const Level<M> &C, bool tr, int tid, int T) {
-  const int half = (F.nx + 1) / 2;
-  const int n = half * F.ny * F.nz;
   const int PX = F.nx + 2, PXY = (F.nx + 2) * (F.ny + 2);
-  for (int e = tid; e < n; e += T) {
-    const int row_ = e / half, m = e - row_ * half;
-    const int k = row_ / F.ny, j = row_ - k * F.ny;
-    const int i = 2 * m + ((j + k + 1) & 1);
+  const int CPX = C.nx + 2, CPXY = (C.nx + 2) * (C.ny + 2);
+  for (Walk w((F.nx + 1) / 2, F.ny, F.nz, tid, T); w.ok(); w.next()) {
+    const int j = w.j, k = w.k, i = 2 * w.m + ((j + k + 1) & 1);
     if (i >= F.nx) continue;
     const int q = idx(F, i + 1, j + 1, k + 1);
     M d, o[6];
     row(F, q, tr, d, o);
-    if (d == M(0)) { F.x[q] = M(0); continue; }
-    auto xp = [&](int ii, int jj, int kk, int qq) -> M {
-      if (ii < 0 || jj < 0 || kk < 0 || ii >= F.nx || jj >= F.ny || kk >= F.nz) return M(0);
-      return __ldcg(F.x + qq) + __ldcg(C.x + idx(C, ii / 2 + 1, jj / 2 + 1, kk / 2 + 1));
-    };
-    const M off = o[0] * xp(i - 1, j, k, q - 1) + o[1] * xp(i + 1, j, k, q + 1) + o[2] * xp(i, j - 1, k, q - PX) +
-                  o[3] * xp(i, j + 1, k, q + PX) + o[4] * xp(i, j, k - 1, q - PXY) + o[5] * xp(i, j, k + 1, q + PXY);
-    M s = F.rhs[q];
-    s += off;
-    F.x[q] = s / d;
+    // the parent P of this cell is the parent of three of its neighbours; on
+    // each axis the other neighbour's parent is P's neighbour on the side of
+    // this cell's parity (P -+ 1 for an even / odd index)
+    const int qc = idx(C, (i >> 1) + 1, (j >> 1) + 1, (k >> 1) + 1);
+    const M cp = __ldcg(C.x + qc);
+    const M cx = __ldcg(C.x + ((i & 1) ? qc + 1 : qc - 1));
+    const M cy = __ldcg(C.x + ((j & 1) ? qc + CPX : qc - CPX));
+    const M cz = __ldcg(C.x + ((k & 1) ? qc + CPXY : qc - CPXY));
+    // neighbour values x + x_coarse(parent); ghosts stay 0 (never prolonged)
+    const M xw = i > 0 ? __ldcg(F.x + q - 1) + ((i & 1) ? cp : cx) : M(0);
+    const M xe = i + 1 < F.nx ? __ldcg(F.x + q + 1) + ((i & 1) ? cx : cp) : M(0);
+    const M xs = j > 0 ? __ldcg(F.x + q - PX) + ((j & 1) ? cp : cy) : M(0);
+    const M xn = j + 1 < F.ny ? __ldcg(F.x + q + PX) + ((j & 1) ? cy : cp) : M(0);
+    const M xb = k > 0 ? __ldcg(F.x + q - PXY) + ((k & 1) ? cp : cz) : M(0);
+    const M xf = k + 1 < F.nz ? __ldcg(F.x + q + PXY) + ((k & 1) ? cz : cp) : M(0);
+    const M off = o[0] * xw + o[1] * xe + o[2] * xs + o[3] * xn + o[4] * xb + o[5] * xf;
+    const M s = F.rhs[q] + off;
+    F.x[q] = d == M(0) ? M(0) : s / d;
   }
+}
+
+// Block 0's shared-memory copy of the coarsest factors and pivots, written
+// by factor() and read by every coarse_solve() of the same launch (one
+// instance per block: function-scope __shared__ storage is static).
+__device__ __forceinline__ double *lu_smem() {
+  __shared__ double a[kMgCoarse * kMgCoarse];
+  return a;
+}
+__device__ __forceinline__ int *piv_smem() {
+  __shared__ int p[kMgCoarse];
+  return p;
 }
 
 // LU with partial pivoting of the coarsest operator (A or A^T), by block 0,
 // in shared memory; the pivot is the largest |a| in the column, the lowest
-// row among equals; the factors are copied to G.lu for coarse_solve
+// row among equals; the factors stay in shared memory for coarse_solve and
+// are also copied to G.lu / G.piv
 template <class M>
 __device__ void factor(const Hier<M> &G, bool tr) {
   if (blockIdx.x != 0) return;
-  __shared__ double a[kMgCoarse * kMgCoarse];
+  double *a = lu_smem();
+  int *sp = piv_smem();
   __shared__ int spiv;
   const Level<M> &C = G.lv[G.L - 1];
   const int nc = C.nx * C.ny * C.nz, PX = C.nx + 2, PXY = (C.nx + 2) * (C.ny + 2);
@@ -334,7 +396,7 @@ __device__ void factor(const Hier<M> &G, bool tr) {
         const int orow = __shfl_xor_sync(0xffffffffu, br, o);
         if (ov > bv || (ov == bv && orow < br)) { bv = ov; br = orow; }
       }
-      if (threadIdx.x == 0) { spiv = br; G.piv[col] = br; }
+      if (threadIdx.x == 0) { spiv = br; sp[col] = br; G.piv[col] = br; }
     }
     __syncthreads();
     const int pr = spiv;
@@ -358,34 +420,38 @@ __device__ void factor(const Hier<M> &G, bool tr) {
   for (int e = threadIdx.x; e < nc * nc; e += blockDim.x) G.lu[e] = a[e];
 }
 
-// exact solve on the coarsest level, by warp 0 of block 0 (the permuted
-// right-hand side in shared memory, triangular solves with warp dot products)
+// exact solve on the coarsest level, by warp 0 of block 0, from the factors
+// in shared memory: the right-hand side gathered by every lane, permuted by
+// lane 0, then the triangular solves with warp dot products
 template <class M>
 __device__ void coarse_solve(const Hier<M> &G) {
   if (threadIdx.x >= 32) return;
   __shared__ double y[kMgCoarse];
+  const double *lu = lu_smem();
+  const int *sp = piv_smem();
   const Level<M> &C = G.lv[G.L - 1];
   const int nc = C.nx * C.ny * C.nz, lane = threadIdx.x;
-  if (lane == 0) {
-    for (int r = 0; r < nc; ++r) y[r] = (double)C.rhs[idx(C, r % C.nx + 1, (r / C.nx) % C.ny + 1, r / (C.nx * C.ny) + 1)];
+  for (int r = lane; r < nc; r += 32)
+    y[r] = (double)C.rhs[idx(C, r % C.nx + 1, (r / C.nx) % C.ny + 1, r / (C.nx * C.ny) + 1)];
+  __syncwarp();
+  if (lane == 0)
     for (int c2 = 0; c2 < nc; ++c2) {
-      const int pr = G.piv[c2];
+      const int pr = sp[c2];
       if (pr != c2) { const double t = y[c2]; y[c2] = y[pr]; y[pr] = t; }
     }
-  }
   __syncwarp();
   for (int r = 0; r < nc; ++r) {
     double a = 0.0;
-    for (int c2 = lane; c2 < r; c2 += 32) a += G.lu[r * nc + c2] * y[c2];
+    for (int c2 = lane; c2 < r; c2 += 32) a += lu[r * nc + c2] * y[c2];
     for (int o = 16; o; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
     if (lane == 0) y[r] -= a;
     __syncwarp();
   }
   for (int r = nc - 1; r >= 0; --r) {
     double a = 0.0;
-    for (int c2 = r + 1 + lane; c2 < nc; c2 += 32) a += G.lu[r * nc + c2] * y[c2];
+    for (int c2 = r + 1 + lane; c2 < nc; c2 += 32) a += lu[r * nc + c2] * y[c2];
     for (int o = 16; o; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
-    if (lane == 0) y[r] = (y[r] - a) / G.lu[r * nc + r];
+    if (lane == 0) y[r] = (y[r] - a) / lu[r * nc + r];
     __syncwarp();
   }
   for (int r = lane; r < nc; r += 32) {
@@ -415,7 +481,7 @@ __device__ void build(const Hier<M> &G, bool tr, cg::grid_group &grid, int tid, 
 }
 
 // lv[0].x = V-cycle applied to lv[0].rhs; the caller has written lv[0].rhs
-// and seeded lv[0] (seed() on every interior cell) before the barrier that
+// and seeded lv[0] (seed_diag / seed_store on every interior cell) before the barrier that
 // precedes this call.  With dot_r, the last level-0 pass also adds this
 // thread's share of sum dot_r x to *dot_acc and the final barrier is left to
 // the caller's reduction (returns true); it returns false, with the barrier
