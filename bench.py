@@ -42,15 +42,20 @@ UNIT = "iter/s"
 PEAKS_FILE = os.path.join(HERE, "MEASURED_PEAKS.json")
 FALLBACK_HBM_GBS = 6650.0
 NAME = "config2"
-# inner tolerances of the at-scale case (config 1 keeps the library defaults,
-# p' rtol 1e-8 as its specification states)
-SOLVER = {"p_tol": 1e-5, "t_tol": 0.5}
+# inner solves of the at-scale case (config 1 keeps the library defaults,
+# p' rtol 1e-8 as its specification states): p' to rtol 1e-5, and one
+# BiCGStab iteration (two V-cycles) of the energy per outer step.  Neither
+# changes the number of outer steps to a global residual of 1e-6 on this case
+# (1393 for p' rtol 1e-8 to 1e-3 and for an energy solve to 1e-2 per step):
+# SIMPLE's rate is set by the relaxation, and the energy residual stays an
+# order below the momentum residuals.
+SOLVER = {"p_tol": 1e-5, "t_tol": 0.5, "t_maxiter": 1}
 CONFIG = {"workload": "channel 256x128x128 (4.19M cells), 8 seeded heated blocks (edges 8-24, q U[0.5,2], "
                       "k_s/k_f U[10,1000]), Re 400, SIMPLE-CHT outer step",
           "grid": [256, 128, 128], "blocks": 8, "seed": 0, "precision": "fp64", "re": 400, "pr": 0.71,
           "relaxation": {"u": 0.7, "p": 0.3, "T": 0.9}, "momentum": "FOU, 2 red-black GS sweeps",
           "pressure_solver": "CG + multigrid V-cycle (FP64), rtol 1e-5 (the reference's HYPRE setting)",
-          "energy_solver": "BiCGStab + multigrid V-cycle (FP64), 0.5 of the initial residual per step",
+          "energy_solver": "BiCGStab + multigrid V-cycle (FP64), one iteration per outer step",
           "l2_policy": "state ~790 MB on the device, larger than L2 (126 MB)", "parallelism": "replicas"}
 # launches per outer step: 4 momentum passes, p' assembly, residual finalize,
 # p' solve, correction, energy assembly, energy BiCGStab, energy relaxation
@@ -398,7 +403,7 @@ def reference_physics(args, torch, hsolver_b200, local, dist):
             "value": args.steps / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms / args.steps}
 
 
-CPU_SAMPLE_P, CPU_SAMPLE_T = 20, 2
+CPU_SAMPLE_P, CPU_SAMPLE_T = 20, 1
 
 
 def cpu_threads():
@@ -410,11 +415,11 @@ def cpu_threads():
 
 def cpu_sample():
     """The FP64 C oracle (OpenMP on all host threads) on one outer step of the
-    same case, after init, with the inner solves capped (CG 20, BiCGStab 2
-    iterations)."""
+    same case, after init, with the inner solves capped (CG 20, BiCGStab 1
+    iteration)."""
     from oracle import oracle
     deck, re_, k, q, _ = workload()
-    o = oracle.ChannelCase(deck, re=re_, p_maxiter=CPU_SAMPLE_P, t_maxiter=CPU_SAMPLE_T, **SOLVER)
+    o = oracle.ChannelCase(deck, re=re_, **dict(SOLVER, p_maxiter=CPU_SAMPLE_P, t_maxiter=CPU_SAMPLE_T))
     o.set_solid(k, q)
     o.init()
     t0 = time.perf_counter()
@@ -427,7 +432,7 @@ def cpu_baseline():
     return {"value": 1.0 / dt, "unit": UNIT, "cores": cpu_threads(), "kind": "port",
             "sample": "1 outer step of the bench case by the FP64 C oracle (OpenMP, %d threads) with the inner "
                       "solves capped at %d CG and %d BiCGStab iterations (unpreconditioned; reaching the GPU's "
-                      "tolerances takes ~1000 and ~200), %.1f s: an upper bound on the CPU rate"
+                      "p' tolerance takes ~1000 CG iterations), %.1f s: an upper bound on the CPU rate"
                       % (cpu_threads(), CPU_SAMPLE_P, CPU_SAMPLE_T, dt)}
 
 

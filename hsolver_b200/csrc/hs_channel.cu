@@ -487,9 +487,10 @@ __global__ void k_ch_init(ChDev<R> H) {
 // ghost cell N0 + 1 is the outlet face, neighbour value 0).  Preconditioner:
 // the V-cycle of hs_mg.cuh in precision M on the same couplings (no
 // convection), solid cells masked.
-// p' system and CG vectors, stored in V (FP64 form: double; mixed form: float,
-// with FP64 arithmetic per element and FP64 dot products: p' is a correction
-// that vanishes at the fixed point, whose residuals are all FP64)
+// p' system and CG vectors, stored in V (FP64 form: double; mixed form:
+// float, with the search-direction update in FP32 and the product, the x and r
+// updates and the dot products in FP64: p' is a correction that vanishes at
+// the fixed point, whose residuals are all FP64)
 template <class V>
 struct CgVec {
   int N0, N1, N2;
@@ -527,15 +528,19 @@ __device__ __forceinline__ int cell_q(int e, int N0, int N1) {
 // blocks, a third of the arrivals at every grid barrier
 constexpr int kPcgT = 768;
 
+// level 0 of the V-cycle: its couplings are the CG's own arrays (the same
+// pointers); the mask, and the diagonal of every interior row for the seeds
 template <class M>
 __device__ void mg_fine_from_couplings(const CgVec<M> &V, const mg::Level<M> &L0, int tid, int T) {
   const int PX = V.N0 + 2, PY = V.N1 + 2;
   const long long np = (long long)PX * PY * (V.N2 + 2);
   for (long long q = tid; q < np; q += T) {
-    L0.gx[q] = (M)V.acx[q]; L0.gy[q] = (M)V.acy[q]; L0.gz[q] = (M)V.acz[q];
     const int i = (int)(q % PX) - 1, j = (int)((q / PX) % PY) - 1, k = (int)(q / ((long long)PX * PY)) - 1;
     const bool in = i >= 0 && j >= 0 && k >= 0 && i < V.N0 && j < V.N1 && k < V.N2;
     L0.m[q] = in && !V.solid[i + V.N0 * (j + V.N1 * k)];
+    M d = M(0), o[6];
+    if (in) mg::row(L0, (int)q, false, d, o);
+    L0.d[q] = d;
   }
 }
 
@@ -589,20 +594,23 @@ __global__ void __launch_bounds__(kPcgT, 1) k_ch_pcg(CgVec<M> V, mg::Hier<M> G, 
     const bool first = it == 0;
     it++;
     acc = 0.0;
-    auto pval = [&](int qq) {
-      const double z = precond ? (double)__ldcg(L0.x + qq) : (double)__ldcg(V.r + qq);
-      return (double)(M)(first ? z : z + beta * (double)__ldcg(po + qq));  // as stored
+    const M bm = (M)beta;
+    auto pval = [&](int qq) -> M {
+      const M z = precond ? __ldcg(L0.x + qq) : __ldcg(V.r + qq);
+      return first ? z : z + bm * __ldcg(po + qq);
     };
+    // p in storage precision; the product in FP64 (in FP32 its cancellation
+    // error for smooth p would reach the near-null modes of the p' system)
     for (mg::Walk w(N0, N1, V.N2, tid, T); w.ok(); w.next()) {
       const int q = (w.m + 1) + PX * ((w.j + 1) + PY * (w.k + 1));
-      const double p0 = pval(q);
+      const M p0 = pval(q);
       const double cw = V.acx[q], ce = V.acx[q + 1], cs = V.acy[q], cn = V.acy[q + PX], cb = V.acz[q], cf = V.acz[q + PXY];
       const double d = cw + ce + cs + cn + cb + cf;
-      const double sv = d * p0 - (cw * pval(q - 1) + ce * pval(q + 1) + cs * pval(q - PX) + cn * pval(q + PX) +
-                                  cb * pval(q - PXY) + cf * pval(q + PXY));
-      pn[q] = (M)p0;
+      const double sv = d * (double)p0 - (cw * (double)pval(q - 1) + ce * (double)pval(q + 1) + cs * (double)pval(q - PX) +
+                                          cn * (double)pval(q + PX) + cb * (double)pval(q - PXY) + cf * (double)pval(q + PXY));
+      pn[q] = p0;
       V.s[q] = (M)sv;
-      acc += (double)(M)sv * p0;
+      acc += (double)(M)sv * (double)p0;
     }
     const double sp = grid_sum(acc, partials, buf, sh, grid);
     if (sp == 0.0) break;
@@ -613,9 +621,9 @@ __global__ void __launch_bounds__(kPcgT, 1) k_ch_pcg(CgVec<M> V, mg::Hier<M> G, 
       const double xv = (double)V.x[q], pv = (double)pn[q], r0 = (double)V.r[q], sv = (double)V.s[q];
       const mg::Seed<M> sd = precond ? mg::seed_at(L0, w.m, w.j, w.k, q, false) : mg::Seed<M>{};
       V.x[q] = (M)(xv + alpha * pv);
-      const double rv = (double)(M)(r0 - alpha * sv);
-      V.r[q] = (M)rv;
-      acc += rv * rv;
+      const M rv = (M)(r0 - alpha * sv);
+      V.r[q] = rv;
+      acc += (double)rv * (double)rv;
       if (precond) sd.store(L0, q, rv);
     }
     rr = grid_sum(acc, partials, buf, sh, grid);
@@ -758,7 +766,7 @@ void setup_cg(ChannelState &S, CgVec<R> &V, const uint8_t *solid, size_t np) {
 }
 
 template <class M>
-void setup_mg(ChannelState &S, mg::Hier<M> &G) {
+void setup_mg(ChannelState &S, mg::Hier<M> &G, const CgVec<M> &V) {
   int nx = S.N0, ny = S.N1, nz = S.N2, L = 0;
   while (true) {
     if (L >= mg::kMgMaxLv) throw std::runtime_error("multigrid: too many levels");
@@ -766,7 +774,13 @@ void setup_mg(ChannelState &S, mg::Hier<M> &G) {
     l.nx = nx; l.ny = ny; l.nz = nz;
     const size_t np = (size_t)(nx + 2) * (ny + 2) * (nz + 2);
     l.x = S.alloc<M>(np); l.rhs = S.alloc<M>(np);
-    l.gx = S.alloc<M>(np); l.gy = S.alloc<M>(np); l.gz = S.alloc<M>(np);
+    if (L == 0) {  // the p' couplings themselves (written by the assembly, read-only in the solve)
+      l.gx = const_cast<M *>(V.acx); l.gy = const_cast<M *>(V.acy); l.gz = const_cast<M *>(V.acz);
+      l.d = S.alloc<M>(np);
+    } else {
+      l.gx = S.alloc<M>(np); l.gy = S.alloc<M>(np); l.gz = S.alloc<M>(np);
+      l.d = nullptr;
+    }
     l.fx = l.fy = l.fz = nullptr;
     l.m = S.alloc<uint8_t>(np);
     ++L;
@@ -907,8 +921,8 @@ ChannelState *ch_create(const Case &c, const ChParams &p, int device) {
   if (S->mixed) setup_cg(*S, S->Vf, solid, np);
   else setup_cg(*S, S->Vd, solid, np);
   S->scratch = S->alloc<double>(np);
-  if (S->mixed) setup_mg(*S, S->Gf);
-  else setup_mg(*S, S->Gd);
+  if (S->mixed) setup_mg(*S, S->Gf, S->Vf);
+  else setup_mg(*S, S->Gd, S->Vd);
   S->mom_blocks = blocks_for((long long)(S->N0 + 1) * (S->N1 + 1) * (S->N2 + 1));
   S->mom_part = S->alloc<double>((size_t)3 * S->mom_blocks);
   S->cont_part = S->alloc<double>((size_t)S->mom_blocks);

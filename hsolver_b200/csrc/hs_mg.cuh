@@ -41,6 +41,7 @@ struct Level {
   M *gx, *gy, *gz;
   M *fx, *fy, *fz;  // null: pure diffusion
   uint8_t *m;       // null: every interior cell is an unknown
+  M *d;             // null, or the diagonal of every row (read by seed_diag)
 };
 
 template <class M>
@@ -242,6 +243,7 @@ __device__ void smooth_dot(const Level<M> &L, bool tr, const RT *r, double &acc,
 template <class M>
 __device__ __forceinline__ M seed_diag(const Level<M> &L, int q, int i, int j, int k, bool tr) {
   if ((i + j + k) & 1) return M(0);
+  if (L.d) return L.d[q];
   M d, o[6];
   row(L, q, tr, d, o);
   return d;
@@ -259,7 +261,8 @@ template <class M>
 struct Seed {
   int i, j, k;
   M d;
-  __device__ __forceinline__ void store(const Level<M> &L, int q, double v) const { seed_store(L, q, i, j, k, (M)v, d); }
+  template <class V>
+  __device__ __forceinline__ void store(const Level<M> &L, int q, V v) const { seed_store(L, q, i, j, k, (M)v, d); }
 };
 
 template <class M>
@@ -275,25 +278,64 @@ __device__ __forceinline__ Seed<M> seed_at(const Level<M> &L, int i, int j, int 
 // coarse rhs = sum over the children of (rhs - A x), and the coarse seed.  It follows the
 // colour-1 half-sweep, after which a colour-1 cell's residual is zero up to
 // rounding (its update solved its own row), so only the colour-0 children
-// are evaluated.
+// are evaluated, in (dk, dj) order.  Large levels: a thread per coarse cell.
+// Levels whose children all fit in one pass of the threads: four lanes per
+// coarse cell, lane c of a group evaluating the colour-0 child of (dj, dk) =
+// (c & 1, c >> 1) (di = (dj + dk) & 1) and the group's first lane summing
+// them in the same order, so that one memory round trip replaces four
+// (every lane of a warp runs the same number of iterations: the shuffles
+// need the full warp).
 template <class M>
 __device__ void restrict_res(const Level<M> &F, const Level<M> &C, bool tr, int tid, int T) {
-  for (Walk w(C.nx, C.ny, C.nz, tid, T); w.ok(); w.next()) {
+  if (4LL * C.nx * C.ny * C.nz > T) {
+    for (Walk w(C.nx, C.ny, C.nz, tid, T); w.ok(); w.next()) {
+      const int I = w.m, J = w.j, K = w.k;
+      M acc = M(0);
+      for (int dk = 0; dk < 2; ++dk)
+        for (int dj = 0; dj < 2; ++dj)
+          for (int di = 0; di < 2; ++di) {
+            const int i = 2 * I + di, j = 2 * J + dj, k = 2 * K + dk;
+            if (i >= F.nx || j >= F.ny || k >= F.nz || ((i + j + k) & 1)) continue;
+            const int q = idx(F, i + 1, j + 1, k + 1);
+            M d, o[6];
+            row(F, q, tr, d, o);
+            acc += F.rhs[q] - (d * __ldcg(F.x + q) - offsum(F, o, F.x, q));
+          }
+      const int qc = idx(C, I + 1, J + 1, K + 1);
+      const M v = unknown(C, qc) ? acc : M(0);
+      seed_store(C, qc, I, J, K, v, seed_diag(C, qc, I, J, K, tr));
+    }
+    return;
+  }
+  const int c = tid & 3, dj = c & 1, dk = c >> 1, di = (dj + dk) & 1;
+  const int g0 = (threadIdx.x & 31) & ~3;
+  for (Walk w(C.nx, C.ny, C.nz, tid >> 2, T >> 2); __any_sync(0xffffffffu, w.ok()); w.next()) {
+    const bool live = w.ok();
     const int I = w.m, J = w.j, K = w.k;
-    M acc = M(0);
-    for (int dk = 0; dk < 2; ++dk)
-      for (int dj = 0; dj < 2; ++dj)
-        for (int di = 0; di < 2; ++di) {
-          const int i = 2 * I + di, j = 2 * J + dj, k = 2 * K + dk;
-          if (i >= F.nx || j >= F.ny || k >= F.nz || ((i + j + k) & 1)) continue;
-          const int q = idx(F, i + 1, j + 1, k + 1);
-          M d, o[6];
-          row(F, q, tr, d, o);
-          acc += F.rhs[q] - (d * __ldcg(F.x + q) - offsum(F, o, F.x, q));
-        }
-    const int qc = idx(C, I + 1, J + 1, K + 1);
-    const M v = unknown(C, qc) ? acc : M(0);
-    seed_store(C, qc, I, J, K, v, seed_diag(C, qc, I, J, K, tr));
+    const int i = 2 * I + di, j = 2 * J + dj, k = 2 * K + dk;
+    const bool has = live && i < F.nx && j < F.ny && k < F.nz;
+    const bool lead = live && c == 0;
+    const int qc = lead ? idx(C, I + 1, J + 1, K + 1) : 0;
+    const M dc = lead ? seed_diag(C, qc, I, J, K, tr) : M(0);
+    const bool uc = lead && unknown(C, qc);
+    M v = M(0);
+    if (has) {
+      const int q = idx(F, i + 1, j + 1, k + 1);
+      M d, o[6];
+      row(F, q, tr, d, o);
+      v = F.rhs[q] - (d * __ldcg(F.x + q) - offsum(F, o, F.x, q));
+    }
+    const M v1 = __shfl_sync(0xffffffffu, v, g0 + 1), v2 = __shfl_sync(0xffffffffu, v, g0 + 2),
+            v3 = __shfl_sync(0xffffffffu, v, g0 + 3);
+    const unsigned hm = __ballot_sync(0xffffffffu, has) >> g0;
+    if (lead) {
+      M acc = M(0);
+      if (hm & 1u) acc += v;
+      if (hm & 2u) acc += v1;
+      if (hm & 4u) acc += v2;
+      if (hm & 8u) acc += v3;
+      seed_store(C, qc, I, J, K, uc ? acc : M(0), dc);
+    }
   }
 }
 
@@ -335,9 +377,10 @@ __device__ void prolong_smooth(const Level<M> &F, const Level<M> &C, bool tr, in
   }
 }
 
-// Block 0's shared-memory copy of the coarsest factors and pivots, written
-// by factor() and read by every coarse_solve() of the same launch (one
-// instance per block: function-scope __shared__ storage is static).
+// Block 0's shared memory for the coarsest operator: the LU factors during
+// factor(), then the explicit inverse read by every coarse_solve() of the
+// same launch; and the pivots (one instance per block: function-scope
+// __shared__ storage is static).
 __device__ __forceinline__ double *lu_smem() {
   __shared__ double a[kMgCoarse * kMgCoarse];
   return a;
@@ -349,8 +392,8 @@ __device__ __forceinline__ int *piv_smem() {
 
 // LU with partial pivoting of the coarsest operator (A or A^T), by block 0,
 // in shared memory; the pivot is the largest |a| in the column, the lowest
-// row among equals; the factors stay in shared memory for coarse_solve and
-// are also copied to G.lu / G.piv
+// row among equals; the factors are copied to G.lu / G.piv and the explicit
+// inverse is left in shared memory for coarse_solve
 template <class M>
 __device__ void factor(const Hier<M> &G, bool tr) {
   if (blockIdx.x != 0) return;
@@ -418,45 +461,48 @@ __device__ void factor(const Hier<M> &G, bool tr) {
     __syncthreads();
   }
   for (int e = threadIdx.x; e < nc * nc; e += blockDim.x) G.lu[e] = a[e];
-}
-
-// exact solve on the coarsest level, by warp 0 of block 0, from the factors
-// in shared memory: the right-hand side gathered by every lane, permuted by
-// lane 0, then the triangular solves with warp dot products
-template <class M>
-__device__ void coarse_solve(const Hier<M> &G) {
-  if (threadIdx.x >= 32) return;
-  __shared__ double y[kMgCoarse];
-  const double *lu = lu_smem();
-  const int *sp = piv_smem();
-  const Level<M> &C = G.lv[G.L - 1];
-  const int nc = C.nx * C.ny * C.nz, lane = threadIdx.x;
-  for (int r = lane; r < nc; r += 32)
-    y[r] = (double)C.rhs[idx(C, r % C.nx + 1, (r / C.nx) % C.ny + 1, r / (C.nx * C.ny) + 1)];
-  __syncwarp();
-  if (lane == 0)
+  __syncthreads();
+  // explicit inverse from the factors (A = P^T L U): thread j solves
+  // A x = e_j and stores x as column j, at a[j * nc + r], over the factors
+  // (read back from G.lu)
+  if (threadIdx.x < nc) {
+    const int j = threadIdx.x;
+    double *x = a + j * nc;
+    int pos = j;  // where the swaps move the 1 of e_j
     for (int c2 = 0; c2 < nc; ++c2) {
       const int pr = sp[c2];
-      if (pr != c2) { const double t = y[c2]; y[c2] = y[pr]; y[pr] = t; }
+      if (pos == c2) pos = pr;
+      else if (pos == pr) pos = c2;
     }
-  __syncwarp();
-  for (int r = 0; r < nc; ++r) {
-    double a = 0.0;
-    for (int c2 = lane; c2 < r; c2 += 32) a += lu[r * nc + c2] * y[c2];
-    for (int o = 16; o; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
-    if (lane == 0) y[r] -= a;
-    __syncwarp();
+    for (int r = 0; r < nc; ++r) {
+      double v = r == pos ? 1.0 : 0.0;
+      for (int c2 = 0; c2 < r; ++c2) v -= G.lu[r * nc + c2] * x[c2];
+      x[r] = v;
+    }
+    for (int r = nc - 1; r >= 0; --r) {
+      double v = x[r];
+      for (int c2 = r + 1; c2 < nc; ++c2) v -= G.lu[r * nc + c2] * x[c2];
+      x[r] = v / G.lu[r * nc + r];
+    }
   }
-  for (int r = nc - 1; r >= 0; --r) {
-    double a = 0.0;
-    for (int c2 = r + 1 + lane; c2 < nc; c2 += 32) a += lu[r * nc + c2] * y[c2];
-    for (int o = 16; o; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
-    if (lane == 0) y[r] = (y[r] - a) / lu[r * nc + r];
-    __syncwarp();
-  }
-  for (int r = lane; r < nc; r += 32) {
-    const int q = idx(C, r % C.nx + 1, (r / C.nx) % C.ny + 1, r / (C.nx * C.ny) + 1);
-    C.x[q] = unknown(C, q) ? (M)y[r] : M(0);
+}
+
+// exact solve on the coarsest level by block 0 (every thread of the block
+// calls it): x = A^-1 rhs with the inverse that factor() left in shared
+// memory, thread r summing row r in column order
+template <class M>
+__device__ void coarse_solve(const Hier<M> &G) {
+  __shared__ double y[kMgCoarse];
+  const double *ainv = lu_smem();
+  const Level<M> &C = G.lv[G.L - 1];
+  const int nc = C.nx * C.ny * C.nz, r = threadIdx.x;
+  const int q = r < nc ? idx(C, r % C.nx + 1, (r / C.nx) % C.ny + 1, r / (C.nx * C.ny) + 1) : 0;
+  if (r < nc) y[r] = (double)C.rhs[q];
+  __syncthreads();
+  if (r < nc) {
+    double v = 0.0;
+    for (int c2 = 0; c2 < nc; ++c2) v += ainv[c2 * nc + r] * y[c2];
+    C.x[q] = unknown(C, q) ? (M)v : M(0);
   }
 }
 
