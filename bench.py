@@ -54,9 +54,12 @@ CONFIG = {"workload": "channel 256x128x128 (4.19M cells), 8 seeded heated blocks
                       "k_s/k_f U[10,1000]), Re 400, SIMPLE-CHT outer step",
           "grid": [256, 128, 128], "blocks": 8, "seed": 0, "precision": "fp64", "re": 400, "pr": 0.71,
           "relaxation": {"u": 0.7, "p": 0.3, "T": 0.9}, "momentum": "FOU, 2 red-black GS sweeps",
-          "pressure_solver": "CG + multigrid V-cycle (FP64), rtol 1e-5 (the reference's HYPRE setting)",
+          "pressure_solver": "CG + multigrid V(2,2)-cycle (FP64), rtol 1e-5 (the reference's HYPRE setting)",
           "energy_solver": "BiCGStab + multigrid V-cycle (FP64), one iteration per outer step",
           "l2_policy": "state ~790 MB on the device, larger than L2 (126 MB)", "parallelism": "replicas"}
+# red-black sweeps before and after each coarse correction of the p' V-cycle
+# (the library default, hs_channel_params.p_mg_sweeps = 0)
+MG_SWEEPS = 2
 # launches per outer step: 4 momentum passes, p' assembly, residual finalize,
 # p' solve, correction, energy assembly, energy BiCGStab, energy relaxation
 LAUNCHES_PER_STEP = 11
@@ -126,19 +129,26 @@ class ClockSampler:
                 "samples": len(self.samples)}
 
 
-def pcg_bytes(ncell, iters, wbytes=8):
-    """Compulsory HBM bytes of one pressure-correction launch (k_ch_pcg) in
-    the FP64 form, per cell: setup (level 0 from the couplings 24 + mask 1,
-    written in V-cycle precision 3w + 1; r, x 16) plus per iteration the CG
-    part (s = A p: p, 3 couplings, mask, s -> 41 B; x, r update and the
-    V-cycle rhs: 32 + 16 + w; <r, z>: 8 + w; p = z + beta p: 8 + w + 8 + 8)
-    and one V-cycle on level 0 (4 smoothing passes of 3 couplings, rhs, mask,
-    x in and out -> 4 (5w + 1); the residual restriction 5w + 1; the
-    prolongation 2w) with the coarser levels adding 1/7."""
+def pcg_bytes(ncell, iters, wbytes=8, sweeps=MG_SWEEPS):
+    """Compulsory HBM bytes of one pressure-correction launch (k_ch_pcg), per
+    cell, with w bytes per stored value (8 in the FP64 form): each array once
+    per pass.
+      setup: couplings 3w and the solid mask 1 read, level-0 mask 1 and
+        diagonal w written; r w read, V-cycle rhs and seed 2w written;
+      per CG iteration:
+        s = A p with p = z + beta p: z, p_old, 3 couplings read, p, s written
+          -> 7w;
+        x, r update with the next V-cycle rhs and seed: x, p, r, s, diagonal
+          read, x, r, rhs, seed written -> 9w;
+        <r, z> in the V-cycle's last pass: r -> w;
+        one V-cycle on level 0: 3 + 4 (sweeps - 1) standalone red-black
+          half-sweeps of 5w (3 couplings, rhs, x read; x written), the
+          restriction 5w + 2w/8 and the coarse values of the prolongation
+          w/8; the coarser levels add 1/7 of that."""
     w = wbytes
-    setup = 24 + 1 + 3 * w + 1 + 16
-    cg = 41 + (48 + w) + (8 + w) + (24 + w)
-    vc = (4 * (5 * w + 1) + (5 * w + 1) + 2 * w) * 8.0 / 7.0
+    setup = 3 * w + 1 + 1 + w + w + 2 * w
+    cg = 7 * w + 9 * w + w
+    vc = ((3 + 4 * (sweeps - 1)) * 5 * w + 5 * w + 0.25 * w + 0.125 * w) * 8.0 / 7.0
     return ncell * (setup + iters * (cg + vc))
 
 

@@ -19,6 +19,7 @@ struct ChParams {
   int t_maxiter;
   int precision;                    // 0 FP64, 1 mixed (FP32 fields, sweeps and V-cycle)
   int p_precond;                    // 0 plain CG, 1 multigrid V-cycle
+  int p_mg_sweeps;                  // V-cycle sweeps before / after the coarse correction (0: 2)
 };
 
 struct ChStats {

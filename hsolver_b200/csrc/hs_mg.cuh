@@ -16,8 +16,9 @@
 // any child is; coarse face g = (sum of the 2x2 fine g) / 2 (the patch area is
 // 4x, the spacing 2x), coarse flux = sum of the fine fluxes (conservative);
 // down to <= kMgCoarse cells, where an LU with partial pivoting (FP64, on the
-// GPU) solves exactly.  Smoother: red-black Gauss-Seidel, one sweep before
-// (red, black) and one after (black, red); the first red half-sweep (from
+// GPU) solves exactly.  Smoother: red-black Gauss-Seidel, G.nsw sweeps
+// before (red, black, ...) and after (black, red, ...), mirrored so that the
+// cycle stays symmetric for CG; the first red half-sweep (from
 // x = 0) is applied by whoever writes the level's rhs, the prolongation is
 // fused into the first post-smoothing half-sweep.  Levels below kMgSmall cells run inside
 // block 0 alone, separated by __syncthreads instead of grid barriers.
@@ -47,6 +48,7 @@ struct Level {
 template <class M>
 struct Hier {
   int L;
+  int nsw;  // red-black sweeps before and after each coarse correction (0 or 1: one)
   Level<M> lv[kMgMaxLv];
   double *lu;  // kMgCoarse^2
   int *piv;    // kMgCoarse
@@ -540,6 +542,12 @@ __device__ bool vcycle(const Hier<M> &G, bool tr, cg::grid_group &grid, int tid,
   for (int l = 0; l < ls; ++l) {
     smooth(G.lv[l], 1, tr, tid, T);
     grid.sync();
+    for (int s = 1; s < G.nsw; ++s) {
+      smooth(G.lv[l], 0, tr, tid, T);
+      grid.sync();
+      smooth(G.lv[l], 1, tr, tid, T);
+      grid.sync();
+    }
     restrict_res(G.lv[l], G.lv[l + 1], tr, tid, T);
     grid.sync();
   }
@@ -548,6 +556,12 @@ __device__ bool vcycle(const Hier<M> &G, bool tr, cg::grid_group &grid, int tid,
     for (int l = ls; l < G.L - 1; ++l) {
       smooth(G.lv[l], 1, tr, t, B);
       __syncthreads();
+      for (int s = 1; s < G.nsw; ++s) {
+        smooth(G.lv[l], 0, tr, t, B);
+        __syncthreads();
+        smooth(G.lv[l], 1, tr, t, B);
+        __syncthreads();
+      }
       restrict_res(G.lv[l], G.lv[l + 1], tr, t, B);
       __syncthreads();
     }
@@ -558,12 +572,24 @@ __device__ bool vcycle(const Hier<M> &G, bool tr, cg::grid_group &grid, int tid,
       __syncthreads();
       smooth(G.lv[l], 0, tr, t, B);
       __syncthreads();
+      for (int s = 1; s < G.nsw; ++s) {
+        smooth(G.lv[l], 1, tr, t, B);
+        __syncthreads();
+        smooth(G.lv[l], 0, tr, t, B);
+        __syncthreads();
+      }
     }
   }
   grid.sync();
   for (int l = ls - 1; l >= 0; --l) {
     prolong_smooth(G.lv[l], G.lv[l + 1], tr, tid, T);
     grid.sync();
+    for (int s = 1; s < G.nsw; ++s) {
+      smooth(G.lv[l], 0, tr, tid, T);
+      grid.sync();
+      smooth(G.lv[l], 1, tr, tid, T);
+      grid.sync();
+    }
     if (l == 0 && dot_r) {
       smooth_dot(G.lv[0], tr, dot_r, *dot_acc, tid, T);
       return true;

@@ -130,10 +130,13 @@ def test_adjoint_at_config4_vs_central_differences():
     """The adjoint configuration: 128x64x64 channel, 4 seeded blocks, the
     FP64 flow converged to a global residual of 1e-6 and frozen; dJ/dq along
     16 seeded directions against central differences of the forward solve,
-    relative error <= 1e-5.  The step is 1e-5 (relative to each q): with
-    forward solves to 1e-13, J carries round-off noise that makes a 1e-6
-    step noise-dominated on this grid (measured: 9.6e-5 at 1e-6, 3.6e-6 at
-    1e-5, 2.6e-7 at 1e-4).  dJ/dk per block at step 1e-3 agrees to 1e-5 of
+    relative error <= 1e-5.  The step is 1e-4 (relative to each q): with
+    forward solves to 1e-13, J carries round-off noise that makes smaller
+    steps noise-dominated on this grid (measured on one converged flow:
+    9.6e-5 at 1e-6, 3.6e-6 at 1e-5, 2.6e-7 at 1e-4; the noise, and so the
+    error at 1e-5, varies by a few times between converged flows that differ
+    at the 1e-6 residual level), while the truncation error of the central
+    difference of this smooth J is O(h^2).  dJ/dk per block at step 1e-3 agrees to 1e-5 of
     the largest block sensitivity (a block J hardly depends on has
     differences at the noise floor, so a relative bound would test the
     noise).  q and k are checked apart: in a joint direction the two parts
@@ -158,7 +161,7 @@ def test_adjoint_at_config4_vs_central_differences():
         return g.adjoint(tol=tol, maxiter=20000)[0]
 
     rng = np.random.default_rng(11)
-    h = 1e-5
+    h = 1e-4
     worst = 0.0
     for _ in range(16):
         dqd = np.where(solid, rng.standard_normal(q.size) * q, 0.0)
