@@ -127,7 +127,14 @@ __device__ __forceinline__ void face(const ChtDev &H, int i, int j, int k, int d
   F = (hi ? u : -u) * A;
 }
 
-__global__ void k_cht_assemble(ChtDev H, double Tb) {
+// The operator rows, and (L0.gx non-null) level 0 of the multigrid
+// hierarchy in its precision from the same face values: each cell's low-face
+// conductance and + direction flux, the ghost past each high end carrying
+// that boundary face (every other entry of the level-0 face arrays stays 0
+// from the allocation).
+template <class MT>
+__global__ void k_cht_assemble(ChtDev H, double Tb, mg::Level<MT> L0) {
+  const int PX = H.Nx + 2, PXY = (H.Nx + 2) * (H.Ny + 2);
   for (mg::Walk w(H.Nx, H.Ny, H.Nz, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x); w.ok(); w.next()) {
     const int i = w.m, j = w.j, k = w.k;
     const int q = pidx(H, i, j, k);
@@ -139,6 +146,13 @@ __global__ void k_cht_assemble(ChtDev H, double Tb) {
       diag += G + fmax(F, 0.0);
       a[d] = has ? G + fmax(-F, 0.0) : 0.0;
       if (!has) rhs += (G + fmax(-F, 0.0)) * Tb;
+      if (L0.gx) {
+        MT *g = d < 2 ? L0.gx : d < 4 ? L0.gy : L0.gz, *f = d < 2 ? L0.fx : d < 4 ? L0.fy : L0.fz;
+        const int st = d < 2 ? 1 : d < 4 ? PX : PXY;
+        const bool last = d == 1 ? i == H.Nx - 1 : d == 3 ? j == H.Ny - 1 : k == H.Nz - 1;
+        if (!(d & 1)) { g[q] = (MT)G; f[q] = (MT)(-F); }
+        else if (last) { g[q + st] = (MT)G; f[q + st] = (MT)F; }
+      }
     }
     H.d[q] = diag; H.dinv[q] = 1.0 / diag;
     H.aw[q] = a[0]; H.ae[q] = a[1]; H.as[q] = a[2]; H.an[q] = a[3]; H.ab[q] = a[4]; H.af[q] = a[5];
@@ -152,37 +166,6 @@ struct Vec {
 
 // Jacobi-preconditioned BiCGStab (van der Vorst, SIAM J. Sci. Stat. Comput.
 // 13(2), 1992) for A x = rhs or A^T x = rhs; x holds the start.
-// level 0 of the multigrid hierarchy: each cell's low-face conductance and +
-// direction flux; the ghost past each high end carries that boundary face
-template <class MT>
-__device__ void cht_mg_fine(const ChtDev &H, const mg::Level<MT> &L0, int tid, int T) {
-  const int PX = H.Nx + 2, PY = H.Ny + 2;
-  const long long np = (long long)PX * PY * (H.Nz + 2);
-  for (long long q = tid; q < np; q += T) {
-    const int i = (int)(q % PX) - 1, j = (int)((q / PX) % PY) - 1, k = (int)(q / ((long long)PX * PY)) - 1;
-    const bool iin = i >= 0 && i < H.Nx, jin = j >= 0 && j < H.Ny, kin = k >= 0 && k < H.Nz;
-    double G, F;
-    bool has;
-    MT g = MT(0), f = MT(0);
-    if (jin && kin && i >= 0 && i <= H.Nx) {
-      if (i < H.Nx) { face(H, i, j, k, 0, G, F, has); g = (MT)G; f = (MT)(-F); }
-      else { face(H, H.Nx - 1, j, k, 1, G, F, has); g = (MT)G; f = (MT)F; }
-    }
-    L0.gx[q] = g; L0.fx[q] = f;
-    g = MT(0); f = MT(0);
-    if (iin && kin && j >= 0 && j <= H.Ny) {
-      if (j < H.Ny) { face(H, i, j, k, 2, G, F, has); g = (MT)G; f = (MT)(-F); }
-      else { face(H, i, H.Ny - 1, k, 3, G, F, has); g = (MT)G; f = (MT)F; }
-    }
-    L0.gy[q] = g; L0.fy[q] = f;
-    g = MT(0); f = MT(0);
-    if (iin && jin && k >= 0 && k <= H.Nz) {
-      if (k < H.Nz) { face(H, i, j, k, 4, G, F, has); g = (MT)G; f = (MT)(-F); }
-      else { face(H, i, j, H.Nz - 1, 5, G, F, has); g = (MT)G; f = (MT)F; }
-    }
-    L0.gz[q] = g; L0.fz[q] = f;
-  }
-}
 
 // y = A x (transpose = 0) or A^T x at padded q, x in any precision
 template <class XT>
@@ -215,11 +198,7 @@ __global__ void __launch_bounds__(kBiT, 1) k_cht_bicgstab(ChtDev H, Vec V, mg::H
   const bool tr = transpose != 0, mgp = Gm.L > 0;
   const MT *z = mgp ? Gm.lv[0].x : nullptr;
   int buf = 0;
-  if (mgp) {
-    cht_mg_fine(H, Gm.lv[0], tid, T);
-    grid.sync();
-    mg::build(Gm, tr, grid, tid, T);
-  }
+  if (mgp) mg::build(Gm, tr, grid, tid, T);  // level 0 written by k_cht_assemble
   double red[2] = {0.0, 0.0};
   for (mg::Walk w(Nx, Ny, H.Nz, tid, T); w.ok(); w.next()) {
     const int q = (w.m + 1) + PX * ((w.j + 1) + (Ny + 2) * (w.k + 1));
@@ -601,6 +580,16 @@ void launch_coop(K kernel, int blocks, cudaStream_t s, A... args) {
   HC_CUDA(cudaLaunchCooperativeKernel((void *)kernel, dim3(blocks), dim3(kBiT), argv, 0, s));
 }
 
+// operator rows and the fine level of the hierarchy in use (every solve is
+// preceded by this, on the same stream)
+void assemble(ChtState *C) {
+  const int nb = gfor((long long)C->H.Nx * C->H.Ny * C->H.Nz);
+  if (C->precond == 2) k_cht_assemble<double><<<nb, kB, 0, C->stream>>>(C->H, C->Tb, C->Gd.lv[0]);
+  else if (C->precond == 1) k_cht_assemble<float><<<nb, kB, 0, C->stream>>>(C->H, C->Tb, C->Gf.lv[0]);
+  else k_cht_assemble<float><<<nb, kB, 0, C->stream>>>(C->H, C->Tb, mg::Level<float>{});
+  HC_CUDA(cudaGetLastError());
+}
+
 void solve(ChtState *C, const double *rhs, int transpose, double tol, int maxiter, int rel0, double *out_r0) {
   if (C->precond == 2)
     launch_coop(k_cht_bicgstab<double>, C->grid, C->stream, C->H, C->V, C->Gd, rhs, transpose, tol, maxiter, C->partials,
@@ -643,7 +632,7 @@ void cht_forward(ChtState *C, double *T_host, double *J, int *iters, double *rel
   HC_CUDA(cudaSetDevice(C->device));
   const ChtDev &H = C->H;
   const size_t np = (size_t)(H.Nx + 2) * (H.Ny + 2) * (H.Nz + 2);
-  k_cht_assemble<<<gfor((long long)H.Nx * H.Ny * H.Nz), kB, 0, C->stream>>>(H, C->Tb);
+  assemble(C);
   k_cht_fill<<<gfor((long long)H.Nx * H.Ny * H.Nz), kB, 0, C->stream>>>(H.Nx * H.Ny * H.Nz, H.Nx, H.Ny, C->Tb, C->V.x);
   solve(C, H.b, 0, C->tol, C->maxiter, 0, nullptr);
   HC_CUDA(cudaMemcpyAsync(C->T, C->V.x, np * 8, cudaMemcpyDeviceToDevice, C->stream));
@@ -708,7 +697,7 @@ void cht_energy_step(ChtState *C, double alpha_t, double tol, int maxiter) {
   const ChtDev &H = C->H;
   const int n = H.Nx * H.Ny * H.Nz;
   const size_t np = (size_t)(H.Nx + 2) * (H.Ny + 2) * (H.Nz + 2);
-  k_cht_assemble<<<gfor(n), kB, 0, C->stream>>>(H, C->Tb);
+  assemble(C);
   HC_CUDA(cudaMemcpyAsync(C->V.x, C->T, np * 8, cudaMemcpyDeviceToDevice, C->stream));
   solve(C, H.b, 0, tol, maxiter, 1, C->res + 1);
   k_cht_relax<<<gfor(n), kB, 0, C->stream>>>(n, H.Nx, H.Ny, alpha_t, (const double *)C->V.x, C->T);
