@@ -54,11 +54,12 @@ CONFIG = {"workload": "channel 256x128x128 (4.19M cells), 8 seeded heated blocks
                       "k_s/k_f U[10,1000]), Re 400, SIMPLE-CHT outer step",
           "grid": [256, 128, 128], "blocks": 8, "seed": 0, "precision": "fp64", "re": 400, "pr": 0.71,
           "relaxation": {"u": 0.7, "p": 0.3, "T": 0.9}, "momentum": "FOU, 2 red-black GS sweeps",
-          "pressure_solver": "CG + multigrid V(2,2)-cycle (FP64), rtol 1e-5 (the reference's HYPRE setting)",
+          "pressure_solver": "CG + multigrid V-cycle (FP64; 2 red-black sweeps each way on the finest level, 3 on the coarser), rtol 1e-5 (the reference's HYPRE setting)",
           "energy_solver": "BiCGStab + multigrid V-cycle (FP64), one iteration per outer step",
           "l2_policy": "state ~790 MB on the device, larger than L2 (126 MB)", "parallelism": "replicas"}
-# red-black sweeps before and after each coarse correction of the p' V-cycle
-# (the library default, hs_channel_params.p_mg_sweeps = 0)
+# red-black sweeps before and after the coarse correction on the finest level
+# of the p' V-cycle, one more on the coarser levels (the library default,
+# hs_channel_params.p_mg_sweeps = 0)
 MG_SWEEPS = 2
 # launches per outer step: 4 momentum passes, p' assembly, residual finalize,
 # p' solve, correction, energy assembly, energy BiCGStab, energy relaxation
@@ -144,11 +145,16 @@ def pcg_bytes(ncell, iters, wbytes=8, sweeps=MG_SWEEPS):
         one V-cycle on level 0: 3 + 4 (sweeps - 1) standalone red-black
           half-sweeps of 5w (3 couplings, rhs, x read; x written), the
           restriction 5w + 2w/8 and the coarse values of the prolongation
-          w/8; the coarser levels add 1/7 of that."""
+          w/8; the coarser levels (one sweep more) add 1/7 of their own
+          per-cell bytes."""
     w = wbytes
     setup = 3 * w + 1 + 1 + w + w + 2 * w
     cg = 7 * w + 9 * w + w
-    vc = ((3 + 4 * (sweeps - 1)) * 5 * w + 5 * w + 0.25 * w + 0.125 * w) * 8.0 / 7.0
+
+    def level(sw):
+        return (3 + 4 * (sw - 1)) * 5 * w + 5 * w + 0.25 * w + 0.125 * w
+
+    vc = level(sweeps) + level(sweeps + 1) / 7.0
     return ncell * (setup + iters * (cg + vc))
 
 

@@ -19,7 +19,7 @@ struct ChParams {
   int t_maxiter;
   int precision;                    // 0 FP64, 1 mixed (FP32 fields, sweeps and V-cycle)
   int p_precond;                    // 0 plain CG, 1 multigrid V-cycle
-  int p_mg_sweeps;                  // V-cycle sweeps before / after the coarse correction (0: 2)
+  int p_mg_sweeps;                  // V-cycle sweeps on the finest level (0: 2); coarser levels one more
 };
 
 struct ChStats {

@@ -16,9 +16,10 @@
 // any child is; coarse face g = (sum of the 2x2 fine g) / 2 (the patch area is
 // 4x, the spacing 2x), coarse flux = sum of the fine fluxes (conservative);
 // down to <= kMgCoarse cells, where an LU with partial pivoting (FP64, on the
-// GPU) solves exactly.  Smoother: red-black Gauss-Seidel, G.nsw sweeps
-// before (red, black, ...) and after (black, red, ...), mirrored so that the
-// cycle stays symmetric for CG; the first red half-sweep (from
+// GPU) solves exactly.  Smoother: red-black Gauss-Seidel, G.nsw sweeps on
+// level 0 and G.nswc on the coarser levels before (red, black, ...) and after
+// (black, red, ...) each coarse correction, mirrored so that the cycle stays
+// symmetric for CG; the first red half-sweep (from
 // x = 0) is applied by whoever writes the level's rhs, the prolongation is
 // fused into the first post-smoothing half-sweep.  Levels below kMgSmall cells run inside
 // block 0 alone, separated by __syncthreads instead of grid barriers.
@@ -48,7 +49,8 @@ struct Level {
 template <class M>
 struct Hier {
   int L;
-  int nsw;  // red-black sweeps before and after each coarse correction (0 or 1: one)
+  int nsw;   // red-black sweeps before and after the coarse correction on level 0 (0 or 1: one)
+  int nswc;  // the same on the coarser levels (0 or 1: one)
   Level<M> lv[kMgMaxLv];
   double *lu;  // kMgCoarse^2
   int *piv;    // kMgCoarse
@@ -542,7 +544,7 @@ __device__ bool vcycle(const Hier<M> &G, bool tr, cg::grid_group &grid, int tid,
   for (int l = 0; l < ls; ++l) {
     smooth(G.lv[l], 1, tr, tid, T);
     grid.sync();
-    for (int s = 1; s < G.nsw; ++s) {
+    for (int s = 1; s < (l == 0 ? G.nsw : G.nswc); ++s) {
       smooth(G.lv[l], 0, tr, tid, T);
       grid.sync();
       smooth(G.lv[l], 1, tr, tid, T);
@@ -556,7 +558,7 @@ __device__ bool vcycle(const Hier<M> &G, bool tr, cg::grid_group &grid, int tid,
     for (int l = ls; l < G.L - 1; ++l) {
       smooth(G.lv[l], 1, tr, t, B);
       __syncthreads();
-      for (int s = 1; s < G.nsw; ++s) {
+      for (int s = 1; s < (l == 0 ? G.nsw : G.nswc); ++s) {
         smooth(G.lv[l], 0, tr, t, B);
         __syncthreads();
         smooth(G.lv[l], 1, tr, t, B);
@@ -572,7 +574,7 @@ __device__ bool vcycle(const Hier<M> &G, bool tr, cg::grid_group &grid, int tid,
       __syncthreads();
       smooth(G.lv[l], 0, tr, t, B);
       __syncthreads();
-      for (int s = 1; s < G.nsw; ++s) {
+      for (int s = 1; s < (l == 0 ? G.nsw : G.nswc); ++s) {
         smooth(G.lv[l], 1, tr, t, B);
         __syncthreads();
         smooth(G.lv[l], 0, tr, t, B);
@@ -584,7 +586,7 @@ __device__ bool vcycle(const Hier<M> &G, bool tr, cg::grid_group &grid, int tid,
   for (int l = ls - 1; l >= 0; --l) {
     prolong_smooth(G.lv[l], G.lv[l + 1], tr, tid, T);
     grid.sync();
-    for (int s = 1; s < G.nsw; ++s) {
+    for (int s = 1; s < (l == 0 ? G.nsw : G.nswc); ++s) {
       smooth(G.lv[l], 0, tr, tid, T);
       grid.sync();
       smooth(G.lv[l], 1, tr, tid, T);

@@ -258,8 +258,10 @@ typedef struct hs_channel_params {
   int t_maxiter;
   int precision;       /* HS_PREC_* */
   int p_precond;       /* 0 plain CG, 1 multigrid V-cycle */
-  int p_mg_sweeps;     /* red-black sweeps before and after each coarse
-                          correction of the p' V-cycle (0: the default, 2) */
+  int p_mg_sweeps;     /* red-black sweeps before and after the coarse
+                          correction on the finest level of the p' V-cycle
+                          (0: the default, 2); the coarser levels take one
+                          more */
   int reserved_i;
   double reserved[5];
 } hs_channel_params;
