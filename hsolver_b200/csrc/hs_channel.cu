@@ -952,6 +952,7 @@ ChannelState *ch_create(const Case &c, const ChParams &p, int device) {
   cs.ctype = c.ctype.data(); cs.region = S->region.data();
   cs.t_boundary = p.t_in; cs.tol = 1e-10; cs.maxiter = 5000; cs.bc = 1;
   cs.precond = p.precision == 1 ? 1 : 2;
+  cs.step_fp32 = p.precision == 1;
   S->cht = cht_create(cs);
   cht_bind_velocities(S->cht, uarr(S.get(), 0), uarr(S.get(), 1), uarr(S.get(), 2));
   S->kratio.assign(S->nreg, 100.0);

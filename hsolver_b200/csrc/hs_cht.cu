@@ -24,6 +24,7 @@
 #include <memory>
 #include <stdexcept>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "hs_cht.hpp"
@@ -160,9 +161,12 @@ __global__ void k_cht_assemble(ChtDev H, double Tb, mg::Level<MT> L0) {
   }
 }
 
-struct Vec {
-  double *x, *r, *rh, *p, *v, *ph, *s, *sh, *t;
+// Krylov vectors (padded cells) in storage precision VT
+template <class VT>
+struct VecT {
+  VT *x, *r, *rh, *p, *v, *ph, *s, *sh, *t;
 };
+using Vec = VecT<double>;
 
 // Jacobi-preconditioned BiCGStab (van der Vorst, SIAM J. Sci. Stat. Comput.
 // 13(2), 1992) for A x = rhs or A^T x = rhs; x holds the start.
@@ -186,10 +190,15 @@ __device__ __forceinline__ double apply_any(const ChtDev &H, const XT *x, int q,
 // output directly and store p^, s^ on the way; <r^, r> of the next iteration
 // is summed with <r, r>.
 // rel0: stop on ||r|| / ||r0|| instead of ||r|| / ||rhs||; out_r0 = ||r0||.
-template <class MT>
-__global__ void __launch_bounds__(kBiT, 1) k_cht_bicgstab(ChtDev H, Vec V, mg::Hier<MT> Gm, const double *rhs,
+// Vectors stored in VT, arithmetic and dot products in FP64.  x0 (FP64,
+// optional, FP32 vectors only): solve for the correction to x0 instead, from
+// x = 0, with the first residual rhs - A x0 (and ||r0||) evaluated in FP64.
+template <class MT, class VT>
+__global__ void __launch_bounds__(kBiT, 1) k_cht_bicgstab(ChtDev H, VecT<VT> V, mg::Hier<MT> Gm, const double *rhs,
                                                         int transpose, double tol, int maxiter, double *partials,
-                                                        int *out_it, double *out_rel, int rel0, double *out_r0) {
+                                                        int *out_it, double *out_rel, int rel0, double *out_r0,
+                                                        const double *x0) {
+  constexpr bool kFp64 = std::is_same<VT, double>::value;
   cg::grid_group grid = cg::this_grid();
   __shared__ double sh[48];
   const int Nx = H.Nx, Ny = H.Ny;
@@ -203,8 +212,15 @@ __global__ void __launch_bounds__(kBiT, 1) k_cht_bicgstab(ChtDev H, Vec V, mg::H
   for (mg::Walk w(Nx, Ny, H.Nz, tid, T); w.ok(); w.next()) {
     const int q = (w.m + 1) + PX * ((w.j + 1) + (Ny + 2) * (w.k + 1));
     const double bq = rhs[q];
-    const double rv = bq - apply_any(H, V.x, q, PX, PXY, tr);
-    V.r[q] = rv; V.rh[q] = rv; V.p[q] = 0.0; V.v[q] = 0.0;
+    double ax;
+    if constexpr (kFp64) {
+      ax = apply_any(H, V.x, q, PX, PXY, tr);
+    } else {
+      ax = x0 ? apply_any(H, x0, q, PX, PXY, tr) : apply_any(H, V.x, q, PX, PXY, tr);
+      if (x0) V.x[q] = VT(0);
+    }
+    const double rv = bq - ax;
+    V.r[q] = (VT)rv; V.rh[q] = (VT)rv; V.p[q] = VT(0); V.v[q] = VT(0);
     red[0] += bq * bq;
     red[1] += rv * rv;
   }
@@ -221,44 +237,44 @@ __global__ void __launch_bounds__(kBiT, 1) k_cht_bicgstab(ChtDev H, Vec V, mg::H
     // each pass issues every load of a cell before its first store
     for (mg::Walk w(Nx, Ny, H.Nz, tid, T); w.ok(); w.next()) {
       const int q = (w.m + 1) + PX * ((w.j + 1) + (Ny + 2) * (w.k + 1));
-      const double r_ = V.r[q], p_ = V.p[q], v_ = V.v[q];
+      const double r_ = (double)V.r[q], p_ = (double)V.p[q], v_ = (double)V.v[q];
       const mg::Seed<MT> sd = mgp ? mg::seed_at(Gm.lv[0], w.m, w.j, w.k, q, tr) : mg::Seed<MT>{};
       const double di = mgp ? 0.0 : H.dinv[q];
-      const double pv = r_ + beta * (p_ - omega * v_);
+      const VT pv = (VT)(r_ + beta * (p_ - omega * v_));
       V.p[q] = pv;
       if (mgp) sd.store(Gm.lv[0], q, pv);
-      else V.ph[q] = pv * di;
+      else V.ph[q] = (VT)((double)pv * di);
     }
     grid.sync();
     if (mgp) mg::vcycle(Gm, tr, grid, tid, T);
     double s2[1] = {0.0};
     for (mg::Walk w(Nx, Ny, H.Nz, tid, T); w.ok(); w.next()) {
       const int q = (w.m + 1) + PX * ((w.j + 1) + (Ny + 2) * (w.k + 1));
-      const double rh = V.rh[q];
-      const double vv = mgp ? apply_any(H, z, q, PX, PXY, tr) : apply_any(H, V.ph, q, PX, PXY, tr);
-      if (mgp) V.ph[q] = (double)__ldcg(z + q);
+      const double rh = (double)V.rh[q];
+      const VT vv = (VT)(mgp ? apply_any(H, z, q, PX, PXY, tr) : apply_any(H, V.ph, q, PX, PXY, tr));
+      if (mgp) V.ph[q] = (VT)__ldcg(z + q);
       V.v[q] = vv;
-      s2[0] += rh * vv;
+      s2[0] += rh * (double)vv;
     }
     grid_sums<1>(s2, partials, buf, sh, grid);
     alpha = rho1 / s2[0];
     double s3[1] = {0.0};
     for (mg::Walk w(Nx, Ny, H.Nz, tid, T); w.ok(); w.next()) {
       const int q = (w.m + 1) + PX * ((w.j + 1) + (Ny + 2) * (w.k + 1));
-      const double r_ = V.r[q], v_ = V.v[q];
+      const double r_ = (double)V.r[q], v_ = (double)V.v[q];
       const mg::Seed<MT> sd = mgp ? mg::seed_at(Gm.lv[0], w.m, w.j, w.k, q, tr) : mg::Seed<MT>{};
       const double di = mgp ? 0.0 : H.dinv[q];
-      const double sv = r_ - alpha * v_;
+      const VT sv = (VT)(r_ - alpha * v_);
       V.s[q] = sv;
       if (mgp) sd.store(Gm.lv[0], q, sv);
-      else V.sh[q] = sv * di;
-      s3[0] += sv * sv;
+      else V.sh[q] = (VT)((double)sv * di);
+      s3[0] += (double)sv * (double)sv;
     }
     grid_sums<1>(s3, partials, buf, sh, grid);
     if (s3[0] / bb < eps) {
       for (mg::Walk w(Nx, Ny, H.Nz, tid, T); w.ok(); w.next()) {
         const int q = (w.m + 1) + PX * ((w.j + 1) + (Ny + 2) * (w.k + 1));
-        V.x[q] += alpha * V.ph[q];
+        V.x[q] = (VT)((double)V.x[q] + alpha * (double)V.ph[q]);
       }
       rr = s3[0];
       break;
@@ -267,24 +283,25 @@ __global__ void __launch_bounds__(kBiT, 1) k_cht_bicgstab(ChtDev H, Vec V, mg::H
     double s4[2] = {0.0, 0.0};
     for (mg::Walk w(Nx, Ny, H.Nz, tid, T); w.ok(); w.next()) {
       const int q = (w.m + 1) + PX * ((w.j + 1) + (Ny + 2) * (w.k + 1));
-      const double sq = V.s[q];
-      const double tv = mgp ? apply_any(H, z, q, PX, PXY, tr) : apply_any(H, V.sh, q, PX, PXY, tr);
-      if (mgp) V.sh[q] = (double)__ldcg(z + q);
+      const double sq = (double)V.s[q];
+      const VT tv = (VT)(mgp ? apply_any(H, z, q, PX, PXY, tr) : apply_any(H, V.sh, q, PX, PXY, tr));
+      if (mgp) V.sh[q] = (VT)__ldcg(z + q);
       V.t[q] = tv;
-      s4[0] += tv * sq;
-      s4[1] += tv * tv;
+      s4[0] += (double)tv * sq;
+      s4[1] += (double)tv * (double)tv;
     }
     grid_sums<2>(s4, partials, buf, sh, grid);
     omega = s4[0] / s4[1];
     double s5[2] = {0.0, 0.0};
     for (mg::Walk w(Nx, Ny, H.Nz, tid, T); w.ok(); w.next()) {
       const int q = (w.m + 1) + PX * ((w.j + 1) + (Ny + 2) * (w.k + 1));
-      const double x_ = V.x[q], ph = V.ph[q], sh_ = V.sh[q], s_ = V.s[q], t_ = V.t[q], rh = V.rh[q];
-      V.x[q] = x_ + (alpha * ph + omega * sh_);
-      const double rv = s_ - omega * t_;
+      const double x_ = (double)V.x[q], ph = (double)V.ph[q], sh_ = (double)V.sh[q], s_ = (double)V.s[q],
+                   t_ = (double)V.t[q], rh = (double)V.rh[q];
+      V.x[q] = (VT)(x_ + (alpha * ph + omega * sh_));
+      const VT rv = (VT)(s_ - omega * t_);
       V.r[q] = rv;
-      s5[0] += rv * rv;
-      s5[1] += rh * rv;
+      s5[0] += (double)rv * (double)rv;
+      s5[1] += rh * (double)rv;
     }
     grid_sums<2>(s5, partials, buf, sh, grid);
     rr = s5[0];
@@ -391,6 +408,14 @@ __global__ void k_cht_relax(int n, int Nx, int Ny, double a, const double *x, do
   }
 }
 
+// T = T + a d on the interior of padded arrays
+__global__ void k_cht_relax_correction(int n, int Nx, int Ny, double a, const float *d, double *T) {
+  for (mg::Walk w(Nx, Ny, n / (Nx * Ny), blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x); w.ok(); w.next()) {
+    const int q = (w.m + 1) + (Nx + 2) * ((w.j + 1) + (Ny + 2) * (w.k + 1));
+    T[q] = T[q] + a * (double)d[q];
+  }
+}
+
 // T = v on the interior
 __global__ void k_cht_fill(int n, int Nx, int Ny, double v, double *T) {
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
@@ -428,6 +453,8 @@ struct ChtState {
   double J = 0;
   bool have_T = false;
   int precond = 0;              // 0 Jacobi, 1 V-cycle FP32, 2 V-cycle FP64
+  bool step_fp32 = false;       // energy steps in correction form with FP32 vectors (Vf)
+  VecT<float> Vf{};             // laid over the storage of V (not used at the same time)
   mg::Hier<float> Gf{};
   mg::Hier<double> Gd{};
   template <class T_>
@@ -515,8 +542,16 @@ ChtState *cht_create(const ChtSetup &S) {
   C->precond = S.precond;
   if (S.precond == 1) setup_levels(*C, C->Gf);
   if (S.precond == 2) setup_levels(*C, C->Gd);
-  C->grid = std::min(coop_grid((const void *)k_cht_bicgstab<float>, S.device),
-                     coop_grid((const void *)k_cht_bicgstab<double>, S.device));
+  C->step_fp32 = S.step_fp32 != 0;
+  if (C->step_fp32) {
+    // nine FP32 vectors in the first five FP64 ones (2 x np floats each)
+    float *base[] = {(float *)C->V.x, (float *)C->V.r, (float *)C->V.rh, (float *)C->V.p, (float *)C->V.v};
+    float **vf[] = {&C->Vf.x, &C->Vf.r, &C->Vf.rh, &C->Vf.p, &C->Vf.v, &C->Vf.ph, &C->Vf.s, &C->Vf.sh, &C->Vf.t};
+    for (int a = 0; a < 9; ++a) *vf[a] = base[a / 2] + (a % 2) * np;
+  }
+  C->grid = std::min({coop_grid((const void *)k_cht_bicgstab<float, double>, S.device),
+                      coop_grid((const void *)k_cht_bicgstab<double, double>, S.device),
+                      coop_grid((const void *)k_cht_bicgstab<float, float>, S.device)});
   C->partials = C->alloc<double>((size_t)2 * C->grid * 2 + 4096);
   C->res = C->alloc<double>(2); C->it = C->alloc<int>(1);
   HC_CUDA(cudaStreamSynchronize(C->stream));
@@ -591,15 +626,26 @@ void assemble(ChtState *C) {
 }
 
 void solve(ChtState *C, const double *rhs, int transpose, double tol, int maxiter, int rel0, double *out_r0) {
+  const double *nox = nullptr;
   if (C->precond == 2)
-    launch_coop(k_cht_bicgstab<double>, C->grid, C->stream, C->H, C->V, C->Gd, rhs, transpose, tol, maxiter, C->partials,
-                C->it, C->res, rel0, out_r0);
+    launch_coop(k_cht_bicgstab<double, double>, C->grid, C->stream, C->H, C->V, C->Gd, rhs, transpose, tol, maxiter,
+                C->partials, C->it, C->res, rel0, out_r0, nox);
   else {
     mg::Hier<float> G = C->Gf;
     if (C->precond == 0) G.L = 0;
-    launch_coop(k_cht_bicgstab<float>, C->grid, C->stream, C->H, C->V, G, rhs, transpose, tol, maxiter, C->partials,
-                C->it, C->res, rel0, out_r0);
+    launch_coop(k_cht_bicgstab<float, double>, C->grid, C->stream, C->H, C->V, G, rhs, transpose, tol, maxiter,
+                C->partials, C->it, C->res, rel0, out_r0, nox);
   }
+}
+
+// A d = b - A T with d from 0 in FP32 vectors (V-cycle in FP32), stopping on
+// ||r|| <= tol ||r0||; ||r0|| (FP64) into out_r0
+void solve_correction(ChtState *C, double tol, int maxiter, double *out_r0) {
+  mg::Hier<float> G = C->Gf;
+  if (C->precond != 1) G.L = 0;
+  const double *x0 = C->T;
+  launch_coop(k_cht_bicgstab<float, float>, C->grid, C->stream, C->H, C->Vf, G, (const double *)C->H.b, 0, tol,
+              maxiter, C->partials, C->it, C->res, 1, out_r0, x0);
 }
 
 void unpad(const ChtDev &H, const double *dev, double *host, cudaStream_t s) {
@@ -698,9 +744,14 @@ void cht_energy_step(ChtState *C, double alpha_t, double tol, int maxiter) {
   const int n = H.Nx * H.Ny * H.Nz;
   const size_t np = (size_t)(H.Nx + 2) * (H.Ny + 2) * (H.Nz + 2);
   assemble(C);
-  HC_CUDA(cudaMemcpyAsync(C->V.x, C->T, np * 8, cudaMemcpyDeviceToDevice, C->stream));
-  solve(C, H.b, 0, tol, maxiter, 1, C->res + 1);
-  k_cht_relax<<<gfor(n), kB, 0, C->stream>>>(n, H.Nx, H.Ny, alpha_t, (const double *)C->V.x, C->T);
+  if (C->step_fp32) {
+    solve_correction(C, tol, maxiter, C->res + 1);
+    k_cht_relax_correction<<<gfor(n), kB, 0, C->stream>>>(n, H.Nx, H.Ny, alpha_t, (const float *)C->Vf.x, C->T);
+  } else {
+    HC_CUDA(cudaMemcpyAsync(C->V.x, C->T, np * 8, cudaMemcpyDeviceToDevice, C->stream));
+    solve(C, H.b, 0, tol, maxiter, 1, C->res + 1);
+    k_cht_relax<<<gfor(n), kB, 0, C->stream>>>(n, H.Nx, H.Ny, alpha_t, (const double *)C->V.x, C->T);
+  }
   HC_CUDA(cudaGetLastError());
   C->have_T = false;
 }

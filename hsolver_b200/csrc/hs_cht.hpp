@@ -17,6 +17,8 @@ struct ChtSetup {
   int bc;                         // 0 Dirichlet t_boundary on every boundary face; 1 channel (Dirichlet at
                                   // x = 0, upwind outflow at x = Nx, adiabatic y / z walls)
   int precond;                    // BiCGStab preconditioner: 0 Jacobi, 1 multigrid V-cycle in FP32, 2 in FP64
+  int step_fp32 = 0;              // cht_energy_step solves for the correction to T with FP32 Krylov vectors
+                                  // (residual, dot products and T in FP64)
 };
 
 // where the face velocities come from: the fluid box's padded u*, v*, w*
@@ -35,8 +37,9 @@ void cht_get_velocities(ChtState *c, double *ug, double *vg, double *wg);
 void cht_forward(ChtState *c, double *T_host, double *J, int *iters, double *relres);
 void cht_adjoint(ChtState *c, double *dJdq_host, double *dJdk_host, int *iters, double *relres);
 // channel use: the owner's device face velocities, T = v everywhere, one relaxed
-// energy step (BiCGStab from the current T to tol * ||r0||, T += alpha (T~ - T)),
-// its results (iterations, ||r|| / ||r0||, ||r0||) after a stream sync
+// energy step (BiCGStab from the current T to tol * ||r0||, T += alpha (T~ - T);
+// with step_fp32, BiCGStab for the correction d = T~ - T from 0 in FP32 vectors,
+// T += alpha d), its results (iterations, ||r|| / ||r0||, ||r0||) after a stream sync
 void cht_bind_velocities(ChtState *c, const double *ug, const double *vg, const double *wg);
 void cht_fill_T(ChtState *c, double v);
 double *cht_T_device(ChtState *c);

@@ -130,7 +130,7 @@ __device__ __forceinline__ bool unknown(const Level<M> &L, int q) { return L.m ?
 
 // coarse level C from fine level F (every padded cell of C that holds a face)
 template <class M>
-__device__ void coarsen(const Level<M> &F, const Level<M> &C, int tid, int T) {
+__device__ __forceinline__ void coarsen(const Level<M> &F, const Level<M> &C, int tid, int T) {
   const int n = (C.nx + 1) * (C.ny + 1) * (C.nz + 1);
   const bool conv = F.fx != nullptr;
   for (int e = tid; e < n; e += T) {
@@ -198,7 +198,7 @@ __device__ void coarsen(const Level<M> &F, const Level<M> &C, int tid, int T) {
 // a masked cell has zero couplings on every face (its faces touch a
 // non-unknown), so d == 0 identifies it without reading the mask
 template <class M>
-__device__ void smooth(const Level<M> &L, int color, bool tr, int tid, int T) {
+__device__ __forceinline__ void smooth(const Level<M> &L, int color, bool tr, int tid, int T) {
   for (Walk w((L.nx + 1) / 2, L.ny, L.nz, tid, T); w.ok(); w.next()) {
     const int j = w.j, k = w.k, i = 2 * w.m + ((j + k + color) & 1);
     if (i >= L.nx) continue;
@@ -215,7 +215,7 @@ __device__ void smooth(const Level<M> &L, int color, bool tr, int tid, int T) {
 // half-sweep): the V-cycle's output dotted with the caller's residual r
 // (padded, any precision; FP64 sums) without a pass of its own.
 template <class M, class RT>
-__device__ void smooth_dot(const Level<M> &L, bool tr, const RT *r, double &acc, int tid, int T) {
+__device__ __forceinline__ void smooth_dot(const Level<M> &L, bool tr, const RT *r, double &acc, int tid, int T) {
   for (Walk w((L.nx + 1) / 2, L.ny, L.nz, tid, T); w.ok(); w.next()) {
     const int j = w.j, k = w.k;
     const int i = 2 * w.m + ((j + k) & 1), ib = 2 * w.m + ((j + k + 1) & 1);
@@ -290,7 +290,7 @@ __device__ __forceinline__ Seed<M> seed_at(const Level<M> &L, int i, int j, int 
 // (every lane of a warp runs the same number of iterations: the shuffles
 // need the full warp).
 template <class M>
-__device__ void restrict_res(const Level<M> &F, const Level<M> &C, bool tr, int tid, int T) {
+__device__ __forceinline__ void restrict_res(const Level<M> &F, const Level<M> &C, bool tr, int tid, int T) {
   if (4LL * C.nx * C.ny * C.nz > T) {
     for (Walk w(C.nx, C.ny, C.nz, tid, T); w.ok(); w.next()) {
       const int I = w.m, J = w.j, K = w.k;
@@ -351,7 +351,7 @@ __device__ void restrict_res(const Level<M> &F, const Level<M> &C, bool tr, int 
 // neighbours are 0, as they are never prolonged; a masked neighbour has a
 // zero coupling.  The arithmetic is that of prolongation followed by smooth().
 template <class M>
-__device__ void prolong_smooth(const Level<M> &F, const Level<M> &C, bool tr, int tid, int T) {
+__device__ __forceinline__ void prolong_smooth(const Level<M> &F, const Level<M> &C, bool tr, int tid, int T) {
   const int PX = F.nx + 2, PXY = (F.nx + 2) * (F.ny + 2);
   const int CPX = C.nx + 2, CPXY = (C.nx + 2) * (C.ny + 2);
   for (Walk w((F.nx + 1) / 2, F.ny, F.nz, tid, T); w.ok(); w.next()) {
@@ -399,7 +399,7 @@ __device__ __forceinline__ int *piv_smem() {
 // row among equals; the factors are copied to G.lu / G.piv and the explicit
 // inverse is left in shared memory for coarse_solve
 template <class M>
-__device__ void factor(const Hier<M> &G, bool tr) {
+__device__ __forceinline__ void factor(const Hier<M> &G, bool tr) {
   if (blockIdx.x != 0) return;
   double *a = lu_smem();
   int *sp = piv_smem();
@@ -495,7 +495,7 @@ __device__ void factor(const Hier<M> &G, bool tr) {
 // calls it): x = A^-1 rhs with the inverse that factor() left in shared
 // memory, thread r summing row r in column order
 template <class M>
-__device__ void coarse_solve(const Hier<M> &G) {
+__device__ __forceinline__ void coarse_solve(const Hier<M> &G) {
   __shared__ double y[kMgCoarse];
   const double *ainv = lu_smem();
   const Level<M> &C = G.lv[G.L - 1];
@@ -515,7 +515,7 @@ __device__ __forceinline__ bool small(const Level<M> &L) { return (long long)L.n
 
 // build levels 1.. from level 0 and factor the coarsest (the caller filled level 0)
 template <class M>
-__device__ void build(const Hier<M> &G, bool tr, cg::grid_group &grid, int tid, int T) {
+__device__ __forceinline__ void build(const Hier<M> &G, bool tr, cg::grid_group &grid, int tid, int T) {
   for (int l = 0; l + 1 < G.L; ++l) {
     if (small(G.lv[l + 1]) && blockIdx.x != 0) break;
     if (small(G.lv[l + 1])) {
@@ -537,7 +537,7 @@ __device__ void build(const Hier<M> &G, bool tr, cg::grid_group &grid, int tid, 
 // the caller's reduction (returns true); it returns false, with the barrier
 // done and nothing added, when level 0 is handled by block 0 alone.
 template <class M, class RT = double>
-__device__ bool vcycle(const Hier<M> &G, bool tr, cg::grid_group &grid, int tid, int T,
+__device__ __forceinline__ bool vcycle(const Hier<M> &G, bool tr, cg::grid_group &grid, int tid, int T,
                        const RT *dot_r = nullptr, double *dot_acc = nullptr) {
   int ls = 0;  // first level handled by block 0 alone
   while (ls < G.L - 1 && !small(G.lv[ls])) ++ls;
