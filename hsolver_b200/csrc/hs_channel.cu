@@ -524,9 +524,19 @@ __device__ __forceinline__ int cell_q(int e, int N0, int N1) {
   return (i + 1) + (N0 + 2) * ((j + 1) + (N1 + 2) * (k + 1));
 }
 
-// one 768-thread block per SM: the same warps per SM as three 256-thread
-// blocks, a third of the arrivals at every grid barrier
-constexpr int kPcgT = 768;
+// one block per SM (few arrivals at every grid barrier), its size by
+// precision: 512 threads for FP64 (128 registers, no spills) and 640 for FP32,
+// the fastest of 512 / 640 / 768 / 1024 for each on a 256x128x128 channel
+// (FP64 5.32 / 5.56 / 5.85 / 5.49 ms per solve, FP32 3.99 / 3.62 / 3.65 /
+// 3.81)
+template <class M>
+struct PcgT {
+  static constexpr int v = 640;
+};
+template <>
+struct PcgT<double> {
+  static constexpr int v = 512;
+};
 
 // level 0 of the V-cycle: its couplings are the CG's own arrays (the same
 // pointers); the mask, and the diagonal of every interior row for the seeds
@@ -550,7 +560,7 @@ __device__ void mg_fine_from_couplings(const CgVec<M> &V, const mg::Level<M> &L0
 // forms the new p of its cell and of the six neighbours from z and the old
 // p; p is double-buffered), and <r, z> inside the V-cycle's last pass.
 template <class M>
-__global__ void __launch_bounds__(kPcgT, 1) k_ch_pcg(CgVec<M> V, mg::Hier<M> G, int precond, double tol, int maxiter, double *partials,
+__global__ void __launch_bounds__(PcgT<M>::v, 1) k_ch_pcg(CgVec<M> V, mg::Hier<M> G, int precond, double tol, int maxiter, double *partials,
                                                int *out_it, double *out_rel) {
   cg::grid_group grid = cg::this_grid();
   __shared__ double sh[40];
@@ -651,9 +661,9 @@ __global__ void k_ch_finalize(const double *mom, const double *cont, int nb, dou
 int blocks_for(long long n) { return (int)std::max<long long>(1, std::min<long long>((n + kT - 1) / kT, 148LL * 8)); }
 
 template <class K, class... A>
-void launch_coop(K kernel, int blocks, cudaStream_t s, A... args) {
+void launch_coop(K kernel, int blocks, int threads, cudaStream_t s, A... args) {
   void *argv[] = {(void *)&args...};
-  CH_CUDA(cudaLaunchCooperativeKernel((void *)kernel, dim3(blocks), dim3(kPcgT), argv, 0, s));
+  CH_CUDA(cudaLaunchCooperativeKernel((void *)kernel, dim3(blocks), dim3(threads), argv, 0, s));
 }
 
 }  // namespace
@@ -822,10 +832,10 @@ void step_once(ChannelState &S, ChDev<R> &H, int flags) {
   if (!(flags & 1)) {
     const int pre = S.prm.p_precond ? 1 : 0;
     if (S.mixed)
-      launch_coop(k_ch_pcg<float>, S.pcg_grid, S.stream, S.Vf, S.Gf, pre, S.prm.p_tol, S.prm.p_maxiter, S.pcg_part, S.pcg_it,
+      launch_coop(k_ch_pcg<float>, S.pcg_grid, PcgT<float>::v, S.stream, S.Vf, S.Gf, pre, S.prm.p_tol, S.prm.p_maxiter, S.pcg_part, S.pcg_it,
                   S.pcg_rel);
     else
-      launch_coop(k_ch_pcg<double>, S.pcg_grid, S.stream, S.Vd, S.Gd, pre, S.prm.p_tol, S.prm.p_maxiter, S.pcg_part, S.pcg_it,
+      launch_coop(k_ch_pcg<double>, S.pcg_grid, PcgT<double>::v, S.stream, S.Vd, S.Gd, pre, S.prm.p_tol, S.prm.p_maxiter, S.pcg_part, S.pcg_it,
                   S.pcg_rel);
   } else {
     const long long np = (long long)(S.N0 + 2) * (S.N1 + 2) * (S.N2 + 2);
@@ -935,8 +945,8 @@ ChannelState *ch_create(const Case &c, const ChParams &p, int device) {
   S->res = S->alloc<double>(4);
   int per = 0, nsm = 0;
   CH_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
-  if (S->mixed) CH_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_ch_pcg<float>, kPcgT, 0));
-  else CH_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_ch_pcg<double>, kPcgT, 0));
+  if (S->mixed) CH_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_ch_pcg<float>, PcgT<float>::v, 0));
+  else CH_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_ch_pcg<double>, PcgT<double>::v, 0));
   if (per < 1) throw std::runtime_error("pressure-correction kernel cannot be resident");
   S->pcg_grid = per * nsm;
   S->pcg_part = S->alloc<double>((size_t)2 * S->pcg_grid + 64);
