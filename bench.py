@@ -65,8 +65,8 @@ MG_SWEEPS = 2
 # p' solve, correction, energy assembly, energy BiCGStab, energy relaxation
 LAUNCHES_PER_STEP = 11
 # DRAM bytes per CG iteration of k_ch_pcg on this case, from one ncu capture
-# (profiles/k_ch_pcg_config2_dram.md: 21.85 GB per 9-iteration launch)
-PCG_TRAFFIC_PER_ITER = 21.85e9 / 9
+# (profiles/k_ch_pcg_config2_dram.md: 18.12 GB per 8-iteration launch)
+PCG_TRAFFIC_PER_ITER = 18.12e9 / 8
 
 
 def workload(name=NAME, seed=0):
@@ -336,7 +336,7 @@ def run_gpu(args):
                                                  "one cooperative launch per outer step)",
                          "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
                          "traffic": PCG_TRAFFIC_PER_ITER * it_mean,
-                         "traffic_source": "ncu dram bytes of 3 launches (9 iterations each), per iteration x "
+                         "traffic_source": "ncu dram bytes of 3 launches (8 iterations each), per iteration x "
                                            "this launch's iterations", "peak_source": peak_kind,
                          "algorithmic_bytes_per_launch": b,
                          "pcg_iters_per_launch": it_mean, "launch_ms": pms},
