@@ -542,14 +542,12 @@ struct PcgT<double> {
 // pointers); the mask, and the diagonal of every interior row for the seeds
 template <class M>
 __device__ void mg_fine_from_couplings(const CgVec<M> &V, const mg::Level<M> &L0, int tid, int T) {
-  const int PX = V.N0 + 2, PY = V.N1 + 2;
-  const long long np = (long long)PX * PY * (V.N2 + 2);
-  for (long long q = tid; q < np; q += T) {
-    const int i = (int)(q % PX) - 1, j = (int)((q / PX) % PY) - 1, k = (int)(q / ((long long)PX * PY)) - 1;
+  for (mg::Walk w(V.N0 + 2, V.N1 + 2, V.N2 + 2, tid, T); w.ok(); w.next()) {
+    const int q = w.flat(), i = w.m - 1, j = w.j - 1, k = w.k - 1;
     const bool in = i >= 0 && j >= 0 && k >= 0 && i < V.N0 && j < V.N1 && k < V.N2;
     L0.m[q] = in && !V.solid[i + V.N0 * (j + V.N1 * k)];
     M d = M(0), o[6];
-    if (in) mg::row(L0, (int)q, false, d, o);
+    if (in) mg::row(L0, q, false, d, o);
     L0.d[q] = d;
   }
 }

@@ -84,6 +84,30 @@ def test_converged_state_matches_oracle_and_conserves_mass():
     assert abs(u[:, :, 0].sum() - u[:, :, -1].sum()) <= 1e-6 * u[:, :, 0].sum()
 
 
+@pytest.mark.parametrize("precision", [0, 1])
+def test_v_cycle_sweep_count_changes_only_the_path(precision):
+    """The p' V-cycle's sweep count (p_mg_sweeps; the coarser levels take one
+    more) is a preconditioner setting: with 1, the default (2) and 3 sweeps
+    the solves take fewer CG iterations as the count grows, and the states
+    converged to a global residual of 1e-8 agree to 1e-7."""
+    deck = _deck(32, 16, 16, ((9, 14, 1, 6, 5, 10), (20, 24, 8, 12, 2, 6)))
+    states, iters = [], []
+    for sweeps in (1, 0, 3):
+        g, _, _ = _pair(deck, re=100.0, precision=precision, p_mg_sweeps=sweeps)
+        st = g.step(3)
+        iters.append(st["pcg_iters"])
+        ok, _, st = g.solve_to(1e-8, 4000)
+        assert ok, (sweeps, st)
+        states.append({f: g.field(f) for f in FACE + ["p", "T"]})
+    assert iters[0] > iters[1] >= iters[2], iters
+    for s in states[1:]:
+        for name in FACE + ["T"]:
+            assert _rel(s[name], states[0][name]) < 1e-7, name
+        # p is defined by its differences: compare with the means removed
+        a, b = s["p"] - s["p"].mean(), states[0]["p"] - states[0]["p"].mean()
+        assert _rel(a, b) < 1e-7
+
+
 def test_mixed_precision_against_fp64():
     deck = _deck()
     g64, _, _ = _pair(deck, re=100.0)
