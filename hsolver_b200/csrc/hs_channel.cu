@@ -25,9 +25,10 @@
 // FMA contraction off, so the FP64 form reproduces it bit for bit; sums of
 // residuals and dot products are per-block partials reduced in a fixed order.
 //
-// Precision: R = double (plain form) or float (mixed form: fields, sweeps and
-// the V-cycle in FP32; residuals, the CG recurrences, dot products, mass
-// imbalance and the coarsest-grid solve in FP64).
+// Precision: R = double (plain form) or float (mixed form: the momentum and
+// energy steps in correction form, with FP64 residuals and FP32 sweeps,
+// Krylov vectors and V-cycles; dot products, mass imbalance, the p and T
+// updates and the coarsest-grid solve in FP64).
 #include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
