@@ -194,7 +194,7 @@ __device__ __forceinline__ void term(const ChDev<R> &H, const int (&c)[3], R Ar,
 // correction).
 template <int A>
 __device__ __forceinline__ void mom_face_mixed_first(const ChDev<float> &H, const int (&c)[3], int f, bool upd,
-                                                     bool last, double &racc) {
+                                                     bool last, double &racc, bool keep) {
   ChDev<double> H64;
   H64.N0 = H.N0; H64.N1 = H.N1; H64.N2 = H.N2;
   H64.d0 = H.xd0; H64.d1 = H.xd1; H64.d2 = H.xd2; H64.h0 = H.xh0; H64.h1 = H.xh1; H64.h2 = H.xh2;
@@ -221,6 +221,7 @@ __device__ __forceinline__ void mom_face_mixed_first(const ChDev<float> &H, cons
 #pragma unroll
   for (int n = 0; n < 6; ++n) s += ad[n] * (nd[n] >= 0 ? UA[nd[n]] : 0.0);
   const double r = (s + bs) - aPd * UA[f];
+  if (!keep) return;
   racc += r * r;
   const float rhs = (float)r;
   Qarr<A>(H)[f] = rhs;
@@ -235,11 +236,11 @@ __device__ __forceinline__ void mom_face_mixed_first(const ChDev<float> &H, cons
 // relaxed Gauss-Seidel update (upd), d (last sweep)
 template <int A, class R>
 __device__ __forceinline__ void mom_face(const ChDev<R> &H, const int (&c)[3], bool first, bool upd, bool last,
-                                         double &racc) {
+                                         double &racc, bool keep) {
   const int f = fidx3<A>(H, c);
   if constexpr (is_mixed(R())) {
     if (first) {
-      mom_face_mixed_first<A>(H, c, f, upd, last, racc);
+      mom_face_mixed_first<A>(H, c, f, upd, last, racc, keep);
       return;
     }
   }
@@ -269,20 +270,22 @@ __device__ __forceinline__ void mom_face(const ChDev<R> &H, const int (&c)[3], b
 #pragma unroll
       for (int n = 0; n < 6; ++n) s += (double)an[n] * (nb[n] >= 0 ? UA[nb[n]] : 0.0);
       const double r = (double)aP * (double)un - (s + (double)bs);
-      racc += r * r;
+      if (keep) racc += r * r;
     }
     if (upd) {
       R s = R(0);
 #pragma unroll
       for (int n = 0; n < 6; ++n) s += an[n] * (nb[n] >= 0 ? src[nb[n]] : R(0));
       const R rhs = s + bs + (R(1) - H.au) * apr * un;
-      SA[f] = rhs / apr;
-      if (last) Darr<A>(H)[f] = Ar / apr;
+      if (keep) {
+        SA[f] = rhs / apr;
+        if (last) Darr<A>(H)[f] = Ar / apr;
+      }
     }
   } else {
     // correction sweeps after the first pass (FP32 operator, FP32 right-hand side from the first pass)
     const R rhs = Qarr<A>(H)[f];
-    if (upd) {
+    if (upd && keep) {
       R s = R(0);
 #pragma unroll
       for (int n = 0; n < 6; ++n) s += an[n] * (nb[n] >= 0 ? SA[nb[n]] : R(0));
@@ -316,29 +319,37 @@ __device__ void mom_pass_axis(const ChDev<R> &H, int color, bool first, bool las
   if (first) {
     for (mg::Walk w(nf0, nf1, nf2, tid, T); w.ok(); w.next()) {
       const int c[3] = {w.m, w.j, w.k};
-      const int kind = face_kind<A>(H, c);
-      if (kind != 0) {
-        const int f = fidx3<A>(H, c);
+      const int f = fidx3<A>(H, c);
+      if (c[A] == 0 || c[A] == ncell<A>(H)) {  // boundary faces: fixed or outlet (an index test)
         Sarr<A>(H)[f] = is_mixed(R()) ? R(0) : face_fixed<A>(H, c);
         Darr<A>(H)[f] = R(0);
         continue;
       }
+      // an interior face: its update is evaluated whatever the solid mask
+      // says (every index it reads is valid) and kept only for an unknown
+      // face, so that no branch on the mask waits ahead of the stencil loads
+      const bool keep = face_kind<A>(H, c) == 0;
       const bool mine = ((c[0] + c[1] + c[2]) & 1) == color;
-      mom_face<A>(H, c, true, mine, last && mine, racc);
+      mom_face<A>(H, c, true, mine, last && mine, racc, keep);
+      if (!keep) {
+        Sarr<A>(H)[f] = R(0);
+        Darr<A>(H)[f] = R(0);
+      }
     }
   } else {
     for (mg::Walk w((nf0 + 1) / 2, nf1, nf2, tid, T); w.ok(); w.next()) {
       const int j = w.j, k = w.k, i = 2 * w.m + ((j + k + color) & 1);
       if (i >= nf0) continue;
       const int c[3] = {i, j, k};
-      if (face_kind<A>(H, c) != 0) continue;
-      mom_face<A>(H, c, false, true, last, racc);
+      if (c[A] == 0 || c[A] == ncell<A>(H)) continue;
+      mom_face<A>(H, c, false, true, last, racc, face_kind<A>(H, c) == 0);
     }
   }
 }
 
+// four 256-thread blocks per SM (64 registers: above that the SM holds three)
 template <class R>
-__global__ void __launch_bounds__(kT) k_ch_mom(ChDev<R> H, int color, int first, int last, double *partials) {
+__global__ void __launch_bounds__(kT, 4) k_ch_mom(ChDev<R> H, int color, int first, int last, double *partials) {
   __shared__ double sh[32];
   double racc = 0.0;
   if (blockIdx.y == 0) mom_pass_axis<0>(H, color, first, last, racc);
