@@ -381,38 +381,44 @@ __global__ void k_ch_passemble(ChDev<R> H, R *acx, R *acy, R *acz, R *r, R *x, d
   const int N0 = H.N0, N1 = H.N1, N2 = H.N2;
   double acc = 0.0;
   if (blockIdx.y == 0) {
+    // every value a face may need is loaded before its kind (from the solid
+    // mask) is known, so no branch on the mask waits ahead of the loads
     for (mg::Walk w(N0 + 1, N1, N2, tid, T); w.ok(); w.next()) {
       const int c[3] = {w.m, w.j, w.k};
+      const double dn = c[0] < N0 ? (double)H.D0[fidx3<0>(H, c)] : 0.0;
+      const double dl = c[0] > 0 ? (double)H.D0[fidx<0>(H, c[0] - 1, c[1], c[2])] : 0.0;
+      const bool lo_fluid = c[0] > 0 && !H.solid[cidx(H, c[0] - 1, c[1], c[2])];
       const int kind = face_kind<0>(H, c);
       double v = 0.0;
-      if (kind == 0) v = (double)face_area<0>(H, c) * (double)H.D0[fidx3<0>(H, c)];
-      else if (kind == 2 && !H.solid[cidx(H, c[0] - 1, c[1], c[2])])
-        v = (double)face_area<0>(H, c) * (double)H.D0[fidx<0>(H, c[0] - 1, c[1], c[2])];
+      if (kind == 0) v = (double)face_area<0>(H, c) * dn;
+      else if (kind == 2 && lo_fluid) v = (double)face_area<0>(H, c) * dl;
       acx[pq(N0, N1, c[0], c[1], c[2])] = (R)v;
     }
   } else if (blockIdx.y == 1) {
     for (mg::Walk w(N0, N1 + 1, N2, tid, T); w.ok(); w.next()) {
       const int c[3] = {w.m, w.j, w.k};
-      acy[pq(N0, N1, c[0], c[1], c[2])] = (R)(face_kind<1>(H, c) == 0 ? (double)face_area<1>(H, c) * (double)H.D1[fidx3<1>(H, c)] : 0.0);
+      const double dn = (double)H.D1[fidx3<1>(H, c)];
+      acy[pq(N0, N1, c[0], c[1], c[2])] = (R)(face_kind<1>(H, c) == 0 ? (double)face_area<1>(H, c) * dn : 0.0);
     }
   } else if (blockIdx.y == 2) {
     for (mg::Walk w(N0, N1, N2 + 1, tid, T); w.ok(); w.next()) {
       const int c[3] = {w.m, w.j, w.k};
-      acz[pq(N0, N1, c[0], c[1], c[2])] = (R)(face_kind<2>(H, c) == 0 ? (double)face_area<2>(H, c) * (double)H.D2[fidx3<2>(H, c)] : 0.0);
+      const double dn = (double)H.D2[fidx3<2>(H, c)];
+      acz[pq(N0, N1, c[0], c[1], c[2])] = (R)(face_kind<2>(H, c) == 0 ? (double)face_area<2>(H, c) * dn : 0.0);
     }
   } else {
     for (mg::Walk w(N0, N1, N2, tid, T); w.ok(); w.next()) {
       const int i = w.m, j = w.j, k = w.k, e = w.flat();
       const int q = pq(N0, N1, i, j, k);
-      x[q] = R(0);
-      if (H.solid[e]) { r[q] = R(0); continue; }
+      const bool sol = H.solid[e] != 0;
       const double uw = ustar<0>(H, fidx<0>(H, i, j, k));
       const double ue = (i + 1 == N0) ? uw : ustar<0>(H, fidx<0>(H, i + 1, j, k));
       const double b = (uw - ue) * ((double)H.d1[j] * (double)H.d2[k]) +
                        (ustar<1>(H, fidx<1>(H, i, j, k)) - ustar<1>(H, fidx<1>(H, i, j + 1, k))) * ((double)H.d0[i] * (double)H.d2[k]) +
                        (ustar<2>(H, fidx<2>(H, i, j, k)) - ustar<2>(H, fidx<2>(H, i, j, k + 1))) * ((double)H.d0[i] * (double)H.d1[j]);
-      r[q] = (R)b;
-      acc += b * b;
+      x[q] = R(0);
+      r[q] = sol ? R(0) : (R)b;
+      if (!sol) acc += b * b;
     }
   }
   const double bsum = block_sum(acc, sh);
@@ -426,23 +432,26 @@ __device__ void correct_axis(const ChDev<R> &H, const R *pp) {
   for (mg::Walk w(nf0, nf1, nf2, tid, T); w.ok(); w.next()) {
     const int c[3] = {w.m, w.j, w.k};
     const int e = w.flat();
+    // the values of every case are loaded before the face kind (from the
+    // solid mask) selects one; p' is padded, so its ghost cells are readable
+    int lo[3] = {c[0], c[1], c[2]};
+    lo[A] -= 1;
+    const double plo = (double)pp[pq(H.N0, H.N1, lo[0], lo[1], lo[2])];
+    const double phi = (double)pp[pq(H.N0, H.N1, c[0], c[1], c[2])];
+    const double sf = is_mixed(R()) ? ustar<A>(H, e) : (double)Sarr<A>(H)[e];
+    const double df = (double)Darr<A>(H)[e];
+    double so = 0.0, dso = 0.0;  // the outlet's upstream face (x faces)
+    bool lo_solid = true;
+    if (A == 0 && c[0] == H.N0) {
+      so = is_mixed(R()) ? ustar<0>(H, e - 1) : (double)H.S0[e - 1];
+      dso = (double)H.D0[e - 1];
+      lo_solid = H.solid[cidx(H, c[0] - 1, c[1], c[2])] != 0;
+    }
     const int kind = face_kind<A>(H, c);
     double val;
-    if (kind == 1) {
-      val = (double)face_fixed<A>(H, c);
-    } else if (kind == 2) {
-      const int fl = fidx<0>(H, c[0] - 1, c[1], c[2]);
-      if (H.solid[cidx(H, c[0] - 1, c[1], c[2])]) val = 0.0;
-      else if constexpr (!is_mixed(R())) val = H.S0[fl] + H.D0[fl] * pp[pq(H.N0, H.N1, c[0] - 1, c[1], c[2])];
-      else val = ustar<0>(H, fl) + (double)H.D0[fl] * pp[pq(H.N0, H.N1, c[0] - 1, c[1], c[2])];
-    } else {
-      int lo[3] = {c[0], c[1], c[2]};
-      lo[A] -= 1;
-      const int f = fidx3<A>(H, c);
-      const double dp = (double)pp[pq(H.N0, H.N1, lo[0], lo[1], lo[2])] - (double)pp[pq(H.N0, H.N1, c[0], c[1], c[2])];
-      if constexpr (!is_mixed(R())) val = Sarr<A>(H)[f] + Darr<A>(H)[f] * dp;
-      else val = ustar<A>(H, f) + (double)Darr<A>(H)[f] * dp;
-    }
+    if (kind == 1) val = (double)face_fixed<A>(H, c);
+    else if (kind == 2) val = lo_solid ? 0.0 : so + dso * plo;
+    else val = sf + df * (plo - phi);
     Uarr<A>(H)[e] = val;
     if constexpr (is_mixed(R())) Carr<A>(H)[e] = (R)val;
   }
