@@ -136,7 +136,7 @@ __device__ __forceinline__ void face(const ChtDev &H, int i, int j, int k, int d
 // that boundary face (every other entry of the level-0 face arrays stays 0
 // from the allocation).
 template <class MT>
-__global__ void k_cht_assemble(ChtDev H, double Tb, mg::Level<MT> L0) {
+__global__ void __launch_bounds__(kB, 4) k_cht_assemble(ChtDev H, double Tb, mg::Level<MT> L0) {  // 64 registers
   const int PX = H.Nx + 2, PXY = (H.Nx + 2) * (H.Ny + 2);
   for (mg::Walk w(H.Nx, H.Ny, H.Nz, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x); w.ok(); w.next()) {
     const int i = w.m, j = w.j, k = w.k;
