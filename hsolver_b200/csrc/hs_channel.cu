@@ -714,6 +714,14 @@ struct ChannelState {
   ChStats st{};
   int iter = 0;
   bool prof = false;
+  // statistics of the steps of one ch_step call, copied without waiting
+  // (pinned), applied in order after one stream synchronisation per kRing steps
+  struct StepRec {
+    double res[4], prel, trr[2];
+    int pit, tit;
+  };
+  static constexpr int kRing = 64;
+  StepRec *ring = nullptr;
   cudaEvent_t ev[6] = {};
   double prof_ms[5] = {0, 0, 0, 0, 0};
   int prof_steps = 0;
@@ -730,6 +738,7 @@ struct ChannelState {
     return (T_ *)p;
   }
   ~ChannelState() {
+    if (ring) cudaFreeHost(ring);
     for (cudaEvent_t e : ev)
       if (e) cudaEventDestroy(e);
     if (cht) cht_destroy(cht);
@@ -869,30 +878,23 @@ void step_once(ChannelState &S, ChDev<R> &H, int flags) {
   if (S.prof) CH_CUDA(cudaEventRecord(S.ev[5], S.stream));
 }
 
-void read_stats(ChannelState &S, int flags) {
-  double r[4];
-  int pit = 0;
-  double prel = 0;
-  CH_CUDA(cudaMemcpyAsync(r, S.res, 32, cudaMemcpyDeviceToHost, S.stream));
-  CH_CUDA(cudaMemcpyAsync(&pit, S.pcg_it, 4, cudaMemcpyDeviceToHost, S.stream));
-  CH_CUDA(cudaMemcpyAsync(&prel, S.pcg_rel, 8, cudaMemcpyDeviceToHost, S.stream));
-  CH_CUDA(cudaStreamSynchronize(S.stream));
-  for (int a = 0; a < 4; ++a) S.st.res[a] = r[a];
-  if (S.prof) {
-    for (int ph = 0; ph < 5; ++ph) {
-      float ms = 0;
-      CH_CUDA(cudaEventElapsedTime(&ms, S.ev[ph], S.ev[ph + 1]));
-      S.prof_ms[ph] += ms;
-    }
-    S.prof_steps++;
-  }
-  S.st.pcg_iters = (flags & 1) ? 0 : pit;
-  S.st.pcg_relres = (flags & 1) ? 0.0 : prel;
+// the step's statistics into rec, on the stream (rec in pinned memory: the
+// copies do not wait; read rec after the stream has passed them)
+void enqueue_stats(ChannelState &S, ChannelState::StepRec &rec, int flags) {
+  CH_CUDA(cudaMemcpyAsync(rec.res, S.res, 32, cudaMemcpyDeviceToHost, S.stream));
+  CH_CUDA(cudaMemcpyAsync(&rec.pit, S.pcg_it, 4, cudaMemcpyDeviceToHost, S.stream));
+  CH_CUDA(cudaMemcpyAsync(&rec.prel, S.pcg_rel, 8, cudaMemcpyDeviceToHost, S.stream));
+  if (!(flags & 2)) cht_step_results_async(S.cht, &rec.tit, rec.trr);
+}
+
+// the step's bookkeeping from its statistics: residuals, the normalisers
+// (maxima over the first five steps) and the global residual
+void apply_stats(ChannelState &S, const ChannelState::StepRec &rec, int flags) {
+  for (int a = 0; a < 4; ++a) S.st.res[a] = rec.res[a];
+  S.st.pcg_iters = (flags & 1) ? 0 : rec.pit;
+  S.st.pcg_relres = (flags & 1) ? 0.0 : rec.prel;
   if (!(flags & 2)) {
-    double rel, r0;
-    int it;
-    cht_step_results(S.cht, &it, &rel, &r0);
-    S.st.res[4] = r0; S.st.t_iters = it; S.st.t_relres = rel;
+    S.st.res[4] = rec.trr[1]; S.st.t_iters = rec.tit; S.st.t_relres = rec.trr[0];
   } else {
     S.st.res[4] = 0.0; S.st.t_iters = 0; S.st.t_relres = 0.0;
   }
@@ -905,6 +907,21 @@ void read_stats(ChannelState &S, int flags) {
     if (q > g) g = q;
   }
   S.st.global = g;
+}
+
+void read_stats(ChannelState &S, int flags) {
+  ChannelState::StepRec &rec = S.ring[0];
+  enqueue_stats(S, rec, flags);
+  CH_CUDA(cudaStreamSynchronize(S.stream));
+  if (S.prof) {
+    for (int ph = 0; ph < 5; ++ph) {
+      float ms = 0;
+      CH_CUDA(cudaEventElapsedTime(&ms, S.ev[ph], S.ev[ph + 1]));
+      S.prof_ms[ph] += ms;
+    }
+    S.prof_steps++;
+  }
+  apply_stats(S, rec, flags);
 }
 
 }  // namespace
@@ -983,6 +1000,7 @@ ChannelState *ch_create(const Case &c, const ChParams &p, int device) {
   cs.precond = p.precision == 1 ? 1 : 2;
   cs.step_fp32 = p.precision == 1;
   S->cht = cht_create(cs);
+  CH_CUDA(cudaHostAlloc((void **)&S->ring, ChannelState::kRing * sizeof(ChannelState::StepRec), cudaHostAllocDefault));
   cht_bind_velocities(S->cht, uarr(S.get(), 0), uarr(S.get(), 1), uarr(S.get(), 2));
   S->kratio.assign(S->nreg, 100.0);
   S->qcell.assign(n, 0.0);
@@ -1029,10 +1047,25 @@ void ch_init(ChannelState *S) {
 
 void ch_step(ChannelState *S, int n, int flags, ChStats *out) {
   CH_CUDA(cudaSetDevice(S->device));
-  for (int s = 0; s < n; ++s) {
-    if (S->mixed) step_once(*S, S->Hf, flags);
-    else step_once(*S, S->Hd, flags);
-    read_stats(*S, flags);
+  if (S->prof) {  // per-phase events of every step: one step at a time
+    for (int s = 0; s < n; ++s) {
+      if (S->mixed) step_once(*S, S->Hf, flags);
+      else step_once(*S, S->Hd, flags);
+      read_stats(*S, flags);
+    }
+  } else {
+    // steps queued back to back, their statistics applied afterwards in order
+    for (int done = 0; done < n;) {
+      const int b = std::min(n - done, ChannelState::kRing);
+      for (int s = 0; s < b; ++s) {
+        if (S->mixed) step_once(*S, S->Hf, flags);
+        else step_once(*S, S->Hd, flags);
+        enqueue_stats(*S, S->ring[s], flags);
+      }
+      CH_CUDA(cudaStreamSynchronize(S->stream));
+      for (int s = 0; s < b; ++s) apply_stats(*S, S->ring[s], flags);
+      done += b;
+    }
   }
   if (out) *out = S->st;
 }

@@ -769,6 +769,11 @@ void cht_step_results(ChtState *C, int *iters, double *relres, double *r0) {
   if (r0) *r0 = rr[1];
 }
 
+void cht_step_results_async(ChtState *C, int *iters, double *relres_r0) {
+  HC_CUDA(cudaMemcpyAsync(iters, C->it, 4, cudaMemcpyDeviceToHost, C->stream));
+  HC_CUDA(cudaMemcpyAsync(relres_r0, C->res, 16, cudaMemcpyDeviceToHost, C->stream));
+}
+
 void cht_set_tolerance(ChtState *C, double tol, int maxiter) { C->tol = tol; C->maxiter = maxiter; }
 
 }  // namespace hs

@@ -45,6 +45,9 @@ void cht_fill_T(ChtState *c, double v);
 double *cht_T_device(ChtState *c);
 void cht_energy_step(ChtState *c, double alpha_t, double tol, int maxiter);
 void cht_step_results(ChtState *c, int *iters, double *relres, double *r0);
+// the same results copied on the owner's stream, without waiting, into
+// (pinned) host memory: iterations, then ||r|| / ||r0|| and ||r0||
+void cht_step_results_async(ChtState *c, int *iters, double *relres_r0);
 void cht_set_tolerance(ChtState *c, double tol, int maxiter);
 
 }  // namespace hs
