@@ -85,6 +85,24 @@ def test_converged_state_matches_oracle_and_conserves_mass():
 
 
 @pytest.mark.parametrize("precision", [0, 1])
+def test_batched_steps_match_single_steps(precision):
+    """hs_channel_step(n) queues its n steps back to back and applies their
+    statistics afterwards (one synchronisation per 64 steps); n = 70 single
+    steps and one call of 70 steps give the same fields bit for bit and the
+    same statistics, normalisers included."""
+    deck = _deck()
+    a, _, _ = _pair(deck, re=100.0, precision=precision)
+    b, _, _ = _pair(deck, re=100.0, precision=precision)
+    for _ in range(70):
+        sa = a.step(1)
+    sb = b.step(70)
+    for name in FACE + ["p", "T"]:
+        assert np.array_equal(a.field(name), b.field(name)), name
+    for key in ("res", "norm", "global", "iter", "pcg_iters", "t_iters", "pcg_relres", "t_relres"):
+        assert sa[key] == sb[key], (key, sa[key], sb[key])
+
+
+@pytest.mark.parametrize("precision", [0, 1])
 def test_v_cycle_sweep_count_changes_only_the_path(precision):
     """The p' V-cycle's sweep count (p_mg_sweeps; the coarser levels take one
     more) is a preconditioner setting: with 1, the default (2) and 3 sweeps
