@@ -865,7 +865,6 @@ __global__ void __launch_bounds__(kBlock) k_pcorr(FluidDev F, Prm P, double *par
   __shared__ double sh[33];
   const int cx = F.cx, cy = F.cy, cz = F.cz, n = cx * cy * cz;
   const int PX = cx + 2, PXY = (cx + 2) * (cy + 2);
-  const long long npad = (long long)PXY * (cz + 2);
   const int tid = blockIdx.x * blockDim.x + threadIdx.x, T = gridDim.x * blockDim.x;
   int buf = 0;
   double acc = 0.0;
