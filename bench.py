@@ -158,7 +158,31 @@ def pcg_bytes(ncell, iters, wbytes=8, sweeps=MG_SWEEPS):
     return ncell * (setup + iters * (cg + vc))
 
 
-def kernel_classes(phases, iters_mean, dims, mom_sweeps, peak):
+def energy_bytes(ncell, iters, w=8, mw=8):
+    """Compulsory HBM bytes of one energy step per cell (FP64 form: Krylov
+    vectors w = 8 and V-cycle values mw = 8 bytes; the operator rows, the
+    assembly's inputs and T are FP64), each array once per pass:
+      assembly: k, q, three face velocities, solid mask read (41), nine
+        operator arrays written (72), level 0 of the hierarchy (conductance
+        and flux per axis) written (6 mw);
+      hierarchy build: level 0 read, coarser levels written (~6.9 mw);
+      first residual: rhs, seven operator arrays, x read; r, r^, p, v
+        written (64 + 5w);
+      per BiCGStab iteration: p update with the V-cycle seed (4w + 8mw), two
+        V-cycles (level 0: three half-sweeps of 9 mw, restriction 8.25 mw,
+        prolongation mw/8, coarser levels 1/7: ~40.4 mw each), two operator
+        products (56 + mw + 3w each), s update with its seed (3w + 8mw), x
+        and r update (8w);
+      relaxation: T and x read, T written (16 + w)."""
+    assemble = 41 + 72 + 6 * mw
+    build = 6.9 * mw
+    r0 = 64 + 5 * w
+    vc = (3 * 9 + 8.25 + 0.125) * mw * 8.0 / 7.0
+    it = (4 * w + 8 * mw) + 2 * vc + 2 * (56 + mw + 3 * w) + (3 * w + 8 * mw) + 8 * w
+    return ncell * (assemble + build + r0 + iters * it + 16 + w)
+
+
+def kernel_classes(phases, iters_mean, dims, mom_sweeps, peak, energy_iters=1):
     """Achieved HBM bandwidth of each phase of the outer step on its
     algorithmic bytes (FP64 form; each array counted once per pass):
       momentum: 49 B per face per red-black pass (u^n of the three
@@ -167,20 +191,19 @@ def kernel_classes(phases, iters_mean, dims, mom_sweeps, peak):
         mask; three couplings and b written);
       p' solve: pcg_bytes();
       correction: 96 B per cell (u*, d, u per face of the three components;
-        p', p read, p written).
-    The energy solve (BiCGStab with two V-cycles per iteration on six
-    coefficient arrays per level) is not modelled here."""
+        p', p read, p written);
+      energy: energy_bytes() with the step's BiCGStab iterations."""
     nx, ny, nz = dims
     ncell = nx * ny * nz
     nface = (nx + 1) * ny * nz + nx * (ny + 1) * nz + nx * ny * (nz + 1)
     model = {"momentum": 49.0 * nface * 2 * mom_sweeps, "p_assembly": 89.0 * ncell,
-             "p_solve": pcg_bytes(ncell, iters_mean), "correction": 96.0 * ncell}
+             "p_solve": pcg_bytes(ncell, iters_mean), "correction": 96.0 * ncell,
+             "energy": energy_bytes(ncell, energy_iters)}
     out = {}
     for k, b in model.items():
         ms = phases.get(k, 0.0)
         gbs = b / (ms * 1e-3) / 1e9 if ms > 0 else None
         out[k] = {"algorithmic_bytes": b, "ms": ms, "achieved_gbs": gbs, "frac": (gbs / peak) if gbs else None}
-    out["energy"] = {"ms": phases.get("energy"), "achieved_gbs": None, "frac": None, "note": "not modelled"}
     return out
 
 
