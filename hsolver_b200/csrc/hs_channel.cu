@@ -656,7 +656,7 @@ __global__ void __launch_bounds__(PcgT<M>::v, 1) k_ch_pcg(CgVec<M> V, mg::Hier<M
       if (precond) sd.store(L0, q, rv);
     }
     rr = grid_sum(acc, partials, buf, sh, grid);
-    if (rr / bb < eps) break;
+    if (rr / bb < eps || it >= maxiter) break;  // no V-cycle for an iteration that will not run
     const double gnew = precond ? rz() : rr;
     beta = gnew / gamma;
     gamma = gnew;
