@@ -559,17 +559,29 @@ struct PcgT<double> {
   static constexpr int v = 512;
 };
 
-// level 0 of the V-cycle: its couplings are the CG's own arrays (the same
-// pointers); the mask, and the diagonal of every interior row for the seeds
+// One pass over the padded cells: level 0 of the V-cycle (its couplings are
+// the CG's own arrays, the same pointers; the mask and the diagonal of every
+// row) and, on the interior, the V-cycle's right-hand side r with its seed
+// (which needs only the cell's own diagonal) and this thread's share of <r, r>
 template <class M>
-__device__ void mg_fine_from_couplings(const CgVec<M> &V, const mg::Level<M> &L0, int tid, int T) {
+__device__ void mg_fine_and_rhs(const CgVec<M> &V, const mg::Level<M> &L0, double &acc, int tid, int T) {
   for (mg::Walk w(V.N0 + 2, V.N1 + 2, V.N2 + 2, tid, T); w.ok(); w.next()) {
     const int q = w.flat(), i = w.m - 1, j = w.j - 1, k = w.k - 1;
     const bool in = i >= 0 && j >= 0 && k >= 0 && i < V.N0 && j < V.N1 && k < V.N2;
-    L0.m[q] = in && !V.solid[i + V.N0 * (j + V.N1 * k)];
     M d = M(0), o[6];
-    if (in) mg::row(L0, q, false, d, o);
+    double rv = 0.0;
+    bool solid = true;
+    if (in) {
+      mg::row(L0, q, false, d, o);
+      rv = (double)V.r[q];
+      solid = V.solid[i + V.N0 * (j + V.N1 * k)] != 0;
+    }
+    L0.m[q] = in && !solid;
     L0.d[q] = d;
+    if (in) {
+      acc += rv * rv;
+      mg::seed_store(L0, q, i, j, k, (M)rv, d);
+    }
   }
 }
 
@@ -587,23 +599,21 @@ __global__ void __launch_bounds__(PcgT<M>::v, 1) k_ch_pcg(CgVec<M> V, mg::Hier<M
   const int N0 = V.N0, N1 = V.N1, PX = N0 + 2, PY = N1 + 2, PXY = (N0 + 2) * (N1 + 2);
   int buf = 0;
   const mg::Level<M> &L0 = G.lv[0];
-  if (precond) {
-    mg_fine_from_couplings(V, L0, tid, T);
-    grid.sync();
-    mg::build(G, false, grid, tid, T);
-  }
   double acc = 0.0;
-  for (mg::Walk w(N0, N1, V.N2, tid, T); w.ok(); w.next()) {
-    const int q = (w.m + 1) + PX * ((w.j + 1) + PY * (w.k + 1));
-    const double rv = (double)V.r[q];
-    acc += rv * rv;
-    if (precond) mg::seed_at(L0, w.m, w.j, w.k, q, false).store(L0, q, rv);
+  if (precond) {
+    mg_fine_and_rhs(V, L0, acc, tid, T);
+  } else {
+    for (mg::Walk w(N0, N1, V.N2, tid, T); w.ok(); w.next()) {
+      const double rv = (double)V.r[(w.m + 1) + PX * ((w.j + 1) + PY * (w.k + 1))];
+      acc += rv * rv;
+    }
   }
   const double bb = grid_sum(acc, partials, buf, sh, grid);
   if (bb == 0.0) {
     if (tid == 0) { *out_it = 0; *out_rel = 0.0; }
     return;
   }
+  if (precond) mg::build(G, false, grid, tid, T);
   const double eps = tol * tol;
   // gamma = <r, z>
   auto rz = [&]() {
