@@ -676,15 +676,24 @@ __global__ void __launch_bounds__(PcgT<M>::v, 1) k_ch_pcg(CgVec<M> V, mg::Hier<M
 }
 
 // residual sums of the momentum pass (3 x nb partials) and continuity (nb) -> res[0..3]
+// (launched with 4 warps: warp a sums array a, each lane over four
+// interleaved strides so that four loads are in flight)
 __global__ void k_ch_finalize(const double *mom, const double *cont, int nb, double *res) {
-  if (threadIdx.x >= 32) return;
-  for (int a = 0; a < 4; ++a) {
-    const double *src = a < 3 ? mom + a * nb : cont;
-    double s = 0.0;
-    for (int q = threadIdx.x; q < nb; q += 32) s += src[q];
-    for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    if (threadIdx.x == 0) res[a] = sqrt(s);
+  const int a = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (a >= 4) return;
+  const double *src = a < 3 ? mom + a * nb : cont;
+  double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+  int q = lane;
+  for (; q + 96 < nb; q += 128) {
+    s0 += src[q];
+    s1 += src[q + 32];
+    s2 += src[q + 64];
+    s3 += src[q + 96];
   }
+  for (; q < nb; q += 32) s0 += src[q];
+  double s = (s0 + s1) + (s2 + s3);
+  for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if (lane == 0) res[a] = sqrt(s);
 }
 
 int blocks_for(long long n) { return (int)std::max<long long>(1, std::min<long long>((n + kT - 1) / kT, 148LL * 8)); }
@@ -864,7 +873,7 @@ void step_once(ChannelState &S, ChDev<R> &H, int flags) {
   CgVec<R> &V = cg_vec<R>(S);
   k_ch_passemble<R><<<dim3(S.mom_blocks, 4), kT, 0, S.stream>>>(H, (R *)V.acx, (R *)V.acy, (R *)V.acz, V.r, V.x,
                                                                 S.cont_part);
-  k_ch_finalize<<<1, 32, 0, S.stream>>>(S.mom_part, S.cont_part, S.mom_blocks, S.res);
+  k_ch_finalize<<<1, 128, 0, S.stream>>>(S.mom_part, S.cont_part, S.mom_blocks, S.res);
   CH_CUDA(cudaGetLastError());
   if (S.prof) CH_CUDA(cudaEventRecord(S.ev[2], S.stream));
   if (!(flags & 1)) {
