@@ -852,8 +852,6 @@ void setup_mg(ChannelState &S, mg::Hier<M> &G, const CgVec<M> &V) {
   G.nsw = S.prm.p_mg_sweeps > 0 ? S.prm.p_mg_sweeps : 2;
   G.nswc = G.nsw + 1;
   G.lu = S.alloc<double>((size_t)mg::kMgCoarse * mg::kMgCoarse);
-  G.piv = S.alloc<int>(mg::kMgCoarse);
-  G.y = S.alloc<double>(mg::kMgCoarse);
 }
 
 template <class R>

@@ -492,8 +492,6 @@ void setup_levels(ChtState &C, mg::Hier<MT> &G) {
   }
   G.L = L;
   G.lu = C.alloc<double>((size_t)mg::kMgCoarse * mg::kMgCoarse);
-  G.piv = C.alloc<int>(mg::kMgCoarse);
-  G.y = C.alloc<double>(mg::kMgCoarse);
 }
 }  // namespace
 

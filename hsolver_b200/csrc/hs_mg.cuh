@@ -52,9 +52,7 @@ struct Hier {
   int nsw;   // red-black sweeps before and after the coarse correction on level 0 (0 or 1: one)
   int nswc;  // the same on the coarser levels (0 or 1: one)
   Level<M> lv[kMgMaxLv];
-  double *lu;  // kMgCoarse^2
-  int *piv;    // kMgCoarse
-  double *y;   // kMgCoarse
+  double *lu;  // kMgCoarse^2: the factors, read back while the inverse is formed
 };
 
 // Grid-stride walk over an mx x ny x nz box in flat order (m fastest): the
@@ -396,7 +394,7 @@ __device__ __forceinline__ int *piv_smem() {
 
 // LU with partial pivoting of the coarsest operator (A or A^T), by block 0,
 // in shared memory; the pivot is the largest |a| in the column, the lowest
-// row among equals; the factors are copied to G.lu / G.piv and the explicit
+// row among equals; the factors are copied to G.lu and the explicit
 // inverse is left in shared memory for coarse_solve
 template <class M>
 __device__ __forceinline__ void factor(const Hier<M> &G, bool tr) {
@@ -443,7 +441,7 @@ __device__ __forceinline__ void factor(const Hier<M> &G, bool tr) {
         const int orow = __shfl_xor_sync(0xffffffffu, br, o);
         if (ov > bv || (ov == bv && orow < br)) { bv = ov; br = orow; }
       }
-      if (threadIdx.x == 0) { spiv = br; sp[col] = br; G.piv[col] = br; }
+      if (threadIdx.x == 0) { spiv = br; sp[col] = br; }
     }
     __syncthreads();
     const int pr = spiv;
