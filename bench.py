@@ -381,10 +381,12 @@ def run_gpu(args):
 def time_to_residual(args, hsolver_b200, local):
     """Wall time of hs_channel_solve_to(1e-6) for the FP64 and mixed forms, and
     the per-field relative L2 difference of the two converged states: config 1
-    (48x24x24) always, and the 256x128x128 case with --residual."""
+    (48x24x24) and config 3 (the same on a tanh-stretched grid, maximum cell
+    aspect ratio 20: the mixed-precision configuration) always, the
+    256x128x128 case with --residual."""
     import numpy as np
     out = {}
-    cases_ = [("config1", 2000)] + ([(NAME, args.residual_max)] if args.residual else [])
+    cases_ = [("config1", 2000), ("config3", 3000)] + ([(NAME, args.residual_max)] if args.residual else [])
     for name, cap in cases_:
         deck, re_, k, q, _ = workload(name)
         res, fields = {}, {}
