@@ -247,3 +247,25 @@ def test_configs_match_oracle(name):
         o.step(1)
     for f in FACE + ["p", "T"]:
         assert _rel(g.field(f), o.field(f)) < 1e-9, f
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_config3_converged_state_matches_oracle(precision):
+    """Configuration 3 (the tanh-stretched channel, cell aspect ratio up to
+    20, the mixed-precision configuration): the GPU converged to a global
+    residual of 1e-6 against the oracle's converged state (tests/golden/
+    channel_config3_converged.npz, made by make_channel_golden.py): the same
+    number of outer steps and every field within 1e-6 relative L2."""
+    import os
+    import bench
+    import hsolver_b200
+    ref = np.load(os.path.join(os.path.dirname(__file__), "golden", "channel_config3_converged.npz"))
+    deck, re_, k, q, _ = bench.workload("config3")
+    g = hsolver_b200.Channel(deck, re=re_, precision=precision)
+    g.set_solid(k, q)
+    g.init()
+    ok, steps, st = g.solve_to(1e-6, 3000)
+    assert ok, st
+    assert steps == int(ref["steps"]), (steps, int(ref["steps"]))
+    for name in FACE + ["p", "T"]:
+        assert _rel(g.field(name), ref[name]) < 1e-6, name
