@@ -81,6 +81,9 @@ struct ChDev {
   double ap;                  // alpha_p
   const double *xd0, *xd1, *xd2, *xh0, *xh1, *xh2;  // FP64 geometry (the residual of the mixed form)
   double nu_d, au_d, u_in_d;
+  // correctly rounded reciprocals of the divisors known ahead (FP64 arithmetic only)
+  const double *rd0, *rd1, *rd2, *rh0, *rh1, *rh2;  // 1 / cell width, 1 / centre distance
+  double rau;                                       // 1 / alpha_u
 };
 
 __host__ __device__ constexpr bool is_mixed(float) { return true; }
@@ -94,6 +97,22 @@ template <int A, class R> __device__ __forceinline__ R *Darr(const ChDev<R> &H) 
 template <int A, class R> __device__ __forceinline__ R wid(const ChDev<R> &H, int i) { return A == 0 ? H.d0[i] : A == 1 ? H.d1[i] : H.d2[i]; }
 template <int A, class R> __device__ __forceinline__ R ctr(const ChDev<R> &H, int i) { return A == 0 ? H.h0[i] : A == 1 ? H.h1[i] : H.h2[i]; }
 template <int A, class R> __device__ __forceinline__ int ncell(const ChDev<R> &H) { return A == 0 ? H.N0 : A == 1 ? H.N1 : H.N2; }
+template <int A, class R> __device__ __forceinline__ double rwid(const ChDev<R> &H, int i) { return A == 0 ? H.rd0[i] : A == 1 ? H.rd1[i] : H.rd2[i]; }
+template <int A, class R> __device__ __forceinline__ double rctr(const ChDev<R> &H, int i) { return A == 0 ? H.rh0[i] : A == 1 ? H.rh1[i] : H.rh2[i]; }
+
+// a / b.  In FP64, for a divisor known ahead of time, from its correctly
+// rounded reciprocal y = RN(1/b) (Markstein, IBM J. Res. Dev. 34(1), 1990):
+// q = RN(a y) is within one ulp of a/b, the remainder a - q b is exact in one
+// FMA, and RN(q + r y) is the correctly rounded quotient -- the IEEE value,
+// for finite normal operands and a nonzero a (as tests/test_gpu_division.py
+// checks for the same construction on the reference path).  FP32 keeps the
+// IEEE division.
+__device__ __forceinline__ double div_known(double a, double b, double y) {
+  const double q = a * y;
+  const double r = __fma_rn(-q, b, a);
+  return __fma_rn(r, y, q);
+}
+__device__ __forceinline__ float div_known(float a, float b, double) { return a / b; }
 
 template <int A, class R>
 __device__ __forceinline__ int fidx(const ChDev<R> &H, int i, int j, int k) {
@@ -144,14 +163,14 @@ __device__ __forceinline__ void term(const ChDev<R> &H, const int (&c)[3], R Ar,
       q[A] += 1;
       if (!(A == 0 && q[0] == H.N0)) {
         const R F = R(0.5) * (CA[fidx3<A>(H, c)] + CA[fidx3<A>(H, q)]) * Ar;
-        const R Dd = H.nu * Ar / wid<A>(H, c[A]);
+        const R Dd = div_known(H.nu * Ar, wid<A>(H, c[A]), rwid<A>(H, c[A]));
         coef = Dd + rmax0(-F);
         nb = fidx3<A>(H, q);
       }
     } else {
       q[A] -= 1;
       const R F = R(0.5) * (CA[fidx3<A>(H, q)] + CA[fidx3<A>(H, c)]) * Ar;
-      const R Dd = H.nu * Ar / wid<A>(H, c[A] - 1);
+      const R Dd = div_known(H.nu * Ar, wid<A>(H, c[A] - 1), rwid<A>(H, c[A] - 1));
       coef = Dd + rmax0(F);
       nb = fidx3<A>(H, q);
     }
@@ -167,17 +186,17 @@ __device__ __forceinline__ void term(const ChDev<R> &H, const int (&c)[3], R Ar,
     int q[3] = {c[0], c[1], c[2]};
     if (HI) {
       if (c[B] + 1 == ncell<B>(H)) {
-        if (B != 0) coef = H.nu * ar / ctr<B>(H, ncell<B>(H)) + rmax0(-F);
+        if (B != 0) coef = div_known(H.nu * ar, ctr<B>(H, ncell<B>(H)), rctr<B>(H, ncell<B>(H))) + rmax0(-F);
       } else {
-        coef = H.nu * ar / ctr<B>(H, c[B] + 1) + rmax0(-F);
+        coef = div_known(H.nu * ar, ctr<B>(H, c[B] + 1), rctr<B>(H, c[B] + 1)) + rmax0(-F);
         q[B] += 1;
         nb = fidx3<A>(H, q);
       }
     } else {
       if (c[B] == 0) {
-        coef = H.nu * ar / ctr<B>(H, 0) + rmax0(F);
+        coef = div_known(H.nu * ar, ctr<B>(H, 0), rctr<B>(H, 0)) + rmax0(F);
       } else {
-        coef = H.nu * ar / ctr<B>(H, c[B]) + rmax0(F);
+        coef = div_known(H.nu * ar, ctr<B>(H, c[B]), rctr<B>(H, c[B])) + rmax0(F);
         q[B] -= 1;
         nb = fidx3<A>(H, q);
       }
@@ -202,6 +221,8 @@ __device__ __forceinline__ void mom_face_mixed_first(const ChDev<float> &H, cons
   H64.U0 = H.U0; H64.U1 = H.U1; H64.U2 = H.U2;
   H64.C0 = H.U0; H64.C1 = H.U1; H64.C2 = H.U2;
   H64.p = H.p; H64.nu = H.nu_d; H64.au = H.au_d; H64.u_in = H.u_in_d;
+  H64.rd0 = H.rd0; H64.rd1 = H.rd1; H64.rd2 = H.rd2; H64.rh0 = H.rh0; H64.rh1 = H.rh1; H64.rh2 = H.rh2;
+  H64.rau = H.rau;
   const double Ad = face_area<A>(H64, c);
   const double dad = ctr<A>(H64, c[A]);
   double ad[6];
@@ -226,7 +247,7 @@ __device__ __forceinline__ void mom_face_mixed_first(const ChDev<float> &H, cons
   const float rhs = (float)r;
   Qarr<A>(H)[f] = rhs;
   if (upd) {
-    const float apr = (float)(aPd / H.au_d);
+    const float apr = (float)div_known(aPd, H.au_d, H.rau);
     Sarr<A>(H)[f] = rhs / apr;
     if (last) Darr<A>(H)[f] = face_area<A>(H, c) / apr;
   }
@@ -255,7 +276,7 @@ __device__ __forceinline__ void mom_face(const ChDev<R> &H, const int (&c)[3], b
   term<A, 2, 1>(H, c, Ar, da, an[4], nb[4]);
   term<A, 2, 0>(H, c, Ar, da, an[5], nb[5]);
   const R aP = an[0] + an[1] + an[2] + an[3] + an[4] + an[5];
-  const R apr = aP / H.au;
+  const R apr = div_known(aP, H.au, H.rau);
   const double *UA = Uarr<A>(H);
   R *SA = Sarr<A>(H);
   if constexpr (!is_mixed(R())) {
@@ -808,6 +829,18 @@ void setup_fields(ChannelState &S, ChDev<R> &H, const std::vector<double> (&d)[3
     CH_CUDA(cudaMemcpyAsync(ph, h[a].data(), h[a].size() * sizeof(double), cudaMemcpyHostToDevice, S.stream));
     *xd[a] = pd; *xh[a] = ph;
   }
+  // RN(1/x) of the FP64 widths and centre distances (IEEE division on the host)
+  const double **rd[3] = {&H.rd0, &H.rd1, &H.rd2}, **rh[3] = {&H.rh0, &H.rh1, &H.rh2};
+  for (int a = 0; a < 3; ++a) {
+    std::vector<double> rdv(d[a].size()), rhv(h[a].size());
+    for (size_t i = 0; i < rdv.size(); ++i) rdv[i] = 1.0 / d[a][i];
+    for (size_t i = 0; i < rhv.size(); ++i) rhv[i] = 1.0 / h[a][i];
+    double *pd = S.alloc<double>(rdv.size()), *ph = S.alloc<double>(rhv.size());
+    CH_CUDA(cudaMemcpyAsync(pd, rdv.data(), rdv.size() * sizeof(double), cudaMemcpyHostToDevice, S.stream));
+    CH_CUDA(cudaMemcpyAsync(ph, rhv.data(), rhv.size() * sizeof(double), cudaMemcpyHostToDevice, S.stream));
+    *rd[a] = pd; *rh[a] = ph;
+  }
+  H.rau = 1.0 / S.prm.alpha_u;
 }
 
 template <class R> CgVec<R> &cg_vec(ChannelState &S);
