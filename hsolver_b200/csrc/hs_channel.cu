@@ -453,6 +453,10 @@ __device__ void correct_axis(const ChDev<R> &H, const R *pp) {
   for (mg::Walk w(nf0, nf1, nf2, tid, T); w.ok(); w.next()) {
     const int c[3] = {w.m, w.j, w.k};
     const int e = w.flat();
+    // mixed form: u* = u^n + delta is read from u^n, which this pass
+    // replaces, so the outlet face (from its upstream face's u*) is written
+    // by the thread of that upstream face, after its own loads (below)
+    if (is_mixed(R()) && A == 0 && c[0] == H.N0) continue;
     // the values of every case are loaded before the face kind (from the
     // solid mask) selects one; p' is padded, so its ghost cells are readable
     int lo[3] = {c[0], c[1], c[2]};
@@ -468,13 +472,22 @@ __device__ void correct_axis(const ChDev<R> &H, const R *pp) {
       dso = (double)H.D0[e - 1];
       lo_solid = H.solid[cidx(H, c[0] - 1, c[1], c[2])] != 0;
     }
+    const bool feeds_outlet = is_mixed(R()) && A == 0 && c[0] == H.N0 - 1;
+    const bool up_solid = feeds_outlet && H.solid[cidx(H, c[0], c[1], c[2])] != 0;
     const int kind = face_kind<A>(H, c);
     double val;
     if (kind == 1) val = (double)face_fixed<A>(H, c);
     else if (kind == 2) val = lo_solid ? 0.0 : so + dso * plo;
     else val = sf + df * (plo - phi);
     Uarr<A>(H)[e] = val;
-    if constexpr (is_mixed(R())) Carr<A>(H)[e] = (R)val;
+    if constexpr (is_mixed(R())) {
+      Carr<A>(H)[e] = (R)val;
+      if (feeds_outlet) {  // the outlet face e + 1, as the FP64 form computes it
+        const double vo = up_solid ? 0.0 : sf + df * phi;
+        Uarr<0>(H)[e + 1] = vo;
+        Carr<0>(H)[e + 1] = (R)vo;
+      }
+    }
   }
 }
 
@@ -720,9 +733,9 @@ __global__ void k_ch_finalize(const double *mom, const double *cont, int nb, dou
 int blocks_for(long long n) { return (int)std::max<long long>(1, std::min<long long>((n + kT - 1) / kT, 148LL * 8)); }
 
 template <class K, class... A>
-void launch_coop(K kernel, int blocks, int threads, cudaStream_t s, A... args) {
+void launch_coop(K kernel, int blocks, int threads, size_t smem, cudaStream_t s, A... args) {
   void *argv[] = {(void *)&args...};
-  CH_CUDA(cudaLaunchCooperativeKernel((void *)kernel, dim3(blocks), dim3(threads), argv, 0, s));
+  CH_CUDA(cudaLaunchCooperativeKernel((void *)kernel, dim3(blocks), dim3(threads), argv, smem, s));
 }
 
 }  // namespace
@@ -885,6 +898,7 @@ void setup_mg(ChannelState &S, mg::Hier<M> &G, const CgVec<M> &V) {
   G.nsw = S.prm.p_mg_sweeps > 0 ? S.prm.p_mg_sweeps : 2;
   G.nswc = G.nsw + 1;
   G.lu = S.alloc<double>((size_t)mg::kMgCoarse * mg::kMgCoarse);
+  mg::plan_stage(G);
 }
 
 template <class R>
@@ -910,10 +924,10 @@ void step_once(ChannelState &S, ChDev<R> &H, int flags) {
   if (!(flags & 1)) {
     const int pre = S.prm.p_precond ? 1 : 0;
     if (S.mixed)
-      launch_coop(k_ch_pcg<float>, S.pcg_grid, PcgT<float>::v, S.stream, S.Vf, S.Gf, pre, S.prm.p_tol, S.prm.p_maxiter, S.pcg_part, S.pcg_it,
+      launch_coop(k_ch_pcg<float>, S.pcg_grid, PcgT<float>::v, S.Gf.stage, S.stream, S.Vf, S.Gf, pre, S.prm.p_tol, S.prm.p_maxiter, S.pcg_part, S.pcg_it,
                   S.pcg_rel);
     else
-      launch_coop(k_ch_pcg<double>, S.pcg_grid, PcgT<double>::v, S.stream, S.Vd, S.Gd, pre, S.prm.p_tol, S.prm.p_maxiter, S.pcg_part, S.pcg_it,
+      launch_coop(k_ch_pcg<double>, S.pcg_grid, PcgT<double>::v, S.Gd.stage, S.stream, S.Vd, S.Gd, pre, S.prm.p_tol, S.prm.p_maxiter, S.pcg_part, S.pcg_it,
                   S.pcg_rel);
   } else {
     const long long np = (long long)(S.N0 + 2) * (S.N1 + 2) * (S.N2 + 2);
@@ -1031,8 +1045,11 @@ ChannelState *ch_create(const Case &c, const ChParams &p, int device) {
   S->res = S->alloc<double>(4);
   int per = 0, nsm = 0;
   CH_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
-  if (S->mixed) CH_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_ch_pcg<float>, PcgT<float>::v, 0));
-  else CH_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_ch_pcg<double>, PcgT<double>::v, 0));
+  // the V-cycle's staging of block 0's levels: up to kMgStageMax bytes per launch
+  const void *pk = S->mixed ? (const void *)k_ch_pcg<float> : (const void *)k_ch_pcg<double>;
+  CH_CUDA(cudaFuncSetAttribute(pk, cudaFuncAttributeMaxDynamicSharedMemorySize, mg::kMgStageMax));
+  CH_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, pk, S->mixed ? PcgT<float>::v : PcgT<double>::v,
+                                                        S->mixed ? S->Gf.stage : S->Gd.stage));
   if (per < 1) throw std::runtime_error("pressure-correction kernel cannot be resident");
   S->pcg_grid = per * nsm;
   S->pcg_part = S->alloc<double>((size_t)2 * S->pcg_grid + 64);

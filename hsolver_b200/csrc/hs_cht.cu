@@ -428,7 +428,9 @@ __global__ void k_cht_fill(int n, int Nx, int Ny, double v, double *T) {
 int coop_grid(const void *kernel, int device) {
   int nsm = 0, per = 0;
   HC_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
-  HC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, kBiT, 0));
+  // the V-cycle's staging of block 0's levels: up to kMgStageMax bytes per launch
+  HC_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, mg::kMgStageMax));
+  HC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, kBiT, mg::kMgStageMax));
   if (per < 1) throw std::runtime_error("cooperative kernel cannot be resident");
   return per * nsm;
 }
@@ -492,6 +494,7 @@ void setup_levels(ChtState &C, mg::Hier<MT> &G) {
   }
   G.L = L;
   G.lu = C.alloc<double>((size_t)mg::kMgCoarse * mg::kMgCoarse);
+  mg::plan_stage(G);
 }
 }  // namespace
 
@@ -610,9 +613,9 @@ void cht_get_velocities(ChtState *C, double *ug, double *vg, double *wg) {
 
 namespace {
 template <class K, class... A>
-void launch_coop(K kernel, int blocks, cudaStream_t s, A... args) {
+void launch_coop(K kernel, int blocks, size_t smem, cudaStream_t s, A... args) {
   void *argv[] = {(void *)&args...};
-  HC_CUDA(cudaLaunchCooperativeKernel((void *)kernel, dim3(blocks), dim3(kBiT), argv, 0, s));
+  HC_CUDA(cudaLaunchCooperativeKernel((void *)kernel, dim3(blocks), dim3(kBiT), argv, smem, s));
 }
 
 // operator rows and the fine level of the hierarchy in use (every solve is
@@ -628,12 +631,12 @@ void assemble(ChtState *C) {
 void solve(ChtState *C, const double *rhs, int transpose, double tol, int maxiter, int rel0, double *out_r0) {
   const double *nox = nullptr;
   if (C->precond == 2)
-    launch_coop(k_cht_bicgstab<double, double>, C->grid, C->stream, C->H, C->V, C->Gd, rhs, transpose, tol, maxiter,
+    launch_coop(k_cht_bicgstab<double, double>, C->grid, C->Gd.stage, C->stream, C->H, C->V, C->Gd, rhs, transpose, tol, maxiter,
                 C->partials, C->it, C->res, rel0, out_r0, nox);
   else {
     mg::Hier<float> G = C->Gf;
     if (C->precond == 0) G.L = 0;
-    launch_coop(k_cht_bicgstab<float, double>, C->grid, C->stream, C->H, C->V, G, rhs, transpose, tol, maxiter,
+    launch_coop(k_cht_bicgstab<float, double>, C->grid, G.stage, C->stream, C->H, C->V, G, rhs, transpose, tol, maxiter,
                 C->partials, C->it, C->res, rel0, out_r0, nox);
   }
 }
@@ -644,7 +647,7 @@ void solve_correction(ChtState *C, double tol, int maxiter, double *out_r0) {
   mg::Hier<float> G = C->Gf;
   if (C->precond != 1) G.L = 0;
   const double *x0 = C->T;
-  launch_coop(k_cht_bicgstab<float, float>, C->grid, C->stream, C->H, C->Vf, G, (const double *)C->H.b, 0, tol,
+  launch_coop(k_cht_bicgstab<float, float>, C->grid, G.stage, C->stream, C->H, C->Vf, G, (const double *)C->H.b, 0, tol,
               maxiter, C->partials, C->it, C->res, 1, out_r0, x0);
 }
 

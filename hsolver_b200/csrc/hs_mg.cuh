@@ -21,11 +21,14 @@
 // (black, red, ...) each coarse correction, mirrored so that the cycle stays
 // symmetric for CG; the first red half-sweep (from
 // x = 0) is applied by whoever writes the level's rhs, the prolongation is
-// fused into the first post-smoothing half-sweep.  Levels below kMgSmall cells run inside
-// block 0 alone, separated by __syncthreads instead of grid barriers.
+// fused into the first post-smoothing half-sweep.  The coarse levels (at most kMgSmall
+// cells each, with x and rhs together at most kMgStageMax bytes) run inside block 0
+// alone, separated by __syncthreads instead of grid barriers, with their x and rhs
+// staged in the launch's dynamic shared memory (plan_stage).
 #pragma once
 #include <cooperative_groups.h>
 #include <cstdint>
+#include <stdexcept>
 
 namespace hs {
 namespace mg {
@@ -35,6 +38,7 @@ namespace cg = cooperative_groups;
 constexpr int kMgMaxLv = 16;
 constexpr int kMgCoarse = 64;
 constexpr long long kMgSmall = 2048;
+constexpr int kMgStageMax = 64 * 1024;  // bytes of dynamic shared memory the solvers' kernels accept
 
 template <class M>
 struct Level {
@@ -53,6 +57,9 @@ struct Hier {
   int nswc;  // the same on the coarser levels (0 or 1: one)
   Level<M> lv[kMgMaxLv];
   double *lu;  // kMgCoarse^2: the factors, read back while the inverse is formed
+  int ls;      // first level that block 0 handles alone (plan_stage)
+  int stage;   // bytes of dynamic shared memory holding x and rhs of levels ls..L-1
+  int sx[kMgMaxLv], sr[kMgMaxLv];  // byte offsets of a staged level's x and rhs in it
 };
 
 // Grid-stride walk over an mx x ny x nz box in flat order (m fastest): the
@@ -83,6 +90,39 @@ struct Walk {
   }
   __host__ __device__ __forceinline__ int flat() const { return m + mx * (j + ny * k); }
 };
+
+template <class M>
+__host__ __device__ __forceinline__ bool small(const Level<M> &L) { return (long long)L.nx * L.ny * L.nz <= kMgSmall; }
+
+// Host: the levels that block 0 handles alone, ls..L-1: every level from the
+// first of at most kMgSmall cells on, less the finest of them while their x
+// and rhs (padded layout as in global memory, each array 16-byte aligned)
+// exceed kMgStageMax bytes; the coarsest (<= kMgCoarse cells) always fits.
+// Places those arrays in the launch's dynamic shared memory (G.stage bytes).
+template <class M>
+inline void plan_stage(Hier<M> &G) {
+  G.ls = 0;
+  G.stage = 0;
+  if (G.L < 1) return;
+  auto bytes = [&](int l) {
+    const Level<M> &L = G.lv[l];
+    return ((long long)(L.nx + 2) * (L.ny + 2) * (L.nz + 2) * (long long)sizeof(M) + 15) / 16 * 16;
+  };
+  int ls = 0;
+  while (ls < G.L - 1 && !small(G.lv[ls])) ++ls;
+  long long tot = 0;
+  for (int l = ls; l < G.L; ++l) tot += 2 * bytes(l);
+  while (tot > kMgStageMax && ls < G.L - 1) tot -= 2 * bytes(ls++);
+  if (tot > kMgStageMax) throw std::runtime_error("multigrid: coarsest level exceeds the shared-memory staging");
+  long long off = 0;
+  for (int l = ls; l < G.L; ++l) {
+    G.sx[l] = (int)off;
+    G.sr[l] = (int)(off + bytes(l));
+    off += 2 * bytes(l);
+  }
+  G.ls = ls;
+  G.stage = (int)off;
+}
 
 template <class M>
 __device__ __forceinline__ int idx(const Level<M> &L, int i, int j, int k) {
@@ -116,11 +156,19 @@ __device__ __forceinline__ void row(const Level<M> &L, int q, bool tr, M &d, M (
   }
 }
 
-template <class M>
+// a value of x: from L2 in the grid-wide passes (other blocks wrote it), by a
+// plain load when x is staged in block 0's shared memory (S)
+template <bool S, class M>
+__device__ __forceinline__ M ldx(const M *p) {
+  if constexpr (S) return *p;
+  else return __ldcg(p);
+}
+
+template <class M, bool S = false>
 __device__ __forceinline__ M offsum(const Level<M> &L, const M (&o)[6], const M *x, int q) {
   const int PX = L.nx + 2, PXY = (L.nx + 2) * (L.ny + 2);
-  return o[0] * __ldcg(x + q - 1) + o[1] * __ldcg(x + q + 1) + o[2] * __ldcg(x + q - PX) + o[3] * __ldcg(x + q + PX) +
-         o[4] * __ldcg(x + q - PXY) + o[5] * __ldcg(x + q + PXY);
+  return o[0] * ldx<S>(x + q - 1) + o[1] * ldx<S>(x + q + 1) + o[2] * ldx<S>(x + q - PX) + o[3] * ldx<S>(x + q + PX) +
+         o[4] * ldx<S>(x + q - PXY) + o[5] * ldx<S>(x + q + PXY);
 }
 
 template <class M>
@@ -195,7 +243,7 @@ __device__ __forceinline__ void coarsen(const Level<M> &F, const Level<M> &C, in
 
 // a masked cell has zero couplings on every face (its faces touch a
 // non-unknown), so d == 0 identifies it without reading the mask
-template <class M>
+template <class M, bool S = false>
 __device__ __forceinline__ void smooth(const Level<M> &L, int color, bool tr, int tid, int T) {
   for (Walk w((L.nx + 1) / 2, L.ny, L.nz, tid, T); w.ok(); w.next()) {
     const int j = w.j, k = w.k, i = 2 * w.m + ((j + k + color) & 1);
@@ -203,7 +251,7 @@ __device__ __forceinline__ void smooth(const Level<M> &L, int color, bool tr, in
     const int q = idx(L, i + 1, j + 1, k + 1);
     M d, o[6];
     row(L, q, tr, d, o);
-    const M s = L.rhs[q] + offsum(L, o, L.x, q);
+    const M s = L.rhs[q] + offsum<M, S>(L, o, L.x, q);
     L.x[q] = d == M(0) ? M(0) : s / d;
   }
 }
@@ -287,7 +335,7 @@ __device__ __forceinline__ Seed<M> seed_at(const Level<M> &L, int i, int j, int 
 // them in the same order, so that one memory round trip replaces four
 // (every lane of a warp runs the same number of iterations: the shuffles
 // need the full warp).
-template <class M>
+template <class M, bool S = false>
 __device__ __forceinline__ void restrict_res(const Level<M> &F, const Level<M> &C, bool tr, int tid, int T) {
   if (4LL * C.nx * C.ny * C.nz > T) {
     for (Walk w(C.nx, C.ny, C.nz, tid, T); w.ok(); w.next()) {
@@ -301,7 +349,7 @@ __device__ __forceinline__ void restrict_res(const Level<M> &F, const Level<M> &
             const int q = idx(F, i + 1, j + 1, k + 1);
             M d, o[6];
             row(F, q, tr, d, o);
-            acc += F.rhs[q] - (d * __ldcg(F.x + q) - offsum(F, o, F.x, q));
+            acc += F.rhs[q] - (d * ldx<S>(F.x + q) - offsum<M, S>(F, o, F.x, q));
           }
       const int qc = idx(C, I + 1, J + 1, K + 1);
       const M v = unknown(C, qc) ? acc : M(0);
@@ -325,7 +373,7 @@ __device__ __forceinline__ void restrict_res(const Level<M> &F, const Level<M> &
       const int q = idx(F, i + 1, j + 1, k + 1);
       M d, o[6];
       row(F, q, tr, d, o);
-      v = F.rhs[q] - (d * __ldcg(F.x + q) - offsum(F, o, F.x, q));
+      v = F.rhs[q] - (d * ldx<S>(F.x + q) - offsum<M, S>(F, o, F.x, q));
     }
     const M v1 = __shfl_sync(0xffffffffu, v, g0 + 1), v2 = __shfl_sync(0xffffffffu, v, g0 + 2),
             v3 = __shfl_sync(0xffffffffu, v, g0 + 3);
@@ -348,7 +396,7 @@ __device__ __forceinline__ void restrict_res(const Level<M> &F, const Level<M> &
 // follows recomputes them) and the colour-1 cells' not at all.  Ghost
 // neighbours are 0, as they are never prolonged; a masked neighbour has a
 // zero coupling.  The arithmetic is that of prolongation followed by smooth().
-template <class M>
+template <class M, bool S = false>
 __device__ __forceinline__ void prolong_smooth(const Level<M> &F, const Level<M> &C, bool tr, int tid, int T) {
   const int PX = F.nx + 2, PXY = (F.nx + 2) * (F.ny + 2);
   const int CPX = C.nx + 2, CPXY = (C.nx + 2) * (C.ny + 2);
@@ -362,17 +410,17 @@ __device__ __forceinline__ void prolong_smooth(const Level<M> &F, const Level<M>
     // each axis the other neighbour's parent is P's neighbour on the side of
     // this cell's parity (P -+ 1 for an even / odd index)
     const int qc = idx(C, (i >> 1) + 1, (j >> 1) + 1, (k >> 1) + 1);
-    const M cp = __ldcg(C.x + qc);
-    const M cx = __ldcg(C.x + ((i & 1) ? qc + 1 : qc - 1));
-    const M cy = __ldcg(C.x + ((j & 1) ? qc + CPX : qc - CPX));
-    const M cz = __ldcg(C.x + ((k & 1) ? qc + CPXY : qc - CPXY));
+    const M cp = ldx<S>(C.x + qc);
+    const M cx = ldx<S>(C.x + ((i & 1) ? qc + 1 : qc - 1));
+    const M cy = ldx<S>(C.x + ((j & 1) ? qc + CPX : qc - CPX));
+    const M cz = ldx<S>(C.x + ((k & 1) ? qc + CPXY : qc - CPXY));
     // neighbour values x + x_coarse(parent); ghosts stay 0 (never prolonged)
-    const M xw = i > 0 ? __ldcg(F.x + q - 1) + ((i & 1) ? cp : cx) : M(0);
-    const M xe = i + 1 < F.nx ? __ldcg(F.x + q + 1) + ((i & 1) ? cx : cp) : M(0);
-    const M xs = j > 0 ? __ldcg(F.x + q - PX) + ((j & 1) ? cp : cy) : M(0);
-    const M xn = j + 1 < F.ny ? __ldcg(F.x + q + PX) + ((j & 1) ? cy : cp) : M(0);
-    const M xb = k > 0 ? __ldcg(F.x + q - PXY) + ((k & 1) ? cp : cz) : M(0);
-    const M xf = k + 1 < F.nz ? __ldcg(F.x + q + PXY) + ((k & 1) ? cz : cp) : M(0);
+    const M xw = i > 0 ? ldx<S>(F.x + q - 1) + ((i & 1) ? cp : cx) : M(0);
+    const M xe = i + 1 < F.nx ? ldx<S>(F.x + q + 1) + ((i & 1) ? cx : cp) : M(0);
+    const M xs = j > 0 ? ldx<S>(F.x + q - PX) + ((j & 1) ? cp : cy) : M(0);
+    const M xn = j + 1 < F.ny ? ldx<S>(F.x + q + PX) + ((j & 1) ? cy : cp) : M(0);
+    const M xb = k > 0 ? ldx<S>(F.x + q - PXY) + ((k & 1) ? cp : cz) : M(0);
+    const M xf = k + 1 < F.nz ? ldx<S>(F.x + q + PXY) + ((k & 1) ? cz : cp) : M(0);
     const M off = o[0] * xw + o[1] * xe + o[2] * xs + o[3] * xn + o[4] * xb + o[5] * xf;
     const M s = F.rhs[q] + off;
     F.x[q] = d == M(0) ? M(0) : s / d;
@@ -489,14 +537,13 @@ __device__ __forceinline__ void factor(const Hier<M> &G, bool tr) {
   }
 }
 
-// exact solve on the coarsest level by block 0 (every thread of the block
-// calls it): x = A^-1 rhs with the inverse that factor() left in shared
-// memory, thread r summing row r in column order
+// exact solve on the coarsest level C (G.lv[G.L - 1], or its staged copy) by
+// block 0 (every thread of the block calls it): x = A^-1 rhs with the inverse
+// that factor() left in shared memory, thread r summing row r in column order
 template <class M>
-__device__ __forceinline__ void coarse_solve(const Hier<M> &G) {
+__device__ __forceinline__ void coarse_solve(const Level<M> &C) {
   __shared__ double y[kMgCoarse];
   const double *ainv = lu_smem();
-  const Level<M> &C = G.lv[G.L - 1];
   const int nc = C.nx * C.ny * C.nz, r = threadIdx.x;
   const int q = r < nc ? idx(C, r % C.nx + 1, (r / C.nx) % C.ny + 1, r / (C.nx * C.ny) + 1) : 0;
   if (r < nc) y[r] = (double)C.rhs[q];
@@ -507,9 +554,6 @@ __device__ __forceinline__ void coarse_solve(const Hier<M> &G) {
     C.x[q] = unknown(C, q) ? (M)v : M(0);
   }
 }
-
-template <class M>
-__device__ __forceinline__ bool small(const Level<M> &L) { return (long long)L.nx * L.ny * L.nz <= kMgSmall; }
 
 // build levels 1.. from level 0 and factor the coarsest (the caller filled level 0)
 template <class M>
@@ -528,6 +572,83 @@ __device__ __forceinline__ void build(const Hier<M> &G, bool tr, cg::grid_group 
   grid.sync();
 }
 
+// the launch's dynamic shared memory (Hier::stage bytes)
+__device__ __forceinline__ unsigned char *stage_smem() {
+  extern __shared__ __align__(16) unsigned char mg_stage[];
+  return mg_stage;
+}
+
+// level l (>= G.ls) with x and rhs in the staging area
+template <class M>
+__device__ __forceinline__ Level<M> staged(const Hier<M> &G, int l) {
+  Level<M> L = G.lv[l];
+  L.x = reinterpret_cast<M *>(stage_smem() + G.sx[l]);
+  L.rhs = reinterpret_cast<M *>(stage_smem() + G.sr[l]);
+  return L;
+}
+
+// Levels G.ls.. of the V-cycle, by block 0 alone (every thread of the block
+// calls it), with x and rhs in shared memory: level ls's are copied in (as
+// the grid-wide passes left them: rhs and the seeded x) and its x is copied
+// back at the end; the coarser levels' x start from 0, so that their ghosts
+// are 0 as in global memory.  The arithmetic is that of the grid-wide passes.
+template <class M>
+__device__ __forceinline__ void small_levels(const Hier<M> &G, bool tr) {
+  const int t = threadIdx.x, B = blockDim.x, ls = G.ls;
+  {
+    const Level<M> &Lg = G.lv[ls];
+    const Level<M> Ls = staged(G, ls);
+    const int n = (Lg.nx + 2) * (Lg.ny + 2) * (Lg.nz + 2);
+    for (int e = t; e < n; e += B) {
+      const M xv = __ldcg(Lg.x + e), rv = __ldcg(Lg.rhs + e);
+      Ls.x[e] = xv;
+      Ls.rhs[e] = rv;
+    }
+    for (int l = ls + 1; l < G.L; ++l) {
+      const Level<M> C = staged(G, l);
+      const int nc = (C.nx + 2) * (C.ny + 2) * (C.nz + 2);
+      for (int e = t; e < nc; e += B) C.x[e] = M(0);
+    }
+    __syncthreads();
+  }
+  for (int l = ls; l < G.L - 1; ++l) {
+    const Level<M> F = staged(G, l), C = staged(G, l + 1);
+    const int ns = l == 0 ? G.nsw : G.nswc;
+    smooth<M, true>(F, 1, tr, t, B);
+    __syncthreads();
+    for (int s = 1; s < ns; ++s) {
+      smooth<M, true>(F, 0, tr, t, B);
+      __syncthreads();
+      smooth<M, true>(F, 1, tr, t, B);
+      __syncthreads();
+    }
+    restrict_res<M, true>(F, C, tr, t, B);
+    __syncthreads();
+  }
+  coarse_solve(staged(G, G.L - 1));
+  __syncthreads();
+  for (int l = G.L - 2; l >= ls; --l) {
+    const Level<M> F = staged(G, l), C = staged(G, l + 1);
+    const int ns = l == 0 ? G.nsw : G.nswc;
+    prolong_smooth<M, true>(F, C, tr, t, B);
+    __syncthreads();
+    smooth<M, true>(F, 0, tr, t, B);
+    __syncthreads();
+    for (int s = 1; s < ns; ++s) {
+      smooth<M, true>(F, 1, tr, t, B);
+      __syncthreads();
+      smooth<M, true>(F, 0, tr, t, B);
+      __syncthreads();
+    }
+  }
+  {
+    const Level<M> &Lg = G.lv[ls];
+    const Level<M> Ls = staged(G, ls);
+    const int n = (Lg.nx + 2) * (Lg.ny + 2) * (Lg.nz + 2);
+    for (int e = t; e < n; e += B) Lg.x[e] = Ls.x[e];
+  }
+}
+
 // lv[0].x = V-cycle applied to lv[0].rhs; the caller has written lv[0].rhs
 // and seeded lv[0] (seed_diag / seed_store on every interior cell) before the barrier that
 // precedes this call.  With dot_r, the last level-0 pass also adds this
@@ -537,8 +658,7 @@ __device__ __forceinline__ void build(const Hier<M> &G, bool tr, cg::grid_group 
 template <class M, class RT = double>
 __device__ __forceinline__ bool vcycle(const Hier<M> &G, bool tr, cg::grid_group &grid, int tid, int T,
                        const RT *dot_r = nullptr, double *dot_acc = nullptr) {
-  int ls = 0;  // first level handled by block 0 alone
-  while (ls < G.L - 1 && !small(G.lv[ls])) ++ls;
+  const int ls = G.ls;  // first level handled by block 0 alone
   for (int l = 0; l < ls; ++l) {
     smooth(G.lv[l], 1, tr, tid, T);
     grid.sync();
@@ -551,35 +671,7 @@ __device__ __forceinline__ bool vcycle(const Hier<M> &G, bool tr, cg::grid_group
     restrict_res(G.lv[l], G.lv[l + 1], tr, tid, T);
     grid.sync();
   }
-  if (blockIdx.x == 0) {
-    const int t = threadIdx.x, B = blockDim.x;
-    for (int l = ls; l < G.L - 1; ++l) {
-      smooth(G.lv[l], 1, tr, t, B);
-      __syncthreads();
-      for (int s = 1; s < (l == 0 ? G.nsw : G.nswc); ++s) {
-        smooth(G.lv[l], 0, tr, t, B);
-        __syncthreads();
-        smooth(G.lv[l], 1, tr, t, B);
-        __syncthreads();
-      }
-      restrict_res(G.lv[l], G.lv[l + 1], tr, t, B);
-      __syncthreads();
-    }
-    coarse_solve(G);
-    __syncthreads();
-    for (int l = G.L - 2; l >= ls; --l) {
-      prolong_smooth(G.lv[l], G.lv[l + 1], tr, t, B);
-      __syncthreads();
-      smooth(G.lv[l], 0, tr, t, B);
-      __syncthreads();
-      for (int s = 1; s < (l == 0 ? G.nsw : G.nswc); ++s) {
-        smooth(G.lv[l], 1, tr, t, B);
-        __syncthreads();
-        smooth(G.lv[l], 0, tr, t, B);
-        __syncthreads();
-      }
-    }
-  }
+  if (blockIdx.x == 0) small_levels(G, tr);
   grid.sync();
   for (int l = ls - 1; l >= 0; --l) {
     prolong_smooth(G.lv[l], G.lv[l + 1], tr, tid, T);

@@ -103,6 +103,29 @@ def test_batched_steps_match_single_steps(precision):
 
 
 @pytest.mark.parametrize("precision", [0, 1])
+def test_steps_reproducible_bit_for_bit(precision):
+    """Two solvers on the 256x128x128 channel with 8 seeded blocks give the
+    same fields bit for bit after 30 outer steps (reductions in a fixed
+    order, no atomics, and no pass that reads what another thread of the
+    same pass writes: in the mixed form the velocity correction reads u* =
+    u^n + delta while it replaces u^n, so the outlet face takes its upstream
+    u* from the thread of that face)."""
+    import bench
+    import hsolver_b200
+    deck, re_, k, q, _ = bench.workload("config2")
+    out = []
+    for _ in range(2):
+        g = hsolver_b200.Channel(deck, re=re_, precision=precision, **bench.SOLVER)
+        g.set_solid(k, q)
+        g.init()
+        g.step(30)
+        out.append({f: g.field(f) for f in FACE + ["p", "T"]})
+        g.close()
+    for f in FACE + ["p", "T"]:
+        assert np.array_equal(out[0][f], out[1][f]), f
+
+
+@pytest.mark.parametrize("precision", [0, 1])
 def test_v_cycle_sweep_count_changes_only_the_path(precision):
     """The p' V-cycle's sweep count (p_mg_sweeps; the coarser levels take one
     more) is a preconditioner setting: with 1, the default (2) and 3 sweeps
