@@ -1275,8 +1275,9 @@ void ch_adjoint(ChannelState *S, double tol, int maxiter, double *J, double *dJd
   CH_CUDA(cudaEventRecord(e0, S->stream));
   cht_forward(S->cht, nullptr, J, fwd_iters, &rel);
   CH_CUDA(cudaEventRecord(e1, S->stream));
-  cht_adjoint(S->cht, dJdq, dJdk, adj_iters, &rel);
-  CH_CUDA(cudaEventRecord(e2, S->stream));
+  // the adjoint's time ends with the gradients on the device: their copies
+  // to the host are left out, as the forward's T stays on the device
+  cht_adjoint(S->cht, dJdq, dJdk, adj_iters, &rel, e2);
   CH_CUDA(cudaEventSynchronize(e2));
   float a = 0, b = 0;
   CH_CUDA(cudaEventElapsedTime(&a, e0, e1));

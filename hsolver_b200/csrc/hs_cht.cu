@@ -698,7 +698,7 @@ void cht_forward(ChtState *C, double *T_host, double *J, int *iters, double *rel
   if (relres) *relres = rr;
 }
 
-void cht_adjoint(ChtState *C, double *dJdq_host, double *dJdk_host, int *iters, double *relres) {
+void cht_adjoint(ChtState *C, double *dJdq_host, double *dJdk_host, int *iters, double *relres, void *device_done) {
   HC_CUDA(cudaSetDevice(C->device));
   if (!C->have_T) throw std::logic_error("adjoint before forward solve");
   const ChtDev &H = C->H;
@@ -709,6 +709,7 @@ void cht_adjoint(ChtState *C, double *dJdq_host, double *dJdk_host, int *iters, 
   solve(C, C->g, 1, C->tol, C->maxiter, 0, nullptr);
   HC_CUDA(cudaMemcpyAsync(C->lam, C->V.x, np * 8, cudaMemcpyDeviceToDevice, C->stream));
   k_cht_grad<<<gfor(n), kB, 0, C->stream>>>(H, C->T, C->lam, C->Tb, C->dJdq, C->dkc);
+  if (device_done) HC_CUDA(cudaEventRecord((cudaEvent_t)device_done, C->stream));
   std::vector<double> dq(n), dk(n);
   int it = 0;
   double rr = 0;

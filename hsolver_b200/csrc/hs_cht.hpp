@@ -35,7 +35,10 @@ void cht_set_solid(ChtState *c, double k_fluid, const double *k_region, const do
 void cht_set_velocities(ChtState *c, const ChtVelSrc &src);
 void cht_get_velocities(ChtState *c, double *ug, double *vg, double *wg);
 void cht_forward(ChtState *c, double *T_host, double *J, int *iters, double *relres);
-void cht_adjoint(ChtState *c, double *dJdq_host, double *dJdk_host, int *iters, double *relres);
+// device_done: a cudaEvent_t recorded on the solver's stream once the
+// gradients are on the device, before their copies to the host (or null)
+void cht_adjoint(ChtState *c, double *dJdq_host, double *dJdk_host, int *iters, double *relres,
+                 void *device_done = nullptr);
 // channel use: the owner's device face velocities, T = v everywhere, one relaxed
 // energy step (BiCGStab from the current T to tol * ||r0||, T += alpha (T~ - T);
 // with step_fp32, BiCGStab for the correction d = T~ - T from 0 in FP32 vectors,

@@ -305,7 +305,10 @@ int hs_channel_device_bytes(hs_channel *h, long long *bytes);
  * T = t_in to ||r|| / ||b|| < tol, then the adjoint.  J = (sum over solid
  * cells of T^8 dV)^(1/8); dJdq per cell (n = Nx*Ny*Nz), dJdk per block
  * (derivative with respect to the block's conductivity k_solid).  Both
- * timings are CUDA-event times on the solver's stream.  The outer loop's
+ * timings are CUDA-event times on the solver's stream: fwd_ms the forward
+ * solve with J, adj_ms from there until dJ/dT, the transposed solve and the
+ * per-cell gradients are done on the device (the copies of dJdq and dJdk to
+ * the host excluded, as the forward's T is not copied).  The outer loop's
  * temperature is left as it was. */
 typedef struct hs_adjoint_info {
   int fwd_iters, adj_iters;
