@@ -286,7 +286,8 @@ def run_gpu(args):
         J, dq, dk, info = g.adjoint(tol=1e-8)
         adj = {"J": J, "fwd_iters": info["fwd_iters"], "adj_iters": info["adj_iters"], "fwd_ms": info["fwd_ms"],
                "adj_ms": info["adj_ms"], "adjoint_over_forward": info["adj_ms"] / info["fwd_ms"],
-               "note": "forward energy solve from T = t_in to rtol 1e-8, then the transposed solve; CUDA events"}
+               "note": "forward energy solve from T = t_in to rtol 1e-8, then the transposed solve to the "
+                       "gradients on the device (their copies to the host excluded); CUDA events"}
     g.close()
 
     # end to end through the public API with pinned host buffers: a fresh
