@@ -16,14 +16,21 @@ relaxation; the stop test includes the FP64 energy residual.)  Synthetic input g
 in-repo; the state (~790 MB on the device) is larger than L2.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
-                  [--residual] [--no-cpu-baseline] [--no-variants]
+                  [--no-cpu-baseline] [--no-variants]
+  python bench.py --probe NAME [--steps K] [--mixed] [--p-tol X] [--t-tol X]
 
 Prints one JSON line.  Variants on the same GPU: the mixed-precision form,
 the adjoint/forward cost of the energy gradient, wall time to a global
-residual of 1e-6 (config 1 by default, also the 256x128x128 case with
---residual), and the reference-faithful lid-cavity step on the same grid.
-`--impl reference` times the CPU restatement (oracle/, FP64, one thread) on a
-bounded sample of the same workload.
+residual of 1e-6 (the 256x128x128 case, config 1 and config 3; the first is
+also `time_to_1e-6` and `speedup_mixed` at the top level), the
+reference-faithful lid-cavity step on the same grid, the reference's own
+compiled code against the GPU on the reference's deck (`like_for_like`),
+and the 512x256x256 case.  `--gpus N` > 1 without a launcher reruns itself
+under torch.distributed.run with N ranks (independent replicas, one per
+GPU).  `--impl reference` times the CPU restatement (oracle/, FP64, OpenMP on
+every host thread, the count in cpu_baseline.cores) on 1-2 outer steps of the
+same workload with the reference's inner-solver settings; it loads no part
+of the CUDA library.
 """
 import argparse
 import ctypes
@@ -69,12 +76,19 @@ LAUNCHES_PER_STEP = 11
 PCG_TRAFFIC_PER_ITER = 18.12e9 / 8
 
 
-def workload(name=NAME, seed=0):
-    import hsolver_b200
+def workload(name=NAME, seed=0, host_side=False):
+    """The seeded deck of a configuration, its Reynolds number, the k ratio
+    per block and q per cell.  The cell types come from the product's case
+    model (hs_case_*), or from the oracle's when host_side is set: the CPU
+    arms load no part of the CUDA library."""
     from hsolver_b200 import cases
     deck = cases.CONFIGS[name](seed) if name in ("config2", "config4", "config5") else cases.CONFIGS[name]()
-    c = hsolver_b200.Case(deck)
-    ctype, region = c.cell_types()
+    if host_side:
+        from oracle import oracle
+        ctype, region = oracle.OracleCase(deck).cell_types()
+    else:
+        import hsolver_b200
+        ctype, region = hsolver_b200.Case(deck).cell_types()
     re_, k, q = cases.block_physics(name, ctype, region, seed)
     return deck, re_, k, q, ctype
 
@@ -342,6 +356,7 @@ def run_gpu(args):
         variants["adjoint"] = adj
         variants["time_to_residual"] = time_to_residual(args, hsolver_b200, local)
         variants["reference_physics"] = reference_physics(args, torch, hsolver_b200, local, dist)
+        variants["like_for_like"] = like_for_like(torch, hsolver_b200, local)
         variants["config5"] = config5(torch, hsolver_b200, local)
 
     if rank == 0:
@@ -372,6 +387,15 @@ def run_gpu(args):
             "variants": variants,
             "clocks": clk,
         }
+        ttr = variants.get("time_to_residual", {}).get(NAME)
+        if ttr:
+            # the specification's headline: wall time to a global residual of
+            # 1e-6 on this case, FP64 and mixed, and their ratio
+            out["time_to_1e-6"] = {"fp64_s": ttr["fp64"]["seconds"], "mixed_s": ttr["mixed"]["seconds"],
+                                   "steps": [ttr["fp64"]["steps"], ttr["mixed"]["steps"]],
+                                   "converged": [ttr["fp64"]["converged"], ttr["mixed"]["converged"]],
+                                   "mixed_vs_fp64_rel_l2": ttr["mixed_vs_fp64_rel_l2"]}
+            out["speedup_mixed"] = ttr.get("speedup_mixed")
         if not args.no_cpu_baseline:
             out["cpu_baseline"] = cpu_baseline()
         print(json.dumps(out), flush=True)
@@ -381,13 +405,13 @@ def run_gpu(args):
 
 def time_to_residual(args, hsolver_b200, local):
     """Wall time of hs_channel_solve_to(1e-6) for the FP64 and mixed forms, and
-    the per-field relative L2 difference of the two converged states: config 1
+    the per-field relative L2 difference of the two converged states: the
+    bench case (256x128x128, the specification's target), config 1
     (48x24x24) and config 3 (the same on a tanh-stretched grid, maximum cell
-    aspect ratio 20: the mixed-precision configuration) always, the
-    256x128x128 case with --residual."""
+    aspect ratio 20: the mixed-precision configuration)."""
     import numpy as np
     out = {}
-    cases_ = [("config1", 2000), ("config3", 3000)] + ([(NAME, args.residual_max)] if args.residual else [])
+    cases_ = [(NAME, args.residual_max), ("config1", 2000), ("config3", 3000)]
     for name, cap in cases_:
         deck, re_, k, q, _ = workload(name)
         res, fields = {}, {}
@@ -463,7 +487,64 @@ def reference_physics(args, torch, hsolver_b200, local, dist):
             "value": args.steps / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms / args.steps}
 
 
-CPU_SAMPLE_P, CPU_SAMPLE_T = 20, 1
+REF_DRIVER = os.path.join(HERE, "oracle", "_ref", "ref_driver")
+DECKS = os.path.join(HERE, "tests", "golden", "decks")
+
+
+def like_for_like(torch, hsolver_b200, local, deck_name="example13", steps=3):
+    """The reference's own code against the GPU on one computation: the
+    reference's lid-cavity SIMPLE step (its FluidSolver / MobSolver / Solver
+    sources compiled single-rank against the in-repo MPI / HYPRE shims,
+    oracle/_ref/ref_driver, one host core) and the reference-faithful GPU
+    step (hs_step), which reproduces it bit for bit without the pressure
+    solve and to 1e-9 with it, on the reference's own deck, the same outer
+    steps from the initial state.  The CPU time per step is the reference's
+    clock() measurement (solver.h:51-58) around the loop body of
+    Solver::solve (solver.h:55-154); the GPU's by CUDA events."""
+    import tempfile
+    deck_path = os.path.join(DECKS, deck_name + ".in")
+    if not os.path.exists(REF_DRIVER):
+        return {"unavailable": "oracle/_ref/ref_driver not built (needs the reference tree at build time)"}
+    with tempfile.TemporaryDirectory() as work:
+        r = subprocess.run([REF_DRIVER, deck_path, os.path.join(work, "wd"), "-", "time:%d" % steps],
+                           capture_output=True, text=True, timeout=900)
+    if r.returncode != 0:
+        return {"unavailable": "ref_driver exited %d" % r.returncode}
+    ref = json.loads(r.stdout.strip().splitlines()[-1])
+    with open(deck_path) as f:
+        g = hsolver_b200.Solver(f.read(), device=local)
+    g.init()
+    stream = torch.cuda.ExternalStream(g.stream(), device=local)
+    gpu_ms, its = [], []
+    for _ in range(steps):
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        st = g.step(1, stats=True)
+        e1.record(stream)
+        e1.synchronize()
+        gpu_ms.append(e0.elapsed_time(e1))
+        its.append(st["pcg_iters"])
+    g.close()
+    cpu_s = [s["clock_s"] for s in ref["steps"]]
+    return {"deck": deck_name + ".in (the reference's own deck)", "steps": steps,
+            "reference_cpu_s_per_step": cpu_s, "reference_wall_s_per_step": [s["wall_s"] for s in ref["steps"]],
+            "reference_pcg_iters": [s["pcg_iters"] for s in ref["steps"]], "reference_cores": 1,
+            "reference_setup_s": ref["setup_s"], "gpu_ms_per_step": gpu_ms, "gpu_pcg_iters": its,
+            "speedup": (sum(cpu_s) * 1e3) / sum(gpu_ms),
+            "parity": "GPU state bit-identical to the reference's without the pressure solve, rel. L2 <= 1e-9 with it "
+                      "(tests/test_gpu_parity.py, tests/test_oracle_golden.py)"}
+
+
+# The CPU step's inner solves as the reference configures its own: the p'
+# system by CG without a preconditioner to rtol 1e-5 with at most 1000
+# iterations (HYPRE PCG, fluid_solver.h:1871-1875), the energy to the GPU
+# step's 0.5 reduction with at most 100 iterations (the reference's sweep cap
+# for its energy Gauss-Seidel, fluid_solver.h:794-881).  The tolerances are
+# the GPU step's; the CPU's solvers are the reference's, so the iteration
+# counts differ and the ratio measures solver and hardware together.
+CPU_SOLVER = {"p_tol": 1e-5, "p_maxiter": 1000, "t_tol": 0.5, "t_maxiter": 100}
 
 
 def cpu_threads():
@@ -473,38 +554,55 @@ def cpu_threads():
     return int(L.or_threads())
 
 
-def cpu_sample():
-    """The FP64 C oracle (OpenMP on all host threads) on one outer step of the
-    same case, after init, with the inner solves capped (CG 20, BiCGStab 1
-    iteration)."""
+def cpu_case():
+    """The bench case on the FP64 C oracle (OpenMP on every host thread),
+    initialised; classification by the oracle (no CUDA library is loaded)."""
     from oracle import oracle
-    deck, re_, k, q, _ = workload()
-    o = oracle.ChannelCase(deck, re=re_, **dict(SOLVER, p_maxiter=CPU_SAMPLE_P, t_maxiter=CPU_SAMPLE_T))
+    deck, re_, k, q, _ = workload(host_side=True)
+    o = oracle.ChannelCase(deck, re=re_, **CPU_SOLVER)
     o.set_solid(k, q)
     o.init()
-    t0 = time.perf_counter()
-    o.step(1)
-    return time.perf_counter() - t0
+    return o
+
+
+def cpu_steps(o, n):
+    """Seconds of each of n outer steps and the solver iterations they took."""
+    dts, its = [], []
+    for _ in range(n):
+        t0 = time.perf_counter()
+        o.step(1)
+        dts.append(time.perf_counter() - t0)
+        st = o.stats()
+        its.append([st["pcg_iters"], st["t_iters"]])
+    return dts, its
+
+
+CPU_SAMPLE_NOTE = ("outer steps of the bench case from the initial state by the FP64 C oracle (OpenMP, %d threads): "
+                   "the same discretisation and outer step as the GPU, with the reference's inner solvers (p' by CG "
+                   "without preconditioner, rtol 1e-5, at most 1000 iterations, fluid_solver.h:1871-1875; energy by "
+                   "Jacobi BiCGStab to 0.5, at most 100 iterations); (p', energy) iterations per step %s")
 
 
 def cpu_baseline():
-    dt = cpu_sample()
-    return {"value": 1.0 / dt, "unit": UNIT, "cores": cpu_threads(), "kind": "port",
-            "sample": "1 outer step of the bench case by the FP64 C oracle (OpenMP, %d threads) with the inner "
-                      "solves capped at %d CG and %d BiCGStab iterations (unpreconditioned; reaching the GPU's "
-                      "p' tolerance takes ~1000 CG iterations), %.1f s: an upper bound on the CPU rate"
-                      % (cpu_threads(), CPU_SAMPLE_P, CPU_SAMPLE_T, dt)}
+    o = cpu_case()
+    dts, its = cpu_steps(o, 1)
+    return {"value": 1.0 / dts[0], "unit": UNIT, "cores": cpu_threads(), "kind": "port",
+            "sample": "1 of the " + CPU_SAMPLE_NOTE % (cpu_threads(), its), "seconds": dts}
 
 
 def run_reference(args):
     """CPU arm: the channel step restated in C (oracle/), the only CPU
     implementation of this physics (the reference solves a lid cavity with
-    no inlet, heat source or conductivity ratio)."""
+    no inlet, heat source or conductivity ratio), with the reference's own
+    inner-solver settings; a bounded sample of 1-2 outer steps (about 20-40 s
+    each on the host) from the initial state.  Under torchrun only rank 0
+    runs it."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     steps = max(1, min(args.steps, 2))
-    dts = [cpu_sample() for _ in range(steps)]
+    o = cpu_case()
+    dts, its = cpu_steps(o, steps)
     dt = sum(dts)
     v = steps / dt
     print(json.dumps({
@@ -512,24 +610,112 @@ def run_reference(args):
         "ms_per_step": 1e3 * dt / steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic (seeded in-repo case generator)", "config": CONFIG, "impl": "reference",
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": cpu_threads(), "kind": "port",
-                         "sample": "%d x 1 outer step after init, inner solves capped at %d CG / %d BiCGStab "
-                                   "iterations (an upper bound on the CPU rate)" % (steps, CPU_SAMPLE_P, CPU_SAMPLE_T)},
+                         "sample": "%d " % steps + CPU_SAMPLE_NOTE % (cpu_threads(), its), "seconds": dts},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }), flush=True)
 
 
-def main():
+def probe(args):
+    """A few outer steps of one case on one GPU, printing the p' and energy
+    iterations of every step: the command the profiles name (ncu runs it on a
+    small case).  NAME: config1 .. config5 (the seeded configurations with
+    their block physics; config2 is the bench case), `reference` (the
+    reference-faithful lid-cavity step on the 256x128x128 grid), or
+    NXxNYxNZ:K (a 2x1x1 channel with K seeded blocks of edges 8-20, seed 1,
+    the bench case's block physics)."""
+    import hsolver_b200
+    from hsolver_b200 import cases
+    t0 = time.perf_counter()
+    if args.probe == "reference":
+        g = hsolver_b200.Solver(cases.config2(seed=0))
+        g.init()
+        st = g.step(args.steps, stats=True)
+        g.sync()
+        print("ok reference steps %d pcg_iters %d (%.2f s)" % (args.steps, st["pcg_iters"], time.perf_counter() - t0))
+        return
+    if args.probe in cases.CONFIGS:
+        deck, re_, k, q, _ = workload(args.probe)
+    else:
+        dims, nb = args.probe.split(":")
+        nx, ny, nz = (int(v) for v in dims.split("x"))
+        deck = cases.channel(nx, ny, nz, cases.place_blocks((nx, ny, nz), int(nb), 8, 20, seed=1))
+        ctype, region = hsolver_b200.Case(deck).cell_types()
+        re_, k, q = cases.block_physics("config2", ctype, region)
+    kw = {}
+    if args.p_tol is not None:
+        kw["p_tol"] = args.p_tol
+    if args.t_tol is not None:
+        kw["t_tol"] = args.t_tol
+    if args.t_maxiter is not None:
+        kw["t_maxiter"] = args.t_maxiter
+    g = hsolver_b200.Channel(deck, re=re_, precision=hsolver_b200.PREC_MIXED if args.mixed else hsolver_b200.PREC_FP64,
+                             **kw)
+    g.set_solid(k, q)
+    g.init()
+    its = []
+    for _ in range(args.steps):
+        st = g.step(1)
+        its.append((st["pcg_iters"], st["t_iters"]))
+    g.sync()
+    print("ok channel %s steps %d (pcg, energy) iterations per step %s (%.2f s)"
+          % (args.probe, args.steps, its, time.perf_counter() - t0))
+
+
+def replica_check(args):
+    """The replica plumbing on the host: every rank joins a gloo group and
+    rank 0 prints the max over ranks of 10 + rank (what the N-GPU bench does
+    with its event times), with the world size."""
+    import datetime
+    import torch
+    import torch.distributed as dist
+    dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=60))
+    rank, world = dist.get_rank(), dist.get_world_size()
+    v = max_over_ranks(torch, dist, 10.0 + rank)
+    if rank == 0:
+        print(json.dumps({"replica_check": True, "n_gpus": world, "max_ms": v}), flush=True)
+    dist.destroy_process_group()
+
+
+def spawn_replicas(args, argv):
+    """--gpus N > 1 without a launcher: rerun this command under
+    torch.distributed.run with N ranks on this node (127.0.0.1, a free port),
+    one per GPU; rank 0 prints the JSON line.  Returns the launcher's exit
+    status."""
+    import socket
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", str(args.gpus),
+           "--master-addr", "127.0.0.1", "--master-port", str(port), os.path.abspath(__file__)] + list(argv)
+    return subprocess.run(cmd).returncode
+
+
+def main(argv=None):
+    argv = sys.argv[1:] if argv is None else argv
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="native", choices=["native", "reference"])
-    ap.add_argument("--residual", action="store_true", help="also time the 256x128x128 case to a residual of 1e-6")
-    ap.add_argument("--residual-max", type=int, default=4000)
+    ap.add_argument("--residual-max", type=int, default=4000,
+                    help="outer-step cap of the 256x128x128 time-to-residual runs")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-variants", action="store_true")
-    args = ap.parse_args()
-    if args.impl == "reference":
+    ap.add_argument("--probe", default=None, metavar="NAME", help="run a few steps of one case (see probe())")
+    ap.add_argument("--mixed", action="store_true", help="--probe: the mixed-precision form")
+    ap.add_argument("--p-tol", type=float, default=None, help="--probe: p' relative tolerance")
+    ap.add_argument("--t-tol", type=float, default=None, help="--probe: energy relative tolerance")
+    ap.add_argument("--t-maxiter", type=int, default=None, help="--probe: energy iteration cap")
+    ap.add_argument("--replica-check", action="store_true", help=argparse.SUPPRESS)
+    args = ap.parse_args(argv)
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ and args.probe is None:
+        sys.exit(spawn_replicas(args, argv))
+    if args.replica_check:
+        replica_check(args)
+    elif args.probe is not None:
+        probe(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_gpu(args)

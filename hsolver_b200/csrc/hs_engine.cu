@@ -1971,10 +1971,15 @@ void pcg_solve(PcgWork *w, const double *acx, const double *acy, const double *a
 // calls may synchronise the device and stall work queued on other streams.
 // pcg_solve_noalloc serves them: the same CG kernel as pcg_solve, with its
 // scratch (four padded vectors, the reduction partials and the two result
-// words) in this file-scope array.  It is loaded with the library and held by
-// every GPU that loads it until the process exits (8.06 MiB per device).
-// Every call shares the array: calls that overlap on the GPU race, so a
-// caller issuing from several streams or threads must serialise them.
+// words) in this file-scope array.  It is part of the library's device code,
+// which the runtime loads on a device at the library's first use there (lazy
+// loading: the first call of this function does it when no other kernel of
+// the library has run on that device), and every GPU that loaded it holds it
+// until the process exits (8.06 MiB per device).  The address looked up below
+// is kept per device for the life of the process, so a cudaDeviceReset in
+// between is not supported.  Every call shares the array: calls that overlap
+// on the GPU race, so a caller issuing from several streams or threads must
+// serialise them.
 constexpr long long kNoAllocMaxPad = 1LL << 18;  // padded cells (nx+2)(ny+2)(nz+2)
 constexpr int kNoAllocMaxBlocks = 4096;           // cooperative grid limit for the partials
 constexpr long long kNoAllocDoubles = 4 * kNoAllocMaxPad + 2 * kNoAllocMaxBlocks + 2;

@@ -478,8 +478,10 @@ __device__ __forceinline__ void factor(const Hier<M> &G, bool tr) {
   __syncthreads();
   for (int col = 0; col < nc; ++col) {
     if (threadIdx.x < 32) {
+      // br starts at the diagonal: a column with no comparable |a| (every
+      // entry NaN) keeps its own row, so the swap below stays in the matrix
       double bv = -1.0;
-      int br = nc;
+      int br = col;
       for (int r = col + threadIdx.x; r < nc; r += 32) {
         const double v = fabs(a[r * nc + col]);
         if (v > bv || (v == bv && r < br)) { bv = v; br = r; }

@@ -189,9 +189,17 @@ void hs_pcg_destroy(hs_pcg *h);
  * array of 8.06 MiB that every GPU loading the library holds until exit.
  * Limit: (nx+2)(ny+2)(nz+2) <= 262144 padded cells; larger grids return
  * HS_ERR_ARG.  The first call on a device looks up the array's device
- * address; make that first call before any stream capture.  All calls share
- * the array, so calls that overlap on the GPU race: serialise them.  It
- * allocates nothing: no cudaMalloc, no cudaFree. */
+ * address; make that first call before any stream capture.  The array
+ * belongs to the library's device code, which the CUDA runtime loads on a
+ * device when the library is first used there (lazy module loading): if no
+ * other solve of this library has run on the device, that first call is
+ * what loads it, so make one call (or any other solve of this library)
+ * before the region that must not allocate.  The looked-up address is kept
+ * for the life of the process: a cudaDeviceReset in between is not
+ * supported.  Each call returns after its iteration count and residual have
+ * reached the host.  All calls share the array, so calls that overlap on the
+ * GPU race: serialise them.  It allocates nothing: no cudaMalloc, no
+ * cudaFree. */
 int hs_pcg_solve_noalloc(int nx, int ny, int nz, const double *acx, const double *acy, const double *acz,
                          const double *b, double *x, double tol, int maxiter, void *stream, int *iters, double *relres);
 

@@ -3,6 +3,7 @@
 //
 //   ref_driver <deck.in> <workdir> <out_prefix> <step,step,...>   per-step dumps
 //   ref_driver <deck.in> <workdir> <out_prefix> solver            Solver::solve() (100 steps)
+//   ref_driver <deck.in> <workdir> - time:N                       N outer steps, timed
 //
 // The deck is decomposed with nParts = 1 (decompose.cpp:8 uses 4), the
 // processor0/ files are written into <workdir> and read back exactly like
@@ -11,7 +12,9 @@
 #include <unistd.h>
 #include <sys/stat.h>
 #include <cstdio>
+#include <chrono>
 #include <cstring>
+#include <ctime>
 #include <set>
 #include <string>
 #include <vector>
@@ -81,6 +84,22 @@ static void dump(const std::string &path, Solver &s, int pcg_iters) {
   std::fclose(f);
 }
 
+// one pass of the loop body of Solver::solve (solver.h:55-154), single rank:
+// the fluid's and the solids' interface messages are self-messages.
+static void one_step(Solver &solver) {
+  for (auto *e : solver.fluids) e->solve();
+  for (auto *e : solver.mobs) e->solve();
+  std::vector<double> fsend, ssend;
+  for (auto *e : solver.fluids) for (auto &kv : e->t_boundary) for (auto a : kv.second) fsend.push_back(e->t_temp[a]);
+  for (auto *e : solver.mobs) for (auto &kv : e->t_boundary) for (auto a : kv.second) ssend.push_back(e->t_temp[a]);
+  size_t n = 0;
+  for (auto *e : solver.fluids) for (auto &kv : e->t_halo) for (auto a : kv.second) e->t_temp[a] = ssend.at(n++);
+  n = 0;
+  for (auto *e : solver.mobs) for (auto &kv : e->t_halo) for (auto a : kv.second) e->t_temp[a] = fsend.at(n++);
+  for (auto *e : solver.fluids) e->setForNext();
+  for (auto *e : solver.mobs) e->setForNext();
+}
+
 int main(int argc, char **argv) {
   if (argc < 5) { std::fprintf(stderr, "usage: %s deck workdir out_prefix steps|solver\n", argv[0]); return 2; }
   char deck[4096];
@@ -90,6 +109,7 @@ int main(int argc, char **argv) {
   mkdir(argv[2], 0755);
   if (chdir(argv[2])) { std::perror(argv[2]); return 2; }
   MPI_Init(&argc, &argv);
+  const auto s0 = std::chrono::steady_clock::now();
   {
     StructuredMesh mesh(deck);
     std::vector<std::vector<I64>> fR, mR;
@@ -106,9 +126,31 @@ int main(int argc, char **argv) {
     solver.addFluids(new FluidSolver(dm, dm.fluidMetadata[kv.first], dm.p[kv.first], dm.ux[kv.first], dm.uy[kv.first], dm.uz[kv.first]));
   for (auto &kv : dm.solidMetadata)
     solver.addMobs(new MobSolver(dm, dm.solidMetadata[kv.first], dm.mt[kv.first], dm.mx[kv.first], dm.my[kv.first], dm.mz[kv.first]));
+  const double setup_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - s0).count();
   if (std::string(argv[4]) == "solver") {
     solver.solve();
     dump(outp + ".solver.bin", solver, hs_shim_last_pcg_iters());
+    return 0;
+  }
+  if (std::string(argv[4]).rfind("time:", 0) == 0) {
+    // the loop body of Solver::solve (solver.h:55-154) timed per step, by
+    // clock() as solver.h:51-58 does and by the wall clock; one JSON line
+    const int n = std::stoi(std::string(argv[4]).substr(5));
+    const auto w0 = std::chrono::steady_clock::now();
+    for (auto *e : solver.fluids) e->init();
+    for (auto *e : solver.mobs) e->init();
+    const double init_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - w0).count();
+    std::printf("{\"setup_s\": %.6f, \"init_s\": %.6f, \"steps\": [", setup_s, init_s);
+    for (int step = 1; step <= n; ++step) {
+      const clock_t c0 = clock();
+      const auto t0 = std::chrono::steady_clock::now();
+      one_step(solver);
+      const double cpu = double(clock() - c0) / CLOCKS_PER_SEC;
+      const double wall = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+      std::printf("%s{\"clock_s\": %.6f, \"wall_s\": %.6f, \"pcg_iters\": %d}", step > 1 ? ", " : "", cpu, wall,
+                  hs_shim_last_pcg_iters());
+    }
+    std::printf("]}\n");
     return 0;
   }
   std::set<int> want;
@@ -118,19 +160,7 @@ int main(int argc, char **argv) {
   for (auto *e : solver.mobs) e->init();
   if (want.count(0)) dump(outp + ".step0.bin", solver, 0);
   for (int step = 1; step <= last; ++step) {
-    // one pass of the loop body of Solver::solve (solver.h:55-154), single rank:
-    // the fluid's and the solids' interface messages are self-messages.
-    for (auto *e : solver.fluids) e->solve();
-    for (auto *e : solver.mobs) e->solve();
-    std::vector<double> fsend, ssend;
-    for (auto *e : solver.fluids) for (auto &kv : e->t_boundary) for (auto a : kv.second) fsend.push_back(e->t_temp[a]);
-    for (auto *e : solver.mobs) for (auto &kv : e->t_boundary) for (auto a : kv.second) ssend.push_back(e->t_temp[a]);
-    size_t n = 0;
-    for (auto *e : solver.fluids) for (auto &kv : e->t_halo) for (auto a : kv.second) e->t_temp[a] = ssend.at(n++);
-    n = 0;
-    for (auto *e : solver.mobs) for (auto &kv : e->t_halo) for (auto a : kv.second) e->t_temp[a] = fsend.at(n++);
-    for (auto *e : solver.fluids) e->setForNext();
-    for (auto *e : solver.mobs) e->setForNext();
+    one_step(solver);
     if (want.count(step)) dump(outp + ".step" + std::to_string(step) + ".bin", solver, hs_shim_last_pcg_iters());
   }
   return 0;

@@ -10,9 +10,10 @@ with `make -C oracle/ref`) on every deck in tests/golden/decks and stores:
   and the PCG iteration count for larger decks, where full arrays would not
   be small fixtures.
 
-Needs the reference tree (default /root/reference); run it in the build
-container, never on the GPU box.  Usage: python tests/golden/make_golden.py
-[--only DECK] (one deck's digests, merged into the existing file).
+Needs the reference tree, named by the REF environment variable when the
+driver is not built yet; run it where that tree is, never on the GPU box.
+Usage: REF=<reference tree> python tests/golden/make_golden.py [--only DECK]
+(one deck's digests, merged into the existing file).
 """
 import hashlib
 import json
@@ -58,7 +59,10 @@ def digest_entries(res):
 
 def main():
     if not os.path.exists(DRIVER):
-        subprocess.run(["make", "-C", os.path.join(REPO, "oracle", "ref")], check=True)
+        ref = os.environ.get("REF")
+        if not ref:
+            sys.exit("set REF to the reference source tree (the driver oracle/_ref/ref_driver is built from it)")
+        subprocess.run(["make", "-C", os.path.join(REPO, "oracle", "ref"), "REF=" + ref], check=True)
     if len(sys.argv) > 2 and sys.argv[1] == "--only":
         # regenerate one deck's digests and merge them into the existing file
         deck = sys.argv[2]

@@ -47,3 +47,36 @@ def test_max_over_ranks_single_process():
     import torch
     import bench
     assert bench.max_over_ranks(torch, None, 3.5) == 3.5
+
+
+def test_bench_spawns_its_own_ranks():
+    """`bench.py --gpus 2` started without a launcher reruns itself under
+    torch.distributed.run with two ranks; here the ranks join a gloo group on
+    the host and rank 0 reports the world size and the max over ranks."""
+    import json
+    import subprocess
+    import sys
+    repo = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    env = {k: v for k, v in os.environ.items() if k not in ("WORLD_SIZE", "RANK", "LOCAL_RANK", "MASTER_ADDR",
+                                                            "MASTER_PORT")}
+    r = subprocess.run([sys.executable, os.path.join(repo, "bench.py"), "--gpus", "2", "--replica-check"],
+                       capture_output=True, text=True, timeout=240, env=env, cwd=repo)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [json.loads(x) for x in r.stdout.splitlines() if x.startswith("{")]
+    assert lines == [{"replica_check": True, "n_gpus": 2, "max_ms": 11.0}], r.stdout
+
+
+def test_reference_arm_loads_no_cuda_library():
+    """The CPU arms classify the cells with the oracle: building the bench
+    case for them maps no part of libhsolver_b200.so into the process."""
+    import subprocess
+    import sys
+    repo = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    code = ("import bench\n"
+            "bench.workload('config1', host_side=True)\n"
+            "maps = open('/proc/self/maps').read()\n"
+            "assert 'liboracle' in maps\n"
+            "print('libhsolver_b200' in maps)\n")
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=240, cwd=repo)
+    assert r.returncode == 0, r.stderr[-2000:]
+    assert r.stdout.strip() == "False"
