@@ -145,31 +145,32 @@ class ClockSampler:
 
 
 def pcg_bytes(ncell, iters, wbytes=8, sweeps=MG_SWEEPS):
-    """Compulsory HBM bytes of one pressure-correction launch (k_ch_pcg), per
-    cell, with w bytes per stored value (8 in the FP64 form): each array once
-    per pass.
-      setup: couplings 3w and the solid mask 1 read, level-0 mask 1 and
-        diagonal w written; r w read, V-cycle rhs and seed 2w written;
+    """Algorithmic HBM bytes of one pressure-correction solve, per cell, with
+    w bytes per stored value (8 in the FP64 form, 4 in the mixed form's FP32
+    storage): the compulsory-traffic model in which every input array of a
+    kernel is read once and every output written once, neighbours hitting in
+    cache, masks at 1 byte:
+      set-up: couplings 3w and the solid mask read, level-0 mask written,
+        r read, diagonal and the V-cycle's seed written -> 7w + 2;
       per CG iteration:
-        s = A p with p = z + beta p: z, p_old, 3 couplings read, p, s written
-          -> 7w;
-        x, r update with the next V-cycle rhs and seed: x, p, r, s, diagonal
-          read, x, r, rhs, seed written -> 9w;
-        <r, z> in the V-cycle's last pass: r -> w;
-        one V-cycle on level 0: 3 + 4 (sweeps - 1) standalone red-black
-          half-sweeps of 5w (3 couplings, rhs, x read; x written), the
-          restriction 5w + 2w/8 and the coarse values of the prolongation
-          w/8; the coarser levels (one sweep more) add 1/7 of their own
+        the fused CG (A p with <s, p>; x, r update with <r, r>; p update):
+          14w + 1 (113 B in FP64);
+        a red-black smoother sweep (both colours) on level 0: x, rhs, three
+          couplings and the mask read, x written -> 6w + 1 (49 B in FP64),
+          `sweeps` of them before and after the coarse correction;
+        restriction and prolongation: 5.375w (43 B in FP64);
+        the coarser levels (one sweep more each way) add 1/7 of their own
           per-cell bytes."""
     w = wbytes
-    setup = 3 * w + 1 + 1 + w + w + 2 * w
-    cg = 7 * w + 9 * w + w
+    setup = 7 * w + 2
+    cg = 14 * w + 1
+    pair = 6 * w + 1
+    transfer = 5.375 * w
 
     def level(sw):
-        return (3 + 4 * (sw - 1)) * 5 * w + 5 * w + 0.25 * w + 0.125 * w
+        return 2 * sw * pair + transfer
 
-    vc = level(sweeps) + level(sweeps + 1) / 7.0
-    return ncell * (setup + iters * (cg + vc))
+    return ncell * (setup + iters * (cg + level(sweeps) + level(sweeps + 1) / 7.0))
 
 
 def energy_bytes(ncell, iters, w=8, mw=8):
@@ -204,14 +205,14 @@ def kernel_classes(phases, iters_mean, dims, mom_sweeps, peak, energy_iters=1):
       p' assembly: 89 B per cell (u*, v*, w*, d of the three components,
         mask; three couplings and b written);
       p' solve: pcg_bytes();
-      correction: 96 B per cell (u*, d, u per face of the three components;
-        p', p read, p written);
+      correction: 97 B per cell (u*, d per face of the three components,
+        p', p and the solid mask read; u, v, w and p written);
       energy: energy_bytes() with the step's BiCGStab iterations."""
     nx, ny, nz = dims
     ncell = nx * ny * nz
     nface = (nx + 1) * ny * nz + nx * (ny + 1) * nz + nx * ny * (nz + 1)
     model = {"momentum": 49.0 * nface * 2 * mom_sweeps, "p_assembly": 89.0 * ncell,
-             "p_solve": pcg_bytes(ncell, iters_mean), "correction": 96.0 * ncell,
+             "p_solve": pcg_bytes(ncell, iters_mean), "correction": 97.0 * ncell,
              "energy": energy_bytes(ncell, energy_iters)}
     out = {}
     for k, b in model.items():

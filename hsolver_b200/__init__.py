@@ -319,7 +319,7 @@ class ChannelParams(ctypes.Structure):
                 ("alpha_u", ctypes.c_double), ("alpha_p", ctypes.c_double), ("alpha_t", ctypes.c_double),
                 ("mom_sweeps", ctypes.c_int), ("p_tol", ctypes.c_double), ("p_maxiter", ctypes.c_int),
                 ("t_tol", ctypes.c_double), ("t_maxiter", ctypes.c_int), ("precision", ctypes.c_int),
-                ("p_precond", ctypes.c_int), ("p_mg_sweeps", ctypes.c_int), ("reserved_i", ctypes.c_int),
+                ("p_precond", ctypes.c_int), ("p_mg_sweeps", ctypes.c_int), ("p_level0", ctypes.c_int),
                 ("reserved", ctypes.c_double * 5)]
 
 

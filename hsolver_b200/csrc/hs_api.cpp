@@ -537,7 +537,7 @@ int hs_channel_create(const char *deck, const hs_channel_params *prm, int device
   q.re = p.re; q.pr = p.pr; q.u_in = p.u_in; q.t_in = p.t_in;
   q.alpha_u = p.alpha_u; q.alpha_p = p.alpha_p; q.alpha_t = p.alpha_t;
   q.mom_sweeps = p.mom_sweeps; q.p_tol = p.p_tol; q.p_maxiter = p.p_maxiter; q.t_tol = p.t_tol; q.t_maxiter = p.t_maxiter;
-  q.precision = p.precision; q.p_precond = p.p_precond; q.p_mg_sweeps = p.p_mg_sweeps;
+  q.precision = p.precision; q.p_precond = p.p_precond; q.p_mg_sweeps = p.p_mg_sweeps; q.p_level0 = p.p_level0;
   hs_channel *h = new (std::nothrow) hs_channel();
   if (!h) return fail(nullptr, HS_ERR_NOMEM, "host allocation failed");
   try {

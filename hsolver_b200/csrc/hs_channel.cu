@@ -42,6 +42,7 @@
 #include "hs_channel.hpp"
 #include "hs_cht.hpp"
 #include "hs_mg.cuh"
+#include "hs_zm.cuh"
 
 namespace cg = cooperative_groups;
 
@@ -68,6 +69,7 @@ constexpr int kT = 256;
 template <class R>
 struct ChDev {
   int N0, N1, N2;
+  int PX;                     // row pitch of the padded p' arrays (a multiple of 4 values, >= N0 + 2)
   const R *d0, *d1, *d2;      // cell widths
   const R *h0, *h1, *h2;      // centre distances, [0] and [N] half widths
   const uint8_t *solid;       // N0 N1 N2
@@ -383,7 +385,7 @@ __global__ void __launch_bounds__(kT, 4) k_ch_mom(ChDev<R> H, int color, int fir
 }
 
 // padded cell index of the CG arrays
-__device__ __forceinline__ int pq(int N0, int N1, int i, int j, int k) { return (i + 1) + (N0 + 2) * ((j + 1) + (N1 + 2) * (k + 1)); }
+__device__ __forceinline__ int pq(int PX, int N1, int i, int j, int k) { return (i + 1) + PX * ((j + 1) + (N1 + 2) * (k + 1)); }
 
 // u* of a face in FP64
 template <int A, class R>
@@ -413,24 +415,24 @@ __global__ void k_ch_passemble(ChDev<R> H, R *acx, R *acy, R *acz, R *r, R *x, d
       double v = 0.0;
       if (kind == 0) v = (double)face_area<0>(H, c) * dn;
       else if (kind == 2 && lo_fluid) v = (double)face_area<0>(H, c) * dl;
-      acx[pq(N0, N1, c[0], c[1], c[2])] = (R)v;
+      acx[pq(H.PX, N1, c[0], c[1], c[2])] = (R)v;
     }
   } else if (blockIdx.y == 1) {
     for (mg::Walk w(N0, N1 + 1, N2, tid, T); w.ok(); w.next()) {
       const int c[3] = {w.m, w.j, w.k};
       const double dn = (double)H.D1[fidx3<1>(H, c)];
-      acy[pq(N0, N1, c[0], c[1], c[2])] = (R)(face_kind<1>(H, c) == 0 ? (double)face_area<1>(H, c) * dn : 0.0);
+      acy[pq(H.PX, N1, c[0], c[1], c[2])] = (R)(face_kind<1>(H, c) == 0 ? (double)face_area<1>(H, c) * dn : 0.0);
     }
   } else if (blockIdx.y == 2) {
     for (mg::Walk w(N0, N1, N2 + 1, tid, T); w.ok(); w.next()) {
       const int c[3] = {w.m, w.j, w.k};
       const double dn = (double)H.D2[fidx3<2>(H, c)];
-      acz[pq(N0, N1, c[0], c[1], c[2])] = (R)(face_kind<2>(H, c) == 0 ? (double)face_area<2>(H, c) * dn : 0.0);
+      acz[pq(H.PX, N1, c[0], c[1], c[2])] = (R)(face_kind<2>(H, c) == 0 ? (double)face_area<2>(H, c) * dn : 0.0);
     }
   } else {
     for (mg::Walk w(N0, N1, N2, tid, T); w.ok(); w.next()) {
       const int i = w.m, j = w.j, k = w.k, e = w.flat();
-      const int q = pq(N0, N1, i, j, k);
+      const int q = pq(H.PX, N1, i, j, k);
       const bool sol = H.solid[e] != 0;
       const double uw = ustar<0>(H, fidx<0>(H, i, j, k));
       const double ue = (i + 1 == N0) ? uw : ustar<0>(H, fidx<0>(H, i + 1, j, k));
@@ -461,8 +463,8 @@ __device__ void correct_axis(const ChDev<R> &H, const R *pp) {
     // solid mask) selects one; p' is padded, so its ghost cells are readable
     int lo[3] = {c[0], c[1], c[2]};
     lo[A] -= 1;
-    const double plo = (double)pp[pq(H.N0, H.N1, lo[0], lo[1], lo[2])];
-    const double phi = (double)pp[pq(H.N0, H.N1, c[0], c[1], c[2])];
+    const double plo = (double)pp[pq(H.PX, H.N1, lo[0], lo[1], lo[2])];
+    const double phi = (double)pp[pq(H.PX, H.N1, c[0], c[1], c[2])];
     const double sf = is_mixed(R()) ? ustar<A>(H, e) : (double)Sarr<A>(H)[e];
     const double df = (double)Darr<A>(H)[e];
     double so = 0.0, dso = 0.0;  // the outlet's upstream face (x faces)
@@ -500,7 +502,7 @@ __global__ void k_ch_correct(ChDev<R> H, const R *pp) {
     for (mg::Walk w(H.N0, H.N1, H.N2, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x); w.ok(); w.next()) {
       const int e = w.flat();
       if (H.solid[e]) continue;
-      H.p[e] = H.p[e] + H.ap * pp[pq(H.N0, H.N1, w.m, w.j, w.k)];
+      H.p[e] = H.p[e] + H.ap * pp[pq(H.PX, H.N1, w.m, w.j, w.k)];
     }
   }
 }
@@ -549,9 +551,11 @@ __global__ void k_ch_init(ChDev<R> H) {
 template <class V>
 struct CgVec {
   int N0, N1, N2;
+  int px;  // row pitch of every padded array (ChDev::PX)
   const V *acx, *acy, *acz;
   const uint8_t *solid;
   V *x, *r, *p, *p2, *s;  // p, p2: search direction, double-buffered
+  V *r2;                  // the z-marching form's second residual buffer
 };
 
 __device__ double grid_sum(double v, double *partials, int &buf, double *sh, cg::grid_group &grid) {
@@ -572,11 +576,11 @@ __device__ double grid_sum(double v, double *partials, int &buf, double *sh, cg:
   return a;
 }
 
-// padded index of the cell with flat index e (x fastest)
-__device__ __forceinline__ int cell_q(int e, int N0, int N1) {
+// padded index (row pitch PX) of the cell with flat index e (x fastest)
+__device__ __forceinline__ int cell_q(int e, int N0, int N1, int PX) {
   const int row_ = e / N0, i = e - row_ * N0;
   const int k = row_ / N1, j = row_ - k * N1;
-  return (i + 1) + (N0 + 2) * ((j + 1) + (N1 + 2) * (k + 1));
+  return (i + 1) + PX * ((j + 1) + (N1 + 2) * (k + 1));
 }
 
 // one block per SM (few arrivals at every grid barrier), its size by
@@ -599,7 +603,7 @@ struct PcgT<double> {
 // (which needs only the cell's own diagonal) and this thread's share of <r, r>
 template <class M>
 __device__ void mg_fine_and_rhs(const CgVec<M> &V, const mg::Level<M> &L0, double &acc, int tid, int T) {
-  for (mg::Walk w(V.N0 + 2, V.N1 + 2, V.N2 + 2, tid, T); w.ok(); w.next()) {
+  for (mg::Walk w(V.px, V.N1 + 2, V.N2 + 2, tid, T); w.ok(); w.next()) {
     const int q = w.flat(), i = w.m - 1, j = w.j - 1, k = w.k - 1;
     const bool in = i >= 0 && j >= 0 && k >= 0 && i < V.N0 && j < V.N1 && k < V.N2;
     M d = M(0), o[6];
@@ -630,7 +634,7 @@ __global__ void __launch_bounds__(PcgT<M>::v, 1) k_ch_pcg(CgVec<M> V, mg::Hier<M
   cg::grid_group grid = cg::this_grid();
   __shared__ double sh[40];
   const int tid = blockIdx.x * blockDim.x + threadIdx.x, T = gridDim.x * blockDim.x;
-  const int N0 = V.N0, N1 = V.N1, PX = N0 + 2, PY = N1 + 2, PXY = (N0 + 2) * (N1 + 2);
+  const int N0 = V.N0, N1 = V.N1, PX = V.px, PY = N1 + 2, PXY = V.px * (N1 + 2);
   int buf = 0;
   const mg::Level<M> &L0 = G.lv[0];
   double acc = 0.0;
@@ -709,6 +713,188 @@ __global__ void __launch_bounds__(PcgT<M>::v, 1) k_ch_pcg(CgVec<M> V, mg::Hier<M
   if (tid == 0) { *out_it = it; *out_rel = sqrt(rr / bb); }
 }
 
+// ---------------------------------------------------------------- p' solve with z-marching level-0 passes
+// The tensor maps of the arrays the z-marching passes stage (hs_zm.cuh):
+// level 0's couplings, both residual buffers, both V-cycle buffers (level 0's
+// x and rhs arrays, which this form uses as two x buffers: the residual is
+// the V-cycle's right-hand side), both search-direction buffers, A p, and
+// level 1's x for the prolongation.
+struct PcgMaps {
+  CUtensorMap acx, acy, acz, r[2], xm[2], p[2], s, x1;
+};
+
+// grid_sum with a per-block failure flag: every block reads the same flags
+// after the barrier, so the decision to stop is the same in every block
+__device__ double grid_sum_f(double v, int fail, double *partials, int &buf, double *sh, cg::grid_group &grid,
+                             int &any_fail) {
+  double *pf = partials + (size_t)(2 + buf) * gridDim.x;
+  if (threadIdx.x == 0) pf[blockIdx.x] = fail ? 1.0 : 0.0;
+  const double s = grid_sum(v, partials, buf, sh, grid);  // flips buf; its barrier orders the flags
+  const double *pr = partials + (size_t)(2 + (buf ^ 1)) * gridDim.x;
+  if (threadIdx.x < 32) {
+    int f = 0;
+    for (int q = threadIdx.x; q < (int)gridDim.x; q += 32) f |= __ldcg(pr + q) != 0.0;
+    f = __any_sync(0xffffffffu, f);
+    if (threadIdx.x == 0) sh[33] = f ? 1.0 : 0.0;
+  }
+  __syncthreads();
+  any_fail = sh[33] != 0.0;
+  __syncthreads();
+  return s;
+}
+
+// The multigrid-preconditioned CG of k_ch_pcg with level 0 of the V-cycle,
+// the product A p and the CG update as z-marching passes (hs_zm.cuh), each
+// one pass over level 0 between two grid barriers:
+//   setup:    the level-0 mask and <b, b>; the hierarchy; V0 = the seed and
+//             first black half-sweep from r;
+//   V-cycle:  nsw - 1 red-black sweeps, the restriction (grid-wide), the
+//             levels below (vcycle from level 1), nsw black-red sweeps, the
+//             first with the prolongation fused, the last with <r, z>;
+//   per CG iteration: p = z + beta p and s = A p with <s, p>; x += alpha p,
+//             r -= alpha s with <r, r> and the next V-cycle's seed and first
+//             black half-sweep; the V-cycle.
+// The residual and search direction are double-buffered (a pass reads one
+// buffer, writes the other), z is level 0's second x buffer.  Needs G.ls >= 1
+// (level 0 grid-wide) and precond; one block of zm::kThreads per SM.
+template <class M>
+__global__ void __launch_bounds__(zm::kThreads, 1)
+    k_ch_pcg_zm(const __grid_constant__ CgVec<M> V, const __grid_constant__ mg::Hier<M> G,
+                const __grid_constant__ PcgMaps TM, double tol, int maxiter, double *partials, int *out_it,
+                double *out_rel) {
+  cg::grid_group grid = cg::this_grid();
+  __shared__ double sh[40];
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x, T = gridDim.x * blockDim.x;
+  const int N0 = V.N0, N1 = V.N1, N2 = V.N2, PX = V.px;
+  zm::Smem<M> S{reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(mg::stage_smem()) + 127) & ~uintptr_t(127))};
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < zm::Box<M>::SLOTS; ++s) zm::mbar_init(S.bars() + s, 1);
+    zm::fence_mbar_init();
+  }
+  __syncthreads();
+  zm::Pipe P{0u, 0u, 0u, 0u, 0};
+  const zm::Tiles Tl{N0, N1, N2, PX, (N0 + zm::kTX - 1) / zm::kTX, (N1 + zm::kTY - 1) / zm::kTY};
+  // the two buffers of each double-buffered vector
+  auto xm = [&](int i) { return i ? G.lv[0].rhs : G.lv[0].x; };
+  auto rb = [&](int i) { return i ? V.r2 : V.r; };
+  auto pb = [&](int i) { return i ? V.p2 : V.p; };
+  int buf = 0, fail = 0;
+  // set-up: level 0's mask (read by the coarsening) and <b, b>
+  double acc = 0.0;
+  for (mg::Walk w(PX, N1 + 2, N2 + 2, tid, T); w.ok(); w.next()) {
+    const int q = w.flat(), i = w.m - 1, j = w.j - 1, k = w.k - 1;
+    const bool in = i >= 0 && j >= 0 && k >= 0 && i < N0 && j < N1 && k < N2;
+    const bool solid = !in || V.solid[i + N0 * (j + N1 * k)] != 0;
+    G.lv[0].m[q] = !solid;
+    if (in) {
+      const double rv = (double)V.r[q];
+      acc += rv * rv;
+    }
+  }
+  const double bb = grid_sum(acc, partials, buf, sh, grid);
+  if (bb == 0.0) {
+    if (tid == 0) { *out_it = 0; *out_rel = 0.0; }
+    return;
+  }
+  mg::build(G, false, grid, tid, T);
+  zm::fence_async_global();
+
+  auto maps = [&](const CUtensorMap *b0, const CUtensorMap *b1, const CUtensorMap *coarse) {
+    zm::PassMaps pm;
+    pm.m[0] = b0; pm.m[1] = b1; pm.m[2] = &TM.acx; pm.m[3] = &TM.acy; pm.m[4] = &TM.acz;
+    pm.coarse = coarse;
+    return pm;
+  };
+  auto pass_end = [&]() {
+    zm::fence_async_global();
+    grid.sync();
+    zm::fence_async_global();
+  };
+  int cur = 0;  // the current residual buffer
+  // z = V(r[cur]) after the seed pass wrote xm(0); returns <r, z> (z in xm(1))
+  auto vtail = [&]() -> double {
+    int in = 0;
+    for (int s = 1; s < G.nsw; ++s) {
+      zm::PassArgs<M> a{};
+      a.kind = zm::kSweep; a.c1 = 0; a.out = xm(in ^ 1);
+      double dummy = 0.0;
+      zm::run_pass(S, P, maps(&TM.xm[in], &TM.r[cur], nullptr), Tl, a, dummy);
+      pass_end();
+      in ^= 1;
+    }
+    mg::Level<M> F = G.lv[0];
+    F.x = xm(in);
+    F.rhs = rb(cur);
+    mg::restrict_res(F, G.lv[1], false, tid, T);
+    grid.sync();
+    mg::vcycle<M, double>(G, false, grid, tid, T, nullptr, nullptr, 1);
+    zm::fence_async_global();  // level 1's x, written before vcycle's last barrier, is read by the TMA unit next
+    double d = 0.0;
+    for (int s = 0; s < G.nsw; ++s) {
+      zm::PassArgs<M> a{};
+      a.kind = s == 0 ? zm::kProlong : zm::kSweep;
+      a.c1 = 1;
+      a.dot = s == G.nsw - 1;
+      a.out = xm(in ^ 1);
+      zm::run_pass(S, P, maps(&TM.xm[in], &TM.r[cur], s == 0 ? &TM.x1 : nullptr), Tl, a, d);
+      in ^= 1;
+      if (s < G.nsw - 1) pass_end();
+    }
+    zm::fence_async_global();
+    const double g = grid_sum_f(d, P.fail, partials, buf, sh, grid, fail);
+    zm::fence_async_global();
+    return g;
+  };
+  {
+    zm::PassArgs<M> a{};
+    a.kind = zm::kSeed; a.c1 = 0; a.out = xm(0);
+    double dummy = 0.0;
+    zm::run_pass(S, P, maps(&TM.r[cur], &TM.r[cur], nullptr), Tl, a, dummy);
+    pass_end();
+  }
+  const double eps = tol * tol;
+  double gamma = vtail(), rr = bb, beta = 0.0;
+  int po = 0, it = 0;
+  while (!fail && it < maxiter && !(rr / bb < eps)) {
+    const bool first = it == 0;
+    it++;
+    // p = z + beta p_old, s = A p, <s, p>
+    double sp;
+    {
+      zm::PassArgs<M> a{};
+      a.kind = zm::kAp; a.first = first; a.beta = (M)beta; a.out = pb(po ^ 1); a.out2 = V.s;
+      acc = 0.0;
+      zm::run_pass(S, P, maps(&TM.xm[1], &TM.p[po], nullptr), Tl, a, acc);
+      zm::fence_async_global();
+      sp = grid_sum_f(acc, P.fail, partials, buf, sh, grid, fail);
+      zm::fence_async_global();
+    }
+    po ^= 1;
+    if (fail || sp == 0.0) break;
+    const double alpha = gamma / sp;
+    // x += alpha p, r -= alpha s, <r, r>, the next V-cycle's seed and first black half-sweep
+    {
+      zm::PassArgs<M> a{};
+      a.kind = zm::kSeed; a.c1 = 0; a.upd = 1; a.alpha = alpha; a.out = xm(0); a.out2 = rb(cur ^ 1);
+      a.xcg = V.x; a.pcg = pb(po);
+      acc = 0.0;
+      zm::run_pass(S, P, maps(&TM.r[cur], &TM.s, nullptr), Tl, a, acc);
+      zm::fence_async_global();
+      rr = grid_sum_f(acc, P.fail, partials, buf, sh, grid, fail);
+      zm::fence_async_global();
+      cur ^= 1;
+    }
+    if (fail || rr / bb < eps || it >= maxiter) break;  // no V-cycle for an iteration that will not run
+    const double gnew = vtail();
+    beta = gnew / gamma;
+    gamma = gnew;
+  }
+  if (tid == 0) {
+    *out_it = fail ? -1 : it;
+    *out_rel = sqrt(rr / bb);
+  }
+}
+
 // residual sums of the momentum pass (3 x nb partials) and continuity (nb) -> res[0..3]
 // (launched with 4 warps: warp a sums array a, each lane over four
 // interleaved strides so that four loads are in flight)
@@ -730,6 +916,9 @@ __global__ void k_ch_finalize(const double *mom, const double *cont, int nb, dou
   if (lane == 0) res[a] = sqrt(s);
 }
 
+// n rounded up to a multiple of 4: a row pitch of 16-byte rows in FP32 and FP64
+int pitch4(int n) { return (n + 3) / 4 * 4; }
+
 int blocks_for(long long n) { return (int)std::max<long long>(1, std::min<long long>((n + kT - 1) / kT, 148LL * 8)); }
 
 template <class K, class... A>
@@ -748,6 +937,7 @@ struct ChannelState {
   cudaStream_t stream = nullptr;
   bool mixed = false;
   int N0 = 0, N1 = 0, N2 = 0, nreg = 0;
+  int PX = 0;  // row pitch of the padded p' arrays and levels: N0 + 2 rounded up to 4 values (16-byte rows)
   double nu = 0, kf = 0;
   std::vector<int> region;
   std::vector<void *> allocs;
@@ -760,6 +950,11 @@ struct ChannelState {
   mg::Hier<double> Gd{};
   mg::Hier<float> Gf{};
   int mom_blocks = 0, pcg_grid = 0;
+  // the z-marching form of the p' solve (k_ch_pcg_zm): its tensor maps, grid and shared memory
+  PcgMaps TMd{}, TMf{};
+  bool use_zm = false;
+  int zm_grid = 0;
+  size_t zm_smem = 0;
   double *mom_part = nullptr, *cont_part = nullptr, *pcg_part = nullptr, *res = nullptr, *pcg_rel = nullptr;
   int *pcg_it = nullptr;
   ChtState *cht = nullptr;
@@ -805,7 +1000,7 @@ namespace {
 template <class R>
 void setup_fields(ChannelState &S, ChDev<R> &H, const std::vector<double> (&d)[3], const std::vector<double> (&h)[3],
                   const uint8_t *solid) {
-  H.N0 = S.N0; H.N1 = S.N1; H.N2 = S.N2;
+  H.N0 = S.N0; H.N1 = S.N1; H.N2 = S.N2; H.PX = S.PX;
   const R **dd[3] = {&H.d0, &H.d1, &H.d2}, **hh[3] = {&H.h0, &H.h1, &H.h2};
   for (int a = 0; a < 3; ++a) {
     std::vector<R> dv(d[a].begin(), d[a].end()), hv(h[a].begin(), h[a].end());
@@ -862,10 +1057,11 @@ template <> CgVec<float> &cg_vec<float>(ChannelState &S) { return S.Vf; }
 
 template <class R>
 void setup_cg(ChannelState &S, CgVec<R> &V, const uint8_t *solid, size_t np) {
-  V.N0 = S.N0; V.N1 = S.N1; V.N2 = S.N2; V.solid = solid;
+  V.N0 = S.N0; V.N1 = S.N1; V.N2 = S.N2; V.px = S.PX; V.solid = solid;
   V.acx = S.alloc<R>(np); V.acy = S.alloc<R>(np); V.acz = S.alloc<R>(np);
   V.x = S.alloc<R>(np); V.r = S.alloc<R>(np); V.p = S.alloc<R>(np); V.s = S.alloc<R>(np);
   V.p2 = S.alloc<R>(np);
+  V.r2 = S.alloc<R>(np);
 }
 
 template <class M>
@@ -874,8 +1070,8 @@ void setup_mg(ChannelState &S, mg::Hier<M> &G, const CgVec<M> &V) {
   while (true) {
     if (L >= mg::kMgMaxLv) throw std::runtime_error("multigrid: too many levels");
     mg::Level<M> &l = G.lv[L];
-    l.nx = nx; l.ny = ny; l.nz = nz;
-    const size_t np = (size_t)(nx + 2) * (ny + 2) * (nz + 2);
+    l.nx = nx; l.ny = ny; l.nz = nz; l.px = pitch4(nx + 2);
+    const size_t np = (size_t)l.px * (ny + 2) * (nz + 2);
     l.x = S.alloc<M>(np); l.rhs = S.alloc<M>(np);
     if (L == 0) {  // the p' couplings themselves (written by the assembly, read-only in the solve)
       l.gx = const_cast<M *>(V.acx); l.gy = const_cast<M *>(V.acy); l.gz = const_cast<M *>(V.acz);
@@ -901,6 +1097,64 @@ void setup_mg(ChannelState &S, mg::Hier<M> &G, const CgVec<M> &V) {
   mg::plan_stage(G);
 }
 
+// ---- TMA tensor maps (the driver's encoder, reached through the runtime)
+using EncodeTiled = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                 const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                 CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiled tensor_map_encoder() {
+  void *fn = nullptr;
+  cudaDriverEntryPointQueryResult q{};
+  CH_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q));
+  if (q != cudaDriverEntryPointSuccess || !fn) throw std::runtime_error("CUDA: cuTensorMapEncodeTiled is not available");
+  return reinterpret_cast<EncodeTiled>(fn);
+}
+
+// a 3-D tiled map over a padded array (px x py x pz values of M, x fastest)
+// with a bx x by x 1 box; reads outside the array are zero-filled
+template <class M>
+CUtensorMap padded_map(EncodeTiled enc, const M *base, int px, int py, int pz, int bx, int by) {
+  CUtensorMap m;
+  const cuuint64_t dims[3] = {(cuuint64_t)px, (cuuint64_t)py, (cuuint64_t)pz};
+  const cuuint64_t strides[2] = {(cuuint64_t)px * sizeof(M), (cuuint64_t)px * py * sizeof(M)};
+  const cuuint32_t box[3] = {(cuuint32_t)bx, (cuuint32_t)by, 1u};
+  const cuuint32_t es[3] = {1u, 1u, 1u};
+  const CUresult r = enc(&m, sizeof(M) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3,
+                         const_cast<M *>(base), dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                         CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) throw std::runtime_error("CUDA: tensor map encoding failed (" + std::to_string((int)r) + ")");
+  return m;
+}
+
+// The z-marching form of the p' solve when the case allows it: the V-cycle
+// preconditioner on, a coarser level below the finest and level 0 handled
+// grid-wide (not by block 0 alone), p_level0 = 0, and one block of
+// zm::kThreads resident per SM with the ring in shared memory.
+template <class M>
+void setup_zm(ChannelState &S, CgVec<M> &V, mg::Hier<M> &G, PcgMaps &TM, int nsm) {
+  S.use_zm = false;
+  if (!S.prm.p_precond || S.prm.p_level0 != 0 || G.L < 2 || G.ls < 1) return;
+  const EncodeTiled enc = tensor_map_encoder();
+  const int py = S.N1 + 2, pz = S.N2 + 2;
+  auto fine = [&](const M *a) { return padded_map<M>(enc, a, S.PX, py, pz, zm::Box<M>::BX, zm::Box<M>::BY); };
+  TM.acx = fine(V.acx); TM.acy = fine(V.acy); TM.acz = fine(V.acz);
+  TM.r[0] = fine(V.r); TM.r[1] = fine(V.r2);
+  TM.xm[0] = fine(G.lv[0].x); TM.xm[1] = fine(G.lv[0].rhs);
+  TM.p[0] = fine(V.p); TM.p[1] = fine(V.p2);
+  TM.s = fine(V.s);
+  const mg::Level<M> &L1 = G.lv[1];
+  TM.x1 = padded_map<M>(enc, L1.x, L1.px, L1.ny + 2, L1.nz + 2, zm::Box<M>::CBX, zm::Box<M>::CBY);
+  // the ring shares the launch's dynamic shared memory with block 0's staging of the small levels
+  const size_t smem = std::max<size_t>((size_t)zm::Box<M>::SMEM + 128, (size_t)G.stage);
+  CH_CUDA(cudaFuncSetAttribute((const void *)k_ch_pcg_zm<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int per = 0;
+  CH_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, (const void *)k_ch_pcg_zm<M>, zm::kThreads, smem));
+  if (per < 1) return;
+  S.zm_grid = per * nsm;
+  S.zm_smem = smem;
+  S.use_zm = true;
+}
+
 template <class R>
 void mom_solve(ChannelState &S, ChDev<R> &H) {
   const int sw = std::max(1, S.prm.mom_sweeps);
@@ -923,14 +1177,20 @@ void step_once(ChannelState &S, ChDev<R> &H, int flags) {
   if (S.prof) CH_CUDA(cudaEventRecord(S.ev[2], S.stream));
   if (!(flags & 1)) {
     const int pre = S.prm.p_precond ? 1 : 0;
-    if (S.mixed)
+    if (S.use_zm && S.mixed)
+      launch_coop(k_ch_pcg_zm<float>, S.zm_grid, zm::kThreads, S.zm_smem, S.stream, S.Vf, S.Gf, S.TMf, S.prm.p_tol,
+                  S.prm.p_maxiter, S.pcg_part, S.pcg_it, S.pcg_rel);
+    else if (S.use_zm)
+      launch_coop(k_ch_pcg_zm<double>, S.zm_grid, zm::kThreads, S.zm_smem, S.stream, S.Vd, S.Gd, S.TMd, S.prm.p_tol,
+                  S.prm.p_maxiter, S.pcg_part, S.pcg_it, S.pcg_rel);
+    else if (S.mixed)
       launch_coop(k_ch_pcg<float>, S.pcg_grid, PcgT<float>::v, S.Gf.stage, S.stream, S.Vf, S.Gf, pre, S.prm.p_tol, S.prm.p_maxiter, S.pcg_part, S.pcg_it,
                   S.pcg_rel);
     else
       launch_coop(k_ch_pcg<double>, S.pcg_grid, PcgT<double>::v, S.Gd.stage, S.stream, S.Vd, S.Gd, pre, S.prm.p_tol, S.prm.p_maxiter, S.pcg_part, S.pcg_it,
                   S.pcg_rel);
   } else {
-    const long long np = (long long)(S.N0 + 2) * (S.N1 + 2) * (S.N2 + 2);
+    const long long np = (long long)S.PX * (S.N1 + 2) * (S.N2 + 2);
     CH_CUDA(cudaMemsetAsync(V.x, 0, np * sizeof(R), S.stream));
     CH_CUDA(cudaMemsetAsync(S.pcg_it, 0, sizeof(int), S.stream));
   }
@@ -954,6 +1214,8 @@ void enqueue_stats(ChannelState &S, ChannelState::StepRec &rec, int flags) {
 // the step's bookkeeping from its statistics: residuals, the normalisers
 // (maxima over the first five steps) and the global residual
 void apply_stats(ChannelState &S, const ChannelState::StepRec &rec, int flags) {
+  if (!(flags & 1) && rec.pit < 0)
+    throw std::runtime_error("pressure-correction solve: a wait for staged planes ran out (the solve was abandoned)");
   for (int a = 0; a < 4; ++a) S.st.res[a] = rec.res[a];
   S.st.pcg_iters = (flags & 1) ? 0 : rec.pit;
   S.st.pcg_relres = (flags & 1) ? 0.0 : rec.prel;
@@ -1000,9 +1262,10 @@ double *uarr(ChannelState *S, int a) {
 ChannelState *ch_create(const Case &c, const ChParams &p, int device) {
   if (!(p.re > 0) || !(p.pr > 0) || !(p.alpha_u > 0 && p.alpha_u <= 1) || !(p.alpha_p > 0 && p.alpha_p <= 1) ||
       !(p.alpha_t > 0 && p.alpha_t <= 1) || p.mom_sweeps < 1 || !(p.p_tol > 0) || p.p_maxiter < 0 || !(p.t_tol > 0) ||
-      p.t_maxiter < 0 || (p.precision != 0 && p.precision != 1) || p.p_mg_sweeps < 0 || p.p_mg_sweeps > 8)
+      p.t_maxiter < 0 || (p.precision != 0 && p.precision != 1) || p.p_mg_sweeps < 0 || p.p_mg_sweeps > 8 ||
+      (p.p_level0 != 0 && p.p_level0 != 1))
     throw std::invalid_argument("invalid channel parameters");
-  if ((long long)(c.Nx + 2) * (c.Ny + 2) * (c.Nz + 2) >= (1LL << 31))
+  if ((long long)pitch4((int)c.Nx + 2) * (c.Ny + 2) * (c.Nz + 2) >= (1LL << 31))
     throw std::invalid_argument("grid too large for 32-bit indices");
   CH_CUDA(cudaSetDevice(device));
   std::unique_ptr<ChannelState> S(new ChannelState());
@@ -1012,6 +1275,7 @@ ChannelState *ch_create(const Case &c, const ChParams &p, int device) {
   S->mixed = p.precision == 1;
   CH_CUDA(cudaStreamCreateWithFlags(&S->stream, cudaStreamNonBlocking));
   S->N0 = (int)c.Nx; S->N1 = (int)c.Ny; S->N2 = (int)c.Nz;
+  S->PX = pitch4(S->N0 + 2);
   S->nreg = c.nsolid_regions;
   const std::vector<double> *pts[3] = {&c.deck.xs, &c.deck.ys, &c.deck.zs};
   std::vector<double> d[3], h[3];
@@ -1032,8 +1296,8 @@ ChannelState *ch_create(const Case &c, const ChParams &p, int device) {
   CH_CUDA(cudaMemcpyAsync(solid, c.ctype.data(), n, cudaMemcpyHostToDevice, S->stream));
   if (S->mixed) setup_fields(*S, S->Hf, d, h, solid);
   else setup_fields(*S, S->Hd, d, h, solid);
-  // CG vectors and couplings (FP64, padded)
-  const size_t np = (size_t)(S->N0 + 2) * (S->N1 + 2) * (S->N2 + 2);
+  // CG vectors and couplings (padded, row pitch PX)
+  const size_t np = (size_t)S->PX * (S->N1 + 2) * (S->N2 + 2);
   if (S->mixed) setup_cg(*S, S->Vf, solid, np);
   else setup_cg(*S, S->Vd, solid, np);
   S->scratch = S->alloc<double>(np);
@@ -1052,7 +1316,9 @@ ChannelState *ch_create(const Case &c, const ChParams &p, int device) {
                                                         S->mixed ? S->Gf.stage : S->Gd.stage));
   if (per < 1) throw std::runtime_error("pressure-correction kernel cannot be resident");
   S->pcg_grid = per * nsm;
-  S->pcg_part = S->alloc<double>((size_t)2 * S->pcg_grid + 64);
+  if (S->mixed) setup_zm(*S, S->Vf, S->Gf, S->TMf, nsm);
+  else setup_zm(*S, S->Vd, S->Gd, S->TMd, nsm);
+  S->pcg_part = S->alloc<double>((size_t)4 * std::max(S->pcg_grid, S->zm_grid) + 64);
   S->pcg_it = S->alloc<int>(1);
   S->pcg_rel = S->alloc<double>(1);
   // energy: the conjugate-heat-transfer operator in channel mode, on this stream
@@ -1164,15 +1430,15 @@ namespace {
 // device-side conversions for the field copies (the caller's host buffer is
 // copied to or from directly; pinned buffers go by DMA)
 template <class T>
-__global__ void k_unpad(const T *src, double *dst, int N0, int N1, int N2) {
+__global__ void k_unpad(const T *src, double *dst, int N0, int N1, int N2, int PX) {
   const int n = N0 * N1 * N2;
   for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x)
-    dst[e] = src[cell_q(e, N0, N1)];
+    dst[e] = src[cell_q(e, N0, N1, PX)];
 }
-__global__ void k_pad(const double *src, double *dst, int N0, int N1, int N2) {
+__global__ void k_pad(const double *src, double *dst, int N0, int N1, int N2, int PX) {
   const int n = N0 * N1 * N2;
   for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x)
-    dst[cell_q(e, N0, N1)] = src[e];
+    dst[cell_q(e, N0, N1, PX)] = src[e];
 }
 template <class R>
 __global__ void k_widen(const R *src, const double *add, double *dst, long long n) {
@@ -1201,9 +1467,9 @@ void ch_get_field(ChannelState *S, int f, double *host, long n) {
   double *scr = S->scratch;
   const int g = blocks_for(n);
   if (f == 4 || f == 11) {
-    if (f == 4) k_unpad<double><<<g, kT, 0, S->stream>>>(cht_T_device(S->cht), scr, S->N0, S->N1, S->N2);
-    else if (S->mixed) k_unpad<float><<<g, kT, 0, S->stream>>>(S->Vf.x, scr, S->N0, S->N1, S->N2);
-    else k_unpad<double><<<g, kT, 0, S->stream>>>(S->Vd.x, scr, S->N0, S->N1, S->N2);
+    if (f == 4) k_unpad<double><<<g, kT, 0, S->stream>>>(cht_T_device(S->cht), scr, S->N0, S->N1, S->N2, S->N0 + 2);
+    else if (S->mixed) k_unpad<float><<<g, kT, 0, S->stream>>>(S->Vf.x, scr, S->N0, S->N1, S->N2, S->PX);
+    else k_unpad<double><<<g, kT, 0, S->stream>>>(S->Vd.x, scr, S->N0, S->N1, S->N2, S->PX);
     CH_CUDA(cudaGetLastError());
     d2h(S, scr, host, n);
     return;
@@ -1230,7 +1496,7 @@ void ch_set_field(ChannelState *S, int f, const double *host, long n) {
   const int g = blocks_for(n);
   if (f == 4) {
     h2d(S, S->scratch, host, n);
-    k_pad<<<g, kT, 0, S->stream>>>(S->scratch, cht_T_device(S->cht), S->N0, S->N1, S->N2);
+    k_pad<<<g, kT, 0, S->stream>>>(S->scratch, cht_T_device(S->cht), S->N0, S->N1, S->N2, S->N0 + 2);
     CH_CUDA(cudaGetLastError());
     return;
   }

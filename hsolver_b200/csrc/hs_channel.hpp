@@ -20,6 +20,7 @@ struct ChParams {
   int precision;                    // 0 FP64, 1 mixed (FP32 fields, sweeps and V-cycle)
   int p_precond;                    // 0 plain CG, 1 multigrid V-cycle
   int p_mg_sweeps;                  // V-cycle sweeps on the finest level (0: 2); coarser levels one more
+  int p_level0;                     // finest level of the p' solve: 0 z-marching passes where possible, 1 grid-wide
 };
 
 struct ChStats {

@@ -482,7 +482,7 @@ void setup_levels(ChtState &C, mg::Hier<MT> &G) {
   while (true) {
     if (L >= mg::kMgMaxLv) throw std::runtime_error("multigrid: too many levels");
     mg::Level<MT> &l = G.lv[L];
-    l.nx = nx; l.ny = ny; l.nz = nz;
+    l.nx = nx; l.ny = ny; l.nz = nz; l.px = nx + 2;
     const size_t np = (size_t)(nx + 2) * (ny + 2) * (nz + 2);
     l.x = C.alloc<MT>(np); l.rhs = C.alloc<MT>(np);
     l.gx = C.alloc<MT>(np); l.gy = C.alloc<MT>(np); l.gz = C.alloc<MT>(np);

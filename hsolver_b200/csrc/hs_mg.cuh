@@ -43,6 +43,7 @@ constexpr int kMgStageMax = 64 * 1024;  // bytes of dynamic shared memory the so
 template <class M>
 struct Level {
   int nx, ny, nz;
+  int px;           // row pitch of the padded arrays (>= nx + 2; the cells past nx + 1 are zero)
   M *x, *rhs;
   M *gx, *gy, *gz;
   M *fx, *fy, *fz;  // null: pure diffusion
@@ -91,6 +92,10 @@ struct Walk {
   __host__ __device__ __forceinline__ int flat() const { return m + mx * (j + ny * k); }
 };
 
+// values in each padded array of level L (row pitch px)
+template <class M>
+__host__ __device__ __forceinline__ long long padded(const Level<M> &L) { return (long long)L.px * (L.ny + 2) * (L.nz + 2); }
+
 template <class M>
 __host__ __device__ __forceinline__ bool small(const Level<M> &L) { return (long long)L.nx * L.ny * L.nz <= kMgSmall; }
 
@@ -106,7 +111,7 @@ inline void plan_stage(Hier<M> &G) {
   if (G.L < 1) return;
   auto bytes = [&](int l) {
     const Level<M> &L = G.lv[l];
-    return ((long long)(L.nx + 2) * (L.ny + 2) * (L.nz + 2) * (long long)sizeof(M) + 15) / 16 * 16;
+    return (padded(L) * (long long)sizeof(M) + 15) / 16 * 16;
   };
   int ls = 0;
   while (ls < G.L - 1 && !small(G.lv[ls])) ++ls;
@@ -126,7 +131,7 @@ inline void plan_stage(Hier<M> &G) {
 
 template <class M>
 __device__ __forceinline__ int idx(const Level<M> &L, int i, int j, int k) {
-  return i + (L.nx + 2) * (j + (L.ny + 2) * k);
+  return i + L.px * (j + (L.ny + 2) * k);
 }
 
 template <class M>
@@ -135,7 +140,7 @@ __device__ __forceinline__ M pos(M a) { return a > M(0) ? a : M(0); }
 // diagonal and the six off-diagonal magnitudes of row q (order W E S N B F)
 template <class M>
 __device__ __forceinline__ void row(const Level<M> &L, int q, bool tr, M &d, M (&o)[6]) {
-  const int PX = L.nx + 2, PXY = (L.nx + 2) * (L.ny + 2);
+  const int PX = L.px, PXY = L.px * (L.ny + 2);
   const int st[3] = {1, PX, PXY};
   const M *g[3] = {L.gx, L.gy, L.gz};
   const M *f[3] = {L.fx, L.fy, L.fz};
@@ -166,7 +171,7 @@ __device__ __forceinline__ M ldx(const M *p) {
 
 template <class M, bool S = false>
 __device__ __forceinline__ M offsum(const Level<M> &L, const M (&o)[6], const M *x, int q) {
-  const int PX = L.nx + 2, PXY = (L.nx + 2) * (L.ny + 2);
+  const int PX = L.px, PXY = L.px * (L.ny + 2);
   return o[0] * ldx<S>(x + q - 1) + o[1] * ldx<S>(x + q + 1) + o[2] * ldx<S>(x + q - PX) + o[3] * ldx<S>(x + q + PX) +
          o[4] * ldx<S>(x + q - PXY) + o[5] * ldx<S>(x + q + PXY);
 }
@@ -398,8 +403,8 @@ __device__ __forceinline__ void restrict_res(const Level<M> &F, const Level<M> &
 // zero coupling.  The arithmetic is that of prolongation followed by smooth().
 template <class M, bool S = false>
 __device__ __forceinline__ void prolong_smooth(const Level<M> &F, const Level<M> &C, bool tr, int tid, int T) {
-  const int PX = F.nx + 2, PXY = (F.nx + 2) * (F.ny + 2);
-  const int CPX = C.nx + 2, CPXY = (C.nx + 2) * (C.ny + 2);
+  const int PX = F.px, PXY = F.px * (F.ny + 2);
+  const int CPX = C.px, CPXY = C.px * (C.ny + 2);
   for (Walk w((F.nx + 1) / 2, F.ny, F.nz, tid, T); w.ok(); w.next()) {
     const int j = w.j, k = w.k, i = 2 * w.m + ((j + k + 1) & 1);
     if (i >= F.nx) continue;
@@ -451,7 +456,7 @@ __device__ __forceinline__ void factor(const Hier<M> &G, bool tr) {
   int *sp = piv_smem();
   __shared__ int spiv;
   const Level<M> &C = G.lv[G.L - 1];
-  const int nc = C.nx * C.ny * C.nz, PX = C.nx + 2, PXY = (C.nx + 2) * (C.ny + 2);
+  const int nc = C.nx * C.ny * C.nz, PX = C.px, PXY = C.px * (C.ny + 2);
   for (int e = threadIdx.x; e < nc * nc; e += blockDim.x) {
     const int r = e / nc, c2 = e % nc;
     const int q = idx(C, r % C.nx + 1, (r / C.nx) % C.ny + 1, r / (C.nx * C.ny) + 1);
@@ -600,7 +605,7 @@ __device__ __forceinline__ void small_levels(const Hier<M> &G, bool tr) {
   {
     const Level<M> &Lg = G.lv[ls];
     const Level<M> Ls = staged(G, ls);
-    const int n = (Lg.nx + 2) * (Lg.ny + 2) * (Lg.nz + 2);
+    const int n = (int)padded(Lg);
     for (int e = t; e < n; e += B) {
       const M xv = __ldcg(Lg.x + e), rv = __ldcg(Lg.rhs + e);
       Ls.x[e] = xv;
@@ -608,7 +613,7 @@ __device__ __forceinline__ void small_levels(const Hier<M> &G, bool tr) {
     }
     for (int l = ls + 1; l < G.L; ++l) {
       const Level<M> C = staged(G, l);
-      const int nc = (C.nx + 2) * (C.ny + 2) * (C.nz + 2);
+      const int nc = (int)padded(C);
       for (int e = t; e < nc; e += B) C.x[e] = M(0);
     }
     __syncthreads();
@@ -646,22 +651,32 @@ __device__ __forceinline__ void small_levels(const Hier<M> &G, bool tr) {
   {
     const Level<M> &Lg = G.lv[ls];
     const Level<M> Ls = staged(G, ls);
-    const int n = (Lg.nx + 2) * (Lg.ny + 2) * (Lg.nz + 2);
+    const int n = (int)padded(Lg);
     for (int e = t; e < n; e += B) Lg.x[e] = Ls.x[e];
   }
 }
 
-// lv[0].x = V-cycle applied to lv[0].rhs; the caller has written lv[0].rhs
-// and seeded lv[0] (seed_diag / seed_store on every interior cell) before the barrier that
+// lv[first].x = V-cycle applied to lv[first].rhs (first = 0: the whole
+// cycle; first = 1: the part below a level 0 that the caller smooths itself,
+// with first < ls); the caller has written lv[first].rhs
+// and seeded lv[first] (seed_diag / seed_store on every interior cell) before the barrier that
 // precedes this call.  With dot_r, the last level-0 pass also adds this
 // thread's share of sum dot_r x to *dot_acc and the final barrier is left to
 // the caller's reduction (returns true); it returns false, with the barrier
-// done and nothing added, when level 0 is handled by block 0 alone.
+// done and nothing added, when level 0 is handled by block 0 alone or is not
+// part of the call.
 template <class M, class RT = double>
 __device__ __forceinline__ bool vcycle(const Hier<M> &G, bool tr, cg::grid_group &grid, int tid, int T,
-                       const RT *dot_r = nullptr, double *dot_acc = nullptr) {
+                       const RT *dot_r = nullptr, double *dot_acc = nullptr, int first = 0) {
   const int ls = G.ls;  // first level handled by block 0 alone
-  for (int l = 0; l < ls; ++l) {
+  // the barrier after the last write of lv[first].x: with first > 0 the
+  // caller's next pass reads it through the TMA unit (async proxy), so each
+  // writing thread orders its writes for that proxy first
+  auto last_sync = [&]() {
+    if (first > 0) asm volatile("fence.proxy.async.global;" ::: "memory");
+    grid.sync();
+  };
+  for (int l = first; l < ls; ++l) {
     smooth(G.lv[l], 1, tr, tid, T);
     grid.sync();
     for (int s = 1; s < (l == 0 ? G.nsw : G.nswc); ++s) {
@@ -674,8 +689,9 @@ __device__ __forceinline__ bool vcycle(const Hier<M> &G, bool tr, cg::grid_group
     grid.sync();
   }
   if (blockIdx.x == 0) small_levels(G, tr);
-  grid.sync();
-  for (int l = ls - 1; l >= 0; --l) {
+  if (ls == first) last_sync();
+  else grid.sync();
+  for (int l = ls - 1; l >= first; --l) {
     prolong_smooth(G.lv[l], G.lv[l + 1], tr, tid, T);
     grid.sync();
     for (int s = 1; s < (l == 0 ? G.nsw : G.nswc); ++s) {
@@ -689,7 +705,8 @@ __device__ __forceinline__ bool vcycle(const Hier<M> &G, bool tr, cg::grid_group
       return true;
     }
     smooth(G.lv[l], 0, tr, tid, T);
-    grid.sync();
+    if (l == first) last_sync();
+    else grid.sync();
   }
   return false;
 }

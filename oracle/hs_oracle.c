@@ -1765,6 +1765,64 @@ void or_ch_destroy(or_ch *C) {
 
 void or_ch_dims(const or_ch *C, I64 *out3) { out3[0] = C->N[0]; out3[1] = C->N[1]; out3[2] = C->N[2]; }
 
+/* One outer step with the pressure correction p' given (N values, x
+ * fastest) instead of solved, and no energy solve: momentum, the p' system's
+ * assembly, p' = pp, the correction.  Returns ||b - A pp|| / ||b|| on the
+ * step's own system (the relative residual of the given p'), or -1 when
+ * b = 0.  Test infrastructure: checks a p' solved elsewhere against this
+ * oracle's assembly and operator. */
+double or_ch_step_given(or_ch *C, const double *pp) {
+  I64 N = C->N[0] * C->N[1] * C->N[2];
+  ch_momentum(C);
+  C->res[3] = ch_passemble(C);
+  memcpy(C->pp, pp, 8 * N);
+  double *y = malloc(8 * N);
+  ch_apply(C, C->pp, y);
+  double rr = 0.0, bb = 0.0;
+  for (I64 c = 0; c < N; ++c) {
+    if (C->solid[c]) continue;
+    double r = C->bc[c] - y[c];
+    rr += r * r;
+    bb += C->bc[c] * C->bc[c];
+  }
+  free(y);
+  C->pcg_iters = 0;
+  ch_correct(C);
+  C->res[4] = 0.0;
+  C->t_iters = 0;
+  C->iter++;
+  return bb > 0 ? sqrt(rr / bb) : -1.0;
+}
+
+/* ||b - A T|| of the channel energy system on the current face velocities
+ * (the system the energy step solves after the correction), for a
+ * temperature field T (N values); *bnorm = ||b||. */
+double or_ch_energy_residual(const or_ch *C, const double *T, double *bnorm) {
+  I64 N = C->N[0] * C->N[1] * C->N[2];
+  or_cht H = ch_cht(C);
+  double *b = malloc(8 * N), *y = malloc(8 * N);
+  cht_rhs(&H, b);
+  cht_apply(&H, T, y, 0);
+  double rr = 0.0, bb = 0.0;
+  for (I64 c = 0; c < N; ++c) {
+    double r = b[c] - y[c];
+    rr += r * r;
+    bb += b[c] * b[c];
+  }
+  free(b); free(y);
+  if (bnorm) *bnorm = sqrt(bb);
+  return sqrt(rr);
+}
+
+/* the thread count of the OpenMP loops (no effect without OpenMP) */
+void or_set_threads(int n) {
+#ifdef _OPENMP
+  if (n > 0) omp_set_num_threads(n);
+#else
+  (void)n;
+#endif
+}
+
 /* threads the OpenMP loops of the channel / CHT paths use (1 without OpenMP) */
 int or_threads(void) {
 #ifdef _OPENMP

@@ -333,3 +333,39 @@ class ChannelCase:
         self.L.or_ch_stats(self.h, res.ctypes.data, norm.ctypes.data, ctypes.byref(glob), it.ctypes.data)
         return {"res": res, "norm": norm, "global": glob.value, "iter": int(it[0]), "pcg_iters": int(it[1]),
                 "t_iters": int(it[2])}
+
+
+def set_threads(n):
+    """The thread count of the oracle's OpenMP loops (the tests run one: every
+    sum in loop order); returns the previous count."""
+    L = lib()
+    L.or_threads.restype = ctypes.c_int
+    L.or_set_threads.argtypes = [ctypes.c_int]
+    prev = int(L.or_threads())
+    L.or_set_threads(int(n))
+    return prev
+
+
+def _channel_extra(L):
+    L.or_ch_step_given.restype = ctypes.c_double
+    L.or_ch_step_given.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+    L.or_ch_energy_residual.restype = ctypes.c_double
+    L.or_ch_energy_residual.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]
+
+
+def channel_step_given(case, pprime):
+    """One outer step of a ChannelCase with p' given instead of solved (no
+    energy): returns ||b - A p'|| / ||b|| on the step's own p' system."""
+    _channel_extra(case.L)
+    a = np.ascontiguousarray(pprime, np.float64)
+    return case.L.or_ch_step_given(case.h, a.ctypes.data)
+
+
+def channel_energy_residual(case, T):
+    """(||b - A T||, ||b||) of a ChannelCase's energy system on its current
+    face velocities."""
+    _channel_extra(case.L)
+    a = np.ascontiguousarray(T, np.float64)
+    bn = ctypes.c_double()
+    r = case.L.or_ch_energy_residual(case.h, a.ctypes.data, ctypes.byref(bn))
+    return r, bn.value

@@ -13,7 +13,7 @@ void plan(int nx, int ny, int nz) {
   hs::mg::Hier<M> G{};
   int L = 0;
   while (true) {
-    G.lv[L].nx = nx; G.lv[L].ny = ny; G.lv[L].nz = nz;
+    G.lv[L].nx = nx; G.lv[L].ny = ny; G.lv[L].nz = nz; G.lv[L].px = nx + 2;
     ++L;
     if ((long long)nx * ny * nz <= hs::mg::kMgCoarse) break;
     nx = (nx + 1) / 2; ny = (ny + 1) / 2; nz = (nz + 1) / 2;

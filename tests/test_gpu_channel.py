@@ -325,3 +325,53 @@ def test_config3_converged_state_matches_oracle(precision):
     assert steps == int(ref["steps"]), (steps, int(ref["steps"]))
     for name in FACE + ["p", "T"]:
         assert _rel(g.field(name), ref[name]) < 1e-6, name
+
+
+RAGGED = {(40, 20, 12): ((9, 14, 1, 6, 4, 8), (20, 26, 10, 16, 3, 9)),
+          (96, 48, 40): ((20, 30, 1, 12, 10, 20), (50, 60, 30, 40, 15, 30))}
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+@pytest.mark.parametrize("dims", list(RAGGED))
+def test_z_marching_v_cycle_matches_grid_wide(precision, dims):
+    """The finest level of the p' V-cycle as z-marching passes over
+    TMA-staged planes (p_level0 = 0, both colours of a sweep in one pass)
+    against the grid-wide passes (p_level0 = 1, one per colour), on grids
+    whose tiles are partial in x and y.  After one CG iteration p' = alpha z
+    with z the V-cycle's output: z is the same bit for bit in both forms and
+    alpha differs only by the summation order of its dot products, so the two
+    p' fields are one scalar apart (to the rounding of the products; FP32
+    storage in the mixed form)."""
+    deck = _deck(*dims, blocks=RAGGED[dims])
+    outs = []
+    for form in (0, 1):
+        g, _, _ = _pair(deck, re=100.0, precision=precision, p_maxiter=1, p_level0=form)
+        st = g.step(1, flags=2)
+        assert st["pcg_iters"] == 1
+        outs.append(g.field("p_prime"))
+        g.close()
+    a, b = outs
+    assert np.linalg.norm(b) > 0
+    c = a.dot(b) / b.dot(b)
+    tol = 1e-14 if precision == 0 else 2e-7
+    assert abs(c - 1.0) < 1e-10
+    assert np.linalg.norm(a - c * b) <= tol * np.linalg.norm(a)
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_z_marching_solves_match_grid_wide(precision):
+    """Full p' solves to 1e-10 in both forms of the finest level: the same
+    CG iteration counts (within one) and the same fields after four outer
+    steps (to 1e-8)."""
+    dims = (96, 48, 40)
+    deck = _deck(*dims, blocks=RAGGED[dims])
+    runs = []
+    for form in (0, 1):
+        g, _, _ = _pair(deck, re=100.0, precision=precision, p_tol=1e-10, p_level0=form)
+        its = [g.step(1)["pcg_iters"] for _ in range(4)]
+        runs.append((its, {f: g.field(f) for f in FACE + ["p", "T", "p_prime"]}))
+        g.close()
+    (ia, fa), (ib, fb) = runs
+    assert all(abs(x - y) <= 1 for x, y in zip(ia, ib)), (ia, ib)
+    for name in FACE + ["p", "T", "p_prime"]:
+        assert _rel(fa[name], fb[name]) < 1e-8, name

@@ -1,0 +1,149 @@
+"""The channel path on the GPU against the oracle at the configurations the
+bench and the specification name:
+
+* 256 x 128 x 128 (the bench case, 8 seeded blocks): the momentum sweeps bit
+  for bit over two steps; one full outer step checked on the oracle's own
+  operators: the GPU's p' solves the oracle's p' system (its residual on
+  that system is the solve's tolerance), the correction from it is bit for
+  bit the oracle's, and the GPU's unrelaxed temperature solves the oracle's
+  energy system;
+* 128 x 64 x 64 (the adjoint configuration, 4 blocks): the state the GPU
+  converges to (global residual 1e-6) is a fixed point of the oracle's
+  discrete equations: the oracle's momentum, continuity and energy residuals
+  of the GPU's fields are at the converged level of the GPU's normalisers;
+  the mixed form converges in the same steps to the same fields;
+* 512 x 256 x 256 (33.5M cells, 32 blocks): the momentum sweeps bit for bit,
+  and the mixed form against the FP64 form over three outer steps.
+
+An oracle trajectory to convergence is out of reach at these sizes (its
+inner solvers are the unpreconditioned ones: ~930 CG and 200 BiCGStab
+iterations per outer step at 128 x 64 x 64, hours to convergence), so the
+larger checks evaluate the GPU's states with the oracle's operators.  The
+oracle runs on every host thread here (bit-exact comparisons do not depend
+on its summation order)."""
+import contextlib
+import os
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+FACE = ["u", "v", "w"]
+
+
+@contextlib.contextmanager
+def _all_threads():
+    from oracle import oracle
+    prev = oracle.set_threads(os.cpu_count() or 1)
+    try:
+        yield
+    finally:
+        oracle.set_threads(prev)
+
+
+def _rel(a, b):
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
+
+
+def _pair(name, **kw):
+    import bench
+    import hsolver_b200
+    from oracle import oracle
+    deck, re_, k, q, _ = bench.workload(name)
+    g = hsolver_b200.Channel(deck, re=re_, **kw)
+    g.set_solid(k, q)
+    g.init()
+    okw = {x: v for x, v in kw.items() if x in ("p_tol", "p_maxiter", "t_tol", "t_maxiter")}
+    o = oracle.ChannelCase(deck, re=re_, **okw)
+    o.set_solid(k, q)
+    o.init()
+    return g, o
+
+
+@pytest.mark.parametrize("name,steps", [("config2", 2), ("config5", 1)])
+def test_momentum_sweeps_bit_exact_at_scale(name, steps):
+    g, o = _pair(name)
+    with _all_threads():
+        for step in range(steps):
+            g.step(1, flags=3)
+            o.step(1, pressure=False, energy=False)
+            for f in FACE + ["u_star", "v_star", "w_star", "d_u", "d_v", "d_w"]:
+                a, b = g.field(f), o.field(f)
+                assert np.array_equal(a, b), (name, step, f, np.abs(a - b).max())
+    g.close()
+
+
+def test_config2_outer_step_on_the_oracles_operators():
+    from oracle import oracle
+    tol = 1e-10
+    g, o = _pair("config2", p_tol=tol, p_maxiter=400, t_tol=tol, t_maxiter=400)
+    with _all_threads():
+        t0 = g.field("T")
+        st = g.step(1)
+        assert st["pcg_relres"] <= tol and st["t_relres"] <= tol, st
+        pp = g.field("p_prime")
+        rel = oracle.channel_step_given(o, pp)
+        assert rel <= 1.05 * tol, rel  # the GPU's p' solves the oracle's system to the tolerance
+        for f in FACE + ["p", "u_star", "d_u"]:
+            assert np.array_equal(g.field(f), o.field(f)), f  # the correction from that p', bit for bit
+        t1 = g.field("T")
+        tt = t0 + (t1 - t0) / 0.9  # the energy solve before the relaxation (alpha_t = 0.9)
+        r, bn = oracle.channel_energy_residual(o, tt)
+        r0, _ = oracle.channel_energy_residual(o, t0)
+        assert r <= 1e-9 * r0, (r, r0, bn)
+    g.close()
+
+
+def test_config4_converged_state_is_a_fixed_point_of_the_oracle():
+    import bench
+    import hsolver_b200
+    from oracle import oracle
+    states = []
+    for prec in (0, 1):
+        deck, re_, k, q, _ = bench.workload("config4")
+        g = hsolver_b200.Channel(deck, re=re_, precision=prec)
+        g.set_solid(k, q)
+        g.init()
+        ok, steps, st = g.solve_to(1e-6, 6000)
+        assert ok, st
+        states.append((steps, st, {f: g.field(f) for f in FACE + ["p", "T"]}))
+        g.close()
+    (s64, st64, f64), (s32, _, f32) = states
+    assert s64 == s32, (s64, s32)  # the mixed form solves the FP64 equations: the same outer steps
+    for f in FACE + ["p", "T"]:
+        assert _rel(f32[f], f64[f]) < 1e-6, f
+    # the oracle's residuals of the GPU's FP64 state, against the GPU's normalisers
+    o = oracle.ChannelCase(deck, re=re_)
+    o.set_solid(k, q)
+    o.init()
+    for f in FACE + ["p", "T"]:
+        o.set_field(f, f64[f])
+    norm = st64["norm"]
+    with _all_threads():
+        r_e, _ = oracle.channel_energy_residual(o, f64["T"])
+        o.step(1, pressure=False, energy=False)  # momentum residuals at the state, continuity of its u*
+    res = o.stats()["res"]
+    for x in range(4):
+        assert res[x] <= 2e-6 * norm[x], (x, res[x], norm[x])
+    assert r_e <= 2e-6 * norm[4], (r_e, norm[4])
+
+
+def test_config5_mixed_against_fp64():
+    """The mixed form against the FP64 form over three outer steps at
+    512 x 256 x 256, with the inner solves converged (p' 1e-10, energy
+    1e-8): FP32 storage and sweeps inside the FP64 refinement leave the
+    fields within 1e-6."""
+    import bench
+    import hsolver_b200
+    deck, re_, k, q, _ = bench.workload("config5")
+    out = []
+    for prec in (0, 1):
+        g = hsolver_b200.Channel(deck, re=re_, precision=prec, p_tol=1e-10, p_maxiter=200, t_tol=1e-8, t_maxiter=200)
+        g.set_solid(k, q)
+        g.init()
+        g.step(3)
+        out.append({f: g.field(f) for f in FACE + ["p", "T"]})
+        g.close()
+    for f in FACE + ["p", "T"]:
+        assert _rel(out[1][f], out[0][f]) < 1e-6, (f, _rel(out[1][f], out[0][f]))
