@@ -20,6 +20,16 @@ struct OutputData {
   int globalid = -1;
 };
 
+// the fields of a channel run (Solver::solve with a ".channel" sidecar) on
+// the global grid: face velocities (Nx+1)NyNz, Nx(Ny+1)Nz, NxNy(Nz+1), cell
+// pressure and temperature, cell type (0 fluid, 1 solid) and solid region
+struct ChannelFields {
+  I64 Nx = 0, Ny = 0, Nz = 0;
+  std::vector<double> u, v, w, p, T;
+  std::vector<unsigned char> type;
+  std::vector<int> region;
+};
+
 struct FluidSolver {
   DistributedMesh &mesh;
   std::vector<I64> &metadata;
@@ -84,6 +94,43 @@ struct FluidSolver {
       p[i].data = pc[i]; p[i].isEmpty = empty[i] != 0;
       t[i].data = tc[i]; t[i].isEmpty = empty[i] != 0;
     }
+  }
+
+  // the public state from a channel run: the fluid box's faces and cells
+  // (metadata {cx,cy,cz,fx,fy,fz,ox,oy,oz}, 1-based origin), row ids
+  // numbering the fluid cells in k-j-i order as the reference's rows do
+  // (fluid_solver.h:1894-1906)
+  void pull_channel(const ChannelFields &F) {
+    const I64 cx = metadata[0], cy = metadata[1], cz = metadata[2], fx = metadata[3], fy = metadata[4],
+              fz = metadata[5];
+    const I64 ox = metadata[6] - 1, oy = metadata[7] - 1, oz = metadata[8] - 1;
+    const I64 Nx = F.Nx, Ny = F.Ny;
+    ux.resize((size_t)(fx * cy * cz));
+    uy.resize((size_t)(cx * fy * cz));
+    uz.resize((size_t)(cx * cy * fz));
+    for (I64 k = 0; k < cz; ++k)
+      for (I64 j = 0; j < cy; ++j)
+        for (I64 i = 0; i < fx; ++i) ux[i + fx * (j + cy * k)].u = F.u[(ox + i) + (Nx + 1) * ((oy + j) + Ny * (oz + k))];
+    for (I64 k = 0; k < cz; ++k)
+      for (I64 j = 0; j < fy; ++j)
+        for (I64 i = 0; i < cx; ++i) uy[i + cx * (j + fy * k)].u = F.v[(ox + i) + Nx * ((oy + j) + (Ny + 1) * (oz + k))];
+    for (I64 k = 0; k < fz; ++k)
+      for (I64 j = 0; j < cy; ++j)
+        for (I64 i = 0; i < cx; ++i) uz[i + cx * (j + cy * k)].u = F.w[(ox + i) + Nx * ((oy + j) + Ny * (oz + k))];
+    const I64 nc = cx * cy * cz;
+    p.resize((size_t)nc);
+    t.resize((size_t)nc);
+    id.assign((size_t)nc, -1);
+    int row = 0;
+    for (I64 k = 0; k < cz; ++k)
+      for (I64 j = 0; j < cy; ++j)
+        for (I64 i = 0; i < cx; ++i) {
+          const I64 c = i + cx * (j + cy * k), g = (ox + i) + Nx * ((oy + j) + Ny * (oz + k));
+          const bool empty = F.type[g] != 0;
+          p[c].data = F.p[g]; p[c].isEmpty = empty;
+          t[c].data = F.T[g]; t[c].isEmpty = empty;
+          if (!empty) id[c] = row++;
+        }
   }
 
   // Solver::getResult for this fluid (solver.h:160-188): one OutputData per

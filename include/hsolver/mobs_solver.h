@@ -71,6 +71,32 @@ struct MobSolver {
         }
   }
 
+  // the public state from a channel run: the temperatures of this box's
+  // cells of solid region r (the deck's region order), padded t_temp with
+  // the neighbouring cells' temperatures in its ghost layer
+  void pull_channel(const ChannelFields &F, int r) {
+    region = r;
+    const I64 cx = metadata[0], cy = metadata[1], cz = metadata[2];
+    const I64 ox = metadata[6] - 1, oy = metadata[7] - 1, oz = metadata[8] - 1;
+    auto gidx = [&](I64 i, I64 j, I64 k) { return i + F.Nx * (j + F.Ny * k); };
+    t.resize((size_t)(cx * cy * cz));
+    for (I64 k = 0; k < cz; ++k)
+      for (I64 j = 0; j < cy; ++j)
+        for (I64 i = 0; i < cx; ++i) {
+          const I64 g = gidx(ox + i, oy + j, oz + k);
+          t[i + cx * (j + cy * k)].data = F.T[g];
+          t[i + cx * (j + cy * k)].isEmpty = !(F.type[g] == 1 && F.region[g] == r);
+        }
+    t_temp.assign((size_t)((cx + 2) * (cy + 2) * (cz + 2)), 0.0);
+    for (I64 k = -1; k <= cz; ++k)
+      for (I64 j = -1; j <= cy; ++j)
+        for (I64 i = -1; i <= cx; ++i) {
+          const I64 gi = ox + i, gj = oy + j, gk = oz + k;
+          if (gi < 0 || gj < 0 || gk < 0 || gi >= F.Nx || gj >= F.Ny || gk >= F.Nz) continue;
+          t_temp[(i + 1) + (cx + 2) * ((j + 1) + (cy + 2) * (k + 1))] = F.T[gidx(gi, gj, gk)];
+        }
+  }
+
   // Solver::getResult for this solid (solver.h:189-211): temperature and location per cell
   void collect() {
     const I64 cx = metadata[0], cy = metadata[1], cz = metadata[2];

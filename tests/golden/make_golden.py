@@ -13,7 +13,8 @@ with `make -C oracle/ref`) on every deck in tests/golden/decks and stores:
 Needs the reference tree, named by the REF environment variable when the
 driver is not built yet; run it where that tree is, never on the GPU box.
 Usage: REF=<reference tree> python tests/golden/make_golden.py [--only DECK]
-(one deck's digests, merged into the existing file).
+(one deck's digests, merged into the existing file) [--proc] (the processor
+files of decks/small.in, tests/golden/proc_small).
 """
 import hashlib
 import json
@@ -57,12 +58,30 @@ def digest_entries(res):
     return out
 
 
+def write_processor_fixture():
+    """proc_small/processor0/{cells,faces,boundary}.txt: the processor files
+    the reference's decompose step writes for decks/small.in (nParts = 1),
+    read back by the drop-in CYCASMesh in tests/test_drop_in.py."""
+    import shutil
+    with tempfile.TemporaryDirectory() as work:
+        wd = os.path.join(work, "wd")
+        subprocess.run([DRIVER, os.path.join(HERE, "decks", "small.in"), wd, "-", "time:1"], check=True,
+                       stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        out = os.path.join(HERE, "proc_small", "processor0")
+        os.makedirs(out, exist_ok=True)
+        for name in ("cells.txt", "faces.txt", "boundary.txt"):
+            shutil.copyfile(os.path.join(wd, "processor0", name), os.path.join(out, name))
+
+
 def main():
     if not os.path.exists(DRIVER):
         ref = os.environ.get("REF")
         if not ref:
             sys.exit("set REF to the reference source tree (the driver oracle/_ref/ref_driver is built from it)")
         subprocess.run(["make", "-C", os.path.join(REPO, "oracle", "ref"), "REF=" + ref], check=True)
+    if len(sys.argv) > 1 and sys.argv[1] == "--proc":
+        write_processor_fixture()
+        return
     if len(sys.argv) > 2 and sys.argv[1] == "--only":
         # regenerate one deck's digests and merge them into the existing file
         deck = sys.argv[2]
