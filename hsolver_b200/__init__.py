@@ -362,6 +362,7 @@ def _channel_api(L):
         "hs_channel_adjoint": ([vp, ctypes.c_double, ctypes.c_int, dp, dp, ll, dp, ctypes.c_int,
                                 ctypes.POINTER(AdjointInfo)], ctypes.c_int),
         "hs_channel_profile": ([vp, ctypes.c_int], ctypes.c_int),
+        "hs_channel_balance": ([vp, dp], ctypes.c_int),
         "hs_channel_profile_read": ([vp, dp, ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
         "hs_channel_destroy": ([vp], None),
     }
@@ -476,6 +477,14 @@ class Channel:
         n = ctypes.c_int()
         self._check(self._L.hs_channel_profile_read(self.h, ms, ctypes.byref(n)))
         return dict(zip(self.PHASES, list(ms))), n.value
+
+    def balance(self):
+        """FP64 global balances of the current state (hs_channel_balance):
+        volume flux in and out, heat source, heat leaving through the
+        boundary."""
+        out = np.empty(4)
+        self._check(self._L.hs_channel_balance(self.h, _dptr(out)))
+        return {"flow_in": out[0], "flow_out": out[1], "heat_source": out[2], "heat_out": out[3]}
 
     def device_bytes(self):
         b = ctypes.c_longlong()

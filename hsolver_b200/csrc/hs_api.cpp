@@ -637,6 +637,14 @@ int hs_channel_sync(hs_channel *h) {
   return ch_guarded(h, [&](hs_channel &c) { hs::ch_sync(c.st); return HS_OK; });
 }
 
+int hs_channel_balance(hs_channel *h, double out[HS_CH_NBAL]) {
+  if (!out) return fail(nullptr, HS_ERR_ARG, "null output pointer");
+  return ch_guarded(h, [&](hs_channel &c) {
+    hs::ch_balance(c.st, out);
+    return HS_OK;
+  });
+}
+
 int hs_channel_device_bytes(hs_channel *h, long long *bytes) {
   if (!bytes) return fail(nullptr, HS_ERR_ARG, "null output pointer");
   return ch_guarded(h, [&](hs_channel &c) { *bytes = hs::ch_device_bytes(c.st); return HS_OK; });

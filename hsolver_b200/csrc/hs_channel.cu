@@ -1523,6 +1523,10 @@ int ch_profile_read(const ChannelState *S, double *ms5) {
 }
 
 void *ch_stream(ChannelState *S) { return S->stream; }
+void ch_balance(ChannelState *S, double out4[4]) {
+  CH_CUDA(cudaSetDevice(S->device));
+  cht_balance(S->cht, out4);
+}
 void ch_sync(ChannelState *S) { CH_CUDA(cudaSetDevice(S->device)); CH_CUDA(cudaStreamSynchronize(S->stream)); }
 long long ch_device_bytes(const ChannelState *S) { return S->bytes; }
 

@@ -50,6 +50,9 @@ void *ch_stream(ChannelState *s);
 void ch_profile(ChannelState *s, bool on);
 int ch_profile_read(const ChannelState *s, double *ms5);
 void ch_sync(ChannelState *s);
+// FP64 global balances of the current state (blocking): volume flux in and
+// out, heat source, heat leaving through the boundary
+void ch_balance(ChannelState *s, double out4[4]);
 long long ch_device_bytes(const ChannelState *s);
 // energy adjoint on the current (frozen) flow: forward solve of the energy
 // equation from T = t_in to tol, then the adjoint; J = (sum_solid T^8 V)^(1/8)

@@ -743,6 +743,53 @@ void cht_fill_T(ChtState *C, double v) {
 
 double *cht_T_device(ChtState *C) { return C->T; }
 
+namespace {
+// Global balances of the channel form (bc = 1) in FP64, by one block in a
+// fixed order: out = {volume flux in through x = 0, out through x = Nx,
+// sum of q V, heat leaving through the boundary}.  A boundary face with
+// outward flux F and conductance G_b carries G_b (T_P - Tb) + max(F, 0) T_P
+// - max(-F, 0) Tb out of the domain (the energy operator's boundary terms):
+// at x = 0, G_b = 2 k_P A / dx_P and F = -u A; at x = Nx, G_b = 0 and
+// F = u A; the walls carry nothing.
+__global__ void k_cht_balance(ChtDev H, const double *T, double Tb, double *out) {
+  __shared__ double sh[32];
+  const int Nx = H.Nx, Ny = H.Ny, Nz = H.Nz;
+  double in = 0.0, outf = 0.0, src = 0.0, heat = 0.0;
+  for (int e = threadIdx.x; e < Ny * Nz; e += blockDim.x) {
+    const int j = e % Ny, k = e / Ny;
+    const double A = H.dy[j] * H.dz[k];
+    const double u0 = H.ug[0 + (Nx + 1) * (j + Ny * k)], u1 = H.ug[Nx + (Nx + 1) * (j + Ny * k)];
+    in += u0 * A;
+    outf += u1 * A;
+    const int p0 = pidx(H, 0, j, k), p1 = pidx(H, Nx - 1, j, k);
+    const double T0 = T[p0], T1 = T[p1];
+    const double G0 = 2.0 * H.k[p0] * A / H.dx[0], F0 = -u0 * A, F1 = u1 * A;
+    heat += G0 * (T0 - Tb) + (F0 > 0.0 ? F0 * T0 : F0 * Tb);
+    heat += F1 > 0.0 ? F1 * T1 : F1 * Tb;
+  }
+  for (int e = threadIdx.x; e < Nx * Ny * Nz; e += blockDim.x) {
+    const int i = e % Nx, j = (e / Nx) % Ny, k = e / (Nx * Ny);
+    src += H.q[pidx(H, i, j, k)] * (H.dx[i] * H.dy[j] * H.dz[k]);
+  }
+  in = blk_sum(in, sh);
+  outf = blk_sum(outf, sh);
+  src = blk_sum(src, sh);
+  heat = blk_sum(heat, sh);
+  if (threadIdx.x == 0) { out[0] = in; out[1] = outf; out[2] = src; out[3] = heat; }
+}
+}  // namespace
+
+void cht_balance(ChtState *C, double out4[4]) {
+  HC_CUDA(cudaSetDevice(C->device));
+  double *d = nullptr;
+  HC_CUDA(cudaMallocAsync((void **)&d, 4 * sizeof(double), C->stream));
+  k_cht_balance<<<1, 1024, 0, C->stream>>>(C->H, C->T, C->Tb, d);
+  HC_CUDA(cudaGetLastError());
+  HC_CUDA(cudaMemcpyAsync(out4, d, 4 * sizeof(double), cudaMemcpyDeviceToHost, C->stream));
+  HC_CUDA(cudaFreeAsync(d, C->stream));
+  HC_CUDA(cudaStreamSynchronize(C->stream));
+}
+
 void cht_energy_step(ChtState *C, double alpha_t, double tol, int maxiter) {
   const ChtDev &H = C->H;
   const int n = H.Nx * H.Ny * H.Nz;

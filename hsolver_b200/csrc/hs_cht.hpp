@@ -52,5 +52,8 @@ void cht_step_results(ChtState *c, int *iters, double *relres, double *r0);
 // (pinned) host memory: iterations, then ||r|| / ||r0|| and ||r0||
 void cht_step_results_async(ChtState *c, int *iters, double *relres_r0);
 void cht_set_tolerance(ChtState *c, double tol, int maxiter);
+// channel form: FP64 global balances {volume flux in at x = 0, out at
+// x = Nx, sum of q V, heat leaving through the boundary faces}, blocking
+void cht_balance(ChtState *c, double out4[4]);
 
 }  // namespace hs

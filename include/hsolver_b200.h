@@ -309,6 +309,16 @@ int hs_channel_stream(hs_channel *h, void **stream);
  * steps since profiling was switched on (which resets them). */
 #define HS_CH_NPHASE 5
 int hs_channel_profile(hs_channel *h, int on);
+/* Global balances of the current state, summed in FP64 on the GPU (no
+ * counterpart in the reference, whose only global sums are the per-sweep
+ * residual allreduces, fluid_solver.h:485,571,654,878): out[0] volume flux
+ * in through the inlet x = 0, out[1] out through the outlet x = Nx (mass
+ * balance: equal at convergence), out[2] the heat source sum q V, out[3]
+ * the heat leaving through the boundary faces (convection at inlet and
+ * outlet relative to t_in, conduction through the inlet; heat balance: equal
+ * to out[2] at convergence).  Blocking. */
+#define HS_CH_NBAL 4
+int hs_channel_balance(hs_channel *h, double out[HS_CH_NBAL]);
 int hs_channel_profile_read(hs_channel *h, double ms[HS_CH_NPHASE], int *steps);
 int hs_channel_sync(hs_channel *h);
 /* Device memory the solver holds (bytes). */

@@ -375,3 +375,61 @@ def test_z_marching_solves_match_grid_wide(precision):
     assert all(abs(x - y) <= 1 for x, y in zip(ia, ib)), (ia, ib)
     for name in FACE + ["p", "T", "p_prime"]:
         assert _rel(fa[name], fb[name]) < 1e-8, name
+
+
+def _balance_numpy(o, deck, ctype, k_ratio, q, re=100.0, pr=0.71, t_in=0.0):
+    """The global balances restated from an oracle state: inlet / outlet
+    volume flux, sum q V, heat leaving through the boundary (inlet
+    conduction with the half-cell conductance 2 k A / dx, upwind convection
+    at inlet and outlet relative to t_in)."""
+    from oracle import oracle
+    Nx, Ny, Nz = o.dims
+    grids = []
+    oc = oracle.OracleCase(deck)
+    for axis in range(3):
+        import ctypes
+        g = np.empty(oc.dims[axis] + 1)
+        oracle.lib().or_get_grid(oc.h, axis, g.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), g.size)
+        grids.append(g)
+    dx, dy, dz = (np.diff(g) for g in grids)
+    A = np.outer(dz, dy)  # [k, j]
+    u = o.field("u").reshape(Nz, Ny, Nx + 1)
+    T = o.field("T").reshape(Nz, Ny, Nx)
+    kf = 1.0 * (grids[1][-1] - grids[1][0]) / re / pr
+    kcell = np.where(ctype.reshape(Nz, Ny, Nx) == 1, 0.0, kf)  # the inlet cells here are fluid
+    flow_in, flow_out = (u[:, :, 0] * A).sum(), (u[:, :, -1] * A).sum()
+    V = dz[:, None, None] * dy[None, :, None] * dx[None, None, :]
+    src = (q.reshape(Nz, Ny, Nx) * V).sum()
+    F0, F1 = -u[:, :, 0] * A, u[:, :, -1] * A
+    G0 = 2.0 * kcell[:, :, 0] * A / dx[0]
+    heat = (G0 * (T[:, :, 0] - t_in) + np.where(F0 > 0, F0 * T[:, :, 0], F0 * t_in)).sum()
+    heat += np.where(F1 > 0, F1 * T[:, :, -1], F1 * t_in).sum()
+    return np.array([flow_in, flow_out, src, heat])
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_global_balances(precision):
+    """hs_channel_balance (FP64 sums on the GPU) against the same sums
+    restated in NumPy on the oracle's state after the same steps, and the
+    balances' closure at convergence: inflow = outflow, heat source = heat
+    leaving through the boundary."""
+    deck = _deck()
+    kw = dict(re=100.0, p_tol=1e-13, p_maxiter=5000, t_tol=1e-13, t_maxiter=5000)
+    g, o, ctype = _pair(deck, precision=precision, **kw)
+    n = o.dims[0] * o.dims[1] * o.dims[2]
+    rng = np.random.default_rng(5)  # _pair's block physics
+    k = rng.uniform(10.0, 1000.0, o.nreg)
+    q = np.where(ctype == 1, rng.uniform(0.5, 2.0, n), 0.0)
+    g.step(4)
+    o.step(4)
+    b = g.balance()
+    got = np.array([b["flow_in"], b["flow_out"], b["heat_source"], b["heat_out"]])
+    exp = _balance_numpy(o, deck, ctype, k, q)
+    tol = 1e-9 if precision == 0 else 1e-6
+    assert np.all(np.abs(got - exp) <= tol * np.abs(exp)), (got, exp)
+    ok, _, _ = g.solve_to(1e-8, 4000)
+    assert ok
+    b = g.balance()
+    assert abs(b["flow_in"] - b["flow_out"]) <= 1e-8 * b["flow_in"], b
+    assert abs(b["heat_source"] - b["heat_out"]) <= 1e-5 * b["heat_source"], b
+    g.close()
