@@ -649,17 +649,22 @@ def probe(args):
         kw["t_tol"] = args.t_tol
     if args.t_maxiter is not None:
         kw["t_maxiter"] = args.t_maxiter
+    if args.p_level0 is not None:
+        kw["p_level0"] = args.p_level0
     g = hsolver_b200.Channel(deck, re=re_, precision=hsolver_b200.PREC_MIXED if args.mixed else hsolver_b200.PREC_FP64,
                              **kw)
     g.set_solid(k, q)
     g.init()
     its = []
+    g.profile(True)
     for _ in range(args.steps):
         st = g.step(1)
         its.append((st["pcg_iters"], st["t_iters"]))
     g.sync()
-    print("ok channel %s steps %d (pcg, energy) iterations per step %s (%.2f s)"
-          % (args.probe, args.steps, its, time.perf_counter() - t0))
+    ph, n = g.profile_read()
+    print("ok channel %s steps %d (pcg, energy) iterations per step %s (%.2f s); ms per step %s"
+          % (args.probe, args.steps, its, time.perf_counter() - t0,
+             {k: round(v / max(n, 1), 3) for k, v in ph.items()}))
 
 
 def replica_check(args):
@@ -708,6 +713,7 @@ def main(argv=None):
     ap.add_argument("--p-tol", type=float, default=None, help="--probe: p' relative tolerance")
     ap.add_argument("--t-tol", type=float, default=None, help="--probe: energy relative tolerance")
     ap.add_argument("--t-maxiter", type=int, default=None, help="--probe: energy iteration cap")
+    ap.add_argument("--p-level0", type=int, default=None, help="--probe: finest p' level form (0 z-marching, 1 grid-wide)")
     ap.add_argument("--replica-check", action="store_true", help=argparse.SUPPRESS)
     args = ap.parse_args(argv)
     if args.gpus > 1 and "WORLD_SIZE" not in os.environ and args.probe is None:

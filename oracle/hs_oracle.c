@@ -79,9 +79,9 @@ const char *or_last_error(void) { return err_buf; }
  * `while (lineiss >> value >> spliter)` does (mesh/mesh.cpp:1677): a value
  * followed by end-of-line (no separator) is dropped. */
 static int parse_line_doubles(const char *s, size_t n, double **out, int *cnt, int *cap) {
-  char buf[4096];
-  size_t m = n < sizeof(buf) - 1 ? n : sizeof(buf) - 1;
-  memcpy(buf, s, m); buf[m] = 0;
+  /* a line of any length, as std::getline reads it */
+  char *buf = malloc(n + 1);
+  memcpy(buf, s, n); buf[n] = 0;
   char *q = strchr(buf, ';');               /* sliceInputString, mesh/mesh.cpp:27-40 */
   if (q) *q = 0;
   char *p = buf;
@@ -99,13 +99,13 @@ static int parse_line_doubles(const char *s, size_t n, double **out, int *cnt, i
     if (*cnt == *cap) { *cap = *cap ? 2 * *cap : 64; *out = (double *)realloc(*out, sizeof(double) * (size_t)*cap); }
     (*out)[(*cnt)++] = v;
   }
+  free(buf);
   return 0;
 }
 
 static int parse_line_ints(const char *s, size_t n, int *vals, int maxv) {
-  char buf[4096];
-  size_t m = n < sizeof(buf) - 1 ? n : sizeof(buf) - 1;
-  memcpy(buf, s, m); buf[m] = 0;
+  char *buf = malloc(n + 1);
+  memcpy(buf, s, n); buf[n] = 0;
   char *q = strchr(buf, ';');
   if (q) *q = 0;
   char *p = buf; int cnt = 0;
@@ -122,6 +122,7 @@ static int parse_line_ints(const char *s, size_t n, int *vals, int maxv) {
     if (cnt < maxv) vals[cnt] = (int)v;
     cnt++;
   }
+  free(buf);
   return cnt;
 }
 

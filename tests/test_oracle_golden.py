@@ -84,3 +84,20 @@ def test_deck_parser_drops_value_without_trailing_comma(oracle_mod):
     with no separator; quirk.in's x-line ends in `2.2` without a comma."""
     oc = oracle_mod.OracleCase(read_deck("quirk"))
     assert oc.dims == (9, 6, 6)
+
+
+def test_oracle_reads_deck_lines_of_any_length():
+    """A 1000-cell axis puts ~8 kB on one deck line (more than the oracle's
+    former 4 kB line buffer held); the oracle reads it
+    whole, as std::getline does in the reference (mesh/mesh.cpp:1673), and
+    agrees with the product's case model."""
+    import numpy as np
+    from hsolver_b200 import cases
+    from oracle import oracle
+    import hsolver_b200
+    deck = cases.deck_text(np.linspace(0.0, 2.0, 1001), np.linspace(0.0, 1.0, 3), np.linspace(0.0, 1.0, 3),
+                           blocks=[(500, 510, 1, 1, 1, 1)])
+    assert max(len(x) for x in deck.splitlines()) > 4096
+    o = oracle.OracleCase(deck)
+    assert tuple(o.dims) == (1000, 2, 2)
+    assert tuple(hsolver_b200.Case(deck).dims) == (1000, 2, 2)
