@@ -552,6 +552,7 @@ template <class V>
 struct CgVec {
   int N0, N1, N2;
   int px;  // row pitch of every padded array (ChDev::PX)
+  int nch;  // the z-marching form's z-chunks (zm::pick_chunks)
   const V *acx, *acy, *acz;
   const uint8_t *solid;
   V *x, *r, *p, *p2, *s;  // p, p2: search direction, double-buffered
@@ -773,7 +774,7 @@ __global__ void __launch_bounds__(zm::kThreads, 1)
   }
   __syncthreads();
   zm::Pipe P{0u, 0u, 0u, 0u, 0};
-  const zm::Tiles Tl{N0, N1, N2, PX, (N0 + zm::kTX - 1) / zm::kTX, (N1 + zm::kTY - 1) / zm::kTY};
+  const zm::Tiles Tl{N0, N1, N2, PX, (N0 + zm::kTX - 1) / zm::kTX, (N1 + zm::kTY - 1) / zm::kTY, V.nch};
   // the two buffers of each double-buffered vector
   auto xm = [&](int i) { return i ? G.lv[0].rhs : G.lv[0].x; };
   auto rb = [&](int i) { return i ? V.r2 : V.r; };
@@ -1133,7 +1134,9 @@ CUtensorMap padded_map(EncodeTiled enc, const M *base, int px, int py, int pz, i
 template <class M>
 void setup_zm(ChannelState &S, CgVec<M> &V, mg::Hier<M> &G, PcgMaps &TM, int nsm) {
   S.use_zm = false;
-  if (!S.prm.p_precond || S.prm.p_level0 != 0 || G.L < 2 || G.ls < 1) return;
+  // p_level0: 0 the faster form on this pool (the grid-wide passes until the
+  // z-marching ones beat them), 1 grid-wide, 2 z-marching
+  if (!S.prm.p_precond || S.prm.p_level0 != 2 || G.L < 2 || G.ls < 1) return;
   const EncodeTiled enc = tensor_map_encoder();
   const int py = S.N1 + 2, pz = S.N2 + 2;
   auto fine = [&](const M *a) { return padded_map<M>(enc, a, S.PX, py, pz, zm::Box<M>::BX, zm::Box<M>::BY); };
@@ -1152,6 +1155,7 @@ void setup_zm(ChannelState &S, CgVec<M> &V, mg::Hier<M> &G, PcgMaps &TM, int nsm
   if (per < 1) return;
   S.zm_grid = per * nsm;
   S.zm_smem = smem;
+  V.nch = zm::pick_chunks(((S.N0 + zm::kTX - 1) / zm::kTX) * ((S.N1 + zm::kTY - 1) / zm::kTY), S.N2, S.zm_grid);
   S.use_zm = true;
 }
 
@@ -1263,7 +1267,7 @@ ChannelState *ch_create(const Case &c, const ChParams &p, int device) {
   if (!(p.re > 0) || !(p.pr > 0) || !(p.alpha_u > 0 && p.alpha_u <= 1) || !(p.alpha_p > 0 && p.alpha_p <= 1) ||
       !(p.alpha_t > 0 && p.alpha_t <= 1) || p.mom_sweeps < 1 || !(p.p_tol > 0) || p.p_maxiter < 0 || !(p.t_tol > 0) ||
       p.t_maxiter < 0 || (p.precision != 0 && p.precision != 1) || p.p_mg_sweeps < 0 || p.p_mg_sweeps > 8 ||
-      (p.p_level0 != 0 && p.p_level0 != 1))
+      p.p_level0 < 0 || p.p_level0 > 2)
     throw std::invalid_argument("invalid channel parameters");
   if ((long long)pitch4((int)c.Nx + 2) * (c.Ny + 2) * (c.Nz + 2) >= (1LL << 31))
     throw std::invalid_argument("grid too large for 32-bit indices");

@@ -3,10 +3,15 @@
 // Accelerator (TMA).  Device code only; every pass runs inside the
 // cooperative kernel of the p' solve (hs_channel.cu).
 //
-// Work split.  The level's interior is cut into kTX x kTY tiles in (x, y);
-// the tile-planes (tile-major, z-minor) are divided evenly over the blocks,
-// so each block marches in z over one or two runs of consecutive planes of a
-// tile (a segment).  Every pass has two stages per z step t:
+// Work split.  The level's interior is cut into kTX x kTY tiles in (x, y)
+// and its planes into nch z-chunks; a unit is one tile over one chunk (a
+// segment of consecutive planes).  The units, in chunk-major order, are dealt
+// round-robin over the blocks, so the blocks of one round march over
+// neighbouring tiles of the same chunk at the same time and each halo row a
+// block stages is, most of the time, a row its neighbour staged moments
+// before (in L2).  The host picks nch to balance the rounds against the two
+// extra planes each segment stages at either end.  Every pass has two stages
+// per z step t:
 //   stage 1: a value v1 on the tile and a one-cell ring around it (T+1) at
 //            plane t, kept in a three-plane shared-memory ring;
 //   stage 2: the pass's outputs on the tile (T) at plane t - 1, from the v1
@@ -106,6 +111,20 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
 }
 
+// waits (suspended in hardware, up to a system-dependent time) for the phase
+// with the given parity to complete; true when it has
+__device__ __forceinline__ bool mbar_try(uint64_t *bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
 __device__ __forceinline__ bool mbar_test(uint64_t *bar, uint32_t parity) {
   uint32_t ok;
   asm volatile(
@@ -190,9 +209,9 @@ __device__ __forceinline__ void wait_next(uint64_t *bars, Pipe &P) {
   if (P.fail) return;
   uint64_t *bar = bars + n % SLOTS;
   const uint32_t par = (n / SLOTS) & 1u;
-  if (!mbar_test(bar, par)) {
+  if (!mbar_try(bar, par)) {
     const uint64_t t0 = gtime();
-    while (!mbar_test(bar, par))
+    while (!mbar_try(bar, par))
       if (gtime() - t0 > kWaitNs) {
         P.fail = 1;
         return;
@@ -220,14 +239,22 @@ __device__ __forceinline__ void drain(uint64_t *bars, Pipe &P) {
 struct Tiles {
   int nx, ny, nz, px;  // level interior and row pitch
   int ntx, nty;        // tiles per axis
-  __device__ __forceinline__ long long units() const { return (long long)ntx * nty * nz; }
+  int nch;             // z-chunks
 };
 
-// this block's tile-planes [u0, u1)
-__device__ __forceinline__ void block_range(const Tiles &T, long long &u0, long long &u1) {
-  const long long U = T.units();
-  u0 = U * blockIdx.x / gridDim.x;
-  u1 = U * (blockIdx.x + 1) / gridDim.x;
+// the z-chunk count for `ntiles` tiles of nz planes over `blocks` blocks:
+// the fewest rounds of units weighed against the two planes each segment
+// stages beyond either end, i.e. minimal ceil(ntiles nch / blocks) * (nz /
+// nch + 4), the first such nch
+inline int pick_chunks(int ntiles, int nz, int blocks) {
+  int best = 1;
+  double cost = 1e300;
+  for (int c = 1; c <= (nz + 3) / 4; ++c) {
+    const long long rounds = ((long long)ntiles * c + blocks - 1) / blocks;
+    const double v = (double)rounds * ((double)(nz + c - 1) / c + 4.0);
+    if (v < cost) { cost = v; best = c; }
+  }
+  return best;
 }
 
 // local (box) coordinates of interior cell (i, j) of the tile at (i0, j0)
@@ -267,29 +294,44 @@ __device__ void run_pass(const Smem<M> &S, Pipe &P, const PassMaps &pm, const Ti
   constexpr int BX = Box<M>::BX, NS = Box<M>::SLOTS;
   const int nx = Tl.nx, ny = Tl.ny, nz = Tl.nz, PX = Tl.px;
   uint64_t *bars = S.bars();
-  long long u0, u1;
-  block_range(Tl, u0, u1);
+  const int ntiles = Tl.ntx * Tl.nty, units = ntiles * Tl.nch;
   const int t_id = threadIdx.x, NT = kThreads;
-  for (long long u = u0; u < u1;) {
-    const long long tile = u / nz;
-    const int k0 = (int)(u - tile * nz);
-    const int k1 = (int)((long long)nz < u1 - tile * nz ? nz : u1 - tile * nz);
-    u = tile * nz + k1;
-    const int i0 = (int)(tile % Tl.ntx) * kTX, j0 = (int)(tile / Tl.ntx) * kTY;
+  for (int u = blockIdx.x; u < units; u += gridDim.x) {
+    const int chunk = u / ntiles, tile = u - chunk * ntiles;
+    const int k0 = (int)((long long)nz * chunk / Tl.nch), k1 = (int)((long long)nz * (chunk + 1) / Tl.nch);
+    if (k1 <= k0) continue;
+    const int i0 = (tile % Tl.ntx) * kTX, j0 = (tile / Tl.ntx) * kTY;
     // planes k0 - 2 .. k1 + 1 are staged, in order; slot of plane k
     const uint32_t base = P.issued;
     const int kfirst = k0 - 2, klast = k1 + 1;
     auto slot_of = [&](int k) { return (int)((base + (uint32_t)(k - kfirst)) % NS); };
     for (int k = kfirst; k <= klast && k < kfirst + NS; ++k) issue(S, P, pm, i0, j0, k);
     int next = kfirst + NS;  // next plane to issue
+    // this thread's stage-2 cell at plane k: for A p the tile in row order;
+    // for the colour passes threads 0..255 take the second colour's cells and
+    // 256..511 the first colour's (row j0 + m / 16, its m % 16-th cell of the
+    // colour), so that no warp splits between updating and copying
+    auto cell = [&](int k, int &ci, int &cj) {
+      if (a.kind == kAp) {
+        ci = i0 + (t_id % kTX);
+        cj = j0 + (t_id / kTX);
+      } else {
+        const int m = t_id & (kTX * kTY / 2 - 1);
+        const int colour = t_id < kTX * kTY / 2 ? 1 - a.c1 : a.c1;
+        cj = j0 + m / (kTX / 2);
+        ci = i0 + 2 * (m % (kTX / 2)) + ((colour - cj - k) & 1);
+      }
+    };
     // the CG's x and p of this thread's stage-2 cell, one plane ahead
-    const int ci = i0 + (t_id % kTX), cj = j0 + (t_id / kTX);
-    const bool own = t_id < kTX * kTY && ci < nx && cj < ny;
     M xpre = M(0), ppre = M(0);
-    if (a.kind == kSeed && a.upd && own) {
-      const int g = (ci + 1) + PX * ((cj + 1) + (ny + 2) * (k0 + 1));
-      xpre = a.xcg[g];
-      ppre = a.pcg[g];
+    if (a.kind == kSeed && a.upd) {
+      int ci, cj;
+      cell(k0, ci, cj);
+      if (ci < nx && cj < ny) {
+        const int g = (ci + 1) + PX * ((cj + 1) + (ny + 2) * (k0 + 1));
+        xpre = a.xcg[g];
+        ppre = a.pcg[g];
+      }
     }
     for (int t = k0 - 1; t <= k1; ++t) {
       // planes t - 1 .. t + 1 resident
@@ -358,8 +400,9 @@ __device__ void run_pass(const Smem<M> &S, Pipe &P, const PassMaps &pm, const Ti
       const int k = t - 1;
       if (k >= k0) {
         const M *vm = S.ring((k + 2) % 3), *vc = S.ring((k + 3) % 3), *vp = v1;  // planes k - 1, k, k + 1
-        if (own) {
-          const int i = ci, j = cj;
+        int i, j;
+        cell(k, i, j);
+        if (i < nx && j < ny) {
           const int q = lq<M>(i, j, i0, j0);
           const int g = (i + 1) + PX * ((j + 1) + (ny + 2) * (k + 1));
           const M gxl = ZM_AT(2, sm, q), gxh = ZM_AT(2, sm, q + 1), gyl = ZM_AT(3, sm, q), gyh = ZM_AT(3, sm, q + BX);
@@ -374,7 +417,7 @@ __device__ void run_pass(const Smem<M> &S, Pipe &P, const PassMaps &pm, const Ti
             a.out2[g] = (M)sv;
             acc += (double)(M)sv * (double)p0;
           } else {
-            const bool second = ((i + j + k) & 1) != a.c1;
+            const bool second = t_id < kTX * kTY / 2;  // ((i + j + k) & 1) != c1
             M rhs;
             if (a.kind == kSeed && a.upd) rhs = (M)((double)ZM_AT(0, sm, q) - a.alpha * (double)ZM_AT(1, sm, q));
             else rhs = ZM_AT(a.kind == kSeed ? 0 : 1, sm, q);
@@ -395,10 +438,14 @@ __device__ void run_pass(const Smem<M> &S, Pipe &P, const PassMaps &pm, const Ti
             }
           }
         }
-        if (a.kind == kSeed && a.upd && own && k + 1 < k1) {  // the next plane's x and p
-          const int g = (ci + 1) + PX * ((cj + 1) + (ny + 2) * (k + 2));
-          xpre = a.xcg[g];
-          ppre = a.pcg[g];
+        if (a.kind == kSeed && a.upd && k + 1 < k1) {  // the next plane's x and p
+          int ci, cj;
+          cell(k + 1, ci, cj);
+          if (ci < nx && cj < ny) {
+            const int g = (ci + 1) + PX * ((cj + 1) + (ny + 2) * (k + 2));
+            xpre = a.xcg[g];
+            ppre = a.pcg[g];
+          }
         }
       }
       // every read of plane t - 1's slot is done: refill it with plane `next`

@@ -271,10 +271,11 @@ typedef struct hs_channel_params {
                           (0: the default, 2); the coarser levels take one
                           more */
   int p_level0;        /* form of the finest level of the p' solve: 0 (the
-                          default) z-marching passes with TMA-staged planes
+                          default) the faster of the two on B200 (today the
+                          grid-wide passes), 1 grid-wide passes (one per
+                          colour), 2 z-marching passes with TMA-staged planes
                           (both colours of a red-black sweep in one pass)
-                          wherever the grid has a coarser level below it, 1
-                          grid-wide passes (one per colour) */
+                          wherever the grid has a coarser level below it */
   double reserved[5];
 } hs_channel_params;
 typedef struct hs_channel_stats {

@@ -335,7 +335,7 @@ RAGGED = {(40, 20, 12): ((9, 14, 1, 6, 4, 8), (20, 26, 10, 16, 3, 9)),
 @pytest.mark.parametrize("dims", list(RAGGED))
 def test_z_marching_v_cycle_matches_grid_wide(precision, dims):
     """The finest level of the p' V-cycle as z-marching passes over
-    TMA-staged planes (p_level0 = 0, both colours of a sweep in one pass)
+    TMA-staged planes (p_level0 = 2, both colours of a sweep in one pass)
     against the grid-wide passes (p_level0 = 1, one per colour), on grids
     whose tiles are partial in x and y.  After one CG iteration p' = alpha z
     with z the V-cycle's output: z is the same bit for bit in both forms and
@@ -344,7 +344,7 @@ def test_z_marching_v_cycle_matches_grid_wide(precision, dims):
     storage in the mixed form)."""
     deck = _deck(*dims, blocks=RAGGED[dims])
     outs = []
-    for form in (0, 1):
+    for form in (2, 1):
         g, _, _ = _pair(deck, re=100.0, precision=precision, p_maxiter=1, p_level0=form)
         st = g.step(1, flags=2)
         assert st["pcg_iters"] == 1
@@ -366,7 +366,7 @@ def test_z_marching_solves_match_grid_wide(precision):
     dims = (96, 48, 40)
     deck = _deck(*dims, blocks=RAGGED[dims])
     runs = []
-    for form in (0, 1):
+    for form in (2, 1):
         g, _, _ = _pair(deck, re=100.0, precision=precision, p_tol=1e-10, p_level0=form)
         its = [g.step(1)["pcg_iters"] for _ in range(4)]
         runs.append((its, {f: g.field(f) for f in FACE + ["p", "T", "p_prime"]}))
