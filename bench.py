@@ -713,7 +713,7 @@ def main(argv=None):
     ap.add_argument("--p-tol", type=float, default=None, help="--probe: p' relative tolerance")
     ap.add_argument("--t-tol", type=float, default=None, help="--probe: energy relative tolerance")
     ap.add_argument("--t-maxiter", type=int, default=None, help="--probe: energy iteration cap")
-    ap.add_argument("--p-level0", type=int, default=None, help="--probe: finest p' level form (0 z-marching, 1 grid-wide)")
+    ap.add_argument("--p-level0", type=int, default=None, help="--probe: finest p' level form (0 the default, 1 grid-wide, 2 z-marching)")
     ap.add_argument("--replica-check", action="store_true", help=argparse.SUPPRESS)
     args = ap.parse_args(argv)
     if args.gpus > 1 and "WORLD_SIZE" not in os.environ and args.probe is None:
