@@ -72,8 +72,8 @@ MG_SWEEPS = 2
 # p' solve, correction, energy assembly, energy BiCGStab, energy relaxation
 LAUNCHES_PER_STEP = 11
 # DRAM bytes per CG iteration of k_ch_pcg on this case, from one ncu capture
-# (profiles/k_ch_pcg_config2_dram.md: 18.12 GB per 8-iteration launch)
-PCG_TRAFFIC_PER_ITER = 18.12e9 / 8
+# (profiles/k_ch_pcg_config2.md: 18.30 GB per 8-iteration launch)
+PCG_TRAFFIC_PER_ITER = 18.30e9 / 8
 
 
 def workload(name=NAME, seed=0, host_side=False):
