@@ -658,7 +658,7 @@ __global__ void __launch_bounds__(PcgT<M>::v, 1) k_ch_pcg(CgVec<M> V, mg::Hier<M
   auto rz = [&]() {
     double a = 0.0;
     if (!precond) return bb;
-    if (!mg::vcycle(G, false, grid, tid, T, V.r, &a))
+    if (!mg::vcycle<M, M, true>(G, false, grid, tid, T, V.r, &a))
       for (mg::Walk w(N0, N1, V.N2, tid, T); w.ok(); w.next()) {
         const int q = (w.m + 1) + PX * ((w.j + 1) + PY * (w.k + 1));
         a += (double)V.r[q] * (double)__ldcg(L0.x + q);
@@ -1147,7 +1147,10 @@ void setup_zm(ChannelState &S, CgVec<M> &V, mg::Hier<M> &G, PcgMaps &TM, int nsm
   TM.s = fine(V.s);
   const mg::Level<M> &L1 = G.lv[1];
   TM.x1 = padded_map<M>(enc, L1.x, L1.px, L1.ny + 2, L1.nz + 2, zm::Box<M>::CBX, zm::Box<M>::CBY);
-  // the ring shares the launch's dynamic shared memory with block 0's staging of the small levels
+  // the ring shares the launch's dynamic shared memory with block 0's staging
+  // of the small levels, which therefore holds their x and rhs only (the
+  // read-only arrays would not survive the ring between V-cycles)
+  mg::plan_stage(G, false);
   const size_t smem = std::max<size_t>((size_t)zm::Box<M>::SMEM + 128, (size_t)G.stage);
   CH_CUDA(cudaFuncSetAttribute((const void *)k_ch_pcg_zm<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int per = 0;
@@ -1313,9 +1316,9 @@ ChannelState *ch_create(const Case &c, const ChParams &p, int device) {
   S->res = S->alloc<double>(4);
   int per = 0, nsm = 0;
   CH_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
-  // the V-cycle's staging of block 0's levels: up to kMgStageMax bytes per launch
+  // the V-cycle's staging of block 0's levels: up to kMgStageTotal bytes per launch
   const void *pk = S->mixed ? (const void *)k_ch_pcg<float> : (const void *)k_ch_pcg<double>;
-  CH_CUDA(cudaFuncSetAttribute(pk, cudaFuncAttributeMaxDynamicSharedMemorySize, mg::kMgStageMax));
+  CH_CUDA(cudaFuncSetAttribute(pk, cudaFuncAttributeMaxDynamicSharedMemorySize, mg::kMgStageTotal));
   CH_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, pk, S->mixed ? PcgT<float>::v : PcgT<double>::v,
                                                         S->mixed ? S->Gf.stage : S->Gd.stage));
   if (per < 1) throw std::runtime_error("pressure-correction kernel cannot be resident");

@@ -428,9 +428,9 @@ __global__ void k_cht_fill(int n, int Nx, int Ny, double v, double *T) {
 int coop_grid(const void *kernel, int device) {
   int nsm = 0, per = 0;
   HC_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
-  // the V-cycle's staging of block 0's levels: up to kMgStageMax bytes per launch
-  HC_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, mg::kMgStageMax));
-  HC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, kBiT, mg::kMgStageMax));
+  // the V-cycle's staging of block 0's levels: up to kMgStageTotal bytes per launch
+  HC_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, mg::kMgStageTotal));
+  HC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, kBiT, mg::kMgStageTotal));
   if (per < 1) throw std::runtime_error("cooperative kernel cannot be resident");
   return per * nsm;
 }
@@ -494,7 +494,7 @@ void setup_levels(ChtState &C, mg::Hier<MT> &G) {
   }
   G.L = L;
   G.lu = C.alloc<double>((size_t)mg::kMgCoarse * mg::kMgCoarse);
-  mg::plan_stage(G);
+  mg::plan_stage(G, false);  // the V-cycles of the energy solves keep their read-only arrays in global memory
 }
 }  // namespace
 

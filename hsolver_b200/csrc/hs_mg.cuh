@@ -24,7 +24,9 @@
 // fused into the first post-smoothing half-sweep.  The coarse levels (at most kMgSmall
 // cells each, with x and rhs together at most kMgStageMax bytes) run inside block 0
 // alone, separated by __syncthreads instead of grid barriers, with their x and rhs
-// staged in the launch's dynamic shared memory (plan_stage).
+// staged in the launch's dynamic shared memory (plan_stage); the couplings, fluxes
+// and masks of as many of them as fit (coarsest first, up to kMgStageTotal bytes
+// in all) are copied there once per solve, after the hierarchy is built.
 #pragma once
 #include <cooperative_groups.h>
 #include <cstdint>
@@ -38,7 +40,8 @@ namespace cg = cooperative_groups;
 constexpr int kMgMaxLv = 16;
 constexpr int kMgCoarse = 64;
 constexpr long long kMgSmall = 2048;
-constexpr int kMgStageMax = 64 * 1024;  // bytes of dynamic shared memory the solvers' kernels accept
+constexpr int kMgStageMax = 64 * 1024;     // bytes of x and rhs of the levels block 0 runs alone
+constexpr int kMgStageTotal = 160 * 1024;  // with their read-only arrays: the dynamic shared memory the kernels accept
 
 template <class M>
 struct Level {
@@ -59,8 +62,10 @@ struct Hier {
   Level<M> lv[kMgMaxLv];
   double *lu;  // kMgCoarse^2: the factors, read back while the inverse is formed
   int ls;      // first level that block 0 handles alone (plan_stage)
-  int stage;   // bytes of dynamic shared memory holding x and rhs of levels ls..L-1
+  int stage;   // bytes of dynamic shared memory holding x and rhs of levels ls..L-1 and the read-only arrays
   int sx[kMgMaxLv], sr[kMgMaxLv];  // byte offsets of a staged level's x and rhs in it
+  int sro;     // first level whose couplings, fluxes and mask are staged too (L: none)
+  int sg[kMgMaxLv][3], sf[kMgMaxLv][3], sm[kMgMaxLv];  // their byte offsets (-1: the array is null)
 };
 
 // Grid-stride walk over an mx x ny x nz box in flat order (m fastest): the
@@ -103,11 +108,17 @@ __host__ __device__ __forceinline__ bool small(const Level<M> &L) { return (long
 // first of at most kMgSmall cells on, less the finest of them while their x
 // and rhs (padded layout as in global memory, each array 16-byte aligned)
 // exceed kMgStageMax bytes; the coarsest (<= kMgCoarse cells) always fits.
-// Places those arrays in the launch's dynamic shared memory (G.stage bytes).
+// Places those arrays in the launch's dynamic shared memory (G.stage bytes),
+// followed, when ro is set, by the couplings, fluxes and mask of the coarsest
+// of those levels, as many as fit in kMgStageTotal bytes in all (levels
+// G.sro..L-1): they do not change during a solve and are copied in once
+// (stage_ro).  A kernel that reuses the staging area between the V-cycles
+// (the z-marching p' solve) plans with ro = false.
 template <class M>
-inline void plan_stage(Hier<M> &G) {
+inline void plan_stage(Hier<M> &G, bool ro = true) {
   G.ls = 0;
   G.stage = 0;
+  G.sro = G.L;
   if (G.L < 1) return;
   auto bytes = [&](int l) {
     const Level<M> &L = G.lv[l];
@@ -126,6 +137,22 @@ inline void plan_stage(Hier<M> &G) {
     off += 2 * bytes(l);
   }
   G.ls = ls;
+  for (int l = G.L - 1; ro && l >= ls; --l) {
+    const Level<M> &L = G.lv[l];
+    const long long mb = L.m ? (padded(L) + 15) / 16 * 16 : 0;
+    if (off + (L.fx ? 6 : 3) * bytes(l) + mb > kMgStageTotal) break;
+    for (int a = 0; a < 3; ++a) {
+      G.sg[l][a] = (int)off;
+      off += bytes(l);
+    }
+    for (int a = 0; a < 3; ++a) {
+      G.sf[l][a] = L.fx ? (int)off : -1;
+      if (L.fx) off += bytes(l);
+    }
+    G.sm[l] = L.m ? (int)off : -1;
+    off += mb;
+    G.sro = l;
+  }
   G.stage = (int)off;
 }
 
@@ -562,6 +589,58 @@ __device__ __forceinline__ void coarse_solve(const Level<M> &C) {
   }
 }
 
+// the launch's dynamic shared memory (Hier::stage bytes)
+__device__ __forceinline__ unsigned char *stage_smem() {
+  extern __shared__ __align__(16) unsigned char mg_stage[];
+  return mg_stage;
+}
+
+// level l (>= G.ls) with x and rhs in the staging area, and its read-only
+// arrays when RO is set and they are staged (l >= G.sro)
+template <bool RO = false, class M>
+__device__ __forceinline__ Level<M> staged(const Hier<M> &G, int l) {
+  Level<M> L = G.lv[l];
+  unsigned char *b = stage_smem();
+  L.x = reinterpret_cast<M *>(b + G.sx[l]);
+  L.rhs = reinterpret_cast<M *>(b + G.sr[l]);
+  if (RO && l >= G.sro) {
+    L.gx = reinterpret_cast<M *>(b + G.sg[l][0]);
+    L.gy = reinterpret_cast<M *>(b + G.sg[l][1]);
+    L.gz = reinterpret_cast<M *>(b + G.sg[l][2]);
+    if (L.fx) {
+      L.fx = reinterpret_cast<M *>(b + G.sf[l][0]);
+      L.fy = reinterpret_cast<M *>(b + G.sf[l][1]);
+      L.fz = reinterpret_cast<M *>(b + G.sf[l][2]);
+    }
+    if (L.m) L.m = b + G.sm[l];
+  }
+  return L;
+}
+
+// Block 0 copies the read-only arrays of levels G.sro.. into the staging
+// area (every thread of the block calls it; the hierarchy is built and
+// visible to block 0).  They stay there for the rest of the launch.
+template <class M>
+__device__ __forceinline__ void stage_ro(const Hier<M> &G) {
+  for (int l = G.sro; l < G.L; ++l) {
+    const Level<M> &Lg = G.lv[l];
+    const Level<M> Ls = staged<true>(G, l);
+    const int n = (int)padded(Lg);
+    for (int e = threadIdx.x; e < n; e += blockDim.x) {
+      Ls.gx[e] = __ldcg(Lg.gx + e);
+      Ls.gy[e] = __ldcg(Lg.gy + e);
+      Ls.gz[e] = __ldcg(Lg.gz + e);
+      if (Lg.fx) {
+        Ls.fx[e] = __ldcg(Lg.fx + e);
+        Ls.fy[e] = __ldcg(Lg.fy + e);
+        Ls.fz[e] = __ldcg(Lg.fz + e);
+      }
+      if (Lg.m) Ls.m[e] = __ldcg(Lg.m + e);
+    }
+  }
+  __syncthreads();
+}
+
 // build levels 1.. from level 0 and factor the coarsest (the caller filled level 0)
 template <class M>
 __device__ __forceinline__ void build(const Hier<M> &G, bool tr, cg::grid_group &grid, int tid, int T) {
@@ -576,22 +655,8 @@ __device__ __forceinline__ void build(const Hier<M> &G, bool tr, cg::grid_group 
     }
   }
   factor(G, tr);
+  if (blockIdx.x == 0) stage_ro(G);
   grid.sync();
-}
-
-// the launch's dynamic shared memory (Hier::stage bytes)
-__device__ __forceinline__ unsigned char *stage_smem() {
-  extern __shared__ __align__(16) unsigned char mg_stage[];
-  return mg_stage;
-}
-
-// level l (>= G.ls) with x and rhs in the staging area
-template <class M>
-__device__ __forceinline__ Level<M> staged(const Hier<M> &G, int l) {
-  Level<M> L = G.lv[l];
-  L.x = reinterpret_cast<M *>(stage_smem() + G.sx[l]);
-  L.rhs = reinterpret_cast<M *>(stage_smem() + G.sr[l]);
-  return L;
 }
 
 // Levels G.ls.. of the V-cycle, by block 0 alone (every thread of the block
@@ -599,12 +664,12 @@ __device__ __forceinline__ Level<M> staged(const Hier<M> &G, int l) {
 // the grid-wide passes left them: rhs and the seeded x) and its x is copied
 // back at the end; the coarser levels' x start from 0, so that their ghosts
 // are 0 as in global memory.  The arithmetic is that of the grid-wide passes.
-template <class M>
+template <bool RO, class M>
 __device__ __forceinline__ void small_levels(const Hier<M> &G, bool tr) {
   const int t = threadIdx.x, B = blockDim.x, ls = G.ls;
   {
     const Level<M> &Lg = G.lv[ls];
-    const Level<M> Ls = staged(G, ls);
+    const Level<M> Ls = staged<RO>(G, ls);
     const int n = (int)padded(Lg);
     for (int e = t; e < n; e += B) {
       const M xv = __ldcg(Lg.x + e), rv = __ldcg(Lg.rhs + e);
@@ -612,14 +677,14 @@ __device__ __forceinline__ void small_levels(const Hier<M> &G, bool tr) {
       Ls.rhs[e] = rv;
     }
     for (int l = ls + 1; l < G.L; ++l) {
-      const Level<M> C = staged(G, l);
+      const Level<M> C = staged<RO>(G, l);
       const int nc = (int)padded(C);
       for (int e = t; e < nc; e += B) C.x[e] = M(0);
     }
     __syncthreads();
   }
   for (int l = ls; l < G.L - 1; ++l) {
-    const Level<M> F = staged(G, l), C = staged(G, l + 1);
+    const Level<M> F = staged<RO>(G, l), C = staged<RO>(G, l + 1);
     const int ns = l == 0 ? G.nsw : G.nswc;
     smooth<M, true>(F, 1, tr, t, B);
     __syncthreads();
@@ -632,10 +697,10 @@ __device__ __forceinline__ void small_levels(const Hier<M> &G, bool tr) {
     restrict_res<M, true>(F, C, tr, t, B);
     __syncthreads();
   }
-  coarse_solve(staged(G, G.L - 1));
+  coarse_solve(staged<RO>(G, G.L - 1));
   __syncthreads();
   for (int l = G.L - 2; l >= ls; --l) {
-    const Level<M> F = staged(G, l), C = staged(G, l + 1);
+    const Level<M> F = staged<RO>(G, l), C = staged<RO>(G, l + 1);
     const int ns = l == 0 ? G.nsw : G.nswc;
     prolong_smooth<M, true>(F, C, tr, t, B);
     __syncthreads();
@@ -650,7 +715,7 @@ __device__ __forceinline__ void small_levels(const Hier<M> &G, bool tr) {
   }
   {
     const Level<M> &Lg = G.lv[ls];
-    const Level<M> Ls = staged(G, ls);
+    const Level<M> Ls = staged<RO>(G, ls);
     const int n = (int)padded(Lg);
     for (int e = t; e < n; e += B) Lg.x[e] = Ls.x[e];
   }
@@ -664,8 +729,9 @@ __device__ __forceinline__ void small_levels(const Hier<M> &G, bool tr) {
 // thread's share of sum dot_r x to *dot_acc and the final barrier is left to
 // the caller's reduction (returns true); it returns false, with the barrier
 // done and nothing added, when level 0 is handled by block 0 alone or is not
-// part of the call.
-template <class M, class RT = double>
+// part of the call.  RO: block 0's levels read the couplings, fluxes and
+// masks that stage_ro copied into shared memory (levels G.sro..).
+template <class M, class RT = double, bool RO = false>
 __device__ __forceinline__ bool vcycle(const Hier<M> &G, bool tr, cg::grid_group &grid, int tid, int T,
                        const RT *dot_r = nullptr, double *dot_acc = nullptr, int first = 0) {
   const int ls = G.ls;  // first level handled by block 0 alone
@@ -688,7 +754,7 @@ __device__ __forceinline__ bool vcycle(const Hier<M> &G, bool tr, cg::grid_group
     restrict_res(G.lv[l], G.lv[l + 1], tr, tid, T);
     grid.sync();
   }
-  if (blockIdx.x == 0) small_levels(G, tr);
+  if (blockIdx.x == 0) small_levels<RO>(G, tr);
   if (ls == first) last_sync();
   else grid.sync();
   for (int l = ls - 1; l >= first; --l) {

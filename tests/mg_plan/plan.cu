@@ -2,7 +2,8 @@
 // level dimensions of a hierarchy the way the solvers' set-up does (2x
 // coarsening, ceil, down to <= kMgCoarse cells) and prints, per precision,
 // the first level block 0 handles alone, the staging bytes and each staged
-// level's x / rhs offsets.  No device code runs.
+// level's x / rhs offsets, then the first level whose couplings are staged too
+// and their offsets.  No device code runs.
 #include <cstdio>
 #include <cstdlib>
 
@@ -22,6 +23,8 @@ void plan(int nx, int ny, int nz) {
   hs::mg::plan_stage(G);
   std::printf("%d %d %d %d", (int)sizeof(M), G.L, G.ls, G.stage);
   for (int l = G.ls; l < G.L; ++l) std::printf(" %d:%d", G.sx[l], G.sr[l]);
+  std::printf(" | %d", G.sro);
+  for (int l = G.sro; l < G.L; ++l) std::printf(" %d:%d:%d", G.sg[l][0], G.sg[l][1], G.sg[l][2]);
   std::printf("\n");
 }
 
