@@ -651,6 +651,10 @@ def probe(args):
         kw["t_maxiter"] = args.t_maxiter
     if args.p_level0 is not None:
         kw["p_level0"] = args.p_level0
+    if args.conv is not None:
+        kw["conv"] = args.conv
+    if args.ri is not None:
+        kw["ri"] = args.ri
     g = hsolver_b200.Channel(deck, re=re_, precision=hsolver_b200.PREC_MIXED if args.mixed else hsolver_b200.PREC_FP64,
                              **kw)
     g.set_solid(k, q)
@@ -714,6 +718,8 @@ def main(argv=None):
     ap.add_argument("--t-tol", type=float, default=None, help="--probe: energy relative tolerance")
     ap.add_argument("--t-maxiter", type=int, default=None, help="--probe: energy iteration cap")
     ap.add_argument("--p-level0", type=int, default=None, help="--probe: finest p' level form (0 the default, 1 grid-wide, 2 z-marching)")
+    ap.add_argument("--conv", type=int, default=None, help="--probe: momentum convection (0 upwind, 1 hybrid, 2 QUICK)")
+    ap.add_argument("--ri", type=float, default=None, help="--probe: Richardson number of the buoyancy term (along +z)")
     ap.add_argument("--replica-check", action="store_true", help=argparse.SUPPRESS)
     args = ap.parse_args(argv)
     if args.gpus > 1 and "WORLD_SIZE" not in os.environ and args.probe is None:

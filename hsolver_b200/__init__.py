@@ -24,6 +24,7 @@ FIELDS = {"u_star": 0, "v_star": 1, "w_star": 2, "p_temp": 3, "t_temp": 4, "up":
 PSOLVE_CG, PSOLVE_MGCG = 0, 1
 PREC_FP64, PREC_MIXED = 0, 1
 CH_SKIP_PRESSURE, CH_SKIP_ENERGY = 1, 2
+CONV_UPWIND, CONV_HYBRID, CONV_QUICK = 0, 1, 2
 CH_FIELDS = {"u": 0, "v": 1, "w": 2, "p": 3, "T": 4, "u_star": 5, "v_star": 6, "w_star": 7, "d_u": 8, "d_v": 9,
              "d_w": 10, "p_prime": 11}
 
@@ -320,7 +321,8 @@ class ChannelParams(ctypes.Structure):
                 ("mom_sweeps", ctypes.c_int), ("p_tol", ctypes.c_double), ("p_maxiter", ctypes.c_int),
                 ("t_tol", ctypes.c_double), ("t_maxiter", ctypes.c_int), ("precision", ctypes.c_int),
                 ("p_precond", ctypes.c_int), ("p_mg_sweeps", ctypes.c_int), ("p_level0", ctypes.c_int),
-                ("reserved", ctypes.c_double * 5)]
+                ("conv", ctypes.c_int), ("g_axis", ctypes.c_int), ("ri", ctypes.c_double),
+                ("reserved", ctypes.c_double * 3)]
 
 
 class ChannelStats(ctypes.Structure):

@@ -520,6 +520,7 @@ void hs_channel_params_default(hs_channel_params *p) {
   p->alpha_u = 0.7; p->alpha_p = 0.3; p->alpha_t = 0.9;
   p->mom_sweeps = 2; p->p_tol = 1e-8; p->p_maxiter = 1000; p->t_tol = 1e-2; p->t_maxiter = 200;
   p->precision = HS_PREC_FP64; p->p_precond = 1;
+  p->conv = HS_CONV_UPWIND; p->g_axis = 2; p->ri = 0.0;
 }
 
 
@@ -538,6 +539,7 @@ int hs_channel_create(const char *deck, const hs_channel_params *prm, int device
   q.alpha_u = p.alpha_u; q.alpha_p = p.alpha_p; q.alpha_t = p.alpha_t;
   q.mom_sweeps = p.mom_sweeps; q.p_tol = p.p_tol; q.p_maxiter = p.p_maxiter; q.t_tol = p.t_tol; q.t_maxiter = p.t_maxiter;
   q.precision = p.precision; q.p_precond = p.p_precond; q.p_mg_sweeps = p.p_mg_sweeps; q.p_level0 = p.p_level0;
+  q.conv = p.conv; q.g_axis = p.g_axis; q.ri = p.ri;
   hs_channel *h = new (std::nothrow) hs_channel();
   if (!h) return fail(nullptr, HS_ERR_NOMEM, "host allocation failed");
   try {

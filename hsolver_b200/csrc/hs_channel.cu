@@ -13,6 +13,13 @@
 //     (a_P/alpha_u) u_P = sum a_nb u_nb + (p_lo - p_hi) A + (1 - alpha_u)(a_P/alpha_u) u^n_P
 //     stencil order E W N S T B; the outlet neighbour is zero-gradient (dropped),
 //     a wall or inlet neighbour is 0 at half a cell; d = A / (a_P/alpha_u)
+//   convection scheme: first-order upwind (above; the reference's), hybrid
+//     a_nb = max(-+F, D -+ F/2, 0), or QUICK by deferred correction: the upwind
+//     operator implicit and b += sum over the control-volume faces of
+//     -+F (u_f^QUICK - u_f^upwind) at u^n, the QUICK value from per-axis weight
+//     tables (quick_weights; upwind where the far-upwind node is off the grid)
+//   buoyancy (Boussinesq): b += ri (T_f - t_in) A h on the faces of axis
+//     g_axis, T_f the mean of the two cells' T^n
 //   red-black Gauss-Seidel on the face colour (i+j+k)&1: one pass per colour,
 //   all three components in one launch (they only read each other's u^n)
 //   p': couplings A d per face (A d(N_x - 1) at the outlet, p' = 0 outside),
@@ -86,6 +93,11 @@ struct ChDev {
   // correctly rounded reciprocals of the divisors known ahead (FP64 arithmetic only)
   const double *rd0, *rd1, *rd2, *rh0, *rh1, *rh2;  // 1 / cell width, 1 / centre distance
   double rau;                                       // 1 / alpha_u
+  int conv;           // 0 upwind, 1 hybrid, 2 QUICK (deferred correction)
+  int g_axis;         // buoyancy along + this axis
+  double ri, t_in;    // Richardson number (0: no buoyancy), reference temperature
+  const double *T;    // T^n, padded cells (row pitch N0 + 2), the energy solver's array
+  const double *qw[3][2];  // QUICK weights per axis: [0] cell nodes, [1] face nodes (6 per control-volume face)
 };
 
 __host__ __device__ constexpr bool is_mixed(float) { return true; }
@@ -151,13 +163,53 @@ __device__ __forceinline__ R face_area(const ChDev<R> &H, const int (&c)[3]) {
 template <int A, class R>
 __device__ __forceinline__ int fidx3(const ChDev<R> &H, const int (&c)[3]) { return fidx<A>(H, c[0], c[1], c[2]); }
 
+template <class R> __device__ __forceinline__ R rmaxd(R a, R b) { return a < b ? b : a; }  // maxd(a, b)
+
+// coefficient of the neighbour across a control-volume face of conductance D
+// and flux F (+ direction) on its high (HI) or low side: upwind D + max(-+F, 0),
+// or hybrid max(-+F, D -+ F/2, 0)
+template <int HI, class R>
+__device__ __forceinline__ R anb(int conv, R D, R F) {
+  if (conv == 1) return HI ? rmaxd(rmaxd(-F, D - R(0.5) * F), R(0)) : rmaxd(rmaxd(F, D + R(0.5) * F), R(0));
+  return HI ? D + rmax0(-F) : D + rmax0(F);
+}
+
+// QUICK deferred-correction term F (u_f^QUICK - u_f^upwind) of the control-
+// volume face e along axis B of component A, from u^n (FP64): the nodes are
+// A's faces with the index along B replaced (faces of axis B itself when
+// B == A, kind 1: e between nodes e and e + 1; cell centres otherwise, kind
+// 0: e between nodes e - 1 and e); weights (far upwind, upwind, downwind)
+// for the flux direction, (0, 1, 0) where a node is off the grid
+template <int A, int B, class R>
+__device__ __forceinline__ double quick_term(const ChDev<R> &H, const int (&c)[3], int e, double F) {
+  constexpr int kind = B == A;
+  const double *w = H.qw[B][kind] + 6 * e + (F > 0.0 ? 0 : 3);
+  const int lo = kind ? e : e - 1;
+  int iuu = F > 0.0 ? lo - 1 : lo + 2, iu = F > 0.0 ? lo : lo + 1, id = F > 0.0 ? lo + 1 : lo;
+  const double w0 = w[0], w1 = w[1], w2 = w[2];
+  if (w0 == 0.0 && w2 == 0.0) iuu = id = iu;
+  const double *UA = Uarr<A>(H);
+  int q[3] = {c[0], c[1], c[2]};
+  q[B] = iuu;
+  const double uuu = UA[fidx3<A>(H, q)];
+  q[B] = iu;
+  const double uu = UA[fidx3<A>(H, q)];
+  q[B] = id;
+  const double ud = UA[fidx3<A>(H, q)];
+  const double uq = (w0 * uuu + w1 * uu) + w2 * ud;
+  return F * (uq - uu);
+}
+
 // one stencil term (neighbour across axis B, high side when HI) of the unknown
 // face (A, c): coefficient at the frozen iterate and the neighbour's face
 // index (-1: the neighbour value is 0 or the term is dropped)
-template <int A, int B, int HI, class R>
-__device__ __forceinline__ void term(const ChDev<R> &H, const int (&c)[3], R Ar, R da, R &coef, int &nb) {
+template <int A, int B, int HI, bool X, class R>
+__device__ __forceinline__ void term(const ChDev<R> &H, const int (&c)[3], R Ar, R da, R &coef, int &nb, R &Fo, int &eo) {
+  const int conv = X ? H.conv : 0;
   coef = R(0);
   nb = -1;
+  Fo = R(0);
+  eo = 0;
   const R *CA = Carr<A>(H);
   if constexpr (B == A) {
     int q[3] = {c[0], c[1], c[2]};
@@ -166,15 +218,19 @@ __device__ __forceinline__ void term(const ChDev<R> &H, const int (&c)[3], R Ar,
       if (!(A == 0 && q[0] == H.N0)) {
         const R F = R(0.5) * (CA[fidx3<A>(H, c)] + CA[fidx3<A>(H, q)]) * Ar;
         const R Dd = div_known(H.nu * Ar, wid<A>(H, c[A]), rwid<A>(H, c[A]));
-        coef = Dd + rmax0(-F);
+        coef = anb<1>(conv, Dd, F);
         nb = fidx3<A>(H, q);
+        Fo = F;
+        eo = c[A];
       }
     } else {
       q[A] -= 1;
       const R F = R(0.5) * (CA[fidx3<A>(H, q)] + CA[fidx3<A>(H, c)]) * Ar;
       const R Dd = div_known(H.nu * Ar, wid<A>(H, c[A] - 1), rwid<A>(H, c[A] - 1));
-      coef = Dd + rmax0(F);
+      coef = anb<0>(conv, Dd, F);
       nb = fidx3<A>(H, q);
+      Fo = F;
+      eo = c[A] - 1;
     }
   } else {
     constexpr int O = 3 - A - B;
@@ -186,24 +242,55 @@ __device__ __forceinline__ void term(const ChDev<R> &H, const int (&c)[3], R Ar,
     if (HI) { flo[B] += 1; fhi[B] += 1; }
     const R F = R(0.5) * (CB[fidx3<B>(H, flo)] * wid<A>(H, c[A] - 1) + CB[fidx3<B>(H, fhi)] * wid<A>(H, c[A])) * wo;
     int q[3] = {c[0], c[1], c[2]};
+    Fo = F;
     if (HI) {
       if (c[B] + 1 == ncell<B>(H)) {
-        if (B != 0) coef = div_known(H.nu * ar, ctr<B>(H, ncell<B>(H)), rctr<B>(H, ncell<B>(H))) + rmax0(-F);
+        if (B != 0) coef = anb<1>(conv, div_known(H.nu * ar, ctr<B>(H, ncell<B>(H)), rctr<B>(H, ncell<B>(H))), F);
       } else {
-        coef = div_known(H.nu * ar, ctr<B>(H, c[B] + 1), rctr<B>(H, c[B] + 1)) + rmax0(-F);
+        coef = anb<1>(conv, div_known(H.nu * ar, ctr<B>(H, c[B] + 1), rctr<B>(H, c[B] + 1)), F);
         q[B] += 1;
         nb = fidx3<A>(H, q);
+        eo = c[B] + 1;
       }
     } else {
       if (c[B] == 0) {
-        coef = div_known(H.nu * ar, ctr<B>(H, 0), rctr<B>(H, 0)) + rmax0(F);
+        coef = anb<0>(conv, div_known(H.nu * ar, ctr<B>(H, 0), rctr<B>(H, 0)), F);
       } else {
-        coef = div_known(H.nu * ar, ctr<B>(H, c[B]), rctr<B>(H, c[B])) + rmax0(F);
+        coef = anb<0>(conv, div_known(H.nu * ar, ctr<B>(H, c[B]), rctr<B>(H, c[B])), F);
         q[B] -= 1;
         nb = fidx3<A>(H, q);
+        eo = c[B];
       }
     }
   }
+}
+
+// The source terms beyond the pressure term of the unknown face (A, c), in
+// FP64 from u^n and T^n: bs (the pressure term) plus the QUICK deferred
+// correction (stencil order, - on the high faces, + on the low ones) and the
+// Boussinesq term, in the oracle's order
+template <int A>
+__device__ __forceinline__ double add_sources(const ChDev<double> &H, const int (&c)[3], const int (&nb)[6],
+                                              const double (&F)[6], const int (&e)[6], double A_, double da, double bs) {
+  if (H.conv == 2) {
+    double dc = 0.0;
+    if (nb[0] >= 0) dc -= quick_term<A, 0>(H, c, e[0], F[0]);
+    if (nb[1] >= 0) dc += quick_term<A, 0>(H, c, e[1], F[1]);
+    if (nb[2] >= 0) dc -= quick_term<A, 1>(H, c, e[2], F[2]);
+    if (nb[3] >= 0) dc += quick_term<A, 1>(H, c, e[3], F[3]);
+    if (nb[4] >= 0) dc -= quick_term<A, 2>(H, c, e[4], F[4]);
+    if (nb[5] >= 0) dc += quick_term<A, 2>(H, c, e[5], F[5]);
+    bs = bs + dc;
+  }
+  if (H.ri != 0.0 && A == H.g_axis) {
+    int lo[3] = {c[0], c[1], c[2]};
+    lo[A] -= 1;
+    const int P0 = H.N0 + 2, P1 = H.N1 + 2;
+    const double tl = H.T[(lo[0] + 1) + P0 * ((lo[1] + 1) + P1 * (lo[2] + 1))];
+    const double th = H.T[(c[0] + 1) + P0 * ((c[1] + 1) + P1 * (c[2] + 1))];
+    bs = bs + H.ri * (0.5 * (tl + th) - H.t_in) * A_ * da;
+  }
+  return bs;
 }
 
 // Mixed form, first pass: the FP64 form's residual of the relaxed equation
@@ -213,7 +300,7 @@ __device__ __forceinline__ void term(const ChDev<R> &H, const int (&c)[3], R Ar,
 // follow use FP32 coefficients from the FP32 copy, which only approximates
 // the correction operator: the fixed point solves the FP64 equations (defect
 // correction).
-template <int A>
+template <int A, bool X>
 __device__ __forceinline__ void mom_face_mixed_first(const ChDev<float> &H, const int (&c)[3], int f, bool upd,
                                                      bool last, double &racc, bool keep) {
   ChDev<double> H64;
@@ -225,21 +312,24 @@ __device__ __forceinline__ void mom_face_mixed_first(const ChDev<float> &H, cons
   H64.p = H.p; H64.nu = H.nu_d; H64.au = H.au_d; H64.u_in = H.u_in_d;
   H64.rd0 = H.rd0; H64.rd1 = H.rd1; H64.rd2 = H.rd2; H64.rh0 = H.rh0; H64.rh1 = H.rh1; H64.rh2 = H.rh2;
   H64.rau = H.rau;
+  H64.conv = H.conv; H64.g_axis = H.g_axis; H64.ri = H.ri; H64.t_in = H.t_in; H64.T = H.T;
+  for (int a = 0; a < 3; ++a) { H64.qw[a][0] = H.qw[a][0]; H64.qw[a][1] = H.qw[a][1]; }
   const double Ad = face_area<A>(H64, c);
   const double dad = ctr<A>(H64, c[A]);
-  double ad[6];
-  int nd[6];
-  term<A, 0, 1>(H64, c, Ad, dad, ad[0], nd[0]);
-  term<A, 0, 0>(H64, c, Ad, dad, ad[1], nd[1]);
-  term<A, 1, 1>(H64, c, Ad, dad, ad[2], nd[2]);
-  term<A, 1, 0>(H64, c, Ad, dad, ad[3], nd[3]);
-  term<A, 2, 1>(H64, c, Ad, dad, ad[4], nd[4]);
-  term<A, 2, 0>(H64, c, Ad, dad, ad[5], nd[5]);
+  double ad[6], Fd[6];
+  int nd[6], ed[6];
+  term<A, 0, 1, X>(H64, c, Ad, dad, ad[0], nd[0], Fd[0], ed[0]);
+  term<A, 0, 0, X>(H64, c, Ad, dad, ad[1], nd[1], Fd[1], ed[1]);
+  term<A, 1, 1, X>(H64, c, Ad, dad, ad[2], nd[2], Fd[2], ed[2]);
+  term<A, 1, 0, X>(H64, c, Ad, dad, ad[3], nd[3], Fd[3], ed[3]);
+  term<A, 2, 1, X>(H64, c, Ad, dad, ad[4], nd[4], Fd[4], ed[4]);
+  term<A, 2, 0, X>(H64, c, Ad, dad, ad[5], nd[5], Fd[5], ed[5]);
   const double aPd = ad[0] + ad[1] + ad[2] + ad[3] + ad[4] + ad[5];
   const double *UA = Uarr<A>(H);
   int lo[3] = {c[0], c[1], c[2]};
   lo[A] -= 1;
-  const double bs = (H.p[cidx(H, lo[0], lo[1], lo[2])] - H.p[cidx(H, c[0], c[1], c[2])]) * Ad;
+  double bs = (H.p[cidx(H, lo[0], lo[1], lo[2])] - H.p[cidx(H, c[0], c[1], c[2])]) * Ad;
+  if constexpr (X) bs = add_sources<A>(H64, c, nd, Fd, ed, Ad, dad, bs);
   double s = 0.0;
 #pragma unroll
   for (int n = 0; n < 6; ++n) s += ad[n] * (nd[n] >= 0 ? UA[nd[n]] : 0.0);
@@ -257,26 +347,26 @@ __device__ __forceinline__ void mom_face_mixed_first(const ChDev<float> &H, cons
 
 // momentum work on the unknown face (A, c): residual at u^n (first pass),
 // relaxed Gauss-Seidel update (upd), d (last sweep)
-template <int A, class R>
+template <int A, bool X, class R>
 __device__ __forceinline__ void mom_face(const ChDev<R> &H, const int (&c)[3], bool first, bool upd, bool last,
                                          double &racc, bool keep) {
   const int f = fidx3<A>(H, c);
   if constexpr (is_mixed(R())) {
     if (first) {
-      mom_face_mixed_first<A>(H, c, f, upd, last, racc, keep);
+      mom_face_mixed_first<A, X>(H, c, f, upd, last, racc, keep);
       return;
     }
   }
   const R Ar = face_area<A>(H, c);
   const R da = ctr<A>(H, c[A]);
-  R an[6];
-  int nb[6];
-  term<A, 0, 1>(H, c, Ar, da, an[0], nb[0]);
-  term<A, 0, 0>(H, c, Ar, da, an[1], nb[1]);
-  term<A, 1, 1>(H, c, Ar, da, an[2], nb[2]);
-  term<A, 1, 0>(H, c, Ar, da, an[3], nb[3]);
-  term<A, 2, 1>(H, c, Ar, da, an[4], nb[4]);
-  term<A, 2, 0>(H, c, Ar, da, an[5], nb[5]);
+  R an[6], Fn[6];
+  int nb[6], en[6];
+  term<A, 0, 1, X>(H, c, Ar, da, an[0], nb[0], Fn[0], en[0]);
+  term<A, 0, 0, X>(H, c, Ar, da, an[1], nb[1], Fn[1], en[1]);
+  term<A, 1, 1, X>(H, c, Ar, da, an[2], nb[2], Fn[2], en[2]);
+  term<A, 1, 0, X>(H, c, Ar, da, an[3], nb[3], Fn[3], en[3]);
+  term<A, 2, 1, X>(H, c, Ar, da, an[4], nb[4], Fn[4], en[4]);
+  term<A, 2, 0, X>(H, c, Ar, da, an[5], nb[5], Fn[5], en[5]);
   const R aP = an[0] + an[1] + an[2] + an[3] + an[4] + an[5];
   const R apr = div_known(aP, H.au, H.rau);
   const double *UA = Uarr<A>(H);
@@ -285,7 +375,8 @@ __device__ __forceinline__ void mom_face(const ChDev<R> &H, const int (&c)[3], b
     // u* in place: a_P/alpha u_P = sum a_nb u_nb + b + (1 - alpha) a_P/alpha u^n_P
     int lo[3] = {c[0], c[1], c[2]};
     lo[A] -= 1;
-    const R bs = (H.p[cidx(H, lo[0], lo[1], lo[2])] - H.p[cidx(H, c[0], c[1], c[2])]) * Ar;
+    R bs = (H.p[cidx(H, lo[0], lo[1], lo[2])] - H.p[cidx(H, c[0], c[1], c[2])]) * Ar;
+    if constexpr (X) bs = add_sources<A>(H, c, nb, Fn, en, Ar, da, bs);
     const R un = UA[f];
     const R *src = first ? (const R *)UA : (const R *)SA;
     if (first) {
@@ -335,7 +426,7 @@ __device__ double block_sum(double v, double *sh) {
 // One red-black pass of all three momentum components (blockIdx.y = axis).
 // first: the pass of colour 0 in sweep 0, which also evaluates the residual of
 // every unknown face at u^n and writes the fixed faces of u* (delta = 0).
-template <int A, class R>
+template <int A, bool X, class R>
 __device__ void mom_pass_axis(const ChDev<R> &H, int color, bool first, bool last, double &racc) {
   const int nf0 = H.N0 + (A == 0), nf1 = H.N1 + (A == 1), nf2 = H.N2 + (A == 2);
   const int T = gridDim.x * blockDim.x, tid = blockIdx.x * blockDim.x + threadIdx.x;
@@ -353,7 +444,7 @@ __device__ void mom_pass_axis(const ChDev<R> &H, int color, bool first, bool las
       // face, so that no branch on the mask waits ahead of the stencil loads
       const bool keep = face_kind<A>(H, c) == 0;
       const bool mine = ((c[0] + c[1] + c[2]) & 1) == color;
-      mom_face<A>(H, c, true, mine, last && mine, racc, keep);
+      mom_face<A, X>(H, c, true, mine, last && mine, racc, keep);
       if (!keep) {
         Sarr<A>(H)[f] = R(0);
         Darr<A>(H)[f] = R(0);
@@ -365,19 +456,21 @@ __device__ void mom_pass_axis(const ChDev<R> &H, int color, bool first, bool las
       if (i >= nf0) continue;
       const int c[3] = {i, j, k};
       if (c[A] == 0 || c[A] == ncell<A>(H)) continue;
-      mom_face<A>(H, c, false, true, last, racc, face_kind<A>(H, c) == 0);
+      mom_face<A, X>(H, c, false, true, last, racc, face_kind<A>(H, c) == 0);
     }
   }
 }
 
-// four 256-thread blocks per SM (64 registers: above that the SM holds three)
-template <class R>
+// four 256-thread blocks per SM (64 registers: above that the SM holds three).
+// X: the extended momentum physics (hybrid or QUICK convection, buoyancy),
+// a separate instantiation so that the upwind form keeps its registers.
+template <class R, bool X>
 __global__ void __launch_bounds__(kT, 4) k_ch_mom(ChDev<R> H, int color, int first, int last, double *partials) {
   __shared__ double sh[32];
   double racc = 0.0;
-  if (blockIdx.y == 0) mom_pass_axis<0>(H, color, first, last, racc);
-  else if (blockIdx.y == 1) mom_pass_axis<1>(H, color, first, last, racc);
-  else mom_pass_axis<2>(H, color, first, last, racc);
+  if (blockIdx.y == 0) mom_pass_axis<0, X>(H, color, first, last, racc);
+  else if (blockIdx.y == 1) mom_pass_axis<1, X>(H, color, first, last, racc);
+  else mom_pass_axis<2, X>(H, color, first, last, racc);
   if (first) {
     const double b = block_sum(racc, sh);
     if (threadIdx.x == 0) partials[blockIdx.y * gridDim.x + blockIdx.x] = b;
@@ -998,6 +1091,41 @@ struct ChannelState {
 
 namespace {
 
+// QUICK weights along one axis (n cells, grid points pts[0..n]): for node kind
+// 1 (faces of this axis: control-volume faces at the cell centres, e = 0 ..
+// n - 1 between nodes e and e + 1) or 0 (cell centres: control-volume faces at
+// the grid points, e = 0 .. n between cells e - 1 and e), per e six weights,
+// (far upwind, upwind, downwind) for a flux in the + direction, then against
+// it: the quadratic through the three nodes at their positions evaluated at
+// the face (Leonard 1979), or (0, 1, 0) where a node is off the grid
+std::vector<double> quick_weights(const std::vector<double> &pts, int n, int kind) {
+  std::vector<double> W(6 * (size_t)(n + 1));
+  const int nn = kind ? n + 1 : n;  // nodes 0 .. nn - 1
+  auto xnode = [&](int m) { return kind ? pts[m] : 0.5 * (pts[m] + pts[m + 1]); };
+  for (int e = 0; e <= n; ++e) {
+    double *w = W.data() + 6 * (size_t)e;
+    if (kind && e == n) {  // no control-volume face there
+      w[0] = w[3] = 0.0; w[1] = w[4] = 1.0; w[2] = w[5] = 0.0;
+      continue;
+    }
+    const double xf = kind ? 0.5 * (pts[e] + pts[e + 1]) : pts[e];
+    const int lo = kind ? e : e - 1;
+    for (int dir = 0; dir < 2; ++dir) {
+      const int iuu = dir == 0 ? lo - 1 : lo + 2, iu = dir == 0 ? lo : lo + 1, id = dir == 0 ? lo + 1 : lo;
+      double *o = w + 3 * dir;
+      if (iuu < 0 || iuu >= nn || iu < 0 || iu >= nn || id < 0 || id >= nn) {
+        o[0] = 0.0; o[1] = 1.0; o[2] = 0.0;
+        continue;
+      }
+      const double xuu = xnode(iuu), xu = xnode(iu), xd = xnode(id);
+      o[0] = ((xf - xu) * (xf - xd)) / ((xuu - xu) * (xuu - xd));
+      o[1] = ((xf - xuu) * (xf - xd)) / ((xu - xuu) * (xu - xd));
+      o[2] = ((xf - xuu) * (xf - xu)) / ((xd - xuu) * (xd - xu));
+    }
+  }
+  return W;
+}
+
 template <class R>
 void setup_fields(ChannelState &S, ChDev<R> &H, const std::vector<double> (&d)[3], const std::vector<double> (&h)[3],
                   const uint8_t *solid) {
@@ -1050,6 +1178,22 @@ void setup_fields(ChannelState &S, ChDev<R> &H, const std::vector<double> (&d)[3
     *rd[a] = pd; *rh[a] = ph;
   }
   H.rau = 1.0 / S.prm.alpha_u;
+  H.conv = S.prm.conv;
+  H.g_axis = S.prm.g_axis;
+  H.ri = S.prm.ri;
+  H.t_in = S.prm.t_in;
+  H.T = nullptr;  // the energy solver's T, bound once it exists
+  const std::vector<double> *pts[3] = {&S.kase.deck.xs, &S.kase.deck.ys, &S.kase.deck.zs};
+  const int N[3] = {S.N0, S.N1, S.N2};
+  for (int a = 0; a < 3; ++a)
+    for (int kind = 0; kind < 2; ++kind) {
+      H.qw[a][kind] = nullptr;
+      if (S.prm.conv != 2) continue;
+      const std::vector<double> W = quick_weights(*pts[a], N[a], kind);
+      double *pw = S.alloc<double>(W.size());
+      CH_CUDA(cudaMemcpyAsync(pw, W.data(), W.size() * sizeof(double), cudaMemcpyHostToDevice, S.stream));
+      H.qw[a][kind] = pw;
+    }
 }
 
 template <class R> CgVec<R> &cg_vec(ChannelState &S);
@@ -1167,7 +1311,12 @@ void mom_solve(ChannelState &S, ChDev<R> &H) {
   const int sw = std::max(1, S.prm.mom_sweeps);
   for (int s = 0; s < sw; ++s)
     for (int color = 0; color < 2; ++color)
-      k_ch_mom<R><<<dim3(S.mom_blocks, 3), kT, 0, S.stream>>>(H, color, s == 0 && color == 0, s == sw - 1, S.mom_part);
+      if (H.conv != 0 || H.ri != 0.0)
+        k_ch_mom<R, true><<<dim3(S.mom_blocks, 3), kT, 0, S.stream>>>(H, color, s == 0 && color == 0, s == sw - 1,
+                                                                     S.mom_part);
+      else
+        k_ch_mom<R, false><<<dim3(S.mom_blocks, 3), kT, 0, S.stream>>>(H, color, s == 0 && color == 0, s == sw - 1,
+                                                                      S.mom_part);
   CH_CUDA(cudaGetLastError());
 }
 
@@ -1270,7 +1419,8 @@ ChannelState *ch_create(const Case &c, const ChParams &p, int device) {
   if (!(p.re > 0) || !(p.pr > 0) || !(p.alpha_u > 0 && p.alpha_u <= 1) || !(p.alpha_p > 0 && p.alpha_p <= 1) ||
       !(p.alpha_t > 0 && p.alpha_t <= 1) || p.mom_sweeps < 1 || !(p.p_tol > 0) || p.p_maxiter < 0 || !(p.t_tol > 0) ||
       p.t_maxiter < 0 || (p.precision != 0 && p.precision != 1) || p.p_mg_sweeps < 0 || p.p_mg_sweeps > 8 ||
-      p.p_level0 < 0 || p.p_level0 > 2)
+      p.p_level0 < 0 || p.p_level0 > 2 || p.conv < 0 || p.conv > 2 || p.g_axis < 0 || p.g_axis > 2 ||
+      !std::isfinite(p.ri))
     throw std::invalid_argument("invalid channel parameters");
   if ((long long)pitch4((int)c.Nx + 2) * (c.Ny + 2) * (c.Nz + 2) >= (1LL << 31))
     throw std::invalid_argument("grid too large for 32-bit indices");
@@ -1342,6 +1492,8 @@ ChannelState *ch_create(const Case &c, const ChParams &p, int device) {
   S->cht = cht_create(cs);
   CH_CUDA(cudaHostAlloc((void **)&S->ring, ChannelState::kRing * sizeof(ChannelState::StepRec), cudaHostAllocDefault));
   cht_bind_velocities(S->cht, uarr(S.get(), 0), uarr(S.get(), 1), uarr(S.get(), 2));
+  if (S->mixed) S->Hf.T = cht_T_device(S->cht);
+  else S->Hd.T = cht_T_device(S->cht);
   S->kratio.assign(S->nreg, 100.0);
   S->qcell.assign(n, 0.0);
   std::vector<double> kabs(S->nreg);

@@ -20,7 +20,10 @@ struct ChParams {
   int precision;                    // 0 FP64, 1 mixed (FP32 fields, sweeps and V-cycle)
   int p_precond;                    // 0 plain CG, 1 multigrid V-cycle
   int p_mg_sweeps;                  // V-cycle sweeps on the finest level (0: 2); coarser levels one more
-  int p_level0;                     // finest level of the p' solve: 0 z-marching passes where possible, 1 grid-wide
+  int p_level0;                     // finest level of the p' solve: 0 the default form, 1 grid-wide, 2 z-marching
+  int conv;                         // momentum convection: 0 first-order upwind, 1 hybrid, 2 QUICK (deferred correction)
+  int g_axis;                       // buoyancy along + this axis (gravity along -g_axis)
+  double ri;                        // Richardson number Gr / Re^2 of the Boussinesq term (0: none)
 };
 
 struct ChStats {

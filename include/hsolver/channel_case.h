@@ -11,6 +11,8 @@
 //   alpha_u, alpha_p, alpha_t           relaxation
 //   mom_sweeps, p_tol, p_maxiter, t_tol, t_maxiter, p_mg_sweeps   inner solvers
 //   precision = fp64 | mixed
+//   convection = upwind | hybrid | quick  momentum convection (upwind: the reference's)
+//   richardson = Ri, gravity_axis = x | y | z   Boussinesq buoyancy along + that axis
 //   k_ratio   = k1, k2, ...             k_solid / k_fluid per block (one value: every block)
 //   q         = q1, q2, ...             volumetric heat source per block (one value: every block)
 //   tol       = 1e-6                    optional: outer steps until the global residual <= tol
@@ -88,6 +90,17 @@ inline ChannelSpec parse_channel_spec(const std::string &text) {
       if (val == "fp64") s.prm.precision = HS_PREC_FP64;
       else if (val == "mixed") s.prm.precision = HS_PREC_MIXED;
       else throw std::runtime_error("channel sidecar: precision must be fp64 or mixed");
+    } else if (key == "convection") {
+      if (val == "upwind") s.prm.conv = HS_CONV_UPWIND;
+      else if (val == "hybrid") s.prm.conv = HS_CONV_HYBRID;
+      else if (val == "quick") s.prm.conv = HS_CONV_QUICK;
+      else throw std::runtime_error("channel sidecar: convection must be upwind, hybrid or quick");
+    } else if (key == "richardson") s.prm.ri = num(val);
+    else if (key == "gravity_axis") {
+      if (val == "x") s.prm.g_axis = 0;
+      else if (val == "y") s.prm.g_axis = 1;
+      else if (val == "z") s.prm.g_axis = 2;
+      else throw std::runtime_error("channel sidecar: gravity_axis must be x, y or z");
     } else if (key == "k_ratio") s.k_ratio = list();
     else if (key == "q") s.q = list();
     else if (key == "tol") s.tol = num(val);

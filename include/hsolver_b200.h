@@ -253,6 +253,9 @@ void hs_cht_destroy(hs_cht *h);
  * divided by its largest value over the first five outer steps. */
 #define HS_PREC_FP64 0
 #define HS_PREC_MIXED 1   /* FP32 fields, sweeps and V-cycle; FP64 residuals, CG recurrences, dots, coarsest solve */
+#define HS_CONV_UPWIND 0  /* a_nb = D + max(-+F, 0) (the reference's scheme) */
+#define HS_CONV_HYBRID 1  /* a_nb = max(-+F, D -+ F/2, 0) (Spalding) */
+#define HS_CONV_QUICK 2   /* upwind implicit, QUICK (Leonard) face values by deferred correction at u^n */
 #define HS_CH_SKIP_PRESSURE 1
 #define HS_CH_SKIP_ENERGY 2
 typedef struct hs_channel hs_channel;
@@ -276,7 +279,14 @@ typedef struct hs_channel_params {
                           colour), 2 z-marching passes with TMA-staged planes
                           (both colours of a red-black sweep in one pass)
                           wherever the grid has a coarser level below it */
-  double reserved[5];
+  int conv;            /* momentum convection, HS_CONV_*: the reference's
+                          first-order upwind (fluid_solver.h:441-447, 526-532,
+                          609-615), hybrid, or QUICK by deferred correction */
+  int g_axis;          /* Boussinesq buoyancy acts along + this axis (0..2) */
+  double ri;           /* Richardson number Gr/Re^2: b += ri (T_f - t_in) V on
+                          the faces of axis g_axis, T_f the mean T of the two
+                          cells at the start of the step (0: no buoyancy) */
+  double reserved[3];
 } hs_channel_params;
 typedef struct hs_channel_stats {
   double res[5];       /* u, v, w momentum, continuity, energy (absolute L2) */

@@ -1348,6 +1348,18 @@ int or_cht_adjoint(const or_cht *H, const double *T, double *lam, double *dJdq, 
  *   energy: the conjugate-heat-transfer operator above with bc = 1, fluid
  *   conductivity 1/(Re Pr), solid k_ratio/(Re Pr), warm-started BiCGStab to
  *   t_tol of its initial residual, T += alpha_t (T~ - T).
+ *   convection scheme (conv): 0 first-order upwind (the reference's); 1 hybrid
+ *     (Spalding 1972; Patankar 1980, sec. 5.2-5.3): a_E = max(-F, D - F/2, 0),
+ *     a_W = max(F, D + F/2, 0); 2 QUICK (Leonard 1979) by deferred correction
+ *     (Khosla & Rubin 1974): the upwind operator stays implicit and
+ *     b += sum over the control-volume faces of -+F (u_f^QUICK - u_f^upwind) at
+ *     u^n (- on the high faces, + on the low ones), u_f^QUICK the quadratic
+ *     through the far-upwind, upwind and downwind nodes at their positions
+ *     (the node values as stored: a fixed face holds its boundary value),
+ *     upwind where the far-upwind node lies outside the grid (ch_quick_w);
+ *   buoyancy (Boussinesq): on the faces of axis g_axis, b += ri (T_f - t_in) V
+ *     with T_f the mean T^n of the two cells and V = A h the face's control
+ *     volume (ri = Gr / Re^2, gravity along -g_axis);
  *   residuals: momentum ||a_P u^n - sum a_nb u^n_nb - b|| over unknown faces,
  *   continuity ||b(u*)||, energy ||b - A T^n||; the global residual is the
  *   largest of them divided by its maximum over the first five outer steps. */
@@ -1359,6 +1371,9 @@ typedef struct {
   int p_maxiter;
   double t_tol;
   int t_maxiter;
+  int conv;      /* 0 upwind, 1 hybrid, 2 QUICK (deferred correction) */
+  int g_axis;    /* buoyancy acts along + this axis (1 or 2) */
+  double ri;     /* Richardson number of the Boussinesq term (0: none) */
 } or_ch_params;
 
 typedef struct {
@@ -1372,6 +1387,7 @@ typedef struct {
   double *U[3], *US[3], *D[3];    /* face arrays */
   double *p, *pp, *T, *kcell, *bc;
   double *ac[3];                  /* p' couplings per face */
+  double *qw[3][2];               /* QUICK weights per axis: [0] cell nodes, [1] face nodes (ch_quick_w) */
   double res[5], norm[5], glob;   /* u v w continuity energy */
   int iter, pcg_iters, t_iters;
   double pcg_relres;
@@ -1405,8 +1421,64 @@ static double ch_get(const or_ch *C, const double *arr, int a, const I64 *c) { r
 
 /* coefficients of the unknown face (a, c) at the frozen u^n: a[6] in order E W N S T B, a_P, the
  * pressure source, and the six neighbour face positions (valid[n] = 0: value 0) */
+/* the coefficient of a neighbour across a control-volume face with conductance D
+ * and flux F (+ direction) on its high (hi) or low side */
+static double ch_anb(const or_ch *C, double D, double F, int hi) {
+  if (C->P.conv == 1) return hi ? maxd(maxd(-F, D - 0.5 * F), 0.0) : maxd(maxd(F, D + 0.5 * F), 0.0);
+  return hi ? D + maxd(-F, 0.0) : D + maxd(F, 0.0);
+}
+
+/* Weights of the QUICK face value along axis b for one control-volume face e
+ * of a momentum component: kind 1 when the nodes are the faces of axis b
+ * (the component of axis b: nodes at the grid points, control-volume faces at
+ * the cell centres, e = 0 .. N_b - 1 between nodes e and e + 1), kind 0 when
+ * they are cell centres (the other components: control-volume faces at the
+ * grid points, e = 0 .. N_b between cells e - 1 and e).  w[0..2] for a flux in
+ * the + direction, w[3..5] against it, each (far upwind, upwind, downwind):
+ * the quadratic through the three nodes evaluated at the face; (0, 1, 0),
+ * the upwind value, where a node lies outside the grid. */
+static void ch_quick_w(const double *pts, I64 n, int kind, I64 e, double *w) {
+  double xf, xn[4];
+  I64 lo, nn = kind ? n + 1 : n;  /* nodes 0 .. nn - 1 */
+  if (kind) { xf = 0.5 * (pts[e] + pts[e + 1]); lo = e; }
+  else { xf = pts[e]; lo = e - 1; }
+  /* candidate nodes lo - 1, lo, lo + 1, lo + 2 */
+  for (int t = 0; t < 4; ++t) {
+    I64 m = lo - 1 + t;
+    xn[t] = (m >= 0 && m < nn) ? (kind ? pts[m] : 0.5 * (pts[m] + pts[m + 1])) : 0.0;
+  }
+  for (int dir = 0; dir < 2; ++dir) {
+    /* + flux: UU = lo - 1, U = lo, D = lo + 1; - flux: UU = lo + 2, U = lo + 1, D = lo */
+    I64 iuu = dir == 0 ? lo - 1 : lo + 2, iu = dir == 0 ? lo : lo + 1, id = dir == 0 ? lo + 1 : lo;
+    double *o = w + 3 * dir;
+    if (iuu < 0 || iuu >= nn || iu < 0 || iu >= nn || id < 0 || id >= nn) { o[0] = 0.0; o[1] = 1.0; o[2] = 0.0; continue; }
+    double xuu = xn[iuu - lo + 1], xu = xn[iu - lo + 1], xd = xn[id - lo + 1];
+    o[0] = ((xf - xu) * (xf - xd)) / ((xuu - xu) * (xuu - xd));
+    o[1] = ((xf - xuu) * (xf - xd)) / ((xu - xuu) * (xu - xd));
+    o[2] = ((xf - xuu) * (xf - xu)) / ((xd - xuu) * (xd - xu));
+  }
+}
+
+/* QUICK correction F (u_f^QUICK - u_f^upwind) of the control-volume face e
+ * along axis b of component a, from u^n; c is any face of the component
+ * (its index along b is replaced by the node indices) */
+static double ch_quick_term(const or_ch *C, int a, int b, const I64 *c, I64 e, double F) {
+  const int kind = b == a;
+  const double *w = C->qw[b][kind] + 6 * e + (F > 0.0 ? 0 : 3);
+  I64 lo = kind ? e : e - 1;
+  I64 iuu = F > 0.0 ? lo - 1 : lo + 2, iu = F > 0.0 ? lo : lo + 1, id = F > 0.0 ? lo + 1 : lo;
+  if (w[0] == 0.0 && w[2] == 0.0) iuu = id = iu;  /* upwind: the weights need no other node */
+  I64 q[3] = {c[0], c[1], c[2]};
+  q[b] = iuu; double uuu = ch_get(C, C->U[a], a, q);
+  q[b] = iu; double uu = ch_get(C, C->U[a], a, q);
+  q[b] = id; double ud = ch_get(C, C->U[a], a, q);
+  double uq = (w[0] * uuu + w[1] * uu) + w[2] * ud;
+  return F * (uq - uu);
+}
+
 static void ch_coef(const or_ch *C, int a, const I64 *c, double *an, double *aP, double *bsrc, I64 (*nb)[3], int *valid) {
   const double A = ch_area(C, a, c), da = C->h[a][c[a]], nu = C->nu;
+  double dc = 0.0;  /* QUICK deferred correction, in stencil order */
   for (int b = 0; b < 3; ++b) {
     for (int hi = 1; hi >= 0; --hi) {
       int n = 2 * b + (1 - hi);
@@ -1419,15 +1491,17 @@ static void ch_coef(const or_ch *C, int a, const I64 *c, double *an, double *aP,
           if (!(a == 0 && q[0] == C->N[0])) {
             double F = 0.5 * (ch_get(C, C->U[a], a, c) + ch_get(C, C->U[a], a, q)) * A;
             double Dd = nu * A / C->d[a][c[a]];
-            coef = Dd + maxd(-F, 0.0);
+            coef = ch_anb(C, Dd, F, 1);
             valid[n] = 1;
+            if (C->P.conv == 2) dc -= ch_quick_term(C, a, b, c, c[a], F);
           }
         } else {
           q[a] -= 1;
           double F = 0.5 * (ch_get(C, C->U[a], a, q) + ch_get(C, C->U[a], a, c)) * A;
           double Dd = nu * A / C->d[a][c[a] - 1];
-          coef = Dd + maxd(F, 0.0);
+          coef = ch_anb(C, Dd, F, 0);
           valid[n] = 1;
+          if (C->P.conv == 2) dc += ch_quick_term(C, a, b, c, c[a] - 1, F);
         }
       } else {
         int o = 3 - a - b;
@@ -1439,14 +1513,18 @@ static void ch_coef(const or_ch *C, int a, const I64 *c, double *an, double *aP,
                    C->d[o][c[o]];
         if (hi) {
           if (c[b] + 1 == C->N[b]) {
-            if (b != 0) coef = nu * ar / C->h[b][C->N[b]] + maxd(-F, 0.0);
+            if (b != 0) coef = ch_anb(C, nu * ar / C->h[b][C->N[b]], F, 1);
           } else {
-            coef = nu * ar / C->h[b][c[b] + 1] + maxd(-F, 0.0);
+            coef = ch_anb(C, nu * ar / C->h[b][c[b] + 1], F, 1);
             q[b] += 1; valid[n] = 1;
+            if (C->P.conv == 2) dc -= ch_quick_term(C, a, b, c, c[b] + 1, F);
           }
         } else {
-          if (c[b] == 0) coef = nu * ar / C->h[b][0] + maxd(F, 0.0);
-          else { coef = nu * ar / C->h[b][c[b]] + maxd(F, 0.0); q[b] -= 1; valid[n] = 1; }
+          if (c[b] == 0) coef = ch_anb(C, nu * ar / C->h[b][0], F, 0);
+          else {
+            coef = ch_anb(C, nu * ar / C->h[b][c[b]], F, 0); q[b] -= 1; valid[n] = 1;
+            if (C->P.conv == 2) dc += ch_quick_term(C, a, b, c, c[b], F);
+          }
         }
       }
       an[n] = coef;
@@ -1456,7 +1534,11 @@ static void ch_coef(const or_ch *C, int a, const I64 *c, double *an, double *aP,
   *aP = an[0] + an[1] + an[2] + an[3] + an[4] + an[5];
   I64 lo[3] = {c[0], c[1], c[2]};
   lo[a] -= 1;
-  *bsrc = (C->p[ch_c(C, lo[0], lo[1], lo[2])] - C->p[ch_c(C, c[0], c[1], c[2])]) * A;
+  double bs = (C->p[ch_c(C, lo[0], lo[1], lo[2])] - C->p[ch_c(C, c[0], c[1], c[2])]) * A;
+  if (C->P.conv == 2) bs = bs + dc;
+  if (C->P.ri != 0.0 && a == C->P.g_axis)
+    bs = bs + C->P.ri * (0.5 * (C->T[ch_c(C, lo[0], lo[1], lo[2])] + C->T[ch_c(C, c[0], c[1], c[2])]) - C->P.t_in) * A * da;
+  *bsrc = bs;
 }
 
 static double ch_nbsum(const or_ch *C, const double *arr, int a, const double *an, I64 (*nb)[3], const int *valid) {
@@ -1626,6 +1708,7 @@ void or_ch_params_default(or_ch_params *P) {
   P->re = 100; P->pr = 0.71; P->u_in = 1.0; P->t_in = 0.0;
   P->alpha_u = 0.7; P->alpha_p = 0.3; P->alpha_t = 0.9;
   P->mom_sweeps = 2; P->p_tol = 1e-8; P->p_maxiter = 1000; P->t_tol = 1e-2; P->t_maxiter = 200;
+  P->conv = 0; P->g_axis = 2; P->ri = 0.0;
 }
 
 or_ch *or_ch_create(const char *deck, const or_ch_params *P) {
@@ -1659,6 +1742,16 @@ or_ch *or_ch_create(const char *deck, const or_ch_params *P) {
     C->U[a] = calloc(nf, 8); C->US[a] = calloc(nf, 8); C->D[a] = calloc(nf, 8); C->ac[a] = calloc(nf, 8);
   }
   C->p = calloc(N, 8); C->pp = calloc(N, 8); C->T = calloc(N, 8); C->kcell = calloc(N, 8); C->bc = calloc(N, 8);
+  for (int b = 0; b < 3; ++b)
+    for (int kind = 0; kind < 2; ++kind) {
+      I64 ne = C->N[b] + 1;
+      C->qw[b][kind] = malloc(8 * 6 * ne);
+      for (I64 e = 0; e < ne; ++e) {
+        double *w = C->qw[b][kind] + 6 * e;
+        if (kind && e == C->N[b]) { w[0] = w[3] = 0.0; w[1] = w[4] = 1.0; w[2] = w[5] = 0.0; continue; }  /* no such face */
+        ch_quick_w(C->pts[b], C->N[b], kind, e, w);
+      }
+    }
   double ly = C->pts[1][C->N[1]] - C->pts[1][0];
   C->nu = P->u_in * ly / P->re;
   C->kf = C->nu / P->pr;
@@ -1761,7 +1854,17 @@ void or_ch_destroy(or_ch *C) {
   for (int a = 0; a < 3; ++a) { free(C->pts[a]); free(C->d[a]); free(C->h[a]); free(C->U[a]); free(C->US[a]); free(C->D[a]); free(C->ac[a]); }
   free(C->solid); free(C->region); free(C->kreg); free(C->qcell);
   free(C->p); free(C->pp); free(C->T); free(C->kcell); free(C->bc);
+  for (int b = 0; b < 3; ++b) { free(C->qw[b][0]); free(C->qw[b][1]); }
   free(C);
+}
+
+/* the QUICK weights of one control-volume face (ch_quick_w) and the
+ * neighbour coefficient of a convection scheme (ch_anb), for tests */
+void or_ch_quick_weights(const double *pts, I64 n, int kind, I64 e, double *w6) { ch_quick_w(pts, n, kind, e, w6); }
+double or_ch_anb(int conv, double D, double F, int hi) {
+  or_ch C;
+  C.P.conv = conv;
+  return ch_anb(&C, D, F, hi);
 }
 
 void or_ch_dims(const or_ch *C, I64 *out3) { out3[0] = C->N[0]; out3[1] = C->N[1]; out3[2] = C->N[2]; }

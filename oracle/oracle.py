@@ -251,7 +251,8 @@ class ChParams(ctypes.Structure):
     _fields_ = [("re", ctypes.c_double), ("pr", ctypes.c_double), ("u_in", ctypes.c_double), ("t_in", ctypes.c_double),
                 ("alpha_u", ctypes.c_double), ("alpha_p", ctypes.c_double), ("alpha_t", ctypes.c_double),
                 ("mom_sweeps", ctypes.c_int), ("p_tol", ctypes.c_double), ("p_maxiter", ctypes.c_int),
-                ("t_tol", ctypes.c_double), ("t_maxiter", ctypes.c_int)]
+                ("t_tol", ctypes.c_double), ("t_maxiter", ctypes.c_int),
+                ("conv", ctypes.c_int), ("g_axis", ctypes.c_int), ("ri", ctypes.c_double)]
 
     @classmethod
     def default(cls, **kw):
@@ -369,3 +370,26 @@ def channel_energy_residual(case, T):
     bn = ctypes.c_double()
     r = case.L.or_ch_energy_residual(case.h, a.ctypes.data, ctypes.byref(bn))
     return r, bn.value
+
+
+def quick_weights(pts, kind, e):
+    """The QUICK weights (far upwind, upwind, downwind) of control-volume face
+    e along an axis with grid points `pts` (hs_oracle.c: ch_quick_w): six
+    values, for a flux in the + direction then against it; node kind 1 = the
+    faces of that axis, 0 = cell centres."""
+    L = lib()
+    L.or_ch_quick_weights.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_int, ctypes.c_int64, ctypes.c_void_p]
+    p = np.ascontiguousarray(pts, np.float64)
+    w = np.zeros(6)
+    L.or_ch_quick_weights(p.ctypes.data, p.size - 1, int(kind), int(e), w.ctypes.data)
+    return w
+
+
+def neighbour_coefficient(conv, D, F, hi):
+    """a_nb of the momentum convection scheme `conv` for a control-volume face
+    of conductance D and flux F (+ direction), neighbour on the high side when
+    hi (hs_oracle.c: ch_anb)."""
+    L = lib()
+    L.or_ch_anb.restype = ctypes.c_double
+    L.or_ch_anb.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_int]
+    return L.or_ch_anb(int(conv), float(D), float(F), int(hi))

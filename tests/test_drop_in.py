@@ -146,6 +146,9 @@ def test_channel_sidecar_errors_are_reported(tmp_path):
     (tmp_path / "chan.in.channel").write_text("re = 100\n")
     r = subprocess.run([exe, path, "2", str(tmp_path / "r.vtk")], capture_output=True, text=True, timeout=120)
     assert r.returncode == 1 and "physics = channel" in r.stderr, r.stderr
+    (tmp_path / "chan.in.channel").write_text("physics = channel\nconvection = central\n")
+    r = subprocess.run([exe, path, "2", str(tmp_path / "r.vtk")], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 1 and "convection must be" in r.stderr, r.stderr
 
 
 @pytest.mark.gpu
@@ -154,14 +157,15 @@ def test_driver_runs_the_channel_physics_from_a_sidecar(tmp_path):
     exe = _build(tmp_path)
     sidecar = ("# the channel case of this deck\nphysics = channel\nre = 100\nprecision = fp64\n"
                "k_ratio = 50, 200\nq = 1.0, 2.5\np_tol = 1e-12\np_maxiter = 20000\n"
-               "t_tol = 1e-12\nt_maxiter = 20000\n")
+               "t_tol = 1e-12\nt_maxiter = 20000\nconvection = quick\nrichardson = 1.5\ngravity_axis = z\n")
     path, deck = _channel_deck(tmp_path, sidecar)
     vtk = str(tmp_path / "result.vtk")
     r = subprocess.run([exe, path, "3", vtk], capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stdout + r.stderr
     got = _read_vtk(vtk)
 
-    o = oracle.ChannelCase(deck, re=100.0, p_tol=1e-12, p_maxiter=20000, t_tol=1e-12, t_maxiter=20000)
+    o = oracle.ChannelCase(deck, re=100.0, p_tol=1e-12, p_maxiter=20000, t_tol=1e-12, t_maxiter=20000, conv=2, ri=1.5,
+                           g_axis=2)
     ctype, region = oracle.OracleCase(deck).cell_types()
     o.set_solid(np.array([50.0, 200.0]), np.where(ctype == 1, np.array([1.0, 2.5])[np.maximum(region, 0)], 0.0))
     o.init()
