@@ -359,6 +359,7 @@ def run_gpu(args):
         variants["reference_physics"] = reference_physics(args, torch, hsolver_b200, local, dist)
         variants["like_for_like"] = like_for_like(torch, hsolver_b200, local)
         variants["config5"] = config5(torch, hsolver_b200, local)
+        variants["convection"] = convection(torch, hsolver_b200, local)
 
     if rank == 0:
         peak, peak_kind = hbm_peak()
@@ -433,6 +434,28 @@ def time_to_residual(args, hsolver_b200, local):
             f: float(np.linalg.norm(fields["mixed"][f] - fields["fp64"][f]) / max(np.linalg.norm(fields["fp64"][f]), 1e-300))
             for f in ("u", "v", "w", "p", "T")}
         out[name] = res
+    return out
+
+
+def convection(torch, hsolver_b200, local):
+    """The momentum convection schemes and buoyancy on the bench case: the
+    outer step with hybrid, and with QUICK (deferred correction) plus a
+    Boussinesq term along +z at Richardson number 1, beside first-order
+    upwind (the reference's scheme, the bench's headline); 3 warm-up and 10
+    timed steps each, per-phase times of 3 more."""
+    deck, re_, k, q, _ = workload()
+    out = {}
+    for name, kw in (("upwind", {}), ("hybrid", {"conv": 1}), ("quick_buoyancy", {"conv": 2, "ri": 1.0}),
+                     ("quick_buoyancy_mixed", {"conv": 2, "ri": 1.0, "precision": 1})):
+        g = hsolver_b200.Channel(deck, device=local, re=re_, **SOLVER, **kw)
+        g.set_solid(k, q)
+        g.init()
+        g.step(3)
+        ms, st = time_steps(torch, g, 10, local)
+        phases, iters = profiled_steps(g, 3)
+        out[name] = {"value": 10 / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms / 10,
+                     "momentum_ms_per_step": phases["momentum"], "pcg_iters": iters}
+        g.close()
     return out
 
 
