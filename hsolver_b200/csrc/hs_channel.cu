@@ -119,14 +119,16 @@ template <int A, class R> __device__ __forceinline__ double rctr(const ChDev<R> 
 // q = RN(a y) is within one ulp of a/b, the remainder a - q b is exact in one
 // FMA, and RN(q + r y) is the correctly rounded quotient -- the IEEE value,
 // for finite normal operands and a nonzero a (as tests/test_gpu_division.py
-// checks for the same construction on the reference path).  FP32 keeps the
-// IEEE division.
+// checks for the same construction on the reference path).  FP32 (the mixed
+// form's correction sweeps, whose operator only approximates the FP64 one:
+// the fixed point is set by the FP64 residual) takes the fast approximate
+// quotient (2 ulp), 0.68 -> 0.58 ms per mixed momentum solve at 256x128x128.
 __device__ __forceinline__ double div_known(double a, double b, double y) {
   const double q = a * y;
   const double r = __fma_rn(-q, b, a);
   return __fma_rn(r, y, q);
 }
-__device__ __forceinline__ float div_known(float a, float b, double) { return a / b; }
+__device__ __forceinline__ float div_known(float a, float b, double) { return __fdividef(a, b); }
 
 template <int A, class R>
 __device__ __forceinline__ int fidx(const ChDev<R> &H, int i, int j, int k) {
@@ -203,9 +205,9 @@ __device__ __forceinline__ double quick_term(const ChDev<R> &H, const int (&c)[3
 // one stencil term (neighbour across axis B, high side when HI) of the unknown
 // face (A, c): coefficient at the frozen iterate and the neighbour's face
 // index (-1: the neighbour value is 0 or the term is dropped)
-template <int A, int B, int HI, bool X, class R>
+template <int A, int B, int HI, int X, class R>
 __device__ __forceinline__ void term(const ChDev<R> &H, const int (&c)[3], R Ar, R da, R &coef, int &nb, R &Fo, int &eo) {
-  const int conv = X ? H.conv : 0;
+  const int conv = X == 0 ? 0 : X == 1 ? 1 : H.conv;
   coef = R(0);
   nb = -1;
   Fo = R(0);
@@ -300,7 +302,7 @@ __device__ __forceinline__ double add_sources(const ChDev<double> &H, const int 
 // follow use FP32 coefficients from the FP32 copy, which only approximates
 // the correction operator: the fixed point solves the FP64 equations (defect
 // correction).
-template <int A, bool X>
+template <int A, int X>
 __device__ __forceinline__ void mom_face_mixed_first(const ChDev<float> &H, const int (&c)[3], int f, bool upd,
                                                      bool last, double &racc, bool keep) {
   ChDev<double> H64;
@@ -329,7 +331,7 @@ __device__ __forceinline__ void mom_face_mixed_first(const ChDev<float> &H, cons
   int lo[3] = {c[0], c[1], c[2]};
   lo[A] -= 1;
   double bs = (H.p[cidx(H, lo[0], lo[1], lo[2])] - H.p[cidx(H, c[0], c[1], c[2])]) * Ad;
-  if constexpr (X) bs = add_sources<A>(H64, c, nd, Fd, ed, Ad, dad, bs);
+  if constexpr (X == 2) bs = add_sources<A>(H64, c, nd, Fd, ed, Ad, dad, bs);
   double s = 0.0;
 #pragma unroll
   for (int n = 0; n < 6; ++n) s += ad[n] * (nd[n] >= 0 ? UA[nd[n]] : 0.0);
@@ -347,7 +349,7 @@ __device__ __forceinline__ void mom_face_mixed_first(const ChDev<float> &H, cons
 
 // momentum work on the unknown face (A, c): residual at u^n (first pass),
 // relaxed Gauss-Seidel update (upd), d (last sweep)
-template <int A, bool X, class R>
+template <int A, int X, class R>
 __device__ __forceinline__ void mom_face(const ChDev<R> &H, const int (&c)[3], bool first, bool upd, bool last,
                                          double &racc, bool keep) {
   const int f = fidx3<A>(H, c);
@@ -376,7 +378,7 @@ __device__ __forceinline__ void mom_face(const ChDev<R> &H, const int (&c)[3], b
     int lo[3] = {c[0], c[1], c[2]};
     lo[A] -= 1;
     R bs = (H.p[cidx(H, lo[0], lo[1], lo[2])] - H.p[cidx(H, c[0], c[1], c[2])]) * Ar;
-    if constexpr (X) bs = add_sources<A>(H, c, nb, Fn, en, Ar, da, bs);
+    if constexpr (X == 2) bs = add_sources<A>(H, c, nb, Fn, en, Ar, da, bs);
     const R un = UA[f];
     const R *src = first ? (const R *)UA : (const R *)SA;
     if (first) {
@@ -403,7 +405,7 @@ __device__ __forceinline__ void mom_face(const ChDev<R> &H, const int (&c)[3], b
       R s = R(0);
 #pragma unroll
       for (int n = 0; n < 6; ++n) s += an[n] * (nb[n] >= 0 ? SA[nb[n]] : R(0));
-      SA[f] = (rhs + s) / apr;
+      SA[f] = __fdividef(rhs + s, apr);
       if (last) Darr<A>(H)[f] = Ar / apr;
     }
   }
@@ -426,10 +428,11 @@ __device__ double block_sum(double v, double *sh) {
 // One red-black pass of all three momentum components (blockIdx.y = axis).
 // first: the pass of colour 0 in sweep 0, which also evaluates the residual of
 // every unknown face at u^n and writes the fixed faces of u* (delta = 0).
-template <int A, bool X, class R>
+template <int A, int X, class R>
 __device__ void mom_pass_axis(const ChDev<R> &H, int color, bool first, bool last, double &racc) {
   const int nf0 = H.N0 + (A == 0), nf1 = H.N1 + (A == 1), nf2 = H.N2 + (A == 2);
-  const int T = gridDim.x * blockDim.x, tid = blockIdx.x * blockDim.x + threadIdx.x;
+  // blocks 3b, 3b + 1, 3b + 2 take chunk b of the three components (k_ch_mom)
+  const int T = (gridDim.x / 3) * blockDim.x, tid = (blockIdx.x / 3) * blockDim.x + threadIdx.x;
   if (first) {
     for (mg::Walk w(nf0, nf1, nf2, tid, T); w.ok(); w.next()) {
       const int c[3] = {w.m, w.j, w.k};
@@ -462,18 +465,25 @@ __device__ void mom_pass_axis(const ChDev<R> &H, int color, bool first, bool las
 }
 
 // four 256-thread blocks per SM (64 registers: above that the SM holds three).
-// X: the extended momentum physics (hybrid or QUICK convection, buoyancy),
-// a separate instantiation so that the upwind form keeps its registers.
-template <class R, bool X>
+// X: 0 first-order upwind, 1 hybrid, 2 any scheme with the source terms
+// (QUICK deferred correction, buoyancy): separate instantiations, so that the
+// upwind and hybrid forms keep their registers.
+// The grid is 3 x (chunks): the three components of one chunk of faces are
+// consecutive blocks, so they run at the same time and share the u^n they
+// all read in L2 (component-major order read the three velocity arrays once
+// per component from DRAM: 0.80 -> 0.71 ms per FP64 momentum solve at
+// 256x128x128).
+template <class R, int X>
 __global__ void __launch_bounds__(kT, 4) k_ch_mom(ChDev<R> H, int color, int first, int last, double *partials) {
   __shared__ double sh[32];
   double racc = 0.0;
-  if (blockIdx.y == 0) mom_pass_axis<0, X>(H, color, first, last, racc);
-  else if (blockIdx.y == 1) mom_pass_axis<1, X>(H, color, first, last, racc);
+  const int comp = blockIdx.x % 3;
+  if (comp == 0) mom_pass_axis<0, X>(H, color, first, last, racc);
+  else if (comp == 1) mom_pass_axis<1, X>(H, color, first, last, racc);
   else mom_pass_axis<2, X>(H, color, first, last, racc);
   if (first) {
     const double b = block_sum(racc, sh);
-    if (threadIdx.x == 0) partials[blockIdx.y * gridDim.x + blockIdx.x] = b;
+    if (threadIdx.x == 0) partials[comp * (gridDim.x / 3) + blockIdx.x / 3] = b;
   }
 }
 
@@ -1311,12 +1321,15 @@ void mom_solve(ChannelState &S, ChDev<R> &H) {
   const int sw = std::max(1, S.prm.mom_sweeps);
   for (int s = 0; s < sw; ++s)
     for (int color = 0; color < 2; ++color)
-      if (H.conv != 0 || H.ri != 0.0)
-        k_ch_mom<R, true><<<dim3(S.mom_blocks, 3), kT, 0, S.stream>>>(H, color, s == 0 && color == 0, s == sw - 1,
-                                                                     S.mom_part);
+      if (H.conv == 2 || H.ri != 0.0)
+        k_ch_mom<R, 2><<<dim3(3 * S.mom_blocks), kT, 0, S.stream>>>(H, color, s == 0 && color == 0, s == sw - 1,
+                                                                  S.mom_part);
+      else if (H.conv == 1)
+        k_ch_mom<R, 1><<<dim3(3 * S.mom_blocks), kT, 0, S.stream>>>(H, color, s == 0 && color == 0, s == sw - 1,
+                                                                  S.mom_part);
       else
-        k_ch_mom<R, false><<<dim3(S.mom_blocks, 3), kT, 0, S.stream>>>(H, color, s == 0 && color == 0, s == sw - 1,
-                                                                      S.mom_part);
+        k_ch_mom<R, 0><<<dim3(3 * S.mom_blocks), kT, 0, S.stream>>>(H, color, s == 0 && color == 0, s == sw - 1,
+                                                                  S.mom_part);
   CH_CUDA(cudaGetLastError());
 }
 
