@@ -10,7 +10,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libhsolver_b200.so")
-SOURCES = ["hs_case.cpp", "hs_api.cpp", "hs_engine.cu", "hs_cht.cu", "hs_channel.cu"]
+SOURCES = ["hs_case.cpp", "hs_api.cpp", "hs_engine.cu", "hs_cht.cu", "hs_channel.cu", "hs_slab.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-fmad=false", "-prec-div=true", "-prec-sqrt=true",
               "-Xcompiler", "-fPIC,-ffp-contract=off", "-Xptxas", "-v"]

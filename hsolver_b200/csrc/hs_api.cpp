@@ -11,6 +11,7 @@
 #include "hs_channel.hpp"
 #include "hs_cht.hpp"
 #include "hs_engine.hpp"
+#include "hs_slab.hpp"
 
 struct hs_ctx {
   hs::Engine *engine = nullptr;
@@ -691,3 +692,84 @@ void hs_destroy(hs_ctx *ctx) {
 const char *hs_last_error(const hs_ctx *ctx) { return ctx ? ctx->err.c_str() : g_err.c_str(); }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------- z-slab p' solve
+struct hs_slab {
+  hs::SlabState *st = nullptr;
+};
+
+namespace {
+template <class Fn>
+int slab_guarded(hs_slab *h, Fn fn) {
+  if (!h || !h->st) return fail(nullptr, HS_ERR_ARG, "null slab handle");
+  try {
+    return fn(h->st);
+  } catch (const std::exception &e) {
+    return fail(nullptr, classify(e), e.what());
+  }
+}
+}  // namespace
+
+int hs_slab_create(int nx, int ny, int nz, int device, hs_slab **out) {
+  if (!out) return fail(nullptr, HS_ERR_ARG, "null output pointer");
+  *out = nullptr;
+  hs_slab *h = new (std::nothrow) hs_slab();
+  if (!h) return fail(nullptr, HS_ERR_NOMEM, "host allocation failed");
+  try {
+    h->st = hs::slab_create(nx, ny, nz, device);
+  } catch (const std::exception &e) {
+    delete h;
+    return fail(nullptr, classify(e), e.what());
+  }
+  *out = h;
+  return HS_OK;
+}
+
+int hs_slab_set_system(hs_slab *h, const double *gx, const double *gy, const double *gz, const double *b) {
+  if (!gx || !gy || !gz || !b) return fail(nullptr, HS_ERR_ARG, "null array");
+  return slab_guarded(h, [&](hs::SlabState *s) { hs::slab_set_system(s, gx, gy, gz, b); return HS_OK; });
+}
+
+int hs_slab_begin(hs_slab *h, double *bb) {
+  return slab_guarded(h, [&](hs::SlabState *s) { const double v = hs::slab_begin(s); if (bb) *bb = v; return HS_OK; });
+}
+
+int hs_slab_precond(hs_slab *h, double *rz) {
+  return slab_guarded(h, [&](hs::SlabState *s) { const double v = hs::slab_precond(s); if (rz) *rz = v; return HS_OK; });
+}
+
+int hs_slab_direction(hs_slab *h, double beta, int first) {
+  return slab_guarded(h, [&](hs::SlabState *s) { hs::slab_direction(s, beta, first); return HS_OK; });
+}
+
+int hs_slab_apply(hs_slab *h, double *sp) {
+  return slab_guarded(h, [&](hs::SlabState *s) { const double v = hs::slab_apply(s); if (sp) *sp = v; return HS_OK; });
+}
+
+int hs_slab_update(hs_slab *h, double alpha, double *rr) {
+  return slab_guarded(h, [&](hs::SlabState *s) { const double v = hs::slab_update(s, alpha); if (rr) *rr = v; return HS_OK; });
+}
+
+int hs_slab_plane_size(hs_slab *h, long long *n) {
+  if (!n) return fail(nullptr, HS_ERR_ARG, "null output pointer");
+  return slab_guarded(h, [&](hs::SlabState *s) { *n = hs::slab_plane_size(s); return HS_OK; });
+}
+
+int hs_slab_halo_get(hs_slab *h, double *lo, double *hi) {
+  return slab_guarded(h, [&](hs::SlabState *s) { hs::slab_halo_get(s, lo, hi); return HS_OK; });
+}
+
+int hs_slab_halo_put(hs_slab *h, const double *lo, const double *hi) {
+  return slab_guarded(h, [&](hs::SlabState *s) { hs::slab_halo_put(s, lo, hi); return HS_OK; });
+}
+
+int hs_slab_get(hs_slab *h, int which, double *host) {
+  if (!host || which < 0 || which > 3) return fail(nullptr, HS_ERR_ARG, "bad field or null output");
+  return slab_guarded(h, [&](hs::SlabState *s) { hs::slab_get(s, which, host); return HS_OK; });
+}
+
+void hs_slab_destroy(hs_slab *h) {
+  if (!h) return;
+  hs::slab_destroy(h->st);
+  delete h;
+}

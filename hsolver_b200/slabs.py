@@ -66,3 +66,186 @@ def allreduce_sum(value, dist, device, group=None):
     x = torch.tensor([float(value)], dtype=torch.float64, device=device)
     dist.all_reduce(x, op=dist.ReduceOp.SUM, group=group)
     return float(x.item())
+
+
+# ---------------------------------------------------------------- the sharded p' solve on GPUs
+class SlabPCG:
+    """One slab of the pressure-correction system on a GPU (hs_slab_* of the
+    C ABI): face couplings gx (nz, ny, nx + 1), gy (nz, ny + 1, nx), gz
+    (nz + 1, ny, nx) with gz[0] and gz[nz] the slab's bottom and top faces,
+    and the right-hand side b (nz, ny, nx), numpy arrays."""
+
+    def __init__(self, nx, ny, nz, device=0):
+        import ctypes
+        from . import load, HsError
+        L = load()
+        vp, dp = ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)
+        sig = {"hs_slab_create": [ctypes.c_int] * 4 + [ctypes.POINTER(vp)],
+               "hs_slab_set_system": [vp, vp, vp, vp, vp], "hs_slab_begin": [vp, dp], "hs_slab_precond": [vp, dp],
+               "hs_slab_direction": [vp, ctypes.c_double, ctypes.c_int], "hs_slab_apply": [vp, dp],
+               "hs_slab_update": [vp, ctypes.c_double, dp], "hs_slab_plane_size": [vp, ctypes.POINTER(ctypes.c_longlong)],
+               "hs_slab_halo_get": [vp, vp, vp], "hs_slab_halo_put": [vp, vp, vp], "hs_slab_get": [vp, ctypes.c_int, vp]}
+        for name, args in sig.items():
+            getattr(L, name).argtypes = args
+            getattr(L, name).restype = ctypes.c_int
+        L.hs_slab_destroy.argtypes = [vp]
+        L.hs_slab_destroy.restype = None
+        import torch
+        self._L, self._ct, self._err = L, ctypes, HsError
+        self.dims = (nx, ny, nz)
+        self.device = device
+        self.torch_device = torch.device("cuda", device)
+        self.h = None
+        h = vp()
+        self._check(L.hs_slab_create(nx, ny, nz, device, ctypes.byref(h)))
+        self.h = h
+        n = ctypes.c_longlong()
+        self._check(L.hs_slab_plane_size(h, ctypes.byref(n)))
+        self.plane = n.value
+
+    def _check(self, rc):
+        if rc < 0:
+            raise self._err(rc, self._L.hs_last_error(None).decode())
+
+    def _scalar(self, fn, *args):
+        v = self._ct.c_double()
+        self._check(fn(self.h, *args, self._ct.byref(v)))
+        return v.value
+
+    def set_system(self, gx, gy, gz, b):
+        import numpy as np
+        nx, ny, nz = self.dims
+        arrs = [np.ascontiguousarray(a, np.float64) for a in (gx, gy, gz, b)]
+        for a, shape in zip(arrs, [(nz, ny, nx + 1), (nz, ny + 1, nx), (nz + 1, ny, nx), (nz, ny, nx)]):
+            if a.shape != shape:
+                raise ValueError("expected shape %s, got %s" % (shape, a.shape))
+        self._check(self._L.hs_slab_set_system(self.h, *[a.ctypes.data for a in arrs]))
+
+    def begin(self):
+        return self._scalar(self._L.hs_slab_begin)
+
+    def precond(self):
+        return self._scalar(self._L.hs_slab_precond)
+
+    def direction(self, beta, first):
+        self._check(self._L.hs_slab_direction(self.h, float(beta), int(first)))
+
+    def apply(self):
+        return self._scalar(self._L.hs_slab_apply)
+
+    def update(self, alpha):
+        return self._scalar(self._L.hs_slab_update, float(alpha))
+
+    def halo_get(self, lo, hi):
+        """p's first and last interior planes into torch CUDA tensors (or None)."""
+        self._check(self._L.hs_slab_halo_get(self.h, lo.data_ptr() if lo is not None else None,
+                                             hi.data_ptr() if hi is not None else None))
+
+    def halo_put(self, lo, hi):
+        """torch CUDA tensors (or None) into p's ghost planes below and above."""
+        self._check(self._L.hs_slab_halo_put(self.h, lo.data_ptr() if lo is not None else None,
+                                             hi.data_ptr() if hi is not None else None))
+
+    def field(self, which="x"):
+        import numpy as np
+        nx, ny, nz = self.dims
+        out = np.empty((nz, ny, nx))
+        self._check(self._L.hs_slab_get(self.h, {"x": 0, "r": 1, "p": 2, "s": 3}[which], out.ctypes.data))
+        return out
+
+    def close(self):
+        if self.h:
+            self._L.hs_slab_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _exchange_local(slabs, bufs):
+    """Each slab's p boundary planes into its neighbours' ghost planes, for
+    consecutive slabs of one process (device-to-device copies)."""
+    for a, b in zip(slabs[:-1], slabs[1:]):
+        up, down = bufs
+        a.halo_get(None, up)    # a's top plane -> b's lower ghost
+        b.halo_get(down, None)  # b's bottom plane -> a's upper ghost
+        b.halo_put(up, None)
+        a.halo_put(None, down)
+
+
+def _exchange_dist(slab, bufs, dist, group):
+    """This rank's slab's p boundary planes to the neighbouring ranks and
+    theirs into its ghost planes (the same steps as exchange_halo, over the
+    process group: NCCL send/recv into the receiver's own memory)."""
+    import torch
+    rank, world = dist.get_rank(group), dist.get_world_size(group)
+    lo_send, hi_send, lo_recv, hi_recv = bufs
+    down, up = rank > 0, rank + 1 < world
+    slab.halo_get(lo_send if down else None, hi_send if up else None)
+    reqs = []
+    if down:
+        reqs.append(dist.isend(lo_send, rank - 1, group=group, tag=1))
+    if up:
+        reqs.append(dist.isend(hi_send, rank + 1, group=group, tag=2))
+    if down:
+        reqs.append(dist.irecv(lo_recv, rank - 1, group=group, tag=2))
+    if up:
+        reqs.append(dist.irecv(hi_recv, rank + 1, group=group, tag=1))
+    for r in reqs:
+        r.wait()
+    if lo_recv.is_cuda:  # NCCL's receives run on the current stream; the slab copies on its own
+        torch.cuda.current_stream(lo_recv.device).synchronize()
+    slab.halo_put(lo_recv if down else None, hi_recv if up else None)
+
+
+def slab_pcg_solve(slabs, tol=1e-8, maxiter=1000, dist=None, group=None):
+    """CG on the pressure-correction system sharded into z-slabs, each
+    preconditioned by its own V-cycle (block Jacobi).  `slabs`: SlabPCG (or
+    any object with its methods, `plane` and `torch_device`): this
+    process's slabs, bottom to top: every slab of the domain when dist is
+    None (one process, one or more slabs on its GPU), or this rank's one slab
+    with dist = torch.distributed (NCCL), ranks in z order.  Dot products are
+    the slabs' FP64 partial sums, all-reduced.  Returns (iterations,
+    ||r|| / ||b||)."""
+    import torch
+    if dist is not None and len(slabs) != 1:
+        raise ValueError("one slab per rank with a process group")
+    dev = slabs[0].torch_device
+    plane = slabs[0].plane
+    if dist is None:
+        bufs = (torch.empty(plane, dtype=torch.float64, device=dev), torch.empty(plane, dtype=torch.float64, device=dev))
+        exchange = lambda: _exchange_local(slabs, bufs)  # noqa: E731
+    else:
+        bufs = tuple(torch.empty(plane, dtype=torch.float64, device=dev) for _ in range(4))
+        exchange = lambda: _exchange_dist(slabs[0], bufs, dist, group)  # noqa: E731
+
+    def total(vals):
+        s = 0.0
+        for v in vals:
+            s += v
+        return allreduce_sum(s, dist, dev, group) if dist is not None else s
+
+    bb = total([s.begin() for s in slabs])
+    if bb == 0.0:
+        return 0, 0.0
+    rz = total([s.precond() for s in slabs])
+    for s in slabs:
+        s.direction(0.0, True)
+    rr, it = bb, 0
+    while it < maxiter and rr / bb >= tol * tol:
+        it += 1
+        exchange()
+        sp = total([s.apply() for s in slabs])
+        alpha = rz / sp
+        rr = total([s.update(alpha) for s in slabs])
+        if rr / bb < tol * tol or it >= maxiter:
+            break
+        rz_new = total([s.precond() for s in slabs])
+        beta = rz_new / rz
+        rz = rz_new
+        for s in slabs:
+            s.direction(beta, False)
+    return it, (rr / bb) ** 0.5

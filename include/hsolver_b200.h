@@ -351,6 +351,38 @@ int hs_channel_adjoint(hs_channel *h, double tol, int maxiter, double *J, double
                        int n_blocks, hs_adjoint_info *info);
 void hs_channel_destroy(hs_channel *h);
 
+/* One rank's z-slab of the channel pressure-correction system, for meshes
+ * sharded over GPUs; the reference's counterpart is its domain decomposition
+ * (Scotch parts, mesh/mesh.cpp:735-1122) with the HYPRE PCG over MPI ranks
+ * (fluid_solver.h:1713-2194, setup 1840-1889).  The slab holds its nz
+ * interior planes of an nx x ny grid and a ghost plane below and above.  The
+ * host runs the CG recurrences: it all-reduces the local partial sums these
+ * calls return (FP64) and, before each hs_slab_apply, moves the search
+ * direction's first and last interior planes (hs_slab_halo_get) into the
+ * neighbouring slabs' ghost planes (hs_slab_halo_put); the end slabs' outer
+ * ghost planes stay zero.  Preconditioner: a multigrid V-cycle on the slab's
+ * own rows (block Jacobi), symmetric positive definite.  hsolver_b200/slabs.py
+ * drives it over NCCL or for several slabs of one process.  Every call is
+ * synchronous. */
+typedef struct hs_slab hs_slab;
+int hs_slab_create(int nx, int ny, int nz, int device, hs_slab **out);
+/* Host face couplings: gx ((nx+1) ny nz), gy (nx (ny+1) nz), gz (nx ny (nz+1):
+ * faces 0 and nz are the slab's bottom and top faces), x fastest; b (nx ny nz). */
+int hs_slab_set_system(hs_slab *h, const double *gx, const double *gy, const double *gz, const double *b);
+int hs_slab_begin(hs_slab *h, double *bb);               /* x = 0, r = b; local <b, b> */
+int hs_slab_precond(hs_slab *h, double *rz);             /* z = V-cycle(r); local <r, z> */
+int hs_slab_direction(hs_slab *h, double beta, int first); /* p = z + beta p (first: p = z) */
+int hs_slab_apply(hs_slab *h, double *sp);               /* s = A p; local <s, p> */
+int hs_slab_update(hs_slab *h, double alpha, double *rr); /* x += alpha p, r -= alpha s; local <r, r> */
+int hs_slab_plane_size(hs_slab *h, long long *n);        /* FP64 values per padded plane */
+/* p's first / last interior plane into device buffers of hs_slab_plane_size
+ * values (NULL: skipped); and device buffers into p's ghost planes below /
+ * above (NULL: left as they are). */
+int hs_slab_halo_get(hs_slab *h, double *lo, double *hi);
+int hs_slab_halo_put(hs_slab *h, const double *lo, const double *hi);
+int hs_slab_get(hs_slab *h, int which, double *host);    /* 0 x, 1 r, 2 p, 3 s: nx ny nz values */
+void hs_slab_destroy(hs_slab *h);
+
 /* Validation of the divisions the sweeps perform with precomputed
  * reciprocals: returns how many of the n host pairs (a[i], b[i]) give a
  * quotient that differs in any bit from IEEE a/b on the current device

@@ -149,3 +149,106 @@ def test_slab_operator_and_cg_match_the_single_domain(world):
     assert np.array_equal(y, y_ref)  # every cell's sum in the same order: bit for bit
     assert len(its) == 1 and abs(its.pop() - it_ref) <= 1
     assert np.linalg.norm(sol - sol_ref) <= 1e-9 * np.linalg.norm(sol_ref)
+
+
+class NumpySlab:
+    """The interface of hsolver_b200.slabs.SlabPCG in NumPy on the CPU
+    (Jacobi in place of the V-cycle: block diagonal and SPD as well), so that
+    the sharded CG driver runs over gloo ranks without a GPU."""
+
+    def __init__(self, gx, gy, gz, b):
+        import torch
+        self.gx, self.gy, self.gz, self.b = gx, gy, gz, b
+        nz, ny, nx = b.shape
+        self.d = gx[:, :, :-1] + gx[:, :, 1:] + gy[:, :-1, :] + gy[:, 1:, :] + gz[:-1] + gz[1:]
+        self.x = np.zeros((nz + 2, ny, nx))
+        self.r = np.zeros((nz + 2, ny, nx))
+        self.p = np.zeros((nz + 2, ny, nx))
+        self.s = np.zeros((nz + 2, ny, nx))
+        self.plane = ny * nx
+        self.torch_device = torch.device("cpu")
+
+    def begin(self):
+        self.x[:] = 0.0
+        self.r[1:-1] = self.b
+        return float((self.b * self.b).sum())
+
+    def precond(self):
+        self.z = np.where(self.d > 0, self.r[1:-1] / np.where(self.d > 0, self.d, 1.0), 0.0)
+        return float((self.r[1:-1] * self.z).sum())
+
+    def direction(self, beta, first):
+        self.p[1:-1] = self.z if first else self.z + beta * self.p[1:-1]
+
+    def apply(self):
+        self.s[1:-1] = apply_slab(self.p, self.gx, self.gy, self.gz)
+        return float((self.s[1:-1] * self.p[1:-1]).sum())
+
+    def update(self, alpha):
+        self.x[1:-1] += alpha * self.p[1:-1]
+        self.r[1:-1] -= alpha * self.s[1:-1]
+        return float((self.r[1:-1] ** 2).sum())
+
+    def halo_get(self, lo, hi):
+        import torch
+        if lo is not None:
+            lo.copy_(torch.from_numpy(self.p[1].ravel().copy()))
+        if hi is not None:
+            hi.copy_(torch.from_numpy(self.p[-2].ravel().copy()))
+
+    def halo_put(self, lo, hi):
+        if lo is not None:
+            self.p[0] = lo.numpy().reshape(self.p[0].shape)
+        if hi is not None:
+            self.p[-1] = hi.numpy().reshape(self.p[-1].shape)
+
+
+def _pcg_rank(rank, world, port, q):
+    import torch.distributed as dist
+    from hsolver_b200 import slabs
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        gx, gy, gz, b = _system()
+        k0, k1 = slabs.slab_bounds(NZ, world, rank)
+        s = NumpySlab(gx[k0:k1], gy[k0:k1], gz[k0:k1 + 1], b[k0:k1])
+        it, rel = slabs.slab_pcg_solve([s], tol=1e-10, maxiter=500, dist=dist)
+        q.put((rank, k0, k1, s.x[1:-1].copy(), it, rel))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_sharded_pcg_driver_over_ranks_matches_one_process(world):
+    """hsolver_b200.slabs.slab_pcg_solve with one slab per gloo rank (halo
+    planes by send/recv, dots all-reduced) gives the iterates of the same
+    slabs driven in one process (halo planes copied): the same iteration
+    count and the solution to round-off; both solve the global system."""
+    import multiprocessing as mp
+    from hsolver_b200 import slabs
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_pcg_rank, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    got = [q.get(timeout=240) for _ in range(world)]
+    for p in procs:
+        p.join(timeout=60)
+    assert all(p.exitcode == 0 for p in procs)
+    gx, gy, gz, b = _system()
+    local = []
+    for r in range(world):
+        k0, k1 = slabs.slab_bounds(NZ, world, r)
+        local.append(NumpySlab(gx[k0:k1], gy[k0:k1], gz[k0:k1 + 1], b[k0:k1]))
+    it_loc, rel_loc = slabs.slab_pcg_solve(local, tol=1e-10, maxiter=500)
+    x_loc = np.concatenate([s.x[1:-1] for s in local])
+    x = np.zeros_like(x_loc)
+    for rank, k0, k1, xl, it, rel in got:
+        x[k0:k1] = xl
+        assert abs(it - it_loc) <= 1 and rel < 1e-10
+    assert np.linalg.norm(x - x_loc) <= 1e-9 * np.linalg.norm(x_loc)
+    pad = lambda v: np.concatenate([np.zeros((1, NY, NX)), v, np.zeros((1, NY, NX))])  # noqa: E731
+    res = b - apply_slab(pad(x), gx, gy, gz)
+    assert np.linalg.norm(res) <= 1e-9 * np.linalg.norm(b)
