@@ -360,6 +360,7 @@ def run_gpu(args):
         variants["like_for_like"] = like_for_like(torch, hsolver_b200, local)
         variants["config5"] = config5(torch, hsolver_b200, local)
         variants["convection"] = convection(torch, hsolver_b200, local)
+        variants["sharded_p_solve"] = sharded_p_solve(local)
 
     if rank == 0:
         peak, peak_kind = hbm_peak()
@@ -456,6 +457,47 @@ def convection(torch, hsolver_b200, local):
         out[name] = {"value": 10 / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms / 10,
                      "momentum_ms_per_step": phases["momentum"], "pcg_iters": iters}
         g.close()
+    return out
+
+
+def sharded_p_solve(local, dims=(256, 128, 128)):
+    """The z-slab pressure-correction solve (hs_slab_*, slabs.slab_pcg_solve)
+    on this GPU: a seeded channel-like system of the bench case's size (face
+    couplings U[0.5, 2], walls, inlet and outlet faces) to rtol 1e-5 cut into
+    1, 2 and 4 slabs whose halo planes are copied between them (the
+    multi-GPU form moves the same planes over NCCL), with block Jacobi alone
+    (the iteration count grows with the slab count) and with the global
+    coarse correction on 8^3-cell aggregates; the per-iteration time
+    includes the host's sums of every dot product (one synchronisation per
+    pass)."""
+    import numpy as np
+    from hsolver_b200 import slabs
+    nx, ny, nz = dims
+    rng = np.random.default_rng(0)
+    gx = rng.uniform(0.5, 2.0, (nz, ny, nx + 1))
+    gy = rng.uniform(0.5, 2.0, (nz, ny + 1, nx))
+    gz = rng.uniform(0.5, 2.0, (nz + 1, ny, nx))
+    gx[:, :, 0] = 0.0
+    gy[:, 0, :] = gy[:, -1, :] = 0.0
+    gz[0] = gz[-1] = 0.0
+    b = rng.standard_normal((nz, ny, nx))
+    out = {"workload": "p' system %dx%dx%d, rtol 1e-5, slabs on one GPU" % dims}
+    for n in (1, 2, 4):
+        for two_level in (False, True):
+            parts = []
+            for r in range(n):
+                k0, k1 = slabs.slab_bounds(nz, n, r)
+                sl = slabs.SlabPCG(nx, ny, k1 - k0, device=local, coarse=(8, k0, nz) if two_level else None)
+                sl.set_system(gx[k0:k1], gy[k0:k1], gz[k0:k1 + 1], b[k0:k1])
+                parts.append(sl)
+            slabs.slab_pcg_solve(parts, tol=1e-5, maxiter=2000)  # warm-up (builds the hierarchies)
+            t0 = time.perf_counter()
+            it, rel = slabs.slab_pcg_solve(parts, tol=1e-5, maxiter=2000)
+            dt = time.perf_counter() - t0
+            for sl in parts:
+                sl.close()
+            out["slabs_%d%s" % (n, "_two_level" if two_level else "")] = {
+                "iters": it, "relres": rel, "ms": dt * 1e3, "ms_per_iter": dt * 1e3 / max(it, 1)}
     return out
 
 

@@ -768,6 +768,35 @@ int hs_slab_get(hs_slab *h, int which, double *host) {
   return slab_guarded(h, [&](hs::SlabState *s) { hs::slab_get(s, which, host); return HS_OK; });
 }
 
+int hs_slab_set_coarse(hs_slab *h, int agg, int kg0, int nzg) {
+  return slab_guarded(h, [&](hs::SlabState *s) { hs::slab_set_coarse(s, agg, kg0, nzg); return HS_OK; });
+}
+
+int hs_slab_coarse_sizes(hs_slab *h, long long *n4) {
+  if (!n4) return fail(nullptr, HS_ERR_ARG, "null output pointer");
+  return slab_guarded(h, [&](hs::SlabState *s) { hs::slab_coarse_sizes(s, n4); return HS_OK; });
+}
+
+int hs_slab_coarse_partial(hs_slab *h, double *cgx, double *cgy, double *cgz) {
+  if (!cgx || !cgy || !cgz) return fail(nullptr, HS_ERR_ARG, "null array");
+  return slab_guarded(h, [&](hs::SlabState *s) { hs::slab_coarse_partial(s, cgx, cgy, cgz); return HS_OK; });
+}
+
+int hs_slab_coarse_build(hs_slab *h, const double *cgx, const double *cgy, const double *cgz) {
+  if (!cgx || !cgy || !cgz) return fail(nullptr, HS_ERR_ARG, "null array");
+  return slab_guarded(h, [&](hs::SlabState *s) { hs::slab_coarse_build(s, cgx, cgy, cgz); return HS_OK; });
+}
+
+int hs_slab_restrict(hs_slab *h, double *rc) {
+  if (!rc) return fail(nullptr, HS_ERR_ARG, "null array");
+  return slab_guarded(h, [&](hs::SlabState *s) { hs::slab_restrict(s, rc); return HS_OK; });
+}
+
+int hs_slab_coarse_correct(hs_slab *h, const double *rc, double *rz) {
+  if (!rc) return fail(nullptr, HS_ERR_ARG, "null array");
+  return slab_guarded(h, [&](hs::SlabState *s) { const double v = hs::slab_coarse_correct(s, rc); if (rz) *rz = v; return HS_OK; });
+}
+
 void hs_slab_destroy(hs_slab *h) {
   if (!h) return;
   hs::slab_destroy(h->st);

@@ -175,6 +175,68 @@ __global__ void k_sl_mask(SlabDev D, uint8_t *m, double *d) {
 
 int pitch4(int n) { return (n + 3) / 4 * 4; }
 
+// The two-level preconditioner's global coarse grid: aggregates of agg^3 fine
+// cells (fine (i, j, kg) with kg the global plane, in coarse cell
+// (i / agg, j / agg, kg / agg)), piecewise-constant prolongation P, the
+// restriction P^T (sums over an aggregate) and A_c = P^T A P, whose face
+// couplings are the sums of the fine couplings on the aggregates' faces.
+struct CoarseMap {
+  int agg, kg0, ncx, ncy, ncz;
+};
+
+// partial P^T r of this slab: one thread per coarse cell sums its fine cells
+// in this slab's planes (k, j, i ascending), 0 where it has none
+__global__ void k_sl_restrict(SlabDev D, CoarseMap M, double *rc) {
+  const int nc = M.ncx * M.ncy * M.ncz;
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += gridDim.x * blockDim.x) {
+    const int I = c % M.ncx, J = (c / M.ncx) % M.ncy, K = c / (M.ncx * M.ncy);
+    const int i0 = I * M.agg, i1 = min(i0 + M.agg, D.nx), j0 = J * M.agg, j1 = min(j0 + M.agg, D.ny);
+    const int k0 = max(K * M.agg - M.kg0, 0), k1 = min((K + 1) * M.agg - M.kg0, D.nz);
+    double acc = 0.0;
+    for (int k = k0; k < k1; ++k)
+      for (int j = j0; j < j1; ++j)
+        for (int i = i0; i < i1; ++i) acc += D.r[sq(D, i, j, k)];
+    rc[c] = acc;
+  }
+}
+
+// coarse correction: the coarse grid's V-cycle on rc (the coarse hierarchy
+// built first when `build` is set), then z += P zc on this slab's unknowns
+// (level 0's x of the slab's hierarchy holds z from slab_precond) and the
+// partial sums of <r, z> per block
+__global__ void __launch_bounds__(kSlVT, 1) k_sl_coarse(SlabDev D, mg::Hier<double> G, mg::Hier<double> C,
+                                                       CoarseMap M, const double *rc, int build, double *part) {
+  cg::grid_group grid = cg::this_grid();
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x, T = gridDim.x * blockDim.x;
+  const mg::Level<double> &C0 = C.lv[0];
+  if (build) {
+    mg::build(C, false, grid, tid, T);
+  } else {
+    mg::factor(C, false);
+    if (blockIdx.x == 0) mg::stage_ro(C);
+    grid.sync();
+  }
+  for (mg::Walk w(C0.nx, C0.ny, C0.nz, tid, T); w.ok(); w.next()) {
+    const int q = mg::idx(C0, w.m + 1, w.j + 1, w.k + 1);
+    const mg::Seed<double> sd = mg::seed_at(C0, w.m, w.j, w.k, q, false);
+    sd.store(C0, q, rc[w.flat()]);
+  }
+  grid.sync();
+  mg::vcycle<double, double, true>(C, false, grid, tid, T);
+  const mg::Level<double> &L0 = G.lv[0];
+  double acc = 0.0;
+  for (mg::Walk w(D.nx, D.ny, D.nz, tid, T); w.ok(); w.next()) {
+    const int q = sq(D, w.m, w.j, w.k);
+    const int qc = mg::idx(C0, w.m / M.agg + 1, w.j / M.agg + 1, (w.k + M.kg0) / M.agg + 1);
+    const double zc = __ldcg(C0.x + qc);
+    const double z = __ldcg(L0.x + q) + (L0.m[q] ? zc : 0.0);
+    L0.x[q] = z;
+    acc += D.r[q] * z;
+  }
+  const double t = sl_block_sum(acc);
+  if (threadIdx.x == 0) part[blockIdx.x] = t;
+}
+
 }  // namespace
 
 struct SlabState {
@@ -188,6 +250,14 @@ struct SlabState {
   mg::Hier<double> G{};
   int vgrid = 0;
   bool built = false;
+  // the global coarse grid of the two-level preconditioner (aggregates of
+  // agg^3 cells; every slab holds the whole coarse grid and its hierarchy)
+  int agg = 0, kg0 = 0, nzg = 0, ncx = 0, ncy = 0, ncz = 0;
+  mg::Hier<double> C{};
+  double *crhs = nullptr;  // coarse rhs (nc values, x fastest), uploaded each application
+  double *crc = nullptr;   // this slab's partial coarse rhs
+  bool cbuilt = false;
+  std::vector<double> cpart[3];  // this slab's partial coarse face couplings (set_system)
 
   template <class T_>
   T_ *alloc(size_t n) {
@@ -281,6 +351,133 @@ SlabState *slab_create(int nx, int ny, int nz, int device) {
 
 void slab_destroy(SlabState *S) { delete S; }
 
+namespace {
+// a hierarchy for an nx x ny x nz level 0 whose couplings are allocated here
+void alloc_hier(SlabState &S, mg::Hier<double> &G, int lx, int ly, int lz, const double *g0x, const double *g0y,
+                const double *g0z) {
+  int L = 0;
+  while (true) {
+    if (L >= mg::kMgMaxLv) throw std::runtime_error("multigrid: too many levels");
+    mg::Level<double> &l = G.lv[L];
+    l.nx = lx; l.ny = ly; l.nz = lz; l.px = pitch4(lx + 2);
+    const size_t n = (size_t)l.px * (ly + 2) * (lz + 2);
+    l.x = S.alloc<double>(n); l.rhs = S.alloc<double>(n);
+    if (L == 0 && g0x) {
+      l.gx = const_cast<double *>(g0x); l.gy = const_cast<double *>(g0y); l.gz = const_cast<double *>(g0z);
+    } else {
+      l.gx = S.alloc<double>(n); l.gy = S.alloc<double>(n); l.gz = S.alloc<double>(n);
+    }
+    l.d = L == 0 ? S.alloc<double>(n) : nullptr;
+    l.fx = l.fy = l.fz = nullptr;
+    l.m = S.alloc<uint8_t>(n);
+    ++L;
+    if ((long long)lx * ly * lz <= mg::kMgCoarse) break;
+    lx = (lx + 1) / 2; ly = (ly + 1) / 2; lz = (lz + 1) / 2;
+  }
+  G.L = L;
+  G.nsw = 2;
+  G.nswc = 3;
+  G.lu = S.alloc<double>((size_t)mg::kMgCoarse * mg::kMgCoarse);
+  mg::plan_stage(G);
+}
+
+// the padded level-0 couplings, mask and diagonal of hierarchy G from host
+// face arrays (as slab_set_system takes them)
+void upload_level0(SlabState &S, const mg::Level<double> &L, const double *gx, const double *gy, const double *gz) {
+  const int nx = L.nx, ny = L.ny, nz = L.nz, px = L.px;
+  const size_t np = (size_t)px * (ny + 2) * (nz + 2);
+  auto pq = [&](int i, int j, int k) { return (size_t)i + px * ((size_t)j + (ny + 2) * (size_t)k); };
+  std::vector<double> a(np), d(np, 0.0);
+  std::vector<uint8_t> m(np, 0);
+  const double *src[3] = {gx, gy, gz};
+  double *dst[3] = {L.gx, L.gy, L.gz};
+  std::vector<double> g[3];
+  for (int ax = 0; ax < 3; ++ax) {
+    std::fill(a.begin(), a.end(), 0.0);
+    const int fx = nx + (ax == 0), fy = ny + (ax == 1), fz = nz + (ax == 2);
+    for (int k = 0; k < fz; ++k)
+      for (int j = 0; j < fy; ++j)
+        for (int i = 0; i < fx; ++i) a[pq(i + 1, j + 1, k + 1)] = src[ax][i + (size_t)fx * (j + (size_t)fy * k)];
+    g[ax] = a;
+    SL_CUDA(cudaMemcpyAsync(dst[ax], a.data(), np * 8, cudaMemcpyHostToDevice, S.stream));
+    SL_CUDA(cudaStreamSynchronize(S.stream));
+  }
+  const size_t PX = px, PXY = (size_t)px * (ny + 2);
+  for (int k = 0; k < nz; ++k)
+    for (int j = 0; j < ny; ++j)
+      for (int i = 0; i < nx; ++i) {
+        const size_t q = pq(i + 1, j + 1, k + 1);
+        const double dv = g[0][q] + g[0][q + 1] + g[1][q] + g[1][q + PX] + g[2][q] + g[2][q + PXY];
+        d[q] = dv;
+        m[q] = dv > 0.0;
+      }
+  SL_CUDA(cudaMemcpyAsync(L.d, d.data(), np * 8, cudaMemcpyHostToDevice, S.stream));
+  SL_CUDA(cudaMemcpyAsync(L.m, m.data(), np, cudaMemcpyHostToDevice, S.stream));
+  SL_CUDA(cudaStreamSynchronize(S.stream));
+}
+}  // namespace
+
+void slab_set_coarse(SlabState *S, int agg, int kg0, int nzg) {
+  if (agg < 2 || kg0 < 0 || kg0 + S->nz > nzg) throw std::invalid_argument("invalid coarse grid");
+  if (S->agg) throw std::invalid_argument("the coarse grid is set already");
+  S->agg = agg;
+  S->kg0 = kg0;
+  S->nzg = nzg;
+  S->ncx = (S->nx + agg - 1) / agg;
+  S->ncy = (S->ny + agg - 1) / agg;
+  S->ncz = (nzg + agg - 1) / agg;
+  alloc_hier(*S, S->C, S->ncx, S->ncy, S->ncz, nullptr, nullptr, nullptr);
+  const size_t nc = (size_t)S->ncx * S->ncy * S->ncz;
+  S->crhs = S->alloc<double>(nc);
+  S->crc = S->alloc<double>(nc);
+  SL_CUDA(cudaFuncSetAttribute((const void *)k_sl_coarse, cudaFuncAttributeMaxDynamicSharedMemorySize, mg::kMgStageTotal));
+  int nsm = 0, per = 0;
+  SL_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, S->device));
+  SL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, (const void *)k_sl_coarse, kSlVT,
+                                                        (size_t)std::max(S->C.stage, S->G.stage)));
+  if (per < 1) throw std::runtime_error("slab coarse-correction kernel cannot be resident");
+  S->vgrid = std::min(S->vgrid, per * nsm);
+  SL_CUDA(cudaStreamSynchronize(S->stream));
+}
+
+// the partial coarse face couplings of this slab (sums of its fine faces on
+// aggregate faces; a z-face between two slabs counted by the upper one)
+void slab_coarse_partial_compute(SlabState *S, const double *gx, const double *gy, const double *gz) {
+  if (!S->agg) return;
+  const int nx = S->nx, ny = S->ny, nz = S->nz, a = S->agg, kg0 = S->kg0;
+  const int ncx = S->ncx, ncy = S->ncy, ncz = S->ncz;
+  std::vector<double> &cx = S->cpart[0], &cy = S->cpart[1], &cz = S->cpart[2];
+  cx.assign((size_t)(ncx + 1) * ncy * ncz, 0.0);
+  cy.assign((size_t)ncx * (ncy + 1) * ncz, 0.0);
+  cz.assign((size_t)ncx * ncy * (ncz + 1), 0.0);
+  for (int k = 0; k < nz; ++k) {
+    const int K = (k + kg0) / a;
+    for (int j = 0; j < ny; ++j)
+      for (int f = 0; f <= nx; ++f)
+        if (f % a == 0 || f == nx) {
+          const int I = (f == nx) ? ncx : f / a;
+          cx[I + (size_t)(ncx + 1) * (j / a + (size_t)ncy * K)] += gx[f + (size_t)(nx + 1) * (j + (size_t)ny * k)];
+        }
+    for (int f = 0; f <= ny; ++f)
+      if (f % a == 0 || f == ny) {
+        const int J = (f == ny) ? ncy : f / a;
+        for (int i = 0; i < nx; ++i)
+          cy[i / a + (size_t)ncx * (J + (size_t)(ncy + 1) * K)] += gy[i + (size_t)nx * (f + (size_t)(ny + 1) * k)];
+      }
+  }
+  // z faces: local face f (global f + kg0) for f in [0, nz), and the top face
+  // nz only when it is the domain's top face (else the slab above owns it)
+  for (int f = 0; f <= nz; ++f) {
+    const int fg = f + kg0;
+    if (f == nz && fg != S->nzg) continue;
+    if (!(fg % a == 0 || fg == S->nzg)) continue;  // inside an aggregate
+    const int Kf = fg == S->nzg ? ncz : fg / a;
+    for (int j = 0; j < ny; ++j)
+      for (int i = 0; i < nx; ++i)
+        cz[i / a + (size_t)ncx * (j / a + (size_t)ncy * Kf)] += gz[i + (size_t)nx * (j + (size_t)ny * f)];
+  }
+}
+
 void slab_set_system(SlabState *S, const double *gx, const double *gy, const double *gz, const double *b) {
   const int nx = S->nx, ny = S->ny, nz = S->nz, px = S->px;
   const size_t np = S->np;
@@ -314,6 +511,51 @@ void slab_set_system(SlabState *S, const double *gx, const double *gy, const dou
   SL_CUDA(cudaGetLastError());
   SL_CUDA(cudaStreamSynchronize(S->stream));
   S->built = false;
+  slab_coarse_partial_compute(S, gx, gy, gz);
+  S->cbuilt = false;
+}
+
+void slab_coarse_sizes(const SlabState *S, long long *n4) {
+  n4[0] = (long long)(S->ncx + 1) * S->ncy * S->ncz;
+  n4[1] = (long long)S->ncx * (S->ncy + 1) * S->ncz;
+  n4[2] = (long long)S->ncx * S->ncy * (S->ncz + 1);
+  n4[3] = (long long)S->ncx * S->ncy * S->ncz;
+}
+
+void slab_coarse_partial(const SlabState *S, double *cgx, double *cgy, double *cgz) {
+  if (!S->agg) throw std::invalid_argument("no coarse grid set (hs_slab_set_coarse)");
+  if (S->cpart[0].empty()) throw std::invalid_argument("no system set (hs_slab_set_system)");
+  std::copy(S->cpart[0].begin(), S->cpart[0].end(), cgx);
+  std::copy(S->cpart[1].begin(), S->cpart[1].end(), cgy);
+  std::copy(S->cpart[2].begin(), S->cpart[2].end(), cgz);
+}
+
+void slab_coarse_build(SlabState *S, const double *cgx, const double *cgy, const double *cgz) {
+  if (!S->agg) throw std::invalid_argument("no coarse grid set (hs_slab_set_coarse)");
+  upload_level0(*S, S->C.lv[0], cgx, cgy, cgz);
+  S->cbuilt = false;
+}
+
+void slab_restrict(SlabState *S, double *rc_host) {
+  if (!S->agg) throw std::invalid_argument("no coarse grid set (hs_slab_set_coarse)");
+  const CoarseMap M{S->agg, S->kg0, S->ncx, S->ncy, S->ncz};
+  const int nc = S->ncx * S->ncy * S->ncz;
+  k_sl_restrict<<<std::max(1, std::min((nc + kSlT - 1) / kSlT, kSlBlocks)), kSlT, 0, S->stream>>>(S->D, M, S->crc);
+  SL_CUDA(cudaGetLastError());
+  SL_CUDA(cudaMemcpyAsync(rc_host, S->crc, (size_t)nc * 8, cudaMemcpyDeviceToHost, S->stream));
+  SL_CUDA(cudaStreamSynchronize(S->stream));
+}
+
+double slab_coarse_correct(SlabState *S, const double *rc_host) {
+  if (!S->agg) throw std::invalid_argument("no coarse grid set (hs_slab_set_coarse)");
+  const CoarseMap M{S->agg, S->kg0, S->ncx, S->ncy, S->ncz};
+  const size_t nc = (size_t)S->ncx * S->ncy * S->ncz;
+  SL_CUDA(cudaMemcpyAsync(S->crhs, rc_host, nc * 8, cudaMemcpyHostToDevice, S->stream));
+  const int build = S->cbuilt ? 0 : 1;
+  sl_coop(k_sl_coarse, S->vgrid, kSlVT, (size_t)S->C.stage, S->stream, S->D, S->G, S->C, M, (const double *)S->crhs,
+          build, S->part);
+  S->cbuilt = true;
+  return sl_sum(*S, S->vgrid);
 }
 
 double slab_begin(SlabState *S) {

@@ -21,5 +21,14 @@ long long slab_plane_size(const SlabState *s);        // values per padded plane
 void slab_halo_get(SlabState *s, double *lo, double *hi);        // p's first / last interior plane -> device buffers
 void slab_halo_put(SlabState *s, const double *lo, const double *hi);  // device buffers -> p's ghost planes
 void slab_get(SlabState *s, int which, double *host);  // 0 x, 1 r, 2 p, 3 s: nx ny nz values
+// the two-level preconditioner's global coarse grid (aggregates of agg^3
+// cells; this slab's first plane is global plane kg0 of nzg): set once, before
+// slab_set_system, which then computes this slab's partial coarse couplings
+void slab_set_coarse(SlabState *s, int agg, int kg0, int nzg);
+void slab_coarse_sizes(const SlabState *s, long long *n4);  // coarse gx, gy, gz, cells
+void slab_coarse_partial(const SlabState *s, double *cgx, double *cgy, double *cgz);
+void slab_coarse_build(SlabState *s, const double *cgx, const double *cgy, const double *cgz);  // the sums over slabs
+void slab_restrict(SlabState *s, double *rc_host);           // this slab's part of P^T r
+double slab_coarse_correct(SlabState *s, const double *rc);  // z += P A_c^-1 rc (summed rc); local <r, z>
 
 }  // namespace hs

@@ -73,9 +73,11 @@ class SlabPCG:
     """One slab of the pressure-correction system on a GPU (hs_slab_* of the
     C ABI): face couplings gx (nz, ny, nx + 1), gy (nz, ny + 1, nx), gz
     (nz + 1, ny, nx) with gz[0] and gz[nz] the slab's bottom and top faces,
-    and the right-hand side b (nz, ny, nx), numpy arrays."""
+    and the right-hand side b (nz, ny, nx), numpy arrays.  coarse = (agg,
+    kg0, nzg): the two-level preconditioner's global coarse grid of agg^3-cell
+    aggregates, this slab starting at global plane kg0 of nzg."""
 
-    def __init__(self, nx, ny, nz, device=0):
+    def __init__(self, nx, ny, nz, device=0, coarse=None):
         import ctypes
         from . import load, HsError
         L = load()
@@ -84,7 +86,11 @@ class SlabPCG:
                "hs_slab_set_system": [vp, vp, vp, vp, vp], "hs_slab_begin": [vp, dp], "hs_slab_precond": [vp, dp],
                "hs_slab_direction": [vp, ctypes.c_double, ctypes.c_int], "hs_slab_apply": [vp, dp],
                "hs_slab_update": [vp, ctypes.c_double, dp], "hs_slab_plane_size": [vp, ctypes.POINTER(ctypes.c_longlong)],
-               "hs_slab_halo_get": [vp, vp, vp], "hs_slab_halo_put": [vp, vp, vp], "hs_slab_get": [vp, ctypes.c_int, vp]}
+               "hs_slab_halo_get": [vp, vp, vp], "hs_slab_halo_put": [vp, vp, vp], "hs_slab_get": [vp, ctypes.c_int, vp],
+               "hs_slab_set_coarse": [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int],
+               "hs_slab_coarse_sizes": [vp, ctypes.POINTER(ctypes.c_longlong)],
+               "hs_slab_coarse_partial": [vp, vp, vp, vp], "hs_slab_coarse_build": [vp, vp, vp, vp],
+               "hs_slab_restrict": [vp, vp], "hs_slab_coarse_correct": [vp, vp, dp]}
         for name, args in sig.items():
             getattr(L, name).argtypes = args
             getattr(L, name).restype = ctypes.c_int
@@ -102,6 +108,14 @@ class SlabPCG:
         n = ctypes.c_longlong()
         self._check(L.hs_slab_plane_size(h, ctypes.byref(n)))
         self.plane = n.value
+        self.coarse = coarse
+        self.coarse_ready = False
+        if coarse is not None:
+            agg, kg0, nzg = coarse
+            self._check(L.hs_slab_set_coarse(h, int(agg), int(kg0), int(nzg)))
+            n4 = (ctypes.c_longlong * 4)()
+            self._check(L.hs_slab_coarse_sizes(h, n4))
+            self.coarse_sizes = tuple(int(v) for v in n4)
 
     def _check(self, rc):
         if rc < 0:
@@ -120,6 +134,31 @@ class SlabPCG:
             if a.shape != shape:
                 raise ValueError("expected shape %s, got %s" % (shape, a.shape))
         self._check(self._L.hs_slab_set_system(self.h, *[a.ctypes.data for a in arrs]))
+        self.coarse_ready = False
+
+    def coarse_partial(self):
+        """This slab's partial coarse face couplings (gx, gy, gz of the coarse grid)."""
+        import numpy as np
+        out = [np.zeros(n) for n in self.coarse_sizes[:3]]
+        self._check(self._L.hs_slab_coarse_partial(self.h, *[a.ctypes.data for a in out]))
+        return out
+
+    def coarse_build(self, cg):
+        import numpy as np
+        arrs = [np.ascontiguousarray(a, np.float64) for a in cg]
+        self._check(self._L.hs_slab_coarse_build(self.h, *[a.ctypes.data for a in arrs]))
+        self.coarse_ready = True
+
+    def restrict(self):
+        import numpy as np
+        out = np.zeros(self.coarse_sizes[3])
+        self._check(self._L.hs_slab_restrict(self.h, out.ctypes.data))
+        return out
+
+    def coarse_correct(self, rc):
+        import numpy as np
+        a = np.ascontiguousarray(rc, np.float64)
+        return self._scalar(self._L.hs_slab_coarse_correct, a.ctypes.data)
 
     def begin(self):
         return self._scalar(self._L.hs_slab_begin)
@@ -203,7 +242,10 @@ def _exchange_dist(slab, bufs, dist, group):
 
 def slab_pcg_solve(slabs, tol=1e-8, maxiter=1000, dist=None, group=None):
     """CG on the pressure-correction system sharded into z-slabs, each
-    preconditioned by its own V-cycle (block Jacobi).  `slabs`: SlabPCG (or
+    preconditioned by its own V-cycle (block Jacobi), plus, when the slabs
+    carry a coarse grid, the additive global coarse correction (its
+    couplings summed over the slabs once per system, the restricted residual
+    summed every application).  `slabs`: SlabPCG (or
     any object with its methods, `plane` and `torch_device`): this
     process's slabs, bottom to top: every slab of the domain when dist is
     None (one process, one or more slabs on its GPU), or this rank's one slab
@@ -228,10 +270,36 @@ def slab_pcg_solve(slabs, tol=1e-8, maxiter=1000, dist=None, group=None):
             s += v
         return allreduce_sum(s, dist, dev, group) if dist is not None else s
 
+    def total_vec(vecs):
+        # element-wise FP64 sum over this process's slabs and over the ranks
+        out = vecs[0].copy()
+        for v in vecs[1:]:
+            out += v
+        if dist is not None:
+            t = torch.from_numpy(out).to(dev)
+            dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
+            out = t.cpu().numpy()
+        return out
+
+    coarse = getattr(slabs[0], "coarse", None) is not None
+    if coarse and not all(s.coarse_ready for s in slabs):
+        parts = [s.coarse_partial() for s in slabs]
+        cg = [total_vec([p[a] for p in parts]) for a in range(3)]
+        for s in slabs:
+            s.coarse_build(cg)
+
+    def precondition():
+        if not coarse:
+            return total([s.precond() for s in slabs])
+        for s in slabs:
+            s.precond()
+        rc = total_vec([s.restrict() for s in slabs])
+        return total([s.coarse_correct(rc) for s in slabs])
+
     bb = total([s.begin() for s in slabs])
     if bb == 0.0:
         return 0, 0.0
-    rz = total([s.precond() for s in slabs])
+    rz = precondition()
     for s in slabs:
         s.direction(0.0, True)
     rr, it = bb, 0
@@ -243,7 +311,7 @@ def slab_pcg_solve(slabs, tol=1e-8, maxiter=1000, dist=None, group=None):
         rr = total([s.update(alpha) for s in slabs])
         if rr / bb < tol * tol or it >= maxiter:
             break
-        rz_new = total([s.precond() for s in slabs])
+        rz_new = precondition()
         beta = rz_new / rz
         rz = rz_new
         for s in slabs:

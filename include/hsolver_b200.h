@@ -381,6 +381,23 @@ int hs_slab_plane_size(hs_slab *h, long long *n);        /* FP64 values per padd
 int hs_slab_halo_get(hs_slab *h, double *lo, double *hi);
 int hs_slab_halo_put(hs_slab *h, const double *lo, const double *hi);
 int hs_slab_get(hs_slab *h, int which, double *host);    /* 0 x, 1 r, 2 p, 3 s: nx ny nz values */
+/* Two-level preconditioner (additive): z = V-cycle(r) on the slab + P A_c^-1
+ * P^T r on a global coarse grid of agg^3-cell aggregates held by every slab
+ * (P piecewise constant, A_c = P^T A P, solved by its own V-cycle), which
+ * restores the global coarse correction that block Jacobi lacks.  Set once
+ * after hs_slab_create (this slab's first plane is global plane kg0 of nzg);
+ * after each hs_slab_set_system, sum every slab's hs_slab_coarse_partial
+ * couplings (sizes from hs_slab_coarse_sizes: coarse gx, gy, gz faces and
+ * cells) and pass the sums to hs_slab_coarse_build on every slab.  Per
+ * application: hs_slab_precond, then sum every slab's hs_slab_restrict and
+ * pass the sum to hs_slab_coarse_correct, whose local <r, z> replaces the
+ * one hs_slab_precond returned. */
+int hs_slab_set_coarse(hs_slab *h, int agg, int kg0, int nzg);
+int hs_slab_coarse_sizes(hs_slab *h, long long n4[4]);
+int hs_slab_coarse_partial(hs_slab *h, double *cgx, double *cgy, double *cgz);
+int hs_slab_coarse_build(hs_slab *h, const double *cgx, const double *cgy, const double *cgz);
+int hs_slab_restrict(hs_slab *h, double *rc);
+int hs_slab_coarse_correct(hs_slab *h, const double *rc, double *rz);
 void hs_slab_destroy(hs_slab *h);
 
 /* Validation of the divisions the sweeps perform with precomputed
