@@ -467,15 +467,16 @@ __device__ void mom_pass_axis(const ChDev<R> &H, int color, bool first, bool las
 // four 256-thread blocks per SM (64 registers: above that the SM holds three).
 // X: 0 first-order upwind, 1 hybrid, 2 any scheme with the source terms
 // (QUICK deferred correction, buoyancy): separate instantiations, so that the
-// upwind and hybrid forms keep their registers; the source-term one takes
-// three blocks per SM (80 registers, no spills; at 64 it spilled 360 B).
+// upwind and hybrid forms keep their registers (the source-term one spills
+// 360 B at 64 registers, and is still faster than at 80 registers without
+// spills and three blocks per SM: 1.42 against 1.58 ms per momentum solve).
 // The grid is 3 x (chunks): the three components of one chunk of faces are
 // consecutive blocks, so they run at the same time and share the u^n they
 // all read in L2 (component-major order read the three velocity arrays once
 // per component from DRAM: 0.80 -> 0.71 ms per FP64 momentum solve at
 // 256x128x128).
 template <class R, int X>
-__global__ void __launch_bounds__(kT, X == 2 ? 3 : 4) k_ch_mom(ChDev<R> H, int color, int first, int last, double *partials) {
+__global__ void __launch_bounds__(kT, 4) k_ch_mom(ChDev<R> H, int color, int first, int last, double *partials) {
   __shared__ double sh[32];
   double racc = 0.0;
   const int comp = blockIdx.x % 3;
