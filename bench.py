@@ -18,6 +18,7 @@ in-repo; the state (~790 MB on the device) is larger than L2.
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
                   [--no-cpu-baseline] [--no-variants]
   python bench.py --probe NAME [--steps K] [--mixed] [--p-tol X] [--t-tol X]
+                  [--t-maxiter N] [--p-level0 L] [--conv C] [--ri X]
 
 Prints one JSON line.  Variants on the same GPU: the mixed-precision form,
 the adjoint/forward cost of the energy gradient, wall time to a global
@@ -25,7 +26,9 @@ residual of 1e-6 (the 256x128x128 case, config 1 and config 3; the first is
 also `time_to_1e-6` and `speedup_mixed` at the top level), the
 reference-faithful lid-cavity step on the same grid, the reference's own
 compiled code against the GPU on the reference's deck (`like_for_like`),
-and the 512x256x256 case.  `--gpus N` > 1 without a launcher reruns itself
+the 512x256x256 case, the momentum convection schemes with buoyancy
+(`convection`) and the z-slab pressure-correction solve on 1, 2 and 4 slabs
+of this GPU (`sharded_p_solve`).  `--gpus N` > 1 without a launcher reruns itself
 under torch.distributed.run with N ranks (independent replicas, one per
 GPU).  `--impl reference` times the CPU restatement (oracle/, FP64, OpenMP on
 every host thread, the count in cpu_baseline.cores) on 1-2 outer steps of the
