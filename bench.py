@@ -470,7 +470,7 @@ def sharded_p_solve(local, dims=(256, 128, 128)):
     1, 2 and 4 slabs whose halo planes are copied between them (the
     multi-GPU form moves the same planes over NCCL), with block Jacobi alone
     (the iteration count grows with the slab count) and with the global
-    coarse correction on 8^3-cell aggregates; the per-iteration time
+    coarse correction on 4^3-cell aggregates; the per-iteration time
     includes the host's sums of every dot product (one synchronisation per
     pass)."""
     import numpy as np
@@ -490,7 +490,7 @@ def sharded_p_solve(local, dims=(256, 128, 128)):
             parts = []
             for r in range(n):
                 k0, k1 = slabs.slab_bounds(nz, n, r)
-                sl = slabs.SlabPCG(nx, ny, k1 - k0, device=local, coarse=(8, k0, nz) if two_level else None)
+                sl = slabs.SlabPCG(nx, ny, k1 - k0, device=local, coarse=(4, k0, nz) if two_level else None)
                 sl.set_system(gx[k0:k1], gy[k0:k1], gz[k0:k1 + 1], b[k0:k1])
                 parts.append(sl)
             slabs.slab_pcg_solve(parts, tol=1e-5, maxiter=2000)  # warm-up (builds the hierarchies)
