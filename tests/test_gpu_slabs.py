@@ -125,3 +125,44 @@ def test_two_level_sharded_solve(nslab):
     if nslab > 1:
         assert its[True] < its[False], its
     assert its[True] <= 60, its
+
+
+def test_two_level_on_a_ragged_grid():
+    """Grid sizes that are no multiples of the aggregate (13 x 5 x 11 with
+    4^3 aggregates: partial aggregates on every axis, ny smaller than two
+    aggregates) on 3 slabs of 4, 4 and 3 planes: the direct solution."""
+    import scipy.sparse as sp
+    import scipy.sparse.linalg as spl
+    from hsolver_b200 import slabs
+    nx, ny, nz = 13, 5, 11
+    rng = np.random.default_rng(12)
+    gx = rng.uniform(0.5, 2.0, (nz, ny, nx + 1))
+    gy = rng.uniform(0.5, 2.0, (nz, ny + 1, nx))
+    gz = rng.uniform(0.5, 2.0, (nz + 1, ny, nx))
+    gx[:, :, 0] = 0.0
+    gy[:, 0, :] = gy[:, -1, :] = 0.0
+    gz[0] = gz[-1] = 0.0
+    b = rng.standard_normal((nz, ny, nx))
+    n = nx * ny * nz
+    idx = np.arange(n).reshape(nz, ny, nx)
+    d = gx[:, :, :-1] + gx[:, :, 1:] + gy[:, :-1, :] + gy[:, 1:, :] + gz[:-1] + gz[1:]
+    rows, cols, vals = [idx.ravel()], [idx.ravel()], [d.ravel()]
+    for c, a, bb in ((gx[:, :, 1:-1], idx[:, :, :-1], idx[:, :, 1:]), (gy[:, 1:-1, :], idx[:, :-1, :], idx[:, 1:, :]),
+                     (gz[1:-1], idx[:-1], idx[1:])):
+        rows += [a.ravel(), bb.ravel()]
+        cols += [bb.ravel(), a.ravel()]
+        vals += [-c.ravel(), -c.ravel()]
+    A = sp.csr_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))), shape=(n, n))
+    xref = spl.spsolve(A, b.ravel()).reshape(nz, ny, nx)
+    parts = []
+    for r in range(3):
+        k0, k1 = slabs.slab_bounds(nz, 3, r)
+        s = slabs.SlabPCG(nx, ny, k1 - k0, device=0, coarse=(4, k0, nz))
+        s.set_system(gx[k0:k1], gy[k0:k1], gz[k0:k1 + 1], b[k0:k1])
+        parts.append(s)
+    it, rel = slabs.slab_pcg_solve(parts, tol=1e-12, maxiter=400)
+    x = np.concatenate([s.field("x") for s in parts])
+    for s in parts:
+        s.close()
+    assert rel < 1e-12
+    assert np.linalg.norm(x - xref) <= 1e-9 * np.linalg.norm(xref)
