@@ -425,7 +425,7 @@ __device__ double block_sum(double v, double *sh) {
   return t;
 }
 
-// One red-black pass of all three momentum components (blockIdx.y = axis).
+// One red-black pass of all three momentum components (component A).
 // first: the pass of colour 0 in sweep 0, which also evaluates the residual of
 // every unknown face at u^n and writes the fixed faces of u* (delta = 0).
 template <int A, int X, class R>
@@ -553,11 +553,30 @@ __global__ void k_ch_passemble(ChDev<R> H, R *acx, R *acy, R *acz, R *r, R *x, d
   if (threadIdx.x == 0 && blockIdx.y == 3) partials[blockIdx.x] = bsum;
 }
 
+// The four-part correction pass (k_ch_correct): block b does part b % 4 (u,
+// v, w, p) on chunk b / 4 of that part's elements in flat order, kT * per of
+// them (thread t: chunk * kT * per + t + kT m, m < per).  The resident blocks
+// of the four parts then cover the same z-planes at a time, so p', which
+// every part reads, comes from DRAM once (with the parts one after another it
+// came four times), and the block scheduler balances parts of unequal cost:
+// 0.102 -> 0.094 ms FP64, 0.126 -> 0.114 ms mixed at 256x128x128.  The
+// p' assembly's parts share only the solid mask and are slower dealt this
+// way (0.101 -> 0.114 ms: more arrays streaming at once).
+struct ChunkWalk : mg::Walk {
+  int left;
+  __device__ __forceinline__ ChunkWalk(int mx, int ny, int nz, int per)
+      : mg::Walk(mx, ny, nz, (int)(blockIdx.x >> 2) * kT * per + (int)threadIdx.x, kT), left(per) {}
+  __device__ __forceinline__ bool ok() const { return left > 0 && mg::Walk::ok(); }
+  __device__ __forceinline__ void next() {
+    --left;
+    mg::Walk::next();
+  }
+};
+
 template <int A, class R>
-__device__ void correct_axis(const ChDev<R> &H, const R *pp) {
+__device__ void correct_axis(const ChDev<R> &H, const R *pp, int per) {
   const int nf0 = H.N0 + (A == 0), nf1 = H.N1 + (A == 1), nf2 = H.N2 + (A == 2);
-  const int T = gridDim.x * blockDim.x, tid = blockIdx.x * blockDim.x + threadIdx.x;
-  for (mg::Walk w(nf0, nf1, nf2, tid, T); w.ok(); w.next()) {
+  for (ChunkWalk w(nf0, nf1, nf2, per); w.ok(); w.next()) {
     const int c[3] = {w.m, w.j, w.k};
     const int e = w.flat();
     // mixed form: u* = u^n + delta is read from u^n, which this pass
@@ -598,13 +617,15 @@ __device__ void correct_axis(const ChDev<R> &H, const R *pp) {
   }
 }
 
+// a four-part pass (ChunkWalk): u, v, w and p, every part reading p'
 template <class R>
-__global__ void k_ch_correct(ChDev<R> H, const R *pp) {
-  if (blockIdx.y == 0) correct_axis<0>(H, pp);
-  else if (blockIdx.y == 1) correct_axis<1>(H, pp);
-  else if (blockIdx.y == 2) correct_axis<2>(H, pp);
+__global__ void __launch_bounds__(kT) k_ch_correct(ChDev<R> H, const R *pp, int per) {
+  const int part = blockIdx.x & 3;
+  if (part == 0) correct_axis<0>(H, pp, per);
+  else if (part == 1) correct_axis<1>(H, pp, per);
+  else if (part == 2) correct_axis<2>(H, pp, per);
   else {
-    for (mg::Walk w(H.N0, H.N1, H.N2, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x); w.ok(); w.next()) {
+    for (ChunkWalk w(H.N0, H.N1, H.N2, per); w.ok(); w.next()) {
       const int e = w.flat();
       if (H.solid[e]) continue;
       H.p[e] = H.p[e] + H.ap * pp[pq(H.PX, H.N1, w.m, w.j, w.k)];
@@ -1001,13 +1022,14 @@ __global__ void __launch_bounds__(zm::kThreads, 1)
   }
 }
 
-// residual sums of the momentum pass (3 x nb partials) and continuity (nb) -> res[0..3]
+// residual sums of the momentum pass (3 x nbm partials) and continuity (nbc) -> res[0..3]
 // (launched with 4 warps: warp a sums array a, each lane over four
 // interleaved strides so that four loads are in flight)
-__global__ void k_ch_finalize(const double *mom, const double *cont, int nb, double *res) {
+__global__ void k_ch_finalize(const double *mom, int nbm, const double *cont, int nbc, double *res) {
   const int a = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (a >= 4) return;
-  const double *src = a < 3 ? mom + a * nb : cont;
+  const double *src = a < 3 ? mom + a * nbm : cont;
+  const int nb = a < 3 ? nbm : nbc;
   double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
   int q = lane;
   for (; q + 96 < nb; q += 128) {
@@ -1056,6 +1078,8 @@ struct ChannelState {
   mg::Hier<double> Gd{};
   mg::Hier<float> Gf{};
   int mom_blocks = 0, pcg_grid = 0;
+  int asm_blocks = 0;             // k_ch_passemble: blocks per part
+  int chunks = 0, chunk_per = 0;  // k_ch_correct: chunks per part, elements per thread
   // the z-marching form of the p' solve (k_ch_pcg_zm): its tensor maps, grid and shared memory
   PcgMaps TMd{}, TMf{};
   bool use_zm = false;
@@ -1341,9 +1365,9 @@ void step_once(ChannelState &S, ChDev<R> &H, int flags) {
   mom_solve(S, H);
   if (S.prof) CH_CUDA(cudaEventRecord(S.ev[1], S.stream));
   CgVec<R> &V = cg_vec<R>(S);
-  k_ch_passemble<R><<<dim3(S.mom_blocks, 4), kT, 0, S.stream>>>(H, (R *)V.acx, (R *)V.acy, (R *)V.acz, V.r, V.x,
+  k_ch_passemble<R><<<dim3(S.asm_blocks, 4), kT, 0, S.stream>>>(H, (R *)V.acx, (R *)V.acy, (R *)V.acz, V.r, V.x,
                                                                 S.cont_part);
-  k_ch_finalize<<<1, 128, 0, S.stream>>>(S.mom_part, S.cont_part, S.mom_blocks, S.res);
+  k_ch_finalize<<<1, 128, 0, S.stream>>>(S.mom_part, S.mom_blocks, S.cont_part, S.asm_blocks, S.res);
   CH_CUDA(cudaGetLastError());
   if (S.prof) CH_CUDA(cudaEventRecord(S.ev[2], S.stream));
   if (!(flags & 1)) {
@@ -1366,7 +1390,7 @@ void step_once(ChannelState &S, ChDev<R> &H, int flags) {
     CH_CUDA(cudaMemsetAsync(S.pcg_it, 0, sizeof(int), S.stream));
   }
   if (S.prof) CH_CUDA(cudaEventRecord(S.ev[3], S.stream));
-  k_ch_correct<R><<<dim3(S.mom_blocks, 4), kT, 0, S.stream>>>(H, (const R *)V.x);
+  k_ch_correct<R><<<dim3(4 * S.chunks), kT, 0, S.stream>>>(H, (const R *)V.x, S.chunk_per);
   CH_CUDA(cudaGetLastError());
   if (S.prof) CH_CUDA(cudaEventRecord(S.ev[4], S.stream));
   if (!(flags & 2)) cht_energy_step(S.cht, S.prm.alpha_t, S.prm.t_tol, S.prm.t_maxiter);
@@ -1475,12 +1499,26 @@ ChannelState *ch_create(const Case &c, const ChParams &p, int device) {
   S->scratch = S->alloc<double>(np);
   if (S->mixed) setup_mg(*S, S->Gf, S->Vf);
   else setup_mg(*S, S->Gd, S->Vd);
-  S->mom_blocks = blocks_for((long long)(S->N0 + 1) * (S->N1 + 1) * (S->N2 + 1));
-  S->mom_part = S->alloc<double>((size_t)3 * S->mom_blocks);
-  S->cont_part = S->alloc<double>((size_t)S->mom_blocks);
-  S->res = S->alloc<double>(4);
   int per = 0, nsm = 0;
   CH_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
+  // momentum: a grid resident at once (its three components of a chunk of
+  // faces in consecutive blocks then march through the z-planes together:
+  // 0.71 -> 0.66 ms per FP64 momentum solve at 256x128x128 against 3 x 1184
+  // blocks); every instantiation holds four blocks per SM (launch bounds)
+  const long long nmax = (long long)(S->N0 + 1) * (S->N1 + 1) * (S->N2 + 1);  // >= any part's element count
+  CH_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+      &per, S->mixed ? (const void *)k_ch_mom<float, 0> : (const void *)k_ch_mom<double, 0>, kT, 0));
+  S->mom_blocks = std::min(blocks_for(nmax), std::max(1, per * nsm / 3));
+  S->mom_part = S->alloc<double>((size_t)3 * S->mom_blocks);
+  S->res = S->alloc<double>(4);
+  S->asm_blocks = blocks_for(nmax);
+  S->cont_part = S->alloc<double>((size_t)S->asm_blocks);
+  // the four-part correction: at least 148 x 8 chunks per part (fewer on a
+  // small grid), each thread taking at most 32 elements, so that the last
+  // wave of blocks is short on large grids too
+  const long long span = (long long)kT * blocks_for(nmax);
+  S->chunk_per = (int)std::min<long long>(32, (nmax + span - 1) / span);
+  S->chunks = (int)((nmax + (long long)kT * S->chunk_per - 1) / ((long long)kT * S->chunk_per));
   // the V-cycle's staging of block 0's levels: up to kMgStageTotal bytes per launch
   const void *pk = S->mixed ? (const void *)k_ch_pcg<float> : (const void *)k_ch_pcg<double>;
   CH_CUDA(cudaFuncSetAttribute(pk, cudaFuncAttributeMaxDynamicSharedMemorySize, mg::kMgStageTotal));
