@@ -105,46 +105,63 @@ def hbm_peak():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons during the timed region."""
+    """nvidia-smi clocks and throttle reasons during the timed region: one
+    nvidia-smi process in its loop mode (a sample every 100 ms), started
+    before the region; start() returns once its first sample is in (at most
+    3 s), and stop() keeps the samples taken after that."""
+
+    QUERY = ("clocks.sm,clocks.max.sm,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
 
     def __init__(self, index):
         self.index = index
         self.samples = []
-        self._stop = threading.Event()
+        self._proc = None
         self._th = None
+        self._t0 = 0.0
 
     def start(self):
-        q = ("clocks.sm,clocks.max.sm,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
-             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
-             "clocks_event_reasons.sw_power_cap")
+        try:
+            self._proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.QUERY,
+                                           "--format=csv,noheader,nounits", "-lms", "100"],
+                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self._proc = None
+            return
 
         def run():
-            while not self._stop.is_set():
-                try:
-                    out = subprocess.run(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + q,
-                                          "--format=csv,noheader,nounits"], capture_output=True, text=True,
-                                         timeout=5).stdout.strip()
-                    if out:
-                        self.samples.append([x.strip() for x in out.split(",")])
-                except Exception:
-                    pass
-                self._stop.wait(0.2)
+            for line in self._proc.stdout:
+                f = [x.strip() for x in line.strip().split(",")]
+                if len(f) >= 7:
+                    self.samples.append((time.perf_counter(), f))
 
         self._th = threading.Thread(target=run, daemon=True)
         self._th.start()
+        t_end = time.perf_counter() + 3.0
+        while not self.samples and time.perf_counter() < t_end and self._proc.poll() is None:
+            time.sleep(0.01)
+        self._t0 = time.perf_counter()
 
     def stop(self):
-        self._stop.set()
-        if self._th:
-            self._th.join(timeout=10)
-        if not self.samples:
+        if self._proc is not None:
+            self._proc.terminate()
+            try:
+                self._proc.wait(timeout=5)
+            except Exception:
+                self._proc.kill()
+            if self._th:
+                self._th.join(timeout=5)
+        region = [f for t, f in self.samples if t >= self._t0] or [f for t, f in self.samples]
+        if not region:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = sorted(float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit())
-        mx = max(float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit())
+        num = lambda v: v.replace(".", "").isdigit()  # noqa: E731
+        sm = sorted(float(f[0]) for f in region if num(f[0]))
+        mxs = [float(f[1]) for f in region if num(f[1])]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[3 + i].strip() == "Active"})
-        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": mx, "reasons": reasons,
-                "samples": len(self.samples)}
+        reasons = sorted({names[i] for f in region for i in range(4) if f[3 + i] == "Active"})
+        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": max(mxs) if mxs else None,
+                "reasons": reasons, "samples": len(region)}
 
 
 def pcg_bytes(ncell, iters, wbytes=8, sweeps=MG_SWEEPS):
