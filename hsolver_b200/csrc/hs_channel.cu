@@ -750,6 +750,155 @@ __device__ void mg_fine_and_rhs(const CgVec<M> &V, const mg::Level<M> &L0, doubl
   }
 }
 
+// The mixed form's two CG passes by runs of W consecutive padded cells of
+// an interior row per thread step (W = 2 or 4; aligned: the row pitch is a
+// multiple of four values), with 8- or 16-byte loads and stores: a fraction
+// 1/W of the load and store instructions of the per-cell passes, whose FP32
+// form was bound by them rather than by DRAM bytes.  Lanes outside the
+// interior (the ghost cells and the row's padding) compute from in-bounds
+// loads and store the zeros those cells hold.  Every interior cell's
+// arithmetic is the per-cell pass's, term for term; only the order of this
+// thread's dot-product terms differs.  Mixed p' solve per outer step at
+// 256x128x128: 3.39 ms per cell, 3.15 ms with W = 2, 3.11 ms with W = 4
+// (which spills 64 bytes at the kernel's 96 registers, and is still faster).
+constexpr int kCgRun = 4;
+
+template <int W>
+__device__ __forceinline__ void ldv(float (&v)[W], const float *p, bool cg_) {
+  if constexpr (W == 4) {
+    const float4 t = cg_ ? __ldcg(reinterpret_cast<const float4 *>(p)) : *reinterpret_cast<const float4 *>(p);
+    v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
+  } else {
+    const float2 t = cg_ ? __ldcg(reinterpret_cast<const float2 *>(p)) : *reinterpret_cast<const float2 *>(p);
+    v[0] = t.x; v[1] = t.y;
+  }
+}
+template <int W>
+__device__ __forceinline__ void stv(float *p, const float (&v)[W]) {
+  if constexpr (W == 4) *reinterpret_cast<float4 *>(p) = make_float4(v[0], v[1], v[2], v[3]);
+  else *reinterpret_cast<float2 *>(p) = make_float2(v[0], v[1]);
+}
+// p = z + beta p_old (or z in the first iteration) at the run q0
+template <int W>
+__device__ __forceinline__ void p_run(float (&v)[W], const float *zs, const float *po, int q0, bool first, float bm) {
+  ldv<W>(v, zs + q0, true);
+  if (!first) {
+    float o[W];
+    ldv<W>(o, po + q0, true);
+#pragma unroll
+    for (int c = 0; c < W; ++c) v[c] = v[c] + bm * o[c];
+  }
+}
+__device__ __forceinline__ float p_one(const float *zs, const float *po, int q, bool first, float bm) {
+  const float z = __ldcg(zs + q);
+  return first ? z : z + bm * __ldcg(po + q);
+}
+
+// s = A p with the new p formed on the way (k_ch_pcg's first pass); returns
+// this thread's share of <s, p>
+template <int W>
+__device__ double cg_ap_runs(const CgVec<float> &V, const float *zs, const float *po, float *pn, bool first, float bm,
+                             int tid, int T) {
+  const int N0 = V.N0, PX = V.px, PY = V.N1 + 2, PXY = V.px * (V.N1 + 2);
+  double acc = 0.0;
+  for (mg::Walk w(PX / W, V.N1, V.N2, tid, T); w.ok(); w.next()) {
+    const int q0 = W * w.m + PX * ((w.j + 1) + PY * (w.k + 1));
+    // the sums d = cw + ce + cs + cn + cb + cf and o = cw pW + ce pE + cs pS
+    // + cn pN + cb pB + cf pF built up in that order, one neighbour run at a
+    // time (fewer values live at once)
+    float pc[W + 2], g[W + 1], v[W], h[W];
+    double d[W], o[W];
+    p_run<W>(v, zs, po, q0, first, bm);
+    pc[0] = p_one(zs, po, q0 - 1, first, bm);
+#pragma unroll
+    for (int c = 0; c < W; ++c) pc[c + 1] = v[c];
+    pc[W + 1] = p_one(zs, po, q0 + W, first, bm);
+    ldv<W>(v, V.acx + q0, false);
+#pragma unroll
+    for (int c = 0; c < W; ++c) g[c] = v[c];
+    g[W] = V.acx[q0 + W];
+#pragma unroll
+    for (int c = 0; c < W; ++c) {
+      d[c] = (double)g[c] + (double)g[c + 1];
+      o[c] = (double)g[c] * (double)pc[c] + (double)g[c + 1] * (double)pc[c + 2];
+    }
+    p_run<W>(v, zs, po, q0 - PX, first, bm);
+    ldv<W>(h, V.acy + q0, false);
+#pragma unroll
+    for (int c = 0; c < W; ++c) { d[c] = d[c] + (double)h[c]; o[c] = o[c] + (double)h[c] * (double)v[c]; }
+    p_run<W>(v, zs, po, q0 + PX, first, bm);
+    ldv<W>(h, V.acy + q0 + PX, false);
+#pragma unroll
+    for (int c = 0; c < W; ++c) { d[c] = d[c] + (double)h[c]; o[c] = o[c] + (double)h[c] * (double)v[c]; }
+    p_run<W>(v, zs, po, q0 - PXY, first, bm);
+    ldv<W>(h, V.acz + q0, false);
+#pragma unroll
+    for (int c = 0; c < W; ++c) { d[c] = d[c] + (double)h[c]; o[c] = o[c] + (double)h[c] * (double)v[c]; }
+    p_run<W>(v, zs, po, q0 + PXY, first, bm);
+    ldv<W>(h, V.acz + q0 + PXY, false);
+    float pv[W], sv[W];
+#pragma unroll
+    for (int c = 0; c < W; ++c) {
+      d[c] = d[c] + (double)h[c];
+      o[c] = o[c] + (double)h[c] * (double)v[c];
+      const int i = W * w.m + c;  // padded x
+      const bool in = i >= 1 && i <= N0;
+      const float p0 = pc[c + 1];
+      const double s_ = d[c] * (double)p0 - o[c];
+      pv[c] = in ? p0 : 0.0f;
+      sv[c] = in ? (float)s_ : 0.0f;
+      if (in) acc += (double)(float)s_ * (double)p0;
+    }
+    stv<W>(pn + q0, pv);
+    stv<W>(V.s + q0, sv);
+  }
+  return acc;
+}
+
+// x += alpha p, r -= alpha s and, with the V-cycle, its level-0 right-hand
+// side r and the seed of the first half-sweep (x = r / d on colour 0; colour
+// 1, which the next half-sweep writes before any pass reads it, gets 0);
+// returns this thread's share of <r, r>
+template <int W>
+__device__ double cg_update_runs(const CgVec<float> &V, const mg::Level<float> &L0, bool pre, const float *pn,
+                                 double alpha, int tid, int T) {
+  const int N0 = V.N0, PX = V.px, PY = V.N1 + 2;
+  double acc = 0.0;
+  for (mg::Walk w(PX / W, V.N1, V.N2, tid, T); w.ok(); w.next()) {
+    const int q0 = W * w.m + PX * ((w.j + 1) + PY * (w.k + 1));
+    float xv[W], pv[W], rv[W], sv[W], dv[W];
+    ldv<W>(xv, V.x + q0, false);
+    ldv<W>(pv, pn + q0, false);
+    ldv<W>(rv, V.r + q0, false);
+    ldv<W>(sv, V.s + q0, false);
+    if (pre) ldv<W>(dv, L0.d + q0, false);
+    else
+#pragma unroll
+      for (int c = 0; c < W; ++c) dv[c] = 0.0f;
+    float xo[W], ro[W], sx[W];
+#pragma unroll
+    for (int c = 0; c < W; ++c) {
+      const int i = W * w.m + c;
+      const bool in = i >= 1 && i <= N0;
+      const float xn = (float)((double)xv[c] + alpha * (double)pv[c]);
+      const float rn = (float)((double)rv[c] - alpha * (double)sv[c]);
+      xo[c] = in ? xn : xv[c];
+      ro[c] = in ? rn : rv[c];
+      if (in) acc += (double)rn * (double)rn;
+      const bool red = in && !(((i - 1) + w.j + w.k) & 1);
+      sx[c] = red ? (dv[c] == 0.0f ? 0.0f : rn / dv[c]) : 0.0f;
+      rv[c] = in ? rn : 0.0f;
+    }
+    stv<W>(V.x + q0, xo);
+    stv<W>(V.r + q0, ro);
+    if (pre) {
+      stv<W>(L0.rhs + q0, rv);
+      stv<W>(L0.x + q0, sx);
+    }
+  }
+  return acc;
+}
+
 // PCG: r = b (assembled), x = 0; z = M r (V-cycle, or z = r when precond = 0);
 // s = A p, alpha = <r,z>/<s,p>, x += alpha p, r -= alpha s, stop on ||r||/||b|| < tol.
 // The update p = z + beta p is done inside the product A p (each thread
@@ -805,7 +954,8 @@ __global__ void __launch_bounds__(PcgT<M>::v, 1) k_ch_pcg(CgVec<M> V, mg::Hier<M
     };
     // p in storage precision; the product in FP64 (in FP32 its cancellation
     // error for smooth p would reach the near-null modes of the p' system)
-    for (mg::Walk w(N0, N1, V.N2, tid, T); w.ok(); w.next()) {
+    if constexpr (is_mixed(M())) acc = cg_ap_runs<kCgRun>(V, precond ? L0.x : V.r, po, pn, first, bm, tid, T);
+    else for (mg::Walk w(N0, N1, V.N2, tid, T); w.ok(); w.next()) {
       const int q = (w.m + 1) + PX * ((w.j + 1) + PY * (w.k + 1));
       const M p0 = pval(q);
       const double cw = V.acx[q], ce = V.acx[q + 1], cs = V.acy[q], cn = V.acy[q + PX], cb = V.acz[q], cf = V.acz[q + PXY];
@@ -820,7 +970,8 @@ __global__ void __launch_bounds__(PcgT<M>::v, 1) k_ch_pcg(CgVec<M> V, mg::Hier<M
     if (sp == 0.0) break;
     const double alpha = gamma / sp;
     acc = 0.0;
-    for (mg::Walk w(N0, N1, V.N2, tid, T); w.ok(); w.next()) {
+    if constexpr (is_mixed(M())) acc = cg_update_runs<kCgRun>(V, L0, precond != 0, pn, alpha, tid, T);
+    else for (mg::Walk w(N0, N1, V.N2, tid, T); w.ok(); w.next()) {
       const int q = (w.m + 1) + PX * ((w.j + 1) + PY * (w.k + 1));
       const double xv = (double)V.x[q], pv = (double)pn[q], r0 = (double)V.r[q], sv = (double)V.s[q];
       const mg::Seed<M> sd = precond ? mg::seed_at(L0, w.m, w.j, w.k, q, false) : mg::Seed<M>{};
