@@ -36,3 +36,39 @@ def test_kernel_classes_fractions():
         gbs = b / (phases[k] * 1e-3) / 1e9
         assert kc[k]["achieved_gbs"] == pytest.approx(gbs), k
         assert kc[k]["frac"] == pytest.approx(gbs / 6650.0), k
+
+
+def _fake_smi(tmp_path, lines):
+    """An nvidia-smi stand-in that prints the given CSV lines in a loop every
+    50 ms, as `nvidia-smi --query-gpu=... -lms` does."""
+    script = tmp_path / "nvidia-smi"
+    body = "".join("echo '%s'\n" % ln for ln in lines)
+    script.write_text("#!/bin/bash\nwhile true; do\n%s sleep 0.05\ndone\n" % body)
+    script.chmod(0o755)
+    return str(tmp_path)
+
+
+def test_clock_sampler_reads_the_loop(tmp_path, monkeypatch):
+    """bench.ClockSampler keeps the samples taken inside the timed region
+    (median SM clock, the maximum, the throttle reasons that were active)."""
+    import os
+    import time
+    d = _fake_smi(tmp_path, ["1965, 1965, 0x0000000000000000, Not Active, Not Active, Not Active, Not Active",
+                             "1800, 1965, 0x0000000000000004, Not Active, Not Active, Not Active, Active"])
+    monkeypatch.setenv("PATH", d + os.pathsep + os.environ["PATH"])
+    c = bench.ClockSampler(0)
+    c.start()
+    time.sleep(0.4)
+    out = c.stop()
+    assert out["samples"] >= 2
+    assert out["sm_max_mhz"] == 1965.0
+    assert out["sm_mhz"] in (1800.0, 1965.0)
+    assert out["reasons"] == ["sw_power_cap"]
+
+
+def test_clock_sampler_without_nvidia_smi(tmp_path, monkeypatch):
+    """No nvidia-smi on the PATH: the line says the clocks went unsampled."""
+    monkeypatch.setenv("PATH", str(tmp_path))
+    c = bench.ClockSampler(0)
+    c.start()
+    assert c.stop() == {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
