@@ -104,62 +104,114 @@ def hbm_peak():
         return FALLBACK_HBM_GBS, "fallback"
 
 
+def _nvml_open(index):
+    """NVML and the handle of CUDA device `index` (found by its PCI address,
+    since NVML numbers the GPUs without regard to CUDA_VISIBLE_DEVICES)."""
+    import pynvml
+    import torch
+    pynvml.nvmlInit()
+    pr = torch.cuda.get_device_properties(index)
+    try:
+        h = pynvml.nvmlDeviceGetHandleByPciBusId("%08X:%02X:%02X.0" % (pr.pci_domain_id, pr.pci_bus_id, pr.pci_device_id))
+    except Exception:
+        u = str(pr.uuid)
+        h = pynvml.nvmlDeviceGetHandleByUUID(u if u.startswith("GPU-") else "GPU-" + u)
+    return pynvml, h
+
+
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons during the timed region: one
-    nvidia-smi process in its loop mode (a sample every 100 ms), started
-    before the region; start() returns once its first sample is in (at most
-    3 s), and stop() keeps the samples taken after that."""
+    """SM clocks and throttle reasons during the timed region: read through
+    NVML every 10 ms by a thread (reading only), or, where NVML cannot be
+    opened, from one nvidia-smi process in its loop mode (every 100 ms;
+    start() then returns once its first sample is in, at most 3 s, and only
+    later samples are kept)."""
 
     QUERY = ("clocks.sm,clocks.max.sm,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
              "clocks_event_reasons.sw_power_cap")
+    REASONS = (("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40), ("sw_thermal_slowdown", 0x20),
+               ("sw_power_cap", 0x4))
 
     def __init__(self, index):
         self.index = index
-        self.samples = []
+        self.samples = []  # (time, sm MHz, max MHz, [reason names])
         self._proc = None
         self._th = None
+        self._stop = threading.Event()
         self._t0 = 0.0
 
-    def start(self):
-        try:
-            self._proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.QUERY,
-                                           "--format=csv,noheader,nounits", "-lms", "100"],
-                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-        except Exception:
-            self._proc = None
-            return
+    def _start_nvml(self):
+        nv, h = _nvml_open(self.index)
+        mx = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+        get_reasons = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+            nv.nvmlDeviceGetCurrentClocksThrottleReasons
+
+        def sample():
+            sm = float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM))
+            bits = int(get_reasons(h))
+            self.samples.append((time.perf_counter(), sm, mx, [n for n, b in self.REASONS if bits & b]))
+
+        sample()  # fails here, before the thread, if NVML cannot read the device
+
+        def run():
+            while not self._stop.wait(0.01):
+                try:
+                    sample()
+                except Exception:
+                    return
+
+        self._th = threading.Thread(target=run, daemon=True)
+        self._th.start()
+
+    def _start_smi(self):
+        self._proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.QUERY,
+                                       "--format=csv,noheader,nounits", "-lms", "100"],
+                                      stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        num = lambda v: float(v) if v.replace(".", "").isdigit() else None  # noqa: E731
 
         def run():
             for line in self._proc.stdout:
                 f = [x.strip() for x in line.strip().split(",")]
                 if len(f) >= 7:
-                    self.samples.append((time.perf_counter(), f))
+                    self.samples.append((time.perf_counter(), num(f[0]), num(f[1]),
+                                         [n for (n, _), v in zip(self.REASONS, f[3:7]) if v == "Active"]))
 
         self._th = threading.Thread(target=run, daemon=True)
         self._th.start()
         t_end = time.perf_counter() + 3.0
         while not self.samples and time.perf_counter() < t_end and self._proc.poll() is None:
             time.sleep(0.01)
+
+    def start(self):
+        try:
+            self._start_nvml()
+        except Exception:
+            self.samples = []
+            try:
+                self._start_smi()
+            except Exception:
+                self._proc = None
         self._t0 = time.perf_counter()
 
     def stop(self):
+        self._stop.set()
         if self._proc is not None:
             self._proc.terminate()
             try:
                 self._proc.wait(timeout=5)
             except Exception:
                 self._proc.kill()
-            if self._th:
-                self._th.join(timeout=5)
-        region = [f for t, f in self.samples if t >= self._t0] or [f for t, f in self.samples]
+        if self._th:
+            self._th.join(timeout=5)
+        # the samples taken in the region (or, for a region shorter than the
+        # sampling interval, the last one before it)
+        region = [x for x in self.samples if x[0] >= self._t0] or \
+            [x for x in self.samples if x[0] < self._t0][-1:]
         if not region:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        num = lambda v: v.replace(".", "").isdigit()  # noqa: E731
-        sm = sorted(float(f[0]) for f in region if num(f[0]))
-        mxs = [float(f[1]) for f in region if num(f[1])]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for f in region for i in range(4) if f[3 + i] == "Active"})
+        sm = sorted(x[1] for x in region if x[1] is not None)
+        mxs = [x[2] for x in region if x[2] is not None]
+        reasons = sorted({n for x in region for n in x[3]})
         return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": max(mxs) if mxs else None,
                 "reasons": reasons, "samples": len(region)}
 

@@ -72,3 +72,36 @@ def test_clock_sampler_without_nvidia_smi(tmp_path, monkeypatch):
     c = bench.ClockSampler(0)
     c.start()
     assert c.stop() == {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+
+
+def test_clock_sampler_nvml(monkeypatch):
+    """The NVML path: SM clock and the clock-event bit mask read every 10 ms,
+    the reasons named from the mask."""
+    import time
+
+    class FakeNvml:
+        NVML_CLOCK_SM = 1
+
+        def __init__(self):
+            self.n = 0
+
+        def nvmlDeviceGetMaxClockInfo(self, h, which):
+            return 1965
+
+        def nvmlDeviceGetClockInfo(self, h, which):
+            self.n += 1
+            return 1965 if self.n % 2 else 1800
+
+        def nvmlDeviceGetCurrentClocksEventReasons(self, h):
+            return 0x4 | 0x1  # sw_power_cap, idle
+
+    fake = FakeNvml()
+    monkeypatch.setattr(bench, "_nvml_open", lambda index: (fake, object()))
+    c = bench.ClockSampler(0)
+    c.start()
+    time.sleep(0.2)
+    out = c.stop()
+    assert out["samples"] >= 5
+    assert out["sm_max_mhz"] == 1965.0
+    assert out["sm_mhz"] in (1800.0, 1965.0)
+    assert out["reasons"] == ["sw_power_cap"]
